@@ -1,0 +1,112 @@
+/*
+ * agocuda.h -- C ABI of the B200 (sm_100a) kernels behind the OpenVX/AGO vision-graph
+ * target.  This is the device-launch boundary: one entry point per AGO low-level kernel,
+ * mirroring the reference's HIP launch layer (amd_openvx/openvx/hipvx/hip_host_decls.h,
+ * `HipExec_<Kernel>`): a stream, the destination size, device pointers with byte strides,
+ * then kernel parameters; every entry returns 0 on success, -10 for invalid parameters,
+ * or the positive cudaError_t of a failed launch.
+ *
+ * Semantics follow the reference's CPU ("HAF") kernels as called by the AGO kernel
+ * wrappers (amd_openvx/openvx/ago/ago_kernel_api.cpp): destination pointers address the
+ * full image (row 0), and 3x3 stencils write the interior rows [1, H-1) -- exactly the rows
+ * the AGO CPU wrapper processes -- so every pixel inside the OpenVX valid region is
+ * bit-identical to the reference.  Pixels outside the valid region are unspecified
+ * (OpenVX border mode UNDEFINED).
+ *
+ * All pointers are device pointers (or pointers the device can dereference).  Streams are
+ * passed as `void *` holding a cudaStream_t (NULL = legacy default stream).
+ */
+#ifndef AGOCUDA_H
+#define AGOCUDA_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------ */
+/* Library information                                                                   */
+/* ------------------------------------------------------------------------------------ */
+
+/* Version of this C ABI (major*10000 + minor*100 + patch). */
+int agocuda_abi_version(void);
+/* Number of device kernels this library has launched since load (all entry points). */
+uint64_t agocuda_launch_count(void);
+
+/* ------------------------------------------------------------------------------------ */
+/* Filters (reference: hipvx/hip_host_decls.h filter_kernels)                            */
+/* ------------------------------------------------------------------------------------ */
+
+/* 3x3 Gaussian [1 2 1]^T[1 2 1] / 16.  Replaces HipExec_Gaussian_U8_U8_3x3
+ * (hipvx/hip_host_decls.h:649); CPU semantics of HafCpu_Gaussian_U8_U8_3x3
+ * (ago/ago_haf_cpu_filter.cpp:1518) as called at ago/ago_kernel_api.cpp:15281. */
+int agocuda_Gaussian_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                               uint8_t *pDst, uint32_t dstStride,
+                               const uint8_t *pSrc, uint32_t srcStride);
+
+/* 3x3 Sobel gradients, S16.  Replaces HipExec_Sobel_S16S16_U8_3x3_GXY
+ * (hipvx/hip_host_decls.h:663); HafCpu_Sobel_S16S16_U8_3x3_GXY (ago_haf_cpu_filter.cpp:2237). */
+int agocuda_Sobel_S16S16_U8_3x3_GXY(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                    int16_t *pGx, uint32_t gxStride, int16_t *pGy, uint32_t gyStride,
+                                    const uint8_t *pSrc, uint32_t srcStride);
+
+/* Sobel 3x3 + L2 magnitude (the node AGO's SOBEL+MAGNITUDE merge rule produces,
+ * ago/ago_drama_remove.cpp:165).  HafCpu_SobelMagnitude_S16_U8_3x3
+ * (ago_haf_cpu_filter.cpp:2468): SIMD body rounds sqrt to nearest even, the scalar
+ * prefix/tail (decided from the row-1 destination address, as the reference does)
+ * truncate.  The reference HIP layer has no counterpart (the merged node ran on CPU). */
+int agocuda_SobelMagnitude_S16_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                      int16_t *pDst, uint32_t dstStride,
+                                      const uint8_t *pSrc, uint32_t srcStride);
+
+/* ------------------------------------------------------------------------------------ */
+/* Arithmetic (reference: hipvx/hip_host_decls.h arithmetic/color kernels)              */
+/* ------------------------------------------------------------------------------------ */
+
+/* Replaces HipExec_Magnitude_S16_S16S16 (hipvx/hip_host_decls.h:219);
+ * HafCpu_Magnitude_S16_S16S16 (ago_haf_cpu_arithmetic.cpp:4989).  Processes all rows. */
+int agocuda_Magnitude_S16_S16S16(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                 int16_t *pMag, uint32_t magStride,
+                                 const int16_t *pGx, uint32_t gxStride,
+                                 const int16_t *pGy, uint32_t gyStride);
+
+/* clamp(v >> shift, 0, 255).  Replaces HipExec_ColorDepth_U8_S16_Sat
+ * (hipvx/hip_host_decls.h:403); HafCpu_ColorDepth_U8_S16_Sat (ago_haf_cpu_arithmetic.cpp:3546). */
+int agocuda_ColorDepth_U8_S16_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                  uint8_t *pDst, uint32_t dstStride,
+                                  const int16_t *pSrc, uint32_t srcStride, int32_t shift);
+
+/* v > threshold ? 255 : 0.  Replaces HipExec_Threshold_U8_U8_Binary
+ * (hipvx/hip_host_decls.h:689); HafCpu_Threshold_U8_U8_Binary (ago_haf_cpu_arithmetic.cpp:3660). */
+int agocuda_Threshold_U8_U8_Binary(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                   uint8_t *pDst, uint32_t dstStride,
+                                   const uint8_t *pSrc, uint32_t srcStride, int32_t threshold);
+
+/* ------------------------------------------------------------------------------------ */
+/* Fused multi-node kernels (no reference counterpart: the HIP target launches one kernel */
+/* per node, ago/ago_util_hip.cpp:686; agoGpuHipSuperNodeLaunch returns -1 at :740)      */
+/* ------------------------------------------------------------------------------------ */
+
+/* One frame descriptor of a batched launch.  Frames may have different sizes. */
+typedef struct agocuda_frame {
+    const uint8_t *src;    /* U8 input, row 0 */
+    uint8_t *dst;          /* U8 output, row 0 */
+    uint32_t width, height;
+    uint32_t srcStride, dstStride;
+    int32_t simdBegin, simdEnd;  /* SobelMagnitude SIMD span in columns (see above) */
+} agocuda_frame;
+
+/* Gaussian3x3 -> SobelMagnitude -> ConvertDepth(SATURATE, shift) -> Threshold(BINARY)
+ * with all intermediates virtual, in one pass over HBM (1 B/px read, 1 B/px write).
+ * Writes rows/cols [2, W-2) x [2, H-2) of dst, which is the valid region of the
+ * unfused graph, bit-identical to it.  `frames` is a DEVICE array of `numFrames`
+ * descriptors; all frames run in one launch. */
+int agocuda_fused_GaussSobelMagDepthThresh(void *stream, const agocuda_frame *frames, uint32_t numFrames,
+                                           uint32_t maxWidth, uint32_t maxHeight,
+                                           int32_t shift, int32_t threshold);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AGOCUDA_H */

@@ -1,0 +1,48 @@
+// agocuda_internal.cuh -- helpers shared by the sm_100a kernels behind include/agocuda.h.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "agocuda.h"
+
+#define AGOCUDA_INVALID_PARAMS (-10)   // same value as VX_ERROR_INVALID_PARAMETERS
+#define AGOCUDA_NO_MEMORY      (-8)    // same value as VX_ERROR_NO_MEMORY
+
+// Map the launch status to the C-ABI return convention: 0 on success, else the
+// cudaError_t (positive) of the failed launch.
+static inline int agocuda_launch_status()
+{
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+static inline cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
+
+static inline unsigned div_up(unsigned a, unsigned b) { return (a + b - 1) / b; }
+
+// The reference HAF kernels split each row into a scalar prefix (bytes up to the next
+// 16-byte boundary of the destination row pointer, used as a pixel count), a 16-wide SIMD
+// body and a scalar tail of (width - prefix) & 15 pixels, and some of them round
+// differently in the scalar parts.  This returns the column range [simd_begin, simd_end)
+// that the reference handles in its SIMD body for a destination row starting at `row`.
+struct SimdSpan { int begin, end; };
+static inline SimdSpan haf_simd_span(const void *row, int width, int lanes_mask = 15)
+{
+    int p = (int)((uintptr_t)row & 15);
+    p = p ? 16 - p : 0;
+    int post = (width - p) & lanes_mask;
+    return SimdSpan{p, width - post};
+}
+
+__device__ __forceinline__ uint32_t ldg_u32(const uint8_t *p) { return __ldg((const unsigned int *)p); }
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Load the 32-bit word that holds columns [c, c+4) of a U8 row, with c clamped into
+// [0, stride-4]; rows are clamped by the caller.  Values read through a clamp only feed
+// pixels outside the valid region, which OpenVX leaves undefined for these kernels.
+__device__ __forceinline__ uint32_t load_word_clamped(const uint8_t *row, int c, int stride)
+{
+    c = clampi(c, 0, stride - 4);
+    return ldg_u32(row + c);
+}
+
+__device__ __forceinline__ int byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xff; }

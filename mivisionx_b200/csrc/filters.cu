@@ -1,0 +1,405 @@
+// filters.cu -- 3x3 stencil kernels of the AGO vision path and the fused
+// Gaussian -> SobelMagnitude -> ConvertDepth -> Threshold chain, for sm_100a.
+//
+// Work decomposition shared by the stencil kernels here: one thread owns a 4-pixel
+// column group (one 32-bit word of a U8 row) and walks down RPT rows, keeping the
+// per-row horizontal partial sums of the rows above in registers, so each input row is
+// loaded once per thread (the neighbouring words come from L1).  A warp covers 128
+// contiguous bytes per row, so every global access is a full coalesced line.
+#include "agocuda_internal.cuh"
+#include <math.h>
+
+namespace {
+
+constexpr int kBX = 32;      // threads across: 32 x 4 px = 128 columns
+constexpr int kBY = 4;       // thread rows per block
+constexpr int kRPT = 8;      // output rows per thread
+
+// Pixels p[x-2 .. x+5] of a U8 row, for the 4-pixel group starting at x.
+struct Row8 { int p[8]; };
+__device__ __forceinline__ Row8 load_row8(const uint8_t *row, int x, int stride)
+{
+    uint32_t l = load_word_clamped(row, x - 4, stride);
+    uint32_t c = load_word_clamped(row, x, stride);
+    uint32_t r = load_word_clamped(row, x + 4, stride);
+    Row8 o;
+    o.p[0] = byte_of(l, 2); o.p[1] = byte_of(l, 3);
+    o.p[2] = byte_of(c, 0); o.p[3] = byte_of(c, 1); o.p[4] = byte_of(c, 2); o.p[5] = byte_of(c, 3);
+    o.p[6] = byte_of(r, 0); o.p[7] = byte_of(r, 1);
+    return o;
+}
+
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d)
+{
+    return (uint32_t)(a & 0xff) | ((uint32_t)(b & 0xff) << 8) | ((uint32_t)(c & 0xff) << 16) | ((uint32_t)(d & 0xff) << 24);
+}
+
+// ---------------------------------------------------------------------------------
+// Gaussian 3x3 (HafCpu_Gaussian_U8_U8_3x3, ago_haf_cpu_filter.cpp:1518)
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBX * kBY)
+k_gaussian3x3(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride)
+{
+    const int x = (blockIdx.x * kBX + threadIdx.x) * 4;
+    const int y0 = 1 + (blockIdx.y * kBY + threadIdx.y) * kRPT;
+    if (x >= W || y0 >= H - 1) return;
+    const int y1 = min(y0 + kRPT, H - 1);
+    int hm[4], hc[4];
+    {
+        Row8 a = load_row8(src + (size_t)(y0 - 1) * srcStride, x, srcStride);
+        Row8 b = load_row8(src + (size_t)y0 * srcStride, x, srcStride);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            hm[i] = a.p[i + 1] + 2 * a.p[i + 2] + a.p[i + 3];
+            hc[i] = b.p[i + 1] + 2 * b.p[i + 2] + b.p[i + 3];
+        }
+    }
+    for (int y = y0; y < y1; y++) {
+        Row8 n = load_row8(src + (size_t)(y + 1) * srcStride, x, srcStride);
+        int o[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int hn = n.p[i + 1] + 2 * n.p[i + 2] + n.p[i + 3];
+            o[i] = (hm[i] + 2 * hc[i] + hn) >> 4;
+            hm[i] = hc[i]; hc[i] = hn;
+        }
+        *(uint32_t *)(dst + (size_t)y * dstStride + x) = pack4(o[0], o[1], o[2], o[3]);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Sobel 3x3 GX/GY (HafCpu_Sobel_S16S16_U8_3x3_GXY, ago_haf_cpu_filter.cpp:2237) and
+// SobelMagnitude (HafCpu_SobelMagnitude_S16_U8_3x3, ago_haf_cpu_filter.cpp:2468).
+// Rolling state per column c in [x-1, x+4]: the row above and the current row.
+// ---------------------------------------------------------------------------------
+struct SobelRows { int a[6], b[6]; };   // pixel columns x-1..x+4 of rows y-1 and y
+
+__device__ __forceinline__ void sobel_at(const int *pa, const int *pb, const int *pc, int i, int &gx, int &gy)
+{
+    // columns i-1, i, i+1 in the 6-wide window are indices i, i+1, i+2
+    gx = (pa[i + 2] - pa[i]) + 2 * (pb[i + 2] - pb[i]) + (pc[i + 2] - pc[i]);
+    gy = (pc[i] + 2 * pc[i + 1] + pc[i + 2]) - (pa[i] + 2 * pa[i + 1] + pa[i + 2]);
+}
+
+__device__ __forceinline__ void row6(const Row8 &r, int *o)
+{
+#pragma unroll
+    for (int i = 0; i < 6; i++) o[i] = r.p[i + 1];
+}
+
+// round(sqrt(n)) to nearest for integer n in [0, 2^31): exact integer fix-up of a float
+// estimate (n is never a perfect half-square, so the rounding direction is exact).
+__device__ __forceinline__ int isqrt_round(int n)
+{
+    int m = __float2int_rn(__fsqrt_rn((float)n));
+    long long mm = (long long)m * m;
+    if ((long long)n > mm + m) m++;
+    else if (m > 0 && (long long)n <= mm - m) m--;   // for m == 0 the lower bound is n >= 0
+    return m;
+}
+
+__global__ void __launch_bounds__(kBX * kBY)
+k_sobel_gxy(int W, int H, int16_t *gxp, int gxStride, int16_t *gyp, int gyStride, const uint8_t *src, int srcStride)
+{
+    const int x = (blockIdx.x * kBX + threadIdx.x) * 4;
+    const int y0 = 1 + (blockIdx.y * kBY + threadIdx.y) * kRPT;
+    if (x >= W || y0 >= H - 1) return;
+    const int y1 = min(y0 + kRPT, H - 1);
+    int pa[6], pb[6], pc[6];
+    row6(load_row8(src + (size_t)(y0 - 1) * srcStride, x, srcStride), pa);
+    row6(load_row8(src + (size_t)y0 * srcStride, x, srcStride), pb);
+    for (int y = y0; y < y1; y++) {
+        row6(load_row8(src + (size_t)(y + 1) * srcStride, x, srcStride), pc);
+        int gx[4], gy[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) sobel_at(pa, pb, pc, i, gx[i], gy[i]);
+        uint2 vx, vy;
+        vx.x = (uint32_t)(uint16_t)gx[0] | ((uint32_t)(uint16_t)gx[1] << 16);
+        vx.y = (uint32_t)(uint16_t)gx[2] | ((uint32_t)(uint16_t)gx[3] << 16);
+        vy.x = (uint32_t)(uint16_t)gy[0] | ((uint32_t)(uint16_t)gy[1] << 16);
+        vy.y = (uint32_t)(uint16_t)gy[2] | ((uint32_t)(uint16_t)gy[3] << 16);
+        *(uint2 *)((uint8_t *)gxp + (size_t)y * gxStride + 2 * x) = vx;
+        *(uint2 *)((uint8_t *)gyp + (size_t)y * gyStride + 2 * x) = vy;
+#pragma unroll
+        for (int i = 0; i < 6; i++) { pa[i] = pb[i]; pb[i] = pc[i]; }
+    }
+}
+
+__global__ void __launch_bounds__(kBX * kBY)
+k_sobel_magnitude(int W, int H, int16_t *dst, int dstStride, const uint8_t *src, int srcStride,
+                  int simdBegin, int simdEnd)
+{
+    const int x = (blockIdx.x * kBX + threadIdx.x) * 4;
+    const int y0 = 1 + (blockIdx.y * kBY + threadIdx.y) * kRPT;
+    if (x >= W || y0 >= H - 1) return;
+    const int y1 = min(y0 + kRPT, H - 1);
+    int pa[6], pb[6], pc[6];
+    row6(load_row8(src + (size_t)(y0 - 1) * srcStride, x, srcStride), pa);
+    row6(load_row8(src + (size_t)y0 * srcStride, x, srcStride), pb);
+    for (int y = y0; y < y1; y++) {
+        row6(load_row8(src + (size_t)(y + 1) * srcStride, x, srcStride), pc);
+        int m[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int gx, gy;
+            sobel_at(pa, pb, pc, i, gx, gy);
+            int n = gx * gx + gy * gy;
+            int xi = x + i;
+            if (xi < simdBegin || xi >= simdEnd)
+                m[i] = (int)(int16_t)(int)__fsqrt_rn(__fadd_rn((float)(gx * gx), (float)(gy * gy)));
+            else
+                m[i] = min(isqrt_round(n), 65535);
+        }
+        uint2 v;
+        v.x = (uint32_t)(uint16_t)m[0] | ((uint32_t)(uint16_t)m[1] << 16);
+        v.y = (uint32_t)(uint16_t)m[2] | ((uint32_t)(uint16_t)m[3] << 16);
+        *(uint2 *)((uint8_t *)dst + (size_t)y * dstStride + 2 * x) = v;
+#pragma unroll
+        for (int i = 0; i < 6; i++) { pa[i] = pb[i]; pb[i] = pc[i]; }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Pointwise kernels: 4 pixels per thread per row, all rows.
+// ---------------------------------------------------------------------------------
+__global__ void k_magnitude(int W, int H, int16_t *mag, int magStride, const int16_t *gxp, int gxStride,
+                            const int16_t *gyp, int gyStride, int prefix, int tail)
+{
+    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    uint2 a = *(const uint2 *)((const uint8_t *)gxp + (size_t)y * gxStride + 2 * x);
+    uint2 b = *(const uint2 *)((const uint8_t *)gyp + (size_t)y * gyStride + 2 * x);
+    int ga[4] = {(int16_t)(a.x & 0xffff), (int16_t)(a.x >> 16), (int16_t)(a.y & 0xffff), (int16_t)(a.y >> 16)};
+    int gb[4] = {(int16_t)(b.x & 0xffff), (int16_t)(b.x >> 16), (int16_t)(b.y & 0xffff), (int16_t)(b.y >> 16)};
+    int m[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int xi = x + i;
+        int sa = ga[i] * ga[i], sb = gb[i] * gb[i];
+        if (xi < prefix) {
+            m[i] = (int)(int16_t)(int)__fsqrt_rn(__fadd_rn((float)sa, (float)sb));
+        } else if (xi >= tail) {
+            float t = __fsqrt_rn(__fadd_rn((float)sa, (float)sb));
+            m[i] = (int)(int16_t)(int)round((double)t);
+        } else {
+            double n = __dadd_rn((double)sa, (double)sb);
+            int r = __double2int_rn(__dsqrt_rn(n));
+            m[i] = min(r, 32767);
+        }
+    }
+    uint2 v;
+    v.x = (uint32_t)(uint16_t)m[0] | ((uint32_t)(uint16_t)m[1] << 16);
+    v.y = (uint32_t)(uint16_t)m[2] | ((uint32_t)(uint16_t)m[3] << 16);
+    *(uint2 *)((uint8_t *)mag + (size_t)y * magStride + 2 * x) = v;
+}
+
+__global__ void k_colordepth_u8_s16_sat(int W, int H, uint8_t *dst, int dstStride, const int16_t *src, int srcStride, int shift)
+{
+    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    uint2 a = *(const uint2 *)((const uint8_t *)src + (size_t)y * srcStride + 2 * x);
+    int v[4] = {(int16_t)(a.x & 0xffff), (int16_t)(a.x >> 16), (int16_t)(a.y & 0xffff), (int16_t)(a.y >> 16)};
+#pragma unroll
+    for (int i = 0; i < 4; i++) v[i] = clampi(v[i] >> shift, 0, 255);
+    *(uint32_t *)(dst + (size_t)y * dstStride + x) = pack4(v[0], v[1], v[2], v[3]);
+}
+
+__global__ void k_threshold_u8_binary(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride, int thr)
+{
+    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    uint32_t a = ldg_u32(src + (size_t)y * srcStride + x);
+    int o[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) o[i] = byte_of(a, i) > thr ? 255 : 0;
+    *(uint32_t *)(dst + (size_t)y * dstStride + x) = pack4(o[0], o[1], o[2], o[3]);
+}
+
+// ---------------------------------------------------------------------------------
+// Fused Gaussian3x3 -> SobelMagnitude -> ColorDepth(SAT, shift) -> Threshold(BINARY, t).
+// ColorDepth and Threshold collapse into one comparison on n = gx^2 + gy^2: with
+// M = (t + 1) << shift, clamp(mag >> shift, 0, 255) > t  <=>  mag >= M, and
+//   SIMD body:  round(sqrt(n)) >= M   <=>  n >= M*M - M + 1
+//   scalar tail: trunc(sqrtf(n)) >= M <=>  n >= M*M
+// (n < 2^22 here, so sqrtf is exact enough for the second equivalence).
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBX * kBY)
+k_fused_gauss_sobelmag_thresh(const agocuda_frame *frames, int nRound, int nTrunc)
+{
+    const agocuda_frame f = frames[blockIdx.z];
+    const int W = (int)f.width, H = (int)f.height;
+    const int x = (blockIdx.x * kBX + threadIdx.x) * 4;
+    const int y0 = 2 + (blockIdx.y * kBY + threadIdx.y) * kRPT;
+    if (x >= W || y0 >= H - 2) return;
+    const int y1 = min(y0 + kRPT, H - 2);
+    const int ss = (int)f.srcStride;
+    const uint8_t *src = f.src;
+    // Gaussian of rows r-1, r (columns x-1..x+4) and horizontal sums of input rows.
+    int h0[6], h1[6], g0[6], g1[6];
+    {
+        Row8 a = load_row8(src + (size_t)(y0 - 2) * ss, x, ss);
+        Row8 b = load_row8(src + (size_t)(y0 - 1) * ss, x, ss);
+        Row8 c = load_row8(src + (size_t)(y0) * ss, x, ss);
+        int ha[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            ha[i] = a.p[i] + 2 * a.p[i + 1] + a.p[i + 2];
+            h0[i] = b.p[i] + 2 * b.p[i + 1] + b.p[i + 2];
+            h1[i] = c.p[i] + 2 * c.p[i + 1] + c.p[i + 2];
+            g0[i] = (ha[i] + 2 * h0[i] + h1[i]) >> 4;   // Gaussian row y0-1
+        }
+        Row8 d = load_row8(src + (size_t)(y0 + 1) * ss, x, ss);
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            int hd = d.p[i] + 2 * d.p[i + 1] + d.p[i + 2];
+            g1[i] = (h0[i] + 2 * h1[i] + hd) >> 4;      // Gaussian row y0
+            h0[i] = h1[i]; h1[i] = hd;
+        }
+    }
+    for (int y = y0; y < y1; y++) {
+        Row8 n = load_row8(src + (size_t)(y + 2) * ss, x, ss);
+        int g2[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            int hn = n.p[i] + 2 * n.p[i + 1] + n.p[i + 2];
+            g2[i] = (h0[i] + 2 * h1[i] + hn) >> 4;      // Gaussian row y+1
+            h0[i] = h1[i]; h1[i] = hn;
+        }
+        int o[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int gx, gy;
+            sobel_at(g0, g1, g2, i, gx, gy);
+            int nn = gx * gx + gy * gy;
+            int xi = x + i;
+            int T = (xi < f.simdBegin || xi >= f.simdEnd) ? nTrunc : nRound;
+            o[i] = nn >= T ? 255 : 0;
+        }
+        *(uint32_t *)(f.dst + (size_t)y * f.dstStride + x) = pack4(o[0], o[1], o[2], o[3]);
+#pragma unroll
+        for (int i = 0; i < 6; i++) { g0[i] = g1[i]; g1[i] = g2[i]; }
+    }
+}
+
+unsigned long long g_launches = 0;
+
+bool aligned(const void *p, unsigned a) { return ((uintptr_t)p & (a - 1)) == 0; }
+
+// Vector paths need the row base aligned to the word size, the stride a multiple of it
+// and at least one full row of pixels.
+bool bad_plane(const void *p, uint32_t stride, uint32_t W, unsigned bpp, unsigned word)
+{
+    return !p || !aligned(p, word) || (stride % word) || stride < W * bpp;
+}
+
+}  // namespace
+
+uint64_t agocuda_count_launch(unsigned n) { return __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
+
+extern "C" uint64_t agocuda_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+extern "C" int agocuda_abi_version(void) { return 100; }
+
+static dim3 stencil_grid(uint32_t W, uint32_t rows)
+{
+    return dim3(div_up(W, kBX * 4), div_up(rows, kBY * kRPT), 1);
+}
+
+extern "C" int agocuda_Gaussian_U8_U8_3x3(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                          const uint8_t *pSrc, uint32_t srcStride)
+{
+    if (W < 3 || H < 3 || bad_plane(pDst, dstStride, W, 1, 4) || bad_plane(pSrc, srcStride, W, 1, 4))
+        return AGOCUDA_INVALID_PARAMS;
+    k_gaussian3x3<<<stencil_grid(W, H - 2), dim3(kBX, kBY), 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_Sobel_S16S16_U8_3x3_GXY(void *stream, uint32_t W, uint32_t H, int16_t *pGx, uint32_t gxStride,
+                                               int16_t *pGy, uint32_t gyStride, const uint8_t *pSrc, uint32_t srcStride)
+{
+    if (W < 3 || H < 3 || bad_plane(pGx, gxStride, W, 2, 8) || bad_plane(pGy, gyStride, W, 2, 8) ||
+        bad_plane(pSrc, srcStride, W, 1, 4))
+        return AGOCUDA_INVALID_PARAMS;
+    k_sobel_gxy<<<stencil_grid(W, H - 2), dim3(kBX, kBY), 0, as_stream(stream)>>>((int)W, (int)H, pGx, (int)gxStride, pGy, (int)gyStride, pSrc, (int)srcStride);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_SobelMagnitude_S16_U8_3x3(void *stream, uint32_t W, uint32_t H, int16_t *pDst, uint32_t dstStride,
+                                                 const uint8_t *pSrc, uint32_t srcStride)
+{
+    if (W < 3 || H < 3 || bad_plane(pDst, dstStride, W, 2, 8) || bad_plane(pSrc, srcStride, W, 1, 4))
+        return AGOCUDA_INVALID_PARAMS;
+    SimdSpan sp = haf_simd_span((const uint8_t *)pDst + dstStride, (int)W);
+    k_sobel_magnitude<<<stencil_grid(W, H - 2), dim3(kBX, kBY), 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride, sp.begin, sp.end);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_Magnitude_S16_S16S16(void *stream, uint32_t W, uint32_t H, int16_t *pMag, uint32_t magStride,
+                                            const int16_t *pGx, uint32_t gxStride, const int16_t *pGy, uint32_t gyStride)
+{
+    if (!W || !H || bad_plane(pMag, magStride, W, 2, 8) || bad_plane(pGx, gxStride, W, 2, 8) ||
+        bad_plane(pGy, gyStride, W, 2, 8))
+        return AGOCUDA_INVALID_PARAMS;
+    // HafCpu_Magnitude_S16_S16S16 (ago_haf_cpu_arithmetic.cpp:4989): prefix in pixels
+    // from the destination's 16-byte misalignment, 8-wide SIMD body.
+    int prefix = (int)((uintptr_t)pMag & 15);
+    prefix = (prefix ? 16 - prefix : 0) >> 1;
+    int tail = (int)W - (((int)W - prefix) & 7);
+    dim3 blk(32, 8);
+    dim3 grd(div_up(W, 128), div_up(H, 8));
+    k_magnitude<<<grd, blk, 0, as_stream(stream)>>>((int)W, (int)H, pMag, (int)magStride, pGx, (int)gxStride, pGy, (int)gyStride, prefix, tail);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_ColorDepth_U8_S16_Sat(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                             const int16_t *pSrc, uint32_t srcStride, int32_t shift)
+{
+    if (!W || !H || bad_plane(pDst, dstStride, W, 1, 4) || bad_plane(pSrc, srcStride, W, 2, 8) ||
+        shift < 0 || shift > 15)
+        return AGOCUDA_INVALID_PARAMS;
+    dim3 blk(32, 8);
+    dim3 grd(div_up(W, 128), div_up(H, 8));
+    k_colordepth_u8_s16_sat<<<grd, blk, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride, shift);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_Threshold_U8_U8_Binary(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                              const uint8_t *pSrc, uint32_t srcStride, int32_t threshold)
+{
+    if (!W || !H || bad_plane(pDst, dstStride, W, 1, 4) || bad_plane(pSrc, srcStride, W, 1, 4))
+        return AGOCUDA_INVALID_PARAMS;
+    dim3 blk(32, 8);
+    dim3 grd(div_up(W, 128), div_up(H, 8));
+    // The reference passes the threshold as vx_uint8 (threshold_value.U1).
+    k_threshold_u8_binary<<<grd, blk, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride, (int)(uint8_t)threshold);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_fused_GaussSobelMagDepthThresh(void *stream, const agocuda_frame *frames, uint32_t numFrames,
+                                                      uint32_t maxWidth, uint32_t maxHeight, int32_t shift, int32_t threshold)
+{
+    if (!frames || !numFrames || numFrames > 65535 || maxWidth < 5 || maxHeight < 5 || shift < 0 || shift > 15)
+        return AGOCUDA_INVALID_PARAMS;
+    const int t = (int)(uint8_t)threshold;
+    const int kNever = 0x7fffffff;
+    int nRound = kNever, nTrunc = kNever;
+    if (t < 255) {
+        long long M = (long long)(t + 1) << shift;
+        if (M <= 46340) {   // beyond this no 3x3 Sobel magnitude can reach M
+            nRound = (int)(M * M - M + 1);
+            nTrunc = (int)(M * M);
+        }
+    }
+    dim3 grd(div_up(maxWidth, kBX * 4), div_up(maxHeight - 4, kBY * kRPT), numFrames);
+    k_fused_gauss_sobelmag_thresh<<<grd, dim3(kBX, kBY), 0, as_stream(stream)>>>(frames, nRound, nTrunc);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}

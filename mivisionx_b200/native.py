@@ -1,0 +1,61 @@
+"""Loading of the in-tree native libraries (no fallback: a missing library is an error)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(PKG, "lib")
+AGOCUDA_SO = os.path.join(LIBDIR, "libagocuda.so")
+OPENVX_SO = os.path.join(LIBDIR, "libopenvx.so")
+
+_agocuda = None
+_openvx = None
+
+u32, i32, u64, vp, f32 = C.c_uint32, C.c_int32, C.c_uint64, C.c_void_p, C.c_float
+
+# name -> argtypes (all return int unless listed in _RESTYPES)
+AGOCUDA_SIGNATURES = {
+    "agocuda_abi_version": [],
+    "agocuda_launch_count": [],
+    "agocuda_Gaussian_U8_U8_3x3": [vp, u32, u32, vp, u32, vp, u32],
+    "agocuda_Sobel_S16S16_U8_3x3_GXY": [vp, u32, u32, vp, u32, vp, u32, vp, u32],
+    "agocuda_SobelMagnitude_S16_U8_3x3": [vp, u32, u32, vp, u32, vp, u32],
+    "agocuda_Magnitude_S16_S16S16": [vp, u32, u32, vp, u32, vp, u32, vp, u32],
+    "agocuda_ColorDepth_U8_S16_Sat": [vp, u32, u32, vp, u32, vp, u32, i32],
+    "agocuda_Threshold_U8_U8_Binary": [vp, u32, u32, vp, u32, vp, u32, i32],
+    "agocuda_fused_GaussSobelMagDepthThresh": [vp, vp, u32, u32, u32, i32, i32],
+}
+_RESTYPES = {"agocuda_launch_count": u64}
+
+
+class AgoFrame(C.Structure):
+    """Mirror of `agocuda_frame` (include/agocuda.h)."""
+    _fields_ = [("src", vp), ("dst", vp), ("width", u32), ("height", u32),
+                ("srcStride", u32), ("dstStride", u32), ("simdBegin", i32), ("simdEnd", i32)]
+
+
+def agocuda() -> C.CDLL:
+    """The CUDA kernel library (include/agocuda.h).  Raises if it has not been built."""
+    global _agocuda
+    if _agocuda is None:
+        if not os.path.exists(AGOCUDA_SO):
+            raise RuntimeError(f"{AGOCUDA_SO} is missing: run `python -m mivisionx_b200.build` first")
+        lib = C.CDLL(AGOCUDA_SO, mode=C.RTLD_GLOBAL)
+        for name, args in AGOCUDA_SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPES.get(name, C.c_int)
+        _agocuda = lib
+    return _agocuda
+
+
+def openvx() -> C.CDLL:
+    """The OpenVX host engine (libopenvx.so of this package).  Raises if not built."""
+    global _openvx
+    if _openvx is None:
+        if not os.path.exists(OPENVX_SO):
+            raise RuntimeError(f"{OPENVX_SO} is missing: run `python -m mivisionx_b200.build` first")
+        agocuda()
+        _openvx = C.CDLL(OPENVX_SO, mode=C.RTLD_LOCAL)
+    return _openvx
