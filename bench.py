@@ -1,0 +1,345 @@
+#!/usr/bin/env python3
+"""Benchmark of the OpenVX/AGO vision-graph path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+One JSON line on stdout (rank 0).  A "step" is one vxProcessGraph of a graph that holds
+`frames` independent copies of the workload's vision graph (one per frame), so every step
+processes a batch of frames larger than the B200 L2 (inputs + outputs > 126 MB; no L2 flush
+is needed between steps).
+
+* value  -- Mpixels/s with the inputs already resident in HBM: the device time of each
+            graph launch (CUDA events recorded by the engine on its own stream), summed over
+            K steps; Mpixels counts input pixels of the first node of every frame.
+* e2e    -- the same metric through the public OpenVX API with host buffers: per step,
+            vxCopyImagePatch(WRITE) of every input frame from pinned host memory,
+            vxProcessGraph, vxCopyImagePatch(READ) of every output frame into pinned host
+            memory; timed with CUDA events bracketing the K steps.
+* roofline -- HBM roofline of the dominant (fused) kernel: algorithmic bytes per launch
+            (non-virtual graph inputs + outputs, each read or written once) / its average
+            launch time, against MEASURED_PEAKS.json's copy bandwidth.
+* cpu_baseline -- the reference AGO CPU library (oracle/_ref, built from the reference's
+            sources) running the same graph on one frame, one host core, bounded sample.
+
+With --gpus N under torchrun every rank processes its own batch (weak scaling; frames are
+independent, no data collective), times are max over ranks and value is the job total.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "gauss_sobel_mag_depth_thresh_1080p": dict(
+        desc="Gaussian3x3->Sobel3x3->Magnitude->ConvertDepth(SATURATE,0)->Threshold(BINARY,128), "
+             "1920x1080 U8, border UNDEFINED, virtual intermediates",
+        width=1920, height=1080, frames=64, bytes_per_px=2.0),
+}
+DEFAULT_WORKLOAD = "gauss_sobel_mag_depth_thresh_1080p"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------------------------------
+# reference CPU path (oracle/_ref: the reference AGO library built from its own sources)
+# ------------------------------------------------------------------------------------------
+def _ref_worker(wl_name, seed, seconds, max_iters, barrier, queue):
+    """Spawned process: build the workload on the reference CPU library, wait for all
+    workers, then run frames back to back for `seconds` (at most `max_iters`)."""
+    sys.path.insert(0, ROOT)
+    import oracle
+    from mivisionx_b200 import vx as V
+    from mivisionx_b200 import workloads as WL
+    lib = oracle.ref_lib()
+    if lib is None:
+        barrier.wait()
+        queue.put(None)
+        return
+    api = V.OpenVX(lib)
+    wl = WORKLOADS[wl_name]
+    ctx = api.vxCreateContext()
+    img = WL.cfg1_image(seed=seed, width=wl["width"], height=wl["height"])
+    g = WL.Cfg1Graph(api, ctx, [(wl["width"], wl["height"])])
+    g.run([img])   # warm-up (first process allocates)
+    barrier.wait()
+    n, t0 = 0, time.perf_counter()
+    while n < max_iters and (time.perf_counter() - t0) < seconds:
+        g.run()
+        n += 1
+    queue.put((n, time.perf_counter() - t0))
+
+
+def reference_cpu(wl_name: str, procs: int, seconds: float, max_iters: int = 1 << 30):
+    """Aggregate Mpixels/s of `procs` independent reference AGO CPU graphs (one per core,
+    process per core because the AGO context creation takes a global lock)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    barrier, queue = ctx.Barrier(procs), ctx.Queue()
+    ps = [ctx.Process(target=_ref_worker, args=(wl_name, 100 + i, seconds, max_iters, barrier, queue)) for i in range(procs)]
+    for p in ps:
+        p.start()
+    res = [queue.get() for _ in ps]
+    for p in ps:
+        p.join()
+    if any(r is None for r in res):
+        return None
+    wl = WORKLOADS[wl_name]
+    frames = sum(r[0] for r in res)
+    wall = max(r[1] for r in res)
+    return frames * wl["width"] * wl["height"] / wall / 1e6, wall, frames
+
+
+def run_reference_arm(a, wl_name):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    import oracle
+    if oracle.ref_lib() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference AGO library (oracle/_ref) not built"}))
+        return 0
+    wl = WORKLOADS[wl_name]
+    cores = os.cpu_count() or 1
+    # one "step": every core runs its own graph for ~1 s (bounded so the run ends in minutes)
+    per_step_s = max(0.25, min(1.0, 90.0 / max(1, a.steps + a.warmup)))
+    vals, frames = [], 0
+    for s in range(a.warmup + a.steps):
+        mpx, _, n = reference_cpu(wl_name, cores, per_step_s)
+        if s >= a.warmup:
+            vals.append(mpx)
+            frames += n
+    v = statistics.median(vals)
+    line = {"metric": "Mpixels/s per vision graph", "value": round(v, 2), "unit": "Mpixels/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "impl": "reference", "higher_is_better": True,
+            "dtype": "u8", "data": "synthetic (seeded PCG32)",
+            "config": {"workload": wl_name, "graph": wl["desc"], "seconds_per_step": per_step_s},
+            "cpu_baseline": {"value": round(v, 2), "unit": "Mpixels/s", "cores": cores, "kind": "reference",
+                             "sample": f"{frames} frames over {a.steps} steps of {per_step_s:.2f} s, {cores} independent "
+                                       f"AGO CPU graphs (one process per core)"},
+            "e2e": {"value": round(v, 2), "unit": "Mpixels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------
+def run_ours(a, wl_name):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from mivisionx_b200 import native
+    from mivisionx_b200 import vx as V
+    from mivisionx_b200 import workloads as WL
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    wl = WORKLOADS[wl_name]
+    W, H, B = wl["width"], wl["height"], wl["frames"]
+    api = V.OpenVX()
+    lib = native.agocuda()
+    ctx = api.obj(api.vxCreateContext(), "context")
+    api.set_device(ctx, local)
+    frames = [WL.cfg1_image(seed=1000 * rank + i, width=W, height=H) for i in range(B)]
+    g = WL.Cfg1Graph(api, ctx, [(W, H)] * B)
+    plan = api.plan(g.graph)
+    kernels_per_step = sum(k for _, k in plan)
+    # pinned host staging for the end-to-end leg
+    pin_in = [torch.from_numpy(f).pin_memory() for f in frames]
+    pin_out = [torch.empty((H, W), dtype=torch.uint8).pin_memory() for _ in range(B)]
+    g.run([p.numpy() for p in pin_in])
+
+    # ---- device-resident throughput
+    for _ in range(a.warmup):
+        g.run()
+    torch.cuda.synchronize()
+    _barrier(ws)
+    gpu_ms = []
+    with ClockSampler(local) as clk:
+        launches0 = lib.agocuda_launch_count()
+        for _ in range(a.steps):
+            g.run()
+            gpu_ms.append(api.gpu_ms_last(g.graph))
+        torch.cuda.synchronize()
+    _barrier(ws)
+    total_ms = _max_over_ranks(sum(gpu_ms), ws)
+    ms_step = total_ms / a.steps
+    px_step = W * H * B
+    value = px_step * ws / (ms_step / 1e3) / 1e6
+
+    # ---- end to end through the OpenVX API with host buffers
+    addr = V.vx_imagepatch_addressing_t()
+    addr.dim_x, addr.dim_y, addr.stride_x, addr.stride_y = W, H, 1, W
+    addr.scale_x = addr.scale_y = 1024
+    addr.step_x = addr.step_y = 1
+    rect = V.vx_rectangle_t(0, 0, W, H)
+
+    def e2e_step():
+        for img, p in zip(g.inputs, pin_in):
+            api.ok(api.vxCopyImagePatch(img, C.byref(rect), 0, C.byref(addr), p.data_ptr(), V.VX_WRITE_ONLY,
+                                        V.VX_MEMORY_TYPE_HOST), "write")
+        api.ok(api.vxProcessGraph(g.graph), "process")
+        for img, p in zip(g.outputs, pin_out):
+            api.ok(api.vxCopyImagePatch(img, C.byref(rect), 0, C.byref(addr), p.data_ptr(), V.VX_READ_ONLY,
+                                        V.VX_MEMORY_TYPE_HOST), "read")
+
+    for _ in range(a.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    _barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = _max_over_ranks(e0.elapsed_time(e1) / a.steps, ws)
+    e2e = px_step * ws / (e2e_ms / 1e3) / 1e6
+    # the e2e result must still be the graph's result
+    ok_sample = bool(np.array_equal(pin_out[0].numpy()[2:H - 2, 2:W - 2], g.results()[0][0][2:H - 2, 2:W - 2]))
+
+    peak, peak_kind = _peaks()
+    alg_bytes = wl["bytes_per_px"] * px_step
+    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(wl_name)
+    line = None
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not a.no_cpu_baseline:
+            r = reference_cpu(wl_name, 1, a.cpu_seconds)
+            if r is not None:
+                cpu = {"value": round(r[0], 2), "unit": "Mpixels/s", "cores": 1, "kind": "reference",
+                       "sample": f"{r[2]} x one {W}x{H} frame through the reference AGO CPU graph "
+                                 f"({r[1]:.1f} s of CPU work, 1 core)"}
+        line = {
+            "metric": "Mpixels/s per vision graph", "value": round(value, 1), "unit": "Mpixels/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded PCG32 uniform U8)",
+            "config": {"workload": wl_name, "graph": wl["desc"], "frames_per_step_per_gpu": B,
+                       "frame": f"{W}x{H}", "l2": "inputs+outputs per step > 126 MB L2 (no flush needed)",
+                       "plan": [n for n, _ in plan], "parallelism": f"replicas x{ws} (frames sharded)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_kind": peak_kind, "alg_bytes_per_launch": alg_bytes,
+                         "kernel": plan[0][0] if plan else None},
+            "e2e": {"value": round(e2e, 1), "unit": "Mpixels/s", "h2d_bytes_per_step": W * H * B,
+                    "d2h_bytes_per_step": W * H * B, "result_checked": ok_sample},
+            "gpu_launches": kernels_per_step * a.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args(argv)
+    a.warmup = max(a.warmup, 3) if a.impl == "ours" else a.warmup
+    if a.impl == "reference":
+        return run_reference_arm(a, a.workload)
+    return run_ours(a, a.workload)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -93,7 +93,10 @@ def build(verbose: bool = False, clean: bool = False) -> None:
     eng_objs = [o for (o, _), s in zip(results, cu + eng) if s.endswith(".cpp")]
     agocuda = os.path.join(LIBDIR, "libagocuda.so")
     if _stale(agocuda, cu_objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", agocuda] + cu_objs + ["-lcuda"])
+        # shared cudart: the engine and the kernels must see one runtime (current device,
+        # streams) -- a static copy per library would keep its own device selection
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "shared", "-o", agocuda] + cu_objs +
+             ["-lcuda", "-Xlinker", f"-rpath,{CUDA_HOME}/lib64"])
     if eng_objs:
         openvx = os.path.join(LIBDIR, "libopenvx.so")
         if _stale(openvx, eng_objs + [agocuda]):

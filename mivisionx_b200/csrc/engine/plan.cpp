@@ -1,0 +1,273 @@
+// plan.cpp -- turns the lowered graph into device work.
+//
+// The reference HIP target launches one kernel per lowered node on one stream
+// (ago/ago_util_hip.cpp:686) and cannot fuse (agoGpuHipSuperNodeLaunch returns -1, :740).
+// Here the planner (1) matches chains of lowered nodes whose intermediates are virtual and
+// private to the chain and replaces each chain by one fused kernel that keeps the
+// intermediates on chip, (2) batches identical fused chains of independent sub-graphs
+// (same kernel, same by-value parameters, any frame sizes) into ONE launch over a frame
+// table, and (3) emits the remaining nodes one launch each.  With
+// VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS bit kOptNoFusion set, every node is its own
+// launch: that is the "plain" one-launch-per-node form the fused form is measured against.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <set>
+#include <sstream>
+
+#include "vx_internal.h"
+
+namespace agovx {
+
+bool lnode_is_output(const LNode &ln, size_t i);
+
+static cudaStream_t S(cudaStream_t s) { return s; }
+
+static uint8_t *dptr(Ref *r) { return IMG(r)->planes[0].dev; }
+static uint32_t dstride(Ref *r) { return IMG(r)->planes[0].dev_stride; }
+static uint32_t W(Ref *r) { return IMG(r)->width; }
+static uint32_t H(Ref *r) { return IMG(r)->height; }
+
+static void *scratch(Graph *g, size_t bytes)
+{
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, bytes);
+    g->dev_scratch.push_back(p);
+    return p;
+}
+
+// number of lowered nodes that read `d` (excluding `self`)
+static int readers(Graph *g, Ref *d, const LNode *self = nullptr)
+{
+    int n = 0;
+    for (const LNode &ln : g->lnodes) {
+        if (&ln == self) continue;
+        for (size_t i = 0; i < ln.p.size(); i++) if (!lnode_is_output(ln, i) && ln.p[i] == d) n++;
+    }
+    return n;
+}
+
+static bool private_virtual(Graph *g, Ref *d) { return d && d->is_virtual && readers(g, d) == 1; }
+
+static const LNode *reader_of(Graph *g, Ref *d)
+{
+    for (const LNode &ln : g->lnodes)
+        for (size_t i = 0; i < ln.p.size(); i++) if (!lnode_is_output(ln, i) && ln.p[i] == d) return &ln;
+    return nullptr;
+}
+
+// ------------------------------------------------------------------------------------
+// plain (one launch per lowered node) steps
+// ------------------------------------------------------------------------------------
+static vx_status plain_step(Graph *g, LNode &ln, Step &st)
+{
+    auto &p = ln.p;
+    st.name = lk_name(ln.k);
+    st.nodes = {&ln};
+    switch (ln.k) {
+    case LK::GAUSSIAN_U8_U8_3x3: {
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        st.launch = [=](cudaStream_t q) { return agocuda_Gaussian_U8_U8_3x3(S(q), w, h, d, ds, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::SOBEL_S16S16_U8_3x3_GXY: case LK::SOBEL_S16_U8_3x3_GX: case LK::SOBEL_S16_U8_3x3_GY: {
+        const bool gxy = ln.k == LK::SOBEL_S16S16_U8_3x3_GXY;
+        Ref *src = gxy ? p[2] : p[1];
+        uint32_t w = W(src), h = H(src);
+        uint32_t tmp_stride = align_up(w * 2, 64);
+        int16_t *gx, *gy; uint32_t gxs, gys;
+        if (gxy) { gx = (int16_t *)dptr(p[0]); gxs = dstride(p[0]); gy = (int16_t *)dptr(p[1]); gys = dstride(p[1]); }
+        else {
+            int16_t *t = (int16_t *)scratch(g, (size_t)tmp_stride * h);
+            if (!t) return VX_ERROR_NO_MEMORY;
+            if (ln.k == LK::SOBEL_S16_U8_3x3_GX) { gx = (int16_t *)dptr(p[0]); gxs = dstride(p[0]); gy = t; gys = tmp_stride; }
+            else { gy = (int16_t *)dptr(p[0]); gys = dstride(p[0]); gx = t; gxs = tmp_stride; }
+        }
+        const uint8_t *s = dptr(src); uint32_t ss = dstride(src);
+        st.launch = [=](cudaStream_t q) { return agocuda_Sobel_S16S16_U8_3x3_GXY(S(q), w, h, gx, gxs, gy, gys, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::SOBEL_MAGNITUDE_S16_U8_3x3: {
+        int16_t *d = (int16_t *)dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        st.launch = [=](cudaStream_t q) { return agocuda_SobelMagnitude_S16_U8_3x3(S(q), w, h, d, ds, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::MAGNITUDE_S16_S16S16: {
+        int16_t *d = (int16_t *)dptr(p[0]); const int16_t *a = (const int16_t *)dptr(p[1]), *b = (const int16_t *)dptr(p[2]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), as_ = dstride(p[1]), bs = dstride(p[2]);
+        st.launch = [=](cudaStream_t q) { return agocuda_Magnitude_S16_S16S16(S(q), w, h, d, ds, a, as_, b, bs); };
+        return VX_SUCCESS;
+    }
+    case LK::COLOR_DEPTH_U8_S16_SAT: {
+        uint8_t *d = dptr(p[0]); const int16_t *s = (const int16_t *)dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        int32_t shift = sc_i32(p[2]);
+        st.launch = [=](cudaStream_t q) { return agocuda_ColorDepth_U8_S16_Sat(S(q), w, h, d, ds, s, ss, shift); };
+        return VX_SUCCESS;
+    }
+    case LK::THRESHOLD_U8_U8_BINARY: {
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        int32_t thr = static_cast<Threshold *>(p[2])->value.U8;   // threshold_value.U1 (ago_kernel_api.cpp:3442)
+        st.launch = [=](cudaStream_t q) { return agocuda_Threshold_U8_U8_Binary(S(q), w, h, d, ds, s, ss, thr); };
+        return VX_SUCCESS;
+    }
+    case LK::CHANNEL_COPY_U8_U8: {
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        st.num_kernels = 0;   // a copy-engine transfer, not a kernel
+        st.launch = [=](cudaStream_t q) {
+            return cudaMemcpy2DAsync(d, ds, s, ss, w, h, cudaMemcpyDeviceToDevice, q) == cudaSuccess ? 0 : -1;
+        };
+        return VX_SUCCESS;
+    }
+    default:
+        log_error(g, VX_ERROR_NOT_IMPLEMENTED, "ERROR: kernel %s has no device implementation yet\n", lk_name(ln.k));
+        return VX_ERROR_NOT_IMPLEMENTED;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// fused chains
+// ------------------------------------------------------------------------------------
+struct Chain {
+    std::string kind;                 // pattern name
+    std::vector<LNode *> nodes;
+    std::vector<int64_t> key;         // by-value parameters: chains with equal keys batch
+    Ref *src = nullptr, *dst = nullptr;
+};
+
+// Gaussian3x3 -> SobelMagnitude -> ColorDepth_U8_S16_Sat -> Threshold_U8_U8_Binary
+static bool match_gauss_sobelmag_thresh(Graph *g, LNode &a, Chain &c)
+{
+    if (a.k != LK::GAUSSIAN_U8_U8_3x3 || !private_virtual(g, a.p[0])) return false;
+    LNode *b = const_cast<LNode *>(reader_of(g, a.p[0]));
+    if (!b || b->removed || b->k != LK::SOBEL_MAGNITUDE_S16_U8_3x3 || !private_virtual(g, b->p[0])) return false;
+    LNode *d = const_cast<LNode *>(reader_of(g, b->p[0]));
+    if (!d || d->k != LK::COLOR_DEPTH_U8_S16_SAT || !private_virtual(g, d->p[0])) return false;
+    LNode *t = const_cast<LNode *>(reader_of(g, d->p[0]));
+    if (!t || t->k != LK::THRESHOLD_U8_U8_BINARY) return false;
+    Image *src = IMG(a.p[1]), *dst = IMG(t->p[0]);
+    if (src->width < 5 || src->height < 5) return false;
+    c.kind = "fused_GaussSobelMagDepthThresh";
+    c.nodes = {&a, b, d, t};
+    c.key = {sc_i32(d->p[2]), static_cast<Threshold *>(t->p[2])->value.U8};
+    c.src = src; c.dst = dst;
+    return true;
+}
+
+static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &st)
+{
+    const Chain &c0 = chains[0];
+    st.name = c0.kind + " x" + std::to_string(chains.size());
+    for (Chain &c : chains) for (LNode *n : c.nodes) st.nodes.push_back(n);
+    if (c0.kind == "fused_GaussSobelMagDepthThresh") {
+        std::vector<agocuda_frame> fr;
+        uint32_t mw = 0, mh = 0;
+        for (Chain &c : chains) {
+            Image *s = IMG(c.src), *d = IMG(c.dst);
+            agocuda_frame f{};
+            f.src = s->planes[0].dev; f.dst = d->planes[0].dev;
+            f.width = s->width; f.height = s->height;
+            f.srcStride = s->planes[0].dev_stride; f.dstStride = d->planes[0].dev_stride;
+            // the virtual SobelMagnitude output AGO allocates is 16-byte aligned: SIMD body
+            // [0, W - W % 16) (ago_haf_cpu_filter.cpp:2480-2483)
+            f.simdBegin = 0; f.simdEnd = (int32_t)(s->width - (s->width & 15));
+            fr.push_back(f);
+            mw = std::max(mw, s->width); mh = std::max(mh, s->height);
+        }
+        void *dev = scratch(g, fr.size() * sizeof(agocuda_frame));
+        if (!dev) return VX_ERROR_NO_MEMORY;
+        cudaMemcpy(dev, fr.data(), fr.size() * sizeof(agocuda_frame), cudaMemcpyHostToDevice);
+        const uint32_t n = (uint32_t)fr.size();
+        const int32_t shift = (int32_t)c0.key[0], thr = (int32_t)c0.key[1];
+        st.launch = [=](cudaStream_t q) {
+            return agocuda_fused_GaussSobelMagDepthThresh(S(q), (const agocuda_frame *)dev, n, mw, mh, shift, thr);
+        };
+        return VX_SUCCESS;
+    }
+    return VX_ERROR_NOT_IMPLEMENTED;
+}
+
+// ------------------------------------------------------------------------------------
+vx_status plan_graph(Graph *g)
+{
+    for (void *p : g->dev_scratch) cudaFree(p);
+    g->dev_scratch.clear();
+    g->steps.clear();
+    g->inputs.clear();
+    g->outputs.clear();
+
+    // graph inputs / outputs and device allocation of every image the plan touches
+    std::set<Ref *> written, read;
+    for (LNode &ln : g->lnodes)
+        for (size_t i = 0; i < ln.p.size(); i++) {
+            Ref *r = ln.p[i];
+            if (!r) continue;
+            (lnode_is_output(ln, i) ? written : read).insert(r);
+            if (ln.k == LK::CANNY_EDGE_TRACE_U8_U8XY && i == 0) written.insert(r);
+        }
+    auto root = [](Ref *r) -> Ref * { return (r->type == VX_TYPE_IMAGE && IMG(r)->parent) ? IMG(r)->parent : r; };
+    for (Ref *r : read)
+        if (!r->is_virtual && (r->type == VX_TYPE_IMAGE || r->type == VX_TYPE_ARRAY || r->type == VX_TYPE_PYRAMID) && !written.count(r))
+            g->inputs.push_back(root(r));
+    for (Ref *r : written)
+        if (!r->is_virtual) g->outputs.push_back(root(r));
+
+    // fusion
+    std::set<LNode *> fused;
+    std::map<std::vector<int64_t>, std::vector<Chain>> groups;   // (pattern id, level, key...) -> chains
+    std::vector<std::vector<int64_t>> group_order;
+    if (!(g->optimizer_flags & kOptNoFusion)) {
+        for (LNode &ln : g->lnodes) {
+            Chain c;
+            if (fused.count(&ln)) continue;
+            if (match_gauss_sobelmag_thresh(g, ln, c)) {
+                std::vector<int64_t> gk{1, ln.level};
+                gk.insert(gk.end(), c.key.begin(), c.key.end());
+                if (!groups.count(gk)) group_order.push_back(gk);
+                groups[gk].push_back(c);
+                for (LNode *n : c.nodes) fused.insert(n);
+            }
+        }
+    }
+    // images eliminated by fusion need no memory; everything else is allocated now
+    std::set<Ref *> elided;
+    for (auto &kv : groups)
+        for (Chain &c : kv.second)
+            for (size_t i = 0; i + 1 < c.nodes.size(); i++) elided.insert(c.nodes[i]->p[0]);
+    for (LNode &ln : g->lnodes)
+        for (Ref *r : ln.p) {
+            if (!r || elided.count(r)) continue;
+            if (r->type == VX_TYPE_IMAGE) { if (image_alloc_device(IMG(r))) return VX_ERROR_NO_MEMORY; }
+            else if (r->type == VX_TYPE_ARRAY) { if (array_alloc_device(static_cast<Array *>(r))) return VX_ERROR_NO_MEMORY; }
+            else if (r->type == VX_TYPE_PYRAMID) { for (Image *lv : static_cast<Pyramid *>(r)->level) if (image_alloc_device(lv)) return VX_ERROR_NO_MEMORY; }
+            else if (r->type == VX_TYPE_SCALAR && r->is_virtual == false) { /* host value */ }
+        }
+
+    // steps in level order: a fused group is emitted where its first node sits
+    std::map<LNode *, std::vector<int64_t>> first_of_group;
+    for (auto &gk : group_order) first_of_group[groups[gk][0].nodes[0]] = gk;
+    std::ostringstream txt;
+    for (LNode &ln : g->lnodes) {
+        Step st;
+        if (fused.count(&ln)) {
+            auto it = first_of_group.find(&ln);
+            if (it == first_of_group.end()) continue;
+            vx_status s = build_fused_batch(g, groups[it->second], st);
+            if (s) return s;
+        } else {
+            vx_status s = plain_step(g, ln, st);
+            if (s) return s;
+        }
+        txt << st.name << "\t" << st.num_kernels << "\n";
+        g->steps.push_back(std::move(st));
+    }
+    g->plan_text = txt.str();
+    return VX_SUCCESS;
+}
+
+}  // namespace agovx

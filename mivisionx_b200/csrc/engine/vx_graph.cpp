@@ -1,0 +1,461 @@
+// vx_graph.cpp -- graphs, nodes, node factories, vxVerifyGraph and vxProcessGraph.
+//
+// vxVerifyGraph (reference: api/vx_api.cpp:2934 -> agoVerifyGraph/agoOptimizeGraph/
+// agoInitializeGraph) here: validates nodes and infers virtual meta, lowers the graph to
+// AGO low-level kernels with AGO's merge rules, propagates valid rectangles, plans the
+// device work (fused multi-node kernels, batched launches over independent same-kernel
+// nodes), allocates device buffers and captures the whole launch sequence into one CUDA
+// graph.  vxProcessGraph uploads stale inputs, replays the CUDA graph and waits.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+
+#include "vx_internal.h"
+
+using namespace agovx;
+
+namespace agovx {
+
+void graph_invalidate(Graph *g)
+{
+    g->verified = false;
+    g->state = VX_GRAPH_STATE_UNVERIFIED;
+    if (g->cexec) { cudaGraphExecDestroy(g->cexec); g->cexec = nullptr; }
+    if (g->cgraph) { cudaGraphDestroy(g->cgraph); g->cgraph = nullptr; }
+    g->steps.clear();
+}
+
+static uint64_t fnv(uint64_t h, const void *p, size_t n)
+{
+    const uint8_t *b = (const uint8_t *)p;
+    for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 1099511628211ull; }
+    return h;
+}
+
+// Kernel parameters passed by value are baked into the captured CUDA graph: a change of
+// any of them (scalar, threshold, matrix, remap table, valid rectangle) re-plans.
+static uint64_t param_signature(Graph *g)
+{
+    uint64_t h = 1469598103934665603ull;
+    for (LNode &ln : g->lnodes) {
+        for (Ref *r : ln.p) {
+            if (!r) continue;
+            switch (r->type) {
+            case VX_TYPE_SCALAR: h = fnv(h, &static_cast<Scalar *>(r)->version, 8); h = fnv(h, static_cast<Scalar *>(r)->v.raw, 8); break;
+            case VX_TYPE_THRESHOLD: h = fnv(h, &static_cast<Threshold *>(r)->version, 8); break;
+            case VX_TYPE_MATRIX: h = fnv(h, &static_cast<Matrix *>(r)->version, 8); break;
+            case VX_TYPE_REMAP: h = fnv(h, &static_cast<Remap *>(r)->version, 8); break;
+            case VX_TYPE_IMAGE: {
+                Image *img = IMG(r);
+                h = fnv(h, &img->valid, sizeof(img->valid));
+                for (int i = 0; i < img->num_planes; i++) h = fnv(h, &img->planes[i].dev, sizeof(void *));
+                break;
+            }
+            default: break;
+            }
+        }
+    }
+    return h;
+}
+
+static vx_status capture(Graph *g)
+{
+    if (g->cexec) { cudaGraphExecDestroy(g->cexec); g->cexec = nullptr; }
+    if (g->cgraph) { cudaGraphDestroy(g->cgraph); g->cgraph = nullptr; }
+    if (g->optimizer_flags & kOptNoGraphCapture) return VX_SUCCESS;
+    if (cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return VX_FAILURE;
+    int rc = 0;
+    for (Step &s : g->steps) { rc = s.launch(g->stream); if (rc) break; }
+    cudaGraph_t cg = nullptr;
+    cudaError_t e = cudaStreamEndCapture(g->stream, &cg);
+    if (rc || e != cudaSuccess) {
+        if (cg) cudaGraphDestroy(cg);
+        cudaGetLastError();
+        log_error(g, VX_FAILURE, "ERROR: CUDA graph capture failed (step rc=%d, %s)\n", rc, cudaGetErrorString(e));
+        return VX_FAILURE;
+    }
+    if (cudaGraphInstantiate(&g->cexec, cg, 0) != cudaSuccess) { cudaGraphDestroy(cg); return VX_FAILURE; }
+    g->cgraph = cg;
+    return VX_SUCCESS;
+}
+
+vx_status graph_verify(Graph *g)
+{
+    std::lock_guard<std::recursive_mutex> lk(g->lock);
+    graph_invalidate(g);
+    cudaSetDevice(g->ctx->device);
+    if (!g->stream && cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) return VX_ERROR_NO_RESOURCES;
+    if (!g->ev0) { cudaEventCreate(&g->ev0); cudaEventCreate(&g->ev1); }
+    vx_status s = lower_graph(g);
+    if (s) return s;
+    s = propagate_valid_rects(g);
+    if (s) return s;
+    s = plan_graph(g);
+    if (s) return s;
+    g->param_signature = param_signature(g);
+    s = capture(g);
+    if (s) return s;
+    g->verified = true;
+    g->state = VX_GRAPH_STATE_VERIFIED;
+    return VX_SUCCESS;
+}
+
+static uint64_t now_ns()
+{
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+        std::chrono::high_resolution_clock::now().time_since_epoch()).count();
+}
+
+vx_status graph_process(Graph *g, bool wait)
+{
+    std::lock_guard<std::recursive_mutex> lk(g->lock);
+    const uint64_t t0 = now_ns();
+    if (!g->verified) { vx_status s = graph_verify(g); if (s) return s; }
+    // by-value parameters changed since capture: re-plan (valid rects and sizes stay put)
+    if (param_signature(g) != g->param_signature) {
+        vx_status s = propagate_valid_rects(g);
+        if (!s) s = plan_graph(g);
+        g->param_signature = param_signature(g);
+        if (!s) s = capture(g);
+        if (s) return s;
+    }
+    cudaSetDevice(g->ctx->device);
+    for (Ref *r : g->inputs) {
+        vx_status s = VX_SUCCESS;
+        if (r->type == VX_TYPE_IMAGE) s = image_sync_to_device(IMG(r), g->stream);
+        else if (r->type == VX_TYPE_ARRAY) s = array_sync_to_device(static_cast<Array *>(r), g->stream);
+        else if (r->type == VX_TYPE_PYRAMID)
+            for (Image *lv : static_cast<Pyramid *>(r)->level) if (!s) s = image_sync_to_device(lv, g->stream);
+        if (s) return s;
+    }
+    g->state = VX_GRAPH_STATE_RUNNING;
+    cudaEventRecord(g->ev0, g->stream);
+    int rc = 0;
+    if (g->cexec) {
+        if (cudaGraphLaunch(g->cexec, g->stream) != cudaSuccess) rc = -1;
+    } else {
+        for (Step &s : g->steps) { rc = s.launch(g->stream); if (rc) break; }
+    }
+    cudaEventRecord(g->ev1, g->stream);
+    // outputs are now current on the device only
+    for (Ref *r : g->outputs) {
+        if (r->type == VX_TYPE_IMAGE) {
+            Image *root = IMG(r)->parent ? IMG(r)->parent : IMG(r);
+            root->dev_valid = true; root->host_valid = false;
+        } else if (r->type == VX_TYPE_ARRAY) {
+            static_cast<Array *>(r)->dev_valid = true; static_cast<Array *>(r)->host_valid = false;
+        } else if (r->type == VX_TYPE_SCALAR) {
+            static_cast<Scalar *>(r)->dev_newer = true;
+        } else if (r->type == VX_TYPE_PYRAMID) {
+            for (Image *lv : static_cast<Pyramid *>(r)->level) { lv->dev_valid = true; lv->host_valid = false; }
+        }
+    }
+    if (rc) {
+        g->state = VX_GRAPH_STATE_ABANDONED;
+        log_error(g, VX_FAILURE, "ERROR: vxProcessGraph: launch failed (%d)\n", rc);
+        return VX_FAILURE;
+    }
+    g->scheduled = true;
+    if (!wait) return VX_SUCCESS;
+    vx_status st = graph_wait(g);
+    const uint64_t t1 = now_ns();
+    vx_perf_t &p = g->perf;
+    p.tmp = t1 - t0; p.beg = t0; p.end = t1; p.sum += p.tmp; p.num++;
+    p.avg = p.sum / p.num;
+    p.min = p.num == 1 ? p.tmp : std::min(p.min, p.tmp);
+    p.max = std::max(p.max, p.tmp);
+    return st;
+}
+
+vx_status graph_wait(Graph *g)
+{
+    if (!g->scheduled) return VX_FAILURE;
+    g->scheduled = false;
+    cudaError_t e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) {
+        g->state = VX_GRAPH_STATE_ABANDONED;
+        log_error(g, VX_FAILURE, "ERROR: graph execution failed: %s\n", cudaGetErrorString(e));
+        return VX_FAILURE;
+    }
+    cudaEventElapsedTime(&g->gpu_ms_last, g->ev0, g->ev1);
+    // kernels that detect a failure (bounded waits, capacity) report through the plan
+    g->state = VX_GRAPH_STATE_COMPLETED;
+    return VX_SUCCESS;
+}
+
+}  // namespace agovx
+
+// ====================================================================================
+// Public API
+// ====================================================================================
+template <class T> static T *as(void *h) { return static_cast<T *>(static_cast<Ref *>(h)); }
+#define CHECK_REF(h, T) if (!is_valid(h, T)) return VX_ERROR_INVALID_REFERENCE
+
+extern "C" {
+
+vx_graph vxCreateGraph(vx_context context)
+{
+    if (!is_valid(context, VX_TYPE_CONTEXT)) return nullptr;
+    Graph *g = new Graph();
+    g->type = VX_TYPE_GRAPH;
+    add_ref(as<Context>(context), g);
+    if (const char *f = getenv("AGO_B200_OPTIMIZER_FLAGS")) g->optimizer_flags = (uint32_t)strtoul(f, nullptr, 0);
+    return (vx_graph)g;
+}
+
+vx_status vxReleaseGraph(vx_graph *graph)
+{
+    if (!graph || !is_valid(*graph, VX_TYPE_GRAPH)) return VX_ERROR_INVALID_REFERENCE;
+    Graph *g = as<Graph>(*graph);
+    if (g->scheduled) graph_wait(g);
+    g->ext_count = 0;
+    g->released = true;
+    *graph = nullptr;
+    return VX_SUCCESS;
+}
+
+vx_status vxVerifyGraph(vx_graph graph)
+{
+    CHECK_REF(graph, VX_TYPE_GRAPH);
+    return graph_verify(as<Graph>(graph));
+}
+
+vx_status vxProcessGraph(vx_graph graph)
+{
+    CHECK_REF(graph, VX_TYPE_GRAPH);
+    return graph_process(as<Graph>(graph), true);
+}
+
+vx_status vxScheduleGraph(vx_graph graph)
+{
+    CHECK_REF(graph, VX_TYPE_GRAPH);
+    Graph *g = as<Graph>(graph);
+    if (g->scheduled) return VX_ERROR_GRAPH_SCHEDULED;
+    return graph_process(g, false);
+}
+
+vx_status vxWaitGraph(vx_graph graph)
+{
+    CHECK_REF(graph, VX_TYPE_GRAPH);
+    return graph_wait(as<Graph>(graph));
+}
+
+vx_status vxQueryGraph(vx_graph graph, vx_enum attribute, void *ptr, vx_size size)
+{
+    CHECK_REF(graph, VX_TYPE_GRAPH);
+    Graph *g = as<Graph>(graph);
+    switch (attribute) {
+    case VX_GRAPH_NUMNODES: if (size != 4) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = (vx_uint32)g->nodes.size(); return VX_SUCCESS;
+    case VX_GRAPH_PERFORMANCE: if (size != sizeof(vx_perf_t)) return VX_ERROR_INVALID_PARAMETERS; *(vx_perf_t *)ptr = g->perf; return VX_SUCCESS;
+    case VX_GRAPH_NUMPARAMETERS: if (size != 4) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = 0; return VX_SUCCESS;
+    case VX_GRAPH_STATE: if (size != 4) return VX_ERROR_INVALID_PARAMETERS; *(vx_enum *)ptr = g->state; return VX_SUCCESS;
+    case VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS: if (size != 4) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = g->optimizer_flags; return VX_SUCCESS;
+    case VX_GRAPH_ATTRIBUTE_AMD_AFFINITY:
+        if (size != sizeof(AgoTargetAffinityInfo)) return VX_ERROR_INVALID_PARAMETERS;
+        memset(ptr, 0, size); ((AgoTargetAffinityInfo *)ptr)->device_type = AGO_TARGET_AFFINITY_GPU; return VX_SUCCESS;
+    case VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_LAST: case VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_AVG: {
+        // device time of the last launch (CUDA events), reported in vx_perf_t nanoseconds
+        if (size != sizeof(vx_perf_t)) return VX_ERROR_INVALID_PARAMETERS;
+        vx_perf_t p = g->perf;
+        p.tmp = (vx_uint64)(g->gpu_ms_last * 1e6);
+        *(vx_perf_t *)ptr = p; return VX_SUCCESS;
+    }
+    case VX_GRAPH_ATTRIBUTE_AMD_EXPORT_TO_TEXT: {
+        // the verified plan as text: one line per step ("kernel nodes...")
+        if (!ptr || size == 0) return VX_ERROR_INVALID_PARAMETERS;
+        snprintf((char *)ptr, size, "%s", g->plan_text.c_str());
+        return VX_SUCCESS;
+    }
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_status vxSetGraphAttribute(vx_graph graph, vx_enum attribute, const void *ptr, vx_size size)
+{
+    CHECK_REF(graph, VX_TYPE_GRAPH);
+    Graph *g = as<Graph>(graph);
+    switch (attribute) {
+    case VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS:
+        if (size != 4) return VX_ERROR_INVALID_PARAMETERS;
+        g->optimizer_flags = *(const vx_uint32 *)ptr; graph_invalidate(g); return VX_SUCCESS;
+    case VX_GRAPH_ATTRIBUTE_AMD_AFFINITY:
+        if (size != sizeof(AgoTargetAffinityInfo)) return VX_ERROR_INVALID_PARAMETERS;
+        g->affinity = ((const AgoTargetAffinityInfo *)ptr)->device_type;
+        return VX_SUCCESS;   // every node runs on the GPU target; CPU affinity is accepted and ignored
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_bool vxIsGraphVerified(vx_graph graph)
+{
+    return is_valid(graph, VX_TYPE_GRAPH) && as<Graph>(graph)->verified ? vx_true_e : vx_false_e;
+}
+
+vx_status vxQueryNode(vx_node node, vx_enum attribute, void *ptr, vx_size size)
+{
+    CHECK_REF(node, VX_TYPE_NODE);
+    Node *n = as<Node>(node);
+    switch (attribute) {
+    case VX_NODE_STATUS: if (size != 4) return VX_ERROR_INVALID_PARAMETERS; *(vx_status *)ptr = n->status; return VX_SUCCESS;
+    case VX_NODE_PERFORMANCE: if (size != sizeof(vx_perf_t)) return VX_ERROR_INVALID_PARAMETERS; *(vx_perf_t *)ptr = n->perf; return VX_SUCCESS;
+    case VX_NODE_BORDER: if (size != sizeof(vx_border_t)) return VX_ERROR_INVALID_PARAMETERS; *(vx_border_t *)ptr = n->border; return VX_SUCCESS;
+    case VX_NODE_PARAMETERS: if (size != 4) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = (vx_uint32)n->params.size(); return VX_SUCCESS;
+    case VX_NODE_LOCAL_DATA_SIZE: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = 0; return VX_SUCCESS;
+    case VX_NODE_ATTRIBUTE_AMD_AFFINITY:
+        if (size != sizeof(AgoTargetAffinityInfo)) return VX_ERROR_INVALID_PARAMETERS;
+        memset(ptr, 0, size); ((AgoTargetAffinityInfo *)ptr)->device_type = AGO_TARGET_AFFINITY_GPU; return VX_SUCCESS;
+    case VX_NODE_ATTRIBUTE_AMD_HIP_STREAM: {
+        // the CUDA stream the node's graph launches on (cudaStream_t)
+        if (size != sizeof(void *)) return VX_ERROR_INVALID_PARAMETERS;
+        Graph *g = n->scope;
+        *(void **)ptr = g ? (void *)g->stream : nullptr; return VX_SUCCESS;
+    }
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_status vxSetNodeAttribute(vx_node node, vx_enum attribute, const void *ptr, vx_size size)
+{
+    CHECK_REF(node, VX_TYPE_NODE);
+    Node *n = as<Node>(node);
+    switch (attribute) {
+    case VX_NODE_BORDER:
+        if (size != sizeof(vx_border_t)) return VX_ERROR_INVALID_PARAMETERS;
+        n->border = *(const vx_border_t *)ptr;
+        if (n->scope) graph_invalidate(n->scope);
+        return VX_SUCCESS;
+    case VX_NODE_ATTRIBUTE_AMD_AFFINITY:
+        if (size != sizeof(AgoTargetAffinityInfo)) return VX_ERROR_INVALID_PARAMETERS;
+        n->affinity = ((const AgoTargetAffinityInfo *)ptr)->device_type;
+        return VX_SUCCESS;
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_status vxReleaseNode(vx_node *node)
+{
+    if (!node || !is_valid(*node, VX_TYPE_NODE)) return VX_ERROR_INVALID_REFERENCE;
+    as<Node>(*node)->ext_count = 0;
+    as<Node>(*node)->released = true;
+    as<Node>(*node)->int_count = 1;     // the graph keeps it
+    *node = nullptr;
+    return VX_SUCCESS;
+}
+
+vx_status vxRemoveNode(vx_node *node)
+{
+    if (!node || !is_valid(*node, VX_TYPE_NODE)) return VX_ERROR_INVALID_REFERENCE;
+    Node *n = as<Node>(*node);
+    n->removed = true;
+    if (n->scope) graph_invalidate(n->scope);
+    *node = nullptr;
+    return VX_SUCCESS;
+}
+
+vx_status vxSetNodeTarget(vx_node node, vx_enum target_enum, const char *target_string)
+{
+    CHECK_REF(node, VX_TYPE_NODE);
+    if (target_enum == VX_TARGET_ANY) return VX_SUCCESS;
+    if (target_enum == VX_TARGET_STRING && target_string) {
+        std::string t(target_string);
+        for (auto &c : t) c = (char)toupper(c);
+        if (t == "GPU" || t == "ANY" || t == "CUDA") return VX_SUCCESS;
+        return VX_ERROR_NOT_SUPPORTED;   // no CPU target on this implementation
+    }
+    return VX_ERROR_NOT_SUPPORTED;
+}
+
+// ---------------------------------------------------------------- node factories
+static vx_node make_node(vx_graph graph, vx_enum kernel, std::initializer_list<Ref *> params)
+{
+    if (!is_valid(graph, VX_TYPE_GRAPH)) return nullptr;
+    Graph *g = as<Graph>(graph);
+    Node *n = new Node();
+    n->type = VX_TYPE_NODE;
+    n->scope = g;
+    n->kernel = kernel;
+    n->params.assign(params.begin(), params.end());
+    for (Ref *r : n->params) retain_internal(r);
+    add_ref(g->ctx, n);
+    g->nodes.push_back(n);
+    graph_invalidate(g);
+    return (vx_node)n;
+}
+
+static Ref *scalar_of(vx_graph graph, vx_enum type, const void *v)
+{
+    if (!is_valid(graph, VX_TYPE_GRAPH)) return nullptr;
+    Scalar *s = make_scalar(as<Graph>(graph)->ctx, as<Graph>(graph), type, v);
+    s->ext_count = 0;
+    s->int_count = 1;
+    return s;
+}
+
+#define R(x) static_cast<Ref *>(static_cast<void *>(x))
+
+vx_node vxColorConvertNode(vx_graph graph, vx_image input, vx_image output)
+{ return make_node(graph, VX_KERNEL_COLOR_CONVERT, {R(input), R(output)}); }
+
+vx_node vxChannelExtractNode(vx_graph graph, vx_image input, vx_enum channel, vx_image output)
+{ return make_node(graph, VX_KERNEL_CHANNEL_EXTRACT, {R(input), scalar_of(graph, VX_TYPE_ENUM, &channel), R(output)}); }
+
+vx_node vxSobel3x3Node(vx_graph graph, vx_image input, vx_image output_x, vx_image output_y)
+{ return make_node(graph, VX_KERNEL_SOBEL_3x3, {R(input), R(output_x), R(output_y)}); }
+
+vx_node vxMagnitudeNode(vx_graph graph, vx_image grad_x, vx_image grad_y, vx_image mag)
+{ return make_node(graph, VX_KERNEL_MAGNITUDE, {R(grad_x), R(grad_y), R(mag)}); }
+
+vx_node vxScaleImageNode(vx_graph graph, vx_image src, vx_image dst, vx_enum type)
+{ return make_node(graph, VX_KERNEL_SCALE_IMAGE, {R(src), R(dst), scalar_of(graph, VX_TYPE_ENUM, &type)}); }
+
+vx_node vxThresholdNode(vx_graph graph, vx_image input, vx_threshold thresh, vx_image output)
+{ return make_node(graph, VX_KERNEL_THRESHOLD, {R(input), R(thresh), R(output)}); }
+
+vx_node vxGaussian3x3Node(vx_graph graph, vx_image input, vx_image output)
+{ return make_node(graph, VX_KERNEL_GAUSSIAN_3x3, {R(input), R(output)}); }
+
+vx_node vxGaussianPyramidNode(vx_graph graph, vx_image input, vx_pyramid gaussian)
+{ return make_node(graph, VX_KERNEL_GAUSSIAN_PYRAMID, {R(input), R(gaussian)}); }
+
+vx_node vxConvertDepthNode(vx_graph graph, vx_image input, vx_image output, vx_enum policy, vx_scalar shift)
+{ return make_node(graph, VX_KERNEL_CONVERTDEPTH, {R(input), R(output), scalar_of(graph, VX_TYPE_ENUM, &policy), R(shift)}); }
+
+vx_node vxCannyEdgeDetectorNode(vx_graph graph, vx_image input, vx_threshold hyst, vx_int32 gradient_size,
+                                vx_enum norm_type, vx_image output)
+{
+    return make_node(graph, VX_KERNEL_CANNY_EDGE_DETECTOR,
+                     {R(input), R(hyst), scalar_of(graph, VX_TYPE_INT32, &gradient_size), scalar_of(graph, VX_TYPE_ENUM, &norm_type), R(output)});
+}
+
+vx_node vxWarpAffineNode(vx_graph graph, vx_image input, vx_matrix matrix, vx_enum type, vx_image output)
+{ return make_node(graph, VX_KERNEL_WARP_AFFINE, {R(input), R(matrix), scalar_of(graph, VX_TYPE_ENUM, &type), R(output)}); }
+
+vx_node vxWarpPerspectiveNode(vx_graph graph, vx_image input, vx_matrix matrix, vx_enum type, vx_image output)
+{ return make_node(graph, VX_KERNEL_WARP_PERSPECTIVE, {R(input), R(matrix), scalar_of(graph, VX_TYPE_ENUM, &type), R(output)}); }
+
+vx_node vxHarrisCornersNode(vx_graph graph, vx_image input, vx_scalar strength_thresh, vx_scalar min_distance,
+                            vx_scalar sensitivity, vx_int32 gradient_size, vx_int32 block_size, vx_array corners,
+                            vx_scalar num_corners)
+{
+    return make_node(graph, VX_KERNEL_HARRIS_CORNERS,
+                     {R(input), R(strength_thresh), R(min_distance), R(sensitivity), scalar_of(graph, VX_TYPE_INT32, &gradient_size),
+                      scalar_of(graph, VX_TYPE_INT32, &block_size), R(corners), R(num_corners)});
+}
+
+vx_node vxOpticalFlowPyrLKNode(vx_graph graph, vx_pyramid old_images, vx_pyramid new_images, vx_array old_points,
+                               vx_array new_points_estimates, vx_array new_points, vx_enum termination, vx_scalar epsilon,
+                               vx_scalar num_iterations, vx_scalar use_initial_estimate, vx_size window_dimension)
+{
+    return make_node(graph, VX_KERNEL_OPTICAL_FLOW_PYR_LK,
+                     {R(old_images), R(new_images), R(old_points), R(new_points_estimates), R(new_points),
+                      scalar_of(graph, VX_TYPE_ENUM, &termination), R(epsilon), R(num_iterations), R(use_initial_estimate),
+                      scalar_of(graph, VX_TYPE_SIZE, &window_dimension)});
+}
+
+vx_node vxRemapNode(vx_graph graph, vx_image input, vx_remap table, vx_enum policy, vx_image output)
+{ return make_node(graph, VX_KERNEL_REMAP, {R(input), R(table), scalar_of(graph, VX_TYPE_ENUM, &policy), R(output)}); }
+
+vx_node vxHalfScaleGaussianNode(vx_graph graph, vx_image input, vx_image output, vx_int32 kernel_size)
+{ return make_node(graph, VX_KERNEL_HALFSCALE_GAUSSIAN, {R(input), R(output), scalar_of(graph, VX_TYPE_INT32, &kernel_size)}); }
+
+}  // extern "C"

@@ -1,0 +1,172 @@
+"""Seeded synthetic inputs and OpenVX graph builders for the benchmark configurations.
+
+The graph builders only use the OpenVX API (through ``vx.OpenVX``), so the same function
+builds the graph on this package's B200 engine and on the reference AGO CPU library.
+
+Random numbers come from PCG32 (O'Neill's pcg32: 64-bit LCG state, XSH-RR output), generated
+in vectorised blocks with LCG jump-ahead so full-size frames are produced in milliseconds.
+A uniform byte is the top 8 bits of a PCG32 output.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import vx as V
+
+_MULT = np.uint64(6364136223846793005)
+
+
+def pcg32(seed: int, n: int, stream: int = 54) -> np.ndarray:
+    """n outputs of pcg32 seeded like pcg32_srandom_r(seed, stream)."""
+    with np.errstate(over="ignore"):
+        inc = np.uint64(((stream << 1) | 1) & 0xFFFFFFFFFFFFFFFF)
+        s = np.uint64(0)
+        s = s * _MULT + inc
+        s = s + np.uint64(seed & 0xFFFFFFFFFFFFFFFF)
+        s = s * _MULT + inc
+        block = 4096
+        # states of the first block, sequentially
+        first = np.empty(block, np.uint64)
+        x = s
+        for i in range(block):
+            first[i] = x
+            x = x * _MULT + inc
+        # affine map of `block` steps: x -> A x + B
+        A, B = np.uint64(1), np.uint64(0)
+        m, c = _MULT, inc
+        k = block
+        while k:
+            if k & 1:
+                A, B = A * m, B * m + c
+            m, c = m * m, c * m + c
+            k >>= 1
+        nb = (n + block - 1) // block
+        states = np.empty(nb * block, np.uint64)
+        cur = first
+        for b in range(nb):
+            states[b * block:(b + 1) * block] = cur
+            cur = cur * A + B
+        old = states[:n]
+        xs = (((old >> np.uint64(18)) ^ old) >> np.uint64(27)).astype(np.uint32)
+        rot = (old >> np.uint64(59)).astype(np.uint32)
+        out = (xs >> rot) | (xs << ((np.uint32(32) - rot) & np.uint32(31)))
+    return out.astype(np.uint32)
+
+
+def uniform_u8(seed: int, shape, stream: int = 54) -> np.ndarray:
+    n = int(np.prod(shape))
+    return (pcg32(seed, n, stream) >> np.uint32(24)).astype(np.uint8).reshape(shape)
+
+
+def uniform01(seed: int, n: int, stream: int = 54) -> np.ndarray:
+    return pcg32(seed, n, stream).astype(np.float64) / 4294967296.0
+
+
+def gaussian(seed: int, n: int, stream: int = 54) -> np.ndarray:
+    """Standard normal samples (Box-Muller over PCG32 uniforms)."""
+    m = (n + 1) // 2
+    u = uniform01(seed, 2 * m, stream)
+    u1 = np.maximum(u[0::2], 1e-12)
+    r = np.sqrt(-2.0 * np.log(u1))
+    t = 2.0 * np.pi * u[1::2]
+    return np.concatenate([r * np.cos(t), r * np.sin(t)])[:n]
+
+
+# ---------------------------------------------------------------- inputs
+def cfg1_image(seed: int = 1, width: int = 1920, height: int = 1080) -> np.ndarray:
+    """One U8 frame, i.i.d. uniform 0..255 from a seeded PCG32."""
+    return uniform_u8(seed, (height, width))
+
+
+def cfg2_scene(seed: int = 2, width: int = 3840, height: int = 2160, rects: int = 200, sigma: float = 8.0) -> np.ndarray:
+    """Linear gradient background (0..200 across x) + `rects` seeded axis-aligned rectangles
+    (sides 16..400 px, intensity uniform 0..255) + Gaussian noise (sigma 8), clipped."""
+    img = np.tile(np.linspace(0.0, 200.0, width, dtype=np.float64), (height, 1))
+    r = pcg32(seed, rects * 5, stream=7)
+    for i in range(rects):
+        w = 16 + int(r[5 * i + 0] % 385)
+        h = 16 + int(r[5 * i + 1] % 385)
+        x0 = int(r[5 * i + 2] % max(1, width - w))
+        y0 = int(r[5 * i + 3] % max(1, height - h))
+        img[y0:y0 + h, x0:x0 + w] = float(r[5 * i + 4] >> 24)
+    img += sigma * gaussian(seed, width * height, stream=11).reshape(height, width)
+    return np.clip(np.rint(img), 0, 255).astype(np.uint8)
+
+
+def cfg3_frame(seed: int = 3, width: int = 3840, height: int = 2160, waves: int = 8) -> np.ndarray:
+    """RGB frame: per channel a sum of `waves` random 2-D sinusoids scaled to 0..255, plus
+    uniform noise in [-10, 10], clipped."""
+    yy, xx = np.meshgrid(np.arange(height, dtype=np.float32), np.arange(width, dtype=np.float32), indexing="ij")
+    out = np.empty((height, width, 3), np.uint8)
+    p = uniform01(seed, 3 * waves * 4, stream=13)
+    for ch in range(3):
+        acc = np.zeros((height, width), np.float32)
+        for k in range(waves):
+            a, b, c, d = p[(ch * waves + k) * 4:(ch * waves + k) * 4 + 4]
+            fx, fy = (a - 0.5) * 0.02, (b - 0.5) * 0.02
+            acc += np.sin(fx * xx + fy * yy + 2 * np.pi * c).astype(np.float32) * np.float32(0.5 + d)
+        acc = (acc - acc.min()) / max(1e-6, float(acc.max() - acc.min())) * 255.0
+        noise = (uniform01(seed + ch + 1, width * height, stream=17).reshape(height, width) * 20.0 - 10.0).astype(np.float32)
+        out[..., ch] = np.clip(np.rint(acc + noise), 0, 255).astype(np.uint8)
+    return out
+
+
+def cfg3_affine(seed: int = 3, cx: float = 960.0, cy: float = 540.0) -> np.ndarray:
+    """OpenVX 2x3 affine matrix in vx_matrix layout (3 rows x 2 columns, m[j][i]): rotation
+    +-15 deg, scale 0.8..1.2, translation +-50 px, about the image centre."""
+    u = uniform01(seed, 4, stream=19)
+    th = math.radians((u[0] * 2 - 1) * 15.0)
+    s = 0.8 + 0.4 * u[1]
+    tx, ty = (u[2] * 2 - 1) * 50.0, (u[3] * 2 - 1) * 50.0
+    a, b = s * math.cos(th), s * math.sin(th)
+    # x' = a x - b y + c0 ; y' = b x + a y + c1 (destination -> source mapping)
+    c0 = cx - a * cx + b * cy + tx
+    c1 = cy - b * cx - a * cy + ty
+    return np.array([[a, b], [-b, a], [c0, c1]], dtype=np.float32)
+
+
+# ---------------------------------------------------------------- graph builders
+class Cfg1Graph:
+    """Gaussian3x3 -> Sobel3x3 -> Magnitude -> ConvertDepth(SATURATE, shift) -> Threshold(BINARY)
+    for each of `sizes` frames, all in ONE OpenVX graph (independent sub-graphs), border
+    UNDEFINED, intermediates virtual."""
+
+    def __init__(self, api: V.OpenVX, ctx, sizes, shift: int = 0, thr: int = 128, flags: int | None = None):
+        self.api, self.ctx = api, ctx
+        a = api
+        self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
+        if flags is not None:
+            a.set_optimizer_flags(self.graph, flags)
+        self.inputs, self.outputs = [], []
+        self.shift = a.scalar(ctx, V.VX_TYPE_INT32, shift)
+        self.thr = a.threshold_binary(ctx, thr)
+        g = self.graph
+        for (w, h) in sizes:
+            src = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+            dst = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+            gau = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_U8)
+            gx = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_S16)
+            gy = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_S16)
+            mag = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_S16)
+            dep = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_U8)
+            for n in (a.vxGaussian3x3Node(g, src, gau), a.vxSobel3x3Node(g, gau, gx, gy),
+                      a.vxMagnitudeNode(g, gx, gy, mag),
+                      a.vxConvertDepthNode(g, mag, dep, V.VX_CONVERT_POLICY_SATURATE, self.shift),
+                      a.vxThresholdNode(g, dep, self.thr, dst)):
+                a.obj(n, "node")
+            self.inputs.append(src)
+            self.outputs.append(dst)
+        a.ok(a.vxVerifyGraph(g), "vxVerifyGraph")
+
+    def run(self, frames=None):
+        a = self.api
+        if frames is not None:
+            for img, f in zip(self.inputs, frames):
+                a.write_plane(img, f)
+        a.ok(a.vxProcessGraph(self.graph), "vxProcessGraph")
+
+    def results(self):
+        return [(self.api.read_plane(o), self.api.valid_region(o)) for o in self.outputs]

@@ -1,0 +1,67 @@
+"""include/agovx.h must be ABI-identical to the Khronos/AMD headers the reference ships:
+every enum constant and struct size declared in agovx.h is compiled once against agovx.h
+and once against the reference's VX/vx.h + vx_ext_amd.h, and the values must agree.
+Also checks that the built libraries export every function the headers declare."""
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HDR = os.path.join(ROOT, "include", "agovx.h")
+AGOCUDA_H = os.path.join(ROOT, "include", "agocuda.h")
+REF_INC = "/root/reference/amd_openvx/openvx/include"
+
+STRUCTS = ["vx_imagepatch_addressing_t", "vx_perf_t", "vx_keypoint_t", "vx_rectangle_t", "vx_coordinates2df_t",
+           "vx_pixel_value_t", "vx_border_t", "AgoTargetAffinityInfo"]
+
+
+def _enum_names():
+    src = open(HDR).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = set()
+    for body in re.findall(r"enum\s*\w*\s*\{(.*?)\}", src, flags=re.S):
+        for m in re.finditer(r"\b((?:VX|AGO)_[A-Z0-9_a-z]+)\s*=", body):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def _run(prog, incs):
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "p.cpp")   # the reference's vx_ext_amd.h needs C++
+        exe = os.path.join(d, "p")
+        open(c, "w").write(prog)
+        subprocess.run(["g++", "-w", "-o", exe, c] + [f"-I{i}" for i in incs], check=True)
+        return subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_INC), reason="reference headers not present")
+def test_enums_and_structs_match_reference():
+    names = _enum_names()
+    assert len(names) > 150
+    body = "".join(f'printf("{n} %ld\\n", (long)({n}));\n' for n in names)
+    body += "".join(f'printf("sizeof_{s} %zu\\n", sizeof({s}));\n' for s in STRUCTS)
+    ours = _run('#include <stdio.h>\n#include "agovx.h"\nint main(){' + body + "return 0;}", [os.path.dirname(HDR)])
+    ref = _run('#include <stdio.h>\n#include <VX/vx.h>\n#include <VX/vx_compatibility.h>\n#include <vx_ext_amd.h>\n'
+               'int main(){' + body + "return 0;}", [REF_INC])
+    assert ours == ref
+
+
+def _declared(path, prefix):
+    src = re.sub(r"/\*.*?\*/", "", open(path).read(), flags=re.S)
+    return sorted(set(re.findall(r"\b(" + prefix + r"\w+)\s*\(", src)))
+
+
+def test_libraries_export_declared_symbols():
+    from mivisionx_b200 import native
+    if not (os.path.exists(native.AGOCUDA_SO) and os.path.exists(native.OPENVX_SO)):
+        pytest.skip("native libraries not built")
+    import ctypes
+    ago = ctypes.CDLL(native.AGOCUDA_SO)
+    for name in _declared(AGOCUDA_H, "agocuda_"):
+        assert hasattr(ago, name), name
+    ovx = native.openvx()
+    for name in _declared(HDR, "vx"):
+        assert hasattr(ovx, name), name
