@@ -6,6 +6,7 @@
  */
 #include "agooracle.h"
 #include <math.h>
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -156,4 +157,290 @@ int oracle_Threshold_U8_U8_Binary(uint32_t W, uint32_t H, uint8_t *pDst, uint32_
         for (uint32_t x = 0; x < W; x++) d[x] = s[x] > threshold ? 255 : 0;
     }
     return 0;
+}
+
+/* =============================== Canny ================================== */
+
+/* ago_haf_cpu_arithmetic.cpp:9638 HafCpu_FastAtan2_Canny: direction quantised to 0..3. */
+static int fast_atan2_canny(int16_t gx, int16_t gy)
+{
+    uint16_t ax = (uint16_t)abs(gx), ay = (uint16_t)abs(gy);
+    float d1 = (float)ax * 0.4142135623730950488016887242097f;
+    float d2 = (float)ax * 2.4142135623730950488016887242097f;
+    int ret = (gx * gy) < 0 ? 3 : 1;
+    if (ay <= d1) ret = 0;
+    if (ay >= d2) ret = 2;
+    return ret;
+}
+
+static uint16_t canny_pack(int16_t gx, int16_t gy)
+{
+    int16_t t = (int16_t)(abs(gx) + abs(gy));
+    t = (int16_t)(t << 2);
+    t = (int16_t)(t | (fast_atan2_canny(gx, gy) & 3));
+    return (uint16_t)t;
+}
+
+/* ago_haf_cpu_canny.cpp:44 HafCpu_CannySobel_U16_U8_3x3_L1NORM, rows 1..H-2 of the full
+ * image (pDst/pSrc point at row 0).  Gy is negated (canny.cpp:79).  The SIMD body keeps
+ * per-row vertical sums r0 = s[y-1]+2s[y]+s[y+1] and r1 = s[y+1]-s[y-1] in a scratch
+ * buffer; at x = 0 it reads r0[-1] (never written: 0) and r1[-1], which aliases
+ * r0[ALIGN16(W)-1] (the column W-1 vertical sum of the current row when W%16 == 0, else
+ * never written: 0).  Columns from (W - (W&15) - 1) on use the scalar formula, which reads
+ * one byte past the row at x = W-1.  Assumes a 16-byte aligned destination and W >= 16. */
+int oracle_CannySobel_U16_U8_3x3_L1NORM(uint32_t W, uint32_t H, uint16_t *pDst, uint32_t dstStride,
+                                        const uint8_t *pSrc, uint32_t srcStride)
+{
+    int prefix, tail_start;
+    haf_split(pDst, (int)W, &prefix, &tail_start);
+    const int aligned = tail_start - prefix;
+    const int A16 = ((int)W + 15) & ~15;
+    const int st = (int)srcStride;
+    for (int y = 1; y < (int)H - 1; y++) {
+        const uint8_t *s = pSrc + (size_t)y * srcStride;
+        uint16_t *d = (uint16_t *)ROW(pDst, dstStride, y);
+        for (int x = 0; x < (int)W; x++) {
+            int16_t gx, gy;
+            if (x >= prefix && x < aligned + prefix - 1 && x <= aligned - 8 + 7) {
+                /* SIMD body: gx = r0[x+1] - r0[x-1]; gy = -(r1[x-1] + 2 r1[x] + r1[x+1]) */
+                int r0m, r1m;
+                if (x == 0) {
+                    r0m = 0;
+                    r1m = (A16 - 1 < aligned) ? ((s[A16 - 1 - st] + 2 * s[A16 - 1] + s[A16 - 1 + st]) & 0xffff) : 0;
+                } else {
+                    r0m = s[x - 1 - st] + 2 * s[x - 1] + s[x - 1 + st];
+                    r1m = s[x - 1 + st] - s[x - 1 - st];
+                }
+                int r0p = s[x + 1 - st] + 2 * s[x + 1] + s[x + 1 + st];
+                int r1c = s[x + st] - s[x - st];
+                int r1p = s[x + 1 + st] - s[x + 1 - st];
+                gx = (int16_t)(r0p - r0m);
+                gy = (int16_t)(0 - (int16_t)(r1m + 2 * r1c + r1p));
+            } else {
+                gx = (int16_t)(s[x + 1 - st] - s[x - 1 - st] + s[x + 1 + st] - s[x - 1 + st] + 2 * (s[x + 1] - s[x - 1]));
+                gy = (int16_t)(s[x - 1 + st] + s[x + 1 + st] - s[x - 1 - st] - s[x + 1 - st] + 2 * (s[x + st] - s[x - st]));
+                gy = (int16_t)(~gy + 1);
+            }
+            d[x] = canny_pack(gx, gy);
+        }
+    }
+    return 0;
+}
+
+static const int kNOffset[4][2][2] = {
+    { { -1, 0 }, { 1, 0 } }, { { 1, -1 }, { -1, 1 } }, { { 0, -1 }, { 0, 1 } }, { { -1, -1 }, { 1, 1 } },
+};
+
+/* ago_haf_cpu_canny.cpp:549 HafCpu_CannySuppThreshold_U8XY_U16_3x3: non-maximum
+ * suppression along the quantised direction (strict > on both sides), then > upper -> 255
+ * (pushed on the stack in raster order), <= lower -> 0, else 127; x,y in [1,W-1)x[1,H-1). */
+int oracle_CannySuppThreshold_U8XY_U16_3x3(uint32_t capacityOfXY, oracle_coord2d_u16 *xyStack, uint32_t *pStackTop,
+                                           uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                           const uint16_t *pSrc, uint32_t srcStride, uint16_t lower, uint16_t upper)
+{
+    (void)capacityOfXY;
+    const int ss = (int)(srcStride >> 1);
+    uint32_t top = 0;
+    for (uint32_t y = 1; y < H - 1; y++) {
+        uint8_t *out = pDst + (size_t)y * dstStride;
+        const uint16_t *p = pSrc + (size_t)y * ss;
+        for (uint32_t x = 1; x < W - 1; x++) {
+            int mag = p[x] >> 2, ang = p[x] & 3;
+            int o0 = kNOffset[ang][0][1] * ss + kNOffset[ang][0][0];
+            int o1 = kNOffset[ang][1][1] * ss + kNOffset[ang][1][0];
+            int edge = (mag > (p[(int)x + o0] >> 2) && mag > (p[(int)x + o1] >> 2)) ? mag : 0;
+            if (edge > upper) {
+                out[x] = 255;
+                xyStack[top].x = (uint16_t)x; xyStack[top].y = (uint16_t)y; top++;
+            } else if (edge <= lower) {
+                out[x] = 0;
+            } else {
+                out[x] = 127;
+            }
+        }
+    }
+    *pStackTop = top;
+    return 0;
+}
+
+/* ago_haf_cpu_canny.cpp:598 HafCpu_CannyEdgeTrace_U8_U8XY: grow strong pixels through
+ * 8-connected 127 pixels (DFS over the stack), then 127 -> 0 over ALIGN16(W) columns. */
+int oracle_CannyEdgeTrace_U8_U8XY(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                  uint32_t capacityOfXY, oracle_coord2d_u16 *xyStack, uint32_t stackTop)
+{
+    (void)capacityOfXY;
+    static const int dx[8] = {-1, 0, 1, -1, 1, -1, 0, 1}, dy[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
+    uint32_t top = stackTop;
+    while (top) {
+        top--;
+        int x = xyStack[top].x, y = xyStack[top].y;
+        for (int i = 0; i < 8; i++) {
+            int x1 = x + dx[i], y1 = y + dy[i];
+            uint8_t *p = pDst + (size_t)y1 * dstStride + x1;
+            if (*p == 127) {
+                *p = 255;
+                xyStack[top].x = (uint16_t)x1; xyStack[top].y = (uint16_t)y1; top++;
+            }
+        }
+    }
+    const uint32_t w16 = (W + 15) & ~15u;
+    for (uint32_t y = 0; y < H; y++) {
+        uint8_t *row = pDst + (size_t)y * dstStride;
+        for (uint32_t x = 0; x < w16; x++) if (row[x] == 127) row[x] = 0;
+    }
+    return 0;
+}
+
+/* =============================== Harris ================================= */
+
+/* ago_haf_cpu_harris.cpp:85 HafCpu_HarrisSobel_HG3_U8_3x3: rows 1..H-2 (pointers at row 0),
+ * all columns (reading one pixel outside the row at x = 0 and x = W-1); products of the
+ * integer 3x3 Sobel gradients in float, div_factor 1 (harris.cpp:129). */
+int oracle_HarrisSobel_HG3_U8_3x3(uint32_t W, uint32_t H, float *pDstGxy, uint32_t dstStride,
+                                  const uint8_t *pSrc, uint32_t srcStride)
+{
+    const int st = (int)srcStride;
+    for (int y = 1; y < (int)H - 1; y++) {
+        const uint8_t *s = pSrc + (size_t)y * srcStride;
+        float *d = (float *)ROW(pDstGxy, dstStride, y);
+        for (int x = 0; x < (int)W; x++) {
+            int16_t hx0 = (int16_t)(s[x + 1 - st] - s[x - 1 - st]);
+            int16_t hx1 = (int16_t)(s[x + 1] - s[x - 1]);
+            int16_t hx2 = (int16_t)(s[x + 1 + st] - s[x - 1 + st]);
+            int16_t hy0 = (int16_t)(s[x - 1 - st] + 2 * s[x - st] + s[x + 1 - st]);
+            int16_t hy2 = (int16_t)(s[x - 1 + st] + 2 * s[x + st] + s[x + 1 + st]);
+            int16_t gx = (int16_t)(hx2 + hx0 + 2 * hx1);
+            int16_t gy = (int16_t)(hy2 - hy0);
+            d[3 * x + 0] = ((float)gx * (float)gx) / 1.0f;
+            d[3 * x + 1] = ((float)gx * (float)gy) / 1.0f;
+            d[3 * x + 2] = ((float)gy * (float)gy) / 1.0f;
+        }
+    }
+    return 0;
+}
+
+/* ago_haf_cpu_harris.cpp:596 HafCpu_HarrisScore_HVC_HG3_3x3: 3x3 window sums in (j, i)
+ * order, Mc = (gx2*gy2 - gxy2*gxy2) - (k*trace)*trace, Mc /= norm, Mc > Tc ? Mc : 0;
+ * first/last row and column are 0.  Plain float multiply-then-add (no FMA). */
+int oracle_HarrisScore_HVC_HG3_3x3(uint32_t W, uint32_t H, float *pDstVc, uint32_t dstStride,
+                                   const float *pSrcGxy, uint32_t srcStride, float k, float Tc, float norm)
+{
+    memset(pDstVc, 0, dstStride);
+    for (uint32_t y = 1; y < H - 1; y++) {
+        float *d = (float *)ROW(pDstVc, dstStride, y);
+        const float *c = (const float *)ROW(pSrcGxy, srcStride, y);
+        d[0] = 0;
+        for (uint32_t x = 1; x < W - 1; x++) {
+            float gx2 = 0, gy2 = 0, gxy2 = 0;
+            for (int j = -1; j <= 1; j++) {
+                const float *t = (const float *)((const uint8_t *)c + (ptrdiff_t)j * (ptrdiff_t)srcStride);
+                for (int i = -1; i <= 1; i++) {
+                    gx2 += t[3 * ((int)x + i) + 0];
+                    gxy2 += t[3 * ((int)x + i) + 1];
+                    gy2 += t[3 * ((int)x + i) + 2];
+                }
+            }
+            float traceA = gx2 + gy2;
+            float detA = (gx2 * gy2) - (gxy2 * gxy2);
+            float Mc = detA - (k * traceA * traceA);
+            Mc /= norm;
+            d[x] = (Mc > Tc) ? Mc : 0;
+        }
+        d[W - 1] = 0;
+    }
+    memset(ROW(pDstVc, dstStride, H - 1), 0, dstStride);
+    return 0;
+}
+
+/* ago_haf_cpu_harris.cpp:882 HafCpu_NonMaxSupp_XY_ANY_3x3: keep v if >= the three pixels
+ * above and the left one, > the right one and the three below; raster-order list. */
+int oracle_NonMaxSupp_XY_ANY_3x3(uint32_t capacity, oracle_xys *list, uint32_t *pCount, uint32_t W, uint32_t H,
+                                 const float *pSrc, uint32_t srcStride)
+{
+    uint32_t n = 0;
+    for (uint32_t y = 1; y < H - 1 && n < capacity; y++) {
+        const float *a = (const float *)ROW(pSrc, srcStride, y - 1);
+        const float *b = (const float *)ROW(pSrc, srcStride, y);
+        const float *c = (const float *)ROW(pSrc, srcStride, y + 1);
+        for (uint32_t x = 1; x < W - 1; x++) {
+            float v = b[x];
+            if (v >= a[x - 1] && v >= a[x] && v >= a[x + 1] && v >= b[x - 1] && v > b[x + 1] &&
+                v > c[x - 1] && v > c[x] && v > c[x + 1]) {
+                list[n].x = (int16_t)x; list[n].y = (int16_t)y; list[n].s = v;
+                if (++n >= capacity) break;
+            }
+        }
+    }
+    *pCount = n;
+    return 0;
+}
+
+static int cmp_i64_desc(const void *a, const void *b)
+{
+    int64_t x = *(const int64_t *)a, y = *(const int64_t *)b;
+    return x < y ? 1 : x > y ? -1 : 0;
+}
+
+/* ago_haf_cpu_harris.cpp:923 HafCpu_HarrisMergeSortAndPick_XY_XYS with the grid set up by
+ * ago_kernel_api.cpp:20801-20815: the XYS records are sorted descending as raw int64
+ * (strength bits, then y, then x); a point is kept when its grid cell (side
+ * floor(min_distance/sqrt 2)) is empty and no kept point in the 5x5 surrounding cells is
+ * closer than ceilf(min_distance^2) (strict).  min_distance <= 2 keeps everything.
+ * *pCount may exceed `capacity`; only `capacity` corners are written. */
+int oracle_HarrisMergeSortAndPick_XY_XYS(uint32_t capacity, oracle_keypoint *corners, uint32_t *pCount,
+                                         oracle_xys *list, uint32_t n, float minDistance, uint32_t W, uint32_t H)
+{
+    qsort(list, n, sizeof(oracle_xys), cmp_i64_desc);
+    uint32_t count = 0;
+    if (minDistance > 2.0f) {
+        uint32_t cell = (uint32_t)floor(minDistance / 1.41421356237309504880);
+        uint32_t gw = (W + cell - 1) / cell, gh = (H + cell - 1) / cell;
+        int16_t *grid = (int16_t *)malloc((size_t)gw * gh * 2 * sizeof(int16_t));
+        for (size_t i = 0; i < (size_t)gw * gh * 2; i++) grid[i] = -1;
+        int32_t md2 = (int32_t)ceilf(minDistance * minDistance);
+        for (uint32_t i = 0; i < n; i++) {
+            int x = list[i].x, y = list[i].y;
+            int cx = x / (int)cell, cy = y / (int)cell;
+            int16_t *cg = grid + 2 * ((size_t)cy * gw + cx);
+            int found = 1;
+            if (cg[0] < 0) {
+                int x0 = cx - 2 > 0 ? cx - 2 : 0, x1 = cx + 2 < (int)gw - 1 ? cx + 2 : (int)gw - 1;
+                int y0 = cy - 2 > 0 ? cy - 2 : 0, y1 = cy + 2 < (int)gh - 1 ? cy + 2 : (int)gh - 1;
+                found = 0;
+                for (int yy = y0; yy <= y1 && !found; yy++)
+                    for (int xx = x0; xx <= x1; xx++) {
+                        int16_t *g = grid + 2 * ((size_t)yy * gw + xx);
+                        if (g[0] >= 0) {
+                            int ddx = g[0] - x, ddy = g[1] - y;
+                            if (ddx * ddx + ddy * ddy < md2) { found = 1; break; }
+                        }
+                    }
+            }
+            if (!found) {
+                if (count < capacity) {
+                    oracle_keypoint *k = &corners[count];
+                    k->x = x; k->y = y; k->strength = list[i].s; k->tracking_status = 1;
+                    k->error = 0; k->scale = 0; k->orientation = 0;
+                }
+                count++;
+                cg[0] = (int16_t)x; cg[1] = (int16_t)y;
+            }
+        }
+        free(grid);
+    } else {
+        count = n < capacity ? n : capacity;
+        for (uint32_t i = 0; i < count; i++) {
+            oracle_keypoint *k = &corners[i];
+            k->x = list[i].x; k->y = list[i].y; k->strength = list[i].s; k->tracking_status = 1;
+            k->error = 0; k->scale = 0; k->orientation = 0;
+        }
+    }
+    *pCount = count;
+    return 0;
+}
+
+float oracle_harris_norm_factor(int32_t gs)
+{
+    float f = 255.0f * (float)(1 << (gs - 1)) * 3;
+    return f * f * f * f;
 }

@@ -34,6 +34,33 @@ int oracle_ColorDepth_U8_S16_Sat(uint32_t dstWidth, uint32_t dstHeight, uint8_t 
 int oracle_Threshold_U8_U8_Binary(uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
                                   const uint8_t *pSrc, uint32_t srcStride, uint8_t threshold);
 
+
+/* ---- Canny (ago_haf_cpu_canny.cpp) ---- */
+typedef struct { uint16_t x, y; } oracle_coord2d_u16;   /* ago_coord2d_ushort_t */
+typedef struct { int16_t x, y; float s; } oracle_xys;    /* ago_keypoint_xys_t */
+typedef struct { int32_t x, y; float strength, scale, orientation; int32_t tracking_status; float error; } oracle_keypoint;
+
+int oracle_CannySobel_U16_U8_3x3_L1NORM(uint32_t dstWidth, uint32_t dstHeight, uint16_t *pDst, uint32_t dstStride,
+                                        const uint8_t *pSrc, uint32_t srcStride);
+int oracle_CannySuppThreshold_U8XY_U16_3x3(uint32_t capacityOfXY, oracle_coord2d_u16 *xyStack, uint32_t *pStackTop,
+                                           uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                           const uint16_t *pSrc, uint32_t srcStride, uint16_t lower, uint16_t upper);
+int oracle_CannyEdgeTrace_U8_U8XY(uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                  uint32_t capacityOfXY, oracle_coord2d_u16 *xyStack, uint32_t stackTop);
+/* ---- Harris (ago_haf_cpu_harris.cpp) ---- */
+int oracle_HarrisSobel_HG3_U8_3x3(uint32_t dstWidth, uint32_t dstHeight, float *pDstGxy, uint32_t dstStride,
+                                  const uint8_t *pSrc, uint32_t srcStride);
+int oracle_HarrisScore_HVC_HG3_3x3(uint32_t dstWidth, uint32_t dstHeight, float *pDstVc, uint32_t dstStride,
+                                   const float *pSrcGxy, uint32_t srcStride, float sensitivity, float threshold,
+                                   float normFactor);
+int oracle_NonMaxSupp_XY_ANY_3x3(uint32_t capacity, oracle_xys *list, uint32_t *pCount, uint32_t srcWidth,
+                                 uint32_t srcHeight, const float *pSrc, uint32_t srcStride);
+int oracle_HarrisMergeSortAndPick_XY_XYS(uint32_t capacity, oracle_keypoint *corners, uint32_t *pCount,
+                                         oracle_xys *list, uint32_t listCount, float minDistance,
+                                         uint32_t imageWidth, uint32_t imageHeight);
+/* AGO wrapper arithmetic (ago_kernel_api.cpp:16941-16942) */
+float oracle_harris_norm_factor(int32_t gradientSize);
+
 #ifdef __cplusplus
 }
 #endif
