@@ -84,6 +84,73 @@ int agocuda_Threshold_U8_U8_Binary(void *stream, uint32_t dstWidth, uint32_t dst
                                    const uint8_t *pSrc, uint32_t srcStride, int32_t threshold);
 
 /* ------------------------------------------------------------------------------------ */
+/* Vision: Canny and Harris (reference: hipvx/hip_host_decls.h vision_kernels)           */
+/*                                                                                      */
+/* Border columns follow the reference CPU kernels, which read one byte outside each row */
+/* (x = -1 and x = W): with AGO's buffer layout (row pitch ALIGN16(W), zero padding) that */
+/* is the neighbouring row's pixel when W % 16 == 0, else 0.  Those values reach the     */
+/* valid region through suppression and hysteresis, so they are reproduced.              */
+/* ------------------------------------------------------------------------------------ */
+
+/* Packed Canny gradient ((|gx|+|gy|) << 2 | direction) of rows [1, H-1); rows 0 and H-1
+ * are written 0.  Replaces HipExec_CannySobel_U16_U8_3x3_L1NORM (hipvx/hip_host_decls.h:828);
+ * HafCpu_CannySobel_U16_U8_3x3_L1NORM (ago_haf_cpu_canny.cpp:44). */
+int agocuda_CannySobel_U16_U8_3x3_L1NORM(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                         uint16_t *pDst, uint32_t dstStride,
+                                         const uint8_t *pSrc, uint32_t srcStride);
+
+/* Non-maximum suppression + double threshold (255 / 127 / 0) on [1,W-1)x[1,H-1); strong
+ * pixels are appended to pStack as (y << 16 | x) (the layout of ago_coord2d_ushort_t), in no
+ * particular order, *pStackCount set to their number.  Replaces
+ * HipExec_CannySuppThreshold_U8XY_U16_3x3 (hipvx/hip_host_decls.h:852);
+ * HafCpu_CannySuppThreshold_U8XY_U16_3x3 (ago_haf_cpu_canny.cpp:549). */
+int agocuda_CannySuppThreshold_U8XY_U16_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                            uint8_t *pDst, uint32_t dstStride,
+                                            const uint16_t *pSrc, uint32_t srcStride,
+                                            uint32_t *pStack, uint32_t *pStackCount, uint32_t stackCapacity,
+                                            uint16_t hystLower, uint16_t hystUpper);
+
+/* Hysteresis in place: pixels 8-connected through non-zero pixels to a strong one become
+ * 255, all others 0 (the whole image is written).  Needs `scratch` device memory of
+ * agocuda_CannyEdgeTrace_scratch_size(W, H) bytes, 256-byte aligned; *pStatus gets bit 0 set
+ * if a union-find walk exceeded its bound.  The reference runs this on the CPU only
+ * (ago_kernel_list.cpp:486); HafCpu_CannyEdgeTrace_U8_U8XY (ago_haf_cpu_canny.cpp:598). */
+size_t agocuda_CannyEdgeTrace_scratch_size(uint32_t width, uint32_t height);
+int agocuda_CannyEdgeTrace_U8_U8XY(void *stream, uint32_t width, uint32_t height, uint8_t *pImg, uint32_t stride,
+                                   const uint32_t *pStack, const uint32_t *pStackCount, uint32_t stackCapacity,
+                                   void *scratch, size_t scratchBytes, uint32_t *pStatus);
+
+/* Harris gradient products {gx*gx, gx*gy, gy*gy} (float x3 per pixel) of rows [1, H-1);
+ * rows 0 and H-1 are written 0.  Replaces HipExec_HarrisSobel_HG3_U8_3x3
+ * (hipvx/hip_host_decls.h:868); HafCpu_HarrisSobel_HG3_U8_3x3 (ago_haf_cpu_harris.cpp:85). */
+int agocuda_HarrisSobel_HG3_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                   float *pDst, uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+
+/* Harris score over a 3x3 window; border rows/columns 0.  Replaces
+ * HipExec_HarrisScore_HVC_HG3_3x3 (hipvx/hip_host_decls.h:880);
+ * HafCpu_HarrisScore_HVC_HG3_3x3 (ago_haf_cpu_harris.cpp:596). */
+int agocuda_HarrisScore_HVC_HG3_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                    float *pDst, uint32_t dstStride, const float *pSrc, uint32_t srcStride,
+                                    float sensitivity, float strengthThreshold, float normFactor);
+
+/* 3x3 non-maximum suppression; candidates appended as 8-byte XYS records (int16 x, int16 y,
+ * float s -- ago_keypoint_xys_t) in no particular order.  Replaces
+ * HipExec_NonMaxSupp_XY_ANY_3x3 (hipvx/hip_host_decls.h:898);
+ * HafCpu_NonMaxSupp_XY_ANY_3x3 (ago_haf_cpu_harris.cpp:882). */
+int agocuda_NonMaxSupp_XY_ANY_3x3(void *stream, uint32_t width, uint32_t height, const float *pSrc, uint32_t srcStride,
+                                  uint64_t *pList, uint32_t *pListCount, uint32_t listCapacity);
+
+/* Sort candidates (descending as int64) and keep those farther than minDistance from kept
+ * ones on the reference's grid; writes vx_keypoint_t records in sorted order, *pCornerCount =
+ * min(kept, capacity), *pNumCorners = kept.  At most 8192 candidates (else *pStatus |= 2 and
+ * nothing is written).  The reference runs this on the CPU only (ago_kernel_list.cpp:483);
+ * HafCpu_HarrisMergeSortAndPick_XY_XYS (ago_haf_cpu_harris.cpp:923). */
+int agocuda_HarrisMergeSortAndPick_XY_XYS(void *stream, uint32_t width, uint32_t height, const uint64_t *pList,
+                                          const uint32_t *pListCount, uint32_t listCapacity, float minDistance,
+                                          void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
+                                          uint32_t *pNumCorners, uint32_t *pStatus);
+
+/* ------------------------------------------------------------------------------------ */
 /* Fused multi-node kernels (no reference counterpart: the HIP target launches one kernel */
 /* per node, ago/ago_util_hip.cpp:686; agoGpuHipSuperNodeLaunch returns -1 at :740)      */
 /* ------------------------------------------------------------------------------------ */
@@ -105,6 +172,25 @@ typedef struct agocuda_frame {
 int agocuda_fused_GaussSobelMagDepthThresh(void *stream, const agocuda_frame *frames, uint32_t numFrames,
                                            uint32_t maxWidth, uint32_t maxHeight,
                                            int32_t shift, int32_t threshold);
+
+/* vxCannyEdgeDetectorNode (gradient 3, L1 norm) as one front-end kernel (gradient,
+ * suppression, thresholds and label initialisation from one read of the image) plus the
+ * union-find hysteresis; the 0/255 edge map is bit-identical to the unfused graph inside
+ * its valid region.  Scratch: agocuda_fused_CannyEdgeDetector_scratch_size(W, H) bytes. */
+size_t agocuda_fused_CannyEdgeDetector_scratch_size(uint32_t width, uint32_t height);
+int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t width, uint32_t height,
+                                           uint8_t *pDst, uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride,
+                                           uint16_t hystLower, uint16_t hystUpper,
+                                           void *scratch, size_t scratchBytes, uint32_t *pStatus);
+
+/* vxHarrisCornersNode (gradient 3, block 3) as one front-end kernel (Sobel products,
+ * window sums, score and non-maximum suppression from one read of the image) plus the
+ * corner pick.  Scratch: agocuda_fused_HarrisCorners_scratch_size(W, H) bytes. */
+size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t width, uint32_t height);
+int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t width, uint32_t height, const uint8_t *pSrc, uint32_t srcStride,
+                                    float sensitivity, float strengthThreshold, float normFactor, float minDistance,
+                                    void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
+                                    uint32_t *pNumCorners, void *scratch, size_t scratchBytes, uint32_t *pStatus);
 
 #ifdef __cplusplus
 }

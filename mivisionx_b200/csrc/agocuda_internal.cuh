@@ -45,4 +45,12 @@ __device__ __forceinline__ uint32_t load_word_clamped(const uint8_t *row, int c,
     return ldg_u32(row + c);
 }
 
+// layout of vx_keypoint_t (OpenVX vx_types.h)
+struct vx_keypoint_like {
+    int32_t x, y;
+    float strength, scale, orientation;
+    int32_t tracking_status;
+    float error;
+};
+
 __device__ __forceinline__ int byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xff; }

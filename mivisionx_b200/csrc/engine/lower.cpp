@@ -95,7 +95,7 @@ vx_status validate_node(Graph *g, Node *n)
         if (!fmt_is(p[0], VX_DF_IMAGE_U8) || !is_valid(p[1], VX_TYPE_THRESHOLD)) return VX_ERROR_INVALID_PARAMETERS;
         if (static_cast<Threshold *>(p[1])->thresh_type != VX_THRESHOLD_TYPE_RANGE) return VX_ERROR_INVALID_TYPE;
         if (sc_i32(p[2]) != 3) return VX_ERROR_NOT_SUPPORTED;   // gradient sizes 5/7 are outside this target
-        if (sc_enum(p[3]) != VX_NORM_L1 && sc_enum(p[3]) != VX_NORM_L2) return VX_ERROR_INVALID_VALUE;
+        if (sc_enum(p[3]) != VX_NORM_L1) return sc_enum(p[3]) == VX_NORM_L2 ? VX_ERROR_NOT_SUPPORTED : VX_ERROR_INVALID_VALUE;
         return set_meta(img(4), img(0)->width, img(0)->height, VX_DF_IMAGE_U8);
     }
     case VX_KERNEL_HARRIS_CORNERS: {

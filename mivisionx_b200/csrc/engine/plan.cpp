@@ -57,6 +57,16 @@ static const LNode *reader_of(Graph *g, Ref *d)
     return nullptr;
 }
 
+// Harris score normalisation of the AGO wrapper (ago_kernel_api.cpp:16941-16942), in float.
+static float harris_norm(int32_t gs)
+{
+    volatile float f = 255.0f * (float)(1 << (gs - 1)) * 3;
+    f = f * f;
+    f = f * (255.0f * (float)(1 << (gs - 1)) * 3);
+    f = f * (255.0f * (float)(1 << (gs - 1)) * 3);
+    return f;
+}
+
 // ------------------------------------------------------------------------------------
 // plain (one launch per lowered node) steps
 // ------------------------------------------------------------------------------------
@@ -115,6 +125,75 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         st.launch = [=](cudaStream_t q) { return agocuda_Threshold_U8_U8_Binary(S(q), w, h, d, ds, s, ss, thr); };
         return VX_SUCCESS;
     }
+    case LK::CANNY_SOBEL_U16_U8_3x3_L1NORM: {
+        uint16_t *d = (uint16_t *)dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        st.launch = [=](cudaStream_t q) { return agocuda_CannySobel_U16_U8_3x3_L1NORM(S(q), w, h, d, ds, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: {
+        uint8_t *d = dptr(p[0]); Array *stk = static_cast<Array *>(p[1]); const uint16_t *s = (const uint16_t *)dptr(p[2]);
+        Threshold *t = static_cast<Threshold *>(p[3]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[2]);
+        // threshold_lower/upper .U1 passed as vx_uint16 (ago_kernel_api.cpp:17967)
+        uint16_t lo = (uint16_t)t->lower.U32, hi = (uint16_t)t->upper.U32;
+        uint32_t *stack = (uint32_t *)stk->dev, *cnt = stk->dev_count; uint32_t cap = (uint32_t)stk->capacity;
+        st.launch = [=](cudaStream_t q) {
+            return agocuda_CannySuppThreshold_U8XY_U16_3x3(S(q), w, h, d, ds, s, ss, stack, cnt, cap, lo, hi);
+        };
+        return VX_SUCCESS;
+    }
+    case LK::CANNY_EDGE_TRACE_U8_U8XY: {
+        uint8_t *d = dptr(p[0]); Array *stk = static_cast<Array *>(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]);
+        size_t sb = agocuda_CannyEdgeTrace_scratch_size(w, h);
+        void *scr = scratch(g, sb);
+        if (!scr) return VX_ERROR_NO_MEMORY;
+        const uint32_t *stack = (const uint32_t *)stk->dev, *cnt = stk->dev_count; uint32_t cap = (uint32_t)stk->capacity;
+        uint32_t *status = g->status_dev;
+        st.num_kernels = 4;
+        st.launch = [=](cudaStream_t q) {
+            return agocuda_CannyEdgeTrace_U8_U8XY(S(q), w, h, d, ds, stack, cnt, cap, scr, sb, status);
+        };
+        return VX_SUCCESS;
+    }
+    case LK::HARRIS_SOBEL_HG3_U8_3x3: {
+        float *d = (float *)dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        st.launch = [=](cudaStream_t q) { return agocuda_HarrisSobel_HG3_U8_3x3(S(q), w, h, d, ds, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::HARRIS_SCORE_HVC_HG3_3x3: {
+        float *d = (float *)dptr(p[0]); const float *s = (const float *)dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        float k = sc_f32(p[2]), tc = sc_f32(p[3]);
+        float norm = harris_norm(sc_i32(p[4]));
+        st.launch = [=](cudaStream_t q) { return agocuda_HarrisScore_HVC_HG3_3x3(S(q), w, h, d, ds, s, ss, k, tc, norm); };
+        return VX_SUCCESS;
+    }
+    case LK::NON_MAX_SUPP_XY_ANY_3x3: {
+        Array *lst = static_cast<Array *>(p[0]); const float *s = (const float *)dptr(p[1]);
+        uint32_t w = W(p[1]), h = H(p[1]), ss = dstride(p[1]);
+        uint64_t *l = (uint64_t *)lst->dev; uint32_t *cnt = lst->dev_count; uint32_t cap = (uint32_t)lst->capacity;
+        st.launch = [=](cudaStream_t q) { return agocuda_NonMaxSupp_XY_ANY_3x3(S(q), w, h, s, ss, l, cnt, cap); };
+        return VX_SUCCESS;
+    }
+    case LK::HARRIS_MERGE_SORT_AND_PICK_XY_XYS: {
+        Array *corners = static_cast<Array *>(p[0]);
+        Scalar *num = p[1] ? static_cast<Scalar *>(p[1]) : nullptr;
+        Array *lst = static_cast<Array *>(p[2]);
+        float mind = sc_f32(p[3]);
+        uint32_t w = static_cast<Scalar *>(p[4])->v.u32, h = static_cast<Scalar *>(p[5])->v.u32;
+        if (num && scalar_alloc_device(num)) return VX_ERROR_NO_MEMORY;
+        const uint64_t *l = (const uint64_t *)lst->dev; const uint32_t *lc = lst->dev_count; uint32_t lcap = (uint32_t)lst->capacity;
+        void *out = corners->dev; uint32_t ocap = (uint32_t)corners->capacity; uint32_t *oc = corners->dev_count;
+        uint32_t *nc = num ? num->dev : nullptr;
+        uint32_t *status = g->status_dev;
+        st.launch = [=](cudaStream_t q) {
+            return agocuda_HarrisMergeSortAndPick_XY_XYS(S(q), w, h, l, lc, lcap, mind, out, ocap, oc, nc, status);
+        };
+        return VX_SUCCESS;
+    }
     case LK::CHANNEL_COPY_U8_U8: {
         uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
         uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
@@ -159,8 +238,86 @@ static bool match_gauss_sobelmag_thresh(Graph *g, LNode &a, Chain &c)
     return true;
 }
 
+// CannySobel -> CannySuppThreshold -> CannyEdgeTrace (one vxCannyEdgeDetectorNode)
+static bool match_canny(Graph *g, LNode &a, Chain &c)
+{
+    if (a.k != LK::CANNY_SOBEL_U16_U8_3x3_L1NORM || !private_virtual(g, a.p[0])) return false;
+    LNode *b = const_cast<LNode *>(reader_of(g, a.p[0]));
+    if (!b || b->k != LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3 || !b->p[1]->is_virtual) return false;
+    LNode *t = const_cast<LNode *>(reader_of(g, b->p[1]));
+    if (!t || t->k != LK::CANNY_EDGE_TRACE_U8_U8XY || t->p[0] != b->p[0]) return false;
+    Threshold *th = static_cast<Threshold *>(b->p[3]);
+    c.kind = "fused_CannyEdgeDetector";
+    c.nodes = {&a, b, t};
+    c.key = {(int64_t)(uint16_t)th->lower.U32, (int64_t)(uint16_t)th->upper.U32};
+    c.src = a.p[1]; c.dst = b->p[0];
+    return true;
+}
+
+// HarrisSobel -> HarrisScore -> NonMaxSupp -> HarrisMergeSortAndPick (one vxHarrisCornersNode)
+static bool match_harris(Graph *g, LNode &a, Chain &c)
+{
+    if (a.k != LK::HARRIS_SOBEL_HG3_U8_3x3 || !private_virtual(g, a.p[0])) return false;
+    LNode *b = const_cast<LNode *>(reader_of(g, a.p[0]));
+    if (!b || b->k != LK::HARRIS_SCORE_HVC_HG3_3x3 || !private_virtual(g, b->p[0])) return false;
+    LNode *n = const_cast<LNode *>(reader_of(g, b->p[0]));
+    if (!n || n->k != LK::NON_MAX_SUPP_XY_ANY_3x3 || !private_virtual(g, n->p[0])) return false;
+    LNode *pk = const_cast<LNode *>(reader_of(g, n->p[0]));
+    if (!pk || pk->k != LK::HARRIS_MERGE_SORT_AND_PICK_XY_XYS) return false;
+    c.kind = "fused_HarrisCorners";
+    c.nodes = {&a, b, n, pk};
+    c.src = a.p[1]; c.dst = pk->p[0];
+    return true;
+}
+
 static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &st)
 {
+    if (chains[0].kind == "fused_CannyEdgeDetector" || chains[0].kind == "fused_HarrisCorners") {
+        // one step holding every frame's launches (one CUDA graph segment)
+        std::vector<std::function<int(cudaStream_t)>> fns;
+        st.name = chains[0].kind + " x" + std::to_string(chains.size());
+        st.num_kernels = 0;
+        uint32_t *status = g->status_dev;
+        for (Chain &c : chains) {
+            for (LNode *n : c.nodes) st.nodes.push_back(n);
+            Image *s = IMG(c.src);
+            const uint32_t w = s->width, h = s->height, ss = s->planes[0].dev_stride;
+            const uint8_t *src = s->planes[0].dev;
+            if (c.kind == "fused_CannyEdgeDetector") {
+                Image *d = IMG(c.dst);
+                uint8_t *dst = d->planes[0].dev; const uint32_t ds = d->planes[0].dev_stride;
+                const size_t sb = agocuda_fused_CannyEdgeDetector_scratch_size(w, h);
+                void *scr = scratch(g, sb);
+                if (!scr) return VX_ERROR_NO_MEMORY;
+                const uint16_t lo = (uint16_t)c.key[0], hi = (uint16_t)c.key[1];
+                fns.push_back([=](cudaStream_t q) {
+                    return agocuda_fused_CannyEdgeDetector_3x3_L1(S(q), w, h, dst, ds, src, ss, lo, hi, scr, sb, status);
+                });
+                st.num_kernels += 4;
+            } else {
+                LNode *sc = c.nodes[1], *pk = c.nodes[3];
+                const float k = sc_f32(sc->p[2]), tc = sc_f32(sc->p[3]), norm = harris_norm(sc_i32(sc->p[4]));
+                const float mind = sc_f32(pk->p[3]);
+                Array *corners = static_cast<Array *>(pk->p[0]);
+                Scalar *num = pk->p[1] ? static_cast<Scalar *>(pk->p[1]) : nullptr;
+                if (num && scalar_alloc_device(num)) return VX_ERROR_NO_MEMORY;
+                void *out = corners->dev; const uint32_t ocap = (uint32_t)corners->capacity; uint32_t *oc = corners->dev_count;
+                uint32_t *nc = num ? num->dev : nullptr;
+                const size_t sb = agocuda_fused_HarrisCorners_scratch_size(w, h);
+                void *scr = scratch(g, sb);
+                if (!scr) return VX_ERROR_NO_MEMORY;
+                fns.push_back([=](cudaStream_t q) {
+                    return agocuda_fused_HarrisCorners_3x3(S(q), w, h, src, ss, k, tc, norm, mind, out, ocap, oc, nc, scr, sb, status);
+                });
+                st.num_kernels += 2;
+            }
+        }
+        st.launch = [fns](cudaStream_t q) {
+            for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
+            return 0;
+        };
+        return VX_SUCCESS;
+    }
     const Chain &c0 = chains[0];
     st.name = c0.kind + " x" + std::to_string(chains.size());
     for (Chain &c : chains) for (LNode *n : c.nodes) st.nodes.push_back(n);
@@ -225,8 +382,12 @@ vx_status plan_graph(Graph *g)
         for (LNode &ln : g->lnodes) {
             Chain c;
             if (fused.count(&ln)) continue;
-            if (match_gauss_sobelmag_thresh(g, ln, c)) {
-                std::vector<int64_t> gk{1, ln.level};
+            int pattern = 0;
+            if (match_gauss_sobelmag_thresh(g, ln, c)) pattern = 1;
+            else if (match_canny(g, ln, c)) pattern = 2;
+            else if (match_harris(g, ln, c)) pattern = 3;
+            if (pattern) {
+                std::vector<int64_t> gk{pattern, ln.level};
                 gk.insert(gk.end(), c.key.begin(), c.key.end());
                 if (!groups.count(gk)) group_order.push_back(gk);
                 groups[gk].push_back(c);
@@ -238,7 +399,10 @@ vx_status plan_graph(Graph *g)
     std::set<Ref *> elided;
     for (auto &kv : groups)
         for (Chain &c : kv.second)
-            for (size_t i = 0; i + 1 < c.nodes.size(); i++) elided.insert(c.nodes[i]->p[0]);
+            for (LNode *n : c.nodes)
+                for (size_t i = 0; i < n->p.size(); i++)
+                    if (n->p[i] && n->p[i]->is_virtual && n->p[i] != c.dst && n->p[i]->type != VX_TYPE_SCALAR)
+                        elided.insert(n->p[i]);
     for (LNode &ln : g->lnodes)
         for (Ref *r : ln.p) {
             if (!r || elided.count(r)) continue;

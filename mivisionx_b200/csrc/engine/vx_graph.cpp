@@ -86,6 +86,11 @@ vx_status graph_verify(Graph *g)
     cudaSetDevice(g->ctx->device);
     if (!g->stream && cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) return VX_ERROR_NO_RESOURCES;
     if (!g->ev0) { cudaEventCreate(&g->ev0); cudaEventCreate(&g->ev1); }
+    if (!g->status_host) {
+        if (cudaHostAlloc((void **)&g->status_host, 64, cudaHostAllocMapped) != cudaSuccess) return VX_ERROR_NO_MEMORY;
+        *g->status_host = 0;
+        if (cudaHostGetDevicePointer((void **)&g->status_dev, g->status_host, 0) != cudaSuccess) return VX_ERROR_NO_RESOURCES;
+    }
     vx_status s = lower_graph(g);
     if (s) return s;
     s = propagate_valid_rects(g);
@@ -178,7 +183,14 @@ vx_status graph_wait(Graph *g)
         return VX_FAILURE;
     }
     cudaEventElapsedTime(&g->gpu_ms_last, g->ev0, g->ev1);
-    // kernels that detect a failure (bounded waits, capacity) report through the plan
+    // kernels that detect a failure (bounded walks, candidate overflow) set status bits
+    if (g->status_host && *(volatile uint32_t *)g->status_host) {
+        const uint32_t st = *g->status_host;
+        *g->status_host = 0;
+        g->state = VX_GRAPH_STATE_ABANDONED;
+        log_error(g, VX_FAILURE, "ERROR: graph execution reported device status 0x%x\n", st);
+        return VX_FAILURE;
+    }
     g->state = VX_GRAPH_STATE_COMPLETED;
     return VX_SUCCESS;
 }

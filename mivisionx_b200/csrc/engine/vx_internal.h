@@ -216,6 +216,9 @@ struct Graph : Ref {
     vx_perf_t perf{};
     float gpu_ms_last = 0.f;
     uint64_t param_signature = 0;                // hash of by-value kernel parameters at capture
+    // Device-side status word (mapped pinned memory): kernels set bits on bounded-wait
+    // expiry or capacity overflow; checked after every launch.
+    uint32_t *status_host = nullptr, *status_dev = nullptr;
     std::string plan_text;                       // human-readable plan (for tests / debugging)
     std::recursive_mutex lock;
     ~Graph() override;

@@ -369,6 +369,7 @@ Graph::~Graph()
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
     for (void *p : dev_scratch) cudaFree(p);
+    if (status_host) cudaFreeHost(status_host);
 }
 
 }  // namespace agovx

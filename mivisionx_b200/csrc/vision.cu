@@ -1,0 +1,757 @@
+// vision.cu -- Canny and Harris on sm_100a: per-node kernels (the plain form), fused
+// front ends (one HBM pass over the image), union-find hysteresis and the corner pick.
+//
+// Border semantics.  The reference CPU kernels compute border columns from one byte
+// outside the row (x = -1 and x = W).  With AGO's layout (row pitch ALIGN16(W), zero
+// padding around each buffer) those bytes are: the last pixel of the previous row / the
+// first pixel of the next row when W % 16 == 0, else 0.  The values enter the interior
+// through non-maximum suppression and hysteresis, so `ago_px` reproduces them.
+#include "agocuda_internal.cuh"
+
+uint64_t agocuda_count_launch(unsigned n);
+
+namespace {
+
+__device__ __forceinline__ int ago_px(const uint8_t *src, int stride, int W, int H, int x, int y)
+{
+    if ((unsigned)y >= (unsigned)H) return 0;
+    if (x >= 0 && x < W) return src[(size_t)y * stride + x];
+    const bool tight = (W & 15) == 0;   // AGO row pitch == W: the neighbouring row's pixel
+    if (x == -1) return (tight && y > 0) ? src[(size_t)(y - 1) * stride + W - 1] : 0;
+    if (x == W) return (tight && y + 1 < H) ? src[(size_t)(y + 1) * stride] : 0;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------
+// Canny gradient: ((|gx| + |gy|) << 2) | direction, Gy negated
+// (HafCpu_CannySobel_U16_U8_3x3_L1NORM, ago_haf_cpu_canny.cpp:44;
+//  HafCpu_FastAtan2_Canny, ago_haf_cpu_arithmetic.cpp:9638)
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ int canny_dir(int gx, int gy)
+{
+    const int ax = abs(gx), ay = abs(gy);
+    const float d1 = __fmul_rn((float)ax, 0.4142135623730950488016887242097f);
+    const float d2 = __fmul_rn((float)ax, 2.4142135623730950488016887242097f);
+    int r = (gx * gy) < 0 ? 3 : 1;
+    if ((float)ay <= d1) r = 0;
+    if ((float)ay >= d2) r = 2;
+    return r;
+}
+
+__device__ __forceinline__ uint16_t canny_pack(int gx, int gy)
+{
+    int16_t t = (int16_t)(abs(gx) + abs(gy));
+    t = (int16_t)(t << 2);
+    return (uint16_t)(t | canny_dir(gx, gy));
+}
+
+// Gradient at one pixel.  `P(dx, dy)` returns the source pixel at (x+dx, y+dy) with
+// ago_px semantics.  `simd_x0` selects the reference's SIMD-body formula at x = 0
+// (W >= 16), which reads r0[-1] = 0 and r1[-1] = r0[ALIGN16(W)-1]: `r1m` is that value
+// (the vertical [1 2 1] sum of column W-1 when W % 16 == 0, else 0).
+template <class PX>
+__device__ __forceinline__ uint16_t canny_grad(PX P, bool simd_x0, int r1m)
+{
+    int gx, gy;
+    if (simd_x0) {
+        const int r0p = P(1, -1) + 2 * P(1, 0) + P(1, 1);
+        const int r1c = P(0, 1) - P(0, -1);
+        const int r1p = P(1, 1) - P(1, -1);
+        gx = (int16_t)r0p;
+        gy = (int16_t)(0 - (int16_t)(r1m + 2 * r1c + r1p));
+    } else {
+        gx = (int16_t)(P(1, -1) - P(-1, -1) + P(1, 1) - P(-1, 1) + 2 * (P(1, 0) - P(-1, 0)));
+        gy = (int16_t)(P(-1, 1) + P(1, 1) - P(-1, -1) - P(1, -1) + 2 * (P(0, 1) - P(0, -1)));
+        gy = (int16_t)(-gy);
+    }
+    return canny_pack(gx, gy);
+}
+
+// offsets of the two neighbours compared for each direction (canny.cpp:24-29)
+__device__ __constant__ int8_t kNOff[4][4] = {{-1, 0, 1, 0}, {1, -1, -1, 1}, {0, -1, 0, 1}, {-1, -1, 1, 1}};
+
+// suppression + double threshold on one pixel of the packed gradient plane G(dx, dy)
+template <class GV>
+__device__ __forceinline__ int canny_supp(GV G, int lower, int upper)
+{
+    const int c = G(0, 0);
+    const int mag = c >> 2, ang = c & 3;
+    const int a = G(kNOff[ang][0], kNOff[ang][1]) >> 2;
+    const int b = G(kNOff[ang][2], kNOff[ang][3]) >> 2;
+    const int edge = (mag > a && mag > b) ? mag : 0;
+    return edge > upper ? 255 : (edge <= lower ? 0 : 127);
+}
+
+// warp-aggregated append of one 32-bit item to a list with a device counter
+__device__ __forceinline__ void list_append(uint32_t *list, uint32_t *count, uint32_t capacity, uint32_t item, bool pred)
+{
+    const unsigned m = __ballot_sync(__activemask(), pred);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (pred) {
+        const uint32_t idx = base + __popc(m & ((1u << lane) - 1));
+        if (idx < capacity) list[idx] = item;
+    }
+}
+
+__global__ void k_canny_sobel(int W, int H, uint16_t *dst, int dstStride, const uint8_t *src, int srcStride)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    uint16_t *d = (uint16_t *)((uint8_t *)dst + (size_t)y * dstStride);
+    if (y == 0 || y == H - 1) { d[x] = 0; return; }
+    auto P = [&](int dx, int dy) { return ago_px(src, srcStride, W, H, x + dx, y + dy); };
+    const bool simd_x0 = x == 0 && W >= 16;
+    int r1m = 0;
+    if (simd_x0 && (W & 15) == 0)
+        r1m = ago_px(src, srcStride, W, H, W - 1, y - 1) + 2 * ago_px(src, srcStride, W, H, W - 1, y) +
+              ago_px(src, srcStride, W, H, W - 1, y + 1);
+    d[x] = canny_grad(P, simd_x0, r1m);
+}
+
+__global__ void k_canny_supp(int W, int H, uint8_t *dst, int dstStride, const uint16_t *g, int gStride,
+                             int lower, int upper, uint32_t *stack, uint32_t *stackCount, uint32_t capacity)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const bool in = x >= 1 && x < W - 1 && y >= 1 && y < H - 1;
+    int v = 0;
+    if (in) {
+        auto G = [&](int dx, int dy) { return (int)*(const uint16_t *)((const uint8_t *)g + (size_t)(y + dy) * gStride + 2 * (x + dx)); };
+        v = canny_supp(G, lower, upper);
+        dst[(size_t)y * dstStride + x] = (uint8_t)v;
+    }
+    list_append(stack, stackCount, capacity, ((uint32_t)y << 16) | (uint32_t)x, in && v == 255);
+}
+
+// ---------------------------------------------------------------------------------
+// Hysteresis (HafCpu_CannyEdgeTrace_U8_U8XY, ago_haf_cpu_canny.cpp:598): a pixel ends up
+// 255 iff it is 8-connected through non-zero pixels to a strong one -- computed as
+// connected components with a lock-free union-find (labels only decrease; a root r has
+// L[r] == r), then components holding a strong pixel are marked.  Fixed launch count, so
+// the whole Canny node captures into one CUDA graph.
+// ---------------------------------------------------------------------------------
+constexpr int kFindLimit = 1 << 24;   // bound on pointer chasing; exceeded only on corruption
+
+__device__ __forceinline__ int uf_find(const int *L, int x)
+{
+    for (int i = 0; i < kFindLimit; i++) {
+        const int p = __ldcg(L + x);
+        if (p == x) return x;
+        x = p;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_union(int *L, int a, int b, uint32_t *err)
+{
+    for (int i = 0; i < kFindLimit; i++) {
+        a = uf_find(L, a);
+        b = uf_find(L, b);
+        if (a == b) return;
+        if (a > b) { int t = a; a = b; b = t; }
+        const int old = atomicMin(L + b, a);
+        if (old == b) return;
+        b = old;
+    }
+    atomicOr(err, 1u);
+}
+
+__global__ void k_hyst_init(int W, int H, const uint8_t *E, int eStride, int *L)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const int p = y * W + x;
+    const bool m = x >= 1 && x < W - 1 && y >= 1 && y < H - 1 && E[(size_t)y * eStride + x] != 0;
+    L[p] = m ? p : -1;
+}
+
+__global__ void k_hyst_union(int W, int H, int *L, uint32_t *err)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W || y < 1 || y >= H - 1) return;
+    const int p = y * W + x;
+    if (__ldcg(L + p) < 0) return;
+    // the four neighbours already visited in raster order
+    if (x > 0 && __ldcg(L + p - 1) >= 0) uf_union(L, p, p - 1, err);
+    if (x > 0 && __ldcg(L + p - W - 1) >= 0) uf_union(L, p, p - W - 1, err);
+    if (__ldcg(L + p - W) >= 0) uf_union(L, p, p - W, err);
+    if (x + 1 < W && __ldcg(L + p - W + 1) >= 0) uf_union(L, p, p - W + 1, err);
+}
+
+__global__ void k_hyst_mark(int W, const int *L, const uint32_t *strong, const uint32_t *strongCount, uint32_t capacity,
+                            uint32_t *rootBits)
+{
+    const uint32_t n = min(*strongCount, capacity);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t xy = strong[i];
+        const int p = (int)(xy >> 16) * W + (int)(xy & 0xffff);
+        const int r = uf_find(L, p);
+        atomicOr(rootBits + (r >> 5), 1u << (r & 31));
+    }
+}
+
+__global__ void k_hyst_output(int W, int H, uint8_t *out, int outStride, const int *L, const uint32_t *rootBits)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const int p = y * W + x;
+    uint8_t v = 0;
+    if (__ldcg(L + p) >= 0) {
+        const int r = uf_find(L, p);
+        v = (rootBits[r >> 5] >> (r & 31)) & 1 ? 255 : 0;
+    }
+    out[(size_t)y * outStride + x] = v;
+}
+
+// ---------------------------------------------------------------------------------
+// Fused Canny front end: gradient + suppression + thresholds for a 128x16 tile, labels
+// initialised and strong pixels listed -- one read of the image, no intermediate planes.
+// ---------------------------------------------------------------------------------
+constexpr int kCTW = 128, kCTH = 16;                 // output tile
+constexpr int kCIW = kCTW + 4, kCIH = kCTH + 4;      // input tile (halo 2)
+constexpr int kCGW = kCTW + 2, kCGH = kCTH + 2;      // gradient tile (halo 1)
+
+__global__ void __launch_bounds__(256)
+k_canny_front(int W, int H, const uint8_t *src, int srcStride, int lower, int upper, int *L,
+              uint32_t *strong, uint32_t *strongCount, uint32_t capacity)
+{
+    __shared__ uint8_t sIn[kCIH][kCIW + 4];
+    __shared__ uint16_t sG[kCGH][kCGW + 2];
+    __shared__ int16_t sV[kCIH];   // per tile row: vertical sum of column W-1 for the x == 0 quirk
+    const int x0 = blockIdx.x * kCTW, y0 = blockIdx.y * kCTH;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < kCIH * kCIW; i += blockDim.x) {
+        const int r = i / kCIW, c = i % kCIW;
+        sIn[r][c] = (uint8_t)ago_px(src, srcStride, W, H, x0 - 2 + c, y0 - 2 + r);
+    }
+    const bool needV = x0 == 0 && (W & 15) == 0 && W >= 16;
+    if (needV && tid < kCIH - 2) {
+        const int y = y0 - 1 + tid;   // gradient row
+        sV[tid] = (y >= 1 && y < H - 1)
+            ? (int16_t)(ago_px(src, srcStride, W, H, W - 1, y - 1) + 2 * ago_px(src, srcStride, W, H, W - 1, y) +
+                        ago_px(src, srcStride, W, H, W - 1, y + 1))
+            : 0;
+    }
+    __syncthreads();
+    for (int i = tid; i < kCGH * kCGW; i += blockDim.x) {
+        const int r = i / kCGW, c = i % kCGW;
+        const int x = x0 - 1 + c, y = y0 - 1 + r;
+        uint16_t g = 0;
+        if (y >= 1 && y < H - 1 && x >= 0 && x < W) {
+            auto P = [&](int dx, int dy) { return (int)sIn[r + 1 + dy][c + 1 + dx]; };
+            const bool simd_x0 = x == 0 && W >= 16;
+            g = canny_grad(P, simd_x0, simd_x0 && (W & 15) == 0 ? (int)sV[r] : 0);
+        }
+        sG[r][c] = g;
+    }
+    __syncthreads();
+    for (int i = tid; i < kCTH * kCTW; i += blockDim.x) {
+        const int r = i / kCTW, c = i % kCTW;
+        const int x = x0 + c, y = y0 + r;
+        if (x >= W || y >= H) continue;
+        const bool in = x >= 1 && x < W - 1 && y >= 1 && y < H - 1;
+        int v = 0;
+        if (in) {
+            auto G = [&](int dx, int dy) { return (int)sG[r + 1 + dy][c + 1 + dx]; };
+            v = canny_supp(G, lower, upper);
+        }
+        const int p = y * W + x;
+        L[p] = v ? p : -1;
+        list_append(strong, strongCount, capacity, ((uint32_t)y << 16) | (uint32_t)x, v == 255);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Harris (ago_haf_cpu_harris.cpp): HG3 = {gx*gx, gx*gy, gy*gy} of the integer 3x3 Sobel
+// (exact in float), 3x3 window sums (exact: integers below 2^24), then the score in
+// round-to-nearest float with the reference's operation order (no FMA).
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ float harris_score(float gx2, float gxy2, float gy2, float k, float Tc, float norm)
+{
+    const float traceA = __fadd_rn(gx2, gy2);
+    const float detA = __fsub_rn(__fmul_rn(gx2, gy2), __fmul_rn(gxy2, gxy2));
+    float Mc = __fsub_rn(detA, __fmul_rn(__fmul_rn(k, traceA), traceA));
+    Mc = __fdiv_rn(Mc, norm);
+    return Mc > Tc ? Mc : 0.0f;
+}
+
+template <class PX>
+__device__ __forceinline__ void harris_grad(PX P, float &gxx, float &gxy, float &gyy)
+{
+    const int gx = (int16_t)((P(1, 1) - P(-1, 1)) + (P(1, -1) - P(-1, -1)) + 2 * (P(1, 0) - P(-1, 0)));
+    const int gy = (int16_t)((P(-1, 1) + 2 * P(0, 1) + P(1, 1)) - (P(-1, -1) + 2 * P(0, -1) + P(1, -1)));
+    gxx = __fmul_rn((float)gx, (float)gx);
+    gxy = __fmul_rn((float)gx, (float)gy);
+    gyy = __fmul_rn((float)gy, (float)gy);
+}
+
+__global__ void k_harris_sobel(int W, int H, float *dst, int dstStride, const uint8_t *src, int srcStride)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    float *d = (float *)((uint8_t *)dst + (size_t)y * dstStride) + 3 * x;
+    if (y == 0 || y == H - 1) { d[0] = d[1] = d[2] = 0.f; return; }
+    auto P = [&](int dx, int dy) { return ago_px(src, srcStride, W, H, x + dx, y + dy); };
+    harris_grad(P, d[0], d[1], d[2]);
+}
+
+__global__ void k_harris_score(int W, int H, float *dst, int dstStride, const float *hg, int hgStride, float k, float Tc, float norm)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    float v = 0.f;
+    if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1) {
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+        for (int j = -1; j <= 1; j++) {
+            const float *r = (const float *)((const uint8_t *)hg + (size_t)(y + j) * hgStride);
+            for (int i = -1; i <= 1; i++) {
+                s0 = __fadd_rn(s0, r[3 * (x + i)]);
+                s1 = __fadd_rn(s1, r[3 * (x + i) + 1]);
+                s2 = __fadd_rn(s2, r[3 * (x + i) + 2]);
+            }
+        }
+        v = harris_score(s0, s1, s2, k, Tc, norm);
+    }
+    *(float *)((uint8_t *)dst + (size_t)y * dstStride + 4 * x) = v;
+}
+
+// XYS record (ago_keypoint_xys_t): int16 x, int16 y, float s -- 8 bytes, read as one int64
+// sort key (strength bits, then y, then x), exactly how the reference sorts it.
+__device__ __forceinline__ uint64_t xys_pack(int x, int y, float s)
+{
+    return (uint64_t)(uint16_t)x | ((uint64_t)(uint16_t)y << 16) | ((uint64_t)__float_as_uint(s) << 32);
+}
+
+// non-maximum suppression rule of HafCpu_NonMaxSupp_XY_ANY_3x3 (harris.cpp:882)
+template <class SV>
+__device__ __forceinline__ bool harris_nms(SV S)
+{
+    const float v = S(0, 0);
+    return v >= S(-1, -1) && v >= S(0, -1) && v >= S(1, -1) && v >= S(-1, 0) && v > S(1, 0) &&
+           v > S(-1, 1) && v > S(0, 1) && v > S(1, 1);
+}
+
+__device__ __forceinline__ void xys_append(uint64_t *list, uint32_t *count, uint32_t capacity, uint64_t item, bool pred)
+{
+    const unsigned m = __ballot_sync(__activemask(), pred);
+    if (!m) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (pred) {
+        const uint32_t idx = base + __popc(m & ((1u << lane) - 1));
+        if (idx < capacity) list[idx] = item;
+    }
+}
+
+__global__ void k_harris_nms(int W, int H, const float *sc, int scStride, uint64_t *list, uint32_t *count, uint32_t capacity)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    const bool in = x >= 1 && x < W - 1 && y >= 1 && y < H - 1;
+    bool keep = false;
+    float v = 0.f;
+    if (in) {
+        auto S = [&](int dx, int dy) { return *(const float *)((const uint8_t *)sc + (size_t)(y + dy) * scStride + 4 * (x + dx)); };
+        keep = harris_nms(S);
+        v = S(0, 0);
+    }
+    xys_append(list, count, capacity, xys_pack(x, y, v), keep);
+}
+
+// Fused Harris front end: Sobel products, window sums, score and NMS for a 64x16 tile.
+constexpr int kHTW = 64, kHTH = 16;
+constexpr int kHIW = kHTW + 6, kHIH = kHTH + 6;   // input halo 3
+constexpr int kHGW = kHTW + 4, kHGH = kHTH + 4;   // HG3 halo 2
+constexpr int kHSW = kHTW + 2, kHSH = kHTH + 2;   // score halo 1
+
+__global__ void __launch_bounds__(256)
+k_harris_front(int W, int H, const uint8_t *src, int srcStride, float k, float Tc, float norm,
+               uint64_t *list, uint32_t *count, uint32_t capacity)
+{
+    __shared__ uint8_t sIn[kHIH][kHIW + 2];
+    __shared__ float sG[3][kHGH][kHGW + 1];
+    __shared__ float sS[kHSH][kHSW + 1];
+    const int x0 = blockIdx.x * kHTW, y0 = blockIdx.y * kHTH, tid = threadIdx.x;
+    for (int i = tid; i < kHIH * kHIW; i += blockDim.x) {
+        const int r = i / kHIW, c = i % kHIW;
+        sIn[r][c] = (uint8_t)ago_px(src, srcStride, W, H, x0 - 3 + c, y0 - 3 + r);
+    }
+    __syncthreads();
+    for (int i = tid; i < kHGH * kHGW; i += blockDim.x) {
+        const int r = i / kHGW, c = i % kHGW;
+        const int x = x0 - 2 + c, y = y0 - 2 + r;
+        float a = 0.f, b = 0.f, d = 0.f;
+        if (y >= 1 && y < H - 1 && x >= 0 && x < W) {
+            auto P = [&](int dx, int dy) { return (int)sIn[r + 1 + dy][c + 1 + dx]; };
+            harris_grad(P, a, b, d);
+        }
+        sG[0][r][c] = a; sG[1][r][c] = b; sG[2][r][c] = d;
+    }
+    __syncthreads();
+    for (int i = tid; i < kHSH * kHSW; i += blockDim.x) {
+        const int r = i / kHSW, c = i % kHSW;
+        const int x = x0 - 1 + c, y = y0 - 1 + r;
+        float v = 0.f;
+        if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1) {
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+            for (int j = 0; j < 3; j++)
+                for (int q = 0; q < 3; q++) {
+                    s0 = __fadd_rn(s0, sG[0][r + j][c + q]);
+                    s1 = __fadd_rn(s1, sG[1][r + j][c + q]);
+                    s2 = __fadd_rn(s2, sG[2][r + j][c + q]);
+                }
+            v = harris_score(s0, s1, s2, k, Tc, norm);
+        }
+        sS[r][c] = v;
+    }
+    __syncthreads();
+    for (int i = tid; i < kHTH * kHTW; i += blockDim.x) {
+        const int r = i / kHTW, c = i % kHTW;
+        const int x = x0 + c, y = y0 + r;
+        const bool in = x >= 1 && x < W - 1 && y >= 1 && y < H - 1;
+        bool keep = false;
+        if (in) {
+            auto S = [&](int dx, int dy) { return sS[r + 1 + dy][c + 1 + dx]; };
+            keep = harris_nms(S);
+        }
+        xys_append(list, count, capacity, xys_pack(x, y, in ? sS[r + 1][c + 1] : 0.f), keep);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Corner pick (HafCpu_HarrisMergeSortAndPick_XY_XYS, harris.cpp:923).  Reference: sort the
+// candidates descending as int64, then walk them in order keeping a point when its grid cell
+// is empty and no kept point in the 5x5 cells around is closer than min_dist2.  That is the
+// greedy maximal independent set of the conflict graph (same cell, or within the cell
+// window and closer than min_dist2) in sorted order; it is computed here in rounds: a
+// candidate is kept once every conflicting predecessor is rejected, and rejected as soon as
+// one is kept -- the same set, in parallel.  One CTA; candidates sit in shared memory.
+// ---------------------------------------------------------------------------------
+constexpr int kPickMax = 8192;                 // candidates held in shared memory
+constexpr int kPickHash = 2 * kPickMax;        // open-addressing cell table
+
+struct PickSmem {
+    uint64_t key[kPickMax];
+    int next[kPickMax];
+    int head[kPickHash];
+    uint8_t state[kPickMax];   // 0 undecided, 1 kept, 2 rejected
+    int changed, undecided, kept;
+};
+
+__device__ __forceinline__ int kx(uint64_t k) { return (int)(int16_t)(k & 0xffff); }
+__device__ __forceinline__ int ky(uint64_t k) { return (int)(int16_t)((k >> 16) & 0xffff); }
+__device__ __forceinline__ float ks(uint64_t k) { return __uint_as_float((uint32_t)(k >> 32)); }
+__device__ __forceinline__ uint32_t hcell(int cx, int cy) { return ((uint32_t)cx * 73856093u) ^ ((uint32_t)cy * 19349663u); }
+
+__global__ void __launch_bounds__(1024)
+k_harris_pick(const uint64_t *list, const uint32_t *listCount, uint32_t listCapacity, float minDistance,
+              int cell, int gridW, int gridH, vx_keypoint_like *out, uint32_t outCapacity, uint32_t *outCount,
+              uint32_t *numCorners, uint32_t *status)
+{
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    PickSmem &S = *reinterpret_cast<PickSmem *>(smem_raw);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int n = (int)min(*listCount, listCapacity);
+    if (n > kPickMax) {   // more candidates than this kernel holds: report, emit nothing
+        if (tid == 0) { atomicOr(status, 2u); *outCount = 0; if (numCorners) *numCorners = 0; }
+        return;
+    }
+    int np2 = 1;
+    while (np2 < n) np2 <<= 1;
+    for (int i = tid; i < np2; i += nt) S.key[i] = i < n ? list[i] : 0;   // 0 sorts last (descending)
+    __syncthreads();
+    // bitonic sort, descending by the signed int64 value
+    for (int k = 2; k <= np2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < np2; i += nt) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const int64_t a = (int64_t)S.key[i], b = (int64_t)S.key[l];
+                    const bool desc = (i & k) == 0;
+                    if (desc ? (a < b) : (a > b)) { S.key[i] = (uint64_t)b; S.key[l] = (uint64_t)a; }
+                }
+            }
+            __syncthreads();
+        }
+    const bool useGrid = minDistance > 2.0f;
+    if (useGrid) {
+        for (int i = tid; i < kPickHash; i += nt) S.head[i] = -1;
+        for (int i = tid; i < n; i += nt) { S.next[i] = -1; S.state[i] = 0; }
+        __syncthreads();
+        // cell lists (any order inside a cell; priorities come from sorted indices)
+        for (int i = tid; i < n; i += nt) {
+            const int cx = kx(S.key[i]) / cell, cy = ky(S.key[i]) / cell;
+            uint32_t h = hcell(cx, cy) & (kPickHash - 1);
+            for (int probe = 0; probe < kPickHash; probe++, h = (h + 1) & (kPickHash - 1)) {
+                int cur = atomicCAS(&S.head[h], -1, i);
+                if (cur == -1) break;                       // new cell: i heads it
+                const int ccx = kx(S.key[cur]) / cell, ccy = ky(S.key[cur]) / cell;
+                if (ccx == cx && ccy == cy) {               // same cell: push i in front of its list
+                    int prev = S.head[h];
+                    for (int t = 0; t < kPickMax; t++) {
+                        S.next[i] = prev;
+                        const int got = atomicCAS(&S.head[h], prev, i);
+                        if (got == prev) break;
+                        prev = got;
+                    }
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        const int md2 = (int)ceilf(__fmul_rn(minDistance, minDistance));
+        for (int round = 0; round <= n; round++) {
+            if (tid == 0) S.changed = 0;
+            __syncthreads();
+            for (int i = tid; i < n; i += nt) {
+                if (S.state[i]) continue;
+                const int x = kx(S.key[i]), y = ky(S.key[i]);
+                const int cx = x / cell, cy = y / cell;
+                bool blocked = false, waiting = false;
+                for (int yy = max(cy - 2, 0); yy <= min(cy + 2, gridH - 1) && !blocked; yy++)
+                    for (int xx = max(cx - 2, 0); xx <= min(cx + 2, gridW - 1) && !blocked; xx++) {
+                        uint32_t h = hcell(xx, yy) & (kPickHash - 1);
+                        int j = -1;
+                        for (int probe = 0; probe < kPickHash; probe++, h = (h + 1) & (kPickHash - 1)) {
+                            const int c = S.head[h];
+                            if (c < 0) break;
+                            if (kx(S.key[c]) / cell == xx && ky(S.key[c]) / cell == yy) { j = c; break; }
+                        }
+                        for (; j >= 0; j = S.next[j]) {
+                            if (j >= i) continue;   // only higher-priority candidates matter
+                            const int dx = kx(S.key[j]) - x, dy = ky(S.key[j]) - y;
+                            const bool conflict = (xx == cx && yy == cy) || (dx * dx + dy * dy < md2);
+                            if (!conflict) continue;
+                            const uint8_t sj = S.state[j];
+                            if (sj == 1) { blocked = true; break; }
+                            if (sj == 0) waiting = true;
+                        }
+                    }
+                if (blocked) { S.state[i] = 2; S.changed = 1; }
+                else if (!waiting) { S.state[i] = 1; S.changed = 1; }
+            }
+            __syncthreads();
+            const int ch = S.changed;
+            __syncthreads();
+            if (!ch) break;
+        }
+    } else {
+        for (int i = tid; i < n; i += nt) S.state[i] = 1;
+        __syncthreads();
+    }
+    // compact kept candidates in sorted order (block-wide scan in chunks of nt)
+    if (tid == 0) S.kept = 0;
+    __syncthreads();
+    __shared__ int warpSums[32];
+    for (int base = 0; base < n; base += nt) {
+        const int i = base + tid;
+        const int f = (i < n && S.state[i] == 1) ? 1 : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        const int lane = tid & 31, w = tid >> 5;
+        if (lane == 0) warpSums[w] = __popc(m);
+        __syncthreads();
+        int off = 0;
+        for (int q = 0; q < w; q++) off += warpSums[q];
+        const int pos = S.kept + off + __popc(m & ((1u << lane) - 1));
+        if (f && pos < (int)outCapacity) {
+            const uint64_t kk = S.key[i];
+            vx_keypoint_like kp;
+            kp.x = kx(kk); kp.y = ky(kk); kp.strength = ks(kk);
+            kp.scale = 0.f; kp.orientation = 0.f; kp.tracking_status = 1; kp.error = 0.f;
+            out[pos] = kp;
+        }
+        __syncthreads();
+        if (tid == 0) { int t = 0; for (int q = 0; q < (nt + 31) / 32; q++) t += warpSums[q]; S.kept += t; }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        *outCount = min((uint32_t)S.kept, outCapacity);
+        if (numCorners) *numCorners = (uint32_t)S.kept;
+    }
+}
+
+bool aligned(const void *p, unsigned a) { return ((uintptr_t)p & (a - 1)) == 0; }
+
+}  // namespace
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+static dim3 row_grid(uint32_t W, uint32_t H, unsigned bx) { return dim3(div_up(W, bx), H, 1); }
+
+extern "C" int agocuda_CannySobel_U16_U8_3x3_L1NORM(void *stream, uint32_t W, uint32_t H, uint16_t *pDst, uint32_t dstStride,
+                                                    const uint8_t *pSrc, uint32_t srcStride)
+{
+    if (!pDst || !pSrc || W < 3 || H < 3 || dstStride < 2 * W || srcStride < W || !aligned(pDst, 2) || (dstStride & 1))
+        return AGOCUDA_INVALID_PARAMS;
+    k_canny_sobel<<<row_grid(W, H, 128), 128, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_CannySuppThreshold_U8XY_U16_3x3(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                                       const uint16_t *pSrc, uint32_t srcStride, uint32_t *pStack,
+                                                       uint32_t *pStackCount, uint32_t stackCapacity,
+                                                       uint16_t hystLower, uint16_t hystUpper)
+{
+    if (!pDst || !pSrc || !pStack || !pStackCount || W < 3 || H < 3 || dstStride < W || srcStride < 2 * W)
+        return AGOCUDA_INVALID_PARAMS;
+    cudaMemsetAsync(pStackCount, 0, sizeof(uint32_t), as_stream(stream));
+    k_canny_supp<<<row_grid(W, H, 128), 128, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride,
+                                                                      hystLower, hystUpper, pStack, pStackCount, stackCapacity);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" size_t agocuda_CannyEdgeTrace_scratch_size(uint32_t W, uint32_t H)
+{
+    const size_t n = (size_t)W * H;
+    return n * sizeof(int) + ((n + 31) / 32) * sizeof(uint32_t) + 256;
+}
+
+// shared by the per-node edge trace and the fused Canny
+static int hysteresis_tail(cudaStream_t s, int W, int H, uint8_t *out, int outStride, int *L, uint32_t *bits,
+                           const uint32_t *strong, const uint32_t *strongCount, uint32_t capacity, uint32_t *err)
+{
+    const size_t n = (size_t)W * H;
+    cudaMemsetAsync(bits, 0, ((n + 31) / 32) * sizeof(uint32_t), s);
+    k_hyst_union<<<row_grid(W, H, 256), 256, 0, s>>>(W, H, L, err);
+    k_hyst_mark<<<1184, 256, 0, s>>>(W, L, strong, strongCount, capacity, bits);
+    k_hyst_output<<<row_grid(W, H, 256), 256, 0, s>>>(W, H, out, outStride, L, bits);
+    agocuda_count_launch(3);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_CannyEdgeTrace_U8_U8XY(void *stream, uint32_t W, uint32_t H, uint8_t *pImg, uint32_t stride,
+                                              const uint32_t *pStack, const uint32_t *pStackCount, uint32_t stackCapacity,
+                                              void *scratch, size_t scratchBytes, uint32_t *pStatus)
+{
+    if (!pImg || !pStack || !pStackCount || !scratch || !pStatus || W < 3 || H < 3 || stride < W || W > 65535 || H > 65535 ||
+        (size_t)W * H >= (1ull << 31) || scratchBytes < agocuda_CannyEdgeTrace_scratch_size(W, H) || !aligned(scratch, 256))
+        return AGOCUDA_INVALID_PARAMS;
+    int *L = (int *)scratch;
+    uint32_t *bits = (uint32_t *)((uint8_t *)scratch + (((size_t)W * H * sizeof(int) + 255) & ~(size_t)255));
+    cudaStream_t s = as_stream(stream);
+    k_hyst_init<<<row_grid(W, H, 256), 256, 0, s>>>((int)W, (int)H, pImg, (int)stride, L);
+    agocuda_count_launch(1);
+    return hysteresis_tail(s, (int)W, (int)H, pImg, (int)stride, L, bits, pStack, pStackCount, stackCapacity, pStatus);
+}
+
+extern "C" int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                                      const uint8_t *pSrc, uint32_t srcStride, uint16_t hystLower,
+                                                      uint16_t hystUpper, void *scratch, size_t scratchBytes, uint32_t *pStatus)
+{
+    const size_t n = (size_t)W * H;
+    const size_t need = agocuda_CannyEdgeTrace_scratch_size(W, H) + n * sizeof(uint32_t) + 512;
+    if (!pDst || !pSrc || !scratch || !pStatus || W < 3 || H < 3 || dstStride < W || srcStride < W || W > 65535 ||
+        H > 65535 || n >= (1ull << 31) || scratchBytes < need || !aligned(scratch, 256))
+        return AGOCUDA_INVALID_PARAMS;
+    uint8_t *sp = (uint8_t *)scratch;
+    int *L = (int *)sp;                         sp += (n * sizeof(int) + 255) & ~(size_t)255;
+    uint32_t *bits = (uint32_t *)sp;            sp += (((n + 31) / 32) * 4 + 255) & ~(size_t)255;
+    uint32_t *cnt = (uint32_t *)sp;             sp += 256;
+    uint32_t *strong = (uint32_t *)sp;
+    cudaStream_t s = as_stream(stream);
+    cudaMemsetAsync(cnt, 0, 4, s);
+    dim3 grd(div_up(W, kCTW), div_up(H, kCTH));
+    k_canny_front<<<grd, 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper, L, strong, cnt, (uint32_t)n);
+    agocuda_count_launch(1);
+    return hysteresis_tail(s, (int)W, (int)H, pDst, (int)dstStride, L, bits, strong, cnt, (uint32_t)n, pStatus);
+}
+
+extern "C" size_t agocuda_fused_CannyEdgeDetector_scratch_size(uint32_t W, uint32_t H)
+{
+    return agocuda_CannyEdgeTrace_scratch_size(W, H) + (size_t)W * H * sizeof(uint32_t) + 512 + 1024;
+}
+
+extern "C" int agocuda_HarrisSobel_HG3_U8_3x3(void *stream, uint32_t W, uint32_t H, float *pDst, uint32_t dstStride,
+                                              const uint8_t *pSrc, uint32_t srcStride)
+{
+    if (!pDst || !pSrc || W < 3 || H < 3 || dstStride < 12 * W || srcStride < W || !aligned(pDst, 4) || (dstStride & 3))
+        return AGOCUDA_INVALID_PARAMS;
+    k_harris_sobel<<<row_grid(W, H, 128), 128, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_HarrisScore_HVC_HG3_3x3(void *stream, uint32_t W, uint32_t H, float *pDst, uint32_t dstStride,
+                                               const float *pSrc, uint32_t srcStride, float sensitivity,
+                                               float strengthThreshold, float normFactor)
+{
+    if (!pDst || !pSrc || W < 3 || H < 3 || dstStride < 4 * W || srcStride < 12 * W || !aligned(pDst, 4) || !aligned(pSrc, 4))
+        return AGOCUDA_INVALID_PARAMS;
+    k_harris_score<<<row_grid(W, H, 128), 128, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride,
+                                                                       sensitivity, strengthThreshold, normFactor);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_NonMaxSupp_XY_ANY_3x3(void *stream, uint32_t W, uint32_t H, const float *pSrc, uint32_t srcStride,
+                                             uint64_t *pList, uint32_t *pListCount, uint32_t listCapacity)
+{
+    if (!pSrc || !pList || !pListCount || W < 3 || H < 3 || srcStride < 4 * W || !aligned(pSrc, 4))
+        return AGOCUDA_INVALID_PARAMS;
+    cudaMemsetAsync(pListCount, 0, 4, as_stream(stream));
+    k_harris_nms<<<row_grid(W, H, 128), 128, 0, as_stream(stream)>>>((int)W, (int)H, pSrc, (int)srcStride, pList, pListCount, listCapacity);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_HarrisMergeSortAndPick_XY_XYS(void *stream, uint32_t W, uint32_t H, const uint64_t *pList,
+                                                     const uint32_t *pListCount, uint32_t listCapacity, float minDistance,
+                                                     void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
+                                                     uint32_t *pNumCorners, uint32_t *pStatus)
+{
+    if (!pList || !pListCount || !pCorners || !pCornerCount || !pStatus || !W || !H || !(minDistance > 0.0f))
+        return AGOCUDA_INVALID_PARAMS;
+    // grid geometry of ago_kernel_api.cpp:20806-20809
+    int cell = 1, gw = 1, gh = 1;
+    if (minDistance > 2.0f) {
+        cell = (int)floor((double)minDistance / 1.41421356237309504880);
+        gw = (int)((W + cell - 1) / cell);
+        gh = (int)((H + cell - 1) / cell);
+    }
+    static bool attr = false;
+    const int smem = (int)sizeof(PickSmem);
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_harris_pick, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+            return agocuda_launch_status();
+        attr = true;
+    }
+    k_harris_pick<<<1, 1024, smem, as_stream(stream)>>>(pList, pListCount, listCapacity, minDistance, cell, gw, gh,
+                                                        (vx_keypoint_like *)pCorners, cornerCapacity, pCornerCount,
+                                                        pNumCorners, pStatus);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t W, uint32_t H, const uint8_t *pSrc, uint32_t srcStride,
+                                               float sensitivity, float strengthThreshold, float normFactor, float minDistance,
+                                               void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
+                                               uint32_t *pNumCorners, void *scratch, size_t scratchBytes, uint32_t *pStatus)
+{
+    const uint32_t cap = kPickMax * 4;   // candidate list capacity (the pick reports overflow)
+    if (!pSrc || !pCorners || !pCornerCount || !scratch || !pStatus || W < 3 || H < 3 || srcStride < W ||
+        scratchBytes < 256 + (size_t)cap * 8 || !aligned(scratch, 256))
+        return AGOCUDA_INVALID_PARAMS;
+    uint32_t *cnt = (uint32_t *)scratch;
+    uint64_t *list = (uint64_t *)((uint8_t *)scratch + 256);
+    cudaStream_t s = as_stream(stream);
+    cudaMemsetAsync(cnt, 0, 4, s);
+    dim3 grd(div_up(W, kHTW), div_up(H, kHTH));
+    k_harris_front<<<grd, 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, sensitivity, strengthThreshold, normFactor, list, cnt, cap);
+    agocuda_count_launch(1);
+    int rc = agocuda_launch_status();
+    if (rc) return rc;
+    return agocuda_HarrisMergeSortAndPick_XY_XYS(stream, W, H, list, cnt, cap, minDistance, pCorners, cornerCapacity,
+                                                 pCornerCount, pNumCorners, pStatus);
+}
+
+extern "C" size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t, uint32_t) { return 256 + (size_t)kPickMax * 4 * 8; }

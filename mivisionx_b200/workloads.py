@@ -170,3 +170,46 @@ class Cfg1Graph:
 
     def results(self):
         return [(self.api.read_plane(o), self.api.valid_region(o)) for o in self.outputs]
+
+
+class Cfg2Graph:
+    """CannyEdgeDetector (3x3 gradient, L1 norm, hysteresis lower/upper) and HarrisCorners
+    (gradient 3, block 3, sensitivity k, strength threshold, min distance) on the same U8
+    input, for each of `sizes` frames, all in one OpenVX graph."""
+
+    def __init__(self, api: V.OpenVX, ctx, sizes, lower=80, upper=100, k=0.04, strength=1e-3, min_distance=5.0,
+                 capacity=32768, flags: int | None = None):
+        self.api, self.ctx = api, ctx
+        a = api
+        self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
+        if flags is not None:
+            a.set_optimizer_flags(self.graph, flags)
+        self.hyst = a.threshold_range(ctx, lower, upper)
+        self.s_strength = a.scalar(ctx, V.VX_TYPE_FLOAT32, strength)
+        self.s_mind = a.scalar(ctx, V.VX_TYPE_FLOAT32, min_distance)
+        self.s_k = a.scalar(ctx, V.VX_TYPE_FLOAT32, k)
+        self.inputs, self.edges, self.corners, self.num = [], [], [], []
+        g = self.graph
+        for (w, h) in sizes:
+            src = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+            edge = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+            arr = a.obj(a.vxCreateArray(ctx, V.VX_TYPE_KEYPOINT, capacity), "array")
+            num = a.scalar(ctx, V.VX_TYPE_SIZE, 0)
+            a.obj(a.vxCannyEdgeDetectorNode(g, src, self.hyst, 3, V.VX_NORM_L1, edge), "canny node")
+            a.obj(a.vxHarrisCornersNode(g, src, self.s_strength, self.s_mind, self.s_k, 3, 3, arr, num), "harris node")
+            self.inputs.append(src); self.edges.append(edge); self.corners.append(arr); self.num.append(num)
+        a.ok(a.vxVerifyGraph(g), "vxVerifyGraph")
+
+    def run(self, frames=None):
+        a = self.api
+        if frames is not None:
+            for img, f in zip(self.inputs, frames):
+                a.write_plane(img, f)
+        a.ok(a.vxProcessGraph(self.graph), "vxProcessGraph")
+
+    def results(self):
+        a = self.api
+        out = []
+        for e, arr, num in zip(self.edges, self.corners, self.num):
+            out.append((a.read_plane(e), a.valid_region(e), a.array_items(arr), a.read_scalar(num)))
+        return out

@@ -33,7 +33,83 @@ def fn(name):
 
 
 def ago_img(h, w, dtype=np.uint8, channels=1):
-    return Img(h, w, dtype, channels=channels, align_off=0)
+    """Buffer laid out as AGO allocates images: 16-byte row pitch, zero padding around."""
+    bpp = np.dtype(dtype).itemsize * channels
+    return Img(h, w, dtype, channels=channels, stride=((w * bpp + 15) // 16) * 16, pad=4, align_off=0)
+
+
+_SIGS.update({
+    "CannySobel_U16_U8_3x3_L1NORM": [u32, u32, vp, u32, vp, u32],
+    "CannySuppThreshold_U8XY_U16_3x3": [u32, vp, C.POINTER(C.c_uint32), u32, u32, vp, u32, vp, u32, C.c_uint16, C.c_uint16],
+    "CannyEdgeTrace_U8_U8XY": [u32, u32, vp, u32, u32, vp, u32],
+    "HarrisSobel_HG3_U8_3x3": [u32, u32, vp, u32, vp, u32],
+    "HarrisScore_HVC_HG3_3x3": [u32, u32, vp, u32, vp, u32, C.c_float, C.c_float, C.c_float],
+    "NonMaxSupp_XY_ANY_3x3": [u32, vp, C.POINTER(C.c_uint32), u32, u32, vp, u32],
+    "HarrisMergeSortAndPick_XY_XYS": [u32, vp, C.POINTER(C.c_uint32), vp, u32, C.c_float, u32, u32],
+})
+
+XYS = np.dtype([("x", "<i2"), ("y", "<i2"), ("s", "<f4")])
+KP = np.dtype([("x", "<i4"), ("y", "<i4"), ("strength", "<f4"), ("scale", "<f4"), ("orientation", "<f4"),
+               ("tracking_status", "<i4"), ("error", "<f4")])
+
+
+def harris_norm(gs=3):
+    f = fn("harris_norm_factor")
+    f.argtypes = [i32]
+    f.restype = C.c_float
+    return f(gs)
+
+
+def canny_parts(img: np.ndarray, lower=80, upper=100):
+    """CannySobel, CannySuppThreshold, CannyEdgeTrace as AGO calls them; returns the packed
+    gradient plane, the 0/127/255 map, the strong stack and the final edge map."""
+    h, w = img.shape
+    src = ago_img(h, w); src.set(img)
+    sob = ago_img(h, w, np.uint16)
+    out = ago_img(h, w)
+    stack = np.zeros(w * h, np.uint32)
+    top = C.c_uint32(0)
+    fn("CannySobel_U16_U8_3x3_L1NORM")(w, h, sob.ptr, sob.stride, src.ptr, src.stride)
+    fn("CannySuppThreshold_U8XY_U16_3x3")(w * h, stack.ctypes.data, C.byref(top), w, h, out.ptr, out.stride,
+                                          sob.ptr, sob.stride, lower, upper)
+    supp = out.get()
+    strong = stack[:top.value].copy()
+    fn("CannyEdgeTrace_U8_U8XY")(w, h, out.ptr, out.stride, w * h, stack.ctypes.data, top.value)
+    return sob.get(), supp, strong, out.get()
+
+
+def canny(img: np.ndarray, lower=80, upper=100):
+    """vxCannyEdgeDetectorNode (3x3, L1): edge map and valid rectangle."""
+    h, w = img.shape
+    return canny_parts(img, lower, upper)[3], (2, 2, w - 2, h - 2)
+
+
+def harris_parts(img: np.ndarray, k=0.04, tc=1e-3):
+    h, w = img.shape
+    src = ago_img(h, w); src.set(img)
+    hg3 = ago_img(h, w, np.float32, 3)
+    hvc = ago_img(h, w, np.float32)
+    lst = np.zeros(w * h, XYS)
+    cnt = C.c_uint32(0)
+    fn("HarrisSobel_HG3_U8_3x3")(w, h, hg3.ptr, hg3.stride, src.ptr, src.stride)
+    fn("HarrisScore_HVC_HG3_3x3")(w, h, hvc.ptr, hvc.stride, hg3.ptr, hg3.stride, k, tc, harris_norm(3))
+    fn("NonMaxSupp_XY_ANY_3x3")(w * h, lst.ctypes.data, C.byref(cnt), w, h, hvc.ptr, hvc.stride)
+    return hg3.get(), hvc.get(), lst[:cnt.value].copy()
+
+
+def harris_pick(lst: np.ndarray, w, h, min_distance=5.0, capacity=1 << 20):
+    lst = lst.copy()
+    out = np.zeros(max(1, capacity), KP)
+    cnt = C.c_uint32(0)
+    fn("HarrisMergeSortAndPick_XY_XYS")(capacity, out.ctypes.data, C.byref(cnt), lst.ctypes.data, len(lst),
+                                        min_distance, w, h)
+    return out[:min(cnt.value, capacity)], cnt.value
+
+
+def harris(img: np.ndarray, k=0.04, tc=1e-3, min_distance=5.0, capacity=1 << 20):
+    """vxHarrisCornersNode (gradient 3, block 3): (corners, num_corners)."""
+    h, w = img.shape
+    return harris_pick(harris_parts(img, k, tc)[2], w, h, min_distance, capacity)
 
 
 def shrink(rect, n):

@@ -1,0 +1,156 @@
+"""GPU parity of the Canny / Harris kernels of include/agocuda.h against the oracle parts
+(bit-exact; lists compared as sets where the device emits them in arbitrary order)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle_chains as OC
+from mivisionx_b200 import workloads as WL
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(64, 48), (37, 19), (200, 120), (1920, 1080)]
+
+u32, vp, u16, f32, sz = C.c_uint32, C.c_void_p, C.c_uint16, C.c_float, C.c_size_t
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from mivisionx_b200 import native
+    L = native.agocuda()
+    sigs = {
+        "agocuda_CannySobel_U16_U8_3x3_L1NORM": [vp, u32, u32, vp, u32, vp, u32],
+        "agocuda_CannySuppThreshold_U8XY_U16_3x3": [vp, u32, u32, vp, u32, vp, u32, vp, vp, u32, u16, u16],
+        "agocuda_CannyEdgeTrace_U8_U8XY": [vp, u32, u32, vp, u32, vp, vp, u32, vp, sz, vp],
+        "agocuda_fused_CannyEdgeDetector_3x3_L1": [vp, u32, u32, vp, u32, vp, u32, u16, u16, vp, sz, vp],
+        "agocuda_HarrisSobel_HG3_U8_3x3": [vp, u32, u32, vp, u32, vp, u32],
+        "agocuda_HarrisScore_HVC_HG3_3x3": [vp, u32, u32, vp, u32, vp, u32, f32, f32, f32],
+        "agocuda_NonMaxSupp_XY_ANY_3x3": [vp, u32, u32, vp, u32, vp, vp, u32],
+        "agocuda_HarrisMergeSortAndPick_XY_XYS": [vp, u32, u32, vp, vp, u32, f32, vp, u32, vp, vp, vp],
+        "agocuda_fused_HarrisCorners_3x3": [vp, u32, u32, vp, u32, f32, f32, f32, f32, vp, u32, vp, vp, vp, sz, vp],
+    }
+    for n, a in sigs.items():
+        getattr(L, n).argtypes = a
+        getattr(L, n).restype = C.c_int
+    for n in ("agocuda_CannyEdgeTrace_scratch_size", "agocuda_fused_CannyEdgeDetector_scratch_size",
+              "agocuda_fused_HarrisCorners_scratch_size"):
+        getattr(L, n).argtypes = [u32, u32]
+        getattr(L, n).restype = C.c_size_t
+    return L
+
+
+def _dev():
+    import devbuf
+    return devbuf
+
+
+def _buf(nbytes):
+    import torch
+    return torch.zeros(nbytes + 256, dtype=torch.uint8, device="cuda")
+
+
+def _img(W, H, seed):
+    return WL.cfg2_scene(seed=seed, width=W, height=H, rects=min(200, max(3, W * H // 300)))
+
+
+@pytest.mark.parametrize("W,H", SIZES)
+def test_canny_kernels(lib, cuda, W, H):
+    D = _dev()
+    img = _img(W, H, W * 3 + H)
+    ref_sob, ref_supp, ref_strong, ref_edges = OC.canny_parts(img)
+    src = D.DevImg(H, W).upload(img)
+    sob = D.DevImg(H, W, np.uint16)
+    assert lib.agocuda_CannySobel_U16_U8_3x3_L1NORM(D.stream_ptr(), W, H, sob.ptr, sob.stride, src.ptr, src.stride) == 0
+    got = sob.download()
+    np.testing.assert_array_equal(got[1:H - 1], ref_sob[1:H - 1])
+    out = D.DevImg(H, W)
+    stack, cnt, status = _buf(4 * W * H), _buf(4), _buf(4)
+    assert lib.agocuda_CannySuppThreshold_U8XY_U16_3x3(D.stream_ptr(), W, H, out.ptr, out.stride, sob.ptr, sob.stride,
+                                                       stack.data_ptr(), cnt.data_ptr(), W * H, 80, 100) == 0
+    supp = out.download()
+    np.testing.assert_array_equal(supp[1:H - 1, 1:W - 1], ref_supp[1:H - 1, 1:W - 1])
+    n = int(cnt[:4].view(dtype=__import__("torch").int32).item())
+    got_strong = np.sort(stack[:4 * n].view(dtype=__import__("torch").int32).cpu().numpy().astype(np.uint32))
+    np.testing.assert_array_equal(got_strong, np.sort(ref_strong))
+    sb = lib.agocuda_CannyEdgeTrace_scratch_size(W, H)
+    scr = _buf(sb)
+    base = scr.data_ptr() + (-scr.data_ptr() % 256)
+    assert lib.agocuda_CannyEdgeTrace_U8_U8XY(D.stream_ptr(), W, H, out.ptr, out.stride, stack.data_ptr(), cnt.data_ptr(),
+                                              W * H, base, sb, status.data_ptr()) == 0
+    edges = out.download()
+    np.testing.assert_array_equal(edges[1:H - 1, 1:W - 1], ref_edges[1:H - 1, 1:W - 1])
+    assert int(status[0].item()) == 0
+
+
+@pytest.mark.parametrize("W,H", SIZES + [(3840, 2160)])
+def test_fused_canny(lib, cuda, W, H):
+    D = _dev()
+    img = _img(W, H, W + 7 * H)
+    ref_edges = OC.canny_parts(img)[3]
+    src, out = D.DevImg(H, W).upload(img), D.DevImg(H, W)
+    sb = lib.agocuda_fused_CannyEdgeDetector_scratch_size(W, H)
+    scr, status = _buf(sb), _buf(4)
+    base = scr.data_ptr() + (-scr.data_ptr() % 256)
+    for _ in range(2):   # twice: scratch state must not leak between runs
+        assert lib.agocuda_fused_CannyEdgeDetector_3x3_L1(D.stream_ptr(), W, H, out.ptr, out.stride, src.ptr, src.stride,
+                                                          80, 100, base, sb - 256, status.data_ptr()) == 0
+        edges = out.download()
+        np.testing.assert_array_equal(edges[1:H - 1, 1:W - 1], ref_edges[1:H - 1, 1:W - 1])
+    assert int(status[0].item()) == 0
+
+
+@pytest.mark.parametrize("W,H", [(64, 48), (36, 19), (200, 120), (1920, 1080)])
+def test_harris_kernels(lib, cuda, W, H):
+    import torch
+    D = _dev()
+    img = _img(W, H, 5 * W + H)
+    ref_hg3, ref_hvc, ref_list = OC.harris_parts(img)
+    src = D.DevImg(H, W).upload(img)
+    hg3 = D.DevImg(H, W, np.float32, channels=3)
+    hvc = D.DevImg(H, W, np.float32)
+    assert lib.agocuda_HarrisSobel_HG3_U8_3x3(D.stream_ptr(), W, H, hg3.ptr, hg3.stride, src.ptr, src.stride) == 0
+    np.testing.assert_array_equal(hg3.download()[1:H - 1], ref_hg3[1:H - 1])
+    norm = OC.harris_norm(3)
+    assert lib.agocuda_HarrisScore_HVC_HG3_3x3(D.stream_ptr(), W, H, hvc.ptr, hvc.stride, hg3.ptr, hg3.stride,
+                                               0.04, 1e-3, norm) == 0
+    np.testing.assert_array_equal(hvc.download(), ref_hvc)
+    lst, cnt = _buf(8 * W * H), _buf(4)
+    assert lib.agocuda_NonMaxSupp_XY_ANY_3x3(D.stream_ptr(), W, H, hvc.ptr, hvc.stride, lst.data_ptr(), cnt.data_ptr(), W * H) == 0
+    n = int(cnt[:4].view(torch.int32).item())
+    got = lst[:8 * n].cpu().numpy().view(OC.XYS)
+    key = lambda a: np.sort(a.view(np.int64))
+    np.testing.assert_array_equal(key(got), key(ref_list))
+    for mind, cap in ((5.0, 32768), (5.0, 7), (1.5, 32768)):
+        ref_c, ref_n = OC.harris_pick(ref_list, W, H, mind, cap)
+        corners, ccount, ncorn, status = _buf(28 * cap), _buf(4), _buf(4), _buf(4)
+        assert lib.agocuda_HarrisMergeSortAndPick_XY_XYS(D.stream_ptr(), W, H, lst.data_ptr(), cnt.data_ptr(), W * H, mind,
+                                                         corners.data_ptr(), cap, ccount.data_ptr(), ncorn.data_ptr(),
+                                                         status.data_ptr()) == 0
+        torch.cuda.synchronize()
+        assert int(status[0].item()) == 0
+        nk = int(ccount[:4].view(torch.int32).item())
+        assert int(ncorn[:4].view(torch.int32).item()) == ref_n
+        assert nk == min(ref_n, cap)
+        np.testing.assert_array_equal(corners[:28 * nk].cpu().numpy().view(OC.KP), ref_c)
+
+
+@pytest.mark.parametrize("W,H", [(200, 120), (1920, 1080), (3840, 2160)])
+def test_fused_harris(lib, cuda, W, H):
+    import torch
+    D = _dev()
+    img = _img(W, H, 9 * W + H)
+    ref_c, ref_n = OC.harris(img, capacity=32768)
+    src = D.DevImg(H, W).upload(img)
+    sb = lib.agocuda_fused_HarrisCorners_scratch_size(W, H)
+    scr, corners, ccount, ncorn, status = _buf(sb), _buf(28 * 32768), _buf(4), _buf(4), _buf(4)
+    base = scr.data_ptr() + (-scr.data_ptr() % 256)
+    for _ in range(2):
+        assert lib.agocuda_fused_HarrisCorners_3x3(D.stream_ptr(), W, H, src.ptr, src.stride, 0.04, 1e-3, OC.harris_norm(3),
+                                                   5.0, corners.data_ptr(), 32768, ccount.data_ptr(), ncorn.data_ptr(),
+                                                   base, sb, status.data_ptr()) == 0
+        torch.cuda.synchronize()
+        assert int(status[0].item()) == 0
+        nk = int(ccount[:4].view(torch.int32).item())
+        assert int(ncorn[:4].view(torch.int32).item()) == ref_n
+        np.testing.assert_array_equal(corners[:28 * nk].cpu().numpy().view(OC.KP), ref_c)
