@@ -151,6 +151,48 @@ int agocuda_HarrisMergeSortAndPick_XY_XYS(void *stream, uint32_t width, uint32_t
                                           uint32_t *pNumCorners, uint32_t *pStatus);
 
 /* ------------------------------------------------------------------------------------ */
+/* Colour conversion, scaling, warps (reference: hipvx/hip_host_decls.h color/geometric)  */
+/* ------------------------------------------------------------------------------------ */
+
+/* RGB (3 B/px) -> NV12 (Y plane + interleaved UV at half resolution), BT.709 float weights,
+ * truncation and the reference's chroma averaging.  W and H even.  Replaces
+ * HipExec_ColorConvert_NV12_RGB (hipvx/hip_host_decls.h:555); HafCpu_ColorConvert_NV12_RGB
+ * (ago_haf_cpu_color_convert.cpp:2707). */
+int agocuda_ColorConvert_NV12_RGB(void *stream, uint32_t width, uint32_t height, uint8_t *pY, uint32_t yStride,
+                                  uint8_t *pUV, uint32_t uvStride, const uint8_t *pSrc, uint32_t srcStride);
+/* RGB -> IYUV (Y, U, V planes).  Replaces HipExec_ColorConvert_IYUV_RGB (hipvx/hip_host_decls.h:565);
+ * HafCpu_ColorConvert_IYUV_RGB (ago_haf_cpu_color_convert.cpp:2492). */
+int agocuda_ColorConvert_IYUV_RGB(void *stream, uint32_t width, uint32_t height, uint8_t *pY, uint32_t yStride,
+                                  uint8_t *pU, uint32_t uStride, uint8_t *pV, uint32_t vStride,
+                                  const uint8_t *pSrc, uint32_t srcStride);
+
+/* ScaleImage U8 -> U8 with the AGO scale matrices (18-bit fixed-point maps).  Replace
+ * HipExec_ScaleImage_U8_U8_{Nearest,Bilinear,Area} (hipvx/hip_host_decls.h:723/728/744);
+ * HafCpu_ScaleImage_U8_U8_* (ago_haf_cpu_geometric.cpp:1874/1977/2491).  Area supports the
+ * exact 1x and 2x ratios (returns -3, not supported, otherwise). */
+int agocuda_ScaleImage_U8_U8_Nearest(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                     uint32_t srcWidth, uint32_t srcHeight, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ScaleImage_U8_U8_Bilinear(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                      uint32_t srcWidth, uint32_t srcHeight, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ScaleImage_U8_U8_Area(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                  uint32_t srcWidth, uint32_t srcHeight, const uint8_t *pSrc, uint32_t srcStride);
+
+/* WarpAffine U8 -> U8 with constant border.  affineMatrix: 6 floats in vx_matrix order
+ * (3 rows x 2 columns: m00 m01 / m10 m11 / m20 m21), read on the host at launch.  The nearest
+ * variant also masks by the source valid rectangle {start_x, start_y, end_x, end_y} (NULL =
+ * whole image).  Widths are processed in 4-pixel groups (dstStride >= ALIGN4(width)).
+ * Replace HipExec_WarpAffine_U8_U8_{Nearest,Bilinear}_Constant (hipvx/hip_host_decls.h:755/768);
+ * HafCpu_WarpAffine_U8_U8_{Nearest,Bilinear}_Constant (ago_haf_cpu_geometric.cpp:658/1100). */
+int agocuda_WarpAffine_U8_U8_Nearest_Constant(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                              uint32_t dstStride, uint32_t srcWidth, uint32_t srcHeight,
+                                              const uint8_t *pSrc, uint32_t srcStride, const float *affineMatrix,
+                                              uint8_t border, const uint32_t *srcValidRect);
+int agocuda_WarpAffine_U8_U8_Bilinear_Constant(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                               uint32_t dstStride, uint32_t srcWidth, uint32_t srcHeight,
+                                               const uint8_t *pSrc, uint32_t srcStride, const float *affineMatrix,
+                                               uint8_t border);
+
+/* ------------------------------------------------------------------------------------ */
 /* Fused multi-node kernels (no reference counterpart: the HIP target launches one kernel */
 /* per node, ago/ago_util_hip.cpp:686; agoGpuHipSuperNodeLaunch returns -1 at :740)      */
 /* ------------------------------------------------------------------------------------ */
@@ -186,6 +228,15 @@ int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t width, uint32_
 /* vxHarrisCornersNode (gradient 3, block 3) as one front-end kernel (Sobel products,
  * window sums, score and non-maximum suppression from one read of the image) plus the
  * corner pick.  Scratch: agocuda_fused_HarrisCorners_scratch_size(W, H) bytes. */
+/* RGB -> NV12 + IYUV + half-size bilinear ScaleImage + half-size area ScaleImage of Y, in
+ * one pass over the RGB frame (W even, >= 16; H even).  Outputs bit-identical to the four
+ * unfused AGO nodes (the scaled images read the Y plane both colour outputs share). */
+int agocuda_fused_ColorScale_RGB(void *stream, uint32_t width, uint32_t height, const uint8_t *pSrc, uint32_t srcStride,
+                                 uint8_t *pNV12Y, uint32_t nv12YStride, uint8_t *pNV12UV, uint32_t nv12UVStride,
+                                 uint8_t *pIYUVY, uint32_t iyuvYStride, uint8_t *pU, uint32_t uStride,
+                                 uint8_t *pV, uint32_t vStride, uint8_t *pHalfBilinear, uint32_t hbStride,
+                                 uint8_t *pHalfArea, uint32_t haStride);
+
 size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t width, uint32_t height);
 int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t width, uint32_t height, const uint8_t *pSrc, uint32_t srcStride,
                                     float sensitivity, float strengthThreshold, float normFactor, float minDistance,

@@ -10,6 +10,7 @@
 // VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS bit kOptNoFusion set, every node is its own
 // launch: that is the "plain" one-launch-per-node form the fused form is measured against.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <map>
 #include <set>
@@ -194,6 +195,49 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         };
         return VX_SUCCESS;
     }
+    case LK::COLOR_CONVERT_NV12_RGB: {
+        uint8_t *y = dptr(p[0]), *uv = dptr(p[1]); const uint8_t *s = dptr(p[2]);
+        uint32_t w = W(p[2]), h = H(p[2]), ys = dstride(p[0]), uvs = dstride(p[1]), ss = dstride(p[2]);
+        st.launch = [=](cudaStream_t q) { return agocuda_ColorConvert_NV12_RGB(S(q), w, h, y, ys, uv, uvs, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::COLOR_CONVERT_IYUV_RGB: {
+        uint8_t *y = dptr(p[0]), *u = dptr(p[1]), *v = dptr(p[2]); const uint8_t *s = dptr(p[3]);
+        uint32_t w = W(p[3]), h = H(p[3]), ys = dstride(p[0]), us = dstride(p[1]), vs = dstride(p[2]), ss = dstride(p[3]);
+        st.launch = [=](cudaStream_t q) { return agocuda_ColorConvert_IYUV_RGB(S(q), w, h, y, ys, u, us, v, vs, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::SCALE_IMAGE_U8_U8_NEAREST: case LK::SCALE_IMAGE_U8_U8_BILINEAR: case LK::SCALE_IMAGE_U8_U8_AREA: {
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), sw = W(p[1]), sh = H(p[1]), ss = dstride(p[1]);
+        if (ln.k == LK::SCALE_IMAGE_U8_U8_AREA && !((sw == 2 * w && sh == 2 * h) || (sw == w && sh == h))) {
+            log_error(g, VX_ERROR_NOT_SUPPORTED, "ERROR: area scaling %ux%u -> %ux%u: only the 1x and 2x ratios are implemented\n", sw, sh, w, h);
+            return VX_ERROR_NOT_SUPPORTED;
+        }
+        const LK k = ln.k;
+        st.launch = [=](cudaStream_t q) {
+            if (k == LK::SCALE_IMAGE_U8_U8_NEAREST) return agocuda_ScaleImage_U8_U8_Nearest(S(q), w, h, d, ds, sw, sh, s, ss);
+            if (k == LK::SCALE_IMAGE_U8_U8_BILINEAR) return agocuda_ScaleImage_U8_U8_Bilinear(S(q), w, h, d, ds, sw, sh, s, ss);
+            return agocuda_ScaleImage_U8_U8_Area(S(q), w, h, d, ds, sw, sh, s, ss);
+        };
+        return VX_SUCCESS;
+    }
+    case LK::WARP_AFFINE_U8_U8_NEAREST_CONSTANT: case LK::WARP_AFFINE_U8_U8_BILINEAR_CONSTANT: {
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), sw = W(p[1]), sh = H(p[1]), ss = dstride(p[1]);
+        Matrix *m = static_cast<Matrix *>(p[2]);
+        std::array<float, 6> mat;
+        memcpy(mat.data(), m->data.data(), sizeof(float) * 6);
+        const uint8_t border = static_cast<Scalar *>(p[3])->v.u8;
+        const vx_rectangle_t vr = IMG(p[1])->valid;   // the nearest kernel masks by the source valid rect
+        const bool nn = ln.k == LK::WARP_AFFINE_U8_U8_NEAREST_CONSTANT;
+        st.launch = [=](cudaStream_t q) {
+            const uint32_t rect[4] = {vr.start_x, vr.start_y, vr.end_x, vr.end_y};
+            return nn ? agocuda_WarpAffine_U8_U8_Nearest_Constant(S(q), w, h, d, ds, sw, sh, s, ss, mat.data(), border, rect)
+                      : agocuda_WarpAffine_U8_U8_Bilinear_Constant(S(q), w, h, d, ds, sw, sh, s, ss, mat.data(), border);
+        };
+        return VX_SUCCESS;
+    }
     case LK::CHANNEL_COPY_U8_U8: {
         uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
         uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
@@ -217,6 +261,7 @@ struct Chain {
     std::vector<LNode *> nodes;
     std::vector<int64_t> key;         // by-value parameters: chains with equal keys batch
     Ref *src = nullptr, *dst = nullptr;
+    std::vector<Ref *> elide;         // intermediates the fused kernel keeps on chip
 };
 
 // Gaussian3x3 -> SobelMagnitude -> ColorDepth_U8_S16_Sat -> Threshold_U8_U8_Binary
@@ -235,6 +280,7 @@ static bool match_gauss_sobelmag_thresh(Graph *g, LNode &a, Chain &c)
     c.nodes = {&a, b, d, t};
     c.key = {sc_i32(d->p[2]), static_cast<Threshold *>(t->p[2])->value.U8};
     c.src = src; c.dst = dst;
+    c.elide = {a.p[0], b->p[0], d->p[0]};
     return true;
 }
 
@@ -251,6 +297,7 @@ static bool match_canny(Graph *g, LNode &a, Chain &c)
     c.nodes = {&a, b, t};
     c.key = {(int64_t)(uint16_t)th->lower.U32, (int64_t)(uint16_t)th->upper.U32};
     c.src = a.p[1]; c.dst = b->p[0];
+    c.elide = {a.p[0], b->p[1]};
     return true;
 }
 
@@ -267,11 +314,65 @@ static bool match_harris(Graph *g, LNode &a, Chain &c)
     c.kind = "fused_HarrisCorners";
     c.nodes = {&a, b, n, pk};
     c.src = a.p[1]; c.dst = pk->p[0];
+    c.elide = {a.p[0], b->p[0], n->p[0]};
+    return true;
+}
+
+// ColorConvert_NV12_RGB + ColorConvert_IYUV_RGB of one RGB image, and a bilinear and an area
+// ScaleImage of (either) Y plane to exactly half size: one pass over the RGB frame.
+static bool match_color_scale(Graph *g, LNode &a, Chain &c)
+{
+    if (a.k != LK::COLOR_CONVERT_NV12_RGB) return false;
+    Ref *rgb = a.p[2];
+    Image *ri = IMG(rgb);
+    if (ri->width < 16 || (ri->width & 1) || (ri->height & 1)) return false;
+    LNode *iy = nullptr, *sb = nullptr, *sa = nullptr;
+    for (LNode &n : g->lnodes) {
+        if (n.removed) continue;
+        if (n.k == LK::COLOR_CONVERT_IYUV_RGB && n.p[3] == rgb && !iy) iy = &n;
+    }
+    if (!iy) return false;
+    for (LNode &n : g->lnodes) {
+        if (n.removed || (n.p.size() < 2)) continue;
+        if (n.p[1] != a.p[0] && n.p[1] != iy->p[0]) continue;
+        Image *o = IMG(n.p[0]);
+        if (o->width * 2 != ri->width || o->height * 2 != ri->height) continue;
+        if (n.k == LK::SCALE_IMAGE_U8_U8_BILINEAR && !sb) sb = &n;
+        if (n.k == LK::SCALE_IMAGE_U8_U8_AREA && !sa) sa = &n;
+    }
+    if (!sb || !sa) return false;
+    c.kind = "fused_ColorScale";
+    c.nodes = {&a, iy, sb, sa};
+    c.src = rgb; c.dst = nullptr;
     return true;
 }
 
 static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &st)
 {
+    if (chains[0].kind == "fused_ColorScale") {
+        std::vector<std::function<int(cudaStream_t)>> fns;
+        st.name = chains[0].kind + " x" + std::to_string(chains.size());
+        st.num_kernels = (int)chains.size();
+        for (Chain &c : chains) {
+            for (LNode *n : c.nodes) st.nodes.push_back(n);
+            LNode *nv = c.nodes[0], *iy = c.nodes[1], *sb = c.nodes[2], *sa = c.nodes[3];
+            Image *s = IMG(c.src);
+            const uint32_t w = s->width, h = s->height, ss = s->planes[0].dev_stride;
+            const uint8_t *src = s->planes[0].dev;
+            uint8_t *y1 = dptr(nv->p[0]), *uv = dptr(nv->p[1]), *y2 = dptr(iy->p[0]), *u = dptr(iy->p[1]), *v = dptr(iy->p[2]);
+            uint8_t *ob = dptr(sb->p[0]), *oa = dptr(sa->p[0]);
+            const uint32_t y1s = dstride(nv->p[0]), uvs = dstride(nv->p[1]), y2s = dstride(iy->p[0]), us = dstride(iy->p[1]),
+                           vs = dstride(iy->p[2]), obs = dstride(sb->p[0]), oas = dstride(sa->p[0]);
+            fns.push_back([=](cudaStream_t q) {
+                return agocuda_fused_ColorScale_RGB(S(q), w, h, src, ss, y1, y1s, uv, uvs, y2, y2s, u, us, v, vs, ob, obs, oa, oas);
+            });
+        }
+        st.launch = [fns](cudaStream_t q) {
+            for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
+            return 0;
+        };
+        return VX_SUCCESS;
+    }
     if (chains[0].kind == "fused_CannyEdgeDetector" || chains[0].kind == "fused_HarrisCorners") {
         // one step holding every frame's launches (one CUDA graph segment)
         std::vector<std::function<int(cudaStream_t)>> fns;
@@ -386,6 +487,8 @@ vx_status plan_graph(Graph *g)
             if (match_gauss_sobelmag_thresh(g, ln, c)) pattern = 1;
             else if (match_canny(g, ln, c)) pattern = 2;
             else if (match_harris(g, ln, c)) pattern = 3;
+            else if (match_color_scale(g, ln, c)) pattern = 4;
+            for (LNode *n : c.nodes) if (pattern && fused.count(n)) pattern = 0;   // a node joins one chain
             if (pattern) {
                 std::vector<int64_t> gk{pattern, ln.level};
                 gk.insert(gk.end(), c.key.begin(), c.key.end());
@@ -399,10 +502,7 @@ vx_status plan_graph(Graph *g)
     std::set<Ref *> elided;
     for (auto &kv : groups)
         for (Chain &c : kv.second)
-            for (LNode *n : c.nodes)
-                for (size_t i = 0; i < n->p.size(); i++)
-                    if (n->p[i] && n->p[i]->is_virtual && n->p[i] != c.dst && n->p[i]->type != VX_TYPE_SCALAR)
-                        elided.insert(n->p[i]);
+            for (Ref *r : c.elide) elided.insert(r);
     for (LNode &ln : g->lnodes)
         for (Ref *r : ln.p) {
             if (!r || elided.count(r)) continue;

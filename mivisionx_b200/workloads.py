@@ -172,6 +172,68 @@ class Cfg1Graph:
         return [(self.api.read_plane(o), self.api.valid_region(o)) for o in self.outputs]
 
 
+class Cfg3Graph:
+    """Colour and geometry: RGB -> NV12 and RGB -> IYUV, ChannelExtract Y (virtual), ScaleImage
+    of Y to half size (bilinear and area), WarpAffine of the bilinear result (nearest and
+    bilinear, border CONSTANT 0), for each of `sizes` RGB frames, in one graph."""
+
+    def __init__(self, api: V.OpenVX, ctx, sizes, matrices=None, flags: int | None = None):
+        self.api, self.ctx = api, ctx
+        a = api
+        self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
+        if flags is not None:
+            a.set_optimizer_flags(self.graph, flags)
+        g = self.graph
+        self.inputs, self.nv12, self.iyuv, self.scaled, self.warped, self.matrices = [], [], [], [], [], []
+        for i, (w, h) in enumerate(sizes):
+            m = matrices[i] if matrices is not None else cfg3_affine(seed=17 + i, cx=w / 4, cy=h / 4)
+            rgb = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_RGB), "rgb")
+            nv12 = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_NV12), "nv12")
+            iyuv = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_IYUV), "iyuv")
+            y = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_U8)
+            sb = a.obj(a.vxCreateImage(ctx, w // 2, h // 2, V.VX_DF_IMAGE_U8), "scaled")
+            sa = a.obj(a.vxCreateImage(ctx, w // 2, h // 2, V.VX_DF_IMAGE_U8), "scaled")
+            wn = a.obj(a.vxCreateImage(ctx, w // 2, h // 2, V.VX_DF_IMAGE_U8), "warped")
+            wb = a.obj(a.vxCreateImage(ctx, w // 2, h // 2, V.VX_DF_IMAGE_U8), "warped")
+            mat = a.matrix_f32(ctx, m)
+            a.obj(a.vxColorConvertNode(g, rgb, nv12), "node")
+            a.obj(a.vxColorConvertNode(g, rgb, iyuv), "node")
+            a.obj(a.vxChannelExtractNode(g, nv12, V.VX_CHANNEL_Y, y), "node")
+            a.obj(a.vxScaleImageNode(g, y, sb, V.VX_INTERPOLATION_BILINEAR), "node")
+            a.obj(a.vxScaleImageNode(g, y, sa, V.VX_INTERPOLATION_AREA), "node")
+            n1 = a.obj(a.vxWarpAffineNode(g, sb, mat, V.VX_INTERPOLATION_NEAREST_NEIGHBOR, wn), "node")
+            n2 = a.obj(a.vxWarpAffineNode(g, sb, mat, V.VX_INTERPOLATION_BILINEAR, wb), "node")
+            a.set_border(n1, V.VX_BORDER_CONSTANT, 0)
+            a.set_border(n2, V.VX_BORDER_CONSTANT, 0)
+            self.inputs.append(rgb); self.nv12.append(nv12); self.iyuv.append(iyuv)
+            self.scaled.append((sb, sa)); self.warped.append((wn, wb)); self.matrices.append(m)
+        a.ok(a.vxVerifyGraph(g), "vxVerifyGraph")
+        self.outputs = [im for i in range(len(sizes)) for im in
+                        (self.nv12[i], self.iyuv[i]) + self.scaled[i] + self.warped[i]]
+
+    def run(self, frames=None):
+        a = self.api
+        if frames is not None:
+            for img, f in zip(self.inputs, frames):
+                a.write_plane(img, f)
+        a.ok(a.vxProcessGraph(self.graph), "vxProcessGraph")
+
+    def results(self):
+        """per frame: dict of planes and valid rectangles"""
+        a = self.api
+        out = []
+        for i in range(len(self.inputs)):
+            d = {"nv12_y": a.read_plane(self.nv12[i], 0), "nv12_uv": a.read_plane(self.nv12[i], 1),
+                 "iyuv_y": a.read_plane(self.iyuv[i], 0), "iyuv_u": a.read_plane(self.iyuv[i], 1),
+                 "iyuv_v": a.read_plane(self.iyuv[i], 2)}
+            for k, im in (("scale_bilinear", self.scaled[i][0]), ("scale_area", self.scaled[i][1]),
+                          ("warp_nearest", self.warped[i][0]), ("warp_bilinear", self.warped[i][1])):
+                d[k] = a.read_plane(im)
+                d[k + "_rect"] = a.valid_region(im)
+            out.append(d)
+        return out
+
+
 class Cfg2Graph:
     """CannyEdgeDetector (3x3 gradient, L1 norm, hysteresis lower/upper) and HarrisCorners
     (gradient 3, block 3, sensitivity k, strength threshold, min distance) on the same U8

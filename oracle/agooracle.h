@@ -61,6 +61,29 @@ int oracle_HarrisMergeSortAndPick_XY_XYS(uint32_t capacity, oracle_keypoint *cor
 /* AGO wrapper arithmetic (ago_kernel_api.cpp:16941-16942) */
 float oracle_harris_norm_factor(int32_t gradientSize);
 
+/* ---- colour conversion (ago_haf_cpu_color_convert.cpp), agooracle_geometry.c ---- */
+int oracle_ColorConvert_NV12_RGB(uint32_t W, uint32_t H, uint8_t *pY, uint32_t yStride, uint8_t *pUV, uint32_t uvStride,
+                                 const uint8_t *pSrc, uint32_t srcStride);
+int oracle_ColorConvert_IYUV_RGB(uint32_t W, uint32_t H, uint8_t *pY, uint32_t yStride, uint8_t *pU, uint32_t uStride,
+                                 uint8_t *pV, uint32_t vStride, const uint8_t *pSrc, uint32_t srcStride);
+/* ---- scaling (ago_haf_cpu_geometric.cpp); m = {xscale, yscale, xoffset, yoffset} ---- */
+void oracle_scale_matrix(int kind /* 0 nearest, 1 bilinear, 2 area */, uint32_t srcW, uint32_t srcH, uint32_t dstW,
+                         uint32_t dstH, float m[4]);
+int oracle_ScaleImage_U8_U8_Bilinear(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW, uint32_t srcH,
+                                     const uint8_t *pSrc, uint32_t srcStride, const float m[4]);
+int oracle_ScaleImage_U8_U8_Nearest(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW, uint32_t srcH,
+                                    const uint8_t *pSrc, uint32_t srcStride, const float m[4]);
+int oracle_ScaleImage_U8_U8_Area(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW, uint32_t srcH,
+                                 const uint8_t *pSrc, uint32_t srcStride, const float m[4]);
+/* ---- warps; m = ago_affine_matrix_t as 6 floats {m00, m01, m10, m11, m20, m21} ---- */
+int oracle_WarpAffine_U8_U8_Nearest_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW,
+                                             uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride, const float *m,
+                                             uint8_t border, uint32_t validStartX, uint32_t validStartY,
+                                             uint32_t validEndX, uint32_t validEndY);
+int oracle_WarpAffine_U8_U8_Bilinear_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW,
+                                              uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride, const float *m,
+                                              uint8_t border);
+
 #ifdef __cplusplus
 }
 #endif

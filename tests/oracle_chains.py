@@ -106,6 +106,64 @@ def harris_pick(lst: np.ndarray, w, h, min_distance=5.0, capacity=1 << 20):
     return out[:min(cnt.value, capacity)], cnt.value
 
 
+def _sfn(name, args):
+    f = getattr(O.oracle_lib(), "oracle_" + name)
+    f.argtypes = args
+    f.restype = C.c_int
+    return f
+
+
+def scale_matrix(kind, sw, sh, dw, dh):
+    m = (C.c_float * 4)()
+    f = O.oracle_lib().oracle_scale_matrix
+    f.argtypes = [C.c_int, u32, u32, u32, u32, vp]
+    f.restype = None
+    f(kind, sw, sh, dw, dh, C.cast(m, vp))
+    return m
+
+
+def color_scale_warp(rgb: np.ndarray, matrix: np.ndarray):
+    """The configuration-3 graph as AGO runs it: NV12 and IYUV from RGB, ScaleImage of the NV12
+    Y plane (the ChannelExtract copy is removed), both warps of the bilinear result."""
+    h, w = rgb.shape[:2]
+    src = ago_img(h, w, np.uint8, 3); src.set(rgb)
+    y, uv = ago_img(h, w), ago_img(h // 2, w // 2, np.uint8, 2)
+    y2, u, v = ago_img(h, w), ago_img(h // 2, w // 2), ago_img(h // 2, w // 2)
+    a8 = [u32, u32, vp, u32, vp, u32, vp, u32]
+    _sfn("ColorConvert_NV12_RGB", a8)(w, h, y.ptr, y.stride, uv.ptr, uv.stride, src.ptr, src.stride)
+    _sfn("ColorConvert_IYUV_RGB", a8 + [vp, u32])(w, h, y2.ptr, y2.stride, u.ptr, u.stride, v.ptr, v.stride, src.ptr, src.stride)
+    out = {"nv12_y": y.get(), "nv12_uv": uv.get(), "iyuv_y": y2.get(), "iyuv_u": u.get(), "iyuv_v": v.get()}
+    dw, dh = w // 2, h // 2
+    sargs = [u32, u32, vp, u32, u32, u32, vp, u32, vp]
+    sb, sa = ago_img(dh, dw), ago_img(dh, dw)
+    _sfn("ScaleImage_U8_U8_Bilinear", sargs)(dw, dh, sb.ptr, sb.stride, w, h, y.ptr, y.stride, C.cast(scale_matrix(1, w, h, dw, dh), vp))
+    _sfn("ScaleImage_U8_U8_Area", sargs)(dw, dh, sa.ptr, sa.stride, w, h, y.ptr, y.stride, C.cast(scale_matrix(2, w, h, dw, dh), vp))
+    out["scale_bilinear"], out["scale_area"] = sb.get(), sa.get()
+    m = np.ascontiguousarray(matrix, np.float32)
+    wn, wb = ago_img(dh, dw), ago_img(dh, dw)
+    _sfn("WarpAffine_U8_U8_Nearest_Constant", [u32, u32, vp, u32, u32, u32, vp, u32, vp, u8, u32, u32, u32, u32])(
+        dw, dh, wn.ptr, wn.stride, dw, dh, sb.ptr, sb.stride, m.ctypes.data, 0, 0, 0, dw, dh)
+    _sfn("WarpAffine_U8_U8_Bilinear_Constant", [u32, u32, vp, u32, u32, u32, vp, u32, vp, u8])(
+        dw, dh, wb.ptr, wb.stride, dw, dh, sb.ptr, sb.stride, m.ctypes.data, 0)
+    out["warp_nearest"], out["warp_bilinear"] = wn.get(), wb.get()
+    # Pixels whose bilinear footprint reaches below the last source row: the reference reads
+    # past its buffer there (geometric.cpp:1190, psrc + stride), so its value is undefined.
+    f = np.float32
+    xs_ = np.arange(((dw + 3) // 4) * 4, dtype=f)[None, :dw]
+    ys_ = np.arange(dh, dtype=f)[:, None]
+    with np.errstate(invalid="ignore"):
+        yd = ys_ * m[1, 1] + m[2, 1]
+        ysrc = (m[0, 1] * xs_).astype(f) + yd.astype(f)
+        xd = ys_ * m[1, 0] + m[2, 0]
+        xsrc = (m[0, 0] * xs_).astype(f) + xd.astype(f)
+    inside = (xsrc >= 0) & (xsrc < dw) & (ysrc >= 0) & (ysrc < dh)
+    out["warp_bilinear_undefined_in_reference"] = inside & (np.trunc(ysrc) >= dh - 1)
+    full = (0, 0, dw, dh)
+    for k in ("scale_bilinear", "scale_area", "warp_nearest", "warp_bilinear"):
+        out[k + "_rect"] = full
+    return out
+
+
 def harris(img: np.ndarray, k=0.04, tc=1e-3, min_distance=5.0, capacity=1 << 20):
     """vxHarrisCornersNode (gradient 3, block 3): (corners, num_corners)."""
     h, w = img.shape

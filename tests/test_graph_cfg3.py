@@ -1,0 +1,62 @@
+"""Colour + geometry graph (configuration 3) through the OpenVX API.
+
+CPU: the reference AGO library runs the graph and must equal the oracle composition on every
+output plane, with the same valid rectangles.  GPU: this package's engine, fused and plain,
+must equal the oracle bit for bit (bilinear warp included: no +-1 tolerance is needed)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import oracle_chains as OC
+from mivisionx_b200 import vx as V
+from mivisionx_b200 import workloads as WL
+
+KEYS = ["nv12_y", "nv12_uv", "iyuv_y", "iyuv_u", "iyuv_v", "scale_bilinear", "scale_area", "warp_nearest", "warp_bilinear"]
+
+
+def _check(got, ref, w, reference_run=False):
+    for k in KEYS:
+        a, b = got[k], ref[k]
+        if k == "scale_area":   # the reference writes the first (W/2 & ~7) columns only
+            n = (w // 2) & ~7
+            a, b = a[:, :n], b[:, :n]
+        if k == "warp_bilinear" and reference_run:
+            # the reference reads past its buffer for footprints below the last row
+            keep = ~ref["warp_bilinear_undefined_in_reference"]
+            a, b = a[keep], b[keep]
+        np.testing.assert_array_equal(a, b, err_msg=k)
+    for k in ("scale_bilinear", "scale_area", "warp_nearest", "warp_bilinear"):
+        assert got[k + "_rect"] == ref[k + "_rect"], k
+
+
+@pytest.mark.parametrize("W,H", [(64, 48), (200, 120), (3840, 64)])
+def test_reference_graph_matches_oracle(W, H):
+    lib = O.ref_lib()
+    if lib is None:
+        pytest.skip("reference library not built")
+    api = V.OpenVX(lib)
+    ctx = api.obj(api.vxCreateContext(), "context")
+    rgb = WL.cfg3_frame(seed=W + H, width=W, height=H)
+    g = WL.Cfg3Graph(api, ctx, [(W, H)])
+    g.run([rgb])
+    got, = g.results()
+    _check(got, OC.color_scale_warp(rgb, g.matrices[0]), W, reference_run=True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flags", [None, V.OPT_NO_FUSION])
+def test_engine_cfg3(cuda, flags):
+    api = V.OpenVX()
+    ctx = api.obj(api.vxCreateContext(), "context")
+    sizes = [(3840, 2160), (200, 120), (64, 48)]
+    frames = [WL.cfg3_frame(seed=i + 5, width=w, height=h) for i, (w, h) in enumerate(sizes)]
+    g = WL.Cfg3Graph(api, ctx, sizes, flags=flags)
+    plan = api.plan_text(g.graph)
+    if flags is None:
+        assert "fused_ColorScale x3" in plan, plan
+    else:
+        assert "ColorConvert_NV12_RGB" in plan and "ScaleImage_U8_U8_Area" in plan, plan
+    for rep in range(2):
+        g.run(frames)
+        for got, rgb, m, (w, h) in zip(g.results(), frames, g.matrices, sizes):
+            _check(got, OC.color_scale_warp(rgb, m), w)
