@@ -120,6 +120,24 @@ int agocuda_CannyEdgeTrace_U8_U8XY(void *stream, uint32_t width, uint32_t height
                                    const uint32_t *pStack, const uint32_t *pStackCount, uint32_t stackCapacity,
                                    void *scratch, size_t scratchBytes, uint32_t *pStatus);
 
+/* The same hysteresis as agocuda_CannyEdgeTrace_U8_U8XY for callers that cannot allocate
+ * device memory -- a real-time loop that must not pay cudaMalloc's implicit device
+ * synchronisation, or a host application that gives this library a fixed memory budget and
+ * owns every device allocation itself.  It allocates nothing: its scratch (union-find
+ * labels and a root bitmap) is a fixed array of 8.25 MiB in the library's own device memory,
+ * which every GPU that loads the library holds until the process exits.  Images are limited
+ * to agocuda_CannyEdgeTrace_noalloc_max_pixels() = 2,097,152 pixels (W*H); larger ones return
+ * -15 without launching anything.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and should be made before any stream capture.  All calls on
+ * a device share that one array: the labels are rewritten and the bitmap is cleared on every
+ * call, but calls whose executions overlap on the GPU (other streams, or host threads
+ * without ordering) race on it.  No counterpart in the reference (its edge trace runs on the
+ * CPU, ago_kernel_list.cpp:486). */
+size_t agocuda_CannyEdgeTrace_noalloc_max_pixels(void);
+int agocuda_CannyEdgeTrace_U8_U8XY_noalloc(void *stream, uint32_t width, uint32_t height, uint8_t *pImg, uint32_t stride,
+                                           const uint32_t *pStack, const uint32_t *pStackCount, uint32_t stackCapacity,
+                                           uint32_t *pStatus);
+
 /* Harris gradient products {gx*gx, gx*gy, gy*gy} (float x3 per pixel) of rows [1, H-1);
  * rows 0 and H-1 are written 0.  Replaces HipExec_HarrisSobel_HG3_U8_3x3
  * (hipvx/hip_host_decls.h:868); HafCpu_HarrisSobel_HG3_U8_3x3 (ago_haf_cpu_harris.cpp:85). */

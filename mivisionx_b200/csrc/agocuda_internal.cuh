@@ -6,6 +6,7 @@
 
 #define AGOCUDA_INVALID_PARAMS (-10)   // same value as VX_ERROR_INVALID_PARAMETERS
 #define AGOCUDA_NO_MEMORY      (-8)    // same value as VX_ERROR_NO_MEMORY
+#define AGOCUDA_TOO_LARGE      (-15)   // same value as VX_ERROR_INVALID_DIMENSION
 
 // Map the launch status to the C-ABI return convention: 0 on success, else the
 // cudaError_t (positive) of the failed launch.

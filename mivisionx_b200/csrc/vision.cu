@@ -8,6 +8,8 @@
 // through non-maximum suppression and hysteresis, so `ago_px` reproduces them.
 #include "agocuda_internal.cuh"
 
+#include <mutex>
+
 uint64_t agocuda_count_launch(unsigned n);
 
 namespace {
@@ -643,6 +645,54 @@ extern "C" int agocuda_CannyEdgeTrace_U8_U8XY(void *stream, uint32_t W, uint32_t
     agocuda_count_launch(1);
     return hysteresis_tail(s, (int)W, (int)H, pImg, (int)stride, L, bits, pStack, pStackCount, stackCapacity, pStatus);
 }
+
+// ---------------------------------------------------------------------------------
+// Hysteresis without any allocation.  The union-find labels and the root bitmap live in a
+// file-scope device array of fixed size (every GPU that loads this library holds it until
+// the process exits), so a caller that must not allocate device memory can still run the
+// edge trace.  Host code may not use the array's name as a device address: the address is
+// looked up once per device with cudaGetSymbolAddress, with that device current.
+// ---------------------------------------------------------------------------------
+constexpr size_t kNoAllocMaxPixels = (size_t)1 << 21;                 // 2,097,152 pixels
+constexpr size_t kNoAllocLabelBytes = kNoAllocMaxPixels * sizeof(int);   // 8 MiB
+constexpr size_t kNoAllocBitBytes = kNoAllocMaxPixels / 8;               // 256 KiB
+static __device__ __align__(256) uint8_t g_noalloc_trace_scratch[kNoAllocLabelBytes + kNoAllocBitBytes];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[256];
+
+extern "C" int agocuda_CannyEdgeTrace_U8_U8XY_noalloc(void *stream, uint32_t W, uint32_t H, uint8_t *pImg, uint32_t stride,
+                                                      const uint32_t *pStack, const uint32_t *pStackCount,
+                                                      uint32_t stackCapacity, uint32_t *pStatus)
+{
+    if (!pImg || !pStack || !pStackCount || !pStatus || W < 3 || H < 3 || stride < W || W > 65535 || H > 65535)
+        return AGOCUDA_INVALID_PARAMS;
+    if ((size_t)W * H > kNoAllocMaxPixels) return AGOCUDA_TOO_LARGE;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    if (dev < 0 || dev >= 256) return AGOCUDA_INVALID_PARAMS;
+    void *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_trace_scratch);
+            if (e != cudaSuccess || !p) return e != cudaSuccess ? (int)e : AGOCUDA_INVALID_PARAMS;
+            g_noalloc_ptr[dev] = p;
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    int *L = (int *)base;
+    uint32_t *bits = (uint32_t *)((uint8_t *)base + kNoAllocLabelBytes);
+    cudaStream_t s = as_stream(stream);
+    // labels are rewritten for every pixel and the bitmap is cleared: nothing carries over
+    k_hyst_init<<<row_grid(W, H, 256), 256, 0, s>>>((int)W, (int)H, pImg, (int)stride, L);
+    agocuda_count_launch(1);
+    return hysteresis_tail(s, (int)W, (int)H, pImg, (int)stride, L, bits, pStack, pStackCount, stackCapacity, pStatus);
+}
+
+extern "C" size_t agocuda_CannyEdgeTrace_noalloc_max_pixels(void) { return kNoAllocMaxPixels; }
 
 extern "C" int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
                                                       const uint8_t *pSrc, uint32_t srcStride, uint16_t hystLower,
