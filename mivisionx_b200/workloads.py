@@ -96,6 +96,59 @@ def cfg2_scene(seed: int = 2, width: int = 3840, height: int = 2160, rects: int 
     return np.clip(np.rint(img), 0, 255).astype(np.uint8)
 
 
+CFG4_SIZES = ((640, 480), (1280, 720), (1920, 1080), (3840, 2160))
+
+
+def cfg4_sizes(n: int = 64, seed: int = 4) -> list[tuple[int, int]]:
+    """Per-frame (width, height), each drawn from CFG4_SIZES by a seeded PCG32."""
+    r = pcg32(seed, n, stream=19)
+    return [CFG4_SIZES[int(v) % len(CFG4_SIZES)] for v in r]
+
+
+def cfg4_pair(seed: int, width: int, height: int, max_shift: float = 8.0, noise_sigma: float = 2.0):
+    """(frame1, frame2, (dx, dy)): frame1 is a config-2 style scene (rectangle count scaled to
+    the area); frame2 is frame1 translated by (dx, dy) ~ U(-max_shift, max_shift) with bilinear
+    interpolation (edge-clamped) plus N(0, noise_sigma^2) noise, rounded and clipped to U8."""
+    rects = max(8, int(round(200 * width * height / (3840 * 2160))))
+    f1 = cfg2_scene(seed=seed, width=width, height=height, rects=rects)
+    dx, dy = (uniform01(seed, 2, stream=23) * 2.0 - 1.0) * max_shift
+    # frame2(x, y) = frame1(x - dx, y - dy)
+    xs = np.clip(np.arange(width, dtype=np.float64) - dx, 0, width - 1)
+    ys = np.clip(np.arange(height, dtype=np.float64) - dy, 0, height - 1)
+    x0 = np.minimum(np.floor(xs).astype(np.int64), width - 2)
+    y0 = np.minimum(np.floor(ys).astype(np.int64), height - 2)
+    fx, fy = xs - x0, ys - y0
+    a = f1.astype(np.float64)
+    top = a[y0][:, x0] * (1 - fx) + a[y0][:, x0 + 1] * fx
+    bot = a[y0 + 1][:, x0] * (1 - fx) + a[y0 + 1][:, x0 + 1] * fx
+    f2 = top * (1 - fy)[:, None] + bot * fy[:, None]
+    f2 += noise_sigma * gaussian(seed, width * height, stream=29).reshape(height, width)
+    return f1, np.clip(np.rint(f2), 0, 255).astype(np.uint8), (float(dx), float(dy))
+
+
+KEYPOINT_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("strength", "<f4"), ("scale", "<f4"),
+                           ("orientation", "<f4"), ("tracking_status", "<i4"), ("error", "<f4")])
+
+
+def cfg4_points(seed: int, width: int, height: int, n: int = 2000) -> np.ndarray:
+    """n vx_keypoint_t records at seeded uniform integer positions, tracking_status 1."""
+    r = pcg32(seed, 2 * n, stream=31)
+    kp = np.zeros(n, KEYPOINT_DTYPE)
+    kp["x"] = (r[0::2] % width).astype(np.int32)
+    kp["y"] = (r[1::2] % height).astype(np.int32)
+    kp["tracking_status"] = 1
+    return kp
+
+
+def pyramid_sizes(width: int, height: int, levels: int, scale: float = 0.5) -> list[tuple[int, int]]:
+    """OpenVX pyramid level sizes: level l is ceil(size * scale^l), as AGO computes them."""
+    out = [(width, height)]
+    for _ in range(1, levels):
+        w, h = out[-1]
+        out.append((int(np.ceil(np.float32(w) * np.float32(scale))), int(np.ceil(np.float32(h) * np.float32(scale)))))
+    return out
+
+
 def cfg3_frame(seed: int = 3, width: int = 3840, height: int = 2160, waves: int = 8) -> np.ndarray:
     """RGB frame: per channel a sum of `waves` random 2-D sinusoids scaled to 0..255, plus
     uniform noise in [-10, 10], clipped."""

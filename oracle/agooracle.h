@@ -14,6 +14,7 @@
  */
 #ifndef AGOORACLE_H
 #define AGOORACLE_H
+#include <stddef.h>
 #include <stdint.h>
 #ifdef __cplusplus
 extern "C" {
@@ -83,6 +84,24 @@ int oracle_WarpAffine_U8_U8_Nearest_Constant(uint32_t W, uint32_t H, uint8_t *pD
 int oracle_WarpAffine_U8_U8_Bilinear_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW,
                                               uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride, const float *m,
                                               uint8_t border);
+
+/* ---- pyramid level and pyramidal LK (ago_haf_cpu_pyramid.cpp, ago_haf_cpu_opticalflow.cpp),
+ *      agooracle_flow.c ---- */
+typedef struct {          /* ago_pyramid_u8_t (ago_haf_cpu.h:75) */
+    uint32_t width, height, stride;
+    uint8_t *image;
+    int32_t computed;
+} oracle_pyramid_level;
+int oracle_ScaleGaussianHalf_U8_U8_5x5(uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                       const uint8_t *pSrc, uint32_t srcStride, int sampleFirstRow,
+                                       int sampleFirstColumn);
+int oracle_OpticalFlowPyrLK_XY_XY(oracle_keypoint *newKP, float pyramidScale, uint32_t levels,
+                                  const oracle_pyramid_level *oldPyr, const oracle_pyramid_level *newPyr,
+                                  uint32_t count, const oracle_keypoint *oldKP,
+                                  const oracle_keypoint *estKP, int32_t termination, float epsilon,
+                                  uint32_t numIterations, int32_t useInitialEstimate, uint32_t dataStride,
+                                  uint8_t *data, int32_t winsz);
+size_t oracle_OpticalFlowPyrLK_scratch_size(uint32_t width0, uint32_t height0, uint32_t capacity);
 
 #ifdef __cplusplus
 }
