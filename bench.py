@@ -11,7 +11,8 @@ min distance 5) on 3840x2160 U8 synthetic scenes.
 
 * value  -- Mpixels/s with the inputs already resident in HBM: the device time of each
             graph launch (CUDA events the engine records on its own stream), summed over
-            K steps.  Mpixels counts input pixels of the first node of every frame.
+            K steps.  Mpixels counts the pixels of every input image of the graph (one
+            per frame; both frames of a pair for the pyramid/LK workload).
 * e2e    -- the same metric through the public OpenVX API with host buffers: per step,
             vxCopyImagePatch(WRITE) of every input frame from pinned host memory,
             vxProcessGraph, vxCopyImagePatch(READ) of every output image and
@@ -100,7 +101,46 @@ class CannyHarris(Workload):
         return 2.0 * self.width * self.height * n + corners * C.sizeof(V.vx_keypoint_t)
 
 
-WORKLOADS = {w.name: w for w in (CannyHarris(), GaussChain())}
+class PyramidLK(Workload):
+    name = "pyramid_lk_uneven_x64"
+    desc = ("Per frame pair: GaussianPyramid(5 levels, scale 0.5) of both frames + OpticalFlowPyrLK(9x9 window, "
+            "20 iterations, epsilon 0.01, BOTH) of 2000 seeded uniform points; 64 pairs per step with sizes drawn "
+            "by seed from {640x480, 1280x720, 1920x1080, 3840x2160}; frame 2 = frame 1 shifted by U(+-8) px "
+            "(bilinear) + N(0, 2^2) noise")
+    frames = 64
+    points = 2000
+
+    def sizes(self, n):
+        from mivisionx_b200 import workloads as WL
+        return WL.cfg4_sizes(n, seed=4)
+
+    def make_frames(self, seed0, n):
+        from mivisionx_b200 import workloads as WL
+        out = []
+        for i, (w, h) in enumerate(self.sizes(n)):
+            f1, f2, _ = WL.cfg4_pair(seed=seed0 + i, width=w, height=h)
+            out += [f1, f2]
+        return out
+
+    def build(self, api, ctx, n, flags=None, seed0=1):
+        from mivisionx_b200 import workloads as WL
+        sizes = self.sizes(n)
+        g = WL.Cfg4Graph(api, ctx, sizes, capacity=self.points, flags=flags)
+        pts = [WL.cfg4_points(seed=seed0 + i, width=w, height=h, n=self.points) for i, (w, h) in enumerate(sizes)]
+        for arr, kp in zip(g.pts, pts):
+            api.array_set(arr, kp)
+        g.out_images, g.out_arrays, g.in_arrays = [], g.out, list(zip(g.pts, pts))
+        return g
+
+    def alg_bytes(self, g, n):
+        from mivisionx_b200 import vx as V
+        px = sum(g.api.query_image(i)[0] * g.api.query_image(i)[1] for i in g.inputs)
+        # pyramid: read level 0 once, write levels 1..4 (sum 4^-k); LK: keypoints in + out
+        pyr = px * (1.0 + sum(4.0 ** -k for k in range(1, 5)))
+        return pyr + 2.0 * self.points * len(g.out) * C.sizeof(V.vx_keypoint_t)
+
+
+WORKLOADS = {w.name: w for w in (CannyHarris(), GaussChain(), PyramidLK())}
 DEFAULT_WORKLOAD = CannyHarris.name
 
 
@@ -209,13 +249,14 @@ def _ref_worker(wl_name, seed, seconds, max_iters, barrier, queue):
     wl = WORKLOADS[wl_name]
     ctx = api.vxCreateContext()
     g = wl.build(api, ctx, 1)
-    g.run(wl.make_frames(seed, 1))   # warm-up (first process allocates)
+    frames = wl.make_frames(seed, 1)
+    g.run(frames)                    # warm-up (first process allocates)
     barrier.wait()
     n, t0 = 0, time.perf_counter()
     while n < max_iters and (time.perf_counter() - t0) < seconds:
         g.run()
         n += 1
-    queue.put((n, time.perf_counter() - t0))
+    queue.put((n, time.perf_counter() - t0, sum(int(f.size) for f in frames)))
 
 
 def reference_cpu(wl_name: str, procs: int, seconds: float, max_iters: int = 1 << 30):
@@ -232,10 +273,9 @@ def reference_cpu(wl_name: str, procs: int, seconds: float, max_iters: int = 1 <
         p.join()
     if any(r is None for r in res):
         return None
-    wl = WORKLOADS[wl_name]
     frames = sum(r[0] for r in res)
     wall = max(r[1] for r in res)
-    return frames * wl.width * wl.height / wall / 1e6, wall, frames
+    return sum(r[0] * r[2] for r in res) / wall / 1e6, wall, frames
 
 
 def run_reference_arm(a, wl_name):
@@ -284,7 +324,6 @@ def run_ours(a, wl_name):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     wl = WORKLOADS[wl_name]
-    W, H = wl.width, wl.height
     B = a.frames or wl.frames
     api = V.OpenVX()
     lib = native.agocuda()
@@ -295,9 +334,15 @@ def run_ours(a, wl_name):
     plan = api.plan(g.graph)
     kernels_per_step = sum(k for _, k in plan)
     pin_in = [torch.from_numpy(f).pin_memory() for f in frames]
-    pin_out = [torch.empty((H, W), dtype=torch.uint8).pin_memory() for _ in g.out_images]
+    out_shapes = [api.query_image(i)[1::-1] for i in g.out_images]
+    pin_out = [torch.empty(shp, dtype=torch.uint8).pin_memory() for shp in out_shapes]
+    in_arrays = [(arr, torch.from_numpy(kp.view('u1')).pin_memory(), kp.dtype.itemsize, len(kp))
+                 for arr, kp in getattr(g, "in_arrays", [])]
     g.run([p.numpy() for p in pin_in])
     alg_bytes = wl.alg_bytes(g, B)
+    shapes = sorted({f.shape for f in frames})
+    frame_desc = f"{shapes[0][1]}x{shapes[0][0]}" if len(shapes) == 1 else "uneven: " + ", ".join(
+        f"{sum(1 for f in frames if f.shape == sh)} x {sh[1]}x{sh[0]}" for sh in shapes)
 
     # ---- device-resident throughput
     for _ in range(a.warmup):
@@ -312,24 +357,30 @@ def run_ours(a, wl_name):
         torch.cuda.synchronize()
     _barrier(ws)
     ms_step = _max_over_ranks(sum(gpu_ms), ws) / a.steps
-    px_step = W * H * B
+    px_step = sum(int(f.size) for f in frames)
     value = px_step * ws / (ms_step / 1e3) / 1e6
 
     # ---- end to end through the OpenVX API with host buffers
-    addr = V.vx_imagepatch_addressing_t()
-    addr.dim_x, addr.dim_y, addr.stride_x, addr.stride_y = W, H, 1, W
-    addr.scale_x = addr.scale_y = 1024
-    addr.step_x = addr.step_y = 1
-    rect = V.vx_rectangle_t(0, 0, W, H)
+    def patch(h, w):
+        addr = V.vx_imagepatch_addressing_t()
+        addr.dim_x, addr.dim_y, addr.stride_x, addr.stride_y = w, h, 1, w
+        addr.scale_x = addr.scale_y = 1024
+        addr.step_x = addr.step_y = 1
+        return V.vx_rectangle_t(0, 0, w, h), addr
+    in_patch = [patch(*f.shape) for f in frames]
+    out_patch = [patch(*shp) for shp in out_shapes]
     arr_bufs = [np.zeros(1 << 16, V.KEYPOINT_DTYPE) for _ in g.out_arrays]
     d2h_arrays = [0]
 
     def e2e_step():
-        for img, p in zip(g.inputs, pin_in):
+        for img, p, (rect, addr) in zip(g.inputs, pin_in, in_patch):
             api.ok(api.vxCopyImagePatch(img, C.byref(rect), 0, C.byref(addr), p.data_ptr(), V.VX_WRITE_ONLY,
                                         V.VX_MEMORY_TYPE_HOST), "write")
+        for arr, p, isz, n in in_arrays:
+            api.ok(api.vxCopyArrayRange(arr, 0, n, isz, p.data_ptr(), V.VX_WRITE_ONLY, V.VX_MEMORY_TYPE_HOST),
+                   "write array")
         api.ok(api.vxProcessGraph(g.graph), "process")
-        for img, p in zip(g.out_images, pin_out):
+        for img, p, (rect, addr) in zip(g.out_images, pin_out, out_patch):
             api.ok(api.vxCopyImagePatch(img, C.byref(rect), 0, C.byref(addr), p.data_ptr(), V.VX_READ_ONLY,
                                         V.VX_MEMORY_TYPE_HOST), "read")
         nbytes = 0
@@ -367,20 +418,21 @@ def run_ours(a, wl_name):
             r = reference_cpu(wl_name, 1, a.cpu_seconds)
             if r is not None:
                 cpu = {"value": round(r[0], 2), "unit": "Mpixels/s", "cores": 1, "kind": "reference",
-                       "sample": f"{r[2]} x one {W}x{H} frame through the reference AGO CPU graph "
-                                 f"({r[1]:.1f} s of CPU work, 1 core)"}
+                       "sample": f"{r[2]} runs of the one-unit graph ({frame_desc.split(',')[0]} class) through "
+                                 f"the reference AGO CPU library ({r[1]:.1f} s of CPU work, 1 core)"}
         print(json.dumps({
             "metric": "Mpixels/s per vision graph", "value": round(value, 1), "unit": "Mpixels/s", "n_gpus": ws,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded PCG32)",
-            "config": {"workload": wl_name, "graph": wl.desc, "frames_per_step_per_gpu": B, "frame": f"{W}x{H}",
+            "config": {"workload": wl_name, "graph": wl.desc, "frames_per_step_per_gpu": B, "frame": frame_desc,
                        "l2": "inputs+outputs per step exceed the 126 MB L2 (no flush needed)",
                        "plan": [n for n, _ in plan], "parallelism": f"replicas x{ws} (frames sharded, no collective)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel": f"one step: {kernels_per_step} kernels in one CUDA graph"},
-            "e2e": {"value": round(e2e, 1), "unit": "Mpixels/s", "h2d_bytes_per_step": W * H * B,
-                    "d2h_bytes_per_step": W * H * len(g.out_images) + d2h_arrays[0]},
+            "e2e": {"value": round(e2e, 1), "unit": "Mpixels/s",
+                    "h2d_bytes_per_step": px_step + sum(isz * n for _, _, isz, n in in_arrays),
+                    "d2h_bytes_per_step": sum(h * w for h, w in out_shapes) + d2h_arrays[0]},
             "gpu_launches": kernels_per_step * a.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,

@@ -243,9 +243,6 @@ int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t width, uint32_
                                            uint16_t hystLower, uint16_t hystUpper,
                                            void *scratch, size_t scratchBytes, uint32_t *pStatus);
 
-/* vxHarrisCornersNode (gradient 3, block 3) as one front-end kernel (Sobel products,
- * window sums, score and non-maximum suppression from one read of the image) plus the
- * corner pick.  Scratch: agocuda_fused_HarrisCorners_scratch_size(W, H) bytes. */
 /* RGB -> NV12 + IYUV + half-size bilinear ScaleImage + half-size area ScaleImage of Y, in
  * one pass over the RGB frame (W even, >= 16; H even).  Outputs bit-identical to the four
  * unfused AGO nodes (the scaled images read the Y plane both colour outputs share). */
@@ -255,11 +252,97 @@ int agocuda_fused_ColorScale_RGB(void *stream, uint32_t width, uint32_t height, 
                                  uint8_t *pV, uint32_t vStride, uint8_t *pHalfBilinear, uint32_t hbStride,
                                  uint8_t *pHalfArea, uint32_t haStride);
 
+/* vxHarrisCornersNode (gradient 3, block 3) as one front-end kernel (Sobel products,
+ * window sums, score and non-maximum suppression from one read of the image) plus the
+ * corner pick.  Scratch: agocuda_fused_HarrisCorners_scratch_size(W, H) bytes. */
 size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t width, uint32_t height);
 int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t width, uint32_t height, const uint8_t *pSrc, uint32_t srcStride,
                                     float sensitivity, float strengthThreshold, float normFactor, float minDistance,
                                     void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
                                     uint32_t *pNumCorners, void *scratch, size_t scratchBytes, uint32_t *pStatus);
+
+/* ---------------------------------------------------------------- Gaussian pyramid */
+/* One pyramid level of VX_SCALE_PYRAMID_HALF: dst (ceil(srcW/2) x ceil(srcH/2)) rows 1..H-2 are
+ * the [1 4 6 4 1]^2 / 256 samples the AGO CPU kernel computes (sample parity from the source
+ * size, two-pixel reads outside the row resolved with AGO's buffer layout); rows 0 and H-1
+ * are written 0 (the reference never writes them).  src/dst 16-byte aligned, strides
+ * multiples of 16.  Replaces HafCpu_ScaleGaussianHalf_U8_U8_5x5 (ago_haf_cpu_pyramid.cpp:94)
+ * as agoKernel_ScaleGaussianHalf_U8_U8_5x5 calls it (ago_kernel_api.cpp:15420); the HIP
+ * target has no 5x5 launcher. */
+int agocuda_ScaleGaussianHalf_U8_U8_5x5(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                        uint32_t dstStride, uint32_t srcWidth, uint32_t srcHeight,
+                                        const uint8_t *pSrc, uint32_t srcStride);
+
+/* Batched levels: one launch computes one level for many images (e.g. level k of every
+ * frame's pyramid).  `jobs` is a DEVICE array sorted by tileBegin; job i owns tiles
+ * [tileBegin, tileBegin + agocuda_ScaleGaussianHalf_tiles(dstW, dstH)). */
+typedef struct agocuda_half_job {
+    const uint8_t *src;
+    uint8_t *dst;
+    uint32_t srcW, srcH, srcStride, dstW, dstH, dstStride, tileBegin, reserved;
+} agocuda_half_job;
+uint32_t agocuda_ScaleGaussianHalf_tiles(uint32_t dstWidth, uint32_t dstHeight);
+int agocuda_fused_ScaleGaussianHalf_batch(void *stream, const agocuda_half_job *jobs, uint32_t numJobs,
+                                          uint32_t totalTiles);
+
+/* ---------------------------------------------------------------- pyramidal LK */
+#define AGOCUDA_LK_MAX_LEVELS 12
+#define AGOCUDA_LK_MAX_WINDOW 15      /* AGO_OPTICALFLOWPYRLK_MAX_DIM */
+/* With termination VX_TERM_CRITERIA_EPSILON alone the reference loop has no iteration bound
+ * (ago_haf_cpu_opticalflow.cpp:431); a point that never converges stops after this many. */
+#define AGOCUDA_LK_EPSILON_ONLY_MAX_ITERATIONS 4096u
+#define AGOCUDA_LK_STATUS_BAD_COUNT 16u  /* old/estimate counts differ or exceed the output capacity */
+
+typedef struct agocuda_pyramid_level {   /* one level: device image, as ago_pyramid_u8_t */
+    const uint8_t *image;
+    uint32_t width, height, stride, reserved;
+} agocuda_pyramid_level;
+
+/* One OpticalFlowPyrLK node (one frame pair).  Keypoint arrays hold vx_keypoint_t records;
+ * counts are device words.  scharrRows is the node's persistent Scharr row-buffer state:
+ * agocuda_OpticalFlowPyrLK_scharr_rows_size(level-0 width) bytes, zeroed when the node is
+ * created and kept across executions (the reference's node scratch, whose stale words
+ * reach the derivatives of column 0).  count and scharrWords are written by the kernels. */
+typedef struct agocuda_lk_frame {
+    agocuda_pyramid_level oldPyr[AGOCUDA_LK_MAX_LEVELS], newPyr[AGOCUDA_LK_MAX_LEVELS];
+    const void *oldPoints, *estPoints;
+    void *newPoints;
+    const uint32_t *pOldCount, *pEstCount;
+    uint32_t *pNewCount;
+    uint16_t *scharrRows;
+    uint32_t newCapacity, levels;
+    int32_t termination;
+    float epsilon;
+    uint32_t numIterations;
+    int32_t useInitialEstimate, windowDimension;
+    uint32_t count;
+    uint32_t scharrWords[AGOCUDA_LK_MAX_LEVELS][2];
+} agocuda_lk_frame;
+size_t agocuda_OpticalFlowPyrLK_scharr_rows_size(uint32_t width0);
+
+/* Pyramidal LK for many frame pairs in two launches (row-buffer replay + one warp per
+ * keypoint).  `frames` is a DEVICE array; maxPoints bounds every frame's count.  Results are
+ * identical to HafCpu_OpticalFlowPyrLK_XY_XY_Generic (ago_haf_cpu_opticalflow.cpp:153; CPU
+ * only in the reference, ago_kernel_api.cpp:20587) for HALF pyramids whose level widths are
+ * all >= 8.  One exception: on a level above 0 whose width % 8 >= 3 the reference's window
+ * can reach derivative columns [W & ~7, W - 3], which it never writes at that level; on a
+ * node's first call they hold 0, on later calls the previous frame's level-0 derivatives.
+ * These kernels always use 0 there (the first-call value). */
+int agocuda_OpticalFlowPyrLK_batch(void *stream, agocuda_lk_frame *frames, uint32_t numFrames, uint32_t maxPoints,
+                                   uint32_t *pStatus);
+
+/* Single node with the reference's argument meaning.  oldPyramid/newPyramid are HOST arrays
+ * of `levels` descriptors (device images); counts are device words.  scratch (device,
+ * agocuda_OpticalFlowPyrLK_scratch_size(width0) bytes, zeroed before the node's first call
+ * and kept between calls) holds the frame descriptor and the Scharr row-buffer state. */
+size_t agocuda_OpticalFlowPyrLK_scratch_size(uint32_t width0);
+int agocuda_OpticalFlowPyrLK_XY_XY(void *stream, void *newKeyPoint, uint32_t newCapacity, uint32_t *pNewCount,
+                                   float pyramidScale, uint32_t levels, const agocuda_pyramid_level *oldPyramid,
+                                   const agocuda_pyramid_level *newPyramid, const uint32_t *pKeyPointCount,
+                                   const void *oldKeyPoint, const uint32_t *pEstimateCount,
+                                   const void *newKeyPointEstimate, int32_t termination, float epsilon,
+                                   uint32_t numIterations, int32_t useInitialEstimate, int32_t windowDimension,
+                                   void *scratch, size_t scratchBytes, uint32_t *pStatus);
 
 #ifdef __cplusplus
 }

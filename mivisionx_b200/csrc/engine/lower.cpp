@@ -168,7 +168,11 @@ vx_status validate_node(Graph *g, Node *n)
         if (o->item_type == VX_TYPE_INVALID && o->is_virtual) { o->item_type = VX_TYPE_KEYPOINT; o->item_size = sizeof(vx_keypoint_t); }
         if (static_cast<Array *>(p[2])->item_type != VX_TYPE_KEYPOINT || o->item_type != VX_TYPE_KEYPOINT) return VX_ERROR_INVALID_TYPE;
         const vx_size win = static_cast<Scalar *>(p[9])->v.sz;
-        if (win < 3 || win > 9 || !(win & 1)) return VX_ERROR_INVALID_VALUE;
+        if (win < 3 || win > AGOCUDA_LK_MAX_WINDOW) return VX_ERROR_INVALID_VALUE;   // ago_kernel_api.cpp:20624
+        if (a->levels > AGOCUDA_LK_MAX_LEVELS) return VX_ERROR_NOT_SUPPORTED;
+        // the reference's Scharr pass loops on `x <= width - 8` in unsigned arithmetic
+        // (ago_haf_cpu_opticalflow.cpp:95), so it cannot process a level narrower than 8
+        for (Image *lv : a->level) if (lv->width < 8 || lv->height < 3) return VX_ERROR_INVALID_DIMENSION;
         return VX_SUCCESS;
     }
     default:
@@ -422,6 +426,8 @@ static bool merge_pass(Graph *g)
 
 static void replace_data(Graph *g, Ref *from, Ref *to)
 {
+    g->replaced[from] = to;
+    for (auto &kv : g->replaced) if (kv.second == from) kv.second = to;
     for (LNode &ln : g->lnodes)
         for (Ref *&r : ln.p) if (r == from) r = to;
 }
@@ -523,6 +529,7 @@ static vx_status sort_lnodes(Graph *g)
 vx_status lower_graph(Graph *g)
 {
     g->lnodes.clear();
+    g->replaced.clear();
     for (Node *n : g->nodes) {
         if (n->removed) continue;
         vx_status s = validate_node(g, n);

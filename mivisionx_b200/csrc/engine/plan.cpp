@@ -69,6 +69,93 @@ static float harris_norm(int32_t gs)
 }
 
 // ------------------------------------------------------------------------------------
+// pyramidal LK: device descriptors of OPTICAL_FLOW_PYR_LK_XY_XY nodes
+// (AGO order: new points, old pyramid, new pyramid, old points, estimates, termination,
+//  epsilon, num_iterations, use_initial_estimate, window_dimension)
+// ------------------------------------------------------------------------------------
+// a pyramid level as the kernels see it: a virtual level-0 copy removed by the copy-removal
+// pass reads its source image (ago_drama_remove.cpp:926)
+static const Image *pyr_level(Graph *g, Pyramid *py, size_t l)
+{
+    auto it = g->replaced.find(py->level[l]);
+    return it == g->replaced.end() ? py->level[l] : IMG(it->second);
+}
+
+static vx_status lk_frame(Graph *g, LNode &ln, agocuda_lk_frame &F, uint32_t &cap)
+{
+    auto &p = ln.p;
+    memset(&F, 0, sizeof F);
+    Pyramid *po = static_cast<Pyramid *>(p[1]), *pn = static_cast<Pyramid *>(p[2]);
+    if (po->levels > AGOCUDA_LK_MAX_LEVELS) return VX_ERROR_NOT_SUPPORTED;
+    for (size_t l = 0; l < po->levels; l++) {
+        const Image *a = pyr_level(g, po, l), *b = pyr_level(g, pn, l);
+        F.oldPyr[l] = agocuda_pyramid_level{a->planes[0].dev, a->width, a->height, a->planes[0].dev_stride, 0};
+        F.newPyr[l] = agocuda_pyramid_level{b->planes[0].dev, b->width, b->height, b->planes[0].dev_stride, 0};
+    }
+    Array *out = static_cast<Array *>(p[0]), *old = static_cast<Array *>(p[3]), *est = static_cast<Array *>(p[4]);
+    F.oldPoints = old->dev; F.estPoints = est->dev; F.newPoints = out->dev;
+    F.pOldCount = old->dev_count; F.pEstCount = est->dev_count; F.pNewCount = out->dev_count;
+    F.newCapacity = (uint32_t)out->capacity;
+    F.levels = (uint32_t)po->levels;
+    F.termination = sc_enum(p[5]);
+    F.epsilon = sc_f32(p[6]);
+    F.numIterations = static_cast<Scalar *>(p[7])->v.u32;
+    F.useInitialEstimate = static_cast<Scalar *>(p[8])->v.b ? 1 : 0;
+    F.windowDimension = (int32_t)static_cast<Scalar *>(p[9])->v.sz;
+    // the node's Scharr row-buffer state starts zeroed, like the reference's node scratch
+    void *rows = scratch(g, agocuda_OpticalFlowPyrLK_scharr_rows_size(po->level[0]->width));
+    if (!rows) return VX_ERROR_NO_MEMORY;
+    F.scharrRows = (uint16_t *)rows;
+    cap = (uint32_t)old->capacity;
+    return VX_SUCCESS;
+}
+
+static vx_status lk_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step &st)
+{
+    std::vector<agocuda_lk_frame> fr(nodes.size());
+    uint32_t maxPts = 0;
+    for (size_t i = 0; i < nodes.size(); i++) {
+        uint32_t cap = 0;
+        if (vx_status s = lk_frame(g, *nodes[i], fr[i], cap)) return s;
+        maxPts = std::max(maxPts, cap);
+    }
+    void *dev = scratch(g, fr.size() * sizeof(agocuda_lk_frame));
+    if (!dev) return VX_ERROR_NO_MEMORY;
+    if (cudaMemcpy(dev, fr.data(), fr.size() * sizeof(agocuda_lk_frame), cudaMemcpyHostToDevice) != cudaSuccess)
+        return VX_FAILURE;
+    const uint32_t n = (uint32_t)fr.size();
+    uint32_t *status = g->status_dev;
+    st.num_kernels = 2;
+    st.launch = [=](cudaStream_t q) {
+        return agocuda_OpticalFlowPyrLK_batch(S(q), (agocuda_lk_frame *)dev, n, maxPts, status);
+    };
+    return VX_SUCCESS;
+}
+
+// ScaleGaussianHalf levels of many images in one launch (one job per lowered node)
+static vx_status half_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step &st)
+{
+    std::vector<agocuda_half_job> jobs;
+    uint32_t tiles = 0;
+    for (LNode *ln : nodes) {
+        const Image *d = IMG(ln->p[0]), *s = IMG(ln->p[1]);
+        agocuda_half_job j{s->planes[0].dev, d->planes[0].dev, s->width, s->height, s->planes[0].dev_stride,
+                           d->width, d->height, d->planes[0].dev_stride, tiles, 0};
+        tiles += agocuda_ScaleGaussianHalf_tiles(d->width, d->height);
+        jobs.push_back(j);
+    }
+    void *dev = scratch(g, jobs.size() * sizeof(agocuda_half_job));
+    if (!dev) return VX_ERROR_NO_MEMORY;
+    if (cudaMemcpy(dev, jobs.data(), jobs.size() * sizeof(agocuda_half_job), cudaMemcpyHostToDevice) != cudaSuccess)
+        return VX_FAILURE;
+    const uint32_t n = (uint32_t)jobs.size();
+    st.launch = [=](cudaStream_t q) {
+        return agocuda_fused_ScaleGaussianHalf_batch(S(q), (const agocuda_half_job *)dev, n, tiles);
+    };
+    return VX_SUCCESS;
+}
+
+// ------------------------------------------------------------------------------------
 // plain (one launch per lowered node) steps
 // ------------------------------------------------------------------------------------
 static vx_status plain_step(Graph *g, LNode &ln, Step &st)
@@ -247,6 +334,14 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         };
         return VX_SUCCESS;
     }
+    case LK::SCALE_GAUSSIAN_HALF_U8_U8_5x5: {                    // ago_kernel_api.cpp:15420
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        const uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), sw = W(p[1]), sh = H(p[1]), ss = dstride(p[1]);
+        st.launch = [=](cudaStream_t q) { return agocuda_ScaleGaussianHalf_U8_U8_5x5(S(q), w, h, d, ds, sw, sh, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::OPTICAL_FLOW_PYR_LK_XY_XY:                           // ago_kernel_api.cpp:20587
+        return lk_batch_step(g, {&ln}, st);
     default:
         log_error(g, VX_ERROR_NOT_IMPLEMENTED, "ERROR: kernel %s has no device implementation yet\n", lk_name(ln.k));
         return VX_ERROR_NOT_IMPLEMENTED;
@@ -349,6 +444,13 @@ static bool match_color_scale(Graph *g, LNode &a, Chain &c)
 
 static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &st)
 {
+    if (chains[0].kind == "batch_ScaleGaussianHalf" || chains[0].kind == "batch_OpticalFlowPyrLK") {
+        std::vector<LNode *> nodes;
+        for (Chain &c : chains) nodes.push_back(c.nodes[0]);
+        st.name = chains[0].kind + " x" + std::to_string(chains.size());
+        st.nodes = nodes;
+        return chains[0].kind == "batch_ScaleGaussianHalf" ? half_batch_step(g, nodes, st) : lk_batch_step(g, nodes, st);
+    }
     if (chains[0].kind == "fused_ColorScale") {
         std::vector<std::function<int(cudaStream_t)>> fns;
         st.name = chains[0].kind + " x" + std::to_string(chains.size());
@@ -488,6 +590,8 @@ vx_status plan_graph(Graph *g)
             else if (match_canny(g, ln, c)) pattern = 2;
             else if (match_harris(g, ln, c)) pattern = 3;
             else if (match_color_scale(g, ln, c)) pattern = 4;
+            else if (ln.k == LK::SCALE_GAUSSIAN_HALF_U8_U8_5x5) { c.kind = "batch_ScaleGaussianHalf"; c.nodes = {&ln}; pattern = 5; }
+            else if (ln.k == LK::OPTICAL_FLOW_PYR_LK_XY_XY) { c.kind = "batch_OpticalFlowPyrLK"; c.nodes = {&ln}; pattern = 6; }
             for (LNode *n : c.nodes) if (pattern && fused.count(n)) pattern = 0;   // a node joins one chain
             if (pattern) {
                 std::vector<int64_t> gk{pattern, ln.level};
@@ -508,7 +612,10 @@ vx_status plan_graph(Graph *g)
             if (!r || elided.count(r)) continue;
             if (r->type == VX_TYPE_IMAGE) { if (image_alloc_device(IMG(r))) return VX_ERROR_NO_MEMORY; }
             else if (r->type == VX_TYPE_ARRAY) { if (array_alloc_device(static_cast<Array *>(r))) return VX_ERROR_NO_MEMORY; }
-            else if (r->type == VX_TYPE_PYRAMID) { for (Image *lv : static_cast<Pyramid *>(r)->level) if (image_alloc_device(lv)) return VX_ERROR_NO_MEMORY; }
+            else if (r->type == VX_TYPE_PYRAMID) {
+                for (Image *lv : static_cast<Pyramid *>(r)->level)
+                    if (!g->replaced.count(lv) && image_alloc_device(lv)) return VX_ERROR_NO_MEMORY;
+            }
             else if (r->type == VX_TYPE_SCALAR && r->is_virtual == false) { /* host value */ }
         }
 

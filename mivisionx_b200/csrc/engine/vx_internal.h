@@ -199,6 +199,7 @@ struct Step {
 struct Graph : Ref {
     std::vector<Node *> nodes;
     std::vector<LNode> lnodes;
+    std::map<Ref *, Ref *> replaced;  // virtual data the copy-removal pass replaced by the copy's source
     std::vector<Step> steps;
     std::vector<Ref *> inputs, outputs;          // non-virtual data read / written by the graph
     std::vector<Ref *> owned_virtual;            // virtual data created for lowering

@@ -290,6 +290,8 @@ vx_status array_alloc_device(Array *a)
     if (a->dev) return VX_SUCCESS;
     if (!a->item_size || !a->capacity) return VX_ERROR_INVALID_PARAMETERS;
     if (cudaMalloc((void **)&a->dev, a->item_size * a->capacity + 64) != cudaSuccess) return VX_ERROR_NO_MEMORY;
+    // zeroed like AGO's buffers (agoAllocMemory uses calloc): fields a kernel leaves alone read 0
+    cudaMemset(a->dev, 0, a->item_size * a->capacity + 64);
     if (cudaMalloc((void **)&a->dev_count, 16) != cudaSuccess) return VX_ERROR_NO_MEMORY;
     cudaMemset(a->dev_count, 0, 16);
     return VX_SUCCESS;

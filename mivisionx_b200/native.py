@@ -35,6 +35,29 @@ class AgoFrame(C.Structure):
                 ("srcStride", u32), ("dstStride", u32), ("simdBegin", i32), ("simdEnd", i32)]
 
 
+LK_MAX_LEVELS = 12
+
+
+class PyramidLevel(C.Structure):
+    """Mirror of `agocuda_pyramid_level`."""
+    _fields_ = [("image", vp), ("width", u32), ("height", u32), ("stride", u32), ("reserved", u32)]
+
+
+class HalfJob(C.Structure):
+    """Mirror of `agocuda_half_job`."""
+    _fields_ = [("src", vp), ("dst", vp), ("srcW", u32), ("srcH", u32), ("srcStride", u32), ("dstW", u32),
+                ("dstH", u32), ("dstStride", u32), ("tileBegin", u32), ("reserved", u32)]
+
+
+class LkFrame(C.Structure):
+    """Mirror of `agocuda_lk_frame`."""
+    _fields_ = [("oldPyr", PyramidLevel * LK_MAX_LEVELS), ("newPyr", PyramidLevel * LK_MAX_LEVELS),
+                ("oldPoints", vp), ("estPoints", vp), ("newPoints", vp), ("pOldCount", vp), ("pEstCount", vp),
+                ("pNewCount", vp), ("scharrRows", vp), ("newCapacity", u32), ("levels", u32), ("termination", i32),
+                ("epsilon", f32), ("numIterations", u32), ("useInitialEstimate", i32), ("windowDimension", i32),
+                ("count", u32), ("scharrWords", (u32 * 2) * LK_MAX_LEVELS)]
+
+
 def agocuda() -> C.CDLL:
     """The CUDA kernel library (include/agocuda.h).  Raises if it has not been built."""
     global _agocuda

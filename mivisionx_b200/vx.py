@@ -59,6 +59,7 @@ VX_MEMORY_TYPE_HIP = _enum_base(0, 0x0E) + 3
 VX_TERM_CRITERIA_ITERATIONS = _enum_base(0, 0x0F) + 0
 VX_TERM_CRITERIA_EPSILON = _enum_base(0, 0x0F) + 1
 VX_TERM_CRITERIA_BOTH = _enum_base(0, 0x0F) + 2
+VX_SCALE_PYRAMID_HALF = 0.5
 VX_NORM_L1 = _enum_base(0, 0x10) + 0
 VX_NORM_L2 = _enum_base(0, 0x10) + 1
 VX_READ_ONLY = _enum_base(0, 0x11) + 1

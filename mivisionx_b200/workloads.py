@@ -328,3 +328,64 @@ class Cfg2Graph:
         for e, arr, num in zip(self.edges, self.corners, self.num):
             out.append((a.read_plane(e), a.valid_region(e), a.array_items(arr), a.read_scalar(num)))
         return out
+
+
+class Cfg4Graph:
+    """Per frame pair: GaussianPyramid (scale 0.5, `levels` levels, virtual pyramids) of both
+    frames and OpticalFlowPyrLK (window, iterations, epsilon, termination) of `points`
+    keypoints, all pairs in one OpenVX graph.  The estimates array is the old-points array
+    (use_initial_estimate false)."""
+
+    def __init__(self, api: V.OpenVX, ctx, sizes, levels=5, window=9, iterations=20, epsilon=0.01,
+                 termination=None, capacity=2000, flags: int | None = None, virtual_pyramids=True):
+        self.api, self.ctx = api, ctx
+        a = api
+        self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
+        if flags is not None:
+            a.set_optimizer_flags(self.graph, flags)
+        term = V.VX_TERM_CRITERIA_BOTH if termination is None else termination
+        self.s_eps = a.scalar(ctx, V.VX_TYPE_FLOAT32, epsilon)
+        self.s_iter = a.scalar(ctx, V.VX_TYPE_UINT32, iterations)
+        self.s_est = a.scalar(ctx, V.VX_TYPE_BOOL, 0)
+        self.old, self.new, self.pts, self.out, self.pyr = [], [], [], [], []
+        g = self.graph
+        for (w, h) in sizes:
+            i0 = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+            i1 = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+            if virtual_pyramids:
+                p0 = a.obj(a.vxCreateVirtualPyramid(g, levels, V.VX_SCALE_PYRAMID_HALF, w, h, V.VX_DF_IMAGE_U8), "pyramid")
+                p1 = a.obj(a.vxCreateVirtualPyramid(g, levels, V.VX_SCALE_PYRAMID_HALF, w, h, V.VX_DF_IMAGE_U8), "pyramid")
+            else:
+                p0 = a.obj(a.vxCreatePyramid(ctx, levels, V.VX_SCALE_PYRAMID_HALF, w, h, V.VX_DF_IMAGE_U8), "pyramid")
+                p1 = a.obj(a.vxCreatePyramid(ctx, levels, V.VX_SCALE_PYRAMID_HALF, w, h, V.VX_DF_IMAGE_U8), "pyramid")
+            pts = a.obj(a.vxCreateArray(ctx, V.VX_TYPE_KEYPOINT, capacity), "array")
+            out = a.obj(a.vxCreateArray(ctx, V.VX_TYPE_KEYPOINT, capacity), "array")
+            a.obj(a.vxGaussianPyramidNode(g, i0, p0), "pyramid node")
+            a.obj(a.vxGaussianPyramidNode(g, i1, p1), "pyramid node")
+            a.obj(a.vxOpticalFlowPyrLKNode(g, p0, p1, pts, pts, out, term, self.s_eps, self.s_iter, self.s_est, window),
+                  "optical flow node")
+            self.old.append(i0); self.new.append(i1); self.pts.append(pts); self.out.append(out)
+            self.pyr.append((p0, p1))
+        a.ok(a.vxVerifyGraph(g), "vxVerifyGraph")
+
+    @property
+    def inputs(self):
+        """Input images in (old, new) pair order."""
+        return [i for pair in zip(self.old, self.new) for i in pair]
+
+    def set_inputs(self, pairs, points):
+        a = self.api
+        for i0, i1, arr, (f1, f2), kp in zip(self.old, self.new, self.pts, pairs, points):
+            a.write_plane(i0, f1)
+            a.write_plane(i1, f2)
+            a.array_set(arr, kp)
+
+    def run(self, frames=None):
+        """frames: optional flat list of input images in `inputs` order."""
+        if frames is not None:
+            for img, f in zip(self.inputs, frames):
+                self.api.write_plane(img, f)
+        self.api.ok(self.api.vxProcessGraph(self.graph), "vxProcessGraph")
+
+    def results(self):
+        return [self.api.array_items(o) for o in self.out]

@@ -65,3 +65,21 @@ def test_libraries_export_declared_symbols():
     ovx = native.openvx()
     for name in _declared(HDR, "vx"):
         assert hasattr(ovx, name), name
+
+
+def test_ctypes_mirrors_match_agocuda_structs():
+    """The ctypes mirrors in mivisionx_b200/native.py have the C layout of include/agocuda.h."""
+    import ctypes
+    from mivisionx_b200 import native
+    checks = {"agocuda_frame": native.AgoFrame, "agocuda_pyramid_level": native.PyramidLevel,
+              "agocuda_half_job": native.HalfJob, "agocuda_lk_frame": native.LkFrame}
+    body = "".join(f'printf("{n} %zu\\n", sizeof({n}));\n' for n in checks)
+    for f in ("count", "scharrWords", "windowDimension", "newCapacity"):
+        body += f'printf("lk.{f} %zu\\n", offsetof(agocuda_lk_frame, {f}));\n'
+    out = _run('#include <stdio.h>\n#include <stddef.h>\n#include "agocuda.h"\nint main(){' + body + "return 0;}",
+               [os.path.dirname(AGOCUDA_H), "/usr/local/cuda/include"])
+    got = dict(line.split() for line in out.strip().splitlines())
+    for n, cls in checks.items():
+        assert int(got[n]) == ctypes.sizeof(cls), n
+    for f in ("count", "scharrWords", "windowDimension", "newCapacity"):
+        assert int(got["lk." + f]) == getattr(native.LkFrame, f).offset, f
