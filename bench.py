@@ -330,7 +330,7 @@ def run_ours(a, wl_name):
     ctx = api.obj(api.vxCreateContext(), "context")
     api.set_device(ctx, local)
     frames = wl.make_frames(1000 * rank + 1, B)
-    g = wl.build(api, ctx, B)
+    g = wl.build(api, ctx, B, flags=V.OPT_NO_FUSION if a.plain else None)
     plan = api.plan(g.graph)
     kernels_per_step = sum(k for _, k in plan)
     pin_in = [torch.from_numpy(f).pin_memory() for f in frames]
@@ -426,7 +426,7 @@ def run_ours(a, wl_name):
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded PCG32)",
             "config": {"workload": wl_name, "graph": wl.desc, "frames_per_step_per_gpu": B, "frame": frame_desc,
                        "l2": "inputs+outputs per step exceed the 126 MB L2 (no flush needed)",
-                       "plan": [n for n, _ in plan], "parallelism": f"replicas x{ws} (frames sharded, no collective)"},
+                       "plan": [n for n, _ in plan], "plan_form": "plain" if a.plain else "fused+batched", "parallelism": f"replicas x{ws} (frames sharded, no collective)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel": f"one step: {kernels_per_step} kernels in one CUDA graph"},
@@ -454,6 +454,8 @@ def main(argv=None):
     ap.add_argument("--frames", type=int, default=0, help="frames per step per GPU (default: the workload's)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", action="store_true",
+                    help="run the one-launch-per-node plan (the unfused, unbatched comparison form)")
     a = ap.parse_args(argv)
     if a.impl == "ours":
         a.warmup = max(a.warmup, 3)

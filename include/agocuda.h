@@ -210,6 +210,43 @@ int agocuda_WarpAffine_U8_U8_Bilinear_Constant(void *stream, uint32_t dstWidth, 
                                                const uint8_t *pSrc, uint32_t srcStride, const float *affineMatrix,
                                                uint8_t border);
 
+/* WarpPerspective, constant border; perspectiveMatrix is a HOST pointer to
+ * ago_perspective_matrix_t (float[3][3], the vx_matrix data): x' = (m00 x + m10 y + m20) /
+ * (m02 x + m12 y + m22), y' likewise with m01, m11, m21.  Source taps are addressed as the
+ * reference addresses them in AGO's buffer layout (row pitch ALIGN16(srcWidth)).  With an
+ * UNDEFINED border the reference runs these with border 0 (geometric.cpp:1372, :1560).
+ * Replace HipExec_WarpPerspective_U8_U8_{Nearest,Bilinear}[_Constant]
+ * (hipvx/hip_host_decls.h:775-794); HafCpu_WarpPerspective_U8_U8_{Nearest,Bilinear}_Constant
+ * (ago_haf_cpu_geometric.cpp:1406 / :1579). */
+int agocuda_WarpPerspective_U8_U8_Nearest_Constant(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                                   uint32_t dstStride, uint32_t srcWidth, uint32_t srcHeight,
+                                                   const uint8_t *pSrc, uint32_t srcStride,
+                                                   const float *perspectiveMatrix, uint8_t border);
+int agocuda_WarpPerspective_U8_U8_Bilinear_Constant(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                                    uint32_t dstStride, uint32_t srcWidth, uint32_t srcHeight,
+                                                    const uint8_t *pSrc, uint32_t srcStride,
+                                                    const float *perspectiveMatrix, uint8_t border);
+
+/* Remap through AGO's fixed-point table: one uint32 per destination pixel (u16 x | u16 y
+ * << 16, 3 fractional bits, 0xFFFF = outside the source: the table vxSetRemapPoint builds,
+ * api/vx_api.cpp:7884), mapStride bytes per row, DEVICE memory.  The constant-border and
+ * undefined-border kernels treat 0xFFFF differently, as the reference does.  Replace
+ * HipExec_Remap_U8_U8_{Nearest,Nearest_Constant,Bilinear,Bilinear_Constant}
+ * (hipvx/hip_host_decls.h:801-819); HafCpu_Remap_U8_U8_* (ago_haf_cpu_geometric.cpp:72 /
+ * :156 / :249 / :372). */
+int agocuda_Remap_U8_U8_Nearest(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                uint32_t srcWidth, uint32_t srcHeight, const uint8_t *pSrc, uint32_t srcStride,
+                                const uint32_t *pMap, uint32_t mapStride);
+int agocuda_Remap_U8_U8_Nearest_Constant(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                         uint32_t dstStride, uint32_t srcWidth, uint32_t srcHeight, const uint8_t *pSrc,
+                                         uint32_t srcStride, const uint32_t *pMap, uint32_t mapStride, uint8_t border);
+int agocuda_Remap_U8_U8_Bilinear(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                 uint32_t srcWidth, uint32_t srcHeight, const uint8_t *pSrc, uint32_t srcStride,
+                                 const uint32_t *pMap, uint32_t mapStride);
+int agocuda_Remap_U8_U8_Bilinear_Constant(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                          uint32_t dstStride, uint32_t srcWidth, uint32_t srcHeight, const uint8_t *pSrc,
+                                          uint32_t srcStride, const uint32_t *pMap, uint32_t mapStride, uint8_t border);
+
 /* ------------------------------------------------------------------------------------ */
 /* Fused multi-node kernels (no reference counterpart: the HIP target launches one kernel */
 /* per node, ago/ago_util_hip.cpp:686; agoGpuHipSuperNodeLaunch returns -1 at :740)      */
@@ -267,8 +304,8 @@ int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t width, uint32_t heigh
  * size, two-pixel reads outside the row resolved with AGO's buffer layout); rows 0 and H-1
  * are written 0 (the reference never writes them).  src/dst 16-byte aligned, strides
  * multiples of 16.  Replaces HafCpu_ScaleGaussianHalf_U8_U8_5x5 (ago_haf_cpu_pyramid.cpp:94)
- * as agoKernel_ScaleGaussianHalf_U8_U8_5x5 calls it (ago_kernel_api.cpp:15420); the HIP
- * target has no 5x5 launcher. */
+ * as agoKernel_ScaleGaussianHalf_U8_U8_5x5 calls it (ago_kernel_api.cpp:15420), and
+ * HipExec_ScaleGaussianHalf_U8_U8_5x5 (hipvx/hip_host_decls.h:681). */
 int agocuda_ScaleGaussianHalf_U8_U8_5x5(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
                                         uint32_t dstStride, uint32_t srcWidth, uint32_t srcHeight,
                                         const uint8_t *pSrc, uint32_t srcStride);

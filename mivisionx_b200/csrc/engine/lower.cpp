@@ -28,6 +28,7 @@ static const char *kLKNames[] = {
     "WarpAffine_U8_U8_Bilinear_Constant", "WarpPerspective_U8_U8_Nearest_Constant",
     "WarpPerspective_U8_U8_Bilinear_Constant", "Remap_U8_U8_Nearest_Constant", "Remap_U8_U8_Bilinear_Constant",
     "ScaleGaussianHalf_U8_U8_5x5", "OpticalFlowPyrLK_XY_XY",
+    "WarpPerspective_U8_U8_Nearest", "WarpPerspective_U8_U8_Bilinear", "Remap_U8_U8_Nearest", "Remap_U8_U8_Bilinear",
 };
 static_assert(sizeof(kLKNames) / sizeof(kLKNames[0]) == (size_t)LK::COUNT, "kernel name table");
 
@@ -297,18 +298,25 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
             LK k = aff ? (t == VX_INTERPOLATION_BILINEAR ? LK::WARP_AFFINE_U8_U8_BILINEAR_CONSTANT : LK::WARP_AFFINE_U8_U8_NEAREST_CONSTANT)
                        : (t == VX_INTERPOLATION_BILINEAR ? LK::WARP_PERSPECTIVE_U8_U8_BILINEAR_CONSTANT : LK::WARP_PERSPECTIVE_U8_U8_NEAREST_CONSTANT);
             add(k, {p[3], p[0], p[1], b});
-        } else if (n->border.mode == VX_BORDER_UNDEFINED && aff) {
-            add(t == VX_INTERPOLATION_BILINEAR ? LK::WARP_AFFINE_U8_U8_BILINEAR : LK::WARP_AFFINE_U8_U8_NEAREST, {p[3], p[0], p[1]});
+        } else if (n->border.mode == VX_BORDER_UNDEFINED) {
+            LK k = aff ? (t == VX_INTERPOLATION_BILINEAR ? LK::WARP_AFFINE_U8_U8_BILINEAR : LK::WARP_AFFINE_U8_U8_NEAREST)
+                       : (t == VX_INTERPOLATION_BILINEAR ? LK::WARP_PERSPECTIVE_U8_U8_BILINEAR : LK::WARP_PERSPECTIVE_U8_U8_NEAREST);
+            add(k, {p[3], p[0], p[1]});
         } else {
             return VX_ERROR_NOT_SUPPORTED;
         }
         return VX_SUCCESS;
     }
-    case VX_KERNEL_REMAP: {
-        Scalar *b = virt_scalar(g, VX_TYPE_UINT8, n->border.constant_value.U8);
-        if (n->border.mode == VX_BORDER_REPLICATE) return VX_ERROR_NOT_SUPPORTED;
-        add(sc_enum(p[2]) == VX_INTERPOLATION_BILINEAR ? LK::REMAP_U8_U8_BILINEAR_CONSTANT : LK::REMAP_U8_U8_NEAREST_CONSTANT,
-            {p[3], p[0], p[1], b});
+    case VX_KERNEL_REMAP: {                                                                            // :1490
+        const bool bl = sc_enum(p[2]) == VX_INTERPOLATION_BILINEAR;
+        if (n->border.mode == VX_BORDER_CONSTANT) {
+            Scalar *b = virt_scalar(g, VX_TYPE_UINT8, n->border.constant_value.U8);
+            add(bl ? LK::REMAP_U8_U8_BILINEAR_CONSTANT : LK::REMAP_U8_U8_NEAREST_CONSTANT, {p[3], p[0], p[1], b});
+        } else if (n->border.mode == VX_BORDER_UNDEFINED) {
+            add(bl ? LK::REMAP_U8_U8_BILINEAR : LK::REMAP_U8_U8_NEAREST, {p[3], p[0], p[1]});
+        } else {
+            return VX_ERROR_NOT_SUPPORTED;
+        }
         return VX_SUCCESS;
     }
     case VX_KERNEL_GAUSSIAN_PYRAMID: {                                                                 // :900

@@ -69,6 +69,33 @@ static float harris_norm(int32_t gs)
 }
 
 // ------------------------------------------------------------------------------------
+// The remap table the reference kernels read: vxSetRemapPoint (api/vx_api.cpp:7884) stores
+// each float source point as u16 fixed point, (u16)(v * 2^bits + 0.5f) in float, with
+// ago_util.cpp:2451's fractional bits, and 0xFFFF in both coordinates for a point outside
+// [0, W-1) x [0, H-1).  One uint32 per destination pixel: x | y << 16.
+// ------------------------------------------------------------------------------------
+static std::vector<uint32_t> remap_fixed_table(const Remap *r)
+{
+    int bits = 3;
+    if (r->src_width >= (1u << 15) || r->src_height >= (1u << 15)) bits = 0;
+    else if (r->src_width >= (1u << 14) || r->src_height >= (1u << 14)) bits = 1;
+    else if (r->src_width >= (1u << 13) || r->src_height >= (1u << 13)) bits = 2;
+    const float sc = (float)(1 << bits), wl = (float)(r->src_width - 1), hl = (float)(r->src_height - 1);
+    // float -> u16 as x86 converts it: to int32 with truncation (0x80000000 when out of range)
+    auto to_u16 = [](float v) -> uint32_t {
+        const int32_t i = (v >= -2147483648.0f && v < 2147483648.0f) ? (int32_t)v : INT32_MIN;
+        return (uint32_t)i & 0xFFFF;
+    };
+    std::vector<uint32_t> out(r->table.size());
+    for (size_t k = 0; k < out.size(); k++) {
+        const float sx = r->table[k].x, sy = r->table[k].y;
+        if (sx < 0.0f || sy < 0.0f || sx >= wl || sy >= hl) out[k] = 0xFFFFFFFFu;
+        else out[k] = to_u16(sx * sc + 0.5f) | (to_u16(sy * sc + 0.5f) << 16);
+    }
+    return out;
+}
+
+// ------------------------------------------------------------------------------------
 // pyramidal LK: device descriptors of OPTICAL_FLOW_PYR_LK_XY_XY nodes
 // (AGO order: new points, old pyramid, new pyramid, old points, estimates, termination,
 //  epsilon, num_iterations, use_initial_estimate, window_dimension)
@@ -331,6 +358,48 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         st.num_kernels = 0;   // a copy-engine transfer, not a kernel
         st.launch = [=](cudaStream_t q) {
             return cudaMemcpy2DAsync(d, ds, s, ss, w, h, cudaMemcpyDeviceToDevice, q) == cudaSuccess ? 0 : -1;
+        };
+        return VX_SUCCESS;
+    }
+    case LK::WARP_PERSPECTIVE_U8_U8_NEAREST_CONSTANT: case LK::WARP_PERSPECTIVE_U8_U8_BILINEAR_CONSTANT:
+    case LK::WARP_PERSPECTIVE_U8_U8_NEAREST: case LK::WARP_PERSPECTIVE_U8_U8_BILINEAR: {
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        const uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), sw = W(p[1]), sh = H(p[1]), ss = dstride(p[1]);
+        std::array<float, 9> mat;
+        memcpy(mat.data(), static_cast<Matrix *>(p[2])->data.data(), sizeof(float) * 9);
+        // the undefined-border kernels are the constant ones with border 0 (geometric.cpp:1372, :1560)
+        const bool cst = ln.k == LK::WARP_PERSPECTIVE_U8_U8_NEAREST_CONSTANT || ln.k == LK::WARP_PERSPECTIVE_U8_U8_BILINEAR_CONSTANT;
+        const uint8_t border = cst ? static_cast<Scalar *>(p[3])->v.u8 : 0;
+        const bool bl = ln.k == LK::WARP_PERSPECTIVE_U8_U8_BILINEAR_CONSTANT || ln.k == LK::WARP_PERSPECTIVE_U8_U8_BILINEAR;
+        st.launch = [=](cudaStream_t q) {
+            return bl ? agocuda_WarpPerspective_U8_U8_Bilinear_Constant(S(q), w, h, d, ds, sw, sh, s, ss, mat.data(), border)
+                      : agocuda_WarpPerspective_U8_U8_Nearest_Constant(S(q), w, h, d, ds, sw, sh, s, ss, mat.data(), border);
+        };
+        return VX_SUCCESS;
+    }
+    case LK::REMAP_U8_U8_NEAREST_CONSTANT: case LK::REMAP_U8_U8_BILINEAR_CONSTANT:
+    case LK::REMAP_U8_U8_NEAREST: case LK::REMAP_U8_U8_BILINEAR: {
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        const uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), sw = W(p[1]), sh = H(p[1]), ss = dstride(p[1]);
+        const Remap *r = static_cast<Remap *>(p[2]);
+        const std::vector<uint32_t> fixed = remap_fixed_table(r);
+        void *map = scratch(g, fixed.size() * sizeof(uint32_t));
+        if (!map) return VX_ERROR_NO_MEMORY;
+        if (cudaMemcpy(map, fixed.data(), fixed.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+            return VX_FAILURE;
+        const uint32_t ms = r->dst_width * 4;
+        const LK k = ln.k;
+        const uint8_t border = (k == LK::REMAP_U8_U8_NEAREST_CONSTANT || k == LK::REMAP_U8_U8_BILINEAR_CONSTANT)
+                                   ? static_cast<Scalar *>(p[3])->v.u8 : 0;
+        const uint32_t *m = (const uint32_t *)map;
+        st.launch = [=](cudaStream_t q) {
+            switch (k) {
+            case LK::REMAP_U8_U8_NEAREST: return agocuda_Remap_U8_U8_Nearest(S(q), w, h, d, ds, sw, sh, s, ss, m, ms);
+            case LK::REMAP_U8_U8_BILINEAR: return agocuda_Remap_U8_U8_Bilinear(S(q), w, h, d, ds, sw, sh, s, ss, m, ms);
+            case LK::REMAP_U8_U8_NEAREST_CONSTANT:
+                return agocuda_Remap_U8_U8_Nearest_Constant(S(q), w, h, d, ds, sw, sh, s, ss, m, ms, border);
+            default: return agocuda_Remap_U8_U8_Bilinear_Constant(S(q), w, h, d, ds, sw, sh, s, ss, m, ms, border);
+            }
         };
         return VX_SUCCESS;
     }

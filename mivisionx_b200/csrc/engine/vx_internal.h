@@ -174,6 +174,7 @@ enum class LK : int {
     WARP_AFFINE_U8_U8_BILINEAR_CONSTANT, WARP_PERSPECTIVE_U8_U8_NEAREST_CONSTANT,
     WARP_PERSPECTIVE_U8_U8_BILINEAR_CONSTANT, REMAP_U8_U8_NEAREST_CONSTANT, REMAP_U8_U8_BILINEAR_CONSTANT,
     SCALE_GAUSSIAN_HALF_U8_U8_5x5, OPTICAL_FLOW_PYR_LK_XY_XY,
+    WARP_PERSPECTIVE_U8_U8_NEAREST, WARP_PERSPECTIVE_U8_U8_BILINEAR, REMAP_U8_U8_NEAREST, REMAP_U8_U8_BILINEAR,
     COUNT
 };
 const char *lk_name(LK k);

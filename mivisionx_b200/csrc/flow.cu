@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kHalfThreads) k_gauss_half(const agocuda_half_
         const uint32_t mid = (lo + hi + 1) >> 1;
         if (jobs[mid].tileBegin <= t) lo = mid; else hi = mid - 1;
     }
-    const agocuda_half_job &J = jobs[lo];
+    const agocuda_half_job J = jobs[lo];               // by value: dst stores may alias a reference
     const uint32_t local = t - J.tileBegin;
     const uint32_t tilesX = (J.dstW + kHalfCols - 1) / kHalfCols;
     const int ox = (int)(local % tilesX) * kHalfCols + 8 * (int)threadIdx.x;
@@ -173,6 +173,8 @@ __global__ void __launch_bounds__(kHalfThreads) k_gauss_half_one(const agocuda_h
 constexpr int kLkWarps = 8;
 constexpr int kWin = AGOCUDA_LK_MAX_WINDOW;
 constexpr int kWBits = 14;
+constexpr int kPatchPerLane = ((kWin + 3) * (kWin + 3) + 31) / 32;   // image patch bytes per lane
+constexpr int kJPerLane = ((kWin + 1) * (kWin + 1) + 31) / 32;       // J window bytes per lane
 constexpr float kFltScale = 1.f / (1 << 20);
 constexpr int kTermEpsilon = 0xF001, kTermBoth = 0xF002;   // VX_TERM_CRITERIA_EPSILON / _BOTH
 
@@ -261,9 +263,17 @@ __device__ void lk_track_point(const agocuda_lk_frame &F, uint32_t pt, LkWarpSme
 
         // ---- image patch rows ipy-1 .. ipy+win+1, cols ipx-1 .. ipx+win+1
         const int P = win + 3, Q = win + 1;
-        for (int i = lane; i < P * P; i += 32) {
-            const int r = ipy - 1 + i / P, c = ipx - 1 + i % P;
-            S.u.s.img[i] = (r >= 0 && c >= 0) ? LI.image[(size_t)r * LI.stride + c] : 0;
+        __syncwarp();
+        {
+            uint8_t v[kPatchPerLane];
+#pragma unroll
+            for (int k = 0; k < kPatchPerLane; k++) {
+                const int i = lane + 32 * k, r = ipy - 1 + i / P, c = ipx - 1 + i % P;
+                v[k] = (i < P * P && r >= 0 && c >= 0) ? LI.image[(size_t)r * LI.stride + c] : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < kPatchPerLane; k++)
+                if (lane + 32 * k < P * P) S.u.s.img[lane + 32 * k] = v[k];
         }
         __syncwarp();
         // ---- Scharr (gx, gy) at window positions (ipy + y, ipx + x), y, x in [0, win]
@@ -382,6 +392,7 @@ __device__ void lk_track_point(const agocuda_lk_frame &F, uint32_t pt, LkWarpSme
 
         // ---- Gauss-Newton iterations
         float prevDx = 0.f, prevDy = 0.f, ddx = 0.f, ddy = 0.f;
+        int jx = INT32_MIN, jy = INT32_MIN;               // integer position of the staged J window
         const bool epsOnly = F.termination == kTermEpsilon;
         const bool epsTest = epsOnly || F.termination == kTermBoth;
         for (unsigned j = 0; j < F.numIterations || (epsOnly && j < AGOCUDA_LK_EPSILON_ONLY_MAX_ITERATIONS);) {
@@ -395,8 +406,19 @@ __device__ void lk_track_point(const agocuda_lk_frame &F, uint32_t pt, LkWarpSme
             b = __fsub_rn(ny, (float)iny);
             lk_weights(a, b, w);
             __syncwarp();
-            for (int i = lane; i < Q * Q; i += 32)
-                S.u.it.J[i] = LJ.image[(size_t)(iny + i / Q) * LJ.stride + inx + i % Q];
+            if (inx != jx || iny != jy) {                 // the J window only moves with the integer position
+                uint8_t v[kJPerLane];
+#pragma unroll
+                for (int k = 0; k < kJPerLane; k++) {
+                    const int i = lane + 32 * k;
+                    v[k] = i < Q * Q ? LJ.image[(size_t)(iny + i / Q) * LJ.stride + inx + i % Q] : 0;
+                }
+#pragma unroll
+                for (int k = 0; k < kJPerLane; k++)
+                    if (lane + 32 * k < Q * Q) S.u.it.J[lane + 32 * k] = v[k];
+                jx = inx;
+                jy = iny;
+            }
             __syncwarp();
             for (int p = lane; p < win * win; p += 32) {
                 const int y = p / win, x = p % win;

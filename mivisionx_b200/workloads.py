@@ -389,3 +389,50 @@ class Cfg4Graph:
 
     def results(self):
         return [self.api.array_items(o) for o in self.out]
+
+
+class WarpRemapGraph:
+    """WarpPerspective (bilinear, border CONSTANT `border`; nearest, border UNDEFINED) and
+    Remap (bilinear, border CONSTANT `border`; nearest, border UNDEFINED) of one U8 image
+    into four non-virtual outputs.  `matrix` is the 3x3 vx_matrix data; `table` the
+    (dst_h, dst_w, 2) float source coordinates of the remap."""
+
+    def __init__(self, api: V.OpenVX, ctx, size, matrix, table, src_size=None, border=0, flags: int | None = None):
+        a = api
+        self.api, self.ctx = api, ctx
+        W, H = size
+        sW, sH = src_size or size
+        dH, dW = table.shape[:2]
+        self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
+        if flags is not None:
+            a.set_optimizer_flags(self.graph, flags)
+        self.src = a.obj(a.vxCreateImage(ctx, sW, sH, V.VX_DF_IMAGE_U8), "image")
+        self.mat = a.matrix_f32(ctx, np.asarray(matrix, np.float32).reshape(3, 3))
+        self.remap = a.obj(a.vxCreateRemap(ctx, sW, sH, dW, dH), "remap")
+        t = np.ascontiguousarray(table, np.float32)
+        rect = V.vx_rectangle_t(0, 0, dW, dH)
+        a.ok(a.vxCopyRemapPatch(self.remap, C.byref(rect), dW * 8, t.ctypes.data, V.VX_TYPE_COORDINATES2DF,
+                                V.VX_WRITE_ONLY, V.VX_MEMORY_TYPE_HOST), "vxCopyRemapPatch")
+        self.outs = {}
+        g = self.graph
+        for name, bl, const, kind in (("persp_bilinear_constant", True, True, "p"), ("persp_nearest", False, False, "p"),
+                                      ("remap_bilinear_constant", True, True, "r"), ("remap_nearest", False, False, "r")):
+            ow, oh = (W, H) if kind == "p" else (dW, dH)
+            out = a.obj(a.vxCreateImage(ctx, ow, oh, V.VX_DF_IMAGE_U8), "image")
+            interp = V.VX_INTERPOLATION_BILINEAR if bl else V.VX_INTERPOLATION_NEAREST_NEIGHBOR
+            if kind == "p":
+                node = a.obj(a.vxWarpPerspectiveNode(g, self.src, self.mat, interp, out), "warp node")
+            else:
+                node = a.obj(a.vxRemapNode(g, self.src, self.remap, interp, out), "remap node")
+            if const:
+                a.set_border(node, V.VX_BORDER_CONSTANT, border)
+            self.outs[name] = out
+        a.ok(a.vxVerifyGraph(g), "vxVerifyGraph")
+
+    def run(self, frame=None):
+        if frame is not None:
+            self.api.write_plane(self.src, frame)
+        self.api.ok(self.api.vxProcessGraph(self.graph), "vxProcessGraph")
+
+    def results(self):
+        return {k: (self.api.read_plane(v), self.api.valid_region(v)) for k, v in self.outs.items()}

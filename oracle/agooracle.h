@@ -85,6 +85,26 @@ int oracle_WarpAffine_U8_U8_Bilinear_Constant(uint32_t W, uint32_t H, uint8_t *p
                                               uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride, const float *m,
                                               uint8_t border);
 
+/* ---- WarpPerspective (m = ago_perspective_matrix_t, 9 floats) and Remap (u16 fixed-point
+ *      table of (x, y) pairs, mapStride bytes per row), agooracle_geometry.c ---- */
+int oracle_WarpPerspective_U8_U8_Nearest_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                                  uint32_t srcW, uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride,
+                                                  const float *m, uint8_t border);
+int oracle_WarpPerspective_U8_U8_Bilinear_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                                   uint32_t srcW, uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride,
+                                                   const float *m, uint8_t border);
+void oracle_remap_fixed(uint32_t srcW, uint32_t srcH, const float *xy, size_t n, uint16_t *out);
+int oracle_Remap_U8_U8_Bilinear_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW,
+                                         uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride, const uint16_t *pMap,
+                                         uint32_t mapStride, uint8_t border);
+int oracle_Remap_U8_U8_Bilinear(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW, uint32_t srcH,
+                                const uint8_t *pSrc, uint32_t srcStride, const uint16_t *pMap, uint32_t mapStride);
+int oracle_Remap_U8_U8_Nearest_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW,
+                                        uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride, const uint16_t *pMap,
+                                        uint32_t mapStride, uint8_t border);
+int oracle_Remap_U8_U8_Nearest(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW, uint32_t srcH,
+                               const uint8_t *pSrc, uint32_t srcStride, const uint16_t *pMap, uint32_t mapStride);
+
 /* ---- pyramid level and pyramidal LK (ago_haf_cpu_pyramid.cpp, ago_haf_cpu_opticalflow.cpp),
  *      agooracle_flow.c ---- */
 typedef struct {          /* ago_pyramid_u8_t (ago_haf_cpu.h:75) */

@@ -290,3 +290,190 @@ int oracle_WarpAffine_U8_U8_Bilinear_Constant(uint32_t W, uint32_t H, uint8_t *p
     }
     return 0;
 }
+
+/* ---------------------------------------------------------------- WarpPerspective */
+/* _mm_cvttps_epi32: truncation, 0x80000000 for NaN and values outside int32 */
+static int32_t cvtt_i32(float f)
+{
+    return (f >= -2147483648.0f && f < 2147483648.0f) ? (int32_t)f : INT32_MIN;
+}
+/* _mm_packus_epi32 then _mm_packus_epi16 of one lane */
+static uint8_t pack_u8(int32_t v)
+{
+    const int32_t u16 = v < 0 ? 0 : (v > 65535 ? 65535 : v);
+    const int16_t s16 = (int16_t)(uint16_t)u16;
+    return (uint8_t)(s16 < 0 ? 0 : (s16 > 255 ? 255 : s16));
+}
+
+/* ago_haf_cpu_geometric.cpp:1406 HafCpu_WarpPerspective_U8_U8_Nearest_Constant.  m is
+ * ago_perspective_matrix_t (float[3][3]); per column a*x, d*x, g*x in float, per row
+ * y*b + c, y*e + f, y*h + i; x' = (a*x + (y*b + c)) * (1 / (g*x + (y*h + i))).  In range
+ * (0 <= x' < W, 0 <= y' < H, float compares): pixel (trunc x', trunc y'), else border.
+ * The UNDEFINED-border kernel (:1372) is this with border 0. */
+int oracle_WarpPerspective_U8_U8_Nearest_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                                  uint32_t srcW, uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride,
+                                                  const float *m, uint8_t border)
+{
+    const float a = m[0], d = m[1], g = m[2], b = m[3], e = m[4], h = m[5], c = m[6], f = m[7], i = m[8];
+    const int32_t srcb = (int32_t)(srcH * srcStride - 1);
+    for (uint32_t y = 0; y < H; y++) {
+        const float xd = (float)y * b + c, yd = (float)y * e + f, zd = (float)y * h + i;
+        for (uint32_t x = 0; x < W; x++) {
+            const float z = 1.0f / ((g * (float)x) + zd);
+            const float xm = ((a * (float)x) + xd) * z, ym = ((d * (float)x) + yd) * z;
+            const int ok = xm >= 0.f && xm < (float)srcW && ym >= 0.f && ym < (float)srcH;
+            int32_t off = (int32_t)((uint32_t)cvtt_i32(ym) * srcStride + (uint32_t)cvtt_i32(xm));
+            off = off > srcb ? srcb : (off < 0 ? 0 : off);
+            pDst[(size_t)y * dstStride + x] = ok ? pSrc[off] : border;
+        }
+    }
+    return 0;
+}
+
+/* ago_haf_cpu_geometric.cpp:1579 HafCpu_WarpPerspective_U8_U8_Bilinear_Constant.  Integer
+ * position trunc(x') - (x' < 0); taps p0 (x, y) and p2 (x, y+1) are the border unless
+ * 0 <= x < W and 0 <= y < H, taps p1 (x+1, y) and p3 (x+1, y+1) unless -1 <= x < W and
+ * -1 <= y < H; the four bytes come from the flat offset y*stride + x clamped to
+ * [0, H*stride - 1] (and the next row).  ((p0*(1-fx))*(1-fy) + (p1*fx)*(1-fy)) +
+ * (p2*(1-fx))*fy + (p3*fx)*fy summed left to right, truncated, saturated. */
+int oracle_WarpPerspective_U8_U8_Bilinear_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
+                                                   uint32_t srcW, uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride,
+                                                   const float *m, uint8_t border)
+{
+    const float a = m[0], d = m[1], g = m[2], b = m[3], e = m[4], h = m[5], c = m[6], f = m[7], i = m[8];
+    const int32_t srcb = (int32_t)(srcH * srcStride - 1);
+    for (uint32_t y = 0; y < H; y++) {
+        const float xd = (float)y * b + c, yd = (float)y * e + f, zd = (float)y * h + i;
+        for (uint32_t x = 0; x < W; x++) {
+            const float z = 1.0f / ((g * (float)x) + zd);
+            const float xm = ((a * (float)x) + xd) * z, ym = ((d * (float)x) + yd) * z;
+            const int32_t xi = (int32_t)((uint32_t)cvtt_i32(xm) - (uint32_t)(xm < 0.f));
+            const int32_t yi = (int32_t)((uint32_t)cvtt_i32(ym) - (uint32_t)(ym < 0.f));
+            const int ok = xi >= 0 && xi < (int32_t)srcW && yi >= 0 && yi < (int32_t)srcH;
+            const int ok1 = xi >= -1 && xi < (int32_t)srcW && yi >= -1 && yi < (int32_t)srcH;
+            const float fx = xm - (float)xi, fy = ym - (float)yi;
+            int32_t off = (int32_t)((uint32_t)yi * srcStride + (uint32_t)xi);
+            off = off > srcb ? srcb : (off < 0 ? 0 : off);
+            const uint8_t *p = pSrc + off;
+            const float p0 = ok ? p[0] : border, p2 = ok ? p[srcStride] : border;
+            const float p1 = ok1 ? p[1] : border, p3 = ok1 ? p[srcStride + 1] : border;
+            const float omx = 1.0f - fx, omy = 1.0f - fy;
+            const float s0 = (p0 * omx) * omy, s1 = (p1 * fx) * omy, s2 = (p2 * omx) * fy, s3 = (p3 * fx) * fy;
+            pDst[(size_t)y * dstStride + x] = pack_u8(cvtt_i32(((s0 + s1) + s2) + s3));
+        }
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------- Remap */
+/* vxSetRemapPoint (api/vx_api.cpp:7884): the table AGO's kernels read holds u16 fixed-point
+ * coordinates with ago_util.cpp:2451's fractional bits (3 below 8192 pixels), rounded with
+ * + 0.5f in float; a source point outside [0, W-1) x [0, H-1) stores 0xFFFF in both. */
+void oracle_remap_fixed(uint32_t srcW, uint32_t srcH, const float *xy, size_t n, uint16_t *out)
+{
+    int bits = 3;
+    if (srcW >= (1u << 15) || srcH >= (1u << 15)) bits = 0;
+    else if (srcW >= (1u << 14) || srcH >= (1u << 14)) bits = 1;
+    else if (srcW >= (1u << 13) || srcH >= (1u << 13)) bits = 2;
+    const float s = (float)(1 << bits);
+    for (size_t k = 0; k < n; k++) {
+        const float sx = xy[2 * k], sy = xy[2 * k + 1];
+        if (sx < 0.0f || sy < 0.0f || sx >= (float)(srcW - 1) || sy >= (float)(srcH - 1)) {
+            out[2 * k] = out[2 * k + 1] = 0xFFFF;
+        } else {
+            out[2 * k] = (uint16_t)(uint32_t)cvtt_i32(sx * s + 0.5f);
+            out[2 * k + 1] = (uint16_t)(uint32_t)cvtt_i32(sy * s + 0.5f);
+        }
+    }
+}
+
+/* ago_haf_cpu_geometric.cpp:372 / :249 HafCpu_Remap_U8_U8_Bilinear[_Constant]: 3 fractional
+ * bits, weights (8-fx)(8-fy), fx(8-fy), (8-fx)fy, fx*fy, (sum + 32) >> 6.  A 0xFFFF x or y
+ * is read as 0 (constant) or 8 (undefined); with a constant border only a 0xFFFF x gives the
+ * border value (the mask is applied per 16-bit half of the 32-bit result). */
+static void remap_bilinear(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, const uint8_t *pSrc,
+                           uint32_t srcStride, const uint16_t *pMap, uint32_t mapStride, int constant, uint8_t border)
+{
+    for (uint32_t y = 0; y < H; y++) {
+        const uint16_t *mr = (const uint16_t *)((const uint8_t *)pMap + (size_t)y * mapStride);
+        for (uint32_t x = 0; x < W; x++) {
+            uint32_t mx = mr[2 * x], my = mr[2 * x + 1];
+            const int bx = mx == 0xFFFF, by = my == 0xFFFF;
+            if (bx) mx = constant ? 0 : 8;
+            if (by) my = constant ? 0 : 8;
+            const uint32_t fx = mx & 7, fy = my & 7;
+            const uint8_t *p = pSrc + (size_t)(my >> 3) * srcStride + (mx >> 3);
+            const uint32_t v = (p[0] * (8 - fx) * (8 - fy) + p[1] * fx * (8 - fy) + p[srcStride] * (8 - fx) * fy +
+                                p[srcStride + 1] * fx * fy + 32) >> 6;
+            pDst[(size_t)y * dstStride + x] = (constant && bx) ? border : pack_u8((int32_t)v);
+        }
+    }
+}
+
+int oracle_Remap_U8_U8_Bilinear_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW,
+                                         uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride, const uint16_t *pMap,
+                                         uint32_t mapStride, uint8_t border)
+{
+    (void)srcW; (void)srcH;
+    remap_bilinear(W, H, pDst, dstStride, pSrc, srcStride, pMap, mapStride, 1, border);
+    return 0;
+}
+
+int oracle_Remap_U8_U8_Bilinear(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW, uint32_t srcH,
+                                const uint8_t *pSrc, uint32_t srcStride, const uint16_t *pMap, uint32_t mapStride)
+{
+    (void)srcW; (void)srcH;
+    remap_bilinear(W, H, pDst, dstStride, pSrc, srcStride, pMap, mapStride, 0, 0);
+    return 0;
+}
+
+/* ago_haf_cpu_geometric.cpp:156 / :72 HafCpu_Remap_U8_U8_Nearest[_Constant]: position
+ * (v >> 3) + (frac > 3).  The 4-pixel SIMD body (x < W & ~3) reads a 0xFFFF coordinate as 0
+ * and emits the border for it (or for a flat offset past the image) with a constant border,
+ * and as 7 (position 1) without one; the scalar tail (x >= W & ~3) replaces a 0xFFFF
+ * coordinate by the border value (constant) or 0 (undefined) and reads that position.
+ * Tail reads outside the source buffer read 0 here (the reference reads past its buffer). */
+static void remap_nearest(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcH, const uint8_t *pSrc,
+                          uint32_t srcStride, const uint16_t *pMap, uint32_t mapStride, int constant, uint8_t border)
+{
+    const int32_t srcb = (int32_t)(srcH * srcStride - 1);
+    const uint32_t W4 = W & ~3u;
+    for (uint32_t y = 0; y < H; y++) {
+        const uint16_t *mr = (const uint16_t *)((const uint8_t *)pMap + (size_t)y * mapStride);
+        uint8_t *d = pDst + (size_t)y * dstStride;
+        for (uint32_t x = 0; x < W4; x++) {
+            uint32_t mx = mr[2 * x], my = mr[2 * x + 1];
+            const int bx = mx == 0xFFFF, by = my == 0xFFFF;
+            if (bx) mx = constant ? 0 : 7;
+            if (by) my = constant ? 0 : 7;
+            const int32_t ix = (int32_t)(mx >> 3) + ((mx & 7) > 3), iy = (int32_t)(my >> 3) + ((my & 7) > 3);
+            const int32_t off = (int32_t)((uint32_t)iy * srcStride + (uint32_t)ix);
+            if (constant && (bx || by || off > srcb)) d[x] = border;
+            else d[x] = pSrc[off];
+        }
+        for (uint32_t x = W4; x < W; x++) {
+            const int16_t sx = (int16_t)mr[2 * x], sy = (int16_t)mr[2 * x + 1];
+            const int xx = sx != -1 ? (sx >> 3) + ((sx & 7) >> 2) : (constant ? border : 0);
+            const int yy = sy != -1 ? (sy >> 3) + ((sy & 7) >> 2) : (constant ? border : 0);
+            const long off = (long)yy * srcStride + xx;
+            d[x] = (off >= 0 && off <= srcb) ? pSrc[off] : 0;
+        }
+    }
+}
+
+int oracle_Remap_U8_U8_Nearest_Constant(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW,
+                                        uint32_t srcH, const uint8_t *pSrc, uint32_t srcStride, const uint16_t *pMap,
+                                        uint32_t mapStride, uint8_t border)
+{
+    (void)srcW;
+    remap_nearest(W, H, pDst, dstStride, srcH, pSrc, srcStride, pMap, mapStride, 1, border);
+    return 0;
+}
+
+int oracle_Remap_U8_U8_Nearest(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, uint32_t srcW, uint32_t srcH,
+                               const uint8_t *pSrc, uint32_t srcStride, const uint16_t *pMap, uint32_t mapStride)
+{
+    (void)srcW;
+    remap_nearest(W, H, pDst, dstStride, srcH, pSrc, srcStride, pMap, mapStride, 0, 0);
+    return 0;
+}
