@@ -444,19 +444,183 @@ def run_ours(a, wl_name):
     return 0
 
 
+# ------------------------------------------------------------------------------------------
+# Differentiable F32 WarpAffine: one step = warp + L2 loss + adjoint for a batch of images
+# (the fused kernel of mivisionx_b200.diffwarp).  No OpenVX graph: the reference has no F32
+# warp, so its CPU leg is the FP64 port (oracle/diffwarp_f64.py).
+# ------------------------------------------------------------------------------------------
+DIFFWARP = "diffwarp_affine_32x1024"
+DIFFWARP_DESC = ("F32 bilinear WarpAffine (border CONSTANT 0) + L2 loss to the image warped by the ground truth + "
+                 "adjoint (d/dsrc, d/dtheta) in one pass; 32 images 1024x1024, uniform [0,1] smoothed by a Gaussian "
+                 "(sigma 2); theta = seeded estimate (GT rotation +-10 deg, scale 0.9-1.1, shift +-20 px, perturbed by "
+                 "+-2 deg, +-0.02, +-3 px)")
+
+
+def _diffwarp_inputs(n, size):
+    import numpy as np
+
+    from mivisionx_b200 import workloads as WL
+    imgs = WL.cfg5_images(n, size=size)
+    gt, init = WL.cfg5_params(n, size=size)
+    return imgs, gt.astype(np.float32), init.astype(np.float32)
+
+
+def _diffwarp_cpu(seconds, size=1024):
+    """FP64 port on one host core: warp + loss + adjoint of one image, repeated for ~seconds."""
+    from oracle import diffwarp_f64 as D
+    imgs, gt, init = _diffwarp_inputs(1, size)
+    img = imgs[0].astype("float64")
+    tgt = D.warp_affine(img, gt[0].astype("float64"))
+    n, t0 = 0, time.perf_counter()
+    while n == 0 or time.perf_counter() - t0 < seconds:
+        out = D.warp_affine(img, init[0].astype("float64"))
+        D.warp_affine_adjoint(img, init[0].astype("float64"), 2 * (out - tgt))
+        n += 1
+    dt = time.perf_counter() - t0
+    return n * size * size / dt / 1e6, dt, n
+
+
+def run_diffwarp(a):
+    import numpy as np
+    import torch
+
+    from mivisionx_b200 import diffwarp, native
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    N, S = a.frames or 32, 1024
+    imgs, gt, init = _diffwarp_inputs(N, S)
+    d_img = torch.from_numpy(imgs).cuda()
+    d_gt, d_th = torch.from_numpy(gt).cuda(), torch.from_numpy(init).cuda()
+    d_tgt = diffwarp.warp_affine(d_img, d_gt)            # target: the image warped by the ground truth
+    gsrc = torch.zeros_like(d_img)
+    acc = torch.zeros((N, 7), dtype=torch.float64, device="cuda")
+    lib = native.agocuda()
+    stream = torch.cuda.current_stream()
+
+    def step():
+        diffwarp.warp_affine_l2_step(d_img, d_th, d_tgt, gsrc=gsrc, acc=acc)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    _barrier(ws)
+    n0 = lib.agocuda_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = lib.agocuda_launch_count() - n0
+    ms_step = _max_over_ranks(e0.elapsed_time(e1) / a.steps, ws)
+    px = N * S * S
+    value = px * ws / (ms_step / 1e3) / 1e6
+
+    # end to end: images, targets and theta from pinned host memory, loss + theta gradients back
+    h_img = torch.from_numpy(imgs).pin_memory()
+    h_tgt = d_tgt.cpu().pin_memory()
+    h_th = torch.from_numpy(init).pin_memory()
+    h_out = torch.empty((N, 7), dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        d_img.copy_(h_img, non_blocking=True)
+        d_tgt.copy_(h_tgt, non_blocking=True)
+        d_th.copy_(h_th, non_blocking=True)
+        step()
+        h_out.copy_(acc, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(a.warmup):
+        e2e_step()
+    _barrier(ws)
+    e0.record(stream)
+    for _ in range(a.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = _max_over_ranks(e0.elapsed_time(e1) / a.steps, ws)
+    peak, peak_kind = _peaks()
+    alg_bytes = 12.0 * px           # read src + target, write d/dsrc (4 B each per pixel)
+    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not a.no_cpu_baseline:
+            v, dt, n = _diffwarp_cpu(a.cpu_seconds)
+            cpu = {"value": round(v, 2), "unit": "Mpixels/s", "cores": 1, "kind": "port",
+                   "sample": f"{n} x warp + loss + adjoint of one 1024x1024 image in FP64 numpy ({dt:.1f} s, 1 core); "
+                             "the reference has no F32 warp"}
+        print(json.dumps({
+            "metric": "Mpixels/s per vision graph", "value": round(value, 1), "unit": "Mpixels/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32)",
+            "config": {"workload": DIFFWARP, "graph": DIFFWARP_DESC, "images_per_step_per_gpu": N, "image": f"{S}x{S}",
+                       "l2": "inputs (128 MB src + 128 MB target) exceed the 126 MB L2 (no flush needed)",
+                       "parallelism": f"replicas x{ws} (images sharded, no collective)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg_bytes, "kernel": "k_warp_affine_f32<fused L2>, 1 launch per step"},
+            "e2e": {"value": round(px * ws / (e2e_ms / 1e3) / 1e6, 1), "unit": "Mpixels/s",
+                    "h2d_bytes_per_step": 2 * 4 * px + N * 6 * 4, "d2h_bytes_per_step": N * 7 * 8},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_diffwarp_reference(a):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    per_step = max(0.5, min(3.0, 120.0 / max(1, a.steps + a.warmup)))
+    vals = []
+    with mp.get_context("spawn").Pool(cores) as pool:
+        for s in range(a.warmup + a.steps):
+            r = pool.map(_diffwarp_cpu, [per_step] * cores)
+            if s >= a.warmup:
+                vals.append(sum(v for v, _, _ in r))
+    v = statistics.median(vals)
+    print(json.dumps({
+        "metric": "Mpixels/s per vision graph", "value": round(v, 2), "unit": "Mpixels/s", "n_gpus": ws,
+        "steps": a.steps, "warmup": a.warmup, "impl": "reference", "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded PCG32)", "config": {"workload": DIFFWARP, "graph": DIFFWARP_DESC},
+        "cpu_baseline": {"value": round(v, 2), "unit": "Mpixels/s", "cores": cores, "kind": "port",
+                         "sample": f"{cores} processes x {per_step:.2f} s per step of FP64 warp + loss + adjoint "
+                                   "(the reference has no F32 warp)"},
+        "e2e": {"value": round(v, 2), "unit": "Mpixels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + [DIFFWARP])
     ap.add_argument("--frames", type=int, default=0, help="frames per step per GPU (default: the workload's)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true",
                     help="run the one-launch-per-node plan (the unfused, unbatched comparison form)")
     a = ap.parse_args(argv)
+    if a.workload == DIFFWARP:
+        if a.impl == "ours":
+            a.warmup = max(a.warmup, 3)
+            return run_diffwarp(a)
+        return run_diffwarp_reference(a)
     if a.impl == "ours":
         a.warmup = max(a.warmup, 3)
         return run_ours(a, a.workload)

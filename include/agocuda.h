@@ -298,6 +298,42 @@ int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t width, uint32_t heigh
                                     void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
                                     uint32_t *pNumCorners, void *scratch, size_t scratchBytes, uint32_t *pStatus);
 
+/* ---------------------------------------------------------------- differentiable F32 warps */
+/* F32 bilinear WarpAffine / Remap with a constant border and their adjoints, for batches of
+ * `n` images (image i at base + i * batch elements; strides in elements; device memory).
+ * No reference counterpart: the reference's warps are U8 only (ago_kernel_api.cpp:19255).
+ * The coordinate convention is its U8 WarpAffine's (ago_haf_cpu_geometric.cpp:679-684):
+ * xs = m00*x + m10*y + m20, ys = m01*x + m11*y + m21 with theta = (m00, m01, m10, m11, m20,
+ * m21) per image (device, n x 6 floats); bilinear from floor(xs), floor(ys), each tap
+ * outside the source reading `border`.  Remap samples at (x + field.x, y + field.y), field
+ * an (H, W, 2) float array per image (8-byte aligned).
+ * Adjoints ADD into the gradients (zero them first): pGradSrc (same layout as the source),
+ * pGradTheta (double, n x 6) or pGradField.  The L2 step computes, for L_i = sum over image
+ * i of (warp - target)^2, the gradients of L_i and L_i itself into pGradThetaLoss (double,
+ * n x 7: six theta gradients, then L_i) from one pass over the images. */
+int agocuda_WarpAffine_F32_Bilinear_Constant_batch(void *stream, int n, int width, int height, float *pDst,
+                                                   long long dstBatch, int dstStride, int srcWidth, int srcHeight,
+                                                   const float *pSrc, long long srcBatch, int srcStride,
+                                                   const float *theta, float border);
+int agocuda_WarpAffine_F32_Bilinear_Constant_adjoint_batch(void *stream, int n, int width, int height,
+                                                           const float *pGradOut, long long goBatch, int goStride,
+                                                           int srcWidth, int srcHeight, const float *pSrc,
+                                                           long long srcBatch, int srcStride, const float *theta,
+                                                           float border, float *pGradSrc, double *pGradTheta);
+int agocuda_WarpAffine_F32_L2_step_batch(void *stream, int n, int width, int height, const float *pTarget,
+                                         long long tBatch, int tStride, int srcWidth, int srcHeight, const float *pSrc,
+                                         long long srcBatch, int srcStride, const float *theta, float border,
+                                         float *pGradSrc, double *pGradThetaLoss);
+int agocuda_Remap_F32_Bilinear_Constant_batch(void *stream, int n, int width, int height, float *pDst, long long dstBatch,
+                                              int dstStride, int srcWidth, int srcHeight, const float *pSrc,
+                                              long long srcBatch, int srcStride, const float *pField, long long fieldBatch,
+                                              int fieldStride, float border);
+int agocuda_Remap_F32_Bilinear_Constant_adjoint_batch(void *stream, int n, int width, int height, const float *pGradOut,
+                                                      long long goBatch, int goStride, int srcWidth, int srcHeight,
+                                                      const float *pSrc, long long srcBatch, int srcStride,
+                                                      const float *pField, long long fieldBatch, int fieldStride,
+                                                      float border, float *pGradSrc, float *pGradField);
+
 /* ---------------------------------------------------------------- Gaussian pyramid */
 /* One pyramid level of VX_SCALE_PYRAMID_HALF: dst (ceil(srcW/2) x ceil(srcH/2)) rows 1..H-2 are
  * the [1 4 6 4 1]^2 / 256 samples the AGO CPU kernel computes (sample parity from the source

@@ -212,37 +212,75 @@ __global__ void k_hyst_output(int W, int H, uint8_t *out, int outStride, const i
 }
 
 // ---------------------------------------------------------------------------------
-// Fused Canny front end: gradient + suppression + thresholds for a 128x16 tile, labels
-// initialised and strong pixels listed -- one read of the image, no intermediate planes.
+// Fused Canny: gradient, suppression and double threshold for a 64x32 tile from one read
+// of the image, then hysteresis as block-based connected components.  The tile's
+// non-zero pixels are labelled in shared memory (lock-free union-find over the W, NW, N
+// and NE neighbours, i.e. 8-connectivity), so only pixels on tile borders reach the global
+// union-find.  Global node ("slot") of a tile pixel: tile * kTS + local index; a
+// component's final root is its smallest local-root slot.  The result is the same set of
+// 255 pixels as the per-pixel union-find above: 8-connected components of the interior
+// non-zero pixels that hold a strong (255) pixel.
 // ---------------------------------------------------------------------------------
-constexpr int kCTW = 128, kCTH = 16;                 // output tile
-constexpr int kCIW = kCTW + 4, kCIH = kCTH + 4;      // input tile (halo 2)
-constexpr int kCGW = kCTW + 2, kCGH = kCTH + 2;      // gradient tile (halo 1)
+constexpr int kTW = 64, kTH = 32, kTS = kTW * kTH;   // tile and its slot count
+constexpr int kIW = kTW + 4, kIH = kTH + 4;          // input tile (halo 2)
+constexpr int kGW = kTW + 2, kGH = kTH + 2;          // gradient tile (halo 1)
+constexpr uint16_t kNoLabel = 0xFFFF;
+
+__device__ __forceinline__ int sfind(const int *lab, int x)
+{
+    for (int i = 0; i < kTS; i++) {
+        const int p = lab[x];
+        if (p == x) return x;
+        x = p;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void sunion(int *lab, int a, int b)
+{
+    for (int i = 0; i < kTS; i++) {
+        a = sfind(lab, a);
+        b = sfind(lab, b);
+        if (a == b) return;
+        if (a > b) { const int t = a; a = b; b = t; }
+        const int old = atomicMin(lab + b, a);
+        if (old == b) return;
+        b = old;
+    }
+}
 
 __global__ void __launch_bounds__(256)
-k_canny_front(int W, int H, const uint8_t *src, int srcStride, int lower, int upper, int *L,
-              uint32_t *strong, uint32_t *strongCount, uint32_t capacity)
+k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, int lower, int upper,
+                  uint16_t *__restrict__ lab16, int labPitch, int *__restrict__ uf, uint32_t *__restrict__ bits)
 {
-    __shared__ uint8_t sIn[kCIH][kCIW + 4];
-    __shared__ uint16_t sG[kCGH][kCGW + 2];
-    __shared__ int16_t sV[kCIH];   // per tile row: vertical sum of column W-1 for the x == 0 quirk
-    const int x0 = blockIdx.x * kCTW, y0 = blockIdx.y * kCTH;
-    const int tid = threadIdx.x;
-    for (int i = tid; i < kCIH * kCIW; i += blockDim.x) {
-        const int r = i / kCIW, c = i % kCIW;
-        sIn[r][c] = (uint8_t)ago_px(src, srcStride, W, H, x0 - 2 + c, y0 - 2 + r);
+    __shared__ uint8_t sIn[kIH][kIW];
+    __shared__ uint16_t sG[kGH][kGW];
+    __shared__ int16_t sV[kIH];              // per tile row: vertical sum of column W-1 (x == 0 quirk)
+    __shared__ int sLab[kTS];
+    __shared__ uint32_t sStrongPx[kTS / 32], sStrongRoot[kTS / 32];
+    const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH, tid = threadIdx.x;
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+
+    // ---- input with a 2-pixel halo; the border tiles follow the reference's reads outside rows
+    const bool inner = x0 >= 2 && y0 >= 2 && x0 + kTW + 2 <= W && y0 + kTH + 2 <= H;
+    for (int i = tid; i < kIH * kIW; i += blockDim.x) {
+        const int r = i / kIW, c = i % kIW;
+        sIn[r][c] = inner ? __ldg(src + (size_t)(y0 - 2 + r) * srcStride + x0 - 2 + c)
+                          : (uint8_t)ago_px(src, srcStride, W, H, x0 - 2 + c, y0 - 2 + r);
     }
+    if (tid < kTS / 32) sStrongRoot[tid] = 0;
     const bool needV = x0 == 0 && (W & 15) == 0 && W >= 16;
-    if (needV && tid < kCIH - 2) {
-        const int y = y0 - 1 + tid;   // gradient row
+    if (needV && tid < kIH - 2) {
+        const int y = y0 - 1 + tid;
         sV[tid] = (y >= 1 && y < H - 1)
             ? (int16_t)(ago_px(src, srcStride, W, H, W - 1, y - 1) + 2 * ago_px(src, srcStride, W, H, W - 1, y) +
                         ago_px(src, srcStride, W, H, W - 1, y + 1))
             : 0;
     }
     __syncthreads();
-    for (int i = tid; i < kCGH * kCGW; i += blockDim.x) {
-        const int r = i / kCGW, c = i % kCGW;
+    // ---- packed gradient with a 1-pixel halo
+    for (int i = tid; i < kGH * kGW; i += blockDim.x) {
+        const int r = i / kGW, c = i % kGW;
         const int x = x0 - 1 + c, y = y0 - 1 + r;
         uint16_t g = 0;
         if (y >= 1 && y < H - 1 && x >= 0 && x < W) {
@@ -253,19 +291,120 @@ k_canny_front(int W, int H, const uint8_t *src, int srcStride, int lower, int up
         sG[r][c] = g;
     }
     __syncthreads();
-    for (int i = tid; i < kCTH * kCTW; i += blockDim.x) {
-        const int r = i / kCTW, c = i % kCTW;
-        const int x = x0 + c, y = y0 + r;
-        if (x >= W || y >= H) continue;
-        const bool in = x >= 1 && x < W - 1 && y >= 1 && y < H - 1;
+    // ---- suppression + thresholds; local labels of the non-zero interior pixels
+    for (int i = tid; i < kTS; i += blockDim.x) {
+        const int r = i / kTW, c = i % kTW, x = x0 + c, y = y0 + r;
         int v = 0;
-        if (in) {
+        if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1) {
             auto G = [&](int dx, int dy) { return (int)sG[r + 1 + dy][c + 1 + dx]; };
             v = canny_supp(G, lower, upper);
         }
-        const int p = y * W + x;
-        L[p] = v ? p : -1;
-        list_append(strong, strongCount, capacity, ((uint32_t)y << 16) | (uint32_t)x, v == 255);
+        sLab[i] = v ? i : -1;
+        const unsigned strong = __ballot_sync(0xffffffffu, v == 255);   // i / 32 is warp-uniform
+        if ((tid & 31) == 0) sStrongPx[i >> 5] = strong;
+    }
+    __syncthreads();
+    // ---- local union-find over the already-visited neighbours inside the tile
+    for (int i = tid; i < kTS; i += blockDim.x) {
+        if (sLab[i] < 0) continue;
+        const int r = i / kTW, c = i % kTW;
+        if (c > 0 && sLab[i - 1] >= 0) sunion(sLab, i, i - 1);
+        if (r > 0) {
+            if (c > 0 && sLab[i - kTW - 1] >= 0) sunion(sLab, i, i - kTW - 1);
+            if (sLab[i - kTW] >= 0) sunion(sLab, i, i - kTW);
+            if (c + 1 < kTW && sLab[i - kTW + 1] >= 0) sunion(sLab, i, i - kTW + 1);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < kTS; i += blockDim.x)
+        if (sLab[i] >= 0) sLab[i] = sfind(sLab, i);
+    __syncthreads();
+    for (int i = tid; i < kTS; i += blockDim.x)
+        if ((sStrongPx[i >> 5] >> (i & 31)) & 1) atomicOr(&sStrongRoot[sLab[i] >> 5], 1u << (sLab[i] & 31));
+    __syncthreads();
+    // ---- labels out; every local root starts as its own global root; strong-root bits
+    for (int i = tid; i < kTS; i += blockDim.x) {
+        const int r = i / kTW, c = i % kTW, x = x0 + c, y = y0 + r;
+        const int l = sLab[i];
+        if (x < W && y < H) lab16[(size_t)y * labPitch + x] = l >= 0 ? (uint16_t)l : kNoLabel;
+        if (l == i) uf[(size_t)tile * kTS + i] = tile * kTS + i;
+    }
+    if (tid < kTS / 32) bits[(size_t)tile * (kTS / 32) + tid] = sStrongRoot[tid];
+}
+
+__device__ __forceinline__ int slot_of(const uint16_t *lab16, int labPitch, int tilesX, int x, int y)
+{
+    const uint16_t l = lab16[(size_t)y * labPitch + x];
+    if (l == kNoLabel) return -1;
+    return ((y / kTH) * tilesX + x / kTW) * kTS + l;
+}
+
+// unions across tile borders: the W / NW / N / NE neighbours of a tile's left column, top
+// row and right column that lie in another tile
+__global__ void k_canny_ccl_border(int W, int H, const uint16_t *__restrict__ lab16, int labPitch, int tilesX,
+                                   int *uf, uint32_t *err)
+{
+    constexpr int kPer = kTH + kTW + kTH;
+    const int tile = blockIdx.y, b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= kPer) return;
+    const int x0 = (tile % tilesX) * kTW, y0 = (tile / tilesX) * kTH;
+    int x, y;
+    if (b < kTH) { x = x0; y = y0 + b; }
+    else if (b < kTH + kTW) { x = x0 + b - kTH; y = y0; }
+    else { x = x0 + kTW - 1; y = y0 + b - kTH - kTW; }
+    if (x >= W || y >= H) return;
+    const int sp = slot_of(lab16, labPitch, tilesX, x, y);
+    if (sp < 0) return;
+    const int dx[4] = {-1, -1, 0, 1}, dy[4] = {0, -1, -1, -1};
+    for (int k = 0; k < 4; k++) {
+        const int nx = x + dx[k], ny = y + dy[k];
+        if (nx < 0 || ny < 0 || nx >= W) continue;
+        if (nx >= x0 && nx < x0 + kTW && ny >= y0) continue;     // same tile: done locally
+        const int sq = slot_of(lab16, labPitch, tilesX, nx, ny);
+        if (sq >= 0) uf_union(uf, sp, sq, err);
+    }
+}
+
+// strong bits from local roots to the roots of their merged components
+__global__ void k_canny_ccl_mark(const int *uf, uint32_t *bits, uint32_t words)
+{
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+        uint32_t m = bits[w];
+        while (m) {
+            const int s = (int)(w * 32 + __ffs(m) - 1);
+            m &= m - 1;
+            const int r = uf_find(uf, s);
+            if (r != s) atomicOr(bits + (r >> 5), 1u << (r & 31));
+        }
+    }
+}
+
+// 8 pixels per thread: labels -> final roots -> 0/255
+__global__ void k_canny_ccl_output(int W, int H, const uint16_t *__restrict__ lab16, int labPitch, int tilesX,
+                                   const int *uf, const uint32_t *bits, uint8_t *__restrict__ out, int outStride)
+{
+    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * 8, y = blockIdx.y;
+    if (x >= W) return;
+    const uint16_t *lr = lab16 + (size_t)y * labPitch;
+    uint8_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        v[k] = 0;
+        const int xx = x + k;
+        if (xx >= W) continue;
+        const uint16_t l = lr[xx];
+        if (l == kNoLabel) continue;
+        const int r = uf_find(uf, ((y / kTH) * tilesX + xx / kTW) * kTS + l);
+        v[k] = (bits[r >> 5] >> (r & 31)) & 1 ? 255 : 0;
+    }
+    uint8_t *o = out + (size_t)y * outStride + x;
+    if (x + 8 <= W && ((uintptr_t)o & 7) == 0) {
+        uint2 w;
+        w.x = v[0] | (v[1] << 8) | (v[2] << 16) | ((uint32_t)v[3] << 24);
+        w.y = v[4] | (v[5] << 8) | (v[6] << 16) | ((uint32_t)v[7] << 24);
+        *(uint2 *)o = w;
+    } else {
+        for (int k = 0; k < 8 && x + k < W; k++) o[k] = v[k];
     }
 }
 
@@ -367,63 +506,85 @@ __global__ void k_harris_nms(int W, int H, const float *sc, int scStride, uint64
     xys_append(list, count, capacity, xys_pack(x, y, v), keep);
 }
 
-// Fused Harris front end: Sobel products, window sums, score and NMS for a 64x16 tile.
-constexpr int kHTW = 64, kHTH = 16;
-constexpr int kHIW = kHTW + 6, kHIH = kHTH + 6;   // input halo 3
-constexpr int kHGW = kHTW + 4, kHGH = kHTH + 4;   // HG3 halo 2
-constexpr int kHSW = kHTW + 2, kHSH = kHTH + 2;   // score halo 1
+// Harris front end as column strips: a warp owns 26 output columns (lanes 3..28; the outer
+// lanes carry the halo) and walks down 64 output rows with rolling registers.  Per input
+// row a lane loads one byte; three rows travel packed in one word, so two shuffles give the
+// gradient's neighbours.  The Sobel products and their 3x3 window sums are integers below
+// 2^24, i.e. exactly the float sums the reference forms; the score keeps the reference's
+// float operation order, and its division is skipped only where the result cannot exceed
+// the threshold.
+constexpr int kHRows = 64, kHCols = 26;
 
-__global__ void __launch_bounds__(256)
-k_harris_front(int W, int H, const uint8_t *src, int srcStride, float k, float Tc, float norm,
-               uint64_t *list, uint32_t *count, uint32_t capacity)
+__device__ __forceinline__ uint32_t harris_in(const uint8_t *src, int stride, int W, int H, int x, int y)
 {
-    __shared__ uint8_t sIn[kHIH][kHIW + 2];
-    __shared__ float sG[3][kHGH][kHGW + 1];
-    __shared__ float sS[kHSH][kHSW + 1];
-    const int x0 = blockIdx.x * kHTW, y0 = blockIdx.y * kHTH, tid = threadIdx.x;
-    for (int i = tid; i < kHIH * kHIW; i += blockDim.x) {
-        const int r = i / kHIW, c = i % kHIW;
-        sIn[r][c] = (uint8_t)ago_px(src, srcStride, W, H, x0 - 3 + c, y0 - 3 + r);
-    }
-    __syncthreads();
-    for (int i = tid; i < kHGH * kHGW; i += blockDim.x) {
-        const int r = i / kHGW, c = i % kHGW;
-        const int x = x0 - 2 + c, y = y0 - 2 + r;
-        float a = 0.f, b = 0.f, d = 0.f;
-        if (y >= 1 && y < H - 1 && x >= 0 && x < W) {
-            auto P = [&](int dx, int dy) { return (int)sIn[r + 1 + dy][c + 1 + dx]; };
-            harris_grad(P, a, b, d);
+    if (x >= 0 && x < W && y >= 0 && y < H) return __ldg(src + (size_t)y * stride + x);
+    return (uint32_t)ago_px(src, stride, W, H, x, y);
+}
+
+__global__ void __launch_bounds__(128)
+k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, float k, float Tc, float norm,
+              uint64_t *list, uint32_t *count, uint32_t capacity)
+{
+    const int lane = threadIdx.x & 31;
+    const int xs = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kHCols;
+    if (xs >= W) return;                                   // warp-uniform
+    const int xc = xs + lane - 3;
+    const int ys = blockIdx.y * kHRows, yEnd = min(ys + kHRows, H);
+    const bool gradCol = xc >= 0 && xc < W, scoreCol = xc >= 1 && xc < W - 1;
+    const bool outLane = lane >= 3 && lane < 3 + kHCols && scoreCol;
+    const float cut = Tc > 0.f ? __fmul_rn(0.999f, __fmul_rn(Tc, norm)) : 0.f;   // Mc below: score 0
+    uint32_t rows = 0;                                     // input rows r-2 | r-1 << 8 | r << 16
+    int v0[3] = {0, 0, 0}, v1[3] = {0, 0, 0};              // products at gradient rows g-2, g-1
+    float sA = 0.f, sB = 0.f;                              // scores at rows s-2, s-1
+    uint32_t next = harris_in(src, srcStride, W, H, xc, ys - 3);
+    for (int r = ys - 3; r <= yEnd + 2; r++) {
+        const uint32_t cur = next;
+        if (r + 1 <= yEnd + 2) next = harris_in(src, srcStride, W, H, xc, r + 1);
+        rows = (rows >> 8) | (cur << 16);
+        // gradient at g = r - 1 from rows r-2, r-1, r
+        const uint32_t Lw = __shfl_up_sync(0xffffffffu, rows, 1), Rw = __shfl_down_sync(0xffffffffu, rows, 1);
+        const int g = r - 1;
+        int p0 = 0, p1 = 0, p2 = 0;
+        if (gradCol && g >= 1 && g < H - 1) {
+            const int L0 = Lw & 255, L1 = (Lw >> 8) & 255, L2 = (Lw >> 16) & 255;
+            const int R0 = Rw & 255, R1 = (Rw >> 8) & 255, R2 = (Rw >> 16) & 255;
+            const int C0 = rows & 255, C2 = (rows >> 16) & 255;
+            const int gx = (R2 - L2) + (R0 - L0) + 2 * (R1 - L1);
+            const int gy = (L2 + 2 * C2 + R2) - (L0 + 2 * C0 + R0);
+            p0 = gx * gx; p1 = gx * gy; p2 = gy * gy;
         }
-        sG[0][r][c] = a; sG[1][r][c] = b; sG[2][r][c] = d;
-    }
-    __syncthreads();
-    for (int i = tid; i < kHSH * kHSW; i += blockDim.x) {
-        const int r = i / kHSW, c = i % kHSW;
-        const int x = x0 - 1 + c, y = y0 - 1 + r;
-        float v = 0.f;
-        if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1) {
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-            for (int j = 0; j < 3; j++)
-                for (int q = 0; q < 3; q++) {
-                    s0 = __fadd_rn(s0, sG[0][r + j][c + q]);
-                    s1 = __fadd_rn(s1, sG[1][r + j][c + q]);
-                    s2 = __fadd_rn(s2, sG[2][r + j][c + q]);
-                }
-            v = harris_score(s0, s1, s2, k, Tc, norm);
+        // vertical sums at s = g - 1 over gradient rows g-2, g-1, g, then horizontal
+        const int c0 = v0[0] + v1[0] + p0, c1 = v0[1] + v1[1] + p1, c2 = v0[2] + v1[2] + p2;
+        v0[0] = v1[0]; v0[1] = v1[1]; v0[2] = v1[2];
+        v1[0] = p0; v1[1] = p1; v1[2] = p2;
+        const int S0 = c0 + __shfl_up_sync(0xffffffffu, c0, 1) + __shfl_down_sync(0xffffffffu, c0, 1);
+        const int S1 = c1 + __shfl_up_sync(0xffffffffu, c1, 1) + __shfl_down_sync(0xffffffffu, c1, 1);
+        const int S2 = c2 + __shfl_up_sync(0xffffffffu, c2, 1) + __shfl_down_sync(0xffffffffu, c2, 1);
+        const int srow = g - 1;
+        float sc = 0.f;
+        if (scoreCol && srow >= 1 && srow < H - 1) {
+            const float gx2 = (float)S0, gxy2 = (float)S1, gy2 = (float)S2;
+            const float traceA = __fadd_rn(gx2, gy2);
+            const float detA = __fsub_rn(__fmul_rn(gx2, gy2), __fmul_rn(gxy2, gxy2));
+            const float Mc = __fsub_rn(detA, __fmul_rn(__fmul_rn(k, traceA), traceA));
+            const bool zero = Tc >= 0.f && (Mc <= 0.f || (Tc > 0.f && Mc < cut));
+            if (!zero) {
+                const float q = __fdiv_rn(Mc, norm);
+                sc = q > Tc ? q : 0.f;
+            }
         }
-        sS[r][c] = v;
-    }
-    __syncthreads();
-    for (int i = tid; i < kHTH * kHTW; i += blockDim.x) {
-        const int r = i / kHTW, c = i % kHTW;
-        const int x = x0 + c, y = y0 + r;
-        const bool in = x >= 1 && x < W - 1 && y >= 1 && y < H - 1;
+        // non-maximum suppression at n = s - 1
+        const int n = srow - 1;
+        const float aL = __shfl_up_sync(0xffffffffu, sA, 1), aR = __shfl_down_sync(0xffffffffu, sA, 1);
+        const float bL = __shfl_up_sync(0xffffffffu, sB, 1), bR = __shfl_down_sync(0xffffffffu, sB, 1);
+        const float cL = __shfl_up_sync(0xffffffffu, sc, 1), cR = __shfl_down_sync(0xffffffffu, sc, 1);
+        const bool rowOut = n >= ys && n < yEnd && n >= 1 && n < H - 1;
         bool keep = false;
-        if (in) {
-            auto S = [&](int dx, int dy) { return sS[r + 1 + dy][c + 1 + dx]; };
-            keep = harris_nms(S);
-        }
-        xys_append(list, count, capacity, xys_pack(x, y, in ? sS[r + 1][c + 1] : 0.f), keep);
+        if (outLane && rowOut)
+            keep = sB >= aL && sB >= sA && sB >= aR && sB >= bL && sB > bR && sB > cL && sB > sc && sB > cR;
+        if (rowOut) xys_append(list, count, capacity, xys_pack(xc, n, sB), keep);
+        sA = sB;
+        sB = sc;
     }
 }
 
@@ -694,31 +855,56 @@ extern "C" int agocuda_CannyEdgeTrace_U8_U8XY_noalloc(void *stream, uint32_t W, 
 
 extern "C" size_t agocuda_CannyEdgeTrace_noalloc_max_pixels(void) { return kNoAllocMaxPixels; }
 
+// scratch of the fused Canny: tile-local labels (u16, pitched), the global union-find over
+// tile slots (int per slot) and the strong-root bitmap (one bit per slot)
+struct CannyScratch { uint16_t *lab; int labPitch; int *uf; uint32_t *bits; size_t bytes; int tilesX, tilesY; };
+
+static CannyScratch canny_scratch_layout(uint32_t W, uint32_t H, void *base)
+{
+    CannyScratch c{};
+    c.tilesX = (int)div_up(W, kTW);
+    c.tilesY = (int)div_up(H, kTH);
+    const size_t slots = (size_t)c.tilesX * c.tilesY * kTS;
+    c.labPitch = (int)((W + 7) & ~7u);                       // elements (16-byte rows)
+    const size_t labBytes = ((size_t)c.labPitch * H * 2 + 255) & ~(size_t)255;
+    const size_t ufBytes = (slots * 4 + 255) & ~(size_t)255;
+    const size_t bitBytes = ((slots / 8) + 255) & ~(size_t)255;
+    c.bytes = labBytes + ufBytes + bitBytes;
+    if (base) {
+        uint8_t *p = (uint8_t *)base;
+        c.lab = (uint16_t *)p;
+        c.uf = (int *)(p + labBytes);
+        c.bits = (uint32_t *)(p + labBytes + ufBytes);
+    }
+    return c;
+}
+
 extern "C" int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
                                                       const uint8_t *pSrc, uint32_t srcStride, uint16_t hystLower,
                                                       uint16_t hystUpper, void *scratch, size_t scratchBytes, uint32_t *pStatus)
 {
-    const size_t n = (size_t)W * H;
-    const size_t need = agocuda_CannyEdgeTrace_scratch_size(W, H) + n * sizeof(uint32_t) + 512;
     if (!pDst || !pSrc || !scratch || !pStatus || W < 3 || H < 3 || dstStride < W || srcStride < W || W > 65535 ||
-        H > 65535 || n >= (1ull << 31) || scratchBytes < need || !aligned(scratch, 256))
+        H > 65535 || !aligned(scratch, 256))
         return AGOCUDA_INVALID_PARAMS;
-    uint8_t *sp = (uint8_t *)scratch;
-    int *L = (int *)sp;                         sp += (n * sizeof(int) + 255) & ~(size_t)255;
-    uint32_t *bits = (uint32_t *)sp;            sp += (((n + 31) / 32) * 4 + 255) & ~(size_t)255;
-    uint32_t *cnt = (uint32_t *)sp;             sp += 256;
-    uint32_t *strong = (uint32_t *)sp;
+    const CannyScratch c = canny_scratch_layout(W, H, scratch);
+    if (scratchBytes < c.bytes || (size_t)c.tilesX * c.tilesY * kTS >= (1ull << 31)) return AGOCUDA_INVALID_PARAMS;
     cudaStream_t s = as_stream(stream);
-    cudaMemsetAsync(cnt, 0, 4, s);
-    dim3 grd(div_up(W, kCTW), div_up(H, kCTH));
-    k_canny_front<<<grd, 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper, L, strong, cnt, (uint32_t)n);
-    agocuda_count_launch(1);
-    return hysteresis_tail(s, (int)W, (int)H, pDst, (int)dstStride, L, bits, strong, cnt, (uint32_t)n, pStatus);
+    const int tiles = c.tilesX * c.tilesY;
+    k_canny_ccl_front<<<dim3(c.tilesX, c.tilesY), 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper,
+                                                               c.lab, c.labPitch, c.uf, c.bits);
+    constexpr int kPer = kTH + kTW + kTH;
+    k_canny_ccl_border<<<dim3(div_up(kPer, 128), tiles), 128, 0, s>>>((int)W, (int)H, c.lab, c.labPitch, c.tilesX, c.uf, pStatus);
+    const uint32_t words = (uint32_t)tiles * (kTS / 32);
+    k_canny_ccl_mark<<<div_up(words, 256), 256, 0, s>>>(c.uf, c.bits, words);
+    k_canny_ccl_output<<<dim3(div_up(div_up(W, 8), 128), H), 128, 0, s>>>((int)W, (int)H, c.lab, c.labPitch, c.tilesX, c.uf,
+                                                                          c.bits, pDst, (int)dstStride);
+    agocuda_count_launch(4);
+    return agocuda_launch_status();
 }
 
 extern "C" size_t agocuda_fused_CannyEdgeDetector_scratch_size(uint32_t W, uint32_t H)
 {
-    return agocuda_CannyEdgeTrace_scratch_size(W, H) + (size_t)W * H * sizeof(uint32_t) + 512 + 1024;
+    return canny_scratch_layout(W, H, nullptr).bytes + 256;   // + room to align an arbitrary base to 256
 }
 
 extern "C" int agocuda_HarrisSobel_HG3_U8_3x3(void *stream, uint32_t W, uint32_t H, float *pDst, uint32_t dstStride,
@@ -795,8 +981,9 @@ extern "C" int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t W, uint32_
     uint64_t *list = (uint64_t *)((uint8_t *)scratch + 256);
     cudaStream_t s = as_stream(stream);
     cudaMemsetAsync(cnt, 0, 4, s);
-    dim3 grd(div_up(W, kHTW), div_up(H, kHTH));
-    k_harris_front<<<grd, 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, sensitivity, strengthThreshold, normFactor, list, cnt, cap);
+    const int strips = (int)div_up(W, kHCols);
+    k_harris_rows<<<dim3(div_up(strips, 4), div_up(H, kHRows)), 128, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, sensitivity,
+                                                                             strengthThreshold, normFactor, list, cnt, cap);
     agocuda_count_launch(1);
     int rc = agocuda_launch_status();
     if (rc) return rc;

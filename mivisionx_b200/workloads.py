@@ -436,3 +436,50 @@ class WarpRemapGraph:
 
     def results(self):
         return {k: (self.api.read_plane(v), self.api.valid_region(v)) for k, v in self.outs.items()}
+
+
+# ---------------------------------------------------------------- config 5 (F32 warp + adjoint)
+def cfg5_images(n: int = 32, seed: int = 5, size: int = 1024) -> np.ndarray:
+    """(n, size, size) float32: uniform [0, 1) from PCG32 smoothed by a Gaussian, sigma 2
+    (separable, truncated at 4 sigma, edges reflected)."""
+    r = np.arange(-8, 9, dtype=np.float64)
+    k = np.exp(-0.5 * (r / 2.0) ** 2)
+    k /= k.sum()
+    out = np.empty((n, size, size), np.float32)
+    for i in range(n):
+        u = uniform01(seed + i, size * size, stream=37).reshape(size, size)
+        p = np.pad(u, 8, mode="reflect")
+        h = sum(k[j] * p[:, j:j + size] for j in range(17))
+        out[i] = sum(k[j] * h[j:j + size, :] for j in range(17)).astype(np.float32)
+    return out
+
+
+def affine_theta(angle_deg: float, scale: float, tx: float, ty: float, size: int) -> np.ndarray:
+    """Matrix entries (m00, m01, m10, m11, m20, m21) of the map output -> source that rotates
+    by `angle_deg` and scales by `scale` about the image centre, then shifts by (tx, ty)."""
+    c = (size - 1) / 2.0
+    t = np.deg2rad(angle_deg)
+    a, b = scale * np.cos(t), -scale * np.sin(t)
+    d, e = scale * np.sin(t), scale * np.cos(t)
+    return np.array([a, d, b, e, c + tx - a * c - b * c, c + ty - d * c - e * c], np.float64)
+
+
+def cfg5_params(n: int = 32, seed: int = 5, size: int = 1024):
+    """(ground truth, initial estimate) theta per image: rotation U(+-10 deg), scale U(0.9, 1.1),
+    shift U(+-20 px); the estimate perturbs them by U(+-2 deg), U(+-0.02), U(+-3 px)."""
+    u = uniform01(seed, 8 * n, stream=41).reshape(n, 8) * 2.0 - 1.0
+    gt, init = [], []
+    for i in range(n):
+        ang, sc, tx, ty = 10 * u[i, 0], 1.0 + 0.1 * u[i, 1], 20 * u[i, 2], 20 * u[i, 3]
+        gt.append(affine_theta(ang, sc, tx, ty, size))
+        init.append(affine_theta(ang + 2 * u[i, 4], sc + 0.02 * u[i, 5], tx + 3 * u[i, 6], ty + 3 * u[i, 7], size))
+    return np.array(gt), np.array(init)
+
+
+def cfg5_field(seed: int = 5, size: int = 1024, amplitude: float = 4.0) -> np.ndarray:
+    """(size, size, 2) float32 displacement field, smooth, within +-amplitude px."""
+    yy, xx = np.meshgrid(np.arange(size, dtype=np.float64), np.arange(size, dtype=np.float64), indexing="ij")
+    p = uniform01(seed, 12, stream=43)
+    fx = np.sin(2 * np.pi * (p[0] * 3 * xx / size + p[1])) * np.cos(2 * np.pi * (p[2] * 3 * yy / size + p[3]))
+    fy = np.cos(2 * np.pi * (p[4] * 3 * xx / size + p[5])) * np.sin(2 * np.pi * (p[6] * 3 * yy / size + p[7]))
+    return (amplitude * np.stack([fx, fy], -1)).astype(np.float32)
