@@ -45,6 +45,43 @@ constexpr int kHalfThreads = 64;
 constexpr int kHalfCols = 8 * kHalfThreads;     // output columns per tile
 constexpr int kHalfRows = 16;                   // output rows per tile
 
+// ago_byte() for a row inside the image and a column within one AGO row pitch of it
+// (c in [-pitch, 2*pitch)), without division: the edge threads of every tile row use it.
+__device__ __forceinline__ uint32_t ago_byte_row(const uint8_t *img, size_t stride, int W, int H, int r, int c)
+{
+    if (c >= 0 && c < W) return img[(size_t)r * stride + c];
+    const int S = (W + 15) & ~15;
+    if (c < 0) {                                   // previous row's tail (padding unless W % 16 == 0)
+        const int cc = c + S;
+        return (r > 0 && cc < W) ? img[(size_t)(r - 1) * stride + cc] : 0;
+    }
+    if (c < S) return 0;                           // this row's padding
+    const int cc = c - S;                          // next row's head
+    return (r + 1 < H && cc < W) ? img[(size_t)(r + 1) * stride + cc] : 0;
+}
+
+struct Row24 { uint32_t w[6]; };
+
+// The border path of a row load, kept out of line and rolled: unrolled at every call site it
+// made the kernel's code large enough to thrash the instruction cache.
+__device__ __noinline__ Row24 half_load_row_edge(const uint8_t *src, int stride, int W, int H, int r, int x0)
+{
+    Row24 out;
+    const bool near = W >= 24;   // columns [x0, x0 + 24) then lie within one pitch of the row
+#pragma unroll 1
+    for (int k = 0; k < 6; k++) {
+        uint32_t v = 0;
+#pragma unroll 1
+        for (int b = 0; b < 4; b++) {
+            const int c = x0 + 4 * k + b;
+            const uint32_t px = near ? ago_byte_row(src, stride, W, H, r, c) : ago_byte(src, stride, W, H, r, c);
+            v |= px << (8 * b);
+        }
+        out.w[k] = v;
+    }
+    return out;
+}
+
 // Six words covering source bytes [x0, x0 + 24) of row r, x0 = 2*ox - 4.
 __device__ __forceinline__ void half_load_row(const agocuda_half_job &J, int r, int x0, bool edge, uint32_t w[6])
 {
@@ -55,14 +92,9 @@ __device__ __forceinline__ void half_load_row(const agocuda_half_job &J, int r, 
         w[1] = m.x; w[2] = m.y; w[3] = m.z; w[4] = m.w;
         w[5] = *(const uint32_t *)(p + 20);
     } else {
+        const Row24 e = half_load_row_edge(J.src, (int)J.srcStride, (int)J.srcW, (int)J.srcH, r, x0);
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
-            uint32_t v = 0;
-#pragma unroll
-            for (int b = 0; b < 4; b++)
-                v |= ago_byte(J.src, J.srcStride, (int)J.srcW, (int)J.srcH, r, x0 + 4 * k + b) << (8 * b);
-            w[k] = v;
-        }
+        for (int k = 0; k < 6; k++) w[k] = e.w[k];
     }
 }
 

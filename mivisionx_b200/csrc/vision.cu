@@ -150,6 +150,17 @@ __device__ __forceinline__ int uf_find(const int *L, int x)
     return x;
 }
 
+// find on a union-find no thread is modifying (after the union pass): L1-cached loads
+__device__ __forceinline__ int uf_find_ro(const int *__restrict__ L, int x)
+{
+    for (int i = 0; i < kFindLimit; i++) {
+        const int p = __ldg(L + x);
+        if (p == x) return x;
+        x = p;
+    }
+    return x;
+}
+
 __device__ __forceinline__ void uf_union(int *L, int a, int b, uint32_t *err)
 {
     for (int i = 0; i < kFindLimit; i++) {
@@ -373,7 +384,7 @@ __global__ void k_canny_ccl_mark(const int *uf, uint32_t *bits, uint32_t words)
         while (m) {
             const int s = (int)(w * 32 + __ffs(m) - 1);
             m &= m - 1;
-            const int r = uf_find(uf, s);
+            const int r = uf_find_ro(uf, s);
             if (r != s) atomicOr(bits + (r >> 5), 1u << (r & 31));
         }
     }
@@ -387,15 +398,21 @@ __global__ void k_canny_ccl_output(int W, int H, const uint16_t *__restrict__ la
     if (x >= W) return;
     const uint16_t *lr = lab16 + (size_t)y * labPitch;
     uint8_t v[8];
+    const int tileBase = ((y / kTH) * tilesX + x / kTW) * kTS;   // 8 pixels never straddle a tile (kTW % 8 == 0)
+    int lastSlot = -1, lastVal = 0;                               // neighbours usually share a component
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         v[k] = 0;
-        const int xx = x + k;
-        if (xx >= W) continue;
-        const uint16_t l = lr[xx];
+        if (x + k >= W) continue;
+        const uint16_t l = lr[x + k];
         if (l == kNoLabel) continue;
-        const int r = uf_find(uf, ((y / kTH) * tilesX + xx / kTW) * kTS + l);
-        v[k] = (bits[r >> 5] >> (r & 31)) & 1 ? 255 : 0;
+        const int slot = tileBase + l;
+        if (slot != lastSlot) {
+            const int r = uf_find_ro(uf, slot);
+            lastSlot = slot;
+            lastVal = (__ldg(bits + (r >> 5)) >> (r & 31)) & 1 ? 255 : 0;
+        }
+        v[k] = (uint8_t)lastVal;
     }
     uint8_t *o = out + (size_t)y * outStride + x;
     if (x + 8 <= W && ((uintptr_t)o & 7) == 0) {
