@@ -108,6 +108,10 @@ static const Image *pyr_level(Graph *g, Pyramid *py, size_t l)
     return it == g->replaced.end() ? py->level[l] : IMG(it->second);
 }
 
+// Batched steps launch over groups of this many frames: a group's kernels can start while
+// later frames are still being uploaded, and groups spread over the capture lanes.
+constexpr size_t kGroupFrames = 8;
+
 static vx_status lk_frame(Graph *g, LNode &ln, agocuda_lk_frame &F, uint32_t &cap)
 {
     auto &p = ln.p;
@@ -140,21 +144,27 @@ static vx_status lk_frame(Graph *g, LNode &ln, agocuda_lk_frame &F, uint32_t &ca
 static vx_status lk_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step &st)
 {
     std::vector<agocuda_lk_frame> fr(nodes.size());
-    uint32_t maxPts = 0;
-    for (size_t i = 0; i < nodes.size(); i++) {
-        uint32_t cap = 0;
-        if (vx_status s = lk_frame(g, *nodes[i], fr[i], cap)) return s;
-        maxPts = std::max(maxPts, cap);
-    }
+    std::vector<uint32_t> cap(nodes.size(), 0);
+    for (size_t i = 0; i < nodes.size(); i++)
+        if (vx_status s = lk_frame(g, *nodes[i], fr[i], cap[i])) return s;
     void *dev = scratch(g, fr.size() * sizeof(agocuda_lk_frame));
     if (!dev) return VX_ERROR_NO_MEMORY;
     if (cudaMemcpy(dev, fr.data(), fr.size() * sizeof(agocuda_lk_frame), cudaMemcpyHostToDevice) != cudaSuccess)
         return VX_FAILURE;
-    const uint32_t n = (uint32_t)fr.size();
     uint32_t *status = g->status_dev;
-    st.num_kernels = 2;
-    st.launch = [=](cudaStream_t q) {
-        return agocuda_OpticalFlowPyrLK_batch(S(q), (agocuda_lk_frame *)dev, n, maxPts, status);
+    std::vector<std::function<int(cudaStream_t)>> fns;
+    for (size_t k0 = 0; k0 < fr.size(); k0 += kGroupFrames) {
+        const size_t k1 = std::min(fr.size(), k0 + kGroupFrames);
+        const uint32_t pts = *std::max_element(cap.begin() + k0, cap.begin() + k1);
+        agocuda_lk_frame *d0 = (agocuda_lk_frame *)dev + k0;
+        const uint32_t n = (uint32_t)(k1 - k0);
+        fns.push_back([=](cudaStream_t q) { return agocuda_OpticalFlowPyrLK_batch(S(q), d0, n, pts, status); });
+        st.parts.push_back(Part{fns.back(), std::vector<LNode *>(nodes.begin() + k0, nodes.begin() + k1)});
+    }
+    st.num_kernels = 2 * (int)fns.size();
+    st.launch = [fns](cudaStream_t q) {
+        for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
+        return 0;
     };
     return VX_SUCCESS;
 }
@@ -162,22 +172,36 @@ static vx_status lk_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step
 // ScaleGaussianHalf levels of many images in one launch (one job per lowered node)
 static vx_status half_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step &st)
 {
+    // launches over groups of images (tile numbering restarts in every group)
+    const size_t kGroupJobs = 2 * kGroupFrames;
     std::vector<agocuda_half_job> jobs;
+    std::vector<uint32_t> group_tiles;
     uint32_t tiles = 0;
-    for (LNode *ln : nodes) {
-        const Image *d = IMG(ln->p[0]), *s = IMG(ln->p[1]);
+    for (size_t i = 0; i < nodes.size(); i++) {
+        if (i % kGroupJobs == 0 && i) { group_tiles.push_back(tiles); tiles = 0; }
+        const Image *d = IMG(nodes[i]->p[0]), *s = IMG(nodes[i]->p[1]);
         agocuda_half_job j{s->planes[0].dev, d->planes[0].dev, s->width, s->height, s->planes[0].dev_stride,
                            d->width, d->height, d->planes[0].dev_stride, tiles, 0};
         tiles += agocuda_ScaleGaussianHalf_tiles(d->width, d->height);
         jobs.push_back(j);
     }
-    void *dev = scratch(g, jobs.size() * sizeof(agocuda_half_job));
+    group_tiles.push_back(tiles);
+    agocuda_half_job *dev = (agocuda_half_job *)scratch(g, jobs.size() * sizeof(agocuda_half_job));
     if (!dev) return VX_ERROR_NO_MEMORY;
     if (cudaMemcpy(dev, jobs.data(), jobs.size() * sizeof(agocuda_half_job), cudaMemcpyHostToDevice) != cudaSuccess)
         return VX_FAILURE;
-    const uint32_t n = (uint32_t)jobs.size();
-    st.launch = [=](cudaStream_t q) {
-        return agocuda_fused_ScaleGaussianHalf_batch(S(q), (const agocuda_half_job *)dev, n, tiles);
+    std::vector<std::function<int(cudaStream_t)>> fns;
+    for (size_t k0 = 0, gi = 0; k0 < jobs.size(); k0 += kGroupJobs, gi++) {
+        const size_t k1 = std::min(jobs.size(), k0 + kGroupJobs);
+        const agocuda_half_job *d0 = dev + k0;
+        const uint32_t n = (uint32_t)(k1 - k0), t = group_tiles[gi];
+        fns.push_back([=](cudaStream_t q) { return agocuda_fused_ScaleGaussianHalf_batch(S(q), d0, n, t); });
+        st.parts.push_back(Part{fns.back(), std::vector<LNode *>(nodes.begin() + k0, nodes.begin() + k1)});
+    }
+    st.num_kernels = (int)fns.size();
+    st.launch = [fns](cudaStream_t q) {
+        for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
+        return 0;
     };
     return VX_SUCCESS;
 }
@@ -537,6 +561,7 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
             fns.push_back([=](cudaStream_t q) {
                 return agocuda_fused_ColorScale_RGB(S(q), w, h, src, ss, y1, y1s, uv, uvs, y2, y2s, u, us, v, vs, ob, obs, oa, oas);
             });
+            st.parts.push_back(Part{fns.back(), c.nodes});
         }
         st.launch = [fns](cudaStream_t q) {
             for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
@@ -565,6 +590,7 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
                 fns.push_back([=](cudaStream_t q) {
                     return agocuda_fused_CannyEdgeDetector_3x3_L1(S(q), w, h, dst, ds, src, ss, lo, hi, scr, sb, status);
                 });
+                st.parts.push_back(Part{fns.back(), c.nodes});
                 st.num_kernels += 4;
             } else {
                 LNode *sc = c.nodes[1], *pk = c.nodes[3];
@@ -581,6 +607,7 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
                 fns.push_back([=](cudaStream_t q) {
                     return agocuda_fused_HarrisCorners_3x3(S(q), w, h, src, ss, k, tc, norm, mind, out, ocap, oc, nc, scr, sb, status);
                 });
+                st.parts.push_back(Part{fns.back(), c.nodes});
                 st.num_kernels += 2;
             }
         }
@@ -595,7 +622,6 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
     for (Chain &c : chains) for (LNode *n : c.nodes) st.nodes.push_back(n);
     if (c0.kind == "fused_GaussSobelMagDepthThresh") {
         std::vector<agocuda_frame> fr;
-        uint32_t mw = 0, mh = 0;
         for (Chain &c : chains) {
             Image *s = IMG(c.src), *d = IMG(c.dst);
             agocuda_frame f{};
@@ -606,15 +632,29 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
             // [0, W - W % 16) (ago_haf_cpu_filter.cpp:2480-2483)
             f.simdBegin = 0; f.simdEnd = (int32_t)(s->width - (s->width & 15));
             fr.push_back(f);
-            mw = std::max(mw, s->width); mh = std::max(mh, s->height);
         }
-        void *dev = scratch(g, fr.size() * sizeof(agocuda_frame));
+        agocuda_frame *dev = (agocuda_frame *)scratch(g, fr.size() * sizeof(agocuda_frame));
         if (!dev) return VX_ERROR_NO_MEMORY;
         cudaMemcpy(dev, fr.data(), fr.size() * sizeof(agocuda_frame), cudaMemcpyHostToDevice);
-        const uint32_t n = (uint32_t)fr.size();
         const int32_t shift = (int32_t)c0.key[0], thr = (int32_t)c0.key[1];
-        st.launch = [=](cudaStream_t q) {
-            return agocuda_fused_GaussSobelMagDepthThresh(S(q), (const agocuda_frame *)dev, n, mw, mh, shift, thr);
+        std::vector<std::function<int(cudaStream_t)>> fns;
+        for (size_t k0 = 0; k0 < fr.size(); k0 += kGroupFrames) {
+            const size_t k1 = std::min(fr.size(), k0 + kGroupFrames);
+            uint32_t gw = 0, gh = 0;
+            for (size_t k = k0; k < k1; k++) { gw = std::max(gw, fr[k].width); gh = std::max(gh, fr[k].height); }
+            const agocuda_frame *d0 = dev + k0;
+            const uint32_t n = (uint32_t)(k1 - k0);
+            fns.push_back([=](cudaStream_t q) {
+                return agocuda_fused_GaussSobelMagDepthThresh(S(q), d0, n, gw, gh, shift, thr);
+            });
+            Part pt{fns.back(), {}};
+            for (size_t k = k0; k < k1; k++) for (LNode *nd : chains[k].nodes) pt.nodes.push_back(nd);
+            st.parts.push_back(std::move(pt));
+        }
+        st.num_kernels = (int)fns.size();
+        st.launch = [fns](cudaStream_t q) {
+            for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
+            return 0;
         };
         return VX_SUCCESS;
     }

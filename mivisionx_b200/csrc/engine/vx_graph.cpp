@@ -6,9 +6,11 @@
 // device work (fused multi-node kernels, batched launches over independent same-kernel
 // nodes), allocates device buffers and captures the whole launch sequence into one CUDA
 // graph.  vxProcessGraph uploads stale inputs, replays the CUDA graph and waits.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <set>
 
 #include "vx_internal.h"
 
@@ -22,6 +24,8 @@ void graph_invalidate(Graph *g)
     g->state = VX_GRAPH_STATE_UNVERIFIED;
     if (g->cexec) { cudaGraphExecDestroy(g->cexec); g->cexec = nullptr; }
     if (g->cgraph) { cudaGraphDestroy(g->cgraph); g->cgraph = nullptr; }
+    g->streamed_in.clear();
+    g->streamed_out.clear();
     g->steps.clear();
 }
 
@@ -58,19 +62,249 @@ static uint64_t param_signature(Graph *g)
     return h;
 }
 
-static vx_status capture(Graph *g)
+// ---- capture ------------------------------------------------------------------------
+// The plan's steps -- split into their per-frame parts where a step batches independent
+// frames -- become the nodes of a dependency graph over the data each one reads and
+// writes.  Stream capture over a few lanes (streams forked from the graph's stream and
+// joined back to it) turns that into a CUDA graph whose independent branches run
+// concurrently: one frame's single-CTA corner pick beside another frame's stencils, the
+// upload of frame i+1 beside the kernels of frame i.  Host-imported images whose memory is
+// page-locked are uploaded and downloaded inside the CUDA graph, on lanes of their own, so
+// vxProcessGraph overlaps the PCIe copies with the kernels.
+constexpr int kComputeLanes = 4;
+constexpr int kUploadLane = kComputeLanes, kDownloadLane = kComputeLanes + 1, kNumLanes = kComputeLanes + 2;
+
+struct CapPart {
+    std::function<int(cudaStream_t)> launch;
+    std::vector<Ref *> rd, wr;
+    bool barrier = false;          // touches unknown data: ordered after and before everything
+    int lane = 0;
+    std::vector<int> deps;
+    cudaEvent_t done = nullptr;    // recorded after the part when another lane waits for it
+};
+
+static bool host_pinned(const void *p)
+{
+    cudaPointerAttributes a{};
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Host-imported image that can be copied inside the CUDA graph.
+static bool streamable(Image *root)
+{
+    if (root->import_type != VX_MEMORY_TYPE_HOST || !root->allocated()) return false;
+    for (int i = 0; i < root->num_planes; i++)
+        if (!host_pinned(root->planes[i].host)) return false;
+    return true;
+}
+
+static void collect_touches(Graph *g, const std::vector<LNode *> &nodes, const std::map<Image *, Ref *> &level_of,
+                            CapPart &cp)
+{
+    auto key = [&](Ref *r) -> Ref * {
+        auto rp = g->replaced.find(r);
+        if (rp != g->replaced.end()) r = rp->second;
+        if (r->type == VX_TYPE_IMAGE) {
+            Image *img = IMG(r);
+            auto lv = level_of.find(img);
+            if (lv != level_of.end()) return lv->second;
+            return img->parent ? img->parent : img;
+        }
+        return r;
+    };
+    if (nodes.empty()) { cp.barrier = true; return; }
+    for (LNode *ln : nodes)
+        for (size_t i = 0; i < ln->p.size(); i++) {
+            Ref *r = ln->p[i];
+            if (!r) continue;
+            const bool w = lnode_is_output(*ln, i) || (ln->k == LK::CANNY_EDGE_TRACE_U8_U8XY && i == 0);
+            (w ? cp.wr : cp.rd).push_back(key(r));
+            if (r->type == VX_TYPE_PYRAMID)   // levels aliased to other images (copy removal)
+                for (Image *lv : static_cast<Pyramid *>(r)->level) {
+                    auto rp = g->replaced.find(lv);
+                    if (rp != g->replaced.end()) (w ? cp.wr : cp.rd).push_back(key(rp->second));
+                }
+        }
+}
+
+static void release_capture(Graph *g)
 {
     if (g->cexec) { cudaGraphExecDestroy(g->cexec); g->cexec = nullptr; }
     if (g->cgraph) { cudaGraphDestroy(g->cgraph); g->cgraph = nullptr; }
+    for (cudaEvent_t e : g->cap_events) cudaEventDestroy(e);
+    g->cap_events.clear();
+    g->streamed_in.clear();
+    g->streamed_out.clear();
+}
+
+static cudaEvent_t cap_event(Graph *g)
+{
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    g->cap_events.push_back(e);
+    return e;
+}
+
+static vx_status capture(Graph *g)
+{
+    release_capture(g);
     if (g->optimizer_flags & kOptNoGraphCapture) return VX_SUCCESS;
+    const bool serial = (g->optimizer_flags & (kOptSerial | kOptNoFusion)) != 0;
+
+    // ---- parts, in plan order, with the data they touch
+    std::map<Image *, Ref *> level_of;
+    for (LNode &ln : g->lnodes)
+        for (Ref *r : ln.p)
+            if (r && r->type == VX_TYPE_PYRAMID)
+                for (Image *lv : static_cast<Pyramid *>(r)->level) level_of[lv] = r;
+    std::vector<CapPart> parts;
+    if (!serial)
+        for (Ref *r : g->inputs)
+            if (r->type == VX_TYPE_IMAGE && streamable(IMG(r))) {
+                Image *img = IMG(r);
+                CapPart cp;
+                cp.wr = {img};
+                cp.lane = kUploadLane;
+                cp.launch = [img](cudaStream_t q) {
+                    for (int i = 0; i < img->num_planes; i++) {
+                        const Plane &p = img->planes[i];
+                        if (cudaMemcpy2DAsync(p.dev, p.dev_stride, p.host, p.host_stride, (size_t)p.width * p.bpp, p.height,
+                                              cudaMemcpyHostToDevice, q) != cudaSuccess)
+                            return -1;
+                    }
+                    return 0;
+                };
+                parts.push_back(std::move(cp));
+                g->streamed_in.push_back(img);
+            }
+    for (Step &st : g->steps) {
+        if (st.parts.empty() || serial) {
+            CapPart cp;
+            cp.launch = st.launch;
+            collect_touches(g, st.nodes, level_of, cp);
+            parts.push_back(std::move(cp));
+        } else {
+            for (Part &pt : st.parts) {
+                CapPart cp;
+                cp.launch = pt.launch;
+                collect_touches(g, pt.nodes, level_of, cp);
+                parts.push_back(std::move(cp));
+            }
+        }
+    }
+    if (!serial)
+        for (Ref *r : g->outputs)
+            if (r->type == VX_TYPE_IMAGE && streamable(IMG(r))) {
+                Image *img = IMG(r);
+                CapPart cp;
+                cp.rd = {img};
+                cp.lane = kDownloadLane;
+                cp.launch = [img](cudaStream_t q) {
+                    for (int i = 0; i < img->num_planes; i++) {
+                        const Plane &p = img->planes[i];
+                        if (cudaMemcpy2DAsync(p.host, p.host_stride, p.dev, p.dev_stride, (size_t)p.width * p.bpp, p.height,
+                                              cudaMemcpyDeviceToHost, q) != cudaSuccess)
+                            return -1;
+                    }
+                    return 0;
+                };
+                parts.push_back(std::move(cp));
+                g->streamed_out.push_back(img);
+            }
+
+    // ---- dependencies: read-after-write, write-after-write, write-after-read
+    std::map<Ref *, int> last_writer;
+    std::map<Ref *, std::vector<int>> readers;
+    int last_barrier = -1;
+    for (int j = 0; j < (int)parts.size(); j++) {
+        CapPart &cp = parts[j];
+        std::set<int> d;
+        if (cp.barrier) {
+            for (int i = 0; i < j; i++) d.insert(i);
+            last_barrier = j;
+        } else {
+            if (last_barrier >= 0) d.insert(last_barrier);
+            for (Ref *r : cp.rd) { auto w = last_writer.find(r); if (w != last_writer.end()) d.insert(w->second); }
+            for (Ref *r : cp.wr) {
+                auto w = last_writer.find(r);
+                if (w != last_writer.end()) d.insert(w->second);
+                for (int i : readers[r]) d.insert(i);
+            }
+        }
+        d.erase(j);
+        cp.deps.assign(d.begin(), d.end());
+        for (Ref *r : cp.rd) readers[r].push_back(j);
+        for (Ref *r : cp.wr) { last_writer[r] = j; readers[r].clear(); }
+        if (cp.barrier) { last_writer.clear(); readers.clear(); }
+    }
+
+    // ---- emission order: by the latest upload a part waits for (a stable topological
+    // order, since uploads are sources), so each lane's FIFO takes frames as they arrive
+    std::vector<int> rank(parts.size(), 0), order(parts.size());
+    for (int j = 0, up = 0; j < (int)parts.size(); j++) {
+        if (parts[j].lane == kUploadLane) { rank[j] = ++up; continue; }
+        for (int i : parts[j].deps) rank[j] = std::max(rank[j], rank[i]);
+    }
+    for (int j = 0; j < (int)parts.size(); j++) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rank[a] < rank[b]; });
+    // compute lanes in emission order: follow the latest compute dependency (no extra
+    // ordering), else take the next lane round-robin
+    int rr = 0;
+    for (int j : order) {
+        CapPart &cp = parts[j];
+        if (cp.lane >= kComputeLanes) continue;
+        if (serial) { cp.lane = 0; continue; }
+        int lane = -1, latest = -1;
+        for (int i : cp.deps)
+            if (parts[i].lane < kComputeLanes && i > latest) { latest = i; lane = parts[i].lane; }
+        cp.lane = lane >= 0 ? lane : (rr++ % kComputeLanes);
+    }
+
+    // ---- record
+    cudaSetDevice(g->ctx->device);
+    while ((int)g->lanes.size() < kNumLanes - 1) {
+        cudaStream_t s = nullptr;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return VX_ERROR_NO_RESOURCES;
+        g->lanes.push_back(s);
+    }
+    std::vector<cudaStream_t> lane(kNumLanes);
+    lane[0] = g->stream;   // lane 0 is the graph's own stream
+    for (int i = 1; i < kNumLanes; i++) lane[i] = g->lanes[i - 1];
+    std::vector<bool> used(kNumLanes, false);
+    for (CapPart &cp : parts)
+        for (int i : cp.deps)
+            if (parts[i].lane != cp.lane && !parts[i].done && !(parts[i].done = cap_event(g))) return VX_ERROR_NO_RESOURCES;
+    cudaEvent_t fork = cap_event(g);
+    if (!fork) return VX_ERROR_NO_RESOURCES;
+
     if (cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return VX_FAILURE;
     int rc = 0;
-    for (Step &s : g->steps) { rc = s.launch(g->stream); if (rc) break; }
+    cudaEventRecord(fork, g->stream);
+    used[0] = true;
+    for (size_t o = 0; o < order.size() && !rc; o++) {
+        CapPart &cp = parts[order[o]];
+        cudaStream_t q = lane[cp.lane];
+        if (!used[cp.lane]) { cudaStreamWaitEvent(q, fork, 0); used[cp.lane] = true; }
+        for (int i : cp.deps)
+            if (parts[i].lane != cp.lane) cudaStreamWaitEvent(q, parts[i].done, 0);
+        rc = cp.launch(q);
+        if (cp.done) cudaEventRecord(cp.done, q);
+    }
+    for (int l = 1; l < kNumLanes && !rc; l++) {
+        if (!used[l]) continue;
+        cudaEvent_t e = cap_event(g);
+        if (!e) { rc = -1; break; }
+        cudaEventRecord(e, lane[l]);
+        cudaStreamWaitEvent(g->stream, e, 0);
+    }
     cudaGraph_t cg = nullptr;
     cudaError_t e = cudaStreamEndCapture(g->stream, &cg);
     if (rc || e != cudaSuccess) {
         if (cg) cudaGraphDestroy(cg);
         cudaGetLastError();
+        g->streamed_in.clear();
+        g->streamed_out.clear();
         log_error(g, VX_FAILURE, "ERROR: CUDA graph capture failed (step rc=%d, %s)\n", rc, cudaGetErrorString(e));
         return VX_FAILURE;
     }
@@ -127,6 +361,14 @@ vx_status graph_process(Graph *g, bool wait)
     cudaSetDevice(g->ctx->device);
     for (Ref *r : g->inputs) {
         vx_status s = VX_SUCCESS;
+        const bool streamed = std::find(g->streamed_in.begin(), g->streamed_in.end(), r) != g->streamed_in.end();
+        if (streamed) {
+            // the CUDA graph uploads the application's buffer: make sure that buffer is current
+            Image *img = IMG(r);
+            if (!img->host_valid && img->dev_valid) s = image_sync_to_host(img);
+            if (s) return s;
+            continue;
+        }
         if (r->type == VX_TYPE_IMAGE) s = image_sync_to_device(IMG(r), g->stream);
         else if (r->type == VX_TYPE_ARRAY) s = array_sync_to_device(static_cast<Array *>(r), g->stream);
         else if (r->type == VX_TYPE_PYRAMID)
@@ -142,11 +384,14 @@ vx_status graph_process(Graph *g, bool wait)
         for (Step &s : g->steps) { rc = s.launch(g->stream); if (rc) break; }
     }
     cudaEventRecord(g->ev1, g->stream);
-    // outputs are now current on the device only
+    for (Image *img : g->streamed_in) img->dev_valid = true;
+    // outputs are now current on the device only (and in the application's buffer when
+    // the CUDA graph downloads them)
     for (Ref *r : g->outputs) {
         if (r->type == VX_TYPE_IMAGE) {
             Image *root = IMG(r)->parent ? IMG(r)->parent : IMG(r);
-            root->dev_valid = true; root->host_valid = false;
+            root->dev_valid = true;
+            root->host_valid = std::find(g->streamed_out.begin(), g->streamed_out.end(), root) != g->streamed_out.end();
         } else if (r->type == VX_TYPE_ARRAY) {
             static_cast<Array *>(r)->dev_valid = true; static_cast<Array *>(r)->host_valid = false;
         } else if (r->type == VX_TYPE_SCALAR) {

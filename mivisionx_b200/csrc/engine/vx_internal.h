@@ -190,11 +190,19 @@ struct LNode {
 };
 
 // One unit of device work in the execution plan: recorded into the CUDA graph.
+// A piece of a step that can be ordered on its own: a batched step over independent
+// frames splits into one part per frame.
+struct Part {
+    std::function<int(cudaStream_t)> launch;
+    std::vector<LNode *> nodes;                 // lowered nodes the part covers
+};
+
 struct Step {
     std::string name;
     std::function<int(cudaStream_t)> launch;   // returns 0 or an agocuda/cuda error
     int num_kernels = 1;
     std::vector<LNode *> nodes;                 // lowered nodes this step covers
+    std::vector<Part> parts;                    // optional split of `launch`, in launch order
 };
 
 struct Graph : Ref {
@@ -213,6 +221,9 @@ struct Graph : Ref {
     cudaGraph_t cgraph = nullptr;
     cudaGraphExec_t cexec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaStream_t> lanes;             // streams forked from `stream` during capture
+    std::vector<cudaEvent_t> cap_events;         // fork/join/dependency events of the capture
+    std::vector<Image *> streamed_in, streamed_out;  // host images copied inside the CUDA graph
     bool scheduled = false;
     vx_status last_status = VX_SUCCESS;
     vx_perf_t perf{};
@@ -242,6 +253,7 @@ struct Context : Ref {
 constexpr uint32_t kOptNoDivide = 0x1, kOptNoRemoveCopy = 0x2, kOptNoRemoveUnused = 0x4, kOptNoMerge = 0x8;
 constexpr uint32_t kOptNoFusion = 0x00010000;       // one launch per lowered node ("plain" form)
 constexpr uint32_t kOptNoGraphCapture = 0x00020000; // launch steps directly instead of a CUDA graph
+constexpr uint32_t kOptSerial = 0x00040000;         // capture on one stream (no concurrent branches)
 
 // helpers implemented in vx_objects.cpp
 void add_ref(Context *ctx, Ref *r);
@@ -270,6 +282,7 @@ void graph_invalidate(Graph *g);
 vx_status lower_graph(Graph *g);
 vx_status plan_graph(Graph *g);
 vx_status propagate_valid_rects(Graph *g);
+bool lnode_is_output(const LNode &ln, size_t i);
 
 // scalar value accessors
 inline int32_t sc_i32(Ref *r) { return static_cast<Scalar *>(r)->v.i32; }

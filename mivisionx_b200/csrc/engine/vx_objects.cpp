@@ -369,6 +369,8 @@ Graph::~Graph()
     if (cgraph) cudaGraphDestroy(cgraph);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t e : cap_events) cudaEventDestroy(e);
+    for (cudaStream_t s : lanes) cudaStreamDestroy(s);
     if (stream) cudaStreamDestroy(stream);
     for (void *p : dev_scratch) cudaFree(p);
     if (status_host) cudaFreeHost(status_host);

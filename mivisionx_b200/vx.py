@@ -281,6 +281,19 @@ class OpenVX:
         self.ok(self.vxQueryImage(img, VX_IMAGE_FORMAT, C.byref(f), 4), "query")
         return w.value, h.value, f.value
 
+    def image_from_host(self, ctx, arr: np.ndarray, fmt=None):
+        """vxCreateImageFromHandle(VX_MEMORY_TYPE_HOST) over an application-owned (H, W)
+        uint8 buffer.  The buffer must outlive the image; when it is page-locked, graphs
+        copy it in (and, for outputs, back) inside their CUDA graph."""
+        h, w = arr.shape[:2]
+        addr = vx_imagepatch_addressing_t()
+        addr.dim_x, addr.dim_y, addr.stride_x, addr.stride_y = w, h, arr.strides[1], arr.strides[0]
+        addr.scale_x = addr.scale_y = 1024
+        addr.step_x = addr.step_y = 1
+        ptrs = (C.c_void_p * 1)(arr.ctypes.data)
+        return self.obj(self.vxCreateImageFromHandle(ctx, VX_DF_IMAGE_U8 if fmt is None else fmt, C.byref(addr), ptrs,
+                                                     VX_MEMORY_TYPE_HOST), "image from handle")
+
     def write_plane(self, img, arr: np.ndarray, plane: int = 0, full_w=None, full_h=None):
         """Copy host pixels into plane `plane` (vxCopyImagePatch WRITE_ONLY)."""
         arr = np.ascontiguousarray(arr)

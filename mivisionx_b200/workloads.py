@@ -123,7 +123,7 @@ def cfg4_pair(seed: int, width: int, height: int, max_shift: float = 8.0, noise_
     bot = a[y0 + 1][:, x0] * (1 - fx) + a[y0 + 1][:, x0 + 1] * fx
     f2 = top * (1 - fy)[:, None] + bot * fy[:, None]
     f2 += noise_sigma * gaussian(seed, width * height, stream=29).reshape(height, width)
-    return f1, np.clip(np.rint(f2), 0, 255).astype(np.uint8), (float(dx), float(dy))
+    return f1, np.ascontiguousarray(np.clip(np.rint(f2), 0, 255).astype(np.uint8)), (float(dx), float(dy))
 
 
 KEYPOINT_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("strength", "<f4"), ("scale", "<f4"),
@@ -182,12 +182,21 @@ def cfg3_affine(seed: int = 3, cx: float = 960.0, cy: float = 540.0) -> np.ndarr
 
 
 # ---------------------------------------------------------------- graph builders
+def _u8_image(a: V.OpenVX, ctx, w: int, h: int, bufs, i: int):
+    """Image i of a graph: from the application buffer bufs[i] when given, else allocated."""
+    if bufs is not None:
+        return a.image_from_host(ctx, bufs[i])
+    return a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+
+
 class Cfg1Graph:
     """Gaussian3x3 -> Sobel3x3 -> Magnitude -> ConvertDepth(SATURATE, shift) -> Threshold(BINARY)
     for each of `sizes` frames, all in ONE OpenVX graph (independent sub-graphs), border
     UNDEFINED, intermediates virtual."""
 
-    def __init__(self, api: V.OpenVX, ctx, sizes, shift: int = 0, thr: int = 128, flags: int | None = None):
+    def __init__(self, api: V.OpenVX, ctx, sizes, shift: int = 0, thr: int = 128, flags: int | None = None,
+                 host_io: dict | None = None):
+        host_io = host_io or {}
         self.api, self.ctx = api, ctx
         a = api
         self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
@@ -197,9 +206,9 @@ class Cfg1Graph:
         self.shift = a.scalar(ctx, V.VX_TYPE_INT32, shift)
         self.thr = a.threshold_binary(ctx, thr)
         g = self.graph
-        for (w, h) in sizes:
-            src = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
-            dst = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+        for i, (w, h) in enumerate(sizes):
+            src = _u8_image(a, ctx, w, h, host_io.get("src"), i)
+            dst = _u8_image(a, ctx, w, h, host_io.get("dst"), i)
             gau = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_U8)
             gx = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_S16)
             gy = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_S16)
@@ -293,7 +302,8 @@ class Cfg2Graph:
     input, for each of `sizes` frames, all in one OpenVX graph."""
 
     def __init__(self, api: V.OpenVX, ctx, sizes, lower=80, upper=100, k=0.04, strength=1e-3, min_distance=5.0,
-                 capacity=32768, flags: int | None = None):
+                 capacity=32768, flags: int | None = None, host_io: dict | None = None):
+        host_io = host_io or {}
         self.api, self.ctx = api, ctx
         a = api
         self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
@@ -305,9 +315,9 @@ class Cfg2Graph:
         self.s_k = a.scalar(ctx, V.VX_TYPE_FLOAT32, k)
         self.inputs, self.edges, self.corners, self.num = [], [], [], []
         g = self.graph
-        for (w, h) in sizes:
-            src = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
-            edge = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+        for i, (w, h) in enumerate(sizes):
+            src = _u8_image(a, ctx, w, h, host_io.get("src"), i)
+            edge = _u8_image(a, ctx, w, h, host_io.get("edge"), i)
             arr = a.obj(a.vxCreateArray(ctx, V.VX_TYPE_KEYPOINT, capacity), "array")
             num = a.scalar(ctx, V.VX_TYPE_SIZE, 0)
             a.obj(a.vxCannyEdgeDetectorNode(g, src, self.hyst, 3, V.VX_NORM_L1, edge), "canny node")
@@ -337,7 +347,9 @@ class Cfg4Graph:
     (use_initial_estimate false)."""
 
     def __init__(self, api: V.OpenVX, ctx, sizes, levels=5, window=9, iterations=20, epsilon=0.01,
-                 termination=None, capacity=2000, flags: int | None = None, virtual_pyramids=True):
+                 termination=None, capacity=2000, flags: int | None = None, virtual_pyramids=True,
+                 host_io: dict | None = None):
+        host_io = host_io or {}
         self.api, self.ctx = api, ctx
         a = api
         self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
@@ -349,9 +361,9 @@ class Cfg4Graph:
         self.s_est = a.scalar(ctx, V.VX_TYPE_BOOL, 0)
         self.old, self.new, self.pts, self.out, self.pyr = [], [], [], [], []
         g = self.graph
-        for (w, h) in sizes:
-            i0 = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
-            i1 = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_U8), "image")
+        for i, (w, h) in enumerate(sizes):
+            i0 = _u8_image(a, ctx, w, h, host_io.get("old"), i)
+            i1 = _u8_image(a, ctx, w, h, host_io.get("new"), i)
             if virtual_pyramids:
                 p0 = a.obj(a.vxCreateVirtualPyramid(g, levels, V.VX_SCALE_PYRAMID_HALF, w, h, V.VX_DF_IMAGE_U8), "pyramid")
                 p1 = a.obj(a.vxCreateVirtualPyramid(g, levels, V.VX_SCALE_PYRAMID_HALF, w, h, V.VX_DF_IMAGE_U8), "pyramid")

@@ -44,12 +44,26 @@ def inputs(sizes, execution, n):
     return pairs, points
 
 
-def run_and_compare(api, ctx, sizes, n, flags=None, levels=5, window=9, executions=2, virtual=True):
-    g = WL.Cfg4Graph(api, ctx, sizes, levels=levels, window=window, capacity=n, flags=flags, virtual_pyramids=virtual)
+def run_and_compare(api, ctx, sizes, n, flags=None, levels=5, window=9, executions=2, virtual=True, host=False):
+    """host: frames in page-locked application buffers (images from handles), which the
+    CUDA graph uploads itself."""
+    keep = []
+    if host:
+        import torch
+        keep = [torch.zeros((h, w), dtype=torch.uint8).pin_memory() for w, h in sizes for _ in range(2)]
+    host_io = {"old": [t.numpy() for t in keep[0::2]], "new": [t.numpy() for t in keep[1::2]]} if host else None
+    g = WL.Cfg4Graph(api, ctx, sizes, levels=levels, window=window, capacity=n, flags=flags, virtual_pyramids=virtual,
+                     host_io=host_io)
     orc = OracleGraph(sizes, n, levels, window, 20, 0.01, V.VX_TERM_CRITERIA_BOTH)
     for e in range(executions):
         pairs, points = inputs(sizes, e, n)
-        g.set_inputs(pairs, points)
+        if host:
+            for i, ((f1, f2), kp) in enumerate(zip(pairs, points)):
+                keep[2 * i].numpy()[:] = f1
+                keep[2 * i + 1].numpy()[:] = f2
+                api.array_set(g.pts[i], kp)
+        else:
+            g.set_inputs(pairs, points)
         g.run()
         got = g.results()
         want = orc.run(pairs, points)
@@ -89,3 +103,18 @@ def test_engine_cfg4_non_virtual_pyramids(cuda):
     api = V.OpenVX()
     ctx = api.obj(api.vxCreateContext(), "context")
     run_and_compare(api, ctx, [(640, 480), (320, 240)], 1000, virtual=False)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True])
+def test_engine_cfg4_launch_groups(cuda, host):
+    """11 pairs: the batched pyramid and LK steps launch over groups of 8 pairs, and with
+    page-locked frame buffers each group starts as soon as its frames are uploaded."""
+    api = V.OpenVX()
+    ctx = api.obj(api.vxCreateContext(), "context")
+    # every level narrower than 8 px or with width % 8 < 3 (second executions, see the
+    # top-level Scharr columns the reference leaves from the previous execution)
+    sizes = [[(384, 288), (128, 96), (256, 200)][i % 3] for i in range(11)]
+    g = run_and_compare(api, ctx, sizes, 300, host=host)
+    plan = dict(api.plan(g.graph))
+    assert plan["batch_ScaleGaussianHalf x22"] == 2 and plan["batch_OpticalFlowPyrLK x11"] == 4, plan
