@@ -417,6 +417,23 @@ int agocuda_OpticalFlowPyrLK_XY_XY(void *stream, void *newKeyPoint, uint32_t new
                                    uint32_t numIterations, int32_t useInitialEstimate, int32_t windowDimension,
                                    void *scratch, size_t scratchBytes, uint32_t *pStatus);
 
+/* ------------------------------------------------------------------------------------ */
+/* Array transfers inside a captured CUDA graph (engine internals; no HIP counterpart: the */
+/* reference copies an array's count word, then its items, with blocking copies in        */
+/* agoGpuHipDataInputSync / agoGpuHipDataOutputSync, ago_util_hip.cpp:321-608).          */
+/* hostItemsMapped and countSlotMapped are DEVICE aliases of page-locked host memory     */
+/* (cudaHostRegister/cudaHostAlloc with the mapped flag).                                */
+/* ------------------------------------------------------------------------------------ */
+#define AGOCUDA_ARRAY_SKIP 0xFFFFFFFFu   /* upload count slot: leave the device array as it is */
+
+/* devItems[0 .. n) = hostItems[0 .. n), *devCount = n, n = min(*countSlot, capacity);
+ * nothing when *countSlot == AGOCUDA_ARRAY_SKIP. */
+int agocuda_array_upload(void *stream, void *devItems, uint32_t *devCount, const void *hostItemsMapped,
+                         const uint32_t *countSlotMapped, uint32_t itemSize, uint32_t capacity);
+/* hostItems[0 .. n) = devItems[0 .. n), *countSlot = n, n = min(*devCount, capacity). */
+int agocuda_array_download(void *stream, void *hostItemsMapped, uint32_t *countSlotMapped, const void *devItems,
+                           const uint32_t *devCount, uint32_t itemSize, uint32_t capacity);
+
 #ifdef __cplusplus
 }
 #endif

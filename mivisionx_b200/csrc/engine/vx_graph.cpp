@@ -72,7 +72,10 @@ static uint64_t param_signature(Graph *g)
 // page-locked are uploaded and downloaded inside the CUDA graph, on lanes of their own, so
 // vxProcessGraph overlaps the PCIe copies with the kernels.
 constexpr int kComputeLanes = 4;
-constexpr int kUploadLane = kComputeLanes, kDownloadLane = kComputeLanes + 1, kNumLanes = kComputeLanes + 2;
+// image uploads and downloads (copy engines) and array transfers (small kernels reading or
+// writing mapped host memory) get lanes of their own, so none waits behind another kind
+constexpr int kUploadLane = kComputeLanes, kDownloadLane = kComputeLanes + 1, kArrayLane = kComputeLanes + 2;
+constexpr int kNumLanes = kComputeLanes + 3;
 
 struct CapPart {
     std::function<int(cudaStream_t)> launch;
@@ -128,6 +131,42 @@ static void collect_touches(Graph *g, const std::vector<LNode *> &nodes, const s
         }
 }
 
+// Array whose items can cross PCIe inside the CUDA graph: its host buffer (allocated at
+// capacity when the array is created) is page-locked and mapped once, here.
+static bool stageable(Array *a)
+{
+    if (a->is_virtual || !a->dev || !a->dev_count || a->host.empty() || a->host.size() < a->capacity * a->item_size)
+        return false;
+    if (!a->host_mapped) {
+        if (cudaHostRegister(a->host.data(), a->host.size(), cudaHostRegisterMapped) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        void *d = nullptr;
+        if (cudaHostGetDevicePointer(&d, a->host.data(), 0) != cudaSuccess) {
+            cudaHostUnregister(a->host.data());
+            cudaGetLastError();
+            return false;
+        }
+        a->host_mapped = (uint8_t *)d;
+    }
+    return true;
+}
+
+// host <-> device copy of one plane; one linear copy when both layouts are packed
+static cudaError_t plane_copy(const Plane &p, cudaMemcpyKind kind, cudaStream_t q)
+{
+    const size_t row = (size_t)p.width * p.bpp;
+    const bool h2d = kind == cudaMemcpyHostToDevice;
+    void *dst = h2d ? (void *)p.dev : (void *)p.host;
+    const void *src = h2d ? (const void *)p.host : (const void *)p.dev;
+    if (p.host_stride == row && p.dev_stride == row) return cudaMemcpyAsync(dst, src, row * p.height, kind, q);
+    return h2d ? cudaMemcpy2DAsync(dst, p.dev_stride, src, p.host_stride, row, p.height, kind, q)
+               : cudaMemcpy2DAsync(dst, p.host_stride, src, p.dev_stride, row, p.height, kind, q);
+}
+
+constexpr size_t kIoSlots = 1024;   // count slots per graph (arrays staged beyond this use blocking copies)
+
 static void release_capture(Graph *g)
 {
     if (g->cexec) { cudaGraphExecDestroy(g->cexec); g->cexec = nullptr; }
@@ -136,6 +175,8 @@ static void release_capture(Graph *g)
     g->cap_events.clear();
     g->streamed_in.clear();
     g->streamed_out.clear();
+    g->staged_in.clear();
+    g->staged_out.clear();
 }
 
 static cudaEvent_t cap_event(Graph *g)
@@ -159,6 +200,27 @@ static vx_status capture(Graph *g)
             if (r && r->type == VX_TYPE_PYRAMID)
                 for (Image *lv : static_cast<Pyramid *>(r)->level) level_of[lv] = r;
     std::vector<CapPart> parts;
+    if (!serial && !g->io_slots_host) {
+        if (cudaHostAlloc((void **)&g->io_slots_host, kIoSlots * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostGetDevicePointer((void **)&g->io_slots_dev, g->io_slots_host, 0) != cudaSuccess)
+            return VX_ERROR_NO_MEMORY;
+    }
+    auto slot_free = [&]() { return g->staged_in.size() + g->staged_out.size() < kIoSlots; };
+    if (!serial)
+        for (Ref *r : g->inputs)
+            if (r->type == VX_TYPE_ARRAY && slot_free() && stageable(static_cast<Array *>(r))) {
+                Array *a = static_cast<Array *>(r);
+                const uint32_t *slot = g->io_slots_dev + g->staged_in.size();
+                CapPart cp;
+                cp.wr = {a};
+                cp.lane = kArrayLane;
+                cp.launch = [a, slot](cudaStream_t q) {
+                    return agocuda_array_upload(q, a->dev, a->dev_count, a->host_mapped, slot, (uint32_t)a->item_size,
+                                                (uint32_t)a->capacity);
+                };
+                parts.push_back(std::move(cp));
+                g->staged_in.push_back(a);
+            }
     if (!serial)
         for (Ref *r : g->inputs)
             if (r->type == VX_TYPE_IMAGE && streamable(IMG(r))) {
@@ -167,12 +229,8 @@ static vx_status capture(Graph *g)
                 cp.wr = {img};
                 cp.lane = kUploadLane;
                 cp.launch = [img](cudaStream_t q) {
-                    for (int i = 0; i < img->num_planes; i++) {
-                        const Plane &p = img->planes[i];
-                        if (cudaMemcpy2DAsync(p.dev, p.dev_stride, p.host, p.host_stride, (size_t)p.width * p.bpp, p.height,
-                                              cudaMemcpyHostToDevice, q) != cudaSuccess)
-                            return -1;
-                    }
+                    for (int i = 0; i < img->num_planes; i++)
+                        if (plane_copy(img->planes[i], cudaMemcpyHostToDevice, q) != cudaSuccess) return -1;
                     return 0;
                 };
                 parts.push_back(std::move(cp));
@@ -201,16 +259,27 @@ static vx_status capture(Graph *g)
                 cp.rd = {img};
                 cp.lane = kDownloadLane;
                 cp.launch = [img](cudaStream_t q) {
-                    for (int i = 0; i < img->num_planes; i++) {
-                        const Plane &p = img->planes[i];
-                        if (cudaMemcpy2DAsync(p.host, p.host_stride, p.dev, p.dev_stride, (size_t)p.width * p.bpp, p.height,
-                                              cudaMemcpyDeviceToHost, q) != cudaSuccess)
-                            return -1;
-                    }
+                    for (int i = 0; i < img->num_planes; i++)
+                        if (plane_copy(img->planes[i], cudaMemcpyDeviceToHost, q) != cudaSuccess) return -1;
                     return 0;
                 };
                 parts.push_back(std::move(cp));
                 g->streamed_out.push_back(img);
+            }
+    if (!serial)
+        for (Ref *r : g->outputs)
+            if (r->type == VX_TYPE_ARRAY && slot_free() && stageable(static_cast<Array *>(r))) {
+                Array *a = static_cast<Array *>(r);
+                uint32_t *slot = g->io_slots_dev + g->staged_in.size() + g->staged_out.size();
+                CapPart cp;
+                cp.rd = {a};
+                cp.lane = kArrayLane;
+                cp.launch = [a, slot](cudaStream_t q) {
+                    return agocuda_array_download(q, a->host_mapped, slot, a->dev, a->dev_count, (uint32_t)a->item_size,
+                                                  (uint32_t)a->capacity);
+                };
+                parts.push_back(std::move(cp));
+                g->staged_out.push_back(a);
             }
 
     // ---- dependencies: read-after-write, write-after-write, write-after-read
@@ -305,6 +374,8 @@ static vx_status capture(Graph *g)
         cudaGetLastError();
         g->streamed_in.clear();
         g->streamed_out.clear();
+        g->staged_in.clear();
+        g->staged_out.clear();
         log_error(g, VX_FAILURE, "ERROR: CUDA graph capture failed (step rc=%d, %s)\n", rc, cudaGetErrorString(e));
         return VX_FAILURE;
     }
@@ -370,7 +441,17 @@ vx_status graph_process(Graph *g, bool wait)
             continue;
         }
         if (r->type == VX_TYPE_IMAGE) s = image_sync_to_device(IMG(r), g->stream);
-        else if (r->type == VX_TYPE_ARRAY) s = array_sync_to_device(static_cast<Array *>(r), g->stream);
+        else if (r->type == VX_TYPE_ARRAY) {
+            Array *a = static_cast<Array *>(r);
+            auto it = std::find(g->staged_in.begin(), g->staged_in.end(), a);
+            if (it != g->staged_in.end()) {
+                // the CUDA graph uploads the host items unless the device copy is current
+                g->io_slots_host[it - g->staged_in.begin()] =
+                    a->dev_valid ? AGOCUDA_ARRAY_SKIP : (uint32_t)std::min(a->num_items, a->capacity);
+                continue;
+            }
+            s = array_sync_to_device(a, g->stream);
+        }
         else if (r->type == VX_TYPE_PYRAMID)
             for (Image *lv : static_cast<Pyramid *>(r)->level) if (!s) s = image_sync_to_device(lv, g->stream);
         if (s) return s;
@@ -385,6 +466,7 @@ vx_status graph_process(Graph *g, bool wait)
     }
     cudaEventRecord(g->ev1, g->stream);
     for (Image *img : g->streamed_in) img->dev_valid = true;
+    for (Array *a : g->staged_in) a->dev_valid = true;
     // outputs are now current on the device only (and in the application's buffer when
     // the CUDA graph downloads them)
     for (Ref *r : g->outputs) {
@@ -428,6 +510,12 @@ vx_status graph_wait(Graph *g)
         return VX_FAILURE;
     }
     cudaEventElapsedTime(&g->gpu_ms_last, g->ev0, g->ev1);
+    // arrays the CUDA graph downloaded: their host buffers and counts are current
+    for (size_t i = 0; i < g->staged_out.size(); i++) {
+        Array *a = g->staged_out[i];
+        a->num_items = std::min((vx_size)g->io_slots_host[g->staged_in.size() + i], a->capacity);
+        a->host_valid = true;
+    }
     // kernels that detect a failure (bounded walks, candidate overflow) set status bits
     if (g->status_host && *(volatile uint32_t *)g->status_host) {
         const uint32_t st = *g->status_host;

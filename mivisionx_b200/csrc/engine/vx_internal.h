@@ -117,6 +117,7 @@ struct Array : Ref {
     std::vector<uint8_t> host;
     vx_size num_items = 0;
     bool host_valid = true, dev_valid = false;
+    uint8_t *host_mapped = nullptr;   // device alias of `host` once it is page-locked (graph staging)
     std::map<vx_map_id, std::pair<vx_size, vx_enum>> maps;
     vx_map_id next_map = 1;
     ~Array() override;
@@ -224,6 +225,10 @@ struct Graph : Ref {
     std::vector<cudaStream_t> lanes;             // streams forked from `stream` during capture
     std::vector<cudaEvent_t> cap_events;         // fork/join/dependency events of the capture
     std::vector<Image *> streamed_in, streamed_out;  // host images copied inside the CUDA graph
+    // arrays copied inside the CUDA graph through their page-locked host buffers, with one
+    // mapped count slot each (io_slots_host[i] <-> staged_in / staged_out in that order)
+    std::vector<Array *> staged_in, staged_out;
+    uint32_t *io_slots_host = nullptr, *io_slots_dev = nullptr;
     bool scheduled = false;
     vx_status last_status = VX_SUCCESS;
     vx_perf_t perf{};

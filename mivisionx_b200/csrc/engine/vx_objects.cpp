@@ -265,6 +265,7 @@ static void mark_written_on_device(Image *img)
 // ---------------------------------------------------------------- arrays / scalars
 Array::~Array()
 {
+    if (host_mapped) cudaHostUnregister(host.data());
     if (dev) cudaFree(dev);
     if (dev_count) cudaFree(dev_count);
 }
@@ -374,6 +375,7 @@ Graph::~Graph()
     if (stream) cudaStreamDestroy(stream);
     for (void *p : dev_scratch) cudaFree(p);
     if (status_host) cudaFreeHost(status_host);
+    if (io_slots_host) cudaFreeHost(io_slots_host);
 }
 
 }  // namespace agovx
