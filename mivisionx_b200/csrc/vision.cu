@@ -233,8 +233,8 @@ __global__ void k_hyst_output(int W, int H, uint8_t *out, int outStride, const i
 // non-zero pixels that hold a strong (255) pixel.
 // ---------------------------------------------------------------------------------
 constexpr int kTW = 64, kTH = 32, kTS = kTW * kTH;   // tile and its slot count
-constexpr int kIW = kTW + 4, kIH = kTH + 4;          // input tile (halo 2)
-constexpr int kGW = kTW + 2, kGH = kTH + 2;          // gradient tile (halo 1)
+constexpr int kIH = kTH + 4;                         // input tile rows (halo 2)
+constexpr int kGH = kTH + 2;                         // gradient tile rows (halo 1)
 constexpr uint16_t kNoLabel = 0xFFFF;
 
 __device__ __forceinline__ int sfind(const int *lab, int x)
@@ -260,28 +260,63 @@ __device__ __forceinline__ void sunion(int *lab, int a, int b)
     }
 }
 
-__global__ void __launch_bounds__(256)
+// --- front end: one block per 64x32 tile, 256 threads -----------------------------
+// Input tile as words: rows y0-2 .. y0+33, columns x0-4 .. x0+67 (18 words of 4 pixels);
+// gradient tile rows y0-1 .. y0+32 over the same 72 columns (the outer ones are unused).
+constexpr int kInWords = (kTW + 8) / 4, kGC = kTW + 8;
+
+// One row's 6 pixels X[-1..4] around a 4-pixel word C (L, R: the words either side) as
+// 16-bit lane pairs: E = (X0, X2), O = (X1, X3), Om = (X-1, X1), Ep = (X2, X4).
+struct Lanes4 { uint32_t E, O, Om, Ep; };
+__device__ __forceinline__ Lanes4 lanes4(uint32_t L, uint32_t C, uint32_t R)
+{
+    Lanes4 v;
+    v.E = __byte_perm(C, 0, 0x4240);
+    v.O = __byte_perm(C, 0, 0x4341);
+    v.Om = __byte_perm(L, v.O, 0x5453);
+    v.Ep = __byte_perm(v.E, R, 0x3432);
+    return v;
+}
+
+// canny_pack for a gradient held as lanes biased by 1024
+__device__ __forceinline__ uint32_t canny_pack_biased(uint32_t bx, uint32_t by)
+{
+    return canny_pack((int)bx - 1024, (int)by - 1024);
+}
+
+__device__ __forceinline__ int sG_mag3(uint32_t g) { return (int)(g | 3u); }   // (mag << 2) | 3: compares as mag
+
+__global__ void __launch_bounds__(256, 4)
 k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, int lower, int upper,
                   uint16_t *__restrict__ lab16, int labPitch, int *__restrict__ uf, uint32_t *__restrict__ bits)
 {
-    __shared__ uint8_t sIn[kIH][kIW];
-    __shared__ uint16_t sG[kGH][kGW];
-    __shared__ int16_t sV[kIH];              // per tile row: vertical sum of column W-1 (x == 0 quirk)
-    __shared__ int sLab[kTS];
-    __shared__ uint32_t sStrongPx[kTS / 32], sStrongRoot[kTS / 32];
+    __shared__ __align__(16) uint32_t sIn[kIH][kInWords];
+    __shared__ __align__(16) uint16_t sG[kGH][kGC];
+    __shared__ __align__(16) int sLab[kTS];
+    __shared__ unsigned long long sNZ[kTH], sST[kTH];   // per tile row: non-zero / strong pixels
+    __shared__ int16_t sV[kIH];                          // per gradient row: vertical sum of column W-1
+    __shared__ uint32_t sStrongRoot[kTS / 32];
     const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH, tid = threadIdx.x;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x;
 
-    // ---- input with a 2-pixel halo; the border tiles follow the reference's reads outside rows
-    const bool inner = x0 >= 2 && y0 >= 2 && x0 + kTW + 2 <= W && y0 + kTH + 2 <= H;
-    for (int i = tid; i < kIH * kIW; i += blockDim.x) {
-        const int r = i / kIW, c = i % kIW;
-        sIn[r][c] = inner ? __ldg(src + (size_t)(y0 - 2 + r) * srcStride + x0 - 2 + c)
-                          : (uint8_t)ago_px(src, srcStride, W, H, x0 - 2 + c, y0 - 2 + r);
+    // ---- input words; border tiles follow the reference's reads outside rows (ago_px)
+    const bool inner = x0 >= 4 && y0 >= 2 && x0 + kTW + 4 <= W && y0 + kTH + 2 <= H &&
+                       (((uintptr_t)src | (uintptr_t)srcStride) & 3) == 0;
+    for (int i = tid; i < kIH * kInWords; i += blockDim.x) {
+        const int r = i / kInWords, q = i - r * kInWords;
+        const int y = y0 - 2 + r, x = x0 - 4 + 4 * q;
+        uint32_t w;
+        if (inner) {
+            w = __ldg((const uint32_t *)(src + (size_t)y * srcStride + x));
+        } else {
+            w = 0;
+            for (int k = 0; k < 4; k++) w |= (uint32_t)ago_px(src, srcStride, W, H, x + k, y) << (8 * k);
+        }
+        sIn[r][q] = w;
     }
     if (tid < kTS / 32) sStrongRoot[tid] = 0;
     const bool needV = x0 == 0 && (W & 15) == 0 && W >= 16;
-    if (needV && tid < kIH - 2) {
+    if (needV && tid < kGH) {
         const int y = y0 - 1 + tid;
         sV[tid] = (y >= 1 && y < H - 1)
             ? (int16_t)(ago_px(src, srcStride, W, H, W - 1, y - 1) + 2 * ago_px(src, srcStride, W, H, W - 1, y) +
@@ -289,57 +324,152 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
             : 0;
     }
     __syncthreads();
-    // ---- packed gradient with a 1-pixel halo
-    for (int i = tid; i < kGH * kGW; i += blockDim.x) {
-        const int r = i / kGW, c = i % kGW;
-        const int x = x0 - 1 + c, y = y0 - 1 + r;
-        uint16_t g = 0;
-        if (y >= 1 && y < H - 1 && x >= 0 && x < W) {
-            auto P = [&](int dx, int dy) { return (int)sIn[r + 1 + dy][c + 1 + dx]; };
-            const bool simd_x0 = x == 0 && W >= 16;
-            g = canny_grad(P, simd_x0, simd_x0 && (W & 15) == 0 ? (int)sV[r] : 0);
+
+    // ---- packed gradient, 4 columns per item, in 16-bit lanes
+    for (int i = tid; i < kGH * kInWords; i += blockDim.x) {
+        const int gr = i / kInWords, q = i - gr * kInWords;
+        const int y = y0 - 1 + gr, xq = x0 - 4 + 4 * q;
+        uint32_t out0 = 0, out1 = 0;
+        if (y >= 1 && y < H - 1) {
+            Lanes4 t, m, b;
+            {
+                const uint32_t *r0 = sIn[gr], *r1 = sIn[gr + 1], *r2 = sIn[gr + 2];
+                const int ql = q > 0 ? q - 1 : q, qr = q + 1 < kInWords ? q + 1 : q;   // edge items: unused columns
+                t = lanes4(r0[ql], r0[q], r0[qr]);
+                m = lanes4(r1[ql], r1[q], r1[qr]);
+                b = lanes4(r2[ql], r2[q], r2[qr]);
+            }
+            const uint32_t vE = t.E + 2 * m.E + b.E, vO = t.O + 2 * m.O + b.O;
+            const uint32_t vOm = t.Om + 2 * m.Om + b.Om, vEp = t.Ep + 2 * m.Ep + b.Ep;
+            const uint32_t bias = 0x04000400u;
+            const uint32_t gx02 = vO + bias - vOm, gx13 = vEp + bias - vE;
+            const uint32_t ts02 = t.Om + 2 * t.E + t.O, ts13 = t.E + 2 * t.O + t.Ep;
+            const uint32_t bs02 = b.Om + 2 * b.E + b.O, bs13 = b.E + 2 * b.O + b.Ep;
+            const uint32_t gy02 = ts02 + bias - bs02, gy13 = ts13 + bias - bs13;   // Gy negated (canny.cpp:79)
+            uint32_t g0 = canny_pack_biased(gx02 & 0xffff, gy02 & 0xffff);
+            uint32_t g1 = canny_pack_biased(gx13 & 0xffff, gy13 & 0xffff);
+            uint32_t g2 = canny_pack_biased(gx02 >> 16, gy02 >> 16);
+            uint32_t g3 = canny_pack_biased(gx13 >> 16, gy13 >> 16);
+            if (xq < 0 || xq + 3 >= W) {   // columns outside the image hold 0
+                if ((unsigned)xq >= (unsigned)W) g0 = 0;
+                if ((unsigned)(xq + 1) >= (unsigned)W) g1 = 0;
+                if ((unsigned)(xq + 2) >= (unsigned)W) g2 = 0;
+                if ((unsigned)(xq + 3) >= (unsigned)W) g3 = 0;
+            }
+            if (xq == 0 && W >= 16) {      // the reference's SIMD-body formula at x = 0
+                const uint8_t *b8 = (const uint8_t *)sIn;
+                auto P = [&](int dx, int dy) { return (int)b8[(gr + 1 + dy) * (kInWords * 4) + 4 + dx]; };
+                g0 = canny_grad(P, true, (W & 15) == 0 ? (int)sV[gr] : 0);
+            }
+            out0 = g0 | (g1 << 16);
+            out1 = g2 | (g3 << 16);
         }
-        sG[r][c] = g;
+        *(uint2 *)&sG[gr][4 * q] = make_uint2(out0, out1);
     }
     __syncthreads();
-    // ---- suppression + thresholds; local labels of the non-zero interior pixels
-    for (int i = tid; i < kTS; i += blockDim.x) {
-        const int r = i / kTW, c = i % kTW, x = x0 + c, y = y0 + r;
-        int v = 0;
-        if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1) {
-            auto G = [&](int dx, int dy) { return (int)sG[r + 1 + dy][c + 1 + dx]; };
-            v = canny_supp(G, lower, upper);
+
+    // ---- suppression + thresholds: 8 pixels of one row per thread; row masks
+    const int r = tid >> 3, sgm = tid & 7, c0 = 8 * sgm;
+    const int y = y0 + r;
+    {
+        int g[3][10];                       // gradient rows y-1 .. y+1, columns c0-1 .. c0+8
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const uint32_t *row = (const uint32_t *)&sG[r + k][c0 + 2];   // columns c0-2 .. c0+9
+            uint32_t w[6];
+#pragma unroll
+            for (int j = 0; j < 6; j++) w[j] = row[j];
+            g[k][0] = (int)(w[0] >> 16);
+#pragma unroll
+            for (int j = 1; j < 5; j++) { g[k][2 * j - 1] = (int)(w[j] & 0xffff); g[k][2 * j] = (int)(w[j] >> 16); }
+            g[k][9] = (int)(w[5] & 0xffff);
         }
-        sLab[i] = v ? i : -1;
-        const unsigned strong = __ballot_sync(0xffffffffu, v == 255);   // i / 32 is warp-uniform
-        if ((tid & 31) == 0) sStrongPx[i >> 5] = strong;
+        uint32_t nz = 0, st = 0;
+        const bool rowIn = y >= 1 && y < H - 1;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int x = x0 + c0 + j;
+            const int c = g[1][j + 1];
+            const int ang = c & 3;
+            // neighbours along the direction (kNOff): 0 W/E, 1 NE/SW, 2 N/S, 3 NW/SE
+            const int a = (ang & 2) ? ((ang & 1) ? g[0][j] : g[0][j + 1]) : ((ang & 1) ? g[0][j + 2] : g[1][j]);
+            const int b = (ang & 2) ? ((ang & 1) ? g[2][j + 2] : g[2][j + 1]) : ((ang & 1) ? g[2][j] : g[1][j + 2]);
+            const int mag = c >> 2;
+            const bool keep = sG_mag3(c) > sG_mag3(a) && sG_mag3(c) > sG_mag3(b);
+            const int edge = keep ? mag : 0;
+            const bool in = rowIn && x >= 1 && x < W - 1;
+            const bool strong = in && edge > upper;   // 255 (canny_supp), else 0 at <= lower, else 127
+            nz |= (uint32_t)(strong || (in && edge > lower)) << j;
+            st |= (uint32_t)strong << j;
+        }
+        ((uint8_t *)&sNZ[r])[sgm] = (uint8_t)nz;
+        ((uint8_t *)&sST[r])[sgm] = (uint8_t)st;
     }
     __syncthreads();
-    // ---- local union-find over the already-visited neighbours inside the tile
-    for (int i = tid; i < kTS; i += blockDim.x) {
-        if (sLab[i] < 0) continue;
-        const int r = i / kTW, c = i % kTW;
-        if (c > 0 && sLab[i - 1] >= 0) sunion(sLab, i, i - 1);
-        if (r > 0) {
-            if (c > 0 && sLab[i - kTW - 1] >= 0) sunion(sLab, i, i - kTW - 1);
-            if (sLab[i - kTW] >= 0) sunion(sLab, i, i - kTW);
-            if (c + 1 < kTW && sLab[i - kTW + 1] >= 0) sunion(sLab, i, i - kTW + 1);
+
+    // ---- provisional labels: every pixel points at the first pixel of its run in the row
+    const unsigned long long m = sNZ[r];
+    const int i0 = r * kTW + c0;
+    {
+        const unsigned long long below = ~m & ((1ull << c0) - 1ull);
+        int start = below ? 64 - __clzll(below) : 0;
+        int lab[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int c = c0 + j;
+            if (j > 0 && !((m >> (c - 1)) & 1)) start = c;
+            lab[j] = ((m >> c) & 1) ? r * kTW + start : -1;
+        }
+        *(int4 *)&sLab[i0] = make_int4(lab[0], lab[1], lab[2], lab[3]);
+        *(int4 *)&sLab[i0 + 4] = make_int4(lab[4], lab[5], lab[6], lab[7]);
+    }
+    __syncthreads();
+    // ---- unions with the row above: one per run of this row and overlapping run above
+    // (N if present, unless the left neighbour already covers it; else NW / NE)
+    if (r > 0) {
+        const unsigned long long a = sNZ[r - 1];
+        const unsigned long long uN = m & a & ~((m << 1) & (a << 1));
+        const unsigned long long uNW = m & ~a & (a << 1) & ~(m << 1);
+        const unsigned long long uNE = m & ~a & (a >> 1) & ~(m >> 1);
+        uint32_t bn = (uint32_t)(uN >> c0) & 0xff, bw = (uint32_t)(uNW >> c0) & 0xff, be = (uint32_t)(uNE >> c0) & 0xff;
+        while (bn) { const int j = __ffs(bn) - 1; bn &= bn - 1; sunion(sLab, i0 + j, i0 + j - kTW); }
+        while (bw) { const int j = __ffs(bw) - 1; bw &= bw - 1; sunion(sLab, i0 + j, i0 + j - kTW - 1); }
+        while (be) { const int j = __ffs(be) - 1; be &= be - 1; sunion(sLab, i0 + j, i0 + j - kTW + 1); }
+    }
+    __syncthreads();
+
+    // ---- roots (the component's smallest pixel index), strong roots, labels out
+    int root[8];
+    {
+        const uint32_t stb = (uint32_t)(sST[r] >> c0) & 0xff;
+        int lastStart = -1, lastRoot = -1, lastOr = -1;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            root[j] = -1;
+            if (!((m >> (c0 + j)) & 1)) continue;
+            const int start = sLab[i0 + j];
+            if (start != lastStart) { lastStart = start; lastRoot = sfind(sLab, start); }
+            root[j] = lastRoot;
+            if (((stb >> j) & 1) && lastRoot != lastOr) {
+                lastOr = lastRoot;
+                atomicOr(&sStrongRoot[lastRoot >> 5], 1u << (lastRoot & 31));
+            }
         }
     }
-    __syncthreads();
-    for (int i = tid; i < kTS; i += blockDim.x)
-        if (sLab[i] >= 0) sLab[i] = sfind(sLab, i);
-    __syncthreads();
-    for (int i = tid; i < kTS; i += blockDim.x)
-        if ((sStrongPx[i >> 5] >> (i & 31)) & 1) atomicOr(&sStrongRoot[sLab[i] >> 5], 1u << (sLab[i] & 31));
-    __syncthreads();
-    // ---- labels out; every local root starts as its own global root; strong-root bits
-    for (int i = tid; i < kTS; i += blockDim.x) {
-        const int r = i / kTW, c = i % kTW, x = x0 + c, y = y0 + r;
-        const int l = sLab[i];
-        if (x < W && y < H) lab16[(size_t)y * labPitch + x] = l >= 0 ? (uint16_t)l : kNoLabel;
-        if (l == i) uf[(size_t)tile * kTS + i] = tile * kTS + i;
+    if (y < H && x0 + c0 < W) {
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t lo = root[2 * j] >= 0 ? (uint32_t)root[2 * j] : kNoLabel;
+            const uint32_t hi = root[2 * j + 1] >= 0 ? (uint32_t)root[2 * j + 1] : kNoLabel;
+            w[j] = lo | (hi << 16);
+        }
+        *(uint4 *)&lab16[(size_t)y * labPitch + x0 + c0] = make_uint4(w[0], w[1], w[2], w[3]);
     }
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+        if (root[j] == i0 + j) uf[(size_t)tile * kTS + i0 + j] = tile * kTS + i0 + j;
+    __syncthreads();
     if (tid < kTS / 32) bits[(size_t)tile * (kTS / 32) + tid] = sStrongRoot[tid];
 }
 
