@@ -653,20 +653,26 @@ __global__ void k_harris_nms(int W, int H, const float *sc, int scStride, uint64
     xys_append(list, count, capacity, xys_pack(x, y, v), keep);
 }
 
-// Harris front end as column strips: a warp owns 26 output columns (lanes 3..28; the outer
-// lanes carry the halo) and walks down 64 output rows with rolling registers.  Per input
-// row a lane loads one byte; three rows travel packed in one word, so two shuffles give the
-// gradient's neighbours.  The Sobel products and their 3x3 window sums are integers below
-// 2^24, i.e. exactly the float sums the reference forms; the score keeps the reference's
-// float operation order, and its division is skipped only where the result cannot exceed
-// the threshold.
-constexpr int kHRows = 64, kHCols = 26;
+// Harris front end as column strips: a warp owns 120 output columns (lanes 1..30, four
+// columns each; lanes 0 and 31 carry the halo) and walks down 32 output rows with rolling
+// registers.  Per input row a lane loads one word; the Sobel sums run in 16-bit lanes
+// (four columns in four registers), the products and window sums in float -- integers
+// below 2^24, i.e. exactly the float sums the reference forms in any order.  The score
+// keeps the reference's float operation order, and its division is skipped only where the
+// result cannot exceed the threshold.
+constexpr int kHRows = 32, kHCols = 120;
 
-__device__ __forceinline__ uint32_t harris_in(const uint8_t *src, int stride, int W, int H, int x, int y)
+__device__ __forceinline__ uint32_t harris_word(const uint8_t *src, int stride, int W, int H, int x, int y, bool fast)
 {
-    if (x >= 0 && x < W && y >= 0 && y < H) return __ldg(src + (size_t)y * stride + x);
-    return (uint32_t)ago_px(src, stride, W, H, x, y);
+    if (fast && y >= 0 && y < H) return __ldg((const uint32_t *)(src + (size_t)y * stride + x));
+    uint32_t w = 0;
+    for (int k = 0; k < 4; k++) w |= (uint32_t)ago_px(src, stride, W, H, x + k, y) << (8 * k);
+    return w;
 }
+
+// biased 16-bit lane (value + 1024) as an exact float
+__device__ __forceinline__ float lane_lo(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8389632.0f; }
+__device__ __forceinline__ float lane_hi(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8389632.0f; }
 
 __global__ void __launch_bounds__(128)
 k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, float k, float Tc, float norm,
@@ -675,63 +681,105 @@ k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, floa
     const int lane = threadIdx.x & 31;
     const int xs = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kHCols;
     if (xs >= W) return;                                   // warp-uniform
-    const int xc = xs + lane - 3;
+    const int xl = xs - 4 + 4 * lane;                      // this lane's columns xl .. xl+3
     const int ys = blockIdx.y * kHRows, yEnd = min(ys + kHRows, H);
-    const bool gradCol = xc >= 0 && xc < W, scoreCol = xc >= 1 && xc < W - 1;
-    const bool outLane = lane >= 3 && lane < 3 + kHCols && scoreCol;
+    const bool fast = ((((uintptr_t)src | (uintptr_t)srcStride) & 3) == 0) && xl >= 0 && xl + 4 <= W;
+    const bool outLane = lane >= 1 && lane <= 30;
+    bool gradCol[4], scoreCol[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        gradCol[c] = xl + c >= 0 && xl + c < W;
+        scoreCol[c] = xl + c >= 1 && xl + c < W - 1;
+    }
     const float cut = Tc > 0.f ? __fmul_rn(0.999f, __fmul_rn(Tc, norm)) : 0.f;   // Mc below: score 0
-    uint32_t rows = 0;                                     // input rows r-2 | r-1 << 8 | r << 16
-    int v0[3] = {0, 0, 0}, v1[3] = {0, 0, 0};              // products at gradient rows g-2, g-1
-    float sA = 0.f, sB = 0.f;                              // scores at rows s-2, s-1
-    uint32_t next = harris_in(src, srcStride, W, H, xc, ys - 3);
+    Lanes4 t{0, 0, 0, 0}, m{0, 0, 0, 0};                   // input rows r-2, r-1 as 16-bit lanes
+    float v0[3][4] = {}, v1[3][4] = {};                     // products at gradient rows g-2, g-1
+    float sA[6] = {}, sB[6] = {};                           // scores (columns -1..4) at rows s-2, s-1
+    uint32_t next = harris_word(src, srcStride, W, H, xl, ys - 3, fast);
     for (int r = ys - 3; r <= yEnd + 2; r++) {
         const uint32_t cur = next;
-        if (r + 1 <= yEnd + 2) next = harris_in(src, srcStride, W, H, xc, r + 1);
-        rows = (rows >> 8) | (cur << 16);
-        // gradient at g = r - 1 from rows r-2, r-1, r
-        const uint32_t Lw = __shfl_up_sync(0xffffffffu, rows, 1), Rw = __shfl_down_sync(0xffffffffu, rows, 1);
+        if (r + 1 <= yEnd + 2) next = harris_word(src, srcStride, W, H, xl, r + 1, fast);
+        const Lanes4 b = lanes4(__shfl_up_sync(0xffffffffu, cur, 1), cur, __shfl_down_sync(0xffffffffu, cur, 1));
+        // gradient at g = r - 1 from rows r-2, r-1, r (HafCpu_HarrisSobel_HG3_U8_3x3, harris.cpp:85)
         const int g = r - 1;
-        int p0 = 0, p1 = 0, p2 = 0;
-        if (gradCol && g >= 1 && g < H - 1) {
-            const int L0 = Lw & 255, L1 = (Lw >> 8) & 255, L2 = (Lw >> 16) & 255;
-            const int R0 = Rw & 255, R1 = (Rw >> 8) & 255, R2 = (Rw >> 16) & 255;
-            const int C0 = rows & 255, C2 = (rows >> 16) & 255;
-            const int gx = (R2 - L2) + (R0 - L0) + 2 * (R1 - L1);
-            const int gy = (L2 + 2 * C2 + R2) - (L0 + 2 * C0 + R0);
-            p0 = gx * gx; p1 = gx * gy; p2 = gy * gy;
+        float p[3][4];
+        {
+            const uint32_t bias = 0x04000400u;
+            const uint32_t vE = t.E + 2 * m.E + b.E, vO = t.O + 2 * m.O + b.O;
+            const uint32_t vOm = t.Om + 2 * m.Om + b.Om, vEp = t.Ep + 2 * m.Ep + b.Ep;
+            const uint32_t gx02 = vO + bias - vOm, gx13 = vEp + bias - vE;
+            const uint32_t gy02 = (b.Om + 2 * b.E + b.O) + bias - (t.Om + 2 * t.E + t.O);
+            const uint32_t gy13 = (b.E + 2 * b.O + b.Ep) + bias - (t.E + 2 * t.O + t.Ep);
+            const float gx[4] = {lane_lo(gx02), lane_lo(gx13), lane_hi(gx02), lane_hi(gx13)};
+            const float gy[4] = {lane_lo(gy02), lane_lo(gy13), lane_hi(gy02), lane_hi(gy13)};
+            const bool rowOk = g >= 1 && g < H - 1;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const bool ok = rowOk && gradCol[c];
+                p[0][c] = ok ? __fmul_rn(gx[c], gx[c]) : 0.f;
+                p[1][c] = ok ? __fmul_rn(gx[c], gy[c]) : 0.f;
+                p[2][c] = ok ? __fmul_rn(gy[c], gy[c]) : 0.f;
+            }
         }
-        // vertical sums at s = g - 1 over gradient rows g-2, g-1, g, then horizontal
-        const int c0 = v0[0] + v1[0] + p0, c1 = v0[1] + v1[1] + p1, c2 = v0[2] + v1[2] + p2;
-        v0[0] = v1[0]; v0[1] = v1[1]; v0[2] = v1[2];
-        v1[0] = p0; v1[1] = p1; v1[2] = p2;
-        const int S0 = c0 + __shfl_up_sync(0xffffffffu, c0, 1) + __shfl_down_sync(0xffffffffu, c0, 1);
-        const int S1 = c1 + __shfl_up_sync(0xffffffffu, c1, 1) + __shfl_down_sync(0xffffffffu, c1, 1);
-        const int S2 = c2 + __shfl_up_sync(0xffffffffu, c2, 1) + __shfl_down_sync(0xffffffffu, c2, 1);
+        t = m; m = b;
+        // window sums at s = g - 1 over gradient rows g-2 .. g, columns -1 .. 4 (HafCpu_HarrisScore_HVC_HG3_3x3)
+        float vs[3][6];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                vs[q][c + 1] = __fadd_rn(__fadd_rn(v0[q][c], v1[q][c]), p[q][c]);
+                v0[q][c] = v1[q][c];
+                v1[q][c] = p[q][c];
+            }
+            vs[q][0] = __shfl_up_sync(0xffffffffu, vs[q][4], 1);
+            vs[q][5] = __shfl_down_sync(0xffffffffu, vs[q][1], 1);
+        }
         const int srow = g - 1;
-        float sc = 0.f;
-        if (scoreCol && srow >= 1 && srow < H - 1) {
-            const float gx2 = (float)S0, gxy2 = (float)S1, gy2 = (float)S2;
+        const bool sRowOk = srow >= 1 && srow < H - 1;
+        float sc[6];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float gx2 = __fadd_rn(__fadd_rn(vs[0][c], vs[0][c + 1]), vs[0][c + 2]);
+            const float gxy2 = __fadd_rn(__fadd_rn(vs[1][c], vs[1][c + 1]), vs[1][c + 2]);
+            const float gy2 = __fadd_rn(__fadd_rn(vs[2][c], vs[2][c + 1]), vs[2][c + 2]);
             const float traceA = __fadd_rn(gx2, gy2);
             const float detA = __fsub_rn(__fmul_rn(gx2, gy2), __fmul_rn(gxy2, gxy2));
             const float Mc = __fsub_rn(detA, __fmul_rn(__fmul_rn(k, traceA), traceA));
-            const bool zero = Tc >= 0.f && (Mc <= 0.f || (Tc > 0.f && Mc < cut));
-            if (!zero) {
-                const float q = __fdiv_rn(Mc, norm);
-                sc = q > Tc ? q : 0.f;
+            float v = 0.f;
+            if (sRowOk && scoreCol[c]) {
+                const bool zero = Tc >= 0.f && (Mc <= 0.f || (Tc > 0.f && Mc < cut));
+                if (!zero) {
+                    const float q = __fdiv_rn(Mc, norm);
+                    v = q > Tc ? q : 0.f;
+                }
+            }
+            sc[c + 1] = v;
+        }
+        sc[0] = __shfl_up_sync(0xffffffffu, sc[4], 1);
+        sc[5] = __shfl_down_sync(0xffffffffu, sc[1], 1);
+        // non-maximum suppression at n = s - 1 (HafCpu_NonMaxSupp_XY_ANY_3x3, harris.cpp:882):
+        // >= the row above and the left neighbour, > the right neighbour and the row below
+        const int n = srow - 1;
+        const bool rowOut = n >= ys && n < yEnd && n >= 1 && n < H - 1;
+        uint32_t keep = 0;
+        if (outLane && rowOut) {
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const float v = sB[c + 1];
+                const float above = fmaxf(fmaxf(sA[c], sA[c + 1]), sA[c + 2]);
+                const float below = fmaxf(fmaxf(sc[c], sc[c + 1]), sc[c + 2]);
+                const bool kc = scoreCol[c] && v >= above && v >= sB[c] && v > sB[c + 2] && v > below;
+                keep |= (uint32_t)kc << c;
             }
         }
-        // non-maximum suppression at n = s - 1
-        const int n = srow - 1;
-        const float aL = __shfl_up_sync(0xffffffffu, sA, 1), aR = __shfl_down_sync(0xffffffffu, sA, 1);
-        const float bL = __shfl_up_sync(0xffffffffu, sB, 1), bR = __shfl_down_sync(0xffffffffu, sB, 1);
-        const float cL = __shfl_up_sync(0xffffffffu, sc, 1), cR = __shfl_down_sync(0xffffffffu, sc, 1);
-        const bool rowOut = n >= ys && n < yEnd && n >= 1 && n < H - 1;
-        bool keep = false;
-        if (outLane && rowOut)
-            keep = sB >= aL && sB >= sA && sB >= aR && sB >= bL && sB > bR && sB > cL && sB > sc && sB > cR;
-        if (rowOut) xys_append(list, count, capacity, xys_pack(xc, n, sB), keep);
-        sA = sB;
-        sB = sc;
+        if (rowOut && __any_sync(0xffffffffu, keep != 0)) {
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                xys_append(list, count, capacity, xys_pack(xl + c, n, sB[c + 1]), (keep >> c) & 1);
+        }
+#pragma unroll
+        for (int c = 0; c < 6; c++) { sA[c] = sB[c]; sB[c] = sc[c]; }
     }
 }
 
