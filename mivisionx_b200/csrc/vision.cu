@@ -654,13 +654,13 @@ __global__ void k_harris_nms(int W, int H, const float *sc, int scStride, uint64
 }
 
 // Harris front end as column strips: a warp owns 120 output columns (lanes 1..30, four
-// columns each; lanes 0 and 31 carry the halo) and walks down 32 output rows with rolling
+// columns each; lanes 0 and 31 carry the halo) and walks down 16 output rows with rolling
 // registers.  Per input row a lane loads one word; the Sobel sums run in 16-bit lanes
 // (four columns in four registers), the products and window sums in float -- integers
 // below 2^24, i.e. exactly the float sums the reference forms in any order.  The score
 // keeps the reference's float operation order, and its division is skipped only where the
 // result cannot exceed the threshold.
-constexpr int kHRows = 32, kHCols = 120;
+constexpr int kHRows = 16, kHCols = 120;
 
 __device__ __forceinline__ uint32_t harris_word(const uint8_t *src, int stride, int W, int H, int x, int y, bool fast)
 {
@@ -691,18 +691,29 @@ k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, floa
         gradCol[c] = xl + c >= 0 && xl + c < W;
         scoreCol[c] = xl + c >= 1 && xl + c < W - 1;
     }
-    const float cut = Tc > 0.f ? __fmul_rn(0.999f, __fmul_rn(Tc, norm)) : 0.f;   // Mc below: score 0
-    Lanes4 t{0, 0, 0, 0}, m{0, 0, 0, 0};                   // input rows r-2, r-1 as 16-bit lanes
-    float v0[3][4] = {}, v1[3][4] = {};                     // products at gradient rows g-2, g-1
-    float sA[6] = {}, sB[6] = {};                           // scores (columns -1..4) at rows s-2, s-1
+    // the score is 0 without the division where Mc < zLess or Mc <= zLessEq:
+    // Tc > 0: Mc < 0.999 Tc norm (the quotient cannot exceed Tc); Tc == 0: Mc <= 0
+    const float cut = Tc > 0.f ? __fmul_rn(0.999f, __fmul_rn(Tc, norm)) : 0.f;
+    const float zLess = Tc > 0.f ? cut : -INFINITY, zLessEq = Tc == 0.f ? 0.f : -INFINITY;
+    // rolling state, rotated by the unrolled loop: input rows as 16-bit lanes, products of
+    // gradient rows, scores (columns -1 .. 4) of score rows
+    Lanes4 X[3] = {};
+    float P[3][3][4] = {};
+    float S[3][6] = {};
     uint32_t next = harris_word(src, srcStride, W, H, xl, ys - 3, fast);
-    for (int r = ys - 3; r <= yEnd + 2; r++) {
+    const int rLast = yEnd + 2;
+
+    // one input row r: t, m = rows r-2, r-1 (b receives row r); v0, v1 = products at
+    // gradient rows g-2, g-1 (p receives g = r-1); sA, sB = scores at rows s-2, s-1 (sc
+    // receives s = g-1); suppression at n = s-1
+    auto step = [&](int r, const Lanes4 &t, const Lanes4 &m, Lanes4 &b, const float (&v0)[3][4],
+                    const float (&v1)[3][4], float (&p)[3][4], const float (&sA)[6], const float (&sB)[6],
+                    float (&sc)[6]) {
         const uint32_t cur = next;
-        if (r + 1 <= yEnd + 2) next = harris_word(src, srcStride, W, H, xl, r + 1, fast);
-        const Lanes4 b = lanes4(__shfl_up_sync(0xffffffffu, cur, 1), cur, __shfl_down_sync(0xffffffffu, cur, 1));
-        // gradient at g = r - 1 from rows r-2, r-1, r (HafCpu_HarrisSobel_HG3_U8_3x3, harris.cpp:85)
+        if (r + 1 <= rLast) next = harris_word(src, srcStride, W, H, xl, r + 1, fast);
+        b = lanes4(__shfl_up_sync(0xffffffffu, cur, 1), cur, __shfl_down_sync(0xffffffffu, cur, 1));
+        // gradient at g = r - 1 (HafCpu_HarrisSobel_HG3_U8_3x3, harris.cpp:85)
         const int g = r - 1;
-        float p[3][4];
         {
             const uint32_t bias = 0x04000400u;
             const uint32_t vE = t.E + 2 * m.E + b.E, vO = t.O + 2 * m.O + b.O;
@@ -721,23 +732,17 @@ k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, floa
                 p[2][c] = ok ? __fmul_rn(gy[c], gy[c]) : 0.f;
             }
         }
-        t = m; m = b;
-        // window sums at s = g - 1 over gradient rows g-2 .. g, columns -1 .. 4 (HafCpu_HarrisScore_HVC_HG3_3x3)
+        // window sums at s = g - 1 over gradient rows g-2 .. g (HafCpu_HarrisScore_HVC_HG3_3x3)
         float vs[3][6];
 #pragma unroll
         for (int q = 0; q < 3; q++) {
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                vs[q][c + 1] = __fadd_rn(__fadd_rn(v0[q][c], v1[q][c]), p[q][c]);
-                v0[q][c] = v1[q][c];
-                v1[q][c] = p[q][c];
-            }
+            for (int c = 0; c < 4; c++) vs[q][c + 1] = __fadd_rn(__fadd_rn(v0[q][c], v1[q][c]), p[q][c]);
             vs[q][0] = __shfl_up_sync(0xffffffffu, vs[q][4], 1);
             vs[q][5] = __shfl_down_sync(0xffffffffu, vs[q][1], 1);
         }
         const int srow = g - 1;
         const bool sRowOk = srow >= 1 && srow < H - 1;
-        float sc[6];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const float gx2 = __fadd_rn(__fadd_rn(vs[0][c], vs[0][c + 1]), vs[0][c + 2]);
@@ -747,12 +752,9 @@ k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, floa
             const float detA = __fsub_rn(__fmul_rn(gx2, gy2), __fmul_rn(gxy2, gxy2));
             const float Mc = __fsub_rn(detA, __fmul_rn(__fmul_rn(k, traceA), traceA));
             float v = 0.f;
-            if (sRowOk && scoreCol[c]) {
-                const bool zero = Tc >= 0.f && (Mc <= 0.f || (Tc > 0.f && Mc < cut));
-                if (!zero) {
-                    const float q = __fdiv_rn(Mc, norm);
-                    v = q > Tc ? q : 0.f;
-                }
+            if (sRowOk && scoreCol[c] && !(Mc < zLess || Mc <= zLessEq)) {
+                const float q = __fdiv_rn(Mc, norm);
+                v = q > Tc ? q : 0.f;
             }
             sc[c + 1] = v;
         }
@@ -778,8 +780,13 @@ k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, floa
             for (int c = 0; c < 4; c++)
                 xys_append(list, count, capacity, xys_pack(xl + c, n, sB[c + 1]), (keep >> c) & 1);
         }
-#pragma unroll
-        for (int c = 0; c < 6; c++) { sA[c] = sB[c]; sB[c] = sc[c]; }
+    };
+    for (int r = ys - 3; r <= rLast; r += 3) {             // r is warp-uniform
+        step(r, X[0], X[1], X[2], P[0], P[1], P[2], S[0], S[1], S[2]);
+        if (r + 1 > rLast) break;
+        step(r + 1, X[1], X[2], X[0], P[1], P[2], P[0], S[1], S[2], S[0]);
+        if (r + 2 > rLast) break;
+        step(r + 2, X[2], X[0], X[1], P[2], P[0], P[1], S[2], S[0], S[1]);
     }
 }
 
