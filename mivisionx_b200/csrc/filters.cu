@@ -225,62 +225,136 @@ __global__ void k_threshold_u8_binary(int W, int H, uint8_t *dst, int dstStride,
 //   SIMD body:  round(sqrt(n)) >= M   <=>  n >= M*M - M + 1
 //   scalar tail: trunc(sqrtf(n)) >= M <=>  n >= M*M
 // (n < 2^22 here, so sqrtf is exact enough for the second equivalence).
+//
+// A thread owns 8 columns and walks down its rows.  The Gaussian runs on pairs of columns
+// in 16-bit lanes of 32-bit words (horizontal [1 2 1] from byte permutes, vertical sum,
+// then the >> 4 kept as a mask, i.e. 16x the Gaussian); the Sobel sums stay in lanes with
+// a bias and turn into exact floats, and n >= T is the sign of one exact fused multiply-add
+// chain: (16gx)^2 + (16gy)^2 - 256 T, all multiples of 256 below 2^30.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBX * kBY)
-k_fused_gauss_sobelmag_thresh(const agocuda_frame *frames, int nRound, int nTrunc)
+constexpr int kC1Rows = 30;     // output rows per thread (a multiple of the 3-way unroll)
+constexpr int kC1BX = 32, kC1BY = 4;
+
+// h = p[c-1] + 2 p[c] + p[c+1] on the 5 lane-pair words of 8 columns x..x+7 plus x-1, x+8:
+// (x, x+2), (x+1, x+3), (x+4, x+6), (x+5, x+7), (x-1, x+8)
+struct C1Row { uint32_t e1, o1, e2, o2, b; };
+
+__device__ __forceinline__ C1Row c1_hsum(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3)
+{
+    const uint32_t E1 = __byte_perm(w1, 0, 0x4240), O1 = __byte_perm(w1, 0, 0x4341);
+    const uint32_t E2 = __byte_perm(w2, 0, 0x4240), O2 = __byte_perm(w2, 0, 0x4341);
+    const uint32_t Om1 = __byte_perm(w0, O1, 0x5453), Ep1 = __byte_perm(E1, w2, 0x3432);
+    const uint32_t Om2 = __byte_perm(w1, O2, 0x5453), Ep2 = __byte_perm(E2, w3, 0x3432);
+    C1Row h;
+    h.e1 = Om1 + 2 * E1 + O1;
+    h.o1 = E1 + 2 * O1 + Ep1;
+    h.e2 = Om2 + 2 * E2 + O2;
+    h.o2 = E2 + 2 * O2 + Ep2;
+    // columns x-1 and x+8: bytes (x-2, x-1, x) and (x+7, x+8, x+9) weighted 1 2 1
+    const uint32_t hl = __dp4a(__funnelshift_r(w0, w1, 16), 0x00010201u, 0u);
+    const uint32_t hr = __dp4a(__funnelshift_r(w2, w3, 24), 0x00010201u, 0u);
+    h.b = hl | (hr << 16);
+    return h;
+}
+
+// 16 x Gaussian: ((h0 + 2 h1 + h2) >> 4) << 4, lanes below 4096
+__device__ __forceinline__ uint32_t c1_g(uint32_t a, uint32_t b, uint32_t c) { return (a + 2 * b + c) & 0xFFF0FFF0u; }
+__device__ __forceinline__ C1Row c1_gauss(const C1Row &a, const C1Row &b, const C1Row &c)
+{
+    return C1Row{c1_g(a.e1, b.e1, c.e1), c1_g(a.o1, b.o1, c.o1), c1_g(a.e2, b.e2, c.e2), c1_g(a.o2, b.o2, c.o2),
+                 c1_g(a.b, b.b, c.b)};
+}
+
+// horizontal [1 2 1] of a 16x Gaussian row at the 8 columns, as (x, x+2), (x+1, x+3),
+// (x+4, x+6), (x+5, x+7) lane pairs (below 2^16)
+struct C1H { uint32_t e1, o1, e2, o2; };
+__device__ __forceinline__ C1H c1_hpass(const C1Row &g)
+{
+    const uint32_t m1 = __byte_perm(g.b, g.o1, 0x5410), p1 = __byte_perm(g.e1, g.e2, 0x5432);
+    const uint32_t m2 = __byte_perm(g.o1, g.o2, 0x5432), p2 = __byte_perm(g.e2, g.b, 0x7632);
+    return C1H{m1 + 2 * g.e1 + g.o1, g.e1 + 2 * g.o1 + p1, m2 + 2 * g.e2 + g.o2, g.e2 + 2 * g.o2 + p2};
+}
+
+// 4 output bytes: 255 where the float is >= 0 (sign bit clear), else 0
+__device__ __forceinline__ uint32_t nonneg_bytes(float a, float b, float c, float d)
+{
+    const uint32_t top = __byte_perm(__byte_perm(__float_as_uint(a), __float_as_uint(b), 0x7373),
+                                     __byte_perm(__float_as_uint(c), __float_as_uint(d), 0x7373), 0x5410);
+    return ((~top & 0x80808080u) >> 7) * 0xFFu;
+}
+
+// lane (value + 16384) of a biased pair word as an exact float value
+__device__ __forceinline__ float c1_lo(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8404992.0f; }
+__device__ __forceinline__ float c1_hi(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8404992.0f; }
+
+__global__ void __launch_bounds__(kC1BX * kC1BY)
+k_fused_gauss_sobelmag_thresh(const agocuda_frame *frames, float tRound, float tTrunc)
 {
     const agocuda_frame f = frames[blockIdx.z];
     const int W = (int)f.width, H = (int)f.height;
-    const int x = (blockIdx.x * kBX + threadIdx.x) * 4;
-    const int y0 = 2 + (blockIdx.y * kBY + threadIdx.y) * kRPT;
+    const int x = (blockIdx.x * kC1BX + threadIdx.x) * 8;
+    const int y0 = 2 + (blockIdx.y * kC1BY + threadIdx.y) * kC1Rows;
     if (x >= W || y0 >= H - 2) return;
-    const int y1 = min(y0 + kRPT, H - 2);
+    const int y1 = min(y0 + kC1Rows, H - 2);
     const int ss = (int)f.srcStride;
     const uint8_t *src = f.src;
-    // Gaussian of rows r-1, r (columns x-1..x+4) and horizontal sums of input rows.
-    int h0[6], h1[6], g0[6], g1[6];
+    float T[8];                                    // -256 T per column (trunc / round span)
+#pragma unroll
+    for (int j = 0; j < 8; j++) T[j] = (x + j < f.simdBegin || x + j >= f.simdEnd) ? tTrunc : tRound;
+    auto hrow = [&](int y) {
+        const uint8_t *row = src + (size_t)y * ss;
+        return c1_hsum(load_word_clamped(row, x - 4, ss), load_word_clamped(row, x, ss),
+                       load_word_clamped(row, x + 4, ss), load_word_clamped(row, x + 8, ss));
+    };
+    // rolling rows, rotated by the unrolled loop: h of input rows y, y+1; 16x Gaussian of
+    // rows y-1, y; horizontal pass of the Gaussian at rows y-1, y
+    C1Row h[3], g[3];
+    C1H hp[3];
     {
-        Row8 a = load_row8(src + (size_t)(y0 - 2) * ss, x, ss);
-        Row8 b = load_row8(src + (size_t)(y0 - 1) * ss, x, ss);
-        Row8 c = load_row8(src + (size_t)(y0) * ss, x, ss);
-        int ha[6];
-#pragma unroll
-        for (int i = 0; i < 6; i++) {
-            ha[i] = a.p[i] + 2 * a.p[i + 1] + a.p[i + 2];
-            h0[i] = b.p[i] + 2 * b.p[i + 1] + b.p[i + 2];
-            h1[i] = c.p[i] + 2 * c.p[i + 1] + c.p[i + 2];
-            g0[i] = (ha[i] + 2 * h0[i] + h1[i]) >> 4;   // Gaussian row y0-1
-        }
-        Row8 d = load_row8(src + (size_t)(y0 + 1) * ss, x, ss);
-#pragma unroll
-        for (int i = 0; i < 6; i++) {
-            int hd = d.p[i] + 2 * d.p[i + 1] + d.p[i + 2];
-            g1[i] = (h0[i] + 2 * h1[i] + hd) >> 4;      // Gaussian row y0
-            h0[i] = h1[i]; h1[i] = hd;
-        }
+        const C1Row a = hrow(y0 - 2), b = hrow(y0 - 1);
+        h[0] = hrow(y0);
+        h[1] = hrow(y0 + 1);
+        g[0] = c1_gauss(a, b, h[0]);
+        g[1] = c1_gauss(b, h[0], h[1]);
+        hp[0] = c1_hpass(g[0]);
+        hp[1] = c1_hpass(g[1]);
     }
-    for (int y = y0; y < y1; y++) {
-        Row8 n = load_row8(src + (size_t)(y + 2) * ss, x, ss);
-        int g2[6];
+    auto step = [&](int y, const C1Row &hA, const C1Row &hB, C1Row &hC, const C1Row &gA, const C1Row &gB, C1Row &gC,
+                    const C1H &pA, const C1H &pB, C1H &pC) {
+        hC = hrow(y + 2);
+        gC = c1_gauss(hA, hB, hC);                 // 16 x Gaussian row y+1
+        pC = c1_hpass(gC);
+        (void)pB;
+        // vertical [1 2 1] of the Gaussian at row y: (x-1, x+8) and the four pairs
+        const uint32_t vE1 = gA.e1 + 2 * gB.e1 + gC.e1, vO1 = gA.o1 + 2 * gB.o1 + gC.o1;
+        const uint32_t vE2 = gA.e2 + 2 * gB.e2 + gC.e2, vO2 = gA.o2 + 2 * gB.o2 + gC.o2;
+        const uint32_t vB = gA.b + 2 * gB.b + gC.b;
+        const uint32_t bias = 0x40004000u;
+        // 16 gx = V(c+1) - V(c-1), 16 gy = H(y+1) - H(y-1), as biased lane pairs
+        const uint32_t gx0 = vO1 + bias - __byte_perm(vB, vO1, 0x5410);     // (x, x+2)
+        const uint32_t gx1 = __byte_perm(vE1, vE2, 0x5432) + bias - vE1;    // (x+1, x+3)
+        const uint32_t gx2 = vO2 + bias - __byte_perm(vO1, vO2, 0x5432);    // (x+4, x+6)
+        const uint32_t gx3 = __byte_perm(vE2, vB, 0x7632) + bias - vE2;     // (x+5, x+7)
+        const uint32_t gy0 = pC.e1 + bias - pA.e1, gy1 = pC.o1 + bias - pA.o1;
+        const uint32_t gy2 = pC.e2 + bias - pA.e2, gy3 = pC.o2 + bias - pA.o2;
+        const float fx[8] = {c1_lo(gx0), c1_lo(gx1), c1_hi(gx0), c1_hi(gx1), c1_lo(gx2), c1_lo(gx3), c1_hi(gx2), c1_hi(gx3)};
+        const float fy[8] = {c1_lo(gy0), c1_lo(gy1), c1_hi(gy0), c1_hi(gy1), c1_lo(gy2), c1_lo(gy3), c1_hi(gy2), c1_hi(gy3)};
+        float rr[8];
 #pragma unroll
-        for (int i = 0; i < 6; i++) {
-            int hn = n.p[i] + 2 * n.p[i + 1] + n.p[i + 2];
-            g2[i] = (h0[i] + 2 * h1[i] + hn) >> 4;      // Gaussian row y+1
-            h0[i] = h1[i]; h1[i] = hn;
-        }
-        int o[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            int gx, gy;
-            sobel_at(g0, g1, g2, i, gx, gy);
-            int nn = gx * gx + gy * gy;
-            int xi = x + i;
-            int T = (xi < f.simdBegin || xi >= f.simdEnd) ? nTrunc : nRound;
-            o[i] = nn >= T ? 255 : 0;
-        }
-        *(uint32_t *)(f.dst + (size_t)y * f.dstStride + x) = pack4(o[0], o[1], o[2], o[3]);
-#pragma unroll
-        for (int i = 0; i < 6; i++) { g0[i] = g1[i]; g1[i] = g2[i]; }
+        for (int j = 0; j < 8; j++) rr[j] = __fmaf_rn(fx[j], fx[j], __fmaf_rn(fy[j], fy[j], T[j]));
+        // 255 where the exact sum is >= 0
+        const uint32_t lo = nonneg_bytes(rr[0], rr[1], rr[2], rr[3]);
+        const uint32_t hi = nonneg_bytes(rr[4], rr[5], rr[6], rr[7]);
+        uint8_t *o = f.dst + (size_t)y * f.dstStride + x;
+        *(uint32_t *)o = lo;
+        if (x + 4 < W) *(uint32_t *)(o + 4) = hi;
+    };
+    for (int y = y0; y < y1; y += 3) {             // y is uniform across the thread's loop
+        step(y, h[0], h[1], h[2], g[0], g[1], g[2], hp[0], hp[1], hp[2]);
+        if (y + 1 >= y1) break;
+        step(y + 1, h[1], h[2], h[0], g[1], g[2], g[0], hp[1], hp[2], hp[0]);
+        if (y + 2 >= y1) break;
+        step(y + 2, h[2], h[0], h[1], g[2], g[0], g[1], hp[2], hp[0], hp[1]);
     }
 }
 
@@ -389,17 +463,19 @@ extern "C" int agocuda_fused_GaussSobelMagDepthThresh(void *stream, const agocud
     if (!frames || !numFrames || numFrames > 65535 || maxWidth < 5 || maxHeight < 5 || shift < 0 || shift > 15)
         return AGOCUDA_INVALID_PARAMS;
     const int t = (int)(uint8_t)threshold;
-    const int kNever = 0x7fffffff;
-    int nRound = kNever, nTrunc = kNever;
+    // -256 n_min: (16 gx)^2 + (16 gy)^2 - 256 n_min >= 0 <=> gx^2 + gy^2 >= n_min.  A 3x3 Sobel
+    // of a Gaussian has gx^2 + gy^2 <= 2 * 1020^2; thresholds beyond it never pass.
+    const double kNever = -256.0 * 4194304.0;
+    double tRound = kNever, tTrunc = kNever;
     if (t < 255) {
         long long M = (long long)(t + 1) << shift;
-        if (M <= 46340) {   // beyond this no 3x3 Sobel magnitude can reach M
-            nRound = (int)(M * M - M + 1);
-            nTrunc = (int)(M * M);
+        if (M <= 2048) {
+            tRound = -256.0 * (double)(M * M - M + 1);
+            tTrunc = -256.0 * (double)(M * M);
         }
     }
-    dim3 grd(div_up(maxWidth, kBX * 4), div_up(maxHeight - 4, kBY * kRPT), numFrames);
-    k_fused_gauss_sobelmag_thresh<<<grd, dim3(kBX, kBY), 0, as_stream(stream)>>>(frames, nRound, nTrunc);
+    dim3 grd(div_up(maxWidth, kC1BX * 8), div_up(maxHeight - 4, kC1BY * kC1Rows), numFrames);
+    k_fused_gauss_sobelmag_thresh<<<grd, dim3(kC1BX, kC1BY), 0, as_stream(stream)>>>(frames, (float)tRound, (float)tTrunc);
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }
