@@ -232,7 +232,7 @@ __global__ void k_threshold_u8_binary(int W, int H, uint8_t *dst, int dstStride,
 // a bias and turn into exact floats, and n >= T is the sign of one exact fused multiply-add
 // chain: (16gx)^2 + (16gy)^2 - 256 T, all multiples of 256 below 2^30.
 // ---------------------------------------------------------------------------------
-constexpr int kC1Rows = 30;     // output rows per thread (a multiple of the 3-way unroll)
+constexpr int kC1Rows = 18;     // output rows per thread (a multiple of the 3-way unroll)
 constexpr int kC1BX = 32, kC1BY = 4;
 
 // h = p[c-1] + 2 p[c] + p[c+1] on the 5 lane-pair words of 8 columns x..x+7 plus x-1, x+8:
@@ -301,10 +301,17 @@ k_fused_gauss_sobelmag_thresh(const agocuda_frame *frames, float tRound, float t
     float T[8];                                    // -256 T per column (trunc / round span)
 #pragma unroll
     for (int j = 0; j < 8; j++) T[j] = (x + j < f.simdBegin || x + j >= f.simdEnd) ? tTrunc : tRound;
+    uint32_t nw[4];                                // words of the next input row, loaded a row ahead
+    auto fetch = [&](int y) {
+        const uint8_t *row = src + (size_t)min(y, H - 1) * ss;
+        nw[0] = load_word_clamped(row, x - 4, ss);
+        nw[1] = load_word_clamped(row, x, ss);
+        nw[2] = load_word_clamped(row, x + 4, ss);
+        nw[3] = load_word_clamped(row, x + 8, ss);
+    };
     auto hrow = [&](int y) {
-        const uint8_t *row = src + (size_t)y * ss;
-        return c1_hsum(load_word_clamped(row, x - 4, ss), load_word_clamped(row, x, ss),
-                       load_word_clamped(row, x + 4, ss), load_word_clamped(row, x + 8, ss));
+        fetch(y);
+        return c1_hsum(nw[0], nw[1], nw[2], nw[3]);
     };
     // rolling rows, rotated by the unrolled loop: h of input rows y, y+1; 16x Gaussian of
     // rows y-1, y; horizontal pass of the Gaussian at rows y-1, y
@@ -318,10 +325,12 @@ k_fused_gauss_sobelmag_thresh(const agocuda_frame *frames, float tRound, float t
         g[1] = c1_gauss(b, h[0], h[1]);
         hp[0] = c1_hpass(g[0]);
         hp[1] = c1_hpass(g[1]);
+        fetch(y0 + 2);
     }
     auto step = [&](int y, const C1Row &hA, const C1Row &hB, C1Row &hC, const C1Row &gA, const C1Row &gB, C1Row &gC,
                     const C1H &pA, const C1H &pB, C1H &pC) {
-        hC = hrow(y + 2);
+        hC = c1_hsum(nw[0], nw[1], nw[2], nw[3]);  // input row y+2, loaded a step earlier
+        fetch(y + 3);
         gC = c1_gauss(hA, hB, hC);                 // 16 x Gaussian row y+1
         pC = c1_hpass(gC);
         (void)pB;
