@@ -80,7 +80,7 @@ class GaussChain(Workload):
         return g
 
     def host_io(self, ins, outs):
-        return {"src": ins, "dst": outs}
+        return {"src": [p[0] for p in ins], "dst": [p[0] for p in outs]}
 
     def alg_bytes(self, g, n):
         return 2.0 * self.width * self.height * n   # 1 B in + 1 B out per pixel
@@ -103,7 +103,7 @@ class CannyHarris(Workload):
         return g
 
     def host_io(self, ins, outs):
-        return {"src": ins, "edge": outs}
+        return {"src": [p[0] for p in ins], "edge": [p[0] for p in outs]}
 
     def alg_bytes(self, g, n):
         from mivisionx_b200 import vx as V
@@ -144,7 +144,7 @@ class PyramidLK(Workload):
         return g
 
     def host_io(self, ins, outs):
-        return {"old": ins[0::2], "new": ins[1::2]}
+        return {"old": [p[0] for p in ins[0::2]], "new": [p[0] for p in ins[1::2]]}
 
     def alg_bytes(self, g, n):
         from mivisionx_b200 import vx as V
@@ -154,7 +154,38 @@ class PyramidLK(Workload):
         return pyr + 2.0 * self.points * len(g.out) * C.sizeof(V.vx_keypoint_t)
 
 
-WORKLOADS = {w.name: w for w in (CannyHarris(), GaussChain(), PyramidLK())}
+class ColorGeometry(Workload):
+    name = "color_geometry_4k"
+    desc = ("ColorConvert RGB->NV12 and RGB->IYUV, ChannelExtract Y (virtual), ScaleImage to 1920x1080 "
+            "(bilinear and area), WarpAffine of the bilinear result (nearest and bilinear, border CONSTANT 0; "
+            "rotation +-15 deg, scale 0.8-1.2, shift +-50 px) on 3840x2160 RGB frames (8 seeded sinusoids per "
+            "channel + U(-10, 10) noise)")
+    width, height, frames = 3840, 2160, 8
+    distinct = 4            # distinct seeded frames, repeated to fill the step
+
+    def make_frames(self, seed0, n):
+        from mivisionx_b200 import workloads as WL
+        base = [WL.cfg3_frame(seed=seed0 + i, width=self.width, height=self.height) for i in range(min(n, self.distinct))]
+        return [base[i % len(base)] for i in range(n)]
+
+    def build(self, api, ctx, n, flags=None, host_io=None):
+        from mivisionx_b200 import workloads as WL
+        g = WL.Cfg3Graph(api, ctx, [(self.width, self.height)] * n, flags=flags, host_io=host_io)
+        g.out_images, g.out_arrays = g.outputs, []
+        return g
+
+    def host_io(self, ins, outs):
+        # outputs per frame: nv12, iyuv, scaled bilinear, scaled area, warp nearest, warp bilinear
+        per = [outs[i:i + 6] for i in range(0, len(outs), 6)]
+        return {"rgb": ins, "nv12": [o[0] for o in per], "iyuv": [o[1] for o in per], "sb": [o[2][0] for o in per],
+                "sa": [o[3][0] for o in per], "wn": [o[4][0] for o in per], "wb": [o[5][0] for o in per]}
+
+    def alg_bytes(self, g, n):
+        # 3 B RGB in + NV12 1.5 + IYUV 1.5 + four quarter-size U8 outputs (Y plane virtual)
+        return 7.0 * self.width * self.height * n
+
+
+WORKLOADS = {w.name: w for w in (CannyHarris(), GaussChain(), PyramidLK(), ColorGeometry())}
 DEFAULT_WORKLOAD = CannyHarris.name
 
 
@@ -270,7 +301,7 @@ def _ref_worker(wl_name, seed, seconds, max_iters, barrier, queue):
     while n < max_iters and (time.perf_counter() - t0) < seconds:
         g.run()
         n += 1
-    queue.put((n, time.perf_counter() - t0, sum(int(f.size) for f in frames)))
+    queue.put((n, time.perf_counter() - t0, sum(int(f.shape[0] * f.shape[1]) for f in frames)))
 
 
 def reference_cpu(wl_name: str, procs: int, seconds: float, max_iters: int = 1 << 30):
@@ -347,12 +378,19 @@ def run_ours(a, wl_name):
     g = wl.build(api, ctx, B, flags=V.OPT_NO_FUSION if a.plain else None)
     plan = api.plan(g.graph)
     kernels_per_step = sum(k for _, k in plan)
-    pin_in = [torch.from_numpy(np.ascontiguousarray(f)).pin_memory() for f in frames]
-    out_shapes = [api.query_image(i)[1::-1] for i in g.out_images]
-    pin_out = [torch.empty(shp, dtype=torch.uint8).pin_memory() for shp in out_shapes]
+    # page-locked host buffers, one per image plane: (rows, row bytes)
+    def planes(img):
+        w, h, fmt = api.query_image(img)
+        return [(pi, ph, pw, bpp) for pi, (ph, pw, bpp) in enumerate(V.image_plane_layout(fmt, w, h))]
+    in_layout = [planes(i) for i in g.inputs]
+    out_layout = [planes(i) for i in g.out_images]
+    pin_in = [[torch.from_numpy(np.ascontiguousarray(f).reshape(ph, pw * bpp)).pin_memory()
+               for (_, ph, pw, bpp) in lay] for f, lay in zip(frames, in_layout)]
+    pin_out = [[torch.empty((ph, pw * bpp), dtype=torch.uint8).pin_memory() for (_, ph, pw, bpp) in lay]
+               for lay in out_layout]
     in_arrays = [(arr, torch.from_numpy(kp.view('u1')).pin_memory(), kp.dtype.itemsize, len(kp))
                  for arr, kp in getattr(g, "in_arrays", [])]
-    g.run([p.numpy() for p in pin_in])
+    g.run([f for f in frames])
     alg_bytes = wl.alg_bytes(g, B)
     shapes = sorted({f.shape for f in frames})
     frame_desc = f"{shapes[0][1]}x{shapes[0][0]}" if len(shapes) == 1 else "uneven: " + ", ".join(
@@ -371,18 +409,22 @@ def run_ours(a, wl_name):
         torch.cuda.synchronize()
     _barrier(ws)
     ms_step = _max_over_ranks(sum(gpu_ms), ws) / a.steps
-    px_step = sum(int(f.size) for f in frames)
+    px_step = sum(int(f.shape[0] * f.shape[1]) for f in frames)   # input pixels of the first node
     value = px_step * ws / (ms_step / 1e3) / 1e6
 
     # ---- end to end through the OpenVX API with host buffers
-    def patch(h, w):
-        addr = V.vx_imagepatch_addressing_t()
-        addr.dim_x, addr.dim_y, addr.stride_x, addr.stride_y = w, h, 1, w
-        addr.scale_x = addr.scale_y = 1024
-        addr.step_x = addr.step_y = 1
-        return V.vx_rectangle_t(0, 0, w, h), addr
-    in_patch = [patch(*f.shape) for f in frames]
-    out_patch = [patch(*shp) for shp in out_shapes]
+    def patches(img, lay):
+        w, h, _ = api.query_image(img)
+        out = []
+        for (pi, ph, pw, bpp) in lay:
+            addr = V.vx_imagepatch_addressing_t()
+            addr.dim_x, addr.dim_y, addr.stride_x, addr.stride_y = pw, ph, bpp, pw * bpp
+            addr.scale_x = addr.scale_y = 1024
+            addr.step_x = addr.step_y = 1
+            out.append((pi, V.vx_rectangle_t(0, 0, w, h), addr))
+        return out
+    in_patch = [patches(i, lay) for i, lay in zip(g.inputs, in_layout)]
+    out_patch = [patches(i, lay) for i, lay in zip(g.out_images, out_layout)]
     arr_bufs = [np.zeros(1 << 16, V.KEYPOINT_DTYPE) for _ in g.out_arrays]
     d2h_arrays = [0]
 
@@ -400,7 +442,8 @@ def run_ours(a, wl_name):
     # (a) images created from the application's page-locked buffers: vxProcessGraph uploads
     # the inputs and downloads the outputs inside its CUDA graph, overlapped with the kernels
     gh = wl.build(api, ctx, B, flags=V.OPT_NO_FUSION if a.plain else None,
-                  host_io=wl.host_io([p.numpy() for p in pin_in], [p.numpy() for p in pin_out]))
+                  host_io=wl.host_io([[p.numpy() for p in ps] for ps in pin_in],
+                                     [[p.numpy() for p in ps] for ps in pin_out]))
     in_arrays_h = [(arr, buf, isz, n) for (arr, kp), (_, buf, isz, n) in
                    zip(getattr(gh, "in_arrays", []), in_arrays)]
 
@@ -413,16 +456,18 @@ def run_ours(a, wl_name):
 
     # (b) device images written and read with vxCopyImagePatch around vxProcessGraph
     def e2e_copy_step():
-        for img, p, (rect, addr) in zip(g.inputs, pin_in, in_patch):
-            api.ok(api.vxCopyImagePatch(img, C.byref(rect), 0, C.byref(addr), p.data_ptr(), V.VX_WRITE_ONLY,
-                                        V.VX_MEMORY_TYPE_HOST), "write")
+        for img, ps, pat in zip(g.inputs, pin_in, in_patch):
+            for p, (pi, rect, addr) in zip(ps, pat):
+                api.ok(api.vxCopyImagePatch(img, C.byref(rect), pi, C.byref(addr), p.data_ptr(), V.VX_WRITE_ONLY,
+                                            V.VX_MEMORY_TYPE_HOST), "write")
         for arr, p, isz, n in in_arrays:
             api.ok(api.vxCopyArrayRange(arr, 0, n, isz, p.data_ptr(), V.VX_WRITE_ONLY, V.VX_MEMORY_TYPE_HOST),
                    "write array")
         api.ok(api.vxProcessGraph(g.graph), "process")
-        for img, p, (rect, addr) in zip(g.out_images, pin_out, out_patch):
-            api.ok(api.vxCopyImagePatch(img, C.byref(rect), 0, C.byref(addr), p.data_ptr(), V.VX_READ_ONLY,
-                                        V.VX_MEMORY_TYPE_HOST), "read")
+        for img, ps, pat in zip(g.out_images, pin_out, out_patch):
+            for p, (pi, rect, addr) in zip(ps, pat):
+                api.ok(api.vxCopyImagePatch(img, C.byref(rect), pi, C.byref(addr), p.data_ptr(), V.VX_READ_ONLY,
+                                            V.VX_MEMORY_TYPE_HOST), "read")
         read_arrays(g)
 
     def time_e2e(step):
@@ -468,8 +513,9 @@ def run_ours(a, wl_name):
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel": f"one step: {kernels_per_step} kernels in one CUDA graph"},
             "e2e": {"value": round(e2e, 1), "unit": "Mpixels/s",
-                    "h2d_bytes_per_step": px_step + sum(isz * n for _, _, isz, n in in_arrays),
-                    "d2h_bytes_per_step": sum(h * w for h, w in out_shapes) + d2h_arrays[0],
+                    "h2d_bytes_per_step": sum(p.numel() for ps in pin_in for p in ps) +
+                                          sum(isz * n for _, _, isz, n in in_arrays),
+                    "d2h_bytes_per_step": sum(p.numel() for ps in pin_out for p in ps) + d2h_arrays[0],
                     "api": "images from page-locked application buffers (vxCreateImageFromHandle HOST) + "
                            "vxProcessGraph (copies inside its CUDA graph) + vxCopyArrayRange for arrays",
                     "ms_per_step": round(e2e_ms, 4),

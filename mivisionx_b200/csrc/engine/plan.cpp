@@ -680,11 +680,14 @@ vx_status plan_graph(Graph *g)
             if (ln.k == LK::CANNY_EDGE_TRACE_U8_U8XY && i == 0) written.insert(r);
         }
     auto root = [](Ref *r) -> Ref * { return (r->type == VX_TYPE_IMAGE && IMG(r)->parent) ? IMG(r)->parent : r; };
+    // by root, each once: the planes of a multi-plane image are images of their own (AGO children)
+    std::set<Ref *> seen_in, seen_out;
     for (Ref *r : read)
-        if (!r->is_virtual && (r->type == VX_TYPE_IMAGE || r->type == VX_TYPE_ARRAY || r->type == VX_TYPE_PYRAMID) && !written.count(r))
+        if (!r->is_virtual && (r->type == VX_TYPE_IMAGE || r->type == VX_TYPE_ARRAY || r->type == VX_TYPE_PYRAMID) &&
+            !written.count(r) && seen_in.insert(root(r)).second)
             g->inputs.push_back(root(r));
     for (Ref *r : written)
-        if (!r->is_virtual) g->outputs.push_back(root(r));
+        if (!r->is_virtual && seen_out.insert(root(r)).second) g->outputs.push_back(root(r));
 
     // fusion
     std::set<LNode *> fused;

@@ -74,8 +74,9 @@ static uint64_t param_signature(Graph *g)
 constexpr int kComputeLanes = 4;
 // image uploads and downloads (copy engines) and array transfers (small kernels reading or
 // writing mapped host memory) get lanes of their own, so none waits behind another kind
-constexpr int kUploadLane = kComputeLanes, kDownloadLane = kComputeLanes + 1, kArrayLane = kComputeLanes + 2;
-constexpr int kNumLanes = kComputeLanes + 3;
+// (two lanes each way: copies of a few MB finish below PCIe rate one at a time)
+constexpr int kUploadLane = kComputeLanes, kDownloadLane = kComputeLanes + 2, kArrayLane = kComputeLanes + 4;
+constexpr int kNumLanes = kComputeLanes + 5;
 
 struct CapPart {
     std::function<int(cudaStream_t)> launch;
@@ -227,7 +228,7 @@ static vx_status capture(Graph *g)
                 Image *img = IMG(r);
                 CapPart cp;
                 cp.wr = {img};
-                cp.lane = kUploadLane;
+                cp.lane = kUploadLane + (int)(g->streamed_in.size() & 1);
                 cp.launch = [img](cudaStream_t q) {
                     for (int i = 0; i < img->num_planes; i++)
                         if (plane_copy(img->planes[i], cudaMemcpyHostToDevice, q) != cudaSuccess) return -1;
@@ -257,7 +258,7 @@ static vx_status capture(Graph *g)
                 Image *img = IMG(r);
                 CapPart cp;
                 cp.rd = {img};
-                cp.lane = kDownloadLane;
+                cp.lane = kDownloadLane + (int)(g->streamed_out.size() & 1);
                 cp.launch = [img](cudaStream_t q) {
                     for (int i = 0; i < img->num_planes; i++)
                         if (plane_copy(img->planes[i], cudaMemcpyDeviceToHost, q) != cudaSuccess) return -1;
@@ -312,7 +313,7 @@ static vx_status capture(Graph *g)
     // order, since uploads are sources), so each lane's FIFO takes frames as they arrive
     std::vector<int> rank(parts.size(), 0), order(parts.size());
     for (int j = 0, up = 0; j < (int)parts.size(); j++) {
-        if (parts[j].lane == kUploadLane) { rank[j] = ++up; continue; }
+        if (parts[j].lane == kUploadLane || parts[j].lane == kUploadLane + 1) { rank[j] = ++up; continue; }
         for (int i : parts[j].deps) rank[j] = std::max(rank[j], rank[i]);
     }
     for (int j = 0; j < (int)parts.size(); j++) order[j] = j;
@@ -510,6 +511,17 @@ vx_status graph_wait(Graph *g)
         return VX_FAILURE;
     }
     cudaEventElapsedTime(&g->gpu_ms_last, g->ev0, g->ev1);
+    // host-imported output images the CUDA graph did not download (pageable buffers, the
+    // serial or uncaptured forms): copy them back, so the application's buffers are current
+    for (Ref *r : g->outputs) {
+        if (r->type != VX_TYPE_IMAGE) continue;
+        Image *root = IMG(r)->parent ? IMG(r)->parent : IMG(r);
+        if (root->import_type == VX_MEMORY_TYPE_HOST && !root->host_valid && image_sync_to_host(root)) {
+            g->state = VX_GRAPH_STATE_ABANDONED;
+            log_error(g, VX_FAILURE, "ERROR: graph output copy to the application's buffer failed\n");
+            return VX_FAILURE;
+        }
+    }
     // arrays the CUDA graph downloaded: their host buffers and counts are current
     for (size_t i = 0; i < g->staged_out.size(); i++) {
         Array *a = g->staged_out[i];

@@ -173,6 +173,19 @@ _PIX = {VX_DF_IMAGE_U8: (np.uint8, 1), VX_DF_IMAGE_U16: (np.uint16, 1), VX_DF_IM
         VX_DF_IMAGE_RGB: (np.uint8, 3), VX_DF_IMAGE_RGBX: (np.uint8, 4), VX_DF_IMAGE_F32_AMD: (np.float32, 1)}
 
 
+def image_plane_layout(fmt, width: int, height: int):
+    """[(rows, pixels per row, bytes per pixel)] of each plane of a U8, RGB, NV12 or IYUV image."""
+    if fmt == VX_DF_IMAGE_U8:
+        return [(height, width, 1)]
+    if fmt == VX_DF_IMAGE_RGB:
+        return [(height, width, 3)]
+    if fmt == VX_DF_IMAGE_NV12:
+        return [(height, width, 1), (height // 2, width // 2, 2)]
+    if fmt == VX_DF_IMAGE_IYUV:
+        return [(height, width, 1), (height // 2, width // 2, 1), (height // 2, width // 2, 1)]
+    raise ValueError(f"no plane layout for format {fmt:#x}")
+
+
 class OpenVX:
     """Typed access to an OpenVX library plus numpy helpers for data exchange."""
 
@@ -281,18 +294,24 @@ class OpenVX:
         self.ok(self.vxQueryImage(img, VX_IMAGE_FORMAT, C.byref(f), 4), "query")
         return w.value, h.value, f.value
 
-    def image_from_host(self, ctx, arr: np.ndarray, fmt=None):
-        """vxCreateImageFromHandle(VX_MEMORY_TYPE_HOST) over an application-owned (H, W)
-        uint8 buffer.  The buffer must outlive the image; when it is page-locked, graphs
-        copy it in (and, for outputs, back) inside their CUDA graph."""
-        h, w = arr.shape[:2]
-        addr = vx_imagepatch_addressing_t()
-        addr.dim_x, addr.dim_y, addr.stride_x, addr.stride_y = w, h, arr.strides[1], arr.strides[0]
-        addr.scale_x = addr.scale_y = 1024
-        addr.step_x = addr.step_y = 1
-        ptrs = (C.c_void_p * 1)(arr.ctypes.data)
-        return self.obj(self.vxCreateImageFromHandle(ctx, VX_DF_IMAGE_U8 if fmt is None else fmt, C.byref(addr), ptrs,
-                                                     VX_MEMORY_TYPE_HOST), "image from handle")
+    def image_from_host(self, ctx, arr, fmt=None, width=None, height=None):
+        """vxCreateImageFromHandle(VX_MEMORY_TYPE_HOST) over application-owned buffers: one
+        (H, W) uint8 array for a U8 image, else a list of per-plane arrays shaped (plane rows,
+        plane row bytes) with `width` x `height` the image size (U8: the array's).  The
+        buffers must outlive the image; when page-locked, graphs copy them in (and, for
+        outputs, back) inside their CUDA graph."""
+        fmt = VX_DF_IMAGE_U8 if fmt is None else fmt
+        planes = [arr] if isinstance(arr, np.ndarray) else list(arr)
+        if width is None:
+            height, width = planes[0].shape[:2]
+        layout = image_plane_layout(fmt, width, height)
+        addrs = (vx_imagepatch_addressing_t * len(planes))()
+        for a, pl, (ph, pw, bpp) in zip(addrs, planes, layout):
+            a.dim_x, a.dim_y, a.stride_x, a.stride_y = pw, ph, bpp, pl.strides[0]
+            a.scale_x = a.scale_y = 1024
+            a.step_x = a.step_y = 1
+        ptrs = (C.c_void_p * len(planes))(*[pl.ctypes.data for pl in planes])
+        return self.obj(self.vxCreateImageFromHandle(ctx, fmt, addrs, ptrs, VX_MEMORY_TYPE_HOST), "image from handle")
 
     def write_plane(self, img, arr: np.ndarray, plane: int = 0, full_w=None, full_h=None):
         """Copy host pixels into plane `plane` (vxCopyImagePatch WRITE_ONLY)."""

@@ -152,7 +152,7 @@ def pyramid_sizes(width: int, height: int, levels: int, scale: float = 0.5) -> l
 def cfg3_frame(seed: int = 3, width: int = 3840, height: int = 2160, waves: int = 8) -> np.ndarray:
     """RGB frame: per channel a sum of `waves` random 2-D sinusoids scaled to 0..255, plus
     uniform noise in [-10, 10], clipped."""
-    yy, xx = np.meshgrid(np.arange(height, dtype=np.float32), np.arange(width, dtype=np.float32), indexing="ij")
+    xs, ys = np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64)
     out = np.empty((height, width, 3), np.uint8)
     p = uniform01(seed, 3 * waves * 4, stream=13)
     for ch in range(3):
@@ -160,7 +160,11 @@ def cfg3_frame(seed: int = 3, width: int = 3840, height: int = 2160, waves: int 
         for k in range(waves):
             a, b, c, d = p[(ch * waves + k) * 4:(ch * waves + k) * 4 + 4]
             fx, fy = (a - 0.5) * 0.02, (b - 0.5) * 0.02
-            acc += np.sin(fx * xx + fy * yy + 2 * np.pi * c).astype(np.float32) * np.float32(0.5 + d)
+            # sin(fx x + fy y + 2 pi c) = sin(fx x) cos(fy y + 2 pi c) + cos(fx x) sin(fy y + 2 pi c)
+            u, v = fy * ys + 2 * np.pi * c, fx * xs
+            amp = np.float32(0.5 + d)
+            acc += np.outer((np.cos(u) * amp).astype(np.float32), np.sin(v).astype(np.float32))
+            acc += np.outer((np.sin(u) * amp).astype(np.float32), np.cos(v).astype(np.float32))
         acc = (acc - acc.min()) / max(1e-6, float(acc.max() - acc.min())) * 255.0
         noise = (uniform01(seed + ch + 1, width * height, stream=17).reshape(height, width) * 20.0 - 10.0).astype(np.float32)
         out[..., ch] = np.clip(np.rint(acc + noise), 0, 255).astype(np.uint8)
@@ -239,24 +243,33 @@ class Cfg3Graph:
     of Y to half size (bilinear and area), WarpAffine of the bilinear result (nearest and
     bilinear, border CONSTANT 0), for each of `sizes` RGB frames, in one graph."""
 
-    def __init__(self, api: V.OpenVX, ctx, sizes, matrices=None, flags: int | None = None):
+    def __init__(self, api: V.OpenVX, ctx, sizes, matrices=None, flags: int | None = None, host_io: dict | None = None):
+        """host_io: application buffers per role ("rgb", "nv12", "iyuv", "sb", "sa", "wn", "wb"),
+        each a list (one per frame) of per-plane arrays."""
+        host_io = host_io or {}
         self.api, self.ctx = api, ctx
         a = api
         self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
         if flags is not None:
             a.set_optimizer_flags(self.graph, flags)
         g = self.graph
+
+        def image(role, i, w, h, fmt):
+            if role in host_io:
+                return a.image_from_host(ctx, host_io[role][i], fmt, w, h)
+            return a.obj(a.vxCreateImage(ctx, w, h, fmt), role)
+
         self.inputs, self.nv12, self.iyuv, self.scaled, self.warped, self.matrices = [], [], [], [], [], []
         for i, (w, h) in enumerate(sizes):
             m = matrices[i] if matrices is not None else cfg3_affine(seed=17 + i, cx=w / 4, cy=h / 4)
-            rgb = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_RGB), "rgb")
-            nv12 = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_NV12), "nv12")
-            iyuv = a.obj(a.vxCreateImage(ctx, w, h, V.VX_DF_IMAGE_IYUV), "iyuv")
+            rgb = image("rgb", i, w, h, V.VX_DF_IMAGE_RGB)
+            nv12 = image("nv12", i, w, h, V.VX_DF_IMAGE_NV12)
+            iyuv = image("iyuv", i, w, h, V.VX_DF_IMAGE_IYUV)
             y = a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_U8)
-            sb = a.obj(a.vxCreateImage(ctx, w // 2, h // 2, V.VX_DF_IMAGE_U8), "scaled")
-            sa = a.obj(a.vxCreateImage(ctx, w // 2, h // 2, V.VX_DF_IMAGE_U8), "scaled")
-            wn = a.obj(a.vxCreateImage(ctx, w // 2, h // 2, V.VX_DF_IMAGE_U8), "warped")
-            wb = a.obj(a.vxCreateImage(ctx, w // 2, h // 2, V.VX_DF_IMAGE_U8), "warped")
+            sb = image("sb", i, w // 2, h // 2, V.VX_DF_IMAGE_U8)
+            sa = image("sa", i, w // 2, h // 2, V.VX_DF_IMAGE_U8)
+            wn = image("wn", i, w // 2, h // 2, V.VX_DF_IMAGE_U8)
+            wb = image("wb", i, w // 2, h // 2, V.VX_DF_IMAGE_U8)
             mat = a.matrix_f32(ctx, m)
             a.obj(a.vxColorConvertNode(g, rgb, nv12), "node")
             a.obj(a.vxColorConvertNode(g, rgb, iyuv), "node")
