@@ -490,10 +490,11 @@ def run_ours(a, wl_name):
 
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (ms_step / 1e3) / 1e9
-    traffic = None
+    traffic, traffic_note = None, None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(wl_name)
+        t = json.load(open(tp)).get(wl_name) or {}
+        traffic, traffic_note = t.get("bytes_per_step"), t.get("note")
     if rank == 0:
         cpu = None
         if ws == 1 and not a.no_cpu_baseline:
@@ -510,7 +511,8 @@ def run_ours(a, wl_name):
                        "l2": "inputs+outputs per step exceed the 126 MB L2 (no flush needed)",
                        "plan": [n for n, _ in plan], "plan_form": "plain" if a.plain else "fused+batched", "parallelism": f"replicas x{ws} (frames sharded, no collective)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_note": traffic_note,
+                         "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel": f"one step: {kernels_per_step} kernels in one CUDA graph"},
             "e2e": {"value": round(e2e, 1), "unit": "Mpixels/s",
                     "h2d_bytes_per_step": sum(p.numel() for ps in pin_in for p in ps) +
