@@ -37,13 +37,13 @@ __device__ __forceinline__ uint32_t ago_byte(const uint8_t *img, size_t stride, 
 }
 
 // ---------------------------------------------------------------------------------
-// ScaleGaussianHalf 5x5.  A thread produces 8 output pixels x 16 output rows.  Pixel
+// ScaleGaussianHalf 5x5.  A thread produces 8 output pixels x 8 output rows.  Pixel
 // pairs live in the two 16-bit halves of a 32-bit register (horizontal sums <= 4080,
 // vertical sums <= 65280, so halves never carry into each other).
 // ---------------------------------------------------------------------------------
-constexpr int kHalfThreads = 64;
+constexpr int kHalfThreads = 32;
 constexpr int kHalfCols = 8 * kHalfThreads;     // output columns per tile
-constexpr int kHalfRows = 16;                   // output rows per tile
+constexpr int kHalfRows = 8;                    // output rows per tile
 
 // ago_byte() for a row inside the image and a column within one AGO row pitch of it
 // (c in [-pitch, 2*pitch)), without division: the edge threads of every tile row use it.
@@ -62,21 +62,26 @@ __device__ __forceinline__ uint32_t ago_byte_row(const uint8_t *img, size_t stri
 
 struct Row24 { uint32_t w[6]; };
 
-// The border path of a row load, kept out of line and rolled: unrolled at every call site it
-// made the kernel's code large enough to thrash the instruction cache.
+// The border path of a row load, kept out of line (inlined at every call site it made the
+// kernel's code large enough to thrash the instruction cache).  The 24 byte loads are
+// independent, so they are all in flight at once.
 __device__ __noinline__ Row24 half_load_row_edge(const uint8_t *src, int stride, int W, int H, int r, int x0)
 {
     Row24 out;
-    const bool near = W >= 24;   // columns [x0, x0 + 24) then lie within one pitch of the row
+    if (W >= 24) {               // columns [x0, x0 + 24) lie within one pitch of the row
+        uint32_t px[24];
+#pragma unroll
+        for (int k = 0; k < 24; k++) px[k] = ago_byte_row(src, stride, W, H, r, x0 + k);
+#pragma unroll
+        for (int k = 0; k < 6; k++)
+            out.w[k] = px[4 * k] | (px[4 * k + 1] << 8) | (px[4 * k + 2] << 16) | (px[4 * k + 3] << 24);
+        return out;
+    }
 #pragma unroll 1
     for (int k = 0; k < 6; k++) {
         uint32_t v = 0;
 #pragma unroll 1
-        for (int b = 0; b < 4; b++) {
-            const int c = x0 + 4 * k + b;
-            const uint32_t px = near ? ago_byte_row(src, stride, W, H, r, c) : ago_byte(src, stride, W, H, r, c);
-            v |= px << (8 * b);
-        }
+        for (int b = 0; b < 4; b++) v |= ago_byte(src, stride, W, H, r, x0 + 4 * k + b) << (8 * b);
         out.w[k] = v;
     }
     return out;
@@ -235,12 +240,15 @@ __device__ __forceinline__ void lk_weights(float a, float b, int w[4])
 
 constexpr unsigned kWrX = 1, kWrY = 2, kWrStrength = 4, kWrStatus = 8, kWrError = 16;
 
+// WIN > 0: the window size as a compile-time constant (index arithmetic without divisions);
+// WIN == 0: any window size from the frame descriptor
+template <int WIN>
 __device__ void lk_track_point(const agocuda_lk_frame &F, uint32_t pt, LkWarpSmem &S, int lane, uint32_t *pStatus)
 {
     const vx_keypoint_like *oldKP = (const vx_keypoint_like *)F.oldPoints;
     const vx_keypoint_like *estKP = (const vx_keypoint_like *)F.estPoints;
     vx_keypoint_like *outKP = (vx_keypoint_like *)F.newPoints;
-    const int win = F.windowDimension;
+    const int win = WIN > 0 ? WIN : F.windowDimension;
     const float fHalf = (float)(win >> 1);
     const vx_keypoint_like o = oldKP[pt];
     if (!o.tracking_status) {                          // untracked input: copied (opticalflow.cpp:199)
@@ -523,13 +531,16 @@ __device__ void lk_track_point(const agocuda_lk_frame &F, uint32_t pt, LkWarpSme
     (void)pStatus;
 }
 
-__global__ void __launch_bounds__(kLkWarps * 32) k_lk_track(agocuda_lk_frame *frames, uint32_t *pStatus)
+// 4 resident blocks (64 registers): the tracking loop is latency-bound, more warps beat the
+// few register spills this costs
+__global__ void __launch_bounds__(kLkWarps * 32, 4) k_lk_track(agocuda_lk_frame *frames, uint32_t *pStatus)
 {
     __shared__ LkWarpSmem smem[kLkWarps];
     const agocuda_lk_frame &F = frames[blockIdx.y];
     const uint32_t pt = blockIdx.x * kLkWarps + (threadIdx.x >> 5);
     if (pt >= F.count) return;
-    lk_track_point(F, pt, smem[threadIdx.x >> 5], threadIdx.x & 31, pStatus);
+    if (F.windowDimension == 9) lk_track_point<9>(F, pt, smem[threadIdx.x >> 5], threadIdx.x & 31, pStatus);
+    else lk_track_point<0>(F, pt, smem[threadIdx.x >> 5], threadIdx.x & 31, pStatus);
 }
 
 // Replays the reference's Scharr row-buffer writes (ComputeSharr, opticalflow.cpp:65): per
