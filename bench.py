@@ -261,13 +261,21 @@ def _dist():
 
 
 def _max_over_ranks(x: float, ws: int) -> float:
+    """Max of a per-rank time over the process group (NCCL on the GPU, gloo on the host)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def frame_seed(rank: int) -> int:
+    """First frame seed of a rank: every rank processes its own frames (weak scaling, no
+    data collective), so whole-job throughput is the sum over ranks."""
+    return 1000 * rank + 1
 
 
 def _barrier(ws):
@@ -374,7 +382,7 @@ def run_ours(a, wl_name):
     lib = native.agocuda()
     ctx = api.obj(api.vxCreateContext(), "context")
     api.set_device(ctx, local)
-    frames = wl.make_frames(1000 * rank + 1, B)
+    frames = wl.make_frames(frame_seed(rank), B)
     g = wl.build(api, ctx, B, flags=V.OPT_NO_FUSION if a.plain else None)
     plan = api.plan(g.graph)
     kernels_per_step = sum(k for _, k in plan)
