@@ -288,14 +288,15 @@ __device__ __forceinline__ int sG_mag3(uint32_t g) { return (int)(g | 3u); }   /
 
 __global__ void __launch_bounds__(256, 4)
 k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, int lower, int upper,
-                  uint16_t *__restrict__ lab16, int labPitch, int *__restrict__ uf, uint32_t *__restrict__ bits)
+                  uint16_t *__restrict__ lab16, int labPitch, int *__restrict__ uf, uint32_t *__restrict__ bits,
+                  uint32_t *__restrict__ roots)
 {
     __shared__ __align__(16) uint32_t sIn[kIH][kInWords];
     __shared__ __align__(16) uint16_t sG[kGH][kGC];
     __shared__ __align__(16) int sLab[kTS];
     __shared__ unsigned long long sNZ[kTH], sST[kTH];   // per tile row: non-zero / strong pixels
     __shared__ int16_t sV[kIH];                          // per gradient row: vertical sum of column W-1
-    __shared__ uint32_t sStrongRoot[kTS / 32];
+    __shared__ uint32_t sStrongRoot[kTS / 32], sRoot[kTS / 32];
     const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH, tid = threadIdx.x;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x;
 
@@ -314,7 +315,7 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
         }
         sIn[r][q] = w;
     }
-    if (tid < kTS / 32) sStrongRoot[tid] = 0;
+    if (tid < kTS / 32) { sStrongRoot[tid] = 0; sRoot[tid] = 0; }
     const bool needV = x0 == 0 && (W & 15) == 0 && W >= 16;
     if (needV && tid < kGH) {
         const int y = y0 - 1 + tid;
@@ -466,11 +467,16 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
         }
         *(uint4 *)&lab16[(size_t)y * labPitch + x0 + c0] = make_uint4(w[0], w[1], w[2], w[3]);
     }
+    uint32_t own = 0;                      // local roots among this thread's 8 pixels
 #pragma unroll
     for (int j = 0; j < 8; j++)
-        if (root[j] == i0 + j) uf[(size_t)tile * kTS + i0 + j] = tile * kTS + i0 + j;
+        if (root[j] == i0 + j) { uf[(size_t)tile * kTS + i0 + j] = tile * kTS + i0 + j; own |= 1u << j; }
+    if (own) atomicOr(&sRoot[i0 >> 5], own << (i0 & 31));
     __syncthreads();
-    if (tid < kTS / 32) bits[(size_t)tile * (kTS / 32) + tid] = sStrongRoot[tid];
+    if (tid < kTS / 32) {
+        bits[(size_t)tile * (kTS / 32) + tid] = sStrongRoot[tid];
+        roots[(size_t)tile * (kTS / 32) + tid] = sRoot[tid];
+    }
 }
 
 __device__ __forceinline__ int slot_of(const uint16_t *lab16, int labPitch, int tilesX, int x, int y)
@@ -520,9 +526,25 @@ __global__ void k_canny_ccl_mark(const int *uf, uint32_t *bits, uint32_t words)
     }
 }
 
-// 8 pixels per thread: labels -> final roots -> 0/255
+// every local root: the strong bit of its component's final root, kept in the root bitmap
+// (each word is rewritten by the one thread that reads it)
+__global__ void k_canny_ccl_resolve(const int *uf, const uint32_t *bits, uint32_t *roots, uint32_t words)
+{
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+        uint32_t m = roots[w], strong = 0;
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            const int r = uf_find_ro(uf, (int)(w * 32 + b));
+            if ((__ldg(bits + (r >> 5)) >> (r & 31)) & 1) strong |= 1u << b;
+        }
+        roots[w] = strong;
+    }
+}
+
+// 8 pixels per thread: local label -> its local root's resolved strong bit -> 0/255
 __global__ void k_canny_ccl_output(int W, int H, const uint16_t *__restrict__ lab16, int labPitch, int tilesX,
-                                   const int *uf, const uint32_t *bits, uint8_t *__restrict__ out, int outStride)
+                                   const uint32_t *__restrict__ strongRoots, uint8_t *__restrict__ out, int outStride)
 {
     const int x = (blockIdx.x * blockDim.x + threadIdx.x) * 8, y = blockIdx.y;
     if (x >= W) return;
@@ -538,9 +560,8 @@ __global__ void k_canny_ccl_output(int W, int H, const uint16_t *__restrict__ la
         if (l == kNoLabel) continue;
         const int slot = tileBase + l;
         if (slot != lastSlot) {
-            const int r = uf_find_ro(uf, slot);
             lastSlot = slot;
-            lastVal = (__ldg(bits + (r >> 5)) >> (r & 31)) & 1 ? 255 : 0;
+            lastVal = (__ldg(strongRoots + (slot >> 5)) >> (slot & 31)) & 1 ? 255 : 0;
         }
         v[k] = (uint8_t)lastVal;
     }
@@ -1059,7 +1080,7 @@ extern "C" size_t agocuda_CannyEdgeTrace_noalloc_max_pixels(void) { return kNoAl
 
 // scratch of the fused Canny: tile-local labels (u16, pitched), the global union-find over
 // tile slots (int per slot) and the strong-root bitmap (one bit per slot)
-struct CannyScratch { uint16_t *lab; int labPitch; int *uf; uint32_t *bits; size_t bytes; int tilesX, tilesY; };
+struct CannyScratch { uint16_t *lab; int labPitch; int *uf; uint32_t *bits, *roots; size_t bytes; int tilesX, tilesY; };
 
 static CannyScratch canny_scratch_layout(uint32_t W, uint32_t H, void *base)
 {
@@ -1071,12 +1092,13 @@ static CannyScratch canny_scratch_layout(uint32_t W, uint32_t H, void *base)
     const size_t labBytes = ((size_t)c.labPitch * H * 2 + 255) & ~(size_t)255;
     const size_t ufBytes = (slots * 4 + 255) & ~(size_t)255;
     const size_t bitBytes = ((slots / 8) + 255) & ~(size_t)255;
-    c.bytes = labBytes + ufBytes + bitBytes;
+    c.bytes = labBytes + ufBytes + 2 * bitBytes;
     if (base) {
         uint8_t *p = (uint8_t *)base;
         c.lab = (uint16_t *)p;
         c.uf = (int *)(p + labBytes);
         c.bits = (uint32_t *)(p + labBytes + ufBytes);
+        c.roots = (uint32_t *)(p + labBytes + ufBytes + bitBytes);
     }
     return c;
 }
@@ -1093,14 +1115,15 @@ extern "C" int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t W, 
     cudaStream_t s = as_stream(stream);
     const int tiles = c.tilesX * c.tilesY;
     k_canny_ccl_front<<<dim3(c.tilesX, c.tilesY), 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper,
-                                                               c.lab, c.labPitch, c.uf, c.bits);
+                                                               c.lab, c.labPitch, c.uf, c.bits, c.roots);
     constexpr int kPer = kTH + kTW + kTH;
     k_canny_ccl_border<<<dim3(div_up(kPer, 128), tiles), 128, 0, s>>>((int)W, (int)H, c.lab, c.labPitch, c.tilesX, c.uf, pStatus);
     const uint32_t words = (uint32_t)tiles * (kTS / 32);
     k_canny_ccl_mark<<<div_up(words, 256), 256, 0, s>>>(c.uf, c.bits, words);
-    k_canny_ccl_output<<<dim3(div_up(div_up(W, 8), 128), H), 128, 0, s>>>((int)W, (int)H, c.lab, c.labPitch, c.tilesX, c.uf,
-                                                                          c.bits, pDst, (int)dstStride);
-    agocuda_count_launch(4);
+    k_canny_ccl_resolve<<<div_up(words, 256), 256, 0, s>>>(c.uf, c.bits, c.roots, words);
+    k_canny_ccl_output<<<dim3(div_up(div_up(W, 8), 128), H), 128, 0, s>>>((int)W, (int)H, c.lab, c.labPitch, c.tilesX,
+                                                                          c.roots, pDst, (int)dstStride);
+    agocuda_count_launch(5);
     return agocuda_launch_status();
 }
 
