@@ -390,25 +390,39 @@ typedef struct agocuda_lk_frame {
     int32_t useInitialEstimate, windowDimension;
     uint32_t count;
     uint32_t scharrWords[AGOCUDA_LK_MAX_LEVELS][2];
+    /* Per node, kept between calls (zeroed before the first): level-0 Scharr (gx, gy) pairs of
+     * the previous call at columns [W_l & ~7, W_l - 3] of every level l >= 1 -- derivative
+     * words the reference reads at level l but only its previous call's level 0 wrote.
+     * Layout [level - 1][column - (W_l & ~7)][row], AGOCUDA_LK_CARRY_COLUMNS columns of
+     * carryRows rows (>= the level-1 height).  NULL: those words read as 0. */
+    int32_t *carry;
+    uint32_t carryRows;
 } agocuda_lk_frame;
+#define AGOCUDA_LK_CARRY_COLUMNS 5
 size_t agocuda_OpticalFlowPyrLK_scharr_rows_size(uint32_t width0);
+/* Bytes of the carry buffer for a pyramid of `levels` levels whose level 1 is height1 rows. */
+size_t agocuda_OpticalFlowPyrLK_carry_size(uint32_t levels, uint32_t height1);
 
-/* Pyramidal LK for many frame pairs in two launches (row-buffer replay + one warp per
- * keypoint).  `frames` is a DEVICE array; maxPoints bounds every frame's count.  Results are
- * identical to HafCpu_OpticalFlowPyrLK_XY_XY_Generic (ago_haf_cpu_opticalflow.cpp:153; CPU
- * only in the reference, ago_kernel_api.cpp:20587) for HALF pyramids whose level widths are
- * all >= 8.  One exception: on a level above 0 whose width % 8 >= 3 the reference's window
- * can reach derivative columns [W & ~7, W - 3], which it never writes at that level; on a
- * node's first call they hold 0, on later calls the previous frame's level-0 derivatives.
- * These kernels always use 0 there (the first-call value). */
+/* Pyramidal LK for many frame pairs in three launches (row-buffer replay, one warp per
+ * keypoint, carry of the level-0 derivative columns for the next call).  `frames` is a DEVICE
+ * array; maxPoints bounds every frame's count.  Results are identical to
+ * HafCpu_OpticalFlowPyrLK_XY_XY_Generic (ago_haf_cpu_opticalflow.cpp:153; CPU only in the
+ * reference, ago_kernel_api.cpp:20587) for HALF pyramids whose level widths are all >= 8,
+ * over consecutive calls too: on a level above 0 whose width % 8 >= 3 the reference's window
+ * can reach derivative columns [W & ~7, W - 3], which it never writes at that level -- they
+ * hold 0 on a node's first call and the previous call's level-0 derivatives afterwards; the
+ * frame's `carry` buffer provides exactly those (without one they read as 0). */
 int agocuda_OpticalFlowPyrLK_batch(void *stream, agocuda_lk_frame *frames, uint32_t numFrames, uint32_t maxPoints,
                                    uint32_t *pStatus);
 
 /* Single node with the reference's argument meaning.  oldPyramid/newPyramid are HOST arrays
  * of `levels` descriptors (device images); counts are device words.  scratch (device,
- * agocuda_OpticalFlowPyrLK_scratch_size(width0) bytes, zeroed before the node's first call
- * and kept between calls) holds the frame descriptor and the Scharr row-buffer state. */
+ * zeroed before the node's first call and kept between calls) holds the frame descriptor and
+ * the Scharr row-buffer state: agocuda_OpticalFlowPyrLK_scratch_size(width0) bytes, or
+ * agocuda_OpticalFlowPyrLK_scratch_size_carry(width0, height0, levels) bytes to also carry the
+ * level-0 derivative columns between calls (see agocuda_OpticalFlowPyrLK_batch). */
 size_t agocuda_OpticalFlowPyrLK_scratch_size(uint32_t width0);
+size_t agocuda_OpticalFlowPyrLK_scratch_size_carry(uint32_t width0, uint32_t height0, uint32_t levels);
 int agocuda_OpticalFlowPyrLK_XY_XY(void *stream, void *newKeyPoint, uint32_t newCapacity, uint32_t *pNewCount,
                                    float pyramidScale, uint32_t levels, const agocuda_pyramid_level *oldPyramid,
                                    const agocuda_pyramid_level *newPyramid, const uint32_t *pKeyPointCount,

@@ -137,6 +137,13 @@ static vx_status lk_frame(Graph *g, LNode &ln, agocuda_lk_frame &F, uint32_t &ca
     void *rows = scratch(g, agocuda_OpticalFlowPyrLK_scharr_rows_size(po->level[0]->width));
     if (!rows) return VX_ERROR_NO_MEMORY;
     F.scharrRows = (uint16_t *)rows;
+    if (po->levels > 1) {   // level-0 derivative columns carried to the next execution (zeroed: none yet)
+        const uint32_t h1 = pyr_level(g, po, 1)->height;
+        void *carry = scratch(g, agocuda_OpticalFlowPyrLK_carry_size((uint32_t)po->levels, h1));
+        if (!carry) return VX_ERROR_NO_MEMORY;
+        F.carry = (int32_t *)carry;
+        F.carryRows = h1;
+    }
     cap = (uint32_t)old->capacity;
     return VX_SUCCESS;
 }
@@ -161,7 +168,7 @@ static vx_status lk_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step
         fns.push_back([=](cudaStream_t q) { return agocuda_OpticalFlowPyrLK_batch(S(q), d0, n, pts, status); });
         st.parts.push_back(Part{fns.back(), std::vector<LNode *>(nodes.begin() + k0, nodes.begin() + k1)});
     }
-    st.num_kernels = 2 * (int)fns.size();
+    st.num_kernels = 3 * (int)fns.size();
     st.launch = [fns](cudaStream_t q) {
         for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
         return 0;

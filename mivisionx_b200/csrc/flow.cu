@@ -324,7 +324,14 @@ __device__ void lk_track_point(const agocuda_lk_frame &F, uint32_t pt, LkWarpSme
             for (int i = lane; i < Q * Q; i += 32) {
                 const int y = i / Q, x = i % Q, gr = ipy + y, gc = ipx + x;
                 int gx = 0, gy = 0;
-                if (gr > 0 && gc < W8) {
+                if (gr > 0 && gc >= W8 && level > 0) {   // the previous call's level-0 derivative here
+                    const int j = gc - W8;
+                    if (F.carry && j < AGOCUDA_LK_CARRY_COLUMNS && gr < (int)F.carryRows) {
+                        const int32_t v = F.carry[((level - 1) * AGOCUDA_LK_CARRY_COLUMNS + j) * (int)F.carryRows + gr];
+                        gx = (int16_t)(v & 0xFFFF);
+                        gy = (int16_t)((uint32_t)v >> 16);
+                    }
+                } else if (gr > 0 && gc < W8) {
                     const uint8_t *r0 = &S.u.s.img[y * P + x + 1], *r1 = r0 + P, *r2 = r1 + P;  // column gc
                     const int v1c = (int)r2[0] - (int)r0[0];
                     int v0l, v1l, v0r, v1r;
@@ -578,6 +585,34 @@ __global__ void __launch_bounds__(256) k_lk_prep(agocuda_lk_frame *frames, uint3
     }
 }
 
+// After tracking: the level-0 Scharr derivative of this call's old image at the columns
+// [W_l & ~7, W_l - 3] of every level l >= 1, which the next call's level l reads (the
+// reference's derivative buffer has the level-0 row pitch at every level, and only level 0
+// reaches those words).  Rows 1 .. H_l - 3; row 0 is never written and stays 0.
+__global__ void __launch_bounds__(256) k_lk_carry(const agocuda_lk_frame *frames)
+{
+    const agocuda_lk_frame &F = frames[blockIdx.x];
+    if (!F.carry) return;
+    const agocuda_pyramid_level L0 = F.oldPyr[0];
+    for (int level = 1; level < (int)F.levels; level++) {
+        const int Wl = (int)F.oldPyr[level].width, Hl = (int)F.oldPyr[level].height, W8 = Wl & ~7;
+        const int cols = min(Wl - 2 - W8, AGOCUDA_LK_CARRY_COLUMNS), rows = min(Hl - 2, (int)F.carryRows);
+        if (cols <= 0 || rows <= 1) continue;
+        for (int i = threadIdx.x; i < cols * rows; i += blockDim.x) {
+            const int j = i / rows, y = i - j * rows, x = W8 + j;
+            int32_t v = 0;
+            if (y >= 1) {
+                const uint8_t *r0 = L0.image + (size_t)(y - 1) * L0.stride, *r1 = r0 + L0.stride, *r2 = r1 + L0.stride;
+                const int t0l = 3 * (r0[x - 1] + r2[x - 1]) + 10 * r1[x - 1], t0r = 3 * (r0[x + 1] + r2[x + 1]) + 10 * r1[x + 1];
+                const int t1l = (int)r2[x - 1] - (int)r0[x - 1], t1c = (int)r2[x] - (int)r0[x], t1r = (int)r2[x + 1] - (int)r0[x + 1];
+                const uint32_t gx = (uint16_t)(t0r - t0l), gy = (uint16_t)(3 * (t1l + t1r) + 10 * t1c);
+                v = (int32_t)(gx | (gy << 16));
+            }
+            F.carry[((level - 1) * AGOCUDA_LK_CARRY_COLUMNS + j) * (int)F.carryRows + y] = v;
+        }
+    }
+}
+
 __global__ void k_lk_store_frame(const agocuda_lk_frame F, agocuda_lk_frame *dst)
 {
     if (threadIdx.x == 0) {
@@ -643,7 +678,20 @@ extern "C" int agocuda_OpticalFlowPyrLK_batch(void *stream, agocuda_lk_frame *fr
         k_lk_track<<<dim3((maxPoints + kLkWarps - 1) / kLkWarps, numFrames), kLkWarps * 32, 0, s>>>(frames, pStatus);
         agocuda_count_launch(1);
     }
+    k_lk_carry<<<numFrames, 256, 0, s>>>(frames);
+    agocuda_count_launch(1);
     return agocuda_launch_status();
+}
+
+extern "C" size_t agocuda_OpticalFlowPyrLK_carry_size(uint32_t levels, uint32_t height1)
+{
+    return levels > 1 ? (size_t)(levels - 1) * AGOCUDA_LK_CARRY_COLUMNS * height1 * sizeof(int32_t) : 0;
+}
+
+extern "C" size_t agocuda_OpticalFlowPyrLK_scratch_size_carry(uint32_t width0, uint32_t height0, uint32_t levels)
+{
+    return ((agocuda_OpticalFlowPyrLK_scratch_size(width0) + 255) & ~(size_t)255) +
+           agocuda_OpticalFlowPyrLK_carry_size(levels, (height0 + 1) / 2);
 }
 
 extern "C" size_t agocuda_OpticalFlowPyrLK_scratch_size(uint32_t width0)
@@ -692,6 +740,10 @@ extern "C" int agocuda_OpticalFlowPyrLK_XY_XY(void *stream, void *newKeyPoint, u
     F.windowDimension = windowDimension;
     auto *dev = (agocuda_lk_frame *)scratch;
     F.scharrRows = (uint16_t *)((uint8_t *)scratch + ((sizeof(agocuda_lk_frame) + 255) & ~(size_t)255));
+    if (levels > 1 && scratchBytes >= agocuda_OpticalFlowPyrLK_scratch_size_carry(oldPyramid[0].width, oldPyramid[0].height, levels)) {
+        F.carry = (int32_t *)((uint8_t *)scratch + ((agocuda_OpticalFlowPyrLK_scratch_size(oldPyramid[0].width) + 255) & ~(size_t)255));
+        F.carryRows = oldPyramid[1].height;
+    }
     cudaStream_t s = as_stream(stream);
     k_lk_store_frame<<<1, 32, 0, s>>>(F, dev);
     agocuda_count_launch(1);

@@ -55,7 +55,7 @@ class LkFrame(C.Structure):
                 ("oldPoints", vp), ("estPoints", vp), ("newPoints", vp), ("pOldCount", vp), ("pEstCount", vp),
                 ("pNewCount", vp), ("scharrRows", vp), ("newCapacity", u32), ("levels", u32), ("termination", i32),
                 ("epsilon", f32), ("numIterations", u32), ("useInitialEstimate", i32), ("windowDimension", i32),
-                ("count", u32), ("scharrWords", (u32 * 2) * LK_MAX_LEVELS)]
+                ("count", u32), ("scharrWords", (u32 * 2) * LK_MAX_LEVELS), ("carry", vp), ("carryRows", u32)]
 
 
 def agocuda() -> C.CDLL:

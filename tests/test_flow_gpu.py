@@ -27,6 +27,10 @@ def lib(cuda):
     L.agocuda_OpticalFlowPyrLK_scratch_size.restype = sz
     L.agocuda_OpticalFlowPyrLK_scharr_rows_size.argtypes = [u32]
     L.agocuda_OpticalFlowPyrLK_scharr_rows_size.restype = sz
+    L.agocuda_OpticalFlowPyrLK_scratch_size_carry.argtypes = [u32, u32, u32]
+    L.agocuda_OpticalFlowPyrLK_scratch_size_carry.restype = sz
+    L.agocuda_OpticalFlowPyrLK_carry_size.argtypes = [u32, u32]
+    L.agocuda_OpticalFlowPyrLK_carry_size.restype = sz
     L.agocuda_OpticalFlowPyrLK_XY_XY.argtypes = [vp, vp, u32, vp, f32, u32, vp, vp, vp, vp, vp, vp, i32, f32, u32, i32,
                                                  i32, vp, sz, vp]
     L.agocuda_OpticalFlowPyrLK_batch.argtypes = [vp, vp, u32, u32, vp]
@@ -115,21 +119,27 @@ def oracle_lk(f1, f2, levels, old_kp, est_kp, term, eps, iters, use_est, win, sc
 
 def first_call_only(W, levels):
     """Levels above 0 with width % 8 >= 3 read derivative columns the reference wrote in an
-    earlier call; the kernels reproduce the first call there (header note)."""
+    earlier call; without a carry buffer the kernels reproduce the first call there."""
     return any(w % 8 >= 3 for (w, _) in WL.pyramid_sizes(W, 8, levels)[1:])
 
 
-@pytest.mark.parametrize("W,H,levels,win,term,eps,iters,use_est", PF.CASES + [(640, 480, 5, 9, PF.TERM_BOTH, 0.01, 20, 0)])
-def test_lk_single_node_matches_oracle_over_two_calls(lib, W, H, levels, win, term, eps, iters, use_est):
+@pytest.mark.parametrize("carry", [True, False])
+@pytest.mark.parametrize("W,H,levels,win,term,eps,iters,use_est", PF.CASES + [(640, 480, 5, 9, PF.TERM_BOTH, 0.01, 20, 0),
+                                                                           (320, 240, 5, 9, PF.TERM_BOTH, 0.01, 20, 0)])
+def test_lk_single_node_matches_oracle_over_calls(lib, W, H, levels, win, term, eps, iters, use_est, carry):
+    """Three consecutive calls of one node (its scratch state carries over); with the carry
+    buffer every call is identical to the oracle, without it the calls after the first only
+    where no level above 0 has width % 8 >= 3."""
     import torch
 
     from devbuf import stream_ptr
     n = 600 if W < 640 else 2000
-    scratch = torch.zeros(lib.agocuda_OpticalFlowPyrLK_scratch_size(W) + 256, dtype=torch.uint8, device="cuda")
+    size = lib.agocuda_OpticalFlowPyrLK_scratch_size_carry(W, H, levels) if carry else lib.agocuda_OpticalFlowPyrLK_scratch_size(W)
+    scratch = torch.zeros(size + 256, dtype=torch.uint8, device="cuda")
     sbase = scratch.data_ptr() + (-scratch.data_ptr() % 256)
     oscratch = PF.lk_scratch(W, H, n)
     status = torch.zeros(4, dtype=torch.int32, device="cuda")
-    for call in range(2):
+    for call in range(3):
         f1, f2, old_kp, est_kp = frame_case(W, H, levels, call, n)
         old_lv, new_lv = gpu_pyramid(lib, f1, levels), gpu_pyramid(lib, f2, levels)
         d_old, d_est = dev_bytes(old_kp), dev_bytes(est_kp)
@@ -145,7 +155,7 @@ def test_lk_single_node_matches_oracle_over_two_calls(lib, W, H, levels, win, te
         got = d_out.cpu().numpy().view(KP)
         want = oracle_lk(f1, f2, levels, old_kp, est_kp, term, eps, iters, use_est, win, oscratch)
         assert int(status[0]) == 0 and int(cnt[2]) == n
-        if call == 1 and first_call_only(W, levels):
+        if call > 0 and not carry and first_call_only(W, levels):
             continue
         bad = np.nonzero(got != want)[0]
         assert bad.size == 0, f"call {call}: {bad.size} keypoints differ, first {bad[:5]}: {got[bad[:3]]} vs {want[bad[:3]]}"
