@@ -45,61 +45,57 @@ constexpr int kHalfThreads = 32;
 constexpr int kHalfCols = 8 * kHalfThreads;     // output columns per tile
 constexpr int kHalfRows = 8;                    // output rows per tile
 
-// ago_byte() for a row inside the image and a column within one AGO row pitch of it
-// (c in [-pitch, 2*pitch)), without division: the edge threads of every tile row use it.
-__device__ __forceinline__ uint32_t ago_byte_row(const uint8_t *img, size_t stride, int W, int H, int r, int c)
+// One word of a row whose 4 columns [c, c+4) reach outside [0, W): ago_byte() per byte,
+// kept out of line (inlined at every call site it made the kernel's code large enough to
+// thrash the instruction cache).  Columns within one AGO row pitch of the row (W >= 24)
+// skip the division, and the 4 loads issue back to back.
+__device__ __noinline__ uint32_t half_edge_word(const uint8_t *src, int stride, int W, int H, int r, int c)
 {
-    if (c >= 0 && c < W) return img[(size_t)r * stride + c];
-    const int S = (W + 15) & ~15;
-    if (c < 0) {                                   // previous row's tail (padding unless W % 16 == 0)
-        const int cc = c + S;
-        return (r > 0 && cc < W) ? img[(size_t)(r - 1) * stride + cc] : 0;
-    }
-    if (c < S) return 0;                           // this row's padding
-    const int cc = c - S;                          // next row's head
-    return (r + 1 < H && cc < W) ? img[(size_t)(r + 1) * stride + cc] : 0;
-}
-
-struct Row24 { uint32_t w[6]; };
-
-// The border path of a row load, kept out of line (inlined at every call site it made the
-// kernel's code large enough to thrash the instruction cache).  The 24 byte loads are
-// independent, so they are all in flight at once.
-__device__ __noinline__ Row24 half_load_row_edge(const uint8_t *src, int stride, int W, int H, int r, int x0)
-{
-    Row24 out;
-    if (W >= 24) {               // columns [x0, x0 + 24) lie within one pitch of the row
-        uint32_t px[24];
+    uint32_t out = 0;
+    if (W >= 24) {
+        const int S = (W + 15) & ~15;
+        const uint8_t *ptr[4];
+        bool ok[4];
 #pragma unroll
-        for (int k = 0; k < 24; k++) px[k] = ago_byte_row(src, stride, W, H, r, x0 + k);
+        for (int k = 0; k < 4; k++) {
+            const int cc0 = c + k;
+            int rr = r, cc = cc0;
+            bool v = true;
+            if (cc0 < 0) { rr = r - 1; cc = cc0 + S; v = r > 0 && cc < W; }
+            else if (cc0 >= W) { rr = r + 1; cc = cc0 - S; v = cc0 >= S && r + 1 < H && cc < W; }
+            ok[k] = v;
+            ptr[k] = v ? src + (size_t)rr * stride + cc : src;
+        }
+        uint32_t px[4];
 #pragma unroll
-        for (int k = 0; k < 6; k++)
-            out.w[k] = px[4 * k] | (px[4 * k + 1] << 8) | (px[4 * k + 2] << 16) | (px[4 * k + 3] << 24);
+        for (int k = 0; k < 4; k++) px[k] = *ptr[k];
+#pragma unroll
+        for (int k = 0; k < 4; k++) out |= (ok[k] ? px[k] : 0u) << (8 * k);
         return out;
     }
 #pragma unroll 1
-    for (int k = 0; k < 6; k++) {
-        uint32_t v = 0;
-#pragma unroll 1
-        for (int b = 0; b < 4; b++) v |= ago_byte(src, stride, W, H, r, x0 + 4 * k + b) << (8 * b);
-        out.w[k] = v;
-    }
+    for (int k = 0; k < 4; k++) out |= ago_byte(src, stride, W, H, r, c + k) << (8 * k);
     return out;
 }
 
-// Six words covering source bytes [x0, x0 + 24) of row r, x0 = 2*ox - 4.
+// Six words covering source bytes [x0, x0 + 24) of row r, x0 = 2*ox - 4 (a multiple of 4):
+// words inside the row load directly, the border ones go through half_edge_word
 __device__ __forceinline__ void half_load_row(const agocuda_half_job &J, int r, int x0, bool edge, uint32_t w[6])
 {
+    const uint8_t *p = J.src + (size_t)r * J.srcStride + x0;
     if (!edge) {
-        const uint8_t *p = J.src + (size_t)r * J.srcStride + x0;
         w[0] = *(const uint32_t *)p;
         const uint4 m = *(const uint4 *)(p + 4);
         w[1] = m.x; w[2] = m.y; w[3] = m.z; w[4] = m.w;
         w[5] = *(const uint32_t *)(p + 20);
     } else {
-        const Row24 e = half_load_row_edge(J.src, (int)J.srcStride, (int)J.srcW, (int)J.srcH, r, x0);
+        const int W = (int)J.srcW;
 #pragma unroll
-        for (int k = 0; k < 6; k++) w[k] = e.w[k];
+        for (int k = 0; k < 6; k++) {
+            const int c = x0 + 4 * k;
+            w[k] = (c >= 0 && c + 4 <= W) ? *(const uint32_t *)(p + 4 * k)
+                                          : half_edge_word(J.src, (int)J.srcStride, W, (int)J.srcH, r, c);
+        }
     }
 }
 
