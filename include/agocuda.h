@@ -444,6 +444,15 @@ int agocuda_OpticalFlowPyrLK_XY_XY(void *stream, void *newKeyPoint, uint32_t new
  * nothing when *countSlot == AGOCUDA_ARRAY_SKIP. */
 int agocuda_array_upload(void *stream, void *devItems, uint32_t *devCount, const void *hostItemsMapped,
                          const uint32_t *countSlotMapped, uint32_t itemSize, uint32_t capacity);
+/* agocuda_array_upload for `count` arrays in one launch; `xfers` is a DEVICE array. */
+typedef struct agocuda_array_xfer {
+    void *devItems;
+    uint32_t *devCount;
+    const void *hostItemsMapped;
+    const uint32_t *countSlotMapped;
+    uint32_t itemSize, capacity;
+} agocuda_array_xfer;
+int agocuda_array_upload_batch(void *stream, const agocuda_array_xfer *xfers, uint32_t count);
 /* hostItems[0 .. n) = devItems[0 .. n), *countSlot = n, n = min(*devCount, capacity). */
 int agocuda_array_download(void *stream, void *hostItemsMapped, uint32_t *countSlotMapped, const void *devItems,
                            const uint32_t *devCount, uint32_t itemSize, uint32_t capacity);

@@ -207,21 +207,31 @@ static vx_status capture(Graph *g)
             return VX_ERROR_NO_MEMORY;
     }
     auto slot_free = [&]() { return g->staged_in.size() + g->staged_out.size() < kIoSlots; };
-    if (!serial)
+    if (!serial) {   // all input arrays in one launch (a table in device memory)
+        std::vector<agocuda_array_xfer> xf;
+        CapPart cp;
         for (Ref *r : g->inputs)
             if (r->type == VX_TYPE_ARRAY && slot_free() && stageable(static_cast<Array *>(r))) {
                 Array *a = static_cast<Array *>(r);
-                const uint32_t *slot = g->io_slots_dev + g->staged_in.size();
-                CapPart cp;
-                cp.wr = {a};
-                cp.lane = kArrayLane;
-                cp.launch = [a, slot](cudaStream_t q) {
-                    return agocuda_array_upload(q, a->dev, a->dev_count, a->host_mapped, slot, (uint32_t)a->item_size,
-                                                (uint32_t)a->capacity);
-                };
-                parts.push_back(std::move(cp));
+                xf.push_back(agocuda_array_xfer{a->dev, a->dev_count, a->host_mapped, g->io_slots_dev + g->staged_in.size(),
+                                                (uint32_t)a->item_size, (uint32_t)a->capacity});
+                cp.wr.push_back(a);
                 g->staged_in.push_back(a);
             }
+        if (!xf.empty()) {
+            void *table = nullptr;
+            if (cudaMalloc(&table, xf.size() * sizeof(agocuda_array_xfer)) != cudaSuccess) return VX_ERROR_NO_MEMORY;
+            g->dev_scratch.push_back(table);
+            if (cudaMemcpy(table, xf.data(), xf.size() * sizeof(agocuda_array_xfer), cudaMemcpyHostToDevice) != cudaSuccess)
+                return VX_FAILURE;
+            const uint32_t n = (uint32_t)xf.size();
+            cp.lane = kArrayLane;
+            cp.launch = [table, n](cudaStream_t q) {
+                return agocuda_array_upload_batch(q, (const agocuda_array_xfer *)table, n);
+            };
+            parts.push_back(std::move(cp));
+        }
+    }
     if (!serial)
         for (Ref *r : g->inputs)
             if (r->type == VX_TYPE_IMAGE && streamable(IMG(r))) {
@@ -282,6 +292,12 @@ static vx_status capture(Graph *g)
                 parts.push_back(std::move(cp));
                 g->staged_out.push_back(a);
             }
+
+    // the array transfers are kernels of the CUDA graph too: list them with the plan
+    if (!g->staged_in.empty()) g->plan_text += "array_upload_batch\t1\n";
+    if (!g->staged_out.empty())
+        g->plan_text += "array_download x" + std::to_string(g->staged_out.size()) + "\t" +
+                        std::to_string(g->staged_out.size()) + "\n";
 
     // ---- dependencies: read-after-write, write-after-write, write-after-read
     std::map<Ref *, int> last_writer;

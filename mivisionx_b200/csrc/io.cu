@@ -39,6 +39,19 @@ k_array_upload(uint8_t *dev, uint32_t *devCount, const uint8_t *host, const vola
     if (blockIdx.x == 0 && threadIdx.x == 0) *devCount = m;
 }
 
+// blockIdx.y: the transfer
+__global__ void __launch_bounds__(kIoThreads) k_array_upload_batch(const agocuda_array_xfer *xfers)
+{
+    const agocuda_array_xfer X = xfers[blockIdx.y];
+    __shared__ uint32_t n;
+    if (threadIdx.x == 0) n = *(const volatile uint32_t *)X.countSlotMapped;
+    __syncthreads();
+    if (n == AGOCUDA_ARRAY_SKIP) return;
+    const uint32_t m = min(n, X.capacity);
+    copy_bytes((uint8_t *)X.devItems, (const uint8_t *)X.hostItemsMapped, (size_t)m * X.itemSize);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *X.devCount = m;
+}
+
 __global__ void __launch_bounds__(kIoThreads)
 k_array_download(uint8_t *host, volatile uint32_t *slot, const uint8_t *dev, const uint32_t *devCount,
                  uint32_t itemSize, uint32_t capacity)
@@ -58,6 +71,14 @@ extern "C" int agocuda_array_upload(void *stream, void *devItems, uint32_t *devC
     k_array_upload<<<kIoBlocks, kIoThreads, 0, as_stream(stream)>>>((uint8_t *)devItems, devCount,
                                                                     (const uint8_t *)hostItemsMapped, countSlotMapped,
                                                                     itemSize, capacity);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_array_upload_batch(void *stream, const agocuda_array_xfer *xfers, uint32_t count)
+{
+    if (!xfers || !count || count > 65535) return AGOCUDA_INVALID_PARAMS;
+    k_array_upload_batch<<<dim3(kIoBlocks, count), kIoThreads, 0, as_stream(stream)>>>(xfers);
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }
