@@ -675,13 +675,13 @@ __global__ void k_harris_nms(int W, int H, const float *sc, int scStride, uint64
 }
 
 // Harris front end as column strips: a warp owns 120 output columns (lanes 1..30, four
-// columns each; lanes 0 and 31 carry the halo) and walks down 16 output rows with rolling
+// columns each; lanes 0 and 31 carry the halo) and walks down 32 output rows with rolling
 // registers.  Per input row a lane loads one word; the Sobel sums run in 16-bit lanes
 // (four columns in four registers), the products and window sums in float -- integers
 // below 2^24, i.e. exactly the float sums the reference forms in any order.  The score
 // keeps the reference's float operation order, and its division is skipped only where the
 // result cannot exceed the threshold.
-constexpr int kHRows = 16, kHCols = 120;
+constexpr int kHRows = 32, kHCols = 120;
 
 __device__ __forceinline__ uint32_t harris_word(const uint8_t *src, int stride, int W, int H, int x, int y, bool fast)
 {
