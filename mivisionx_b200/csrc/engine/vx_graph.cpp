@@ -71,7 +71,7 @@ static uint64_t param_signature(Graph *g)
 // upload of frame i+1 beside the kernels of frame i.  Host-imported images whose memory is
 // page-locked are uploaded and downloaded inside the CUDA graph, on lanes of their own, so
 // vxProcessGraph overlaps the PCIe copies with the kernels.
-constexpr int kComputeLanes = 4;
+constexpr int kComputeLanes = 8;
 // image uploads and downloads (copy engines) and array transfers (small kernels reading or
 // writing mapped host memory) get lanes of their own, so none waits behind another kind
 // (two lanes each way: copies of a few MB finish below PCIe rate one at a time)
