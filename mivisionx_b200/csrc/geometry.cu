@@ -169,54 +169,102 @@ struct AffineParams {
     float vl, vr, vt, vb;      // source valid rectangle (nearest)
 };
 
+// Both warps: a thread owns 4 consecutive output pixels of a row (the reference's 4-pixel
+// groups; W4 = W rounded up to 4), computes their source positions with the reference's
+// float order, issues all source loads before using any, and stores the 4 bytes as one
+// word when the destination allows it.
+__device__ __forceinline__ void warp_store4(uint8_t *d, const int v[4], bool word)
+{
+    if (word) *(uint32_t *)d = (uint32_t)v[0] | ((uint32_t)v[1] << 8) | ((uint32_t)v[2] << 16) | ((uint32_t)v[3] << 24);
+    else { d[0] = (uint8_t)v[0]; d[1] = (uint8_t)v[1]; d[2] = (uint8_t)v[2]; d[3] = (uint8_t)v[3]; }
+}
+
 __global__ void k_warp_affine_nearest(int W4, int H, uint8_t *dst, int ds, int sW, int sH, const uint8_t *src, int ss,
                                       AffineParams a)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W4) return;
+    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x), y = blockIdx.y;
+    if (x0 >= W4) return;
     const float xd = __fadd_rn(__fmul_rn((float)y, a.r01), a.c1), yd = __fadd_rn(__fmul_rn((float)y, a.r11), a.c2);
-    const float xs = __fadd_rn(__fmul_rn(a.r00, (float)x), xd), ys = __fadd_rn(__fmul_rn(a.r10, (float)x), yd);
-    long long idx = (long long)__float2int_rz(ys) * ss + __float2int_rz(xs);
-    int v;
-    if (a.checkBorder) {
-        const bool ok = xs >= 0.f && xs < (float)sW && ys >= 0.f && ys < (float)sH && xs >= a.vl && xs < a.vr &&
-                        ys >= a.vt && ys < a.vb;
-        const long long lim = (long long)sH * ss - 1;
-        idx = idx > lim ? lim : (idx < 0 ? 0 : idx);
-        v = ok ? src[idx] : a.border;
-    } else {
-        v = src[idx];
+    const long long lim = (long long)sH * ss - 1;
+    long long idx[4];
+    bool ok[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int x = x0 + k;
+        const float xs = __fadd_rn(__fmul_rn(a.r00, (float)x), xd), ys = __fadd_rn(__fmul_rn(a.r10, (float)x), yd);
+        idx[k] = (long long)__float2int_rz(ys) * ss + __float2int_rz(xs);
+        ok[k] = true;
+        if (a.checkBorder) {
+            ok[k] = xs >= 0.f && xs < (float)sW && ys >= 0.f && ys < (float)sH && xs >= a.vl && xs < a.vr &&
+                    ys >= a.vt && ys < a.vb;
+            idx[k] = idx[k] > lim ? lim : (idx[k] < 0 ? 0 : idx[k]);
+        }
     }
-    dst[(size_t)y * ds + x] = (uint8_t)v;
+    int v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = src[idx[k]];
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = ok[k] ? v[k] : a.border;
+    uint8_t *d = dst + (size_t)y * ds + x0;
+    warp_store4(d, v, ((uintptr_t)d & 3) == 0);
 }
 
-__device__ __forceinline__ int warp_bilinear_px(const uint8_t *src, int ss, int sW, int sH, const AffineParams &a, float xs, float ys)
-{
-    const int xi = __float2int_rz(xs), yi = __float2int_rz(ys);
-    const float fx = __fsub_rn(xs, (float)xi), fy = __fsub_rn(ys, (float)yi);
-    const float omx = __fsub_rn(1.0f, fx), omy = __fsub_rn(1.0f, fy);
-    long long idx = (long long)yi * ss + xi;
-    const long long lim = (long long)sH * ss - 1;
-    idx = idx > lim ? lim : (idx < 0 ? 0 : idx);
-    const int py = (int)(idx / ss), pxx = (int)(idx - (long long)py * ss);
-    // the reference reads 4 bytes at the (clamped) index and at index + stride
-    const int p0 = ago_px8(src, ss, sW, sH, pxx, py), p1 = ago_px8(src, ss, sW, sH, pxx + 1, py);
-    const int p2 = ago_px8(src, ss, sW, sH, pxx, py + 1), p3 = ago_px8(src, ss, sW, sH, pxx + 1, py + 1);
-    const float f0 = __fmul_rn(__fmul_rn((float)p0, omx), omy), f1 = __fmul_rn(__fmul_rn((float)p1, fx), omy);
-    const float f2 = __fmul_rn(__fmul_rn((float)p2, omx), fy), f3 = __fmul_rn(__fmul_rn((float)p3, fx), fy);
-    const int v = __float2int_rn(__fadd_rn(__fadd_rn(f0, f1), __fadd_rn(f2, f3)));
-    const bool ok = !a.checkBorder || (xs >= 0.f && xs < (float)sW && ys >= 0.f && ys < (float)sH);
-    return sat8(ok ? v : a.border);
-}
+// taps (x, y), (x+1, y), (x, y+1), (x+1, y+1) of the flat index the reference forms
+struct BilinearTap { const uint8_t *p; int px, py; bool direct; };
 
 __global__ void k_warp_affine_bilinear(int W4, int H, uint8_t *dst, int ds, int sW, int sH, const uint8_t *src, int ss,
                                        AffineParams a)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W4) return;
+    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x), y = blockIdx.y;
+    if (x0 >= W4) return;
     const float xd = __fadd_rn(__fmul_rn((float)y, a.r01), a.c1), yd = __fadd_rn(__fmul_rn((float)y, a.r11), a.c2);
-    const float xs = __fadd_rn(__fmul_rn(a.r00, (float)x), xd), ys = __fadd_rn(__fmul_rn(a.r10, (float)x), yd);
-    dst[(size_t)y * ds + x] = (uint8_t)warp_bilinear_px(src, ss, sW, sH, a, xs, ys);
+    const long long lim = (long long)sH * ss - 1;
+    float fx[4], fy[4];
+    bool ok[4];
+    BilinearTap t[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int x = x0 + k;
+        const float xs = __fadd_rn(__fmul_rn(a.r00, (float)x), xd), ys = __fadd_rn(__fmul_rn(a.r10, (float)x), yd);
+        const int xi = __float2int_rz(xs), yi = __float2int_rz(ys);
+        fx[k] = __fsub_rn(xs, (float)xi);
+        fy[k] = __fsub_rn(ys, (float)yi);
+        ok[k] = !a.checkBorder || (xs >= 0.f && xs < (float)sW && ys >= 0.f && ys < (float)sH);
+        int py, pxx;
+        if (yi >= 0 && yi < sH && xi >= 0 && xi < ss) {          // flat index inside, no wrap
+            py = yi; pxx = xi;
+        } else {                                               // the reference clamps the flat index
+            long long idx = (long long)yi * ss + xi;
+            idx = idx > lim ? lim : (idx < 0 ? 0 : idx);
+            py = (int)(idx / ss); pxx = (int)(idx - (long long)py * ss);
+        }
+        t[k].px = pxx; t[k].py = py;
+        t[k].direct = pxx >= 0 && pxx + 1 < sW && py + 1 < sH;
+        t[k].p = src + (size_t)py * ss + pxx;
+    }
+    int q[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (t[k].direct) {
+            q[k][0] = t[k].p[0]; q[k][1] = t[k].p[1]; q[k][2] = t[k].p[ss]; q[k][3] = t[k].p[ss + 1];
+        } else {   // the reference reads 4 bytes at the (clamped) index and at index + stride
+            q[k][0] = ago_px8(src, ss, sW, sH, t[k].px, t[k].py);
+            q[k][1] = ago_px8(src, ss, sW, sH, t[k].px + 1, t[k].py);
+            q[k][2] = ago_px8(src, ss, sW, sH, t[k].px, t[k].py + 1);
+            q[k][3] = ago_px8(src, ss, sW, sH, t[k].px + 1, t[k].py + 1);
+        }
+    }
+    int v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float omx = __fsub_rn(1.0f, fx[k]), omy = __fsub_rn(1.0f, fy[k]);
+        const float f0 = __fmul_rn(__fmul_rn((float)q[k][0], omx), omy), f1 = __fmul_rn(__fmul_rn((float)q[k][1], fx[k]), omy);
+        const float f2 = __fmul_rn(__fmul_rn((float)q[k][2], omx), fy[k]), f3 = __fmul_rn(__fmul_rn((float)q[k][3], fx[k]), fy[k]);
+        const int val = __float2int_rn(__fadd_rn(__fadd_rn(f0, f1), __fadd_rn(f2, f3)));
+        v[k] = sat8(ok[k] ? val : a.border);
+    }
+    uint8_t *d = dst + (size_t)y * ds + x0;
+    warp_store4(d, v, ((uintptr_t)d & 3) == 0);
 }
 
 // ------------------------------------------------------------------------------------
@@ -389,7 +437,7 @@ extern "C" int agocuda_WarpAffine_U8_U8_Nearest_Constant(void *stream, uint32_t 
     if (!pDst || !pSrc || !affineMatrix || !W || !H || dstStride < W4 || srcStride < srcW || !srcW || !srcH)
         return AGOCUDA_INVALID_PARAMS;
     AffineParams a = affine_params(affineMatrix, W, H, srcW, srcH, border, srcValidRect);
-    k_warp_affine_nearest<<<dim3(div_up(W4, 128), H), 128, 0, as_stream(stream)>>>((int)W4, (int)H, pDst, (int)dstStride, (int)srcW,
+    k_warp_affine_nearest<<<dim3(div_up(W4, 512), H), 128, 0, as_stream(stream)>>>((int)W4, (int)H, pDst, (int)dstStride, (int)srcW,
                                                                                    (int)srcH, pSrc, (int)srcStride, a);
     agocuda_count_launch(1);
     return agocuda_launch_status();
@@ -403,7 +451,7 @@ extern "C" int agocuda_WarpAffine_U8_U8_Bilinear_Constant(void *stream, uint32_t
     if (!pDst || !pSrc || !affineMatrix || !W || !H || dstStride < W4 || srcStride < srcW || !srcW || !srcH)
         return AGOCUDA_INVALID_PARAMS;
     AffineParams a = affine_params(affineMatrix, W, H, srcW, srcH, border, nullptr);
-    k_warp_affine_bilinear<<<dim3(div_up(W4, 128), H), 128, 0, as_stream(stream)>>>((int)W4, (int)H, pDst, (int)dstStride, (int)srcW,
+    k_warp_affine_bilinear<<<dim3(div_up(W4, 512), H), 128, 0, as_stream(stream)>>>((int)W4, (int)H, pDst, (int)dstStride, (int)srcW,
                                                                                     (int)srcH, pSrc, (int)srcStride, a);
     agocuda_count_launch(1);
     return agocuda_launch_status();
