@@ -198,7 +198,7 @@ def _peaks():
 
 
 class ClockSampler:
-    """SM clock and clock-event (throttle) reasons sampled through NVML every 5 ms while the
+    """SM clock and clock-event (throttle) reasons sampled through NVML every 1 ms while the
     timed region runs (the same counters `nvidia-smi --query-gpu=clocks.sm,...` reads)."""
 
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
@@ -230,7 +230,7 @@ class ClockSampler:
                 except AttributeError:
                     rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
                 self.rows.append((sm, rs))
-                self._stop.wait(0.005)
+                self._stop.wait(0.001)
         except Exception as e:   # NVML unavailable: report it instead of inventing numbers
             self.err = repr(e)
 
@@ -244,6 +244,10 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        n = len(self.rows)
+        t0 = time.time()
+        while len(self.rows) == n and n == 0 and self.err is None and time.time() - t0 < 0.1:
+            time.sleep(0.0005)   # a timed region shorter than one period: its closing sample
         self._stop.set()
         self.t.join(timeout=2)
 
@@ -252,7 +256,7 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "error": self.err}
         reasons = sorted({n for _, r in self.rows for bit, n in self.REASONS.items() if r & bit})
         return {"sm_mhz": statistics.median(s for s, _ in self.rows), "sm_max_mhz": self.max_mhz,
-                "reasons": reasons, "samples": len(self.rows), "source": "NVML, 5 ms period, timed region only"}
+                "reasons": reasons, "samples": len(self.rows), "source": "NVML, 1 ms period, timed region only"}
 
 
 def _dist():
