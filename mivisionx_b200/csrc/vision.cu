@@ -300,14 +300,18 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
     const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH, tid = threadIdx.x;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x;
 
-    // ---- input words; border tiles follow the reference's reads outside rows (ago_px)
-    const bool inner = x0 >= 4 && y0 >= 2 && x0 + kTW + 4 <= W && y0 + kTH + 2 <= H &&
-                       (((uintptr_t)src | (uintptr_t)srcStride) & 3) == 0;
-    for (int i = tid; i < kIH * kInWords; i += blockDim.x) {
+    // ---- input words; words reaching outside the image follow the reference's reads
+    // outside rows (ago_px), byte by byte
+    const bool al = (((uintptr_t)src | (uintptr_t)srcStride) & 3) == 0;
+    static_assert(kIH * kInWords <= 3 * 256, "three words per thread");
+#pragma unroll
+    for (int it = 0; it < 3; it++) {
+        const int i = tid + it * 256;
+        if (i >= kIH * kInWords) break;
         const int r = i / kInWords, q = i - r * kInWords;
         const int y = y0 - 2 + r, x = x0 - 4 + 4 * q;
         uint32_t w;
-        if (inner) {
+        if (al && (unsigned)y < (unsigned)H && x >= 0 && x + 4 <= W) {
             w = __ldg((const uint32_t *)(src + (size_t)y * srcStride + x));
         } else {
             w = 0;
@@ -439,21 +443,29 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
     }
     __syncthreads();
 
-    // ---- roots (the component's smallest pixel index), strong roots, labels out
+    // ---- roots (the component's smallest pixel index): each run start finds its root and
+    // keeps it (no unions run any more), then every pixel reads start -> root in two steps
+    {
+        uint32_t starts = (uint32_t)((m & ~(m << 1)) >> c0) & 0xff;
+        while (starts) {
+            const int j = __ffs(starts) - 1;
+            starts &= starts - 1;
+            sLab[i0 + j] = sfind(sLab, i0 + j);
+        }
+    }
+    __syncthreads();
     int root[8];
     {
+        const int4 a = *(const int4 *)&sLab[i0], b = *(const int4 *)&sLab[i0 + 4];
+        const int s1[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
         const uint32_t stb = (uint32_t)(sST[r] >> c0) & 0xff;
-        int lastStart = -1, lastRoot = -1, lastOr = -1;
+        int lastOr = -1;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-            root[j] = -1;
-            if (!((m >> (c0 + j)) & 1)) continue;
-            const int start = sLab[i0 + j];
-            if (start != lastStart) { lastStart = start; lastRoot = sfind(sLab, start); }
-            root[j] = lastRoot;
-            if (((stb >> j) & 1) && lastRoot != lastOr) {
-                lastOr = lastRoot;
-                atomicOr(&sStrongRoot[lastRoot >> 5], 1u << (lastRoot & 31));
+            root[j] = s1[j] >= 0 ? sLab[s1[j]] : -1;   // start -> root (a root maps to itself)
+            if (((stb >> j) & 1) && root[j] != lastOr) {
+                lastOr = root[j];
+                atomicOr(&sStrongRoot[lastOr >> 5], 1u << (lastOr & 31));
             }
         }
     }
