@@ -457,6 +457,101 @@ int agocuda_array_upload_batch(void *stream, const agocuda_array_xfer *xfers, ui
 int agocuda_array_download(void *stream, void *hostItemsMapped, uint32_t *countSlotMapped, const void *devItems,
                            const uint32_t *devCount, uint32_t itemSize, uint32_t capacity);
 
+/* ------------------------------------------------------------------------------------ */
+/* Element-wise kernels (reference: hipvx/hip_host_decls.h arithmetic/logical kernels;   */
+/* CPU semantics ago/ago_haf_cpu_arithmetic.cpp, ago/ago_haf_cpu_logical.cpp)            */
+/* Every pixel of [0,W)x[0,H).  Planes: row base aligned to 8 pixels' bytes (8 B for U8,  */
+/* 16 B for S16) and the stride a multiple of it.  _Wrap keeps the low bits of the exact  */
+/* result, _Sat clamps it to the output type; S16 results of two U8 inputs are exact.     */
+/* ------------------------------------------------------------------------------------ */
+
+/* dst = src1 + src2.  Replace HipExec_Add_U8_U8U8_Wrap / _Sat (hip_host_decls.h:43, :48),
+ * HipExec_Add_S16_U8U8 (:53), HipExec_Add_S16_S16U8_Wrap / _Sat (:58, :63) and
+ * HipExec_Add_S16_S16S16_Wrap / _Sat (:68, :73). */
+int agocuda_Add_U8_U8U8_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                             const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Add_U8_U8U8_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                            const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Add_S16_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                         const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Add_S16_S16U8_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                               const int16_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Add_S16_S16U8_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                              const int16_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Add_S16_S16S16_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                                const int16_t *pSrc1, uint32_t src1Stride, const int16_t *pSrc2, uint32_t src2Stride);
+int agocuda_Add_S16_S16S16_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                               const int16_t *pSrc1, uint32_t src1Stride, const int16_t *pSrc2, uint32_t src2Stride);
+
+/* dst = src1 - src2.  Replace HipExec_Sub_U8_U8U8_Wrap / _Sat (hip_host_decls.h:78, :83),
+ * HipExec_Sub_S16_U8U8 (:88), HipExec_Sub_S16_S16U8_Wrap / _Sat (:93, :98),
+ * HipExec_Sub_S16_U8S16_Wrap / _Sat (:103, :108), HipExec_Sub_S16_S16S16_Wrap / _Sat (:113, :118). */
+int agocuda_Sub_U8_U8U8_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                             const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Sub_U8_U8U8_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                            const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Sub_S16_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                         const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Sub_S16_S16U8_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                               const int16_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Sub_S16_S16U8_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                              const int16_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Sub_S16_U8S16_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                               const uint8_t *pSrc1, uint32_t src1Stride, const int16_t *pSrc2, uint32_t src2Stride);
+int agocuda_Sub_S16_U8S16_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                              const uint8_t *pSrc1, uint32_t src1Stride, const int16_t *pSrc2, uint32_t src2Stride);
+int agocuda_Sub_S16_S16S16_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                                const int16_t *pSrc1, uint32_t src1Stride, const int16_t *pSrc2, uint32_t src2Stride);
+int agocuda_Sub_S16_S16S16_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                               const int16_t *pSrc1, uint32_t src1Stride, const int16_t *pSrc2, uint32_t src2Stride);
+
+/* dst = |src1 - src2| (S16: clamped to 32767).  Replace HipExec_AbsDiff_U8_U8U8
+ * (hip_host_decls.h:33) and HipExec_AbsDiff_S16_S16S16_Sat (:38). */
+int agocuda_AbsDiff_U8_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                            const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_AbsDiff_S16_S16S16_Sat(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                                   const int16_t *pSrc1, uint32_t src1Stride, const int16_t *pSrc2, uint32_t src2Stride);
+
+/* Bitwise and / or / xor / not.  Replace HipExec_And_U8_U8U8 (hip_host_decls.h:238),
+ * HipExec_Or_U8_U8U8 (:278), HipExec_Xor_U8_U8U8 (:318), HipExec_Not_U8_U8 (:358). */
+int agocuda_And_U8_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                        const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Or_U8_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                       const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Xor_U8_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                        const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride);
+int agocuda_Not_U8_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                      const uint8_t *pSrc, uint32_t srcStride);
+
+/* 255 where lower <= v <= upper, else 0 (bounds taken as vx_uint8).  Replaces
+ * HipExec_Threshold_U8_U8_Range (hip_host_decls.h:694); HafCpu_Threshold_U8_U8_Range
+ * (ago_haf_cpu_arithmetic.cpp:3742). */
+int agocuda_Threshold_U8_U8_Range(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                  uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride, int32_t thresholdLower,
+                                  int32_t thresholdUpper);
+
+/* ------------------------------------------------------------------------------------ */
+/* 3x3 neighbourhood filters on U8 (reference: hipvx/hip_host_decls.h filter_kernels;    */
+/* CPU semantics ago/ago_haf_cpu_filter.cpp).  Rows [1, H-1) are written, every column;  */
+/* pixels of columns 0 and W-1 are unspecified (outside the valid region).  Row bases   */
+/* 4-byte aligned, strides multiples of 4.                                                */
+/* ------------------------------------------------------------------------------------ */
+
+/* floor(sum of the 3x3 window / 9).  Replaces HipExec_Box_U8_U8_3x3 (hip_host_decls.h:633);
+ * HafCpu_Box_U8_U8_3x3 (ago_haf_cpu_filter.cpp:34). */
+int agocuda_Box_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                          const uint8_t *pSrc, uint32_t srcStride);
+/* Maximum / minimum of the 3x3 window.  Replace HipExec_Dilate_U8_U8_3x3 (hip_host_decls.h:637)
+ * and HipExec_Erode_U8_U8_3x3 (:641); ago_haf_cpu_filter.cpp:221, :298. */
+int agocuda_Dilate_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                             const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_Erode_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                            const uint8_t *pSrc, uint32_t srcStride);
+/* Median of the 3x3 window.  Replaces HipExec_Median_U8_U8_3x3 (hip_host_decls.h:645);
+ * HafCpu_Median_U8_U8_3x3 (ago_haf_cpu_filter.cpp:3842). */
+int agocuda_Median_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                             const uint8_t *pSrc, uint32_t srcStride);
+
 #ifdef __cplusplus
 }
 #endif

@@ -221,7 +221,10 @@ typedef struct {
 enum vx_kernel_e {
     VX_KERNEL_COLOR_CONVERT = VX__K(0x1), VX_KERNEL_CHANNEL_EXTRACT = VX__K(0x2), VX_KERNEL_CHANNEL_COMBINE = VX__K(0x3),
     VX_KERNEL_SOBEL_3x3 = VX__K(0x4), VX_KERNEL_MAGNITUDE = VX__K(0x5), VX_KERNEL_PHASE = VX__K(0x6),
-    VX_KERNEL_SCALE_IMAGE = VX__K(0x7), VX_KERNEL_THRESHOLD = VX__K(0xD), VX_KERNEL_BOX_3x3 = VX__K(0x12),
+    VX_KERNEL_SCALE_IMAGE = VX__K(0x7), VX_KERNEL_ABSDIFF = VX__K(0xB), VX_KERNEL_THRESHOLD = VX__K(0xD),
+    VX_KERNEL_DILATE_3x3 = VX__K(0xF), VX_KERNEL_ERODE_3x3 = VX__K(0x10), VX_KERNEL_MEDIAN_3x3 = VX__K(0x11),
+    VX_KERNEL_BOX_3x3 = VX__K(0x12), VX_KERNEL_AND = VX__K(0x1C), VX_KERNEL_OR = VX__K(0x1D), VX_KERNEL_XOR = VX__K(0x1E),
+    VX_KERNEL_NOT = VX__K(0x1F), VX_KERNEL_ADD = VX__K(0x21), VX_KERNEL_SUBTRACT = VX__K(0x22),
     VX_KERNEL_GAUSSIAN_3x3 = VX__K(0x13), VX_KERNEL_GAUSSIAN_PYRAMID = VX__K(0x15),
     VX_KERNEL_CONVERTDEPTH = VX__K(0x1A), VX_KERNEL_CANNY_EDGE_DETECTOR = VX__K(0x1B),
     VX_KERNEL_WARP_AFFINE = VX__K(0x23), VX_KERNEL_WARP_PERSPECTIVE = VX__K(0x24),
@@ -368,6 +371,17 @@ vx_node vxOpticalFlowPyrLKNode(vx_graph graph, vx_pyramid old_images, vx_pyramid
                                vx_scalar num_iterations, vx_scalar use_initial_estimate, vx_size window_dimension);
 vx_node vxRemapNode(vx_graph graph, vx_image input, vx_remap table, vx_enum policy, vx_image output);
 vx_node vxHalfScaleGaussianNode(vx_graph graph, vx_image input, vx_image output, vx_int32 kernel_size);
+vx_node vxBox3x3Node(vx_graph graph, vx_image input, vx_image output);
+vx_node vxMedian3x3Node(vx_graph graph, vx_image input, vx_image output);
+vx_node vxDilate3x3Node(vx_graph graph, vx_image input, vx_image output);
+vx_node vxErode3x3Node(vx_graph graph, vx_image input, vx_image output);
+vx_node vxAbsDiffNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
+vx_node vxAddNode(vx_graph graph, vx_image in1, vx_image in2, vx_enum policy, vx_image out);
+vx_node vxSubtractNode(vx_graph graph, vx_image in1, vx_image in2, vx_enum policy, vx_image out);
+vx_node vxAndNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
+vx_node vxOrNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
+vx_node vxXorNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
+vx_node vxNotNode(vx_graph graph, vx_image input, vx_image output);
 
 #ifdef __cplusplus
 }

@@ -29,6 +29,13 @@ static const char *kLKNames[] = {
     "WarpPerspective_U8_U8_Bilinear_Constant", "Remap_U8_U8_Nearest_Constant", "Remap_U8_U8_Bilinear_Constant",
     "ScaleGaussianHalf_U8_U8_5x5", "OpticalFlowPyrLK_XY_XY",
     "WarpPerspective_U8_U8_Nearest", "WarpPerspective_U8_U8_Bilinear", "Remap_U8_U8_Nearest", "Remap_U8_U8_Bilinear",
+    "Box_U8_U8_3x3", "Dilate_U8_U8_3x3", "Erode_U8_U8_3x3", "Median_U8_U8_3x3",
+    "AbsDiff_U8_U8U8", "AbsDiff_S16_S16S16_Sat",
+    "Add_U8_U8U8_Wrap", "Add_U8_U8U8_Sat", "Add_S16_U8U8", "Add_S16_S16U8_Wrap", "Add_S16_S16U8_Sat",
+    "Add_S16_S16S16_Wrap", "Add_S16_S16S16_Sat",
+    "Sub_U8_U8U8_Wrap", "Sub_U8_U8U8_Sat", "Sub_S16_U8U8", "Sub_S16_S16U8_Wrap", "Sub_S16_S16U8_Sat",
+    "Sub_S16_U8S16_Wrap", "Sub_S16_U8S16_Sat", "Sub_S16_S16S16_Wrap", "Sub_S16_S16S16_Sat",
+    "And_U8_U8U8", "Or_U8_U8U8", "Xor_U8_U8U8", "Not_U8_U8", "Threshold_U8_U8_Range",
 };
 static_assert(sizeof(kLKNames) / sizeof(kLKNames[0]) == (size_t)LK::COUNT, "kernel name table");
 
@@ -89,8 +96,35 @@ vx_status validate_node(Graph *g, Node *n)
     case VX_KERNEL_THRESHOLD: {
         if (!fmt_is(p[0], VX_DF_IMAGE_U8) || !is_valid(p[1], VX_TYPE_THRESHOLD)) return VX_ERROR_INVALID_PARAMETERS;
         Threshold *t = static_cast<Threshold *>(p[1]);
-        if (t->thresh_type != VX_THRESHOLD_TYPE_BINARY) return VX_ERROR_NOT_SUPPORTED;
+        if (t->thresh_type != VX_THRESHOLD_TYPE_BINARY && t->thresh_type != VX_THRESHOLD_TYPE_RANGE) return VX_ERROR_NOT_SUPPORTED;
         return set_meta(img(2), img(0)->width, img(0)->height, VX_DF_IMAGE_U8);
+    }
+    // ago_kernel_api.cpp ovxKernel_Box3x3 (:1052) and the Median / Dilate / Erode validators
+    case VX_KERNEL_BOX_3x3: case VX_KERNEL_MEDIAN_3x3: case VX_KERNEL_DILATE_3x3: case VX_KERNEL_ERODE_3x3:
+    case VX_KERNEL_NOT:
+        if (!fmt_is(p[0], VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
+        return set_meta(img(1), img(0)->width, img(0)->height, VX_DF_IMAGE_U8);
+    case VX_KERNEL_AND: case VX_KERNEL_OR: case VX_KERNEL_XOR:      // ovxKernel_And (:1473)
+    case VX_KERNEL_ABSDIFF: {                                       // ovxKernel_AbsDiff (:782)
+        Image *a = img(0), *b = img(1);
+        const vx_df_image f = a && a->num_planes ? a->format : VX_DF_IMAGE_VIRT;
+        const bool ok = n->kernel == VX_KERNEL_ABSDIFF ? (f == VX_DF_IMAGE_U8 || f == VX_DF_IMAGE_S16) : f == VX_DF_IMAGE_U8;
+        if (!ok || !fmt_is(b, f)) return VX_ERROR_INVALID_FORMAT;
+        if (a->width != b->width || a->height != b->height) return VX_ERROR_INVALID_DIMENSION;
+        return set_meta(img(2), a->width, a->height, f);
+    }
+    case VX_KERNEL_ADD: case VX_KERNEL_SUBTRACT: {                  // ovxKernel_Add (:1681), _Subtract (:1729)
+        Image *a = img(0), *b = img(1), *o = img(3);
+        auto u8s16 = [](Image *i) { return i && i->num_planes && (i->format == VX_DF_IMAGE_U8 || i->format == VX_DF_IMAGE_S16); };
+        if (!u8s16(a) || !u8s16(b) || !o) return VX_ERROR_INVALID_FORMAT;
+        if (a->width != b->width || a->height != b->height) return VX_ERROR_INVALID_DIMENSION;
+        if (!is_valid(p[2], VX_TYPE_SCALAR) || static_cast<Scalar *>(p[2])->data_type != VX_TYPE_ENUM) return VX_ERROR_INVALID_TYPE;
+        const vx_enum pol = sc_enum(p[2]);
+        if (pol != VX_CONVERT_POLICY_WRAP && pol != VX_CONVERT_POLICY_SATURATE) return VX_ERROR_INVALID_VALUE;
+        // U8 only when both inputs and the output are U8; a virtual output of unset format is S16
+        const vx_df_image f = a->format == VX_DF_IMAGE_U8 && b->format == VX_DF_IMAGE_U8 && o->format == VX_DF_IMAGE_U8
+                                  ? VX_DF_IMAGE_U8 : VX_DF_IMAGE_S16;
+        return set_meta(o, a->width, a->height, f);
     }
     case VX_KERNEL_CANNY_EDGE_DETECTOR: {
         if (!fmt_is(p[0], VX_DF_IMAGE_U8) || !is_valid(p[1], VX_TYPE_THRESHOLD)) return VX_ERROR_INVALID_PARAMETERS;
@@ -234,7 +268,45 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
         add(sc_enum(p[2]) == VX_CONVERT_POLICY_WRAP ? LK::COLOR_DEPTH_U8_S16_WRAP : LK::COLOR_DEPTH_U8_S16_SAT, {p[1], p[0], p[3]});
         return VX_SUCCESS;
     }
-    case VX_KERNEL_THRESHOLD: add(LK::THRESHOLD_U8_U8_BINARY, {p[2], p[0], p[1]}); return VX_SUCCESS;   // :741
+    case VX_KERNEL_THRESHOLD:                                                                          // :741
+        add(static_cast<Threshold *>(p[1])->thresh_type == VX_THRESHOLD_TYPE_RANGE ? LK::THRESHOLD_U8_U8_RANGE
+                                                                                 : LK::THRESHOLD_U8_U8_BINARY,
+            {p[2], p[0], p[1]});
+        return VX_SUCCESS;
+    case VX_KERNEL_BOX_3x3: add(LK::BOX_U8_U8_3x3, {p[1], p[0]}); return VX_SUCCESS;                  // :849
+    case VX_KERNEL_MEDIAN_3x3: add(LK::MEDIAN_U8_U8_3x3, {p[1], p[0]}); return VX_SUCCESS;            // :835
+    case VX_KERNEL_DILATE_3x3: add(LK::DILATE_U8_U8_3x3, {p[1], p[0]}); return VX_SUCCESS;            // :786
+    case VX_KERNEL_ERODE_3x3: add(LK::ERODE_U8_U8_3x3, {p[1], p[0]}); return VX_SUCCESS;              // :810
+    case VX_KERNEL_NOT: add(LK::NOT_U8_U8, {p[1], p[0]}); return VX_SUCCESS;                          // :1293
+    case VX_KERNEL_AND: add(LK::AND_U8_U8U8, {p[2], p[0], p[1]}); return VX_SUCCESS;                  // :1191
+    case VX_KERNEL_OR: add(LK::OR_U8_U8U8, {p[2], p[0], p[1]}); return VX_SUCCESS;                    // :1225
+    case VX_KERNEL_XOR: add(LK::XOR_U8_U8U8, {p[2], p[0], p[1]}); return VX_SUCCESS;                  // :1259
+    case VX_KERNEL_ABSDIFF:                                                                            // :689
+        add(IMG(p[2])->format == VX_DF_IMAGE_U8 ? LK::ABS_DIFF_U8_U8U8 : LK::ABS_DIFF_S16_S16S16_SAT, {p[2], p[0], p[1]});
+        return VX_SUCCESS;
+    case VX_KERNEL_ADD: case VX_KERNEL_SUBTRACT: {                                                     // :1386, :1428
+        const vx_df_image fa = IMG(p[0])->format, fb = IMG(p[1])->format, fo = IMG(p[3])->format;
+        const bool sat = sc_enum(p[2]) == VX_CONVERT_POLICY_SATURATE;
+        const bool u8a = fa == VX_DF_IMAGE_U8, u8b = fb == VX_DF_IMAGE_U8;
+        Ref *A = p[0], *B = p[1];
+        LK k = LK::INVALID;
+        if (n->kernel == VX_KERNEL_ADD) {
+            if (fo == VX_DF_IMAGE_U8) k = sat ? LK::ADD_U8_U8U8_SAT : LK::ADD_U8_U8U8_WRAP;
+            else if (u8a && u8b) k = LK::ADD_S16_U8U8;
+            else if (u8a || u8b) {
+                k = sat ? LK::ADD_S16_S16U8_SAT : LK::ADD_S16_S16U8_WRAP;
+                if (u8a) std::swap(A, B);   // the S16 operand goes first
+            } else k = sat ? LK::ADD_S16_S16S16_SAT : LK::ADD_S16_S16S16_WRAP;
+        } else {
+            if (fo == VX_DF_IMAGE_U8) k = sat ? LK::SUB_U8_U8U8_SAT : LK::SUB_U8_U8U8_WRAP;
+            else if (u8a && u8b) k = LK::SUB_S16_U8U8;
+            else if (u8b) k = sat ? LK::SUB_S16_S16U8_SAT : LK::SUB_S16_S16U8_WRAP;
+            else if (u8a) k = sat ? LK::SUB_S16_U8S16_SAT : LK::SUB_S16_U8S16_WRAP;
+            else k = sat ? LK::SUB_S16_S16S16_SAT : LK::SUB_S16_S16S16_WRAP;
+        }
+        add(k, {p[3], A, B});
+        return VX_SUCCESS;
+    }
     case VX_KERNEL_CANNY_EDGE_DETECTOR: {                                                              // :1618
         Image *i0 = IMG(p[0]);
         Array *stack = virt_array(g, kItemCoord2dU16, (vx_size)i0->width * i0->height);
@@ -603,7 +675,22 @@ vx_status propagate_valid_rects(Graph *g)
         }
         case LK::COLOR_DEPTH_U8_S16_SAT: case LK::COLOR_DEPTH_U8_S16_WRAP: case LK::COLOR_DEPTH_S16_U8:
         case LK::THRESHOLD_U8_U8_BINARY: case LK::CHANNEL_COPY_U8_U8:
+        case LK::THRESHOLD_U8_U8_RANGE: case LK::NOT_U8_U8:
             copy_rect(I(0), I(1)); break;
+        case LK::BOX_U8_U8_3x3: case LK::DILATE_U8_U8_3x3: case LK::ERODE_U8_U8_3x3: case LK::MEDIAN_U8_U8_3x3:
+            shrink_from(I(0), I(1), 1); break;                  // e.g. :15033 (Box)
+        case LK::ABS_DIFF_U8_U8U8: case LK::ABS_DIFF_S16_S16S16_SAT:
+        case LK::ADD_U8_U8U8_WRAP: case LK::ADD_U8_U8U8_SAT: case LK::ADD_S16_U8U8: case LK::ADD_S16_S16U8_WRAP:
+        case LK::ADD_S16_S16U8_SAT: case LK::ADD_S16_S16S16_WRAP: case LK::ADD_S16_S16S16_SAT:
+        case LK::SUB_U8_U8U8_WRAP: case LK::SUB_U8_U8U8_SAT: case LK::SUB_S16_U8U8: case LK::SUB_S16_S16U8_WRAP:
+        case LK::SUB_S16_S16U8_SAT: case LK::SUB_S16_U8S16_WRAP: case LK::SUB_S16_U8S16_SAT:
+        case LK::SUB_S16_S16S16_WRAP: case LK::SUB_S16_S16S16_SAT:
+        case LK::AND_U8_U8U8: case LK::OR_U8_U8U8: case LK::XOR_U8_U8U8: {   // e.g. :4514 (Add_U8_U8U8_Wrap)
+            Image *o = I(0), *a = I(1), *b = I(2);
+            o->valid = vx_rectangle_t{std::max(a->valid.start_x, b->valid.start_x), std::max(a->valid.start_y, b->valid.start_y),
+                                      std::min(a->valid.end_x, b->valid.end_x), std::min(a->valid.end_y, b->valid.end_y)};
+            break;
+        }
         case LK::COLOR_CONVERT_NV12_RGB: {                      // :13953
             Image *in = I(2);
             copy_rect(I(0), in);

@@ -271,6 +271,54 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         st.launch = [=](cudaStream_t q) { return agocuda_Threshold_U8_U8_Binary(S(q), w, h, d, ds, s, ss, thr); };
         return VX_SUCCESS;
     }
+    case LK::THRESHOLD_U8_U8_RANGE: {
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        Threshold *t = static_cast<Threshold *>(p[2]);
+        int32_t lo = t->lower.U8, hi = t->upper.U8;   // threshold_lower/upper.U1 as vx_uint8 (ago_kernel_api.cpp:3511)
+        st.launch = [=](cudaStream_t q) { return agocuda_Threshold_U8_U8_Range(S(q), w, h, d, ds, s, ss, lo, hi); };
+        return VX_SUCCESS;
+    }
+    case LK::BOX_U8_U8_3x3: case LK::DILATE_U8_U8_3x3: case LK::ERODE_U8_U8_3x3: case LK::MEDIAN_U8_U8_3x3:
+    case LK::NOT_U8_U8: {
+        using Fn = int (*)(void *, uint32_t, uint32_t, uint8_t *, uint32_t, const uint8_t *, uint32_t);
+        const Fn fn = ln.k == LK::BOX_U8_U8_3x3 ? agocuda_Box_U8_U8_3x3 : ln.k == LK::DILATE_U8_U8_3x3 ? agocuda_Dilate_U8_U8_3x3
+                    : ln.k == LK::ERODE_U8_U8_3x3 ? agocuda_Erode_U8_U8_3x3 : ln.k == LK::MEDIAN_U8_U8_3x3 ? agocuda_Median_U8_U8_3x3
+                    : agocuda_Not_U8_U8;
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        st.launch = [=](cudaStream_t q) { return fn(S(q), w, h, d, ds, s, ss); };
+        return VX_SUCCESS;
+    }
+#define EW(KIND, FN, TO, TA, TB)                                                                     \
+    case LK::KIND: {                                                                                \
+        TO *d = (TO *)dptr(p[0]); const TA *a = (const TA *)dptr(p[1]); const TB *b = (const TB *)dptr(p[2]); \
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), as_ = dstride(p[1]), bs = dstride(p[2]);   \
+        st.launch = [=](cudaStream_t q) { return FN(S(q), w, h, d, ds, a, as_, b, bs); };            \
+        return VX_SUCCESS;                                                                          \
+    }
+    EW(ABS_DIFF_U8_U8U8, agocuda_AbsDiff_U8_U8U8, uint8_t, uint8_t, uint8_t)
+    EW(ABS_DIFF_S16_S16S16_SAT, agocuda_AbsDiff_S16_S16S16_Sat, int16_t, int16_t, int16_t)
+    EW(ADD_U8_U8U8_WRAP, agocuda_Add_U8_U8U8_Wrap, uint8_t, uint8_t, uint8_t)
+    EW(ADD_U8_U8U8_SAT, agocuda_Add_U8_U8U8_Sat, uint8_t, uint8_t, uint8_t)
+    EW(ADD_S16_U8U8, agocuda_Add_S16_U8U8, int16_t, uint8_t, uint8_t)
+    EW(ADD_S16_S16U8_WRAP, agocuda_Add_S16_S16U8_Wrap, int16_t, int16_t, uint8_t)
+    EW(ADD_S16_S16U8_SAT, agocuda_Add_S16_S16U8_Sat, int16_t, int16_t, uint8_t)
+    EW(ADD_S16_S16S16_WRAP, agocuda_Add_S16_S16S16_Wrap, int16_t, int16_t, int16_t)
+    EW(ADD_S16_S16S16_SAT, agocuda_Add_S16_S16S16_Sat, int16_t, int16_t, int16_t)
+    EW(SUB_U8_U8U8_WRAP, agocuda_Sub_U8_U8U8_Wrap, uint8_t, uint8_t, uint8_t)
+    EW(SUB_U8_U8U8_SAT, agocuda_Sub_U8_U8U8_Sat, uint8_t, uint8_t, uint8_t)
+    EW(SUB_S16_U8U8, agocuda_Sub_S16_U8U8, int16_t, uint8_t, uint8_t)
+    EW(SUB_S16_S16U8_WRAP, agocuda_Sub_S16_S16U8_Wrap, int16_t, int16_t, uint8_t)
+    EW(SUB_S16_S16U8_SAT, agocuda_Sub_S16_S16U8_Sat, int16_t, int16_t, uint8_t)
+    EW(SUB_S16_U8S16_WRAP, agocuda_Sub_S16_U8S16_Wrap, int16_t, uint8_t, int16_t)
+    EW(SUB_S16_U8S16_SAT, agocuda_Sub_S16_U8S16_Sat, int16_t, uint8_t, int16_t)
+    EW(SUB_S16_S16S16_WRAP, agocuda_Sub_S16_S16S16_Wrap, int16_t, int16_t, int16_t)
+    EW(SUB_S16_S16S16_SAT, agocuda_Sub_S16_S16S16_Sat, int16_t, int16_t, int16_t)
+    EW(AND_U8_U8U8, agocuda_And_U8_U8U8, uint8_t, uint8_t, uint8_t)
+    EW(OR_U8_U8U8, agocuda_Or_U8_U8U8, uint8_t, uint8_t, uint8_t)
+    EW(XOR_U8_U8U8, agocuda_Xor_U8_U8U8, uint8_t, uint8_t, uint8_t)
+#undef EW
     case LK::CANNY_SOBEL_U16_U8_3x3_L1NORM: {
         uint16_t *d = (uint16_t *)dptr(p[0]); const uint8_t *s = dptr(p[1]);
         uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);

@@ -831,4 +831,37 @@ vx_node vxRemapNode(vx_graph graph, vx_image input, vx_remap table, vx_enum poli
 vx_node vxHalfScaleGaussianNode(vx_graph graph, vx_image input, vx_image output, vx_int32 kernel_size)
 { return make_node(graph, VX_KERNEL_HALFSCALE_GAUSSIAN, {R(input), R(output), scalar_of(graph, VX_TYPE_INT32, &kernel_size)}); }
 
+vx_node vxBox3x3Node(vx_graph graph, vx_image input, vx_image output)
+{ return make_node(graph, VX_KERNEL_BOX_3x3, {R(input), R(output)}); }
+
+vx_node vxMedian3x3Node(vx_graph graph, vx_image input, vx_image output)
+{ return make_node(graph, VX_KERNEL_MEDIAN_3x3, {R(input), R(output)}); }
+
+vx_node vxDilate3x3Node(vx_graph graph, vx_image input, vx_image output)
+{ return make_node(graph, VX_KERNEL_DILATE_3x3, {R(input), R(output)}); }
+
+vx_node vxErode3x3Node(vx_graph graph, vx_image input, vx_image output)
+{ return make_node(graph, VX_KERNEL_ERODE_3x3, {R(input), R(output)}); }
+
+vx_node vxAbsDiffNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out)
+{ return make_node(graph, VX_KERNEL_ABSDIFF, {R(in1), R(in2), R(out)}); }
+
+vx_node vxAddNode(vx_graph graph, vx_image in1, vx_image in2, vx_enum policy, vx_image out)
+{ return make_node(graph, VX_KERNEL_ADD, {R(in1), R(in2), scalar_of(graph, VX_TYPE_ENUM, &policy), R(out)}); }
+
+vx_node vxSubtractNode(vx_graph graph, vx_image in1, vx_image in2, vx_enum policy, vx_image out)
+{ return make_node(graph, VX_KERNEL_SUBTRACT, {R(in1), R(in2), scalar_of(graph, VX_TYPE_ENUM, &policy), R(out)}); }
+
+vx_node vxAndNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out)
+{ return make_node(graph, VX_KERNEL_AND, {R(in1), R(in2), R(out)}); }
+
+vx_node vxOrNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out)
+{ return make_node(graph, VX_KERNEL_OR, {R(in1), R(in2), R(out)}); }
+
+vx_node vxXorNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out)
+{ return make_node(graph, VX_KERNEL_XOR, {R(in1), R(in2), R(out)}); }
+
+vx_node vxNotNode(vx_graph graph, vx_image input, vx_image output)
+{ return make_node(graph, VX_KERNEL_NOT, {R(input), R(output)}); }
+
 }  // extern "C"

@@ -176,6 +176,13 @@ enum class LK : int {
     WARP_PERSPECTIVE_U8_U8_BILINEAR_CONSTANT, REMAP_U8_U8_NEAREST_CONSTANT, REMAP_U8_U8_BILINEAR_CONSTANT,
     SCALE_GAUSSIAN_HALF_U8_U8_5x5, OPTICAL_FLOW_PYR_LK_XY_XY,
     WARP_PERSPECTIVE_U8_U8_NEAREST, WARP_PERSPECTIVE_U8_U8_BILINEAR, REMAP_U8_U8_NEAREST, REMAP_U8_U8_BILINEAR,
+    BOX_U8_U8_3x3, DILATE_U8_U8_3x3, ERODE_U8_U8_3x3, MEDIAN_U8_U8_3x3,
+    ABS_DIFF_U8_U8U8, ABS_DIFF_S16_S16S16_SAT,
+    ADD_U8_U8U8_WRAP, ADD_U8_U8U8_SAT, ADD_S16_U8U8, ADD_S16_S16U8_WRAP, ADD_S16_S16U8_SAT,
+    ADD_S16_S16S16_WRAP, ADD_S16_S16S16_SAT,
+    SUB_U8_U8U8_WRAP, SUB_U8_U8U8_SAT, SUB_S16_U8U8, SUB_S16_S16U8_WRAP, SUB_S16_S16U8_SAT,
+    SUB_S16_U8S16_WRAP, SUB_S16_U8S16_SAT, SUB_S16_S16S16_WRAP, SUB_S16_S16S16_SAT,
+    AND_U8_U8U8, OR_U8_U8U8, XOR_U8_U8U8, NOT_U8_U8, THRESHOLD_U8_U8_RANGE,
     COUNT
 };
 const char *lk_name(LK k);

@@ -167,6 +167,11 @@ _SIGS = {
     "vxWarpPerspectiveNode": (vp, [vp, vp, vp, i32, vp]), "vxRemapNode": (vp, [vp, vp, vp, i32, vp]),
     "vxGaussianPyramidNode": (vp, [vp, vp, vp]), "vxHalfScaleGaussianNode": (vp, [vp, vp, vp, i32]),
     "vxOpticalFlowPyrLKNode": (vp, [vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, sz]),
+    "vxBox3x3Node": (vp, [vp, vp, vp]), "vxMedian3x3Node": (vp, [vp, vp, vp]),
+    "vxDilate3x3Node": (vp, [vp, vp, vp]), "vxErode3x3Node": (vp, [vp, vp, vp]),
+    "vxAbsDiffNode": (vp, [vp, vp, vp, vp]), "vxAndNode": (vp, [vp, vp, vp, vp]), "vxOrNode": (vp, [vp, vp, vp, vp]),
+    "vxXorNode": (vp, [vp, vp, vp, vp]), "vxNotNode": (vp, [vp, vp, vp]),
+    "vxAddNode": (vp, [vp, vp, vp, i32, vp]), "vxSubtractNode": (vp, [vp, vp, vp, i32, vp]),
 }
 
 _PIX = {VX_DF_IMAGE_U8: (np.uint8, 1), VX_DF_IMAGE_U16: (np.uint16, 1), VX_DF_IMAGE_S16: (np.int16, 1),
