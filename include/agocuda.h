@@ -552,6 +552,49 @@ int agocuda_Erode_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight,
 int agocuda_Median_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
                              const uint8_t *pSrc, uint32_t srcStride);
 
+/* ------------------------------------------------------------------------------------ */
+/* Fused U8 pixel chains: element-wise and 3x3 kernels through on-chip intermediates.    */
+/* The device counterpart of AGO's GPU supernodes (ago/ago_drama_alloc.cpp:484), which   */
+/* merge element-wise and fixed-neighbourhood kernels into one generated kernel; the     */
+/* HIP target has no equivalent.  Each op applies to the chain's current value; binary   */
+/* ops take their other operand from the frame's side image `side`.                     */
+/* ------------------------------------------------------------------------------------ */
+enum agocuda_pixel_opcode {
+    AGOCUDA_PX_NOT = 1,                /* Not_U8_U8                                         */
+    AGOCUDA_PX_AND, AGOCUDA_PX_OR, AGOCUDA_PX_XOR, AGOCUDA_PX_ABSDIFF,
+    AGOCUDA_PX_ADD_WRAP, AGOCUDA_PX_ADD_SAT, AGOCUDA_PX_SUB_WRAP, AGOCUDA_PX_SUB_SAT,
+    AGOCUDA_PX_THRESHOLD_BINARY,       /* p0: threshold (v > p0 -> 255)                     */
+    AGOCUDA_PX_THRESHOLD_RANGE,        /* p0, p1: lower, upper                              */
+    AGOCUDA_PX_BOX3x3, AGOCUDA_PX_MEDIAN3x3, AGOCUDA_PX_DILATE3x3, AGOCUDA_PX_ERODE3x3,
+    AGOCUDA_PX_GAUSSIAN3x3
+};
+#define AGOCUDA_PX_MAX_OPS 16
+#define AGOCUDA_PX_MAX_SIDES 3
+#define AGOCUDA_PX_MAX_STENCILS 4      /* 3x3 ops per chain */
+typedef struct agocuda_pixel_op {
+    int32_t code;                      /* agocuda_pixel_opcode */
+    int32_t side;                      /* binary ops: index into agocuda_pixel_frame.side */
+    int32_t sideFirst;                 /* SUB: 1 when the side image is the minuend */
+    int32_t p0, p1;                    /* threshold parameters (as vx_uint8) */
+} agocuda_pixel_op;
+typedef struct agocuda_pixel_program {
+    int32_t numOps;
+    agocuda_pixel_op ops[AGOCUDA_PX_MAX_OPS];
+} agocuda_pixel_program;
+/* Row bases 4-byte aligned, strides multiples of 4 and at least the width. */
+typedef struct agocuda_pixel_frame {
+    const uint8_t *src;
+    uint8_t *dst;
+    const uint8_t *side[AGOCUDA_PX_MAX_SIDES];
+    uint32_t width, height, srcStride, dstStride, sideStride[AGOCUDA_PX_MAX_SIDES];
+} agocuda_pixel_frame;
+/* Runs `program` over every frame (`frames` is a DEVICE array) in one launch.  Inside the
+ * valid rectangle of the chain's last output (every 3x3 op trims one pixel per side) the
+ * result equals the ops run one by one; other pixels are unspecified. */
+int agocuda_fused_PixelChain_U8(void *stream, const agocuda_pixel_program *program,
+                                const agocuda_pixel_frame *frames, uint32_t numFrames, uint32_t maxWidth,
+                                uint32_t maxHeight);
+
 #ifdef __cplusplus
 }
 #endif

@@ -505,7 +505,124 @@ struct Chain {
     std::vector<int64_t> key;         // by-value parameters: chains with equal keys batch
     Ref *src = nullptr, *dst = nullptr;
     std::vector<Ref *> elide;         // intermediates the fused kernel keeps on chip
+    agocuda_pixel_program prog{};     // fused_PixelChain: the ops
+    std::vector<Ref *> sides;         // fused_PixelChain: second operands of binary ops
 };
+
+// U8 -> U8 kernels the fused pixel-chain kernel runs (0: not one of them)
+static int px_code(LK k)
+{
+    switch (k) {
+    case LK::NOT_U8_U8: return AGOCUDA_PX_NOT;
+    case LK::AND_U8_U8U8: return AGOCUDA_PX_AND;
+    case LK::OR_U8_U8U8: return AGOCUDA_PX_OR;
+    case LK::XOR_U8_U8U8: return AGOCUDA_PX_XOR;
+    case LK::ABS_DIFF_U8_U8U8: return AGOCUDA_PX_ABSDIFF;
+    case LK::ADD_U8_U8U8_WRAP: return AGOCUDA_PX_ADD_WRAP;
+    case LK::ADD_U8_U8U8_SAT: return AGOCUDA_PX_ADD_SAT;
+    case LK::SUB_U8_U8U8_WRAP: return AGOCUDA_PX_SUB_WRAP;
+    case LK::SUB_U8_U8U8_SAT: return AGOCUDA_PX_SUB_SAT;
+    case LK::THRESHOLD_U8_U8_BINARY: return AGOCUDA_PX_THRESHOLD_BINARY;
+    case LK::THRESHOLD_U8_U8_RANGE: return AGOCUDA_PX_THRESHOLD_RANGE;
+    case LK::BOX_U8_U8_3x3: return AGOCUDA_PX_BOX3x3;
+    case LK::MEDIAN_U8_U8_3x3: return AGOCUDA_PX_MEDIAN3x3;
+    case LK::DILATE_U8_U8_3x3: return AGOCUDA_PX_DILATE3x3;
+    case LK::ERODE_U8_U8_3x3: return AGOCUDA_PX_ERODE3x3;
+    case LK::GAUSSIAN_U8_U8_3x3: return AGOCUDA_PX_GAUSSIAN3x3;
+    default: return 0;
+    }
+}
+static bool px_binary(int code) { return code >= AGOCUDA_PX_AND && code <= AGOCUDA_PX_SUB_SAT; }
+static bool px_stencil(int code) { return code >= AGOCUDA_PX_BOX3x3; }
+
+static int writer_level(Graph *g, Ref *d)
+{
+    int lv = -1;
+    for (const LNode &ln : g->lnodes) {
+        if (ln.removed) continue;
+        for (size_t i = 0; i < ln.p.size(); i++)
+            if (lnode_is_output(ln, i) && ln.p[i] == d) lv = std::max(lv, ln.level);
+    }
+    return lv;
+}
+
+// A maximal run of U8 pixel kernels linked by private virtual images (two or more nodes).
+// The second operands of binary kernels become side inputs; each must be ready before the
+// chain's first node runs (written at a lower level, or a graph input).
+static bool match_pixel_chain(Graph *g, LNode &a, const std::set<LNode *> &taken, Chain &c)
+{
+    const int code0 = px_code(a.k);
+    if (!code0) return false;
+    agocuda_pixel_program P{};
+    std::vector<Ref *> sides, elide;
+    std::vector<LNode *> nodes;
+    int stencils = 0;
+    auto add_op = [&](const LNode &n, int code, Ref *other, int first) -> bool {
+        if (P.numOps >= AGOCUDA_PX_MAX_OPS) return false;
+        if (px_stencil(code) && stencils >= AGOCUDA_PX_MAX_STENCILS) return false;
+        agocuda_pixel_op op{code, -1, first, 0, 0};
+        if (px_binary(code)) {
+            if (!other || other->type != VX_TYPE_IMAGE || IMG(other)->format != VX_DF_IMAGE_U8) return false;
+            if (writer_level(g, other) >= a.level) return false;
+            size_t k = std::find(sides.begin(), sides.end(), other) - sides.begin();
+            if (k == sides.size()) {
+                if (sides.size() >= AGOCUDA_PX_MAX_SIDES) return false;
+                sides.push_back(other);
+            }
+            op.side = (int32_t)k;
+        }
+        if (code == AGOCUDA_PX_THRESHOLD_BINARY) op.p0 = static_cast<Threshold *>(n.p[2])->value.U8;
+        if (code == AGOCUDA_PX_THRESHOLD_RANGE) {
+            op.p0 = static_cast<Threshold *>(n.p[2])->lower.U8;
+            op.p1 = static_cast<Threshold *>(n.p[2])->upper.U8;
+        }
+        if (px_stencil(code)) stencils++;
+        P.ops[P.numOps++] = op;
+        return true;
+    };
+    Ref *src = a.p[1];
+    if (!add_op(a, code0, px_binary(code0) ? a.p[2] : nullptr, 0)) return false;
+    nodes.push_back(&a);
+    Ref *out = a.p[0];
+    for (;;) {
+        if (!private_virtual(g, out) || IMG(out)->parent) break;
+        LNode *n = const_cast<LNode *>(reader_of(g, out));
+        if (!n || n->removed || taken.count(n)) break;
+        const int cd = px_code(n->k);
+        if (!cd) break;
+        Ref *other = nullptr;
+        int first = 0;
+        if (px_binary(cd)) {
+            if (n->p[1] == out && n->p[2] != out) other = n->p[2];
+            else if (n->p[2] == out && n->p[1] != out) { other = n->p[1]; first = 1; }
+            else break;
+        } else if (n->p[1] != out) {
+            break;
+        }
+        const agocuda_pixel_program keep = P;
+        const size_t nsides = sides.size();
+        const int kst = stencils;
+        if (!add_op(*n, cd, other, first)) { P = keep; sides.resize(nsides); stencils = kst; break; }
+        elide.push_back(out);
+        nodes.push_back(n);
+        out = n->p[0];
+    }
+    if (nodes.size() < 2) return false;
+    Image *s = IMG(src), *d = IMG(out);
+    if (s->width != d->width || s->height != d->height || s->width < 4 || s->height < 3) return false;
+    c.kind = "fused_PixelChain";
+    c.nodes = nodes;
+    c.src = src; c.dst = out;
+    c.elide = elide;
+    c.prog = P;
+    c.sides = sides;
+    c.key = {P.numOps, (int64_t)sides.size()};
+    for (int k = 0; k < P.numOps; k++) {
+        const agocuda_pixel_op &op = P.ops[k];
+        c.key.insert(c.key.end(), {op.code, op.side, op.sideFirst, op.p0, op.p1});
+    }
+    return true;
+}
 
 // Gaussian3x3 -> SobelMagnitude -> ColorDepth_U8_S16_Sat -> Threshold_U8_U8_Binary
 static bool match_gauss_sobelmag_thresh(Graph *g, LNode &a, Chain &c)
@@ -675,6 +792,44 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
     const Chain &c0 = chains[0];
     st.name = c0.kind + " x" + std::to_string(chains.size());
     for (Chain &c : chains) for (LNode *n : c.nodes) st.nodes.push_back(n);
+    if (c0.kind == "fused_PixelChain") {
+        std::vector<agocuda_pixel_frame> fr;
+        for (Chain &c : chains) {
+            Image *s = IMG(c.src), *d = IMG(c.dst);
+            agocuda_pixel_frame f{};
+            f.src = s->planes[0].dev; f.srcStride = s->planes[0].dev_stride;
+            f.dst = d->planes[0].dev; f.dstStride = d->planes[0].dev_stride;
+            f.width = d->width; f.height = d->height;
+            for (size_t k = 0; k < c.sides.size(); k++) {
+                Image *sd = IMG(c.sides[k]);
+                if (sd->width != d->width || sd->height != d->height) return VX_ERROR_INVALID_DIMENSION;
+                f.side[k] = sd->planes[0].dev; f.sideStride[k] = sd->planes[0].dev_stride;
+            }
+            fr.push_back(f);
+        }
+        agocuda_pixel_frame *dev = (agocuda_pixel_frame *)scratch(g, fr.size() * sizeof(agocuda_pixel_frame));
+        if (!dev) return VX_ERROR_NO_MEMORY;
+        cudaMemcpy(dev, fr.data(), fr.size() * sizeof(agocuda_pixel_frame), cudaMemcpyHostToDevice);
+        const agocuda_pixel_program prog = c0.prog;
+        std::vector<std::function<int(cudaStream_t)>> fns;
+        for (size_t k0 = 0; k0 < fr.size(); k0 += kGroupFrames) {
+            const size_t k1 = std::min(fr.size(), k0 + kGroupFrames);
+            uint32_t gw = 0, gh = 0;
+            for (size_t k = k0; k < k1; k++) { gw = std::max(gw, fr[k].width); gh = std::max(gh, fr[k].height); }
+            const agocuda_pixel_frame *d0 = dev + k0;
+            const uint32_t n = (uint32_t)(k1 - k0);
+            fns.push_back([=](cudaStream_t q) { return agocuda_fused_PixelChain_U8(S(q), &prog, d0, n, gw, gh); });
+            Part pt{fns.back(), {}};
+            for (size_t k = k0; k < k1; k++) for (LNode *nd : chains[k].nodes) pt.nodes.push_back(nd);
+            st.parts.push_back(std::move(pt));
+        }
+        st.num_kernels = (int)fns.size();
+        st.launch = [fns](cudaStream_t q) {
+            for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
+            return 0;
+        };
+        return VX_SUCCESS;
+    }
     if (c0.kind == "fused_GaussSobelMagDepthThresh") {
         std::vector<agocuda_frame> fr;
         for (Chain &c : chains) {
@@ -759,6 +914,7 @@ vx_status plan_graph(Graph *g)
             else if (match_color_scale(g, ln, c)) pattern = 4;
             else if (ln.k == LK::SCALE_GAUSSIAN_HALF_U8_U8_5x5) { c.kind = "batch_ScaleGaussianHalf"; c.nodes = {&ln}; pattern = 5; }
             else if (ln.k == LK::OPTICAL_FLOW_PYR_LK_XY_XY) { c.kind = "batch_OpticalFlowPyrLK"; c.nodes = {&ln}; pattern = 6; }
+            else if (match_pixel_chain(g, ln, fused, c)) pattern = 7;
             for (LNode *n : c.nodes) if (pattern && fused.count(n)) pattern = 0;   // a node joins one chain
             if (pattern) {
                 std::vector<int64_t> gk{pattern, ln.level};

@@ -308,3 +308,190 @@ FILTER(Dilate_U8_U8_3x3, F_DILATE)
 FILTER(Erode_U8_U8_3x3, F_ERODE)
 FILTER(Median_U8_U8_3x3, F_MEDIAN)
 #undef FILTER
+
+// ---------------------------------------------------------------------------------
+// Fused U8 pixel chains: a sequence of element-wise and 3x3 neighbourhood kernels whose
+// intermediates are private virtual images runs as one kernel; the intermediates live in
+// shared memory.  This is the device-side counterpart of AGO's GPU "supernodes", which group
+// element-wise (AGO_KERNEL_OP_TYPE_ELEMENT_WISE) and fixed-neighbourhood kernels
+// (AGO_KERNEL_OP_TYPE_FIXED_NEIGHBORS, ago_internal.h:96-97) into one generated kernel
+// (ago_drama_alloc.cpp:484).
+//
+// A block owns a 128x32 output tile.  It loads the input (and each side input of a binary
+// op) over the tile plus 4 columns and K rows on every side, K = number of 3x3 stages, as
+// 32-bit words into shared memory; each 3x3 stage shrinks the rows it produces by one on
+// each side (the columns keep their 4-pixel margin, enough for K <= 4), element-wise
+// stages update in place.  Pixels inside the chain's valid rectangle read only image
+// pixels, so they equal the per-node kernels' results; pixels outside it are unspecified.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr int kPxTW = 128, kPxTH = 32, kPxWords = (kPxTW + 8) / 4;   // 34 words: 4-column margins
+constexpr int kPxMaxBH = kPxTH + 2 * AGOCUDA_PX_MAX_STENCILS;
+constexpr int kPxThreads = 256, kPxGroups = kPxThreads / kPxWords;    // 7 row groups of 34 word columns
+
+__device__ __forceinline__ bool px_stencil(int code)
+{
+    return code == AGOCUDA_PX_BOX3x3 || code == AGOCUDA_PX_MEDIAN3x3 || code == AGOCUDA_PX_DILATE3x3 ||
+           code == AGOCUDA_PX_ERODE3x3 || code == AGOCUDA_PX_GAUSSIAN3x3;
+}
+
+__device__ __forceinline__ Row3 srow3(const uint32_t (*b)[kPxWords], int r, int w)
+{
+    const uint32_t L = b[r][w > 0 ? w - 1 : 0], C = b[r][w], R = b[r][w + 1 < kPxWords ? w + 1 : w];
+    return Row3{__funnelshift_r(L, C, 24), C, __funnelshift_r(C, R, 8)};
+}
+
+// Gaussian 3x3 ([1 2 1]^T [1 2 1]) >> 4 (HafCpu_Gaussian_U8_U8_3x3, ago_haf_cpu_filter.cpp:1518)
+__device__ __forceinline__ Sum3 gsum(const Row3 &r)
+{
+    return Sum3{__byte_perm(r.l, 0, 0x4240) + 2 * __byte_perm(r.c, 0, 0x4240) + __byte_perm(r.r, 0, 0x4240),
+                __byte_perm(r.l, 0, 0x4341) + 2 * __byte_perm(r.c, 0, 0x4341) + __byte_perm(r.r, 0, 0x4341)};
+}
+
+__device__ __forceinline__ uint32_t gauss_word(const Row3 &a, const Row3 &b, const Row3 &c)
+{
+    const Sum3 A = gsum(a), B = gsum(b), C = gsum(c);
+    const uint32_t e = ((A.E + 2 * B.E + C.E) >> 4) & 0x00ff00ffu, o = ((A.O + 2 * B.O + C.O) >> 4) & 0x00ff00ffu;
+    return e | (o << 8);
+}
+
+__device__ __forceinline__ uint32_t stencil_word(int code, const Row3 &a, const Row3 &b, const Row3 &c)
+{
+    switch (code) {
+    case AGOCUDA_PX_BOX3x3: return box_word(sum3(a), sum3(b), sum3(c));
+    case AGOCUDA_PX_GAUSSIAN3x3: return gauss_word(a, b, c);
+    case AGOCUDA_PX_DILATE3x3:
+        return __vmaxu4(__vmaxu4(__vmaxu4(a.l, a.c), __vmaxu4(a.r, b.l)),
+                        __vmaxu4(__vmaxu4(b.c, b.r), __vmaxu4(__vmaxu4(c.l, c.c), c.r)));
+    case AGOCUDA_PX_ERODE3x3:
+        return __vminu4(__vminu4(__vminu4(a.l, a.c), __vminu4(a.r, b.l)),
+                        __vminu4(__vminu4(b.c, b.r), __vminu4(__vminu4(c.l, c.c), c.r)));
+    default: {   // median
+        uint32_t lL, mL, hL, lC, mC, hC, lR, mR, hR;
+        sort3(a.l, b.l, c.l, lL, mL, hL);
+        sort3(a.c, b.c, c.c, lC, mC, hC);
+        sort3(a.r, b.r, c.r, lR, mR, hR);
+        return med3(__vmaxu4(__vmaxu4(lL, lC), lR), med3(mL, mC, mR), __vminu4(__vminu4(hL, hC), hR));
+    }
+    }
+}
+
+// element-wise op on 4 pixels: v = the chain's value, o = the side operand
+__device__ __forceinline__ uint32_t ew_word(const agocuda_pixel_op &op, uint32_t v, uint32_t o)
+{
+    const uint32_t a = op.sideFirst ? o : v, b = op.sideFirst ? v : o;
+    switch (op.code) {
+    case AGOCUDA_PX_NOT: return ~v;
+    case AGOCUDA_PX_AND: return v & o;
+    case AGOCUDA_PX_OR: return v | o;
+    case AGOCUDA_PX_XOR: return v ^ o;
+    case AGOCUDA_PX_ABSDIFF: return __vabsdiffu4(v, o);
+    case AGOCUDA_PX_ADD_WRAP: return __vadd4(v, o);
+    case AGOCUDA_PX_ADD_SAT: return __vaddus4(v, o);
+    case AGOCUDA_PX_SUB_WRAP: return __vsub4(a, b);
+    case AGOCUDA_PX_SUB_SAT: return __vsubus4(a, b);
+    case AGOCUDA_PX_THRESHOLD_BINARY: return __vcmpgtu4(v, (uint32_t)(op.p0 & 0xff) * 0x01010101u);
+    case AGOCUDA_PX_THRESHOLD_RANGE:
+        return ~(__vcmpgtu4(v, (uint32_t)(op.p1 & 0xff) * 0x01010101u) | __vcmpltu4(v, (uint32_t)(op.p0 & 0xff) * 0x01010101u));
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kPxThreads)
+k_pixel_chain(const agocuda_pixel_program prog, const agocuda_pixel_frame *__restrict__ frames, int K, int nSides)
+{
+    __shared__ uint32_t buf[2][kPxMaxBH][kPxWords];
+    __shared__ uint32_t side[AGOCUDA_PX_MAX_SIDES][kPxMaxBH][kPxWords];
+    const agocuda_pixel_frame f = frames[blockIdx.z];
+    const int W = (int)f.width, H = (int)f.height;
+    const int x0 = blockIdx.x * kPxTW, y0 = blockIdx.y * kPxTH, tid = threadIdx.x;
+    if (x0 >= W || y0 >= H) return;
+    const int BH = kPxTH + 2 * K;
+    for (int i = tid; i < BH * kPxWords; i += kPxThreads) {
+        const int r = i / kPxWords, w = i - r * kPxWords;
+        const int y = clampi(y0 - K + r, 0, H - 1), x = x0 - 4 + 4 * w;
+        buf[0][r][w] = load_word_clamped(f.src + (size_t)y * f.srcStride, x, (int)f.srcStride);
+        for (int s = 0; s < nSides; s++)
+            side[s][r][w] = load_word_clamped(f.side[s] + (size_t)y * f.sideStride[s], x, (int)f.sideStride[s]);
+    }
+    __syncthreads();
+    int cur = 0, st = 0;
+    for (int k = 0; k < prog.numOps; k++) {
+        const agocuda_pixel_op op = prog.ops[k];
+        if (px_stencil(op.code)) {
+            st++;
+            // rows [st, BH - st) from rows [st - 1, BH - st + 1): a word column per thread,
+            // its rows split over the row groups, the three rows of the window in registers
+            const int rows = BH - 2 * st, per = (rows + kPxGroups - 1) / kPxGroups;
+            const int w = tid % kPxWords, grp = tid / kPxWords;
+            const int r0 = st + grp * per, r1 = min(r0 + per, BH - st);
+            if (grp < kPxGroups && r0 < r1) {
+                Row3 a = srow3(buf[cur], r0 - 1, w), b = srow3(buf[cur], r0, w);
+                for (int r = r0; r < r1; r++) {
+                    const Row3 c = srow3(buf[cur], r + 1, w);
+                    buf[cur ^ 1][r][w] = stencil_word(op.code, a, b, c);
+                    a = b;
+                    b = c;
+                }
+            }
+            cur ^= 1;
+        } else {
+            const int rows = BH - 2 * st;
+            for (int i = tid; i < rows * kPxWords; i += kPxThreads) {
+                const int r = st + i / kPxWords, w = i % kPxWords;
+                const uint32_t o = op.side >= 0 ? side[op.side][r][w] : 0u;
+                buf[cur][r][w] = ew_word(op, buf[cur][r][w], o);
+            }
+        }
+        __syncthreads();
+    }
+    // tile rows [K, K + 32) of the buffer, words 1..32 (columns x0 .. x0 + 127)
+    for (int i = tid; i < kPxTH * (kPxTW / 4); i += kPxThreads) {
+        const int r = i / (kPxTW / 4), w = i % (kPxTW / 4);
+        const int y = y0 + r, x = x0 + 4 * w;
+        if (y >= H || x >= W) continue;
+        const uint32_t v = buf[cur][K + r][w + 1];
+        uint8_t *d = f.dst + (size_t)y * f.dstStride + x;
+        if (x + 4 <= W) {
+            *(uint32_t *)d = v;
+        } else {
+            for (int j = 0; j < W - x; j++) d[j] = (uint8_t)(v >> (8 * j));
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int agocuda_fused_PixelChain_U8(void *stream, const agocuda_pixel_program *program,
+                                           const agocuda_pixel_frame *frames, uint32_t numFrames, uint32_t maxWidth,
+                                           uint32_t maxHeight)
+{
+    if (!program || !frames || !numFrames || numFrames > 65535 || !maxWidth || !maxHeight || program->numOps < 1 ||
+        program->numOps > AGOCUDA_PX_MAX_OPS)
+        return AGOCUDA_INVALID_PARAMS;
+    int K = 0, nSides = 0;
+    for (int k = 0; k < program->numOps; k++) {
+        const agocuda_pixel_op &op = program->ops[k];
+        if (op.code < AGOCUDA_PX_NOT || op.code > AGOCUDA_PX_GAUSSIAN3x3) return AGOCUDA_INVALID_PARAMS;
+        const bool stencil = op.code >= AGOCUDA_PX_BOX3x3;
+        const bool binary = op.code >= AGOCUDA_PX_AND && op.code <= AGOCUDA_PX_SUB_SAT;
+        if (stencil) K++;
+        if (binary) {
+            if (op.side < 0 || op.side >= AGOCUDA_PX_MAX_SIDES) return AGOCUDA_INVALID_PARAMS;
+            nSides = op.side + 1 > nSides ? op.side + 1 : nSides;
+        } else if (op.side >= AGOCUDA_PX_MAX_SIDES) {
+            return AGOCUDA_INVALID_PARAMS;
+        }
+    }
+    if (K > AGOCUDA_PX_MAX_STENCILS) return AGOCUDA_INVALID_PARAMS;
+    agocuda_pixel_program p = *program;
+    for (int k = 0; k < p.numOps; k++) {   // unary ops read no side operand
+        const int c = p.ops[k].code;
+        if (!(c >= AGOCUDA_PX_AND && c <= AGOCUDA_PX_SUB_SAT)) p.ops[k].side = -1;
+    }
+    dim3 grd(div_up(maxWidth, kPxTW), div_up(maxHeight, kPxTH), numFrames);
+    k_pixel_chain<<<grd, kPxThreads, 0, as_stream(stream)>>>(p, frames, K, nSides);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}

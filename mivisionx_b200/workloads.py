@@ -238,6 +238,69 @@ class Cfg1Graph:
         return [(self.api.read_plane(o), self.api.valid_region(o)) for o in self.outputs]
 
 
+def motion_pair(seed: int = 1, width: int = 3840, height: int = 2160, rects: int = 150, sigma: float = 3.0):
+    """Two U8 frames of a scene: a horizontal gradient with `rects` seeded rectangles (sides
+    16..256 px, intensity uniform 0..255), each displaced by up to 12 px in the second frame,
+    plus independent N(0, sigma^2) noise per frame."""
+    r = np.random.default_rng(seed)
+    base = np.tile(np.linspace(0.0, 160.0, width), (height, 1))
+    f0, f1 = base.copy(), base.copy()
+    for _ in range(rects):
+        w, h = (int(v) for v in r.integers(16, 257, 2))
+        x, y = int(r.integers(0, max(1, width - w))), int(r.integers(0, max(1, height - h)))
+        dx, dy = (int(v) for v in r.integers(-12, 13, 2))
+        level = float(r.integers(0, 256))
+        f0[y:y + h, x:x + w] = level
+        x1, y1 = min(max(x + dx, 0), max(0, width - w)), min(max(y + dy, 0), max(0, height - h))
+        f1[y1:y1 + h, x1:x1 + w] = level
+    out = []
+    for f in (f0, f1):
+        f = f + sigma * r.standard_normal(f.shape)
+        out.append(np.clip(np.rint(f), 0, 255).astype(np.uint8))
+    return out[0], out[1]
+
+
+class MotionGraph:
+    """Motion mask of frame pairs: AbsDiff(cur, prev) -> Gaussian3x3 -> Threshold(BINARY, thr) ->
+    Dilate3x3 -> Erode3x3 -> Median3x3, for each of `sizes` pairs in one graph, intermediates
+    virtual (fused into one pixel-chain kernel by this target)."""
+
+    def __init__(self, api: V.OpenVX, ctx, sizes, thr: int = 24, flags: int | None = None,
+                 host_io: dict | None = None):
+        host_io = host_io or {}
+        self.api, self.ctx = api, ctx
+        a = api
+        self.graph = a.obj(a.vxCreateGraph(ctx), "graph")
+        if flags is not None:
+            a.set_optimizer_flags(self.graph, flags)
+        self.thr = a.threshold_binary(ctx, thr)
+        self.inputs, self.outputs = [], []
+        g = self.graph
+        for i, (w, h) in enumerate(sizes):
+            prev = _u8_image(a, ctx, w, h, host_io.get("prev"), i)
+            cur = _u8_image(a, ctx, w, h, host_io.get("cur"), i)
+            dst = _u8_image(a, ctx, w, h, host_io.get("dst"), i)
+            v = [a.vxCreateVirtualImage(g, w, h, V.VX_DF_IMAGE_U8) for _ in range(5)]
+            for n in (a.vxAbsDiffNode(g, cur, prev, v[0]), a.vxGaussian3x3Node(g, v[0], v[1]),
+                      a.vxThresholdNode(g, v[1], self.thr, v[2]), a.vxDilate3x3Node(g, v[2], v[3]),
+                      a.vxErode3x3Node(g, v[3], v[4]), a.vxMedian3x3Node(g, v[4], dst)):
+                a.obj(n, "node")
+            self.inputs += [prev, cur]
+            self.outputs.append(dst)
+        a.ok(a.vxVerifyGraph(g), "vxVerifyGraph")
+
+    def run(self, frames=None):
+        """frames: [prev0, cur0, prev1, cur1, ...]"""
+        a = self.api
+        if frames is not None:
+            for img, f in zip(self.inputs, frames):
+                a.write_plane(img, f)
+        a.ok(a.vxProcessGraph(self.graph), "vxProcessGraph")
+
+    def results(self):
+        return [(self.api.read_plane(o), self.api.valid_region(o)) for o in self.outputs]
+
+
 class Cfg3Graph:
     """Colour and geometry: RGB -> NV12 and RGB -> IYUV, ChannelExtract Y (virtual), ScaleImage
     of Y to half size (bilinear and area), WarpAffine of the bilinear result (nearest and

@@ -86,6 +86,26 @@ def box3x3(img):
     return _interior(img, ((s * 7282) >> 16).astype(np.uint8))
 
 
+def gaussian3x3(img):
+    """HafCpu_Gaussian_U8_U8_3x3 (ago_haf_cpu_filter.cpp:1518): [1 2 1]^T [1 2 1] sum >> 4."""
+    img = np.asarray(img, np.uint8)
+    w = _windows(img)
+    k = ((1, 2, 1), (2, 4, 2), (1, 2, 1))
+    s = sum(k[i][j] * _i32(w[i][j]) for i in range(3) for j in range(3))
+    return _interior(img, (s >> 4).astype(np.uint8))
+
+
+def threshold_binary(a, value):
+    """HafCpu_Threshold_U8_U8_Binary (ago_haf_cpu_arithmetic.cpp:3660): 255 where v > value."""
+    return np.where(np.asarray(a, np.uint8) > (int(value) & 0xFF), 255, 0).astype(np.uint8)
+
+
+def motion_mask(prev, cur, thr):
+    """AbsDiff(cur, prev) -> Gaussian3x3 -> Threshold(BINARY, thr) -> Dilate3x3 -> Erode3x3 ->
+    Median3x3; valid on [4, W-4) x [4, H-4)."""
+    return median3x3(erode3x3(dilate3x3(threshold_binary(gaussian3x3(absdiff(cur, prev)), thr))))
+
+
 def dilate3x3(img):
     """HafCpu_Dilate_U8_U8_3x3 (ago_haf_cpu_filter.cpp:221): maximum of the window."""
     img = np.asarray(img, np.uint8)
