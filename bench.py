@@ -185,7 +185,34 @@ class ColorGeometry(Workload):
         return 7.0 * self.width * self.height * n
 
 
-WORKLOADS = {w.name: w for w in (CannyHarris(), GaussChain(), PyramidLK(), ColorGeometry())}
+class MotionMask(Workload):
+    name = "motion_mask_4k"
+    desc = ("Motion mask of frame pairs: AbsDiff(cur, prev) -> Gaussian3x3 -> Threshold(BINARY, 24) -> Dilate3x3 -> "
+            "Erode3x3 -> Median3x3, border UNDEFINED, virtual intermediates; 3840x2160 U8 pairs (gradient + 150 "
+            "seeded rectangles displaced by up to 12 px + N(0, 3^2) noise per frame)")
+    width, height, frames = 3840, 2160, 16     # frame pairs per step
+
+    def make_frames(self, seed0, n):
+        from mivisionx_b200 import workloads as WL
+        out = []
+        for i in range(n):
+            out += list(WL.motion_pair(seed=seed0 + i, width=self.width, height=self.height))
+        return out
+
+    def build(self, api, ctx, n, flags=None, host_io=None):
+        from mivisionx_b200 import workloads as WL
+        g = WL.MotionGraph(api, ctx, [(self.width, self.height)] * n, flags=flags, host_io=host_io)
+        g.out_images, g.out_arrays = g.outputs, []
+        return g
+
+    def host_io(self, ins, outs):
+        return {"prev": [p[0] for p in ins[0::2]], "cur": [p[0] for p in ins[1::2]], "dst": [p[0] for p in outs]}
+
+    def alg_bytes(self, g, n):
+        return 3.0 * self.width * self.height * n   # two U8 frames in + one U8 mask out per pixel
+
+
+WORKLOADS = {w.name: w for w in (CannyHarris(), GaussChain(), PyramidLK(), ColorGeometry(), MotionMask())}
 DEFAULT_WORKLOAD = CannyHarris.name
 
 

@@ -460,9 +460,9 @@ int agocuda_array_download(void *stream, void *hostItemsMapped, uint32_t *countS
 /* ------------------------------------------------------------------------------------ */
 /* Element-wise kernels (reference: hipvx/hip_host_decls.h arithmetic/logical kernels;   */
 /* CPU semantics ago/ago_haf_cpu_arithmetic.cpp, ago/ago_haf_cpu_logical.cpp)            */
-/* Every pixel of [0,W)x[0,H).  Planes: row base aligned to 8 pixels' bytes (8 B for U8,  */
-/* 16 B for S16) and the stride a multiple of it.  _Wrap keeps the low bits of the exact  */
-/* result, _Sat clamps it to the output type; S16 results of two U8 inputs are exact.     */
+/* Every pixel of [0,W)x[0,H).  Planes: row base 16-byte aligned and the stride a         */
+/* multiple of 16.  _Wrap keeps the low bits of the exact result, _Sat clamps it to the    */
+/* output type; S16 results of two U8 inputs are exact.                                   */
 /* ------------------------------------------------------------------------------------ */
 
 /* dst = src1 + src2.  Replace HipExec_Add_U8_U8U8_Wrap / _Sat (hip_host_decls.h:43, :48),
@@ -581,7 +581,8 @@ typedef struct agocuda_pixel_program {
     int32_t numOps;
     agocuda_pixel_op ops[AGOCUDA_PX_MAX_OPS];
 } agocuda_pixel_program;
-/* Row bases 4-byte aligned, strides multiples of 4 and at least the width. */
+/* src / side planes: row bases 16-byte aligned, strides multiples of 16; dst: 4-byte aligned
+ * base and stride; every stride at least the width. */
 typedef struct agocuda_pixel_frame {
     const uint8_t *src;
     uint8_t *dst;

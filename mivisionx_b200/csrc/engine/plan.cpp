@@ -610,6 +610,18 @@ static bool match_pixel_chain(Graph *g, LNode &a, const std::set<LNode *> &taken
     if (nodes.size() < 2) return false;
     Image *s = IMG(src), *d = IMG(out);
     if (s->width != d->width || s->height != d->height || s->width < 4 || s->height < 3) return false;
+    // the kernel copies src / side rows in 16-byte chunks (images imported from device
+    // pointers may not allow that: they run per node)
+    auto a16 = [](Ref *r) {
+        const Plane &pl = IMG(r)->planes[0];
+        return IMG(r)->import_type != VX_MEMORY_TYPE_HIP || (((uintptr_t)pl.dev | pl.dev_stride) & 15) == 0;
+    };
+    auto a4 = [](Ref *r) {
+        const Plane &pl = IMG(r)->planes[0];
+        return IMG(r)->import_type != VX_MEMORY_TYPE_HIP || (((uintptr_t)pl.dev | pl.dev_stride) & 3) == 0;
+    };
+    if (!a16(src) || !a4(out)) return false;
+    for (Ref *sd : sides) if (!a16(sd)) return false;
     c.kind = "fused_PixelChain";
     c.nodes = nodes;
     c.src = src; c.dst = out;

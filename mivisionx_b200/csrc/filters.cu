@@ -35,39 +35,6 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d)
 }
 
 // ---------------------------------------------------------------------------------
-// Gaussian 3x3 (HafCpu_Gaussian_U8_U8_3x3, ago_haf_cpu_filter.cpp:1518)
-// ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBX * kBY)
-k_gaussian3x3(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride)
-{
-    const int x = (blockIdx.x * kBX + threadIdx.x) * 4;
-    const int y0 = 1 + (blockIdx.y * kBY + threadIdx.y) * kRPT;
-    if (x >= W || y0 >= H - 1) return;
-    const int y1 = min(y0 + kRPT, H - 1);
-    int hm[4], hc[4];
-    {
-        Row8 a = load_row8(src + (size_t)(y0 - 1) * srcStride, x, srcStride);
-        Row8 b = load_row8(src + (size_t)y0 * srcStride, x, srcStride);
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            hm[i] = a.p[i + 1] + 2 * a.p[i + 2] + a.p[i + 3];
-            hc[i] = b.p[i + 1] + 2 * b.p[i + 2] + b.p[i + 3];
-        }
-    }
-    for (int y = y0; y < y1; y++) {
-        Row8 n = load_row8(src + (size_t)(y + 1) * srcStride, x, srcStride);
-        int o[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            int hn = n.p[i + 1] + 2 * n.p[i + 2] + n.p[i + 3];
-            o[i] = (hm[i] + 2 * hc[i] + hn) >> 4;
-            hm[i] = hc[i]; hc[i] = hn;
-        }
-        *(uint32_t *)(dst + (size_t)y * dstStride + x) = pack4(o[0], o[1], o[2], o[3]);
-    }
-}
-
-// ---------------------------------------------------------------------------------
 // Sobel 3x3 GX/GY (HafCpu_Sobel_S16S16_U8_3x3_GXY, ago_haf_cpu_filter.cpp:2237) and
 // SobelMagnitude (HafCpu_SobelMagnitude_S16_U8_3x3, ago_haf_cpu_filter.cpp:2468).
 // Rolling state per column c in [x-1, x+4]: the row above and the current row.
@@ -388,16 +355,6 @@ extern "C" int agocuda_abi_version(void) { return 100; }
 static dim3 stencil_grid(uint32_t W, uint32_t rows)
 {
     return dim3(div_up(W, kBX * 4), div_up(rows, kBY * kRPT), 1);
-}
-
-extern "C" int agocuda_Gaussian_U8_U8_3x3(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
-                                          const uint8_t *pSrc, uint32_t srcStride)
-{
-    if (W < 3 || H < 3 || bad_plane(pDst, dstStride, W, 1, 4) || bad_plane(pSrc, srcStride, W, 1, 4))
-        return AGOCUDA_INVALID_PARAMS;
-    k_gaussian3x3<<<stencil_grid(W, H - 2), dim3(kBX, kBY), 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride);
-    agocuda_count_launch(1);
-    return agocuda_launch_status();
 }
 
 extern "C" int agocuda_Sobel_S16S16_U8_3x3_GXY(void *stream, uint32_t W, uint32_t H, int16_t *pGx, uint32_t gxStride,

@@ -2,12 +2,15 @@
 // element-wise arithmetic / logical / range-threshold kernels and the 3x3 Box, Median,
 // Dilate and Erode filters.
 //
-// Element-wise kernels are HBM-bound: a thread owns 8 pixels of a row (one 8- or 16-byte
-// vector per plane), a warp 256 contiguous pixels, and rows are spread over blockIdx.y.
-// The 3x3 filters use the stencil decomposition of filters.cu (one 32-bit word of 4 pixels
-// per thread, rows walked downwards with the previous rows' partial results in registers);
-// Dilate, Erode and Median run on all 4 pixels at once with byte-lane min/max.
+// Element-wise kernels are HBM-bound: a thread owns 16 pixels of a row (16-byte vectors),
+// a warp 512 contiguous pixels, and rows are spread over blockIdx.y.
+// The 3x3 filters give a thread 8 pixels of a row and walk it down the rows with the window's
+// rows in registers, two pixels per 32-bit register: 16-bit integer lanes for Box and
+// Gaussian, and for Dilate, Erode and Median half-float lanes holding 1024 + v, which
+// f16x2 min / max order exactly like the bytes.
 #include "agocuda_internal.cuh"
+
+#include <mutex>
 
 uint64_t agocuda_count_launch(unsigned n);
 
@@ -52,49 +55,53 @@ __device__ __forceinline__ int ew_apply(int a, int b, int p0, int p1)
     return 0;
 }
 
-template <typename T> struct Vec8;
-template <> struct Vec8<uint8_t> { using V = uint2; };
-template <> struct Vec8<int16_t> { using V = uint4; };
+constexpr int kEwPx = 16;                        // pixels per thread: 16 B of a U8 plane, 32 B of S16
 
 template <typename T>
-__device__ __forceinline__ void load8(const T *p, int *v)
+__device__ __forceinline__ void load16(const T *p, int *v)
 {
-    const typename Vec8<T>::V w = __ldg((const typename Vec8<T>::V *)p);
-    const T *e = (const T *)&w;
 #pragma unroll
-    for (int i = 0; i < 8; i++) v[i] = (int)e[i];
+    for (int h = 0; h < (int)sizeof(T); h++) {
+        const uint4 w = __ldg((const uint4 *)p + h);
+        const T *e = (const T *)&w;
+#pragma unroll
+        for (int i = 0; i < 16 / (int)sizeof(T); i++) v[h * (16 / sizeof(T)) + i] = (int)e[i];
+    }
 }
 
 template <typename T>
-__device__ __forceinline__ void store8(T *p, const int *v)
+__device__ __forceinline__ void store16(T *p, const int *v)
 {
-    typename Vec8<T>::V w;
-    T *e = (T *)&w;
 #pragma unroll
-    for (int i = 0; i < 8; i++) e[i] = (T)v[i];
-    *(typename Vec8<T>::V *)p = w;
+    for (int h = 0; h < (int)sizeof(T); h++) {
+        uint4 w;
+        T *e = (T *)&w;
+#pragma unroll
+        for (int i = 0; i < 16 / (int)sizeof(T); i++) e[i] = (T)v[h * (16 / sizeof(T)) + i];
+        *((uint4 *)p + h) = w;
+    }
 }
 
 constexpr int kEwBX = 32, kEwBY = 8;
 
-// one thread: pixels [x, x+8) of row y; the last group of a row that W cuts goes pixel by pixel
+// one thread: pixels [x, x+16) of row y; the last group of a row that W cuts goes pixel by pixel
 template <int OP, typename TO, typename TA, typename TB>
 __global__ void __launch_bounds__(kEwBX * kEwBY)
 k_elementwise(int W, int H, TO *dst, int dstStride, const TA *a, int aStride, const TB *b, int bStride, int p0, int p1)
 {
-    const int x = (blockIdx.x * kEwBX + threadIdx.x) * 8;
+    const int x = (blockIdx.x * kEwBX + threadIdx.x) * kEwPx;
     const int y = blockIdx.y * kEwBY + threadIdx.y;
     if (x >= W || y >= H) return;
     TO *d = (TO *)((uint8_t *)dst + (size_t)y * dstStride) + x;
     const TA *pa = (const TA *)((const uint8_t *)a + (size_t)y * aStride) + x;
     const TB *pb = b ? (const TB *)((const uint8_t *)b + (size_t)y * bStride) + x : nullptr;
-    if (x + 8 <= W) {
-        int va[8], vb[8] = {0, 0, 0, 0, 0, 0, 0, 0}, r[8];
-        load8(pa, va);
-        if (pb) load8(pb, vb);
+    if (x + kEwPx <= W) {
+        int va[kEwPx], vb[kEwPx], r[kEwPx];
+        load16(pa, va);
+        if (pb) load16(pb, vb);
 #pragma unroll
-        for (int i = 0; i < 8; i++) r[i] = ew_apply<OP>(va[i], vb[i], p0, p1);
-        store8(d, r);
+        for (int i = 0; i < kEwPx; i++) r[i] = ew_apply<OP>(va[i], pb ? vb[i] : 0, p0, p1);
+        store16(d, r);
     } else {
         for (int i = 0; i < W - x; i++) d[i] = (TO)ew_apply<OP>((int)pa[i], pb ? (int)pb[i] : 0, p0, p1);
     }
@@ -102,8 +109,7 @@ k_elementwise(int W, int H, TO *dst, int dstStride, const TA *a, int aStride, co
 
 template <typename T> bool ew_plane_ok(const T *p, uint32_t stride, uint32_t W)
 {
-    constexpr unsigned vec = 8 * sizeof(T);      // bytes of an 8-pixel vector
-    return p && ((uintptr_t)p % vec) == 0 && (stride % vec) == 0 && stride >= W * sizeof(T);
+    return p && ((uintptr_t)p % 16) == 0 && (stride % 16) == 0 && stride >= W * sizeof(T);
 }
 
 template <int OP, typename TO, typename TA, typename TB>
@@ -114,135 +120,9 @@ int ew_launch(void *stream, uint32_t W, uint32_t H, TO *dst, uint32_t dstStride,
     if (!W || !H || !ew_plane_ok(dst, dstStride, W) || !ew_plane_ok(a, aStride, W) ||
         (!unary && !ew_plane_ok(b, bStride, W)))
         return AGOCUDA_INVALID_PARAMS;
-    dim3 grd(div_up(W, kEwBX * 8), div_up(H, kEwBY));
+    dim3 grd(div_up(W, kEwBX * kEwPx), div_up(H, kEwBY));
     k_elementwise<OP, TO, TA, TB><<<grd, dim3(kEwBX, kEwBY), 0, as_stream(stream)>>>(
         (int)W, (int)H, dst, (int)dstStride, a, (int)aStride, unary ? nullptr : b, (int)bStride, p0, p1);
-    agocuda_count_launch(1);
-    return agocuda_launch_status();
-}
-
-// ---------------------------------------------------------------------------------
-// 3x3 filters on U8 (ago_haf_cpu_filter.cpp): interior rows [1, H-1), every column
-// ---------------------------------------------------------------------------------
-enum FOp : int { F_BOX, F_DILATE, F_ERODE, F_MEDIAN };   // F_BOX runs k_box3x3
-constexpr int kFBX = 32, kFBY = 4, kFRows = 8;
-
-// one row around the word at x: columns x-1..x+2 (l), x..x+3 (c), x+1..x+4 (r)
-struct Row3 { uint32_t l, c, r; };
-__device__ __forceinline__ Row3 row3(const uint8_t *row, int x, int stride)
-{
-    const uint32_t L = load_word_clamped(row, x - 4, stride), C = load_word_clamped(row, x, stride),
-                   R = load_word_clamped(row, x + 4, stride);
-    return Row3{__funnelshift_r(L, C, 24), C, __funnelshift_r(C, R, 8)};
-}
-
-// per-byte sort of three words
-__device__ __forceinline__ void sort3(uint32_t a, uint32_t b, uint32_t c, uint32_t &lo, uint32_t &mid, uint32_t &hi)
-{
-    const uint32_t l1 = __vminu4(a, b), h1 = __vmaxu4(a, b);
-    lo = __vminu4(l1, c);
-    const uint32_t t = __vmaxu4(l1, c);
-    mid = __vminu4(h1, t);
-    hi = __vmaxu4(h1, t);
-}
-
-__device__ __forceinline__ uint32_t med3(uint32_t a, uint32_t b, uint32_t c)
-{
-    return __vmaxu4(__vminu4(a, b), __vminu4(__vmaxu4(a, b), c));
-}
-
-// Row sums of three neighbours in 16-bit lanes: E = columns (x, x+2), O = (x+1, x+3)
-struct Sum3 { uint32_t E, O; };
-__device__ __forceinline__ Sum3 sum3(const Row3 &r)
-{
-    return Sum3{__byte_perm(r.l, 0, 0x4240) + __byte_perm(r.c, 0, 0x4240) + __byte_perm(r.r, 0, 0x4240),
-                __byte_perm(r.l, 0, 0x4341) + __byte_perm(r.c, 0, 0x4341) + __byte_perm(r.r, 0, 0x4341)};
-}
-
-// Box: floor(sum / 9) -- the reference's SIMD body computes (sum * 7282) >> 16 and its
-// scalar parts (int)((float)sum / 9.0f); both equal floor(sum / 9) for every sum of nine
-// bytes (<= 2295), and so does (sum * 7282) >> 16 here.
-__device__ __forceinline__ uint32_t box_word(const Sum3 &a, const Sum3 &b, const Sum3 &c)
-{
-    const uint32_t e = a.E + b.E + c.E, o = a.O + b.O + c.O;
-    const uint32_t q0 = ((e & 0xffff) * 7282u) >> 16, q2 = ((e >> 16) * 7282u) >> 16;
-    const uint32_t q1 = ((o & 0xffff) * 7282u) >> 16, q3 = ((o >> 16) * 7282u) >> 16;
-    return q0 | (q1 << 8) | (q2 << 16) | (q3 << 24);
-}
-
-__global__ void __launch_bounds__(kFBX * kFBY)
-k_box3x3(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride)
-{
-    const int x = (blockIdx.x * kFBX + threadIdx.x) * 4;
-    const int y0 = 1 + (blockIdx.y * kFBY + threadIdx.y) * kFRows;
-    if (x >= W || y0 >= H - 1) return;
-    const int y1 = min(y0 + kFRows, H - 1);
-    Sum3 a = sum3(row3(src + (size_t)(y0 - 1) * srcStride, x, srcStride));
-    Sum3 b = sum3(row3(src + (size_t)y0 * srcStride, x, srcStride));
-    for (int y = y0; y < y1; y++) {
-        const Sum3 c = sum3(row3(src + (size_t)(y + 1) * srcStride, x, srcStride));
-        const uint32_t o = box_word(a, b, c);
-        uint8_t *d = dst + (size_t)y * dstStride + x;
-        if (x + 4 <= W) {
-            *(uint32_t *)d = o;
-        } else {
-            for (int i = 0; i < W - x; i++) d[i] = (uint8_t)(o >> (8 * i));
-        }
-        a = b;
-        b = c;
-    }
-}
-
-template <int OP>
-__global__ void __launch_bounds__(kFBX * kFBY)
-k_filter3x3(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride)
-{
-    const int x = (blockIdx.x * kFBX + threadIdx.x) * 4;
-    const int y0 = 1 + (blockIdx.y * kFBY + threadIdx.y) * kFRows;
-    if (x >= W || y0 >= H - 1) return;
-    const int y1 = min(y0 + kFRows, H - 1);
-    Row3 a = row3(src + (size_t)(y0 - 1) * srcStride, x, srcStride);
-    Row3 b = row3(src + (size_t)y0 * srcStride, x, srcStride);
-    for (int y = y0; y < y1; y++) {
-        const Row3 c = row3(src + (size_t)(y + 1) * srcStride, x, srcStride);
-        uint32_t o;
-        if (OP == F_DILATE) {
-            o = __vmaxu4(__vmaxu4(__vmaxu4(a.l, a.c), __vmaxu4(a.r, b.l)),
-                         __vmaxu4(__vmaxu4(b.c, b.r), __vmaxu4(__vmaxu4(c.l, c.c), c.r)));
-        } else if (OP == F_ERODE) {
-            o = __vminu4(__vminu4(__vminu4(a.l, a.c), __vminu4(a.r, b.l)),
-                         __vminu4(__vminu4(b.c, b.r), __vminu4(__vminu4(c.l, c.c), c.r)));
-        } else {
-            // median of 9 = med3(max of the column minima, med3 of the column medians,
-            // min of the column maxima) once each column is sorted
-            uint32_t lL, mL, hL, lC, mC, hC, lR, mR, hR;
-            sort3(a.l, b.l, c.l, lL, mL, hL);
-            sort3(a.c, b.c, c.c, lC, mC, hC);
-            sort3(a.r, b.r, c.r, lR, mR, hR);
-            o = med3(__vmaxu4(__vmaxu4(lL, lC), lR), med3(mL, mC, mR), __vminu4(__vminu4(hL, hC), hR));
-        }
-        uint8_t *d = dst + (size_t)y * dstStride + x;
-        if (x + 4 <= W) {
-            *(uint32_t *)d = o;
-        } else {
-            for (int i = 0; i < W - x; i++) d[i] = (uint8_t)(o >> (8 * i));
-        }
-        a = b;
-        b = c;
-    }
-}
-
-template <int OP>
-int filter_launch(void *stream, uint32_t W, uint32_t H, uint8_t *dst, uint32_t dstStride, const uint8_t *src,
-                  uint32_t srcStride)
-{
-    auto ok = [&](const uint8_t *p, uint32_t s) { return p && ((uintptr_t)p & 3) == 0 && (s & 3) == 0 && s >= W; };
-    if (W < 3 || H < 3 || !ok(dst, dstStride) || !ok(src, srcStride)) return AGOCUDA_INVALID_PARAMS;
-    dim3 grd(div_up(W, kFBX * 4), div_up(H - 2, kFBY * kFRows));
-    if (OP == F_BOX)
-        k_box3x3<<<grd, dim3(kFBX, kFBY), 0, as_stream(stream)>>>((int)W, (int)H, dst, (int)dstStride, src, (int)srcStride);
-    else
-        k_filter3x3<OP><<<grd, dim3(kFBX, kFBY), 0, as_stream(stream)>>>((int)W, (int)H, dst, (int)dstStride, src, (int)srcStride);
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }
@@ -297,17 +177,6 @@ extern "C" int agocuda_Threshold_U8_U8_Range(void *stream, uint32_t dstWidth, ui
                                (int)(uint8_t)thresholdLower, (int)(uint8_t)thresholdUpper);
 }
 
-#define FILTER(NAME, OP)                                                                                          \
-    extern "C" int agocuda_##NAME(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride, \
-                                  const uint8_t *pSrc, uint32_t srcStride)                                        \
-    {                                                                                                          \
-        return filter_launch<OP>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc, srcStride);                \
-    }
-FILTER(Box_U8_U8_3x3, F_BOX)
-FILTER(Dilate_U8_U8_3x3, F_DILATE)
-FILTER(Erode_U8_U8_3x3, F_ERODE)
-FILTER(Median_U8_U8_3x3, F_MEDIAN)
-#undef FILTER
 
 // ---------------------------------------------------------------------------------
 // Fused U8 pixel chains: a sequence of element-wise and 3x3 neighbourhood kernels whose
@@ -317,71 +186,194 @@ FILTER(Median_U8_U8_3x3, F_MEDIAN)
 // (AGO_KERNEL_OP_TYPE_FIXED_NEIGHBORS, ago_internal.h:96-97) into one generated kernel
 // (ago_drama_alloc.cpp:484).
 //
-// A block owns a 128x32 output tile.  It loads the input (and each side input of a binary
-// op) over the tile plus 4 columns and K rows on every side, K = number of 3x3 stages, as
-// 32-bit words into shared memory; each 3x3 stage shrinks the rows it produces by one on
-// each side (the columns keep their 4-pixel margin, enough for K <= 4), element-wise
-// stages update in place.  Pixels inside the chain's valid rectangle read only image
-// pixels, so they equal the per-node kernels' results; pixels outside it are unspecified.
+// A block owns a 128x64 output tile.  It copies the input (and each side input of a binary
+// op) over the tile plus 16 columns and K rows on every side, K = number of 3x3 stages, into
+// shared memory with 16-byte cp.async copies, all in flight at once; each 3x3 stage shrinks
+// the rows it produces by one on each side (the columns keep a margin of at least 4, enough
+// for K <= 4) and runs on 16-bit lanes of 8 pixels per thread; element-wise stages update in
+// place.  Pixels inside the chain's valid rectangle read only image pixels, so they equal
+// the per-node kernels' results; pixels outside it are unspecified.
 // ---------------------------------------------------------------------------------
 namespace {
 
-constexpr int kPxTW = 128, kPxTH = 32, kPxWords = (kPxTW + 8) / 4;   // 34 words: 4-column margins
-constexpr int kPxMaxBH = kPxTH + 2 * AGOCUDA_PX_MAX_STENCILS;
-constexpr int kPxThreads = 256, kPxGroups = kPxThreads / kPxWords;    // 7 row groups of 34 word columns
+constexpr int kPxTW = 128, kPxTH = 64;                  // output tile
+constexpr int kPxWords = (kPxTW + 32) / 4;              // 40 words per buffer row: columns x0-16 .. x0+143
+constexpr int kPxChunks = kPxWords / 4;                 // 16-byte chunks per row
+constexpr int kPxPairs = 18;                            // 3x3 stages compute words 2..37 (columns x0-8 .. x0+135),
+constexpr int kPxThreads = 256, kPxGroups = kPxThreads / kPxPairs;   // 8 pixels per thread; 14 row groups
 
-__device__ __forceinline__ bool px_stencil(int code)
+// 16-bit lane pairs of the 10 columns x-1 .. x+8 around words C0 (x..x+3) and C1 (x+4..x+7):
+// e0 = (x, x+2), o0 = (x+1, x+3), e1 = (x+4, x+6), o1 = (x+5, x+7), b = (x-1, x+8).  The high
+// byte of every lane is `hi`: 0 for integer sums, 0x64 for min / max as half floats (the half
+// with bits 0x64vv is 1024 + vv, exact and ordered like vv).
+struct Lanes8 { uint32_t e0, o0, e1, o1, b; };
+__device__ __forceinline__ Lanes8 lanes8(uint32_t L, uint32_t C0, uint32_t C1, uint32_t R, uint32_t hi)
 {
-    return code == AGOCUDA_PX_BOX3x3 || code == AGOCUDA_PX_MEDIAN3x3 || code == AGOCUDA_PX_DILATE3x3 ||
-           code == AGOCUDA_PX_ERODE3x3 || code == AGOCUDA_PX_GAUSSIAN3x3;
+    Lanes8 v;
+    v.e0 = __byte_perm(C0, hi, 0x4240);
+    v.o0 = __byte_perm(C0, hi, 0x4341);
+    v.e1 = __byte_perm(C1, hi, 0x4240);
+    v.o1 = __byte_perm(C1, hi, 0x4341);
+    v.b = __byte_perm(__byte_perm(L, R, 0x0043), hi, 0x4140);
+    return v;
 }
 
-__device__ __forceinline__ Row3 srow3(const uint32_t (*b)[kPxWords], int r, int w)
+// the neighbour lane pairs of the four outputs: left of e0 = (x-1, x+1), right of o0 =
+// (x+2, x+4), left of e1 = (x+3, x+5), right of o1 = (x+6, x+8)
+__device__ __forceinline__ uint32_t lft_e0(const Lanes8 &v) { return __byte_perm(v.b, v.o0, 0x5410); }
+__device__ __forceinline__ uint32_t rgt_o0(const Lanes8 &v) { return __byte_perm(v.e0, v.e1, 0x5432); }
+__device__ __forceinline__ uint32_t lft_e1(const Lanes8 &v) { return __byte_perm(v.o0, v.o1, 0x5432); }
+__device__ __forceinline__ uint32_t rgt_o1(const Lanes8 &v) { return __byte_perm(v.e1, v.b, 0x7632); }
+
+// low bytes of the four output lane pairs -> words x..x+3, x+4..x+7
+__device__ __forceinline__ uint2 pack8(uint32_t e0, uint32_t o0, uint32_t e1, uint32_t o1)
 {
-    const uint32_t L = b[r][w > 0 ? w - 1 : 0], C = b[r][w], R = b[r][w + 1 < kPxWords ? w + 1 : w];
-    return Row3{__funnelshift_r(L, C, 24), C, __funnelshift_r(C, R, 8)};
+    return make_uint2(__byte_perm(e0, o0, 0x6240), __byte_perm(e1, o1, 0x6240));
 }
 
-// Gaussian 3x3 ([1 2 1]^T [1 2 1]) >> 4 (HafCpu_Gaussian_U8_U8_3x3, ago_haf_cpu_filter.cpp:1518)
-__device__ __forceinline__ Sum3 gsum(const Row3 &r)
+// lane-wise max / min of two f16x2 registers (no NaNs occur: every lane is 1024 + a byte)
+__device__ __forceinline__ uint32_t hmx(uint32_t a, uint32_t b)
 {
-    return Sum3{__byte_perm(r.l, 0, 0x4240) + 2 * __byte_perm(r.c, 0, 0x4240) + __byte_perm(r.r, 0, 0x4240),
-                __byte_perm(r.l, 0, 0x4341) + 2 * __byte_perm(r.c, 0, 0x4341) + __byte_perm(r.r, 0, 0x4341)};
+    uint32_t d;
+    asm("max.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
 }
-
-__device__ __forceinline__ uint32_t gauss_word(const Row3 &a, const Row3 &b, const Row3 &c)
+__device__ __forceinline__ uint32_t hmn(uint32_t a, uint32_t b)
 {
-    const Sum3 A = gsum(a), B = gsum(b), C = gsum(c);
-    const uint32_t e = ((A.E + 2 * B.E + C.E) >> 4) & 0x00ff00ffu, o = ((A.O + 2 * B.O + C.O) >> 4) & 0x00ff00ffu;
-    return e | (o << 8);
+    uint32_t d;
+    asm("min.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
 }
+__device__ __forceinline__ uint32_t hmed3(uint32_t a, uint32_t b, uint32_t c) { return hmx(hmn(a, b), hmn(hmx(a, b), c)); }
 
-__device__ __forceinline__ uint32_t stencil_word(int code, const Row3 &a, const Row3 &b, const Row3 &c)
-{
-    switch (code) {
-    case AGOCUDA_PX_BOX3x3: return box_word(sum3(a), sum3(b), sum3(c));
-    case AGOCUDA_PX_GAUSSIAN3x3: return gauss_word(a, b, c);
-    case AGOCUDA_PX_DILATE3x3:
-        return __vmaxu4(__vmaxu4(__vmaxu4(a.l, a.c), __vmaxu4(a.r, b.l)),
-                        __vmaxu4(__vmaxu4(b.c, b.r), __vmaxu4(__vmaxu4(c.l, c.c), c.r)));
-    case AGOCUDA_PX_ERODE3x3:
-        return __vminu4(__vminu4(__vminu4(a.l, a.c), __vminu4(a.r, b.l)),
-                        __vminu4(__vminu4(b.c, b.r), __vminu4(__vminu4(c.l, c.c), c.r)));
-    default: {   // median
-        uint32_t lL, mL, hL, lC, mC, hC, lR, mR, hR;
-        sort3(a.l, b.l, c.l, lL, mL, hL);
-        sort3(a.c, b.c, c.c, lC, mC, hC);
-        sort3(a.r, b.r, c.r, lR, mR, hR);
-        return med3(__vmaxu4(__vmaxu4(lL, lC), lR), med3(mL, mC, mR), __vminu4(__vminu4(hL, hC), hR));
+// Row sources / sinks of the 3x3 stages: 8 pixels (word pair p) of a shared-memory tile
+// row, or of an image row in global memory
+struct SmemRows {
+    const uint32_t *buf;
+    int p;
+    __device__ __forceinline__ Lanes8 row(int r, uint32_t hi) const
+    {
+        const uint32_t *w = buf + r * kPxWords + 2 * p;   // words 2 .. 37: the neighbour words exist
+        return lanes8(w[-1], w[0], w[1], w[2], hi);
     }
+};
+struct SmemOut {
+    uint32_t *buf;
+    int p;
+    __device__ __forceinline__ void put(int r, uint2 v) const { *reinterpret_cast<uint2 *>(buf + r * kPxWords + 2 * p) = v; }
+};
+struct GlobalRows {
+    const uint8_t *src;
+    int stride, x;
+    __device__ __forceinline__ Lanes8 row(int r, uint32_t hi) const
+    {
+        const uint8_t *q = src + (size_t)r * stride;
+        return lanes8(load_word_clamped(q, x - 4, stride), load_word_clamped(q, x, stride),
+                      load_word_clamped(q, x + 4, stride), load_word_clamped(q, x + 8, stride), hi);
+    }
+};
+struct GlobalOut {
+    uint8_t *dst;
+    int stride, x, W;
+    __device__ __forceinline__ void put(int r, uint2 v) const
+    {
+        uint8_t *d = dst + (size_t)r * stride + x;
+        if (x + 8 <= W) {
+            *reinterpret_cast<uint32_t *>(d) = v.x;
+            *reinterpret_cast<uint32_t *>(d + 4) = v.y;
+        } else {
+            for (int j = 0; j < W - x; j++) d[j] = (uint8_t)((j < 4 ? v.x : v.y) >> (8 * (j & 3)));
+        }
+    }
+};
+
+// Dilate (max) / Erode (min) over rows [r0, r1): column extreme of three rows, then across
+template <bool MAX, class In, class Out>
+__device__ __forceinline__ void stage_minmax(const In &in, const Out &out, int r0, int r1)
+{
+    auto f = [](uint32_t a, uint32_t b) { return MAX ? hmx(a, b) : hmn(a, b); };
+    const uint32_t hi = 0x64646464u;
+    Lanes8 a = in.row(r0 - 1, hi), b = in.row(r0, hi);
+    Lanes8 pr{f(a.e0, b.e0), f(a.o0, b.o0), f(a.e1, b.e1), f(a.o1, b.o1), f(a.b, b.b)};   // rows r-1, r
+    for (int r = r0; r < r1; r++) {
+        const Lanes8 c = in.row(r + 1, hi);
+        const Lanes8 v{f(pr.e0, c.e0), f(pr.o0, c.o0), f(pr.e1, c.e1), f(pr.o1, c.o1), f(pr.b, c.b)};
+        out.put(r, pack8(f(f(lft_e0(v), v.e0), v.o0), f(f(v.e0, v.o0), rgt_o0(v)),
+                                f(f(lft_e1(v), v.e1), v.o1), f(f(v.e1, v.o1), rgt_o1(v))));
+        pr = Lanes8{f(b.e0, c.e0), f(b.o0, c.o0), f(b.e1, c.e1), f(b.o1, c.o1), f(b.b, c.b)};
+        b = c;
+    }
+}
+
+// Median: sort each column of the three rows, then med3(max of minima, med3 of medians,
+// min of maxima) over the three columns of each output
+template <class In, class Out>
+__device__ __forceinline__ void stage_median(const In &in, const Out &out, int r0, int r1)
+{
+    const uint32_t hi = 0x64646464u;
+    Lanes8 a = in.row(r0 - 1, hi), b = in.row(r0, hi);
+    for (int r = r0; r < r1; r++) {
+        const Lanes8 c = in.row(r + 1, hi);
+        Lanes8 lo, md, hg;
+        auto sort = [](uint32_t x, uint32_t y, uint32_t z, uint32_t &l, uint32_t &m, uint32_t &h) {
+            const uint32_t l1 = hmn(x, y), h1 = hmx(x, y), t = hmx(l1, z);
+            l = hmn(l1, z);
+            m = hmn(h1, t);
+            h = hmx(h1, t);
+        };
+        sort(a.e0, b.e0, c.e0, lo.e0, md.e0, hg.e0);
+        sort(a.o0, b.o0, c.o0, lo.o0, md.o0, hg.o0);
+        sort(a.e1, b.e1, c.e1, lo.e1, md.e1, hg.e1);
+        sort(a.o1, b.o1, c.o1, lo.o1, md.o1, hg.o1);
+        sort(a.b, b.b, c.b, lo.b, md.b, hg.b);
+        auto med9 = [&](uint32_t l0, uint32_t l1, uint32_t l2, uint32_t m0, uint32_t m1, uint32_t m2, uint32_t h0,
+                        uint32_t h1, uint32_t h2) {
+            return hmed3(hmx(hmx(l0, l1), l2), hmed3(m0, m1, m2), hmn(hmn(h0, h1), h2));
+        };
+        const uint32_t oe0 = med9(lft_e0(lo), lo.e0, lo.o0, lft_e0(md), md.e0, md.o0, lft_e0(hg), hg.e0, hg.o0);
+        const uint32_t oo0 = med9(lo.e0, lo.o0, rgt_o0(lo), md.e0, md.o0, rgt_o0(md), hg.e0, hg.o0, rgt_o0(hg));
+        const uint32_t oe1 = med9(lft_e1(lo), lo.e1, lo.o1, lft_e1(md), md.e1, md.o1, lft_e1(hg), hg.e1, hg.o1);
+        const uint32_t oo1 = med9(lo.e1, lo.o1, rgt_o1(lo), md.e1, md.o1, rgt_o1(md), hg.e1, hg.o1, rgt_o1(hg));
+        out.put(r, pack8(oe0, oo0, oe1, oo1));
+        a = b;
+        b = c;
+    }
+}
+
+// Box and Gaussian ([1 2 1]^T [1 2 1] >> 4) in integer lanes: row sums of three columns,
+// rolled down the rows.  Box is floor(sum / 9): the reference's SIMD body computes
+// (sum * 7282) >> 16 and its scalar parts (int)((float)sum / 9.0f) (HafCpu_Box_U8_U8_3x3,
+// ago_haf_cpu_filter.cpp:34); both equal floor(sum / 9) for every sum of nine bytes (<= 2295),
+// and so does (sum * 7282) >> 16 here.
+template <bool GAUSS, class In, class Out>
+__device__ __forceinline__ void stage_linear(const In &in, const Out &out, int r0, int r1)
+{
+    auto hsum = [](const Lanes8 &v) {
+        const uint32_t k = GAUSS ? 2u : 1u;
+        return Lanes8{lft_e0(v) + k * v.e0 + v.o0, v.e0 + k * v.o0 + rgt_o0(v), lft_e1(v) + k * v.e1 + v.o1,
+                      v.e1 + k * v.o1 + rgt_o1(v), 0u};
+    };
+    Lanes8 ha = hsum(in.row(r0 - 1, 0u)), hb = hsum(in.row(r0, 0u));
+    for (int r = r0; r < r1; r++) {
+        const Lanes8 hc = hsum(in.row(r + 1, 0u));
+        uint32_t q[4];
+        const uint32_t s[4] = {ha.e0 + (GAUSS ? 2u : 1u) * hb.e0 + hc.e0, ha.o0 + (GAUSS ? 2u : 1u) * hb.o0 + hc.o0,
+                               ha.e1 + (GAUSS ? 2u : 1u) * hb.e1 + hc.e1, ha.o1 + (GAUSS ? 2u : 1u) * hb.o1 + hc.o1};
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            q[i] = GAUSS ? (s[i] >> 4) & 0x00ff00ffu
+                         : ((((s[i] & 0xffffu) * 7282u) >> 16) | ((((s[i] >> 16) * 7282u) >> 16) << 16));
+        out.put(r, pack8(q[0], q[1], q[2], q[3]));
+        ha = hb;
+        hb = hc;
     }
 }
 
 // element-wise op on 4 pixels: v = the chain's value, o = the side operand
-__device__ __forceinline__ uint32_t ew_word(const agocuda_pixel_op &op, uint32_t v, uint32_t o)
+__device__ __forceinline__ uint32_t ew_word(int code, int sideFirst, int p0, int p1, uint32_t v, uint32_t o)
 {
-    const uint32_t a = op.sideFirst ? o : v, b = op.sideFirst ? v : o;
-    switch (op.code) {
+    const uint32_t a = sideFirst ? o : v, b = sideFirst ? v : o;
+    switch (code) {
     case AGOCUDA_PX_NOT: return ~v;
     case AGOCUDA_PX_AND: return v & o;
     case AGOCUDA_PX_OR: return v | o;
@@ -391,67 +383,85 @@ __device__ __forceinline__ uint32_t ew_word(const agocuda_pixel_op &op, uint32_t
     case AGOCUDA_PX_ADD_SAT: return __vaddus4(v, o);
     case AGOCUDA_PX_SUB_WRAP: return __vsub4(a, b);
     case AGOCUDA_PX_SUB_SAT: return __vsubus4(a, b);
-    case AGOCUDA_PX_THRESHOLD_BINARY: return __vcmpgtu4(v, (uint32_t)(op.p0 & 0xff) * 0x01010101u);
+    case AGOCUDA_PX_THRESHOLD_BINARY: return __vcmpgtu4(v, (uint32_t)(p0 & 0xff) * 0x01010101u);
     case AGOCUDA_PX_THRESHOLD_RANGE:
-        return ~(__vcmpgtu4(v, (uint32_t)(op.p1 & 0xff) * 0x01010101u) | __vcmpltu4(v, (uint32_t)(op.p0 & 0xff) * 0x01010101u));
+        return ~(__vcmpgtu4(v, (uint32_t)(p1 & 0xff) * 0x01010101u) | __vcmpltu4(v, (uint32_t)(p0 & 0xff) * 0x01010101u));
     }
     return v;
 }
 
+// dynamic shared memory: two buffers of BH x 40 words, then one per side input
 __global__ void __launch_bounds__(kPxThreads)
 k_pixel_chain(const agocuda_pixel_program prog, const agocuda_pixel_frame *__restrict__ frames, int K, int nSides)
 {
-    __shared__ uint32_t buf[2][kPxMaxBH][kPxWords];
-    __shared__ uint32_t side[AGOCUDA_PX_MAX_SIDES][kPxMaxBH][kPxWords];
+    extern __shared__ uint32_t smem[];
+    __shared__ int4 sop[AGOCUDA_PX_MAX_OPS];            // code, side, sideFirst, p0 | p1 << 16
     const agocuda_pixel_frame f = frames[blockIdx.z];
     const int W = (int)f.width, H = (int)f.height;
     const int x0 = blockIdx.x * kPxTW, y0 = blockIdx.y * kPxTH, tid = threadIdx.x;
     if (x0 >= W || y0 >= H) return;
-    const int BH = kPxTH + 2 * K;
-    for (int i = tid; i < BH * kPxWords; i += kPxThreads) {
-        const int r = i / kPxWords, w = i - r * kPxWords;
-        const int y = clampi(y0 - K + r, 0, H - 1), x = x0 - 4 + 4 * w;
-        buf[0][r][w] = load_word_clamped(f.src + (size_t)y * f.srcStride, x, (int)f.srcStride);
-        for (int s = 0; s < nSides; s++)
-            side[s][r][w] = load_word_clamped(f.side[s] + (size_t)y * f.sideStride[s], x, (int)f.sideStride[s]);
+    const int BH = kPxTH + 2 * K, plane = BH * kPxWords;
+    uint32_t *const buf0 = smem, *const buf1 = smem + plane;
+    uint32_t *const side = smem + 2 * plane;
+    if (tid < prog.numOps) {
+        const agocuda_pixel_op &o = prog.ops[tid];
+        sop[tid] = make_int4(o.code, o.side, o.sideFirst, (o.p0 & 0xffff) | (o.p1 << 16));
     }
+    // every 16-byte chunk of every plane in flight at once (cp.async, global -> shared); a
+    // chunk outside the row is read from inside it instead (its columns are outside the image)
+    for (int s = -1; s < nSides; s++) {
+        const agocuda_pixel_frame *fp = frames + blockIdx.z;   // side[s]: indexed in global memory
+        const uint8_t *base = s < 0 ? f.src : fp->side[s];
+        const int stride = (int)(s < 0 ? f.srcStride : fp->sideStride[s]);
+        uint32_t *dst = s < 0 ? buf0 : side + s * plane;
+        for (int i = tid; i < BH * kPxChunks; i += kPxThreads) {
+            const int r = i / kPxChunks, c = i - r * kPxChunks;
+            const int y = clampi(y0 - K + r, 0, H - 1), x = clampi(x0 - 16 + 16 * c, 0, stride - 16);
+            const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + r * kPxWords + 4 * c);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(base + (size_t)y * stride + x) : "memory");
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     int cur = 0, st = 0;
+    const int pp = 1 + tid % kPxPairs, grp = tid / kPxPairs;
     for (int k = 0; k < prog.numOps; k++) {
-        const agocuda_pixel_op op = prog.ops[k];
-        if (px_stencil(op.code)) {
+        const int4 op = sop[k];
+        const int code = op.x;
+        if (code >= AGOCUDA_PX_BOX3x3) {
             st++;
-            // rows [st, BH - st) from rows [st - 1, BH - st + 1): a word column per thread,
-            // its rows split over the row groups, the three rows of the window in registers
+            // rows [st, BH - st) from rows [st - 1, BH - st + 1): 8 pixels of a row per thread,
+            // the rows split over the row groups
             const int rows = BH - 2 * st, per = (rows + kPxGroups - 1) / kPxGroups;
-            const int w = tid % kPxWords, grp = tid / kPxWords;
             const int r0 = st + grp * per, r1 = min(r0 + per, BH - st);
             if (grp < kPxGroups && r0 < r1) {
-                Row3 a = srow3(buf[cur], r0 - 1, w), b = srow3(buf[cur], r0, w);
-                for (int r = r0; r < r1; r++) {
-                    const Row3 c = srow3(buf[cur], r + 1, w);
-                    buf[cur ^ 1][r][w] = stencil_word(op.code, a, b, c);
-                    a = b;
-                    b = c;
+                const SmemRows in{cur ? buf1 : buf0, pp};
+                const SmemOut out{cur ? buf0 : buf1, pp};
+                switch (code) {
+                case AGOCUDA_PX_DILATE3x3: stage_minmax<true>(in, out, r0, r1); break;
+                case AGOCUDA_PX_ERODE3x3: stage_minmax<false>(in, out, r0, r1); break;
+                case AGOCUDA_PX_MEDIAN3x3: stage_median(in, out, r0, r1); break;
+                case AGOCUDA_PX_GAUSSIAN3x3: stage_linear<true>(in, out, r0, r1); break;
+                default: stage_linear<false>(in, out, r0, r1); break;
                 }
             }
             cur ^= 1;
         } else {
+            const int sd = op.y, sf = op.z, p0 = op.w & 0xffff, p1 = op.w >> 16;
             const int rows = BH - 2 * st;
-            for (int i = tid; i < rows * kPxWords; i += kPxThreads) {
-                const int r = st + i / kPxWords, w = i % kPxWords;
-                const uint32_t o = op.side >= 0 ? side[op.side][r][w] : 0u;
-                buf[cur][r][w] = ew_word(op, buf[cur][r][w], o);
-            }
+            uint32_t *b = (cur ? buf1 : buf0) + st * kPxWords;
+            const uint32_t *o = sd >= 0 ? side + sd * plane + st * kPxWords : nullptr;
+            for (int i = tid; i < rows * kPxWords; i += kPxThreads) b[i] = ew_word(code, sf, p0, p1, b[i], o ? o[i] : 0u);
         }
         __syncthreads();
     }
-    // tile rows [K, K + 32) of the buffer, words 1..32 (columns x0 .. x0 + 127)
+    // tile rows [K, K + 64) of the buffer, words 4..35 (columns x0 .. x0 + 127)
+    const uint32_t *res = cur ? buf1 : buf0;
     for (int i = tid; i < kPxTH * (kPxTW / 4); i += kPxThreads) {
         const int r = i / (kPxTW / 4), w = i % (kPxTW / 4);
         const int y = y0 + r, x = x0 + 4 * w;
         if (y >= H || x >= W) continue;
-        const uint32_t v = buf[cur][K + r][w + 1];
+        const uint32_t v = res[(K + r) * kPxWords + w + 4];
         uint8_t *d = f.dst + (size_t)y * f.dstStride + x;
         if (x + 4 <= W) {
             *(uint32_t *)d = v;
@@ -491,7 +501,67 @@ extern "C" int agocuda_fused_PixelChain_U8(void *stream, const agocuda_pixel_pro
         if (!(c >= AGOCUDA_PX_AND && c <= AGOCUDA_PX_SUB_SAT)) p.ops[k].side = -1;
     }
     dim3 grd(div_up(maxWidth, kPxTW), div_up(maxHeight, kPxTH), numFrames);
-    k_pixel_chain<<<grd, kPxThreads, 0, as_stream(stream)>>>(p, frames, K, nSides);
+    const size_t smem = (size_t)(2 + nSides) * (kPxTH + 2 * K) * kPxWords * sizeof(uint32_t);
+    static std::once_flag once;
+    std::call_once(once, [] {   // up to 5 planes of 72 x 40 words: above the 48 KB default
+        cudaFuncSetAttribute(k_pixel_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (2 + AGOCUDA_PX_MAX_SIDES) * (kPxTH + 2 * AGOCUDA_PX_MAX_STENCILS) * kPxWords * 4);
+    });
+    k_pixel_chain<<<grd, kPxThreads, smem, as_stream(stream)>>>(p, frames, K, nSides);
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }
+
+// ---------------------------------------------------------------------------------
+// 3x3 filters on U8 (ago_haf_cpu_filter.cpp) as per-node kernels: the pixel-chain stages on
+// image rows in global memory; interior rows [1, H-1), every column.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr int kFBX = 32, kFBY = 4, kFRows = 16;   // 8 pixels x 16 rows per thread
+
+template <int OP>
+__global__ void __launch_bounds__(kFBX * kFBY)
+k_filter3x3(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride)
+{
+    const int x = (blockIdx.x * kFBX + threadIdx.x) * 8;
+    const int y0 = 1 + (blockIdx.y * kFBY + threadIdx.y) * kFRows;
+    if (x >= W || y0 >= H - 1) return;
+    const int y1 = min(y0 + kFRows, H - 1);
+    const GlobalRows in{src, srcStride, x};
+    const GlobalOut out{dst, dstStride, x, W};
+    switch (OP) {
+    case AGOCUDA_PX_DILATE3x3: stage_minmax<true>(in, out, y0, y1); break;
+    case AGOCUDA_PX_ERODE3x3: stage_minmax<false>(in, out, y0, y1); break;
+    case AGOCUDA_PX_MEDIAN3x3: stage_median(in, out, y0, y1); break;
+    case AGOCUDA_PX_GAUSSIAN3x3: stage_linear<true>(in, out, y0, y1); break;
+    default: stage_linear<false>(in, out, y0, y1); break;   // box
+    }
+}
+
+template <int OP>
+int filter_launch(void *stream, uint32_t W, uint32_t H, uint8_t *dst, uint32_t dstStride, const uint8_t *src,
+                  uint32_t srcStride)
+{
+    auto ok = [&](const uint8_t *p, uint32_t s) { return p && ((uintptr_t)p & 3) == 0 && (s & 3) == 0 && s >= W; };
+    if (W < 3 || H < 3 || !ok(dst, dstStride) || !ok(src, srcStride)) return AGOCUDA_INVALID_PARAMS;
+    dim3 grd(div_up(W, kFBX * 8), div_up(H - 2, kFBY * kFRows));
+    k_filter3x3<OP><<<grd, dim3(kFBX, kFBY), 0, as_stream(stream)>>>((int)W, (int)H, dst, (int)dstStride, src, (int)srcStride);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+}  // namespace
+
+#define FILTER(NAME, OP)                                                                                          \
+    extern "C" int agocuda_##NAME(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride, \
+                                  const uint8_t *pSrc, uint32_t srcStride)                                        \
+    {                                                                                                          \
+        return filter_launch<OP>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc, srcStride);                \
+    }
+FILTER(Gaussian_U8_U8_3x3, AGOCUDA_PX_GAUSSIAN3x3)   // HafCpu_Gaussian_U8_U8_3x3 (ago_haf_cpu_filter.cpp:1518)
+FILTER(Box_U8_U8_3x3, AGOCUDA_PX_BOX3x3)
+FILTER(Dilate_U8_U8_3x3, AGOCUDA_PX_DILATE3x3)
+FILTER(Erode_U8_U8_3x3, AGOCUDA_PX_ERODE3x3)
+FILTER(Median_U8_U8_3x3, AGOCUDA_PX_MEDIAN3x3)
+#undef FILTER
