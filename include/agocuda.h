@@ -77,8 +77,9 @@ int agocuda_ColorDepth_U8_S16_Sat(void *stream, uint32_t dstWidth, uint32_t dstH
                                   uint8_t *pDst, uint32_t dstStride,
                                   const int16_t *pSrc, uint32_t srcStride, int32_t shift);
 
-/* v > threshold ? 255 : 0.  Replaces HipExec_Threshold_U8_U8_Binary
- * (hipvx/hip_host_decls.h:689); HafCpu_Threshold_U8_U8_Binary (ago_haf_cpu_arithmetic.cpp:3660). */
+/* v > threshold ? 255 : 0 (threshold as vx_uint8).  Replaces HipExec_Threshold_U8_U8_Binary
+ * (hipvx/hip_host_decls.h:689); HafCpu_Threshold_U8_U8_Binary (ago_haf_cpu_arithmetic.cpp:3660).
+ * Planes as for the element-wise kernels below (16-byte aligned rows). */
 int agocuda_Threshold_U8_U8_Binary(void *stream, uint32_t dstWidth, uint32_t dstHeight,
                                    uint8_t *pDst, uint32_t dstStride,
                                    const uint8_t *pSrc, uint32_t srcStride, int32_t threshold);

@@ -173,18 +173,6 @@ __global__ void k_colordepth_u8_s16_sat(int W, int H, uint8_t *dst, int dstStrid
     *(uint32_t *)(dst + (size_t)y * dstStride + x) = pack4(v[0], v[1], v[2], v[3]);
 }
 
-__global__ void k_threshold_u8_binary(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride, int thr)
-{
-    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= W || y >= H) return;
-    uint32_t a = ldg_u32(src + (size_t)y * srcStride + x);
-    int o[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) o[i] = byte_of(a, i) > thr ? 255 : 0;
-    *(uint32_t *)(dst + (size_t)y * dstStride + x) = pack4(o[0], o[1], o[2], o[3]);
-}
-
 // ---------------------------------------------------------------------------------
 // Fused Gaussian3x3 -> SobelMagnitude -> ColorDepth(SAT, shift) -> Threshold(BINARY, t).
 // ColorDepth and Threshold collapse into one comparison on n = gx^2 + gy^2: with
@@ -406,19 +394,6 @@ extern "C" int agocuda_ColorDepth_U8_S16_Sat(void *stream, uint32_t W, uint32_t 
     dim3 blk(32, 8);
     dim3 grd(div_up(W, 128), div_up(H, 8));
     k_colordepth_u8_s16_sat<<<grd, blk, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride, shift);
-    agocuda_count_launch(1);
-    return agocuda_launch_status();
-}
-
-extern "C" int agocuda_Threshold_U8_U8_Binary(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
-                                              const uint8_t *pSrc, uint32_t srcStride, int32_t threshold)
-{
-    if (!W || !H || bad_plane(pDst, dstStride, W, 1, 4) || bad_plane(pSrc, srcStride, W, 1, 4))
-        return AGOCUDA_INVALID_PARAMS;
-    dim3 blk(32, 8);
-    dim3 grd(div_up(W, 128), div_up(H, 8));
-    // The reference passes the threshold as vx_uint8 (threshold_value.U1).
-    k_threshold_u8_binary<<<grd, blk, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride, (int)(uint8_t)threshold);
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }

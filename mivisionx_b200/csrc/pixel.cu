@@ -26,6 +26,7 @@ enum EwOp : int {
     EW_ABSDIFF_U8, EW_ABSDIFF_SAT_S16,
     EW_AND, EW_OR, EW_XOR, EW_NOT,
     EW_RANGE,                                    // 255 inside [lower, upper], else 0
+    EW_BINARY,                                   // 255 above the threshold, else 0
 };
 
 __device__ __forceinline__ int sat_s16(int v) { return v < -32768 ? -32768 : (v > 32767 ? 32767 : v); }
@@ -51,6 +52,7 @@ __device__ __forceinline__ int ew_apply(int a, int b, int p0, int p1)
     case EW_XOR: return a ^ b;
     case EW_NOT: return ~a & 0xff;
     case EW_RANGE: return (a > p1 || a < p0) ? 0 : 255;                // :3742
+    case EW_BINARY: return a > p0 ? 255 : 0;                           // :3660
     }
     return 0;
 }
@@ -116,7 +118,7 @@ template <int OP, typename TO, typename TA, typename TB>
 int ew_launch(void *stream, uint32_t W, uint32_t H, TO *dst, uint32_t dstStride, const TA *a, uint32_t aStride,
               const TB *b, uint32_t bStride, int p0 = 0, int p1 = 0)
 {
-    const bool unary = OP == EW_NOT || OP == EW_RANGE;
+    const bool unary = OP == EW_NOT || OP == EW_RANGE || OP == EW_BINARY;
     if (!W || !H || !ew_plane_ok(dst, dstStride, W) || !ew_plane_ok(a, aStride, W) ||
         (!unary && !ew_plane_ok(b, bStride, W)))
         return AGOCUDA_INVALID_PARAMS;
@@ -166,6 +168,14 @@ extern "C" int agocuda_Not_U8_U8(void *stream, uint32_t dstWidth, uint32_t dstHe
                                  const uint8_t *pSrc, uint32_t srcStride)
 {
     return ew_launch<EW_NOT>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc, srcStride, (const uint8_t *)nullptr, 0);
+}
+
+extern "C" int agocuda_Threshold_U8_U8_Binary(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                              uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride, int32_t threshold)
+{
+    // the reference passes the threshold as vx_uint8 (threshold_value.U1, ago_kernel_api.cpp:3442)
+    return ew_launch<EW_BINARY>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc, srcStride, (const uint8_t *)nullptr, 0,
+                                (int)(uint8_t)threshold);
 }
 
 extern "C" int agocuda_Threshold_U8_U8_Range(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
