@@ -524,6 +524,14 @@ int agocuda_Xor_U8_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uin
 int agocuda_Not_U8_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
                       const uint8_t *pSrc, uint32_t srcStride);
 
+/* ConvertDepth WRAP: low byte of (v >> shift) (arithmetic shift); and U8 -> S16: v << shift
+ * kept to 16 bits.  Replace HipExec_ColorDepth_U8_S16_Wrap (hip_host_decls.h:398) and
+ * HipExec_ColorDepth_S16_U8 (:408); ago_haf_cpu_arithmetic.cpp:3488, :3604.  shift 0..15. */
+int agocuda_ColorDepth_U8_S16_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                   uint32_t dstStride, const int16_t *pSrc, uint32_t srcStride, int32_t shift);
+int agocuda_ColorDepth_S16_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                              const uint8_t *pSrc, uint32_t srcStride, int32_t shift);
+
 /* 255 where lower <= v <= upper, else 0 (bounds taken as vx_uint8).  Replaces
  * HipExec_Threshold_U8_U8_Range (hip_host_decls.h:694); HafCpu_Threshold_U8_U8_Range
  * (ago_haf_cpu_arithmetic.cpp:3742). */
@@ -552,6 +560,58 @@ int agocuda_Erode_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight,
  * HafCpu_Median_U8_U8_3x3 (ago_haf_cpu_filter.cpp:3842). */
 int agocuda_Median_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
                              const uint8_t *pSrc, uint32_t srcStride);
+
+/* ------------------------------------------------------------------------------------ */
+/* Channel extract / combine (reference: hipvx/hip_host_decls.h:413-492; CPU semantics    */
+/* ago/ago_haf_cpu_ch_extract_combine.cpp).  Row bases 4-byte aligned, strides multiples  */
+/* of 4.                                                                                   */
+/* ------------------------------------------------------------------------------------ */
+
+/* dst[x] = src[x * n + k] for the n-byte units of an interleaved plane (U16: NV12/NV21 UV
+ * plane, YUYV/UYVY luma; U24: RGB; U32: RGBX, or YUYV/UYVY chroma over pixel pairs);
+ * dstWidth counts output pixels.  Replace HipExec_ChannelExtract_U8_U16_Pos0 .. _U8_U32_Pos3
+ * (hip_host_decls.h:413-448). */
+int agocuda_ChannelExtract_U8_U16_Pos0(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ChannelExtract_U8_U16_Pos1(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ChannelExtract_U8_U24_Pos0(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ChannelExtract_U8_U24_Pos1(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ChannelExtract_U8_U24_Pos2(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ChannelExtract_U8_U32_Pos0(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ChannelExtract_U8_U32_Pos1(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ChannelExtract_U8_U32_Pos2(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_ChannelExtract_U8_U32_Pos3(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                       uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+/* Interleave U8 planes: UV (NV12 chroma), RGB, RGBX, and UYVY / YUYV from Y (full width) +
+ * U, V (half width), dstWidth in pixels.  Replace HipExec_ChannelCombine_U16_U8U8 (:465),
+ * _U24_U8U8U8_RGB (:470), _U32_U8U8U8_UYVY (:476), _U32_U8U8U8_YUYV (:482),
+ * _U32_U8U8U8U8_RGBX (:488). */
+int agocuda_ChannelCombine_U16_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                    uint32_t dstStride, const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2,
+                                    uint32_t src2Stride);
+int agocuda_ChannelCombine_U24_U8U8U8_RGB(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                          uint32_t dstStride, const uint8_t *pSrc1, uint32_t src1Stride,
+                                          const uint8_t *pSrc2, uint32_t src2Stride, const uint8_t *pSrc3,
+                                          uint32_t src3Stride);
+int agocuda_ChannelCombine_U32_U8U8U8_UYVY(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                           uint32_t dstStride, const uint8_t *pSrc1, uint32_t src1Stride,
+                                           const uint8_t *pSrc2, uint32_t src2Stride, const uint8_t *pSrc3,
+                                           uint32_t src3Stride);
+int agocuda_ChannelCombine_U32_U8U8U8_YUYV(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                           uint32_t dstStride, const uint8_t *pSrc1, uint32_t src1Stride,
+                                           const uint8_t *pSrc2, uint32_t src2Stride, const uint8_t *pSrc3,
+                                           uint32_t src3Stride);
+int agocuda_ChannelCombine_U32_U8U8U8U8_RGBX(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                             uint32_t dstStride, const uint8_t *pSrc1, uint32_t src1Stride,
+                                             const uint8_t *pSrc2, uint32_t src2Stride, const uint8_t *pSrc3,
+                                             uint32_t src3Stride, const uint8_t *pSrc4, uint32_t src4Stride);
 
 /* ------------------------------------------------------------------------------------ */
 /* Fused U8 pixel chains: element-wise and 3x3 kernels through on-chip intermediates.    */

@@ -382,6 +382,8 @@ vx_node vxAndNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
 vx_node vxOrNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
 vx_node vxXorNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
 vx_node vxNotNode(vx_graph graph, vx_image input, vx_image output);
+vx_node vxChannelCombineNode(vx_graph graph, vx_image plane0, vx_image plane1, vx_image plane2, vx_image plane3,
+                             vx_image output);
 
 #ifdef __cplusplus
 }

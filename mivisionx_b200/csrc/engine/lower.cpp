@@ -36,6 +36,10 @@ static const char *kLKNames[] = {
     "Sub_U8_U8U8_Wrap", "Sub_U8_U8U8_Sat", "Sub_S16_U8U8", "Sub_S16_S16U8_Wrap", "Sub_S16_S16U8_Sat",
     "Sub_S16_U8S16_Wrap", "Sub_S16_U8S16_Sat", "Sub_S16_S16S16_Wrap", "Sub_S16_S16S16_Sat",
     "And_U8_U8U8", "Or_U8_U8U8", "Xor_U8_U8U8", "Not_U8_U8", "Threshold_U8_U8_Range",
+    "ChannelExtract_U8_U16_Pos0", "ChannelExtract_U8_U16_Pos1", "ChannelExtract_U8_U24_Pos0", "ChannelExtract_U8_U24_Pos1",
+    "ChannelExtract_U8_U24_Pos2", "ChannelExtract_U8_U32_Pos0", "ChannelExtract_U8_U32_Pos1", "ChannelExtract_U8_U32_Pos2",
+    "ChannelExtract_U8_U32_Pos3", "ChannelCombine_U16_U8U8", "ChannelCombine_U24_U8U8U8_RGB",
+    "ChannelCombine_U32_U8U8U8_UYVY", "ChannelCombine_U32_U8U8U8_YUYV", "ChannelCombine_U32_U8U8U8U8_RGBX",
 };
 static_assert(sizeof(kLKNames) / sizeof(kLKNames[0]) == (size_t)LK::COUNT, "kernel name table");
 
@@ -60,6 +64,18 @@ static vx_status set_meta(Image *out, uint32_t w, uint32_t h, vx_df_image f)
     if (out->format != f) return VX_ERROR_INVALID_FORMAT;
     if (out->width != w || out->height != h) return VX_ERROR_INVALID_DIMENSION;
     return VX_SUCCESS;
+}
+
+// agoChannelEnum2Index: R / Y / channel 0 -> 0, G / U / 1 -> 1, B / V / 2 -> 2, A / 3 -> 3
+static int channel_index(vx_enum ch)
+{
+    switch (ch) {
+    case VX_CHANNEL_0: case VX_CHANNEL_R: case VX_CHANNEL_Y: return 0;
+    case VX_CHANNEL_1: case VX_CHANNEL_G: case VX_CHANNEL_U: return 1;
+    case VX_CHANNEL_2: case VX_CHANNEL_B: case VX_CHANNEL_V: return 2;
+    case VX_CHANNEL_3: case VX_CHANNEL_A: return 3;
+    default: return -1;
+    }
 }
 
 static bool fmt_is(Ref *r, vx_df_image f) { return r && r->type == VX_TYPE_IMAGE && IMG(r)->format == f && IMG(r)->num_planes; }
@@ -150,16 +166,38 @@ vx_status validate_node(Graph *g, Node *n)
         if (o->format != VX_DF_IMAGE_NV12 && o->format != VX_DF_IMAGE_IYUV) return VX_ERROR_NOT_SUPPORTED;
         return set_meta(o, i0->width, i0->height, o->format);
     }
-    case VX_KERNEL_CHANNEL_EXTRACT: {
+    case VX_KERNEL_CHANNEL_EXTRACT: {                   // ovxKernel_ChannelExtract (ago_kernel_api.cpp)
         Image *i0 = img(0), *o = img(2);
         if (!i0 || !i0->num_planes) return VX_ERROR_INVALID_PARAMETERS;
-        vx_enum ch = sc_enum(p[1]);
-        int plane = -1;
-        if ((i0->format == VX_DF_IMAGE_NV12 || i0->format == VX_DF_IMAGE_IYUV || i0->format == VX_DF_IMAGE_YUV4) && ch == VX_CHANNEL_Y) plane = 0;
-        if ((i0->format == VX_DF_IMAGE_IYUV || i0->format == VX_DF_IMAGE_YUV4) && ch == VX_CHANNEL_U) plane = 1;
-        if ((i0->format == VX_DF_IMAGE_IYUV || i0->format == VX_DF_IMAGE_YUV4) && ch == VX_CHANNEL_V) plane = 2;
-        if (plane < 0) return VX_ERROR_NOT_SUPPORTED;
-        return set_meta(o, i0->planes[plane].width, i0->planes[plane].height, VX_DF_IMAGE_U8);
+        const vx_df_image f = i0->format;
+        if (f != VX_DF_IMAGE_RGB && f != VX_DF_IMAGE_RGBX && f != VX_DF_IMAGE_NV12 && f != VX_DF_IMAGE_NV21 &&
+            f != VX_DF_IMAGE_IYUV && f != VX_DF_IMAGE_YUYV && f != VX_DF_IMAGE_UYVY && f != VX_DF_IMAGE_YUV4)
+            return VX_ERROR_INVALID_FORMAT;
+        if ((i0->width & 1) || (i0->height & 1)) return VX_ERROR_INVALID_DIMENSION;
+        const int idx = channel_index(sc_enum(p[1]));
+        if (!is_valid(p[1], VX_TYPE_SCALAR) || idx < 0 || idx > (f == VX_DF_IMAGE_RGBX ? 3 : 2)) return VX_ERROR_INVALID_VALUE;
+        uint32_t w = i0->width, h = i0->height;
+        if (idx > 0 && (f == VX_DF_IMAGE_NV12 || f == VX_DF_IMAGE_NV21 || f == VX_DF_IMAGE_IYUV)) { w >>= 1; h >>= 1; }
+        if (idx > 0 && (f == VX_DF_IMAGE_YUYV || f == VX_DF_IMAGE_UYVY)) w >>= 1;
+        return set_meta(o, w, h, VX_DF_IMAGE_U8);
+    }
+    case VX_KERNEL_CHANNEL_COMBINE: {                   // ovxKernel_ChannelCombine (ago_kernel_api.cpp)
+        Image *o = img(4);
+        if (!o || o->format == VX_DF_IMAGE_VIRT) return VX_ERROR_INVALID_FORMAT;
+        const vx_df_image f = o->format;
+        int sx = 0, sy = 0;
+        if (f == VX_DF_IMAGE_IYUV || f == VX_DF_IMAGE_NV12 || f == VX_DF_IMAGE_NV21) sx = sy = 1;
+        else if (f == VX_DF_IMAGE_YUYV || f == VX_DF_IMAGE_UYVY) sx = 1;
+        else if (f != VX_DF_IMAGE_RGB && f != VX_DF_IMAGE_RGBX && f != VX_DF_IMAGE_YUV4) return VX_ERROR_INVALID_FORMAT;
+        const int planes = 2 + (img(2) ? 1 : 0) + (img(2) && img(3) ? 1 : 0);
+        if ((!img(2) && img(3)) || planes != (f == VX_DF_IMAGE_RGBX ? 4 : 3)) return VX_ERROR_INVALID_PARAMETERS;
+        Image *i0 = img(0);
+        if (!fmt_is(i0, VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
+        for (int k = 1; k < planes; k++) {
+            if (!fmt_is(img(k), VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
+            if ((img(k)->width << sx) != i0->width || (img(k)->height << sy) != i0->height) return VX_ERROR_INVALID_DIMENSION;
+        }
+        return set_meta(o, i0->width, i0->height, f);
     }
     case VX_KERNEL_SCALE_IMAGE: {
         Image *i0 = img(0), *o = img(1);
@@ -344,9 +382,43 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
     }
     case VX_KERNEL_CHANNEL_EXTRACT: {                                                                  // :342
         Image *i0 = IMG(p[0]);
-        vx_enum ch = sc_enum(p[1]);
-        int plane = ch == VX_CHANNEL_Y ? 0 : ch == VX_CHANNEL_U ? 1 : 2;
-        add(LK::CHANNEL_COPY_U8_U8, {p[2], i0->children.empty() ? (Ref *)i0 : (Ref *)i0->children[plane]});
+        const int idx = channel_index(sc_enum(p[1]));
+        const vx_df_image f = i0->format;
+        static const LK u24[3] = {LK::CHANNEL_EXTRACT_U8_U24_POS0, LK::CHANNEL_EXTRACT_U8_U24_POS1, LK::CHANNEL_EXTRACT_U8_U24_POS2};
+        static const LK u32[4] = {LK::CHANNEL_EXTRACT_U8_U32_POS0, LK::CHANNEL_EXTRACT_U8_U32_POS1, LK::CHANNEL_EXTRACT_U8_U32_POS2,
+                                  LK::CHANNEL_EXTRACT_U8_U32_POS3};
+        if (f == VX_DF_IMAGE_RGB) add(u24[idx], {p[2], p[0]});
+        else if (f == VX_DF_IMAGE_RGBX) add(u32[idx], {p[2], p[0]});
+        else if (f == VX_DF_IMAGE_NV12 || f == VX_DF_IMAGE_NV21) {
+            if (idx == 0) add(LK::CHANNEL_COPY_U8_U8, {p[2], i0->children[0]});
+            else add((idx == 1) == (f == VX_DF_IMAGE_NV12) ? LK::CHANNEL_EXTRACT_U8_U16_POS0 : LK::CHANNEL_EXTRACT_U8_U16_POS1,
+                     {p[2], i0->children[1]});
+        } else if (f == VX_DF_IMAGE_UYVY) {
+            add(idx == 0 ? LK::CHANNEL_EXTRACT_U8_U16_POS1 : idx == 1 ? LK::CHANNEL_EXTRACT_U8_U32_POS0 : LK::CHANNEL_EXTRACT_U8_U32_POS2,
+                {p[2], p[0]});
+        } else if (f == VX_DF_IMAGE_YUYV) {
+            add(idx == 0 ? LK::CHANNEL_EXTRACT_U8_U16_POS0 : idx == 1 ? LK::CHANNEL_EXTRACT_U8_U32_POS1 : LK::CHANNEL_EXTRACT_U8_U32_POS3,
+                {p[2], p[0]});
+        } else {
+            add(LK::CHANNEL_COPY_U8_U8, {p[2], i0->children[idx]});
+        }
+        return VX_SUCCESS;
+    }
+    case VX_KERNEL_CHANNEL_COMBINE: {                                                                  // :416
+        Image *o = IMG(p[4]);
+        const vx_df_image f = o->format;
+        auto plane0 = [](Ref *r) -> Ref * { return IMG(r)->children.empty() ? r : (Ref *)IMG(r)->children[0]; };
+        if (f == VX_DF_IMAGE_RGB) add(LK::CHANNEL_COMBINE_U24_U8U8U8_RGB, {p[4], p[0], p[1], p[2]});
+        else if (f == VX_DF_IMAGE_RGBX) add(LK::CHANNEL_COMBINE_U32_U8U8U8U8_RGBX, {p[4], p[0], p[1], p[2], p[3]});
+        else if (f == VX_DF_IMAGE_UYVY) add(LK::CHANNEL_COMBINE_U32_U8U8U8_UYVY, {p[4], p[0], p[1], p[2]});
+        else if (f == VX_DF_IMAGE_YUYV) add(LK::CHANNEL_COMBINE_U32_U8U8U8_YUYV, {p[4], p[0], p[1], p[2]});
+        else if (f == VX_DF_IMAGE_NV12 || f == VX_DF_IMAGE_NV21) {
+            add(LK::CHANNEL_COPY_U8_U8, {o->children[0], plane0(p[0])});
+            add(LK::CHANNEL_COMBINE_U16_U8U8, f == VX_DF_IMAGE_NV12 ? std::vector<Ref *>{o->children[1], p[1], p[2]}
+                                                                     : std::vector<Ref *>{o->children[1], p[2], p[1]});
+        } else {                                                    // IYUV, YUV4: plane copies
+            for (int k = 0; k < 3; k++) add(LK::CHANNEL_COPY_U8_U8, {o->children[k], plane0(p[k])});
+        }
         return VX_SUCCESS;
     }
     case VX_KERNEL_SCALE_IMAGE: {                                                                      // :563
@@ -676,7 +748,21 @@ vx_status propagate_valid_rects(Graph *g)
         case LK::COLOR_DEPTH_U8_S16_SAT: case LK::COLOR_DEPTH_U8_S16_WRAP: case LK::COLOR_DEPTH_S16_U8:
         case LK::THRESHOLD_U8_U8_BINARY: case LK::CHANNEL_COPY_U8_U8:
         case LK::THRESHOLD_U8_U8_RANGE: case LK::NOT_U8_U8:
+        case LK::CHANNEL_EXTRACT_U8_U16_POS0: case LK::CHANNEL_EXTRACT_U8_U16_POS1: case LK::CHANNEL_EXTRACT_U8_U24_POS0:
+        case LK::CHANNEL_EXTRACT_U8_U24_POS1: case LK::CHANNEL_EXTRACT_U8_U24_POS2: case LK::CHANNEL_EXTRACT_U8_U32_POS0:
+        case LK::CHANNEL_EXTRACT_U8_U32_POS1: case LK::CHANNEL_EXTRACT_U8_U32_POS2: case LK::CHANNEL_EXTRACT_U8_U32_POS3:
+        case LK::CHANNEL_COMBINE_U32_U8U8U8_UYVY: case LK::CHANNEL_COMBINE_U32_U8U8U8_YUYV:   // :11847 (first input)
             copy_rect(I(0), I(1)); break;
+        case LK::CHANNEL_COMBINE_U16_U8U8: case LK::CHANNEL_COMBINE_U24_U8U8U8_RGB: case LK::CHANNEL_COMBINE_U32_U8U8U8U8_RGBX: {
+            Image *o = I(0);                                     // :11693, :11767: intersection of the inputs
+            o->valid = I(1)->valid;
+            for (size_t k = 2; k < ln.p.size(); k++) {
+                const vx_rectangle_t &r = I((int)k)->valid;
+                o->valid = vx_rectangle_t{std::max(o->valid.start_x, r.start_x), std::max(o->valid.start_y, r.start_y),
+                                          std::min(o->valid.end_x, r.end_x), std::min(o->valid.end_y, r.end_y)};
+            }
+            break;
+        }
         case LK::BOX_U8_U8_3x3: case LK::DILATE_U8_U8_3x3: case LK::ERODE_U8_U8_3x3: case LK::MEDIAN_U8_U8_3x3:
             shrink_from(I(0), I(1), 1); break;                  // e.g. :15033 (Box)
         case LK::ABS_DIFF_U8_U8U8: case LK::ABS_DIFF_S16_S16S16_SAT:

@@ -271,6 +271,61 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         st.launch = [=](cudaStream_t q) { return agocuda_Threshold_U8_U8_Binary(S(q), w, h, d, ds, s, ss, thr); };
         return VX_SUCCESS;
     }
+    case LK::COLOR_DEPTH_U8_S16_WRAP: {
+        uint8_t *d = dptr(p[0]); const int16_t *s = (const int16_t *)dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        int32_t shift = sc_i32(p[2]);
+        st.launch = [=](cudaStream_t q) { return agocuda_ColorDepth_U8_S16_Wrap(S(q), w, h, d, ds, s, ss, shift); };
+        return VX_SUCCESS;
+    }
+    case LK::COLOR_DEPTH_S16_U8: {
+        int16_t *d = (int16_t *)dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        int32_t shift = sc_i32(p[2]);
+        st.launch = [=](cudaStream_t q) { return agocuda_ColorDepth_S16_U8(S(q), w, h, d, ds, s, ss, shift); };
+        return VX_SUCCESS;
+    }
+    case LK::CHANNEL_EXTRACT_U8_U16_POS0: case LK::CHANNEL_EXTRACT_U8_U16_POS1: case LK::CHANNEL_EXTRACT_U8_U24_POS0:
+    case LK::CHANNEL_EXTRACT_U8_U24_POS1: case LK::CHANNEL_EXTRACT_U8_U24_POS2: case LK::CHANNEL_EXTRACT_U8_U32_POS0:
+    case LK::CHANNEL_EXTRACT_U8_U32_POS1: case LK::CHANNEL_EXTRACT_U8_U32_POS2: case LK::CHANNEL_EXTRACT_U8_U32_POS3: {
+        using Fn = int (*)(void *, uint32_t, uint32_t, uint8_t *, uint32_t, const uint8_t *, uint32_t);
+        static const Fn fns[] = {agocuda_ChannelExtract_U8_U16_Pos0, agocuda_ChannelExtract_U8_U16_Pos1,
+                                 agocuda_ChannelExtract_U8_U24_Pos0, agocuda_ChannelExtract_U8_U24_Pos1,
+                                 agocuda_ChannelExtract_U8_U24_Pos2, agocuda_ChannelExtract_U8_U32_Pos0,
+                                 agocuda_ChannelExtract_U8_U32_Pos1, agocuda_ChannelExtract_U8_U32_Pos2,
+                                 agocuda_ChannelExtract_U8_U32_Pos3};
+        const Fn fn = fns[(int)ln.k - (int)LK::CHANNEL_EXTRACT_U8_U16_POS0];
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        st.launch = [=](cudaStream_t q) { return fn(S(q), w, h, d, ds, s, ss); };
+        return VX_SUCCESS;
+    }
+    case LK::CHANNEL_COMBINE_U16_U8U8: {
+        uint8_t *d = dptr(p[0]); const uint8_t *a = dptr(p[1]), *b = dptr(p[2]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), as_ = dstride(p[1]), bs = dstride(p[2]);
+        st.launch = [=](cudaStream_t q) { return agocuda_ChannelCombine_U16_U8U8(S(q), w, h, d, ds, a, as_, b, bs); };
+        return VX_SUCCESS;
+    }
+    case LK::CHANNEL_COMBINE_U24_U8U8U8_RGB: case LK::CHANNEL_COMBINE_U32_U8U8U8_UYVY: case LK::CHANNEL_COMBINE_U32_U8U8U8_YUYV: {
+        using Fn = int (*)(void *, uint32_t, uint32_t, uint8_t *, uint32_t, const uint8_t *, uint32_t, const uint8_t *,
+                           uint32_t, const uint8_t *, uint32_t);
+        const Fn fn = ln.k == LK::CHANNEL_COMBINE_U24_U8U8U8_RGB ? agocuda_ChannelCombine_U24_U8U8U8_RGB
+                    : ln.k == LK::CHANNEL_COMBINE_U32_U8U8U8_UYVY ? agocuda_ChannelCombine_U32_U8U8U8_UYVY
+                                                                  : agocuda_ChannelCombine_U32_U8U8U8_YUYV;
+        uint8_t *d = dptr(p[0]); const uint8_t *a = dptr(p[1]), *b = dptr(p[2]), *c = dptr(p[3]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), as_ = dstride(p[1]), bs = dstride(p[2]), cs = dstride(p[3]);
+        st.launch = [=](cudaStream_t q) { return fn(S(q), w, h, d, ds, a, as_, b, bs, c, cs); };
+        return VX_SUCCESS;
+    }
+    case LK::CHANNEL_COMBINE_U32_U8U8U8U8_RGBX: {
+        uint8_t *d = dptr(p[0]); const uint8_t *a = dptr(p[1]), *b = dptr(p[2]), *c = dptr(p[3]), *e = dptr(p[4]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), as_ = dstride(p[1]), bs = dstride(p[2]), cs = dstride(p[3]),
+                 es = dstride(p[4]);
+        st.launch = [=](cudaStream_t q) {
+            return agocuda_ChannelCombine_U32_U8U8U8U8_RGBX(S(q), w, h, d, ds, a, as_, b, bs, c, cs, e, es);
+        };
+        return VX_SUCCESS;
+    }
     case LK::THRESHOLD_U8_U8_RANGE: {
         uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
         uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);

@@ -864,4 +864,8 @@ vx_node vxXorNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out)
 vx_node vxNotNode(vx_graph graph, vx_image input, vx_image output)
 { return make_node(graph, VX_KERNEL_NOT, {R(input), R(output)}); }
 
+vx_node vxChannelCombineNode(vx_graph graph, vx_image plane0, vx_image plane1, vx_image plane2, vx_image plane3,
+                             vx_image output)
+{ return make_node(graph, VX_KERNEL_CHANNEL_COMBINE, {R(plane0), R(plane1), R(plane2), R(plane3), R(output)}); }
+
 }  // extern "C"

@@ -183,6 +183,10 @@ enum class LK : int {
     SUB_U8_U8U8_WRAP, SUB_U8_U8U8_SAT, SUB_S16_U8U8, SUB_S16_S16U8_WRAP, SUB_S16_S16U8_SAT,
     SUB_S16_U8S16_WRAP, SUB_S16_U8S16_SAT, SUB_S16_S16S16_WRAP, SUB_S16_S16S16_SAT,
     AND_U8_U8U8, OR_U8_U8U8, XOR_U8_U8U8, NOT_U8_U8, THRESHOLD_U8_U8_RANGE,
+    CHANNEL_EXTRACT_U8_U16_POS0, CHANNEL_EXTRACT_U8_U16_POS1, CHANNEL_EXTRACT_U8_U24_POS0, CHANNEL_EXTRACT_U8_U24_POS1,
+    CHANNEL_EXTRACT_U8_U24_POS2, CHANNEL_EXTRACT_U8_U32_POS0, CHANNEL_EXTRACT_U8_U32_POS1, CHANNEL_EXTRACT_U8_U32_POS2,
+    CHANNEL_EXTRACT_U8_U32_POS3, CHANNEL_COMBINE_U16_U8U8, CHANNEL_COMBINE_U24_U8U8U8_RGB,
+    CHANNEL_COMBINE_U32_U8U8U8_UYVY, CHANNEL_COMBINE_U32_U8U8U8_YUYV, CHANNEL_COMBINE_U32_U8U8U8U8_RGBX,
     COUNT
 };
 const char *lk_name(LK k);

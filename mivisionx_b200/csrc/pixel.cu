@@ -27,6 +27,8 @@ enum EwOp : int {
     EW_AND, EW_OR, EW_XOR, EW_NOT,
     EW_RANGE,                                    // 255 inside [lower, upper], else 0
     EW_BINARY,                                   // 255 above the threshold, else 0
+    EW_DEPTH_DOWN_WRAP,                          // S16 -> U8: low byte of v >> shift
+    EW_DEPTH_UP,                                 // U8 -> S16: v << shift in 16 bits
 };
 
 __device__ __forceinline__ int sat_s16(int v) { return v < -32768 ? -32768 : (v > 32767 ? 32767 : v); }
@@ -53,6 +55,8 @@ __device__ __forceinline__ int ew_apply(int a, int b, int p0, int p1)
     case EW_NOT: return ~a & 0xff;
     case EW_RANGE: return (a > p1 || a < p0) ? 0 : 255;                // :3742
     case EW_BINARY: return a > p0 ? 255 : 0;                           // :3660
+    case EW_DEPTH_DOWN_WRAP: return (a >> p0) & 0xff;                  // :3488
+    case EW_DEPTH_UP: return (int)(int16_t)(a << p0);                  // :3604
     }
     return 0;
 }
@@ -118,7 +122,7 @@ template <int OP, typename TO, typename TA, typename TB>
 int ew_launch(void *stream, uint32_t W, uint32_t H, TO *dst, uint32_t dstStride, const TA *a, uint32_t aStride,
               const TB *b, uint32_t bStride, int p0 = 0, int p1 = 0)
 {
-    const bool unary = OP == EW_NOT || OP == EW_RANGE || OP == EW_BINARY;
+    const bool unary = OP == EW_NOT || OP == EW_RANGE || OP == EW_BINARY || OP == EW_DEPTH_DOWN_WRAP || OP == EW_DEPTH_UP;
     if (!W || !H || !ew_plane_ok(dst, dstStride, W) || !ew_plane_ok(a, aStride, W) ||
         (!unary && !ew_plane_ok(b, bStride, W)))
         return AGOCUDA_INVALID_PARAMS;
@@ -176,6 +180,22 @@ extern "C" int agocuda_Threshold_U8_U8_Binary(void *stream, uint32_t dstWidth, u
     // the reference passes the threshold as vx_uint8 (threshold_value.U1, ago_kernel_api.cpp:3442)
     return ew_launch<EW_BINARY>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc, srcStride, (const uint8_t *)nullptr, 0,
                                 (int)(uint8_t)threshold);
+}
+
+extern "C" int agocuda_ColorDepth_U8_S16_Wrap(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                              uint32_t dstStride, const int16_t *pSrc, uint32_t srcStride, int32_t shift)
+{
+    if (shift < 0 || shift > 15) return AGOCUDA_INVALID_PARAMS;
+    return ew_launch<EW_DEPTH_DOWN_WRAP>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc, srcStride,
+                                         (const uint8_t *)nullptr, 0, shift);
+}
+
+extern "C" int agocuda_ColorDepth_S16_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst,
+                                         uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride, int32_t shift)
+{
+    if (shift < 0 || shift > 15) return AGOCUDA_INVALID_PARAMS;
+    return ew_launch<EW_DEPTH_UP>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc, srcStride, (const uint8_t *)nullptr,
+                                  0, shift);
 }
 
 extern "C" int agocuda_Threshold_U8_U8_Range(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
@@ -575,3 +595,161 @@ FILTER(Dilate_U8_U8_3x3, AGOCUDA_PX_DILATE3x3)
 FILTER(Erode_U8_U8_3x3, AGOCUDA_PX_ERODE3x3)
 FILTER(Median_U8_U8_3x3, AGOCUDA_PX_MEDIAN3x3)
 #undef FILTER
+
+// ---------------------------------------------------------------------------------
+// Channel extract / combine between U8 planes and interleaved formats
+// (ago_haf_cpu_ch_extract_combine.cpp).  A thread owns 4 output units: their bytes are
+// gathered with 32-bit loads and byte permutes and written as whole words; the units a row's
+// width cuts go byte by byte.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr int kChBX = 64, kChBY = 4;
+
+// dst[x] = src[x * UNIT + POS]
+template <int UNIT, int POS>
+__global__ void __launch_bounds__(kChBX * kChBY)
+k_channel_extract(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride)
+{
+    const int x = (blockIdx.x * kChBX + threadIdx.x) * 4;
+    const int y = blockIdx.y * kChBY + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const uint8_t *s = src + (size_t)y * srcStride + (size_t)x * UNIT;
+    uint8_t *d = dst + (size_t)y * dstStride + x;
+    if (x + 4 <= W) {
+        uint32_t w[UNIT];
+#pragma unroll
+        for (int i = 0; i < UNIT; i++) w[i] = __ldg((const uint32_t *)s + i);
+        auto byte = [&](int k) { return (w[k >> 2] >> (8 * (k & 3))) & 0xffu; };
+        *(uint32_t *)d = byte(POS) | (byte(UNIT + POS) << 8) | (byte(2 * UNIT + POS) << 16) | (byte(3 * UNIT + POS) << 24);
+    } else {
+        for (int i = 0; i < W - x; i++) d[i] = s[i * UNIT + POS];
+    }
+}
+
+enum ChCombine { CH_UV, CH_RGB, CH_RGBX, CH_UYVY, CH_YUYV };
+
+// one output unit: UV = (u, v); RGB = (r, g, b); RGBX = (r, g, b, x); UYVY = (u, y0, v, y1) and
+// YUYV = (y0, u, y1, v) for a pair of pixels (y at 2x, 2x+1; u, v at x)
+template <int MODE>
+__global__ void __launch_bounds__(kChBX * kChBY)
+k_channel_combine(int W, int H, uint8_t *dst, int dstStride, const uint8_t *a, int aStride, const uint8_t *b,
+                  int bStride, const uint8_t *c, int cStride, const uint8_t *e, int eStride)
+{
+    constexpr int UNIT = MODE == CH_UV ? 2 : MODE == CH_RGB ? 3 : 4;
+    const int x = (blockIdx.x * kChBX + threadIdx.x) * 4;   // first output unit
+    const int y = blockIdx.y * kChBY + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const uint8_t *pa = a + (size_t)y * aStride, *pb = b + (size_t)y * bStride;
+    const uint8_t *pc = c ? c + (size_t)y * cStride : nullptr, *pe = e ? e + (size_t)y * eStride : nullptr;
+    uint8_t *d = dst + (size_t)y * dstStride + (size_t)x * UNIT;
+    auto unit_byte = [&](int u, int k) -> uint32_t {   // byte k of output unit u
+        switch (MODE) {
+        case CH_UV: return k == 0 ? pa[u] : pb[u];
+        case CH_RGB: return k == 0 ? pa[u] : k == 1 ? pb[u] : pc[u];
+        case CH_RGBX: return k == 0 ? pa[u] : k == 1 ? pb[u] : k == 2 ? pc[u] : pe[u];
+        case CH_UYVY: return k == 0 ? pb[u] : k == 1 ? pa[2 * u] : k == 2 ? pc[u] : pa[2 * u + 1];
+        default: return k == 0 ? pa[2 * u] : k == 1 ? pb[u] : k == 2 ? pa[2 * u + 1] : pc[u];
+        }
+    };
+    if (x + 4 <= W) {
+        uint32_t out[UNIT] = {};
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int k = 0; k < UNIT; k++) {
+                const int o = u * UNIT + k;
+                out[o >> 2] |= unit_byte(x + u, k) << (8 * (o & 3));
+            }
+#pragma unroll
+        for (int i = 0; i < UNIT; i++) ((uint32_t *)d)[i] = out[i];
+    } else {
+        for (int u = 0; u < W - x; u++)
+            for (int k = 0; k < UNIT; k++) d[u * UNIT + k] = (uint8_t)unit_byte(x + u, k);
+    }
+}
+
+bool ch_plane_ok(const uint8_t *p, uint32_t stride) { return p && ((uintptr_t)p & 3) == 0 && (stride & 3) == 0; }
+
+template <int UNIT, int POS>
+int extract_launch(void *stream, uint32_t W, uint32_t H, uint8_t *dst, uint32_t dstStride, const uint8_t *src,
+                   uint32_t srcStride)
+{
+    if (!W || !H || !ch_plane_ok(dst, dstStride) || !ch_plane_ok(src, srcStride) || dstStride < W || srcStride < W * UNIT)
+        return AGOCUDA_INVALID_PARAMS;
+    dim3 grd(div_up(W, kChBX * 4), div_up(H, kChBY));
+    k_channel_extract<UNIT, POS><<<grd, dim3(kChBX, kChBY), 0, as_stream(stream)>>>((int)W, (int)H, dst, (int)dstStride,
+                                                                                    src, (int)srcStride);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+template <int MODE>
+int combine_launch(void *stream, uint32_t W, uint32_t H, uint8_t *dst, uint32_t dstStride, const uint8_t *a,
+                   uint32_t aStride, const uint8_t *b, uint32_t bStride, const uint8_t *c, uint32_t cStride,
+                   const uint8_t *e, uint32_t eStride)
+{
+    constexpr int UNIT = MODE == CH_UV ? 2 : MODE == CH_RGB ? 3 : 4;
+    const int planes = MODE == CH_UV ? 2 : MODE == CH_RGBX ? 4 : 3;
+    const bool pairs = MODE == CH_UYVY || MODE == CH_YUYV;   // W counts pixels: one unit per pair
+    const uint32_t units = pairs ? W / 2 : W;
+    if (!units || !H || (pairs && (W & 1)) || !ch_plane_ok(dst, dstStride) || dstStride < units * UNIT || !a || !b ||
+        (planes > 2 && !c) || (planes > 3 && !e))
+        return AGOCUDA_INVALID_PARAMS;
+    dim3 grd(div_up(units, kChBX * 4), div_up(H, kChBY));
+    k_channel_combine<MODE><<<grd, dim3(kChBX, kChBY), 0, as_stream(stream)>>>(
+        (int)units, (int)H, dst, (int)dstStride, a, (int)aStride, b, (int)bStride, planes > 2 ? c : nullptr, (int)cStride,
+        planes > 3 ? e : nullptr, (int)eStride);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+}  // namespace
+
+#define EXTRACT(NAME, UNIT, POS)                                                                                  \
+    extern "C" int agocuda_##NAME(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride, \
+                                  const uint8_t *pSrc, uint32_t srcStride)                                        \
+    {                                                                                                          \
+        return extract_launch<UNIT, POS>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc, srcStride);        \
+    }
+EXTRACT(ChannelExtract_U8_U16_Pos0, 2, 0)
+EXTRACT(ChannelExtract_U8_U16_Pos1, 2, 1)
+EXTRACT(ChannelExtract_U8_U24_Pos0, 3, 0)
+EXTRACT(ChannelExtract_U8_U24_Pos1, 3, 1)
+EXTRACT(ChannelExtract_U8_U24_Pos2, 3, 2)
+EXTRACT(ChannelExtract_U8_U32_Pos0, 4, 0)
+EXTRACT(ChannelExtract_U8_U32_Pos1, 4, 1)
+EXTRACT(ChannelExtract_U8_U32_Pos2, 4, 2)
+EXTRACT(ChannelExtract_U8_U32_Pos3, 4, 3)
+#undef EXTRACT
+
+extern "C" int agocuda_ChannelCombine_U16_U8U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst,
+                                               uint32_t dstStride, const uint8_t *pSrc1, uint32_t src1Stride,
+                                               const uint8_t *pSrc2, uint32_t src2Stride)
+{
+    return combine_launch<CH_UV>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc1, src1Stride, pSrc2, src2Stride,
+                                 nullptr, 0, nullptr, 0);
+}
+
+#define COMBINE3(NAME, MODE)                                                                                      \
+    extern "C" int agocuda_##NAME(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride, \
+                                  const uint8_t *pSrc1, uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride, \
+                                  const uint8_t *pSrc3, uint32_t src3Stride)                                      \
+    {                                                                                                          \
+        return combine_launch<MODE>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc1, src1Stride, pSrc2, src2Stride, \
+                                    pSrc3, src3Stride, nullptr, 0);                                            \
+    }
+COMBINE3(ChannelCombine_U24_U8U8U8_RGB, CH_RGB)
+COMBINE3(ChannelCombine_U32_U8U8U8_UYVY, CH_UYVY)
+COMBINE3(ChannelCombine_U32_U8U8U8_YUYV, CH_YUYV)
+#undef COMBINE3
+
+extern "C" int agocuda_ChannelCombine_U32_U8U8U8U8_RGBX(void *stream, uint32_t dstWidth, uint32_t dstHeight,
+                                                       uint8_t *pDst, uint32_t dstStride, const uint8_t *pSrc1,
+                                                       uint32_t src1Stride, const uint8_t *pSrc2, uint32_t src2Stride,
+                                                       const uint8_t *pSrc3, uint32_t src3Stride, const uint8_t *pSrc4,
+                                                       uint32_t src4Stride)
+{
+    return combine_launch<CH_RGBX>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc1, src1Stride, pSrc2, src2Stride,
+                                   pSrc3, src3Stride, pSrc4, src4Stride);
+}

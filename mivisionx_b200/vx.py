@@ -172,6 +172,7 @@ _SIGS = {
     "vxAbsDiffNode": (vp, [vp, vp, vp, vp]), "vxAndNode": (vp, [vp, vp, vp, vp]), "vxOrNode": (vp, [vp, vp, vp, vp]),
     "vxXorNode": (vp, [vp, vp, vp, vp]), "vxNotNode": (vp, [vp, vp, vp]),
     "vxAddNode": (vp, [vp, vp, vp, i32, vp]), "vxSubtractNode": (vp, [vp, vp, vp, i32, vp]),
+    "vxChannelCombineNode": (vp, [vp, vp, vp, vp, vp, vp]),
 }
 
 _PIX = {VX_DF_IMAGE_U8: (np.uint8, 1), VX_DF_IMAGE_U16: (np.uint16, 1), VX_DF_IMAGE_S16: (np.int16, 1),

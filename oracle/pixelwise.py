@@ -48,6 +48,17 @@ def absdiff(a, b):
     return d.astype(np.uint8) if np.asarray(a).dtype == np.uint8 else np.minimum(d, 32767).astype(np.int16)
 
 
+def convert_depth(a, out_dtype, policy_saturate, shift):
+    """HafCpu_ColorDepth_U8_S16_Wrap (ago_haf_cpu_arithmetic.cpp:3488): low byte of v >> shift;
+    _Sat (:3546): clamp(v >> shift, 0, 255); HafCpu_ColorDepth_S16_U8 (:3604): v << shift in
+    16 bits."""
+    v = _i32(a)
+    if out_dtype == np.uint8:
+        v = v >> shift
+        return (np.clip(v, 0, 255) if policy_saturate else v & 0xFF).astype(np.uint8)
+    return _wrap_s16(v << shift)
+
+
 def logical(op, a, b=None):
     """HafCpu_And/Or/Xor_U8_U8U8, HafCpu_Not_U8_U8 (ago_haf_cpu_logical.cpp:518, :31)."""
     a = np.asarray(a, np.uint8)

@@ -68,6 +68,13 @@ def _cases():
     out.append(("not", "not", None, (U8,), U8, lambda a: P.logical("not", a)))
     for op, fn in (("box", P.box3x3), ("median", P.median3x3), ("dilate", P.dilate3x3), ("erode", P.erode3x3)):
         out.append((op, op, None, (U8,), U8, fn))
+    for shift in (0, 3, 7):
+        out.append((f"depth_wrap_{shift}", "depth", (WRAP, shift), (S16,), U8,
+                    lambda a, s=shift: P.convert_depth(a, np.uint8, False, s)))
+        out.append((f"depth_sat_{shift}", "depth", (SAT, shift), (S16,), U8,
+                    lambda a, s=shift: P.convert_depth(a, np.uint8, True, s)))
+        out.append((f"depth_up_{shift}", "depth", (WRAP, shift), (U8,), S16,
+                    lambda a, s=shift: P.convert_depth(a, np.int16, False, s)))
     out.append(("range", "range", (37, 201), (U8,), U8, lambda a: P.threshold_range(a, 37, 201)))
     out.append(("range_empty", "range", (200, 100), (U8,), U8, lambda a: P.threshold_range(a, 200, 100)))
     return out
@@ -86,6 +93,8 @@ def _node(api, ctx, g, op, extra, ins, out):
         return f(g, ins[0], ins[1], out)
     if op == "range":
         return api.vxThresholdNode(g, ins[0], api.threshold_range(ctx, *extra), out)
+    if op == "depth":
+        return api.vxConvertDepthNode(g, ins[0], out, extra[0], api.scalar(ctx, V.VX_TYPE_INT32, extra[1]))
     f = {"not": api.vxNotNode, "box": api.vxBox3x3Node, "median": api.vxMedian3x3Node,
          "dilate": api.vxDilate3x3Node, "erode": api.vxErode3x3Node}[op]
     return f(g, ins[0], out)
