@@ -561,6 +561,29 @@ int agocuda_Erode_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight,
 int agocuda_Median_U8_U8_3x3(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
                              const uint8_t *pSrc, uint32_t srcStride);
 
+/* dst = lut[src] for U8 (pLut: 256 device bytes); dst = lut[clamp(src + offset, 0, count-1)]
+ * for S16 (pLut: count device int16, offset = count / 2 for OpenVX LUTs).  Planes 16-byte
+ * aligned.  Replace HipExec_Lut_U8_U8 (hip_host_decls.h:377) and the CPU-only
+ * HafCpu_Lut_S16_S16 (ago_haf_cpu_arithmetic.cpp:4916). */
+int agocuda_Lut_U8_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                      const uint8_t *pSrc, uint32_t srcStride, const uint8_t *pLut);
+int agocuda_Lut_S16_S16(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                        const int16_t *pSrc, uint32_t srcStride, const int16_t *pLut, uint32_t count, uint32_t offset);
+
+/* Integral image: dst(x, y) = sum of src over [0, x] x [0, y], modulo 2^32.  Needs `scratch`
+ * device memory of agocuda_IntegralImage_scratch_size(W, H) bytes; three launches.  Replaces
+ * HafCpu_IntegralImage_U32_U8 (ago_haf_cpu_arithmetic.cpp:7057; CPU only in the reference). */
+size_t agocuda_IntegralImage_scratch_size(uint32_t width, uint32_t height);
+int agocuda_IntegralImage_U32_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint32_t *pDst, uint32_t dstStride,
+                                 const uint8_t *pSrc, uint32_t srcStride, void *scratch, size_t scratchBytes);
+
+/* Histogram into pHist[numBins] (device; cleared first): pixels v with offset <= v <
+ * offset + range count into bin (v - offset) * numBins / range.  Source rows 16-byte
+ * aligned.  The reference computes it on the CPU only (HafCpu_HistogramFixedBins_DATA_U8,
+ * ago_haf_cpu_histogram.cpp:519). */
+int agocuda_Histogram_DATA_U8(void *stream, uint32_t *pHist, uint32_t srcWidth, uint32_t srcHeight, const uint8_t *pSrc,
+                              uint32_t srcStride, uint32_t numBins, int32_t offset, uint32_t range);
+
 /* ------------------------------------------------------------------------------------ */
 /* Channel extract / combine (reference: hipvx/hip_host_decls.h:413-492; CPU semantics    */
 /* ago/ago_haf_cpu_ch_extract_combine.cpp).  Row bases 4-byte aligned, strides multiples  */

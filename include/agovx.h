@@ -55,6 +55,8 @@ typedef struct _vx_pyramid *vx_pyramid;
 typedef struct _vx_remap *vx_remap;
 typedef struct _vx_convolution *vx_convolution;
 typedef struct _vx_delay *vx_delay;
+typedef struct _vx_lut *vx_lut;
+typedef struct _vx_distribution *vx_distribution;
 
 #define VX_ID_KHRONOS 0x000
 #define VX_ID_AMD 0x00D
@@ -181,6 +183,11 @@ enum { VX_THRESHOLD_TYPE = VX__A(VX_TYPE_THRESHOLD, 0), VX_THRESHOLD_THRESHOLD_V
        VX_THRESHOLD_TRUE_VALUE = VX__A(VX_TYPE_THRESHOLD, 4), VX_THRESHOLD_FALSE_VALUE = VX__A(VX_TYPE_THRESHOLD, 5),
        VX_THRESHOLD_DATA_TYPE = VX__A(VX_TYPE_THRESHOLD, 6), VX_THRESHOLD_INPUT_FORMAT = VX__A(VX_TYPE_THRESHOLD, 7),
        VX_THRESHOLD_OUTPUT_FORMAT = VX__A(VX_TYPE_THRESHOLD, 8) };
+enum { VX_DISTRIBUTION_DIMENSIONS = VX__A(VX_TYPE_DISTRIBUTION, 0), VX_DISTRIBUTION_OFFSET = VX__A(VX_TYPE_DISTRIBUTION, 1),
+       VX_DISTRIBUTION_RANGE = VX__A(VX_TYPE_DISTRIBUTION, 2), VX_DISTRIBUTION_BINS = VX__A(VX_TYPE_DISTRIBUTION, 3),
+       VX_DISTRIBUTION_WINDOW = VX__A(VX_TYPE_DISTRIBUTION, 4), VX_DISTRIBUTION_SIZE = VX__A(VX_TYPE_DISTRIBUTION, 5) };
+enum { VX_LUT_TYPE = VX__A(VX_TYPE_LUT, 0), VX_LUT_COUNT = VX__A(VX_TYPE_LUT, 1), VX_LUT_SIZE = VX__A(VX_TYPE_LUT, 2),
+       VX_LUT_OFFSET = VX__A(VX_TYPE_LUT, 3) };
 enum { VX_MATRIX_TYPE = VX__A(VX_TYPE_MATRIX, 0), VX_MATRIX_ROWS = VX__A(VX_TYPE_MATRIX, 1),
        VX_MATRIX_COLUMNS = VX__A(VX_TYPE_MATRIX, 2), VX_MATRIX_SIZE = VX__A(VX_TYPE_MATRIX, 3) };
 enum { VX_PYRAMID_LEVELS = VX__A(VX_TYPE_PYRAMID, 0), VX_PYRAMID_SCALE = VX__A(VX_TYPE_PYRAMID, 1),
@@ -221,7 +228,8 @@ typedef struct {
 enum vx_kernel_e {
     VX_KERNEL_COLOR_CONVERT = VX__K(0x1), VX_KERNEL_CHANNEL_EXTRACT = VX__K(0x2), VX_KERNEL_CHANNEL_COMBINE = VX__K(0x3),
     VX_KERNEL_SOBEL_3x3 = VX__K(0x4), VX_KERNEL_MAGNITUDE = VX__K(0x5), VX_KERNEL_PHASE = VX__K(0x6),
-    VX_KERNEL_SCALE_IMAGE = VX__K(0x7), VX_KERNEL_ABSDIFF = VX__K(0xB), VX_KERNEL_THRESHOLD = VX__K(0xD),
+    VX_KERNEL_SCALE_IMAGE = VX__K(0x7), VX_KERNEL_TABLE_LOOKUP = VX__K(0x8), VX_KERNEL_ABSDIFF = VX__K(0xB), VX_KERNEL_THRESHOLD = VX__K(0xD),
+    VX_KERNEL_INTEGRAL_IMAGE = VX__K(0xE), VX_KERNEL_HISTOGRAM = VX__K(0x9),
     VX_KERNEL_DILATE_3x3 = VX__K(0xF), VX_KERNEL_ERODE_3x3 = VX__K(0x10), VX_KERNEL_MEDIAN_3x3 = VX__K(0x11),
     VX_KERNEL_BOX_3x3 = VX__K(0x12), VX_KERNEL_AND = VX__K(0x1C), VX_KERNEL_OR = VX__K(0x1D), VX_KERNEL_XOR = VX__K(0x1E),
     VX_KERNEL_NOT = VX__K(0x1F), VX_KERNEL_ADD = VX__K(0x21), VX_KERNEL_SUBTRACT = VX__K(0x22),
@@ -319,6 +327,23 @@ vx_status vxCopyThresholdValue(vx_threshold thresh, vx_pixel_value_t *value_ptr,
 vx_status vxCopyThresholdRange(vx_threshold thresh, vx_pixel_value_t *lower_value_ptr, vx_pixel_value_t *upper_value_ptr,
                                vx_enum usage, vx_enum user_mem_type);
 
+vx_distribution vxCreateDistribution(vx_context context, vx_size numBins, vx_int32 offset, vx_uint32 range);
+vx_distribution vxCreateVirtualDistribution(vx_graph graph, vx_size numBins, vx_int32 offset, vx_uint32 range);
+vx_status vxReleaseDistribution(vx_distribution *distribution);
+vx_status vxQueryDistribution(vx_distribution distribution, vx_enum attribute, void *ptr, vx_size size);
+vx_status vxCopyDistribution(vx_distribution distribution, void *user_ptr, vx_enum usage, vx_enum user_mem_type);
+vx_status vxMapDistribution(vx_distribution distribution, vx_map_id *map_id, void **ptr, vx_enum usage, vx_enum mem_type,
+                            vx_uint32 flags);
+vx_status vxUnmapDistribution(vx_distribution distribution, vx_map_id map_id);
+
+vx_lut vxCreateLUT(vx_context context, vx_enum data_type, vx_size count);
+vx_lut vxCreateVirtualLUT(vx_graph graph, vx_enum data_type, vx_size count);
+vx_status vxReleaseLUT(vx_lut *lut);
+vx_status vxQueryLUT(vx_lut lut, vx_enum attribute, void *ptr, vx_size size);
+vx_status vxCopyLUT(vx_lut lut, void *user_ptr, vx_enum usage, vx_enum user_mem_type);
+vx_status vxMapLUT(vx_lut lut, vx_map_id *map_id, void **ptr, vx_enum usage, vx_enum mem_type, vx_uint32 flags);
+vx_status vxUnmapLUT(vx_lut lut, vx_map_id map_id);
+
 vx_matrix vxCreateMatrix(vx_context c, vx_enum data_type, vx_size columns, vx_size rows);
 vx_status vxReleaseMatrix(vx_matrix *mat);
 vx_status vxQueryMatrix(vx_matrix mat, vx_enum attribute, void *ptr, vx_size size);
@@ -382,6 +407,9 @@ vx_node vxAndNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
 vx_node vxOrNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
 vx_node vxXorNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out);
 vx_node vxNotNode(vx_graph graph, vx_image input, vx_image output);
+vx_node vxTableLookupNode(vx_graph graph, vx_image input, vx_lut lut, vx_image output);
+vx_node vxIntegralImageNode(vx_graph graph, vx_image input, vx_image output);
+vx_node vxHistogramNode(vx_graph graph, vx_image input, vx_distribution distribution);
 vx_node vxChannelCombineNode(vx_graph graph, vx_image plane0, vx_image plane1, vx_image plane2, vx_image plane3,
                              vx_image output);
 

@@ -40,6 +40,7 @@ static const char *kLKNames[] = {
     "ChannelExtract_U8_U24_Pos2", "ChannelExtract_U8_U32_Pos0", "ChannelExtract_U8_U32_Pos1", "ChannelExtract_U8_U32_Pos2",
     "ChannelExtract_U8_U32_Pos3", "ChannelCombine_U16_U8U8", "ChannelCombine_U24_U8U8U8_RGB",
     "ChannelCombine_U32_U8U8U8_UYVY", "ChannelCombine_U32_U8U8U8_YUYV", "ChannelCombine_U32_U8U8U8U8_RGBX",
+    "Lut_U8_U8", "Lut_S16_S16", "IntegralImage_U32_U8", "Histogram_DATA_U8",
 };
 static_assert(sizeof(kLKNames) / sizeof(kLKNames[0]) == (size_t)LK::COUNT, "kernel name table");
 
@@ -180,6 +181,22 @@ vx_status validate_node(Graph *g, Node *n)
         if (idx > 0 && (f == VX_DF_IMAGE_NV12 || f == VX_DF_IMAGE_NV21 || f == VX_DF_IMAGE_IYUV)) { w >>= 1; h >>= 1; }
         if (idx > 0 && (f == VX_DF_IMAGE_YUYV || f == VX_DF_IMAGE_UYVY)) w >>= 1;
         return set_meta(o, w, h, VX_DF_IMAGE_U8);
+    }
+    case VX_KERNEL_HISTOGRAM:                           // agoKernel_Histogram_DATA_U8: ValidateArguments_Img_1IN(U8)
+        if (!fmt_is(p[0], VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
+        return is_valid(p[1], VX_TYPE_DISTRIBUTION) ? VX_SUCCESS : VX_ERROR_INVALID_PARAMETERS;
+    case VX_KERNEL_INTEGRAL_IMAGE:                      // ValidateArguments_Img_1OUT_1IN(U32, U8)
+        if (!fmt_is(p[0], VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
+        return set_meta(img(1), img(0)->width, img(0)->height, VX_DF_IMAGE_U32);
+    case VX_KERNEL_TABLE_LOOKUP: {                      // ovxKernel_TableLookup (ago_kernel_api.cpp)
+        Image *i0 = img(0);
+        if (!is_valid(p[1], VX_TYPE_LUT) || !i0 || !i0->num_planes) return VX_ERROR_INVALID_PARAMETERS;
+        const Lut *l = static_cast<Lut *>(p[1]);
+        const bool u8 = i0->format == VX_DF_IMAGE_U8 && l->data_type == VX_TYPE_UINT8;
+        if (!u8 && !(i0->format == VX_DF_IMAGE_S16 && l->data_type == VX_TYPE_INT16)) return VX_ERROR_INVALID_FORMAT;
+        // a U8 table shorter than 256 entries would be read past its end (undefined): refused
+        if (u8 && l->count != 256) return VX_ERROR_NOT_SUPPORTED;
+        return set_meta(img(2), i0->width, i0->height, i0->format);
     }
     case VX_KERNEL_CHANNEL_COMBINE: {                   // ovxKernel_ChannelCombine (ago_kernel_api.cpp)
         Image *o = img(4);
@@ -404,6 +421,11 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
         }
         return VX_SUCCESS;
     }
+    case VX_KERNEL_INTEGRAL_IMAGE: add(LK::INTEGRAL_IMAGE_U32_U8, {p[1], p[0]}); return VX_SUCCESS;     // :772
+    case VX_KERNEL_HISTOGRAM: add(LK::HISTOGRAM_DATA_U8, {p[1], p[0]}); return VX_SUCCESS;             // :639
+    case VX_KERNEL_TABLE_LOOKUP:                                                                       // :618
+        add(IMG(p[0])->format == VX_DF_IMAGE_U8 ? LK::LUT_U8_U8 : LK::LUT_S16_S16, {p[2], p[0], p[1]});
+        return VX_SUCCESS;
     case VX_KERNEL_CHANNEL_COMBINE: {                                                                  // :416
         Image *o = IMG(p[4]);
         const vx_df_image f = o->format;
@@ -747,7 +769,8 @@ vx_status propagate_valid_rects(Graph *g)
         }
         case LK::COLOR_DEPTH_U8_S16_SAT: case LK::COLOR_DEPTH_U8_S16_WRAP: case LK::COLOR_DEPTH_S16_U8:
         case LK::THRESHOLD_U8_U8_BINARY: case LK::CHANNEL_COPY_U8_U8:
-        case LK::THRESHOLD_U8_U8_RANGE: case LK::NOT_U8_U8:
+        case LK::THRESHOLD_U8_U8_RANGE: case LK::NOT_U8_U8: case LK::LUT_U8_U8: case LK::LUT_S16_S16:
+        case LK::INTEGRAL_IMAGE_U32_U8:
         case LK::CHANNEL_EXTRACT_U8_U16_POS0: case LK::CHANNEL_EXTRACT_U8_U16_POS1: case LK::CHANNEL_EXTRACT_U8_U24_POS0:
         case LK::CHANNEL_EXTRACT_U8_U24_POS1: case LK::CHANNEL_EXTRACT_U8_U24_POS2: case LK::CHANNEL_EXTRACT_U8_U32_POS0:
         case LK::CHANNEL_EXTRACT_U8_U32_POS1: case LK::CHANNEL_EXTRACT_U8_U32_POS2: case LK::CHANNEL_EXTRACT_U8_U32_POS3:

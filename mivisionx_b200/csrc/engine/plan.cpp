@@ -326,6 +326,47 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         };
         return VX_SUCCESS;
     }
+    case LK::HISTOGRAM_DATA_U8: {
+        Distribution *dist = static_cast<Distribution *>(p[0]);
+        if (!dist->dev && cudaMalloc((void **)&dist->dev, dist->bins * sizeof(uint32_t)) != cudaSuccess) return VX_ERROR_NO_MEMORY;
+        uint32_t *hist = dist->dev;
+        const uint8_t *s = dptr(p[1]);
+        const uint32_t w = W(p[1]), h = H(p[1]), ss = dstride(p[1]), bins = (uint32_t)dist->bins, range = dist->range;
+        const int32_t off = dist->offset;
+        st.launch = [=](cudaStream_t q) { return agocuda_Histogram_DATA_U8(S(q), hist, w, h, s, ss, bins, off, range); };
+        return VX_SUCCESS;
+    }
+    case LK::INTEGRAL_IMAGE_U32_U8: {
+        uint32_t *d = (uint32_t *)dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        const size_t sb = agocuda_IntegralImage_scratch_size(w, h);
+        void *scr = scratch(g, sb);
+        if (!scr) return VX_ERROR_NO_MEMORY;
+        st.num_kernels = 3;
+        st.launch = [=](cudaStream_t q) { return agocuda_IntegralImage_U32_U8(S(q), w, h, d, ds, s, ss, scr, sb); };
+        return VX_SUCCESS;
+    }
+    case LK::LUT_U8_U8: case LK::LUT_S16_S16: {
+        // the table's current contents go to device memory with the plan; a changed table
+        // changes the graph's parameter hash and re-plans
+        const Lut *l = static_cast<Lut *>(p[2]);
+        void *tab = scratch(g, l->data.size());
+        if (!tab || cudaMemcpy(tab, l->data.data(), l->data.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return VX_ERROR_NO_MEMORY;
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        if (ln.k == LK::LUT_U8_U8) {
+            const uint8_t *t = (const uint8_t *)tab;
+            st.launch = [=](cudaStream_t q) { return agocuda_Lut_U8_U8(S(q), w, h, d, ds, s, ss, t); };
+        } else {
+            const int16_t *t = (const int16_t *)tab;
+            const uint32_t cnt = (uint32_t)l->count, off = l->offset;
+            st.launch = [=](cudaStream_t q) {
+                return agocuda_Lut_S16_S16(S(q), w, h, (int16_t *)d, ds, (const int16_t *)s, ss, t, cnt, off);
+            };
+        }
+        return VX_SUCCESS;
+    }
     case LK::THRESHOLD_U8_U8_RANGE: {
         uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
         uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);

@@ -48,6 +48,7 @@ static uint64_t param_signature(Graph *g)
             case VX_TYPE_SCALAR: h = fnv(h, &static_cast<Scalar *>(r)->version, 8); h = fnv(h, static_cast<Scalar *>(r)->v.raw, 8); break;
             case VX_TYPE_THRESHOLD: h = fnv(h, &static_cast<Threshold *>(r)->version, 8); break;
             case VX_TYPE_MATRIX: h = fnv(h, &static_cast<Matrix *>(r)->version, 8); break;
+            case VX_TYPE_LUT: h = fnv(h, &static_cast<Lut *>(r)->version, 8); break;
             case VX_TYPE_REMAP: h = fnv(h, &static_cast<Remap *>(r)->version, 8); break;
             case VX_TYPE_IMAGE: {
                 Image *img = IMG(r);
@@ -495,6 +496,8 @@ vx_status graph_process(Graph *g, bool wait)
             static_cast<Array *>(r)->dev_valid = true; static_cast<Array *>(r)->host_valid = false;
         } else if (r->type == VX_TYPE_SCALAR) {
             static_cast<Scalar *>(r)->dev_newer = true;
+        } else if (r->type == VX_TYPE_DISTRIBUTION) {
+            static_cast<Distribution *>(r)->dev_newer = true;
         } else if (r->type == VX_TYPE_PYRAMID) {
             for (Image *lv : static_cast<Pyramid *>(r)->level) { lv->dev_valid = true; lv->host_valid = false; }
         }
@@ -863,6 +866,15 @@ vx_node vxXorNode(vx_graph graph, vx_image in1, vx_image in2, vx_image out)
 
 vx_node vxNotNode(vx_graph graph, vx_image input, vx_image output)
 { return make_node(graph, VX_KERNEL_NOT, {R(input), R(output)}); }
+
+vx_node vxTableLookupNode(vx_graph graph, vx_image input, vx_lut lut, vx_image output)
+{ return make_node(graph, VX_KERNEL_TABLE_LOOKUP, {R(input), R(lut), R(output)}); }
+
+vx_node vxIntegralImageNode(vx_graph graph, vx_image input, vx_image output)
+{ return make_node(graph, VX_KERNEL_INTEGRAL_IMAGE, {R(input), R(output)}); }
+
+vx_node vxHistogramNode(vx_graph graph, vx_image input, vx_distribution distribution)
+{ return make_node(graph, VX_KERNEL_HISTOGRAM, {R(input), R(distribution)}); }
 
 vx_node vxChannelCombineNode(vx_graph graph, vx_image plane0, vx_image plane1, vx_image plane2, vx_image plane3,
                              vx_image output)

@@ -131,6 +131,29 @@ struct Pyramid : Ref {
     std::vector<Image *> level;
 };
 
+// Counts live on the device (written by the histogram kernel) and are read back on demand.
+struct Distribution : Ref {
+    vx_size bins = 0;
+    vx_int32 offset = 0;
+    vx_uint32 range = 0, window = 0;  // window = ceil(range / bins) (ago_util.cpp:2396)
+    std::vector<uint32_t> host;
+    uint32_t *dev = nullptr;
+    bool dev_newer = false;
+    std::map<vx_map_id, vx_enum> maps;
+    vx_map_id next_map = 1;
+    ~Distribution() override;
+};
+
+struct Lut : Ref {
+    vx_enum data_type = VX_TYPE_UINT8;  // UINT8 (count <= 256) or INT16 (count <= 65536)
+    vx_size count = 0;
+    uint32_t offset = 0;              // index of element 0: 0 for UINT8, count / 2 for INT16
+    std::vector<uint8_t> data;
+    uint64_t version = 0;
+    std::map<vx_map_id, vx_enum> maps;
+    vx_map_id next_map = 1;
+};
+
 struct Remap : Ref {
     uint32_t src_width = 0, src_height = 0, dst_width = 0, dst_height = 0;
     std::vector<vx_coordinates2df_t> table;     // dst_width * dst_height
@@ -187,6 +210,7 @@ enum class LK : int {
     CHANNEL_EXTRACT_U8_U24_POS2, CHANNEL_EXTRACT_U8_U32_POS0, CHANNEL_EXTRACT_U8_U32_POS1, CHANNEL_EXTRACT_U8_U32_POS2,
     CHANNEL_EXTRACT_U8_U32_POS3, CHANNEL_COMBINE_U16_U8U8, CHANNEL_COMBINE_U24_U8U8U8_RGB,
     CHANNEL_COMBINE_U32_U8U8U8_UYVY, CHANNEL_COMBINE_U32_U8U8U8_YUYV, CHANNEL_COMBINE_U32_U8U8U8U8_RGBX,
+    LUT_U8_U8, LUT_S16_S16, INTEGRAL_IMAGE_U32_U8, HISTOGRAM_DATA_U8,
     COUNT
 };
 const char *lk_name(LK k);

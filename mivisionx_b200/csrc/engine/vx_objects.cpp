@@ -930,6 +930,198 @@ vx_status vxCopyThresholdRange(vx_threshold thresh, vx_pixel_value_t *lower_valu
     return VX_SUCCESS;
 }
 
+// ---------------------------------------------------------------- distributions
+// vx_api.cpp vxCreateDistribution ("distribution:<bins>,<offset>,<range>", ago_util.cpp:1459)
+Distribution::~Distribution() { if (dev) cudaFree(dev); }
+
+static Distribution *make_distribution(Context *c, Graph *scope, vx_size bins, vx_int32 offset, vx_uint32 range)
+{
+    if (!bins || !range || bins > range) return nullptr;
+    Distribution *d = new Distribution();
+    d->type = VX_TYPE_DISTRIBUTION;
+    d->scope = scope;
+    d->is_virtual = scope != nullptr;
+    d->bins = bins; d->offset = offset; d->range = range;
+    d->window = (vx_uint32)((range + bins - 1) / bins);
+    d->host.assign(bins, 0);
+    add_ref(c, d);
+    return d;
+}
+
+vx_status distribution_sync_to_host(Distribution *d)
+{
+    if (!d->dev_newer || !d->dev) return VX_SUCCESS;
+    if (cudaMemcpy(d->host.data(), d->dev, d->bins * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return VX_FAILURE;
+    d->dev_newer = false;
+    return VX_SUCCESS;
+}
+
+vx_distribution vxCreateDistribution(vx_context context, vx_size numBins, vx_int32 offset, vx_uint32 range)
+{
+    if (!is_valid(context, VX_TYPE_CONTEXT)) return nullptr;
+    return (vx_distribution)make_distribution(as<Context>(context), nullptr, numBins, offset, range);
+}
+
+vx_distribution vxCreateVirtualDistribution(vx_graph graph, vx_size numBins, vx_int32 offset, vx_uint32 range)
+{
+    if (!is_valid(graph, VX_TYPE_GRAPH)) return nullptr;
+    return (vx_distribution)make_distribution(as<Graph>(graph)->ctx, as<Graph>(graph), numBins, offset, range);
+}
+
+vx_status vxReleaseDistribution(vx_distribution *distribution)
+{
+    if (!distribution || !is_valid(*distribution, VX_TYPE_DISTRIBUTION)) return VX_ERROR_INVALID_REFERENCE;
+    vx_status s = release_ref(as<Ref>(*distribution));
+    if (!s) *distribution = nullptr;
+    return s;
+}
+
+vx_status vxQueryDistribution(vx_distribution distribution, vx_enum attribute, void *ptr, vx_size size)
+{
+    CHECK_REF(distribution, VX_TYPE_DISTRIBUTION);
+    Distribution *d = as<Distribution>(distribution);
+    if (!ptr) return VX_ERROR_INVALID_PARAMETERS;
+    switch (attribute) {
+    case VX_DISTRIBUTION_DIMENSIONS: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = 1; return VX_SUCCESS;
+    case VX_DISTRIBUTION_OFFSET: if (size != sizeof(vx_int32)) return VX_ERROR_INVALID_PARAMETERS; *(vx_int32 *)ptr = d->offset; return VX_SUCCESS;
+    case VX_DISTRIBUTION_RANGE: if (size != sizeof(vx_uint32)) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = d->range; return VX_SUCCESS;
+    case VX_DISTRIBUTION_BINS: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = d->bins; return VX_SUCCESS;
+    case VX_DISTRIBUTION_WINDOW: if (size != sizeof(vx_uint32)) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = d->window; return VX_SUCCESS;
+    case VX_DISTRIBUTION_SIZE: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = d->bins * 4; return VX_SUCCESS;
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_status vxCopyDistribution(vx_distribution distribution, void *user_ptr, vx_enum usage, vx_enum user_mem_type)
+{
+    CHECK_REF(distribution, VX_TYPE_DISTRIBUTION);
+    Distribution *d = as<Distribution>(distribution);
+    if (!user_ptr || user_mem_type != VX_MEMORY_TYPE_HOST) return VX_ERROR_INVALID_PARAMETERS;
+    if (usage == VX_READ_ONLY) {
+        if (distribution_sync_to_host(d)) return VX_FAILURE;
+        memcpy(user_ptr, d->host.data(), d->bins * 4);
+    } else if (usage == VX_WRITE_ONLY) {
+        memcpy(d->host.data(), user_ptr, d->bins * 4);
+        d->dev_newer = false;
+    } else {
+        return VX_ERROR_INVALID_PARAMETERS;
+    }
+    return VX_SUCCESS;
+}
+
+vx_status vxMapDistribution(vx_distribution distribution, vx_map_id *map_id, void **ptr, vx_enum usage, vx_enum mem_type,
+                            vx_uint32 flags)
+{
+    (void)flags;
+    CHECK_REF(distribution, VX_TYPE_DISTRIBUTION);
+    Distribution *d = as<Distribution>(distribution);
+    if (!map_id || !ptr || mem_type != VX_MEMORY_TYPE_HOST) return VX_ERROR_INVALID_PARAMETERS;
+    if (distribution_sync_to_host(d)) return VX_FAILURE;
+    *ptr = d->host.data();
+    vx_map_id id = d->next_map++;
+    d->maps[id] = usage;
+    *map_id = id;
+    return VX_SUCCESS;
+}
+
+vx_status vxUnmapDistribution(vx_distribution distribution, vx_map_id map_id)
+{
+    CHECK_REF(distribution, VX_TYPE_DISTRIBUTION);
+    Distribution *d = as<Distribution>(distribution);
+    auto it = d->maps.find(map_id);
+    if (it == d->maps.end()) return VX_ERROR_INVALID_PARAMETERS;
+    d->maps.erase(it);
+    return VX_SUCCESS;
+}
+
+// ---------------------------------------------------------------- LUTs
+// vx_api.cpp:4859-5200 (data description "lut:<type>,<count>", ago_util.cpp:1476: offset 0
+// for UINT8, count / 2 for INT16)
+static Lut *make_lut(Context *c, Graph *scope, vx_enum data_type, vx_size count)
+{
+    if ((data_type != VX_TYPE_UINT8 && data_type != VX_TYPE_INT16) || !count) return nullptr;
+    if ((data_type == VX_TYPE_UINT8 && count > 256) || (data_type == VX_TYPE_INT16 && count > 65536)) return nullptr;
+    Lut *l = new Lut();
+    l->type = VX_TYPE_LUT;
+    l->scope = scope;
+    l->is_virtual = scope != nullptr;
+    l->data_type = data_type; l->count = count;
+    l->offset = data_type == VX_TYPE_INT16 ? (uint32_t)(count / 2) : 0;
+    l->data.assign(count * type_size(data_type), 0);
+    add_ref(c, l);
+    return l;
+}
+
+vx_lut vxCreateLUT(vx_context context, vx_enum data_type, vx_size count)
+{
+    if (!is_valid(context, VX_TYPE_CONTEXT)) return nullptr;
+    return (vx_lut)make_lut(as<Context>(context), nullptr, data_type, count);
+}
+
+vx_lut vxCreateVirtualLUT(vx_graph graph, vx_enum data_type, vx_size count)
+{
+    if (!is_valid(graph, VX_TYPE_GRAPH)) return nullptr;
+    return (vx_lut)make_lut(as<Graph>(graph)->ctx, as<Graph>(graph), data_type, count);
+}
+
+vx_status vxReleaseLUT(vx_lut *lut)
+{
+    if (!lut || !is_valid(*lut, VX_TYPE_LUT)) return VX_ERROR_INVALID_REFERENCE;
+    vx_status s = release_ref(as<Ref>(*lut));
+    if (!s) *lut = nullptr;
+    return s;
+}
+
+vx_status vxQueryLUT(vx_lut lut, vx_enum attribute, void *ptr, vx_size size)
+{
+    CHECK_REF(lut, VX_TYPE_LUT);
+    Lut *l = as<Lut>(lut);
+    if (!ptr) return VX_ERROR_INVALID_PARAMETERS;
+    switch (attribute) {
+    case VX_LUT_TYPE: if (size != sizeof(vx_enum)) return VX_ERROR_INVALID_PARAMETERS; *(vx_enum *)ptr = l->data_type; return VX_SUCCESS;
+    case VX_LUT_COUNT: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = l->count; return VX_SUCCESS;
+    case VX_LUT_SIZE: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = l->data.size(); return VX_SUCCESS;
+    case VX_LUT_OFFSET: if (size != sizeof(vx_uint32)) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = l->offset; return VX_SUCCESS;
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_status vxCopyLUT(vx_lut lut, void *user_ptr, vx_enum usage, vx_enum user_mem_type)
+{
+    CHECK_REF(lut, VX_TYPE_LUT);
+    Lut *l = as<Lut>(lut);
+    if (!user_ptr || user_mem_type != VX_MEMORY_TYPE_HOST) return VX_ERROR_INVALID_PARAMETERS;
+    if (usage == VX_READ_ONLY) memcpy(user_ptr, l->data.data(), l->data.size());
+    else if (usage == VX_WRITE_ONLY) { memcpy(l->data.data(), user_ptr, l->data.size()); l->version++; }
+    else return VX_ERROR_INVALID_PARAMETERS;
+    return VX_SUCCESS;
+}
+
+vx_status vxMapLUT(vx_lut lut, vx_map_id *map_id, void **ptr, vx_enum usage, vx_enum mem_type, vx_uint32 flags)
+{
+    (void)flags;
+    CHECK_REF(lut, VX_TYPE_LUT);
+    Lut *l = as<Lut>(lut);
+    if (!map_id || !ptr || mem_type != VX_MEMORY_TYPE_HOST) return VX_ERROR_INVALID_PARAMETERS;
+    if (usage != VX_READ_ONLY && usage != VX_WRITE_ONLY && usage != VX_READ_AND_WRITE) return VX_ERROR_INVALID_PARAMETERS;
+    *ptr = l->data.data();
+    vx_map_id id = l->next_map++;
+    l->maps[id] = usage;
+    *map_id = id;
+    return VX_SUCCESS;
+}
+
+vx_status vxUnmapLUT(vx_lut lut, vx_map_id map_id)
+{
+    CHECK_REF(lut, VX_TYPE_LUT);
+    Lut *l = as<Lut>(lut);
+    auto it = l->maps.find(map_id);
+    if (it == l->maps.end()) return VX_ERROR_INVALID_PARAMETERS;
+    if (it->second != VX_READ_ONLY) l->version++;
+    l->maps.erase(it);
+    return VX_SUCCESS;
+}
+
 // ---------------------------------------------------------------- matrices
 vx_matrix vxCreateMatrix(vx_context c, vx_enum data_type, vx_size columns, vx_size rows)
 {

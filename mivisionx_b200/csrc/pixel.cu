@@ -753,3 +753,234 @@ extern "C" int agocuda_ChannelCombine_U32_U8U8U8U8_RGBX(void *stream, uint32_t d
     return combine_launch<CH_RGBX>(stream, dstWidth, dstHeight, pDst, dstStride, pSrc1, src1Stride, pSrc2, src2Stride,
                                    pSrc3, src3Stride, pSrc4, src4Stride);
 }
+
+// ---------------------------------------------------------------------------------
+// Table lookup (HafCpu_Lut_U8_U8, ago_haf_cpu_arithmetic.cpp; HafCpu_Lut_S16_S16 :4916)
+// ---------------------------------------------------------------------------------
+namespace {
+
+// U8: the 256-entry table in shared memory, 16 pixels (one 16-byte vector) per thread
+__global__ void __launch_bounds__(kEwBX * kEwBY)
+k_lut_u8(int W, int H, uint8_t *dst, int dstStride, const uint8_t *src, int srcStride, const uint8_t *__restrict__ lut)
+{
+    __shared__ uint8_t tab[256];
+    const int tid = threadIdx.y * kEwBX + threadIdx.x;
+    if (tid < 256) tab[tid] = lut[tid];
+    __syncthreads();
+    const int x = (blockIdx.x * kEwBX + threadIdx.x) * 16;
+    const int y = blockIdx.y * kEwBY + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const uint8_t *s = src + (size_t)y * srcStride + x;
+    uint8_t *d = dst + (size_t)y * dstStride + x;
+    if (x + 16 <= W) {
+        const uint4 v = __ldg((const uint4 *)s);
+        const uint32_t in[4] = {v.x, v.y, v.z, v.w};
+        uint32_t out[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            out[k] = (uint32_t)tab[in[k] & 0xff] | ((uint32_t)tab[(in[k] >> 8) & 0xff] << 8) |
+                     ((uint32_t)tab[(in[k] >> 16) & 0xff] << 16) | ((uint32_t)tab[in[k] >> 24] << 24);
+        *(uint4 *)d = make_uint4(out[0], out[1], out[2], out[3]);
+    } else {
+        for (int i = 0; i < W - x; i++) d[i] = tab[s[i]];
+    }
+}
+
+// S16: table in global memory (cached), index v + offset clamped into the table
+__global__ void __launch_bounds__(kEwBX * kEwBY)
+k_lut_s16(int W, int H, int16_t *dst, int dstStride, const int16_t *src, int srcStride, const int16_t *__restrict__ lut,
+          int count, int offset)
+{
+    const int x = (blockIdx.x * kEwBX + threadIdx.x) * 8;
+    const int y = blockIdx.y * kEwBY + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const int16_t *s = (const int16_t *)((const uint8_t *)src + (size_t)y * srcStride) + x;
+    int16_t *d = (int16_t *)((uint8_t *)dst + (size_t)y * dstStride) + x;
+    auto look = [&](int v) { return __ldg(lut + clampi(v + offset, 0, count - 1)); };
+    if (x + 8 <= W) {
+        const uint4 v = __ldg((const uint4 *)s);
+        const int16_t *e = (const int16_t *)&v;
+        uint4 o;
+        int16_t *oe = (int16_t *)&o;
+#pragma unroll
+        for (int i = 0; i < 8; i++) oe[i] = look(e[i]);
+        *(uint4 *)d = o;
+    } else {
+        for (int i = 0; i < W - x; i++) d[i] = look(s[i]);
+    }
+}
+
+}  // namespace
+
+extern "C" int agocuda_Lut_U8_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                                 const uint8_t *pSrc, uint32_t srcStride, const uint8_t *pLut)
+{
+    if (!dstWidth || !dstHeight || !pLut || !ew_plane_ok(pDst, dstStride, dstWidth) || !ew_plane_ok(pSrc, srcStride, dstWidth))
+        return AGOCUDA_INVALID_PARAMS;
+    dim3 grd(div_up(dstWidth, kEwBX * 16), div_up(dstHeight, kEwBY));
+    k_lut_u8<<<grd, dim3(kEwBX, kEwBY), 0, as_stream(stream)>>>((int)dstWidth, (int)dstHeight, pDst, (int)dstStride, pSrc,
+                                                                (int)srcStride, pLut);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_Lut_S16_S16(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                                   const int16_t *pSrc, uint32_t srcStride, const int16_t *pLut, uint32_t count,
+                                   uint32_t offset)
+{
+    if (!dstWidth || !dstHeight || !pLut || !count || count > 65536 || offset >= count ||
+        !ew_plane_ok(pDst, dstStride, dstWidth) || !ew_plane_ok(pSrc, srcStride, dstWidth))
+        return AGOCUDA_INVALID_PARAMS;
+    dim3 grd(div_up(dstWidth, kEwBX * 8), div_up(dstHeight, kEwBY));
+    k_lut_s16<<<grd, dim3(kEwBX, kEwBY), 0, as_stream(stream)>>>((int)dstWidth, (int)dstHeight, pDst, (int)dstStride, pSrc,
+                                                                 (int)srcStride, pLut, (int)count, (int)offset);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+// ---------------------------------------------------------------------------------
+// Integral image U8 -> U32 (HafCpu_IntegralImage_U32_U8, ago_haf_cpu_arithmetic.cpp:7057):
+// out(x, y) = sum of in(i, j) for i <= x, j <= y, modulo 2^32.  Three launches: row prefix
+// sums (a block per row), column totals of 32-row segments, then each segment's rows get
+// the totals of the segments above plus their running column sum.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr int kIiThreads = 256, kIiSeg = 32;
+
+__global__ void __launch_bounds__(kIiThreads)
+k_integral_rows(int W, uint32_t *dst, int dstStride, const uint8_t *src, int srcStride)
+{
+    __shared__ uint32_t warpSum[kIiThreads / 32];
+    const int y = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int per = (W + kIiThreads - 1) / kIiThreads, x0 = tid * per, x1 = min(x0 + per, W);
+    const uint8_t *s = src + (size_t)y * srcStride;
+    uint32_t *d = (uint32_t *)((uint8_t *)dst + (size_t)y * dstStride);
+    uint32_t sum = 0;
+    for (int x = x0; x < x1; x++) sum += s[x];
+    // exclusive prefix of the threads' sums
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warpSum[warp] = incl;
+    __syncthreads();
+    uint32_t base = 0;
+    for (int w = 0; w < warp; w++) base += warpSum[w];
+    uint32_t run = base + incl - sum;
+    for (int x = x0; x < x1; x++) { run += s[x]; d[x] = run; }
+}
+
+__global__ void __launch_bounds__(kIiThreads)
+k_integral_seg_totals(int W, int H, const uint32_t *dst, int dstStride, uint32_t *totals)
+{
+    const int x = blockIdx.x * kIiThreads + threadIdx.x, seg = blockIdx.y;
+    if (x >= W) return;
+    const int y0 = seg * kIiSeg, y1 = min(y0 + kIiSeg, H);
+    uint32_t t = 0;
+    for (int y = y0; y < y1; y++) t += ((const uint32_t *)((const uint8_t *)dst + (size_t)y * dstStride))[x];
+    totals[(size_t)seg * W + x] = t;
+}
+
+__global__ void __launch_bounds__(kIiThreads)
+k_integral_columns(int W, int H, uint32_t *dst, int dstStride, const uint32_t *totals)
+{
+    const int x = blockIdx.x * kIiThreads + threadIdx.x, seg = blockIdx.y;
+    if (x >= W) return;
+    uint32_t run = 0;
+    for (int s = 0; s < seg; s++) run += totals[(size_t)s * W + x];
+    const int y0 = seg * kIiSeg, y1 = min(y0 + kIiSeg, H);
+    for (int y = y0; y < y1; y++) {
+        uint32_t *p = (uint32_t *)((uint8_t *)dst + (size_t)y * dstStride) + x;
+        run += *p;
+        *p = run;
+    }
+}
+
+}  // namespace
+
+extern "C" size_t agocuda_IntegralImage_scratch_size(uint32_t width, uint32_t height)
+{
+    return (size_t)div_up(height, kIiSeg) * width * sizeof(uint32_t);
+}
+
+extern "C" int agocuda_IntegralImage_U32_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint32_t *pDst,
+                                            uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride, void *scratch,
+                                            size_t scratchBytes)
+{
+    const uint32_t W = dstWidth, H = dstHeight;
+    if (!W || !H || !pDst || !pSrc || ((uintptr_t)pDst & 3) || (dstStride & 3) || dstStride < 4 * W || srcStride < W ||
+        !scratch || scratchBytes < agocuda_IntegralImage_scratch_size(W, H) || H > 65535u * kIiSeg)
+        return AGOCUDA_INVALID_PARAMS;
+    cudaStream_t s = as_stream(stream);
+    uint32_t *tot = (uint32_t *)scratch;
+    k_integral_rows<<<H, kIiThreads, 0, s>>>((int)W, pDst, (int)dstStride, pSrc, (int)srcStride);
+    const dim3 grd(div_up(W, kIiThreads), div_up(H, kIiSeg));
+    k_integral_seg_totals<<<grd, kIiThreads, 0, s>>>((int)W, (int)H, pDst, (int)dstStride, tot);
+    k_integral_columns<<<grd, kIiThreads, 0, s>>>((int)W, (int)H, pDst, (int)dstStride, tot);
+    agocuda_count_launch(3);
+    return agocuda_launch_status();
+}
+
+// ---------------------------------------------------------------------------------
+// Histogram of a U8 image into a distribution (OpenVX binning: v in [offset, offset+range)
+// counts into bin (v - offset) * bins / range).  Blocks count pixel values into per-warp
+// 256-entry shared histograms (16 pixels per load), fold them, and add each value's count to
+// its bin with one global atomic.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr int kHistThreads = 256;
+
+__global__ void __launch_bounds__(kHistThreads)
+k_histogram(int W, int H, const uint8_t *src, int srcStride, uint32_t *hist, int bins, int offset, int range)
+{
+    __shared__ uint32_t sub[kHistThreads / 32][256];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int i = tid; i < (kHistThreads / 32) * 256; i += kHistThreads) (&sub[0][0])[i] = 0;
+    __syncthreads();
+    const int vecs = (W + 15) / 16;                       // 16-pixel groups per row
+    const long long total = (long long)vecs * H;
+    for (long long i = (long long)blockIdx.x * kHistThreads + tid; i < total; i += (long long)gridDim.x * kHistThreads) {
+        const int y = (int)(i / vecs), x = (int)(i - (long long)y * vecs) * 16;
+        const uint8_t *s = src + (size_t)y * srcStride + x;
+        if (x + 16 <= W) {
+            const uint4 v = __ldg((const uint4 *)s);
+            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+#pragma unroll
+                for (int b = 0; b < 4; b++) atomicAdd(&sub[warp][(w[k] >> (8 * b)) & 0xff], 1u);
+        } else {
+            for (int j = 0; j < W - x; j++) atomicAdd(&sub[warp][s[j]], 1u);
+        }
+    }
+    __syncthreads();
+    for (int v = tid; v < 256; v += kHistThreads) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int w = 0; w < kHistThreads / 32; w++) c += sub[w][v];
+        if (c && v >= offset && v < offset + range) atomicAdd(&hist[(long long)(v - offset) * bins / range], c);
+    }
+}
+
+}  // namespace
+
+extern "C" int agocuda_Histogram_DATA_U8(void *stream, uint32_t *pHist, uint32_t srcWidth, uint32_t srcHeight,
+                                         const uint8_t *pSrc, uint32_t srcStride, uint32_t numBins, int32_t offset,
+                                         uint32_t range)
+{
+    if (!pHist || !pSrc || !srcWidth || !srcHeight || !numBins || !range || numBins > range || srcStride < srcWidth ||
+        (((uintptr_t)pSrc | srcStride) & 15) || range > (1u << 30))
+        return AGOCUDA_INVALID_PARAMS;
+    cudaStream_t s = as_stream(stream);
+    if (cudaMemsetAsync(pHist, 0, (size_t)numBins * sizeof(uint32_t), s) != cudaSuccess) return agocuda_launch_status();
+    const long long groups = (long long)div_up(srcWidth, 16) * srcHeight;
+    const int blocks = (int)std::min<long long>(4 * 148, div_up((unsigned)std::min<long long>(groups, 1ll << 31), kHistThreads));
+    k_histogram<<<std::max(1, blocks), kHistThreads, 0, s>>>((int)srcWidth, (int)srcHeight, pSrc, (int)srcStride, pHist,
+                                                             (int)numBins, (int)offset, (int)range);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}

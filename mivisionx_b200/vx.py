@@ -46,6 +46,7 @@ VX_DF_IMAGE_NV12 = _df('N', 'V', '1', '2')
 VX_DF_IMAGE_IYUV = _df('I', 'Y', 'U', 'V')
 VX_DF_IMAGE_VIRT = _df('V', 'I', 'R', 'T')
 VX_DF_IMAGE_F32_AMD = _df('F', '0', '3', '2')
+VX_DF_IMAGE_U32 = _df('U', '0', '3', '2')
 
 VX_CONVERT_POLICY_WRAP = _enum_base(0, 0x0A) + 0
 VX_CONVERT_POLICY_SATURATE = _enum_base(0, 0x0A) + 1
@@ -173,10 +174,15 @@ _SIGS = {
     "vxXorNode": (vp, [vp, vp, vp, vp]), "vxNotNode": (vp, [vp, vp, vp]),
     "vxAddNode": (vp, [vp, vp, vp, i32, vp]), "vxSubtractNode": (vp, [vp, vp, vp, i32, vp]),
     "vxChannelCombineNode": (vp, [vp, vp, vp, vp, vp, vp]),
+    "vxCreateLUT": (vp, [vp, i32, sz]), "vxCopyLUT": (i32, [vp, vp, i32, i32]), "vxQueryLUT": (i32, [vp, i32, vp, sz]),
+    "vxTableLookupNode": (vp, [vp, vp, vp, vp]), "vxIntegralImageNode": (vp, [vp, vp, vp]),
+    "vxCreateDistribution": (vp, [vp, sz, i32, u32]), "vxCopyDistribution": (i32, [vp, vp, i32, i32]),
+    "vxHistogramNode": (vp, [vp, vp, vp]),
 }
 
 _PIX = {VX_DF_IMAGE_U8: (np.uint8, 1), VX_DF_IMAGE_U16: (np.uint16, 1), VX_DF_IMAGE_S16: (np.int16, 1),
-        VX_DF_IMAGE_RGB: (np.uint8, 3), VX_DF_IMAGE_RGBX: (np.uint8, 4), VX_DF_IMAGE_F32_AMD: (np.float32, 1)}
+        VX_DF_IMAGE_RGB: (np.uint8, 3), VX_DF_IMAGE_RGBX: (np.uint8, 4), VX_DF_IMAGE_F32_AMD: (np.float32, 1),
+        VX_DF_IMAGE_U32: (np.uint32, 1)}
 
 
 def image_plane_layout(fmt, width: int, height: int):

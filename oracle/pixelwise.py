@@ -59,6 +59,26 @@ def convert_depth(a, out_dtype, policy_saturate, shift):
     return _wrap_s16(v << shift)
 
 
+def table_lookup(a, table, offset=0):
+    """HafCpu_Lut_U8_U8 / HafCpu_Lut_S16_S16 (ago_haf_cpu_arithmetic.cpp:4916): table[v + offset]
+    (offset 0 for U8 tables, count / 2 for S16 ones)."""
+    return np.asarray(table)[_i32(a) + int(offset)]
+
+
+def integral_image(a):
+    """HafCpu_IntegralImage_U32_U8 (ago_haf_cpu_arithmetic.cpp:7057): sum over [0, x] x [0, y]."""
+    return np.cumsum(np.cumsum(np.asarray(a, np.uint64), axis=0), axis=1).astype(np.uint32)
+
+
+def histogram(a, bins, offset, rng):
+    """OpenVX histogram binning: v in [offset, offset + range) counts into (v - offset) * bins /
+    range.  The reference (HafCpu_HistogramFixedBins_DATA_U8, ago_haf_cpu_histogram.cpp:519)
+    bins by window = ceil(range / bins) in its fast paths, which agrees when range % bins == 0."""
+    v = np.asarray(a, np.int64).ravel()
+    v = v[(v >= offset) & (v < offset + rng)]
+    return np.bincount((v - offset) * bins // rng, minlength=bins).astype(np.uint32)
+
+
 def logical(op, a, b=None):
     """HafCpu_And/Or/Xor_U8_U8U8, HafCpu_Not_U8_U8 (ago_haf_cpu_logical.cpp:518, :31)."""
     a = np.asarray(a, np.uint8)

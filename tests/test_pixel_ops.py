@@ -75,6 +75,11 @@ def _cases():
                     lambda a, s=shift: P.convert_depth(a, np.uint8, True, s)))
         out.append((f"depth_up_{shift}", "depth", (WRAP, shift), (U8,), S16,
                     lambda a, s=shift: P.convert_depth(a, np.int16, False, s)))
+    tab8 = np.random.default_rng(11).integers(0, 256, 256).astype(np.uint8)
+    tab16 = np.random.default_rng(12).integers(-32768, 32768, 65536).astype(np.int16)
+    out.append(("lut_u8", "lut", (V.VX_TYPE_UINT8, tab8), (U8,), U8, lambda a, t=tab8: P.table_lookup(a, t)))
+    out.append(("lut_s16", "lut", (V.VX_TYPE_INT16, tab16), (S16,), S16, lambda a, t=tab16: P.table_lookup(a, t, 32768)))
+    out.append(("integral", "integral", None, (U8,), V.VX_DF_IMAGE_U32, P.integral_image))
     out.append(("range", "range", (37, 201), (U8,), U8, lambda a: P.threshold_range(a, 37, 201)))
     out.append(("range_empty", "range", (200, 100), (U8,), U8, lambda a: P.threshold_range(a, 200, 100)))
     return out
@@ -93,6 +98,13 @@ def _node(api, ctx, g, op, extra, ins, out):
         return f(g, ins[0], ins[1], out)
     if op == "range":
         return api.vxThresholdNode(g, ins[0], api.threshold_range(ctx, *extra), out)
+    if op == "integral":
+        return api.vxIntegralImageNode(g, ins[0], out)
+    if op == "lut":
+        lut = api.obj(api.vxCreateLUT(ctx, extra[0], len(extra[1])), "lut")
+        tab = np.ascontiguousarray(extra[1])
+        api.ok(api.vxCopyLUT(lut, tab.ctypes.data, V.VX_WRITE_ONLY, V.VX_MEMORY_TYPE_HOST), "vxCopyLUT")
+        return api.vxTableLookupNode(g, ins[0], lut, out)
     if op == "depth":
         return api.vxConvertDepthNode(g, ins[0], out, extra[0], api.scalar(ctx, V.VX_TYPE_INT32, extra[1]))
     f = {"not": api.vxNotNode, "box": api.vxBox3x3Node, "median": api.vxMedian3x3Node,
@@ -137,6 +149,10 @@ def _check(name, got, rect, want, w, h):
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
 def test_reference_matches_oracle(case, W, H):
     name, op, extra, fmts, fo, fn = case
+    if name == "lut_s16" and W % 8:
+        # HafCpu_Lut_S16_S16 walks the planes as if rows had no padding (it never applies the
+        # strides), so its rows are misplaced unless the 16-byte-aligned stride equals 2 W
+        pytest.skip("reference S16 table lookup ignores the row stride when W % 8 != 0")
     api = _ref_api()
     arrays = _inputs(op, fmts, W, H)
     got, rect = run_node(api, op, extra, fmts, fo, arrays)
