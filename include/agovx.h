@@ -327,6 +327,14 @@ vx_status vxCopyThresholdValue(vx_threshold thresh, vx_pixel_value_t *value_ptr,
 vx_status vxCopyThresholdRange(vx_threshold thresh, vx_pixel_value_t *lower_value_ptr, vx_pixel_value_t *upper_value_ptr,
                                vx_enum usage, vx_enum user_mem_type);
 
+enum { VX_DELAY_TYPE = VX__A(VX_TYPE_DELAY, 0), VX_DELAY_SLOTS = VX__A(VX_TYPE_DELAY, 1) };
+vx_delay vxCreateDelay(vx_context context, vx_reference exemplar, vx_size num_slots);
+vx_status vxReleaseDelay(vx_delay *delay);
+vx_status vxQueryDelay(vx_delay delay, vx_enum attribute, void *ptr, vx_size size);
+vx_reference vxGetReferenceFromDelay(vx_delay delay, vx_int32 index);
+vx_status vxAgeDelay(vx_delay delay);
+vx_status vxRegisterAutoAging(vx_graph graph, vx_delay delay);
+
 vx_distribution vxCreateDistribution(vx_context context, vx_size numBins, vx_int32 offset, vx_uint32 range);
 vx_distribution vxCreateVirtualDistribution(vx_graph graph, vx_size numBins, vx_int32 offset, vx_uint32 range);
 vx_status vxReleaseDistribution(vx_distribution *distribution);

@@ -133,13 +133,15 @@ static vx_status lk_frame(Graph *g, LNode &ln, agocuda_lk_frame &F, uint32_t &ca
     F.numIterations = static_cast<Scalar *>(p[7])->v.u32;
     F.useInitialEstimate = static_cast<Scalar *>(p[8])->v.b ? 1 : 0;
     F.windowDimension = (int32_t)static_cast<Scalar *>(p[9])->v.sz;
-    // the node's Scharr row-buffer state starts zeroed, like the reference's node scratch
-    void *rows = scratch(g, agocuda_OpticalFlowPyrLK_scharr_rows_size(po->level[0]->width));
+    // the node's Scharr row-buffer state starts zeroed and persists across executions and
+    // re-plans, like the reference's node scratch
+    Node *nd = ln.origin;
+    void *rows = nd->node_state(0, agocuda_OpticalFlowPyrLK_scharr_rows_size(po->level[0]->width));
     if (!rows) return VX_ERROR_NO_MEMORY;
     F.scharrRows = (uint16_t *)rows;
     if (po->levels > 1) {   // level-0 derivative columns carried to the next execution (zeroed: none yet)
         const uint32_t h1 = pyr_level(g, po, 1)->height;
-        void *carry = scratch(g, agocuda_OpticalFlowPyrLK_carry_size((uint32_t)po->levels, h1));
+        void *carry = nd->node_state(1, agocuda_OpticalFlowPyrLK_carry_size((uint32_t)po->levels, h1));
         if (!carry) return VX_ERROR_NO_MEMORY;
         F.carry = (int32_t *)carry;
         F.carryRows = h1;

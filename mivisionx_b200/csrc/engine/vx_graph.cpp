@@ -18,8 +18,39 @@ using namespace agovx;
 
 namespace agovx {
 
+static void plan_state_free(PlanState &ps)
+{
+    if (ps.cexec) cudaGraphExecDestroy(ps.cexec);
+    if (ps.cgraph) cudaGraphDestroy(ps.cgraph);
+    for (void *p : ps.dev_scratch) cudaFree(p);
+    ps = PlanState{};
+}
+
+// move the graph's current plan into `ps` (and the other way round)
+static void plan_state_swap(Graph *g, PlanState &ps)
+{
+    std::swap(g->steps, ps.steps);
+    std::swap(g->dev_scratch, ps.dev_scratch);
+    std::swap(g->cgraph, ps.cgraph);
+    std::swap(g->cexec, ps.cexec);
+    std::swap(g->inputs, ps.inputs);
+    std::swap(g->outputs, ps.outputs);
+    std::swap(g->streamed_in, ps.streamed_in);
+    std::swap(g->streamed_out, ps.streamed_out);
+    std::swap(g->staged_in, ps.staged_in);
+    std::swap(g->staged_out, ps.staged_out);
+    std::swap(g->plan_text, ps.plan_text);
+}
+
+void graph_plan_cache_clear(Graph *g)
+{
+    for (auto &kv : g->plan_cache) plan_state_free(kv.second);
+    g->plan_cache.clear();
+}
+
 void graph_invalidate(Graph *g)
 {
+    graph_plan_cache_clear(g);
     g->verified = false;
     g->state = VX_GRAPH_STATE_UNVERIFIED;
     if (g->cexec) { cudaGraphExecDestroy(g->cexec); g->cexec = nullptr; }
@@ -56,6 +87,11 @@ static uint64_t param_signature(Graph *g)
                 for (int i = 0; i < img->num_planes; i++) h = fnv(h, &img->planes[i].dev, sizeof(void *));
                 break;
             }
+            // storage that ageing a delay moves between objects
+            case VX_TYPE_ARRAY: h = fnv(h, &static_cast<Array *>(r)->dev, sizeof(void *)); break;
+            case VX_TYPE_PYRAMID:
+                for (Image *lv : static_cast<Pyramid *>(r)->level) h = fnv(h, &lv->planes[0].dev, sizeof(void *));
+                break;
             default: break;
             }
         }
@@ -439,13 +475,36 @@ vx_status graph_process(Graph *g, bool wait)
     std::lock_guard<std::recursive_mutex> lk(g->lock);
     const uint64_t t0 = now_ns();
     if (!g->verified) { vx_status s = graph_verify(g); if (s) return s; }
-    // by-value parameters changed since capture: re-plan (valid rects and sizes stay put)
+    // by-value parameters or storage (delay ageing) changed since capture: switch to the
+    // plan made for this signature before, else re-plan (valid rects and sizes stay put)
     if (param_signature(g) != g->param_signature) {
         vx_status s = propagate_valid_rects(g);
-        if (!s) s = plan_graph(g);
-        g->param_signature = param_signature(g);
-        if (!s) s = capture(g);
         if (s) return s;
+        const uint64_t sig = param_signature(g);
+        if (sig != g->param_signature) {
+            constexpr size_t kCachedPlans = 3;
+            PlanState &old = g->plan_cache[g->param_signature];
+            plan_state_free(old);
+            plan_state_swap(g, old);                    // the graph now holds no plan
+            old.use = ++g->plan_uses;
+            auto it = g->plan_cache.find(sig);
+            if (it != g->plan_cache.end()) {
+                plan_state_swap(g, it->second);
+                g->plan_cache.erase(it);
+            } else {
+                s = plan_graph(g);
+                if (!s) s = capture(g);
+            }
+            g->param_signature = sig;
+            while (g->plan_cache.size() > kCachedPlans) {
+                auto lru = g->plan_cache.begin();
+                for (auto i = g->plan_cache.begin(); i != g->plan_cache.end(); ++i)
+                    if (i->second.use < lru->second.use) lru = i;
+                plan_state_free(lru->second);
+                g->plan_cache.erase(lru);
+            }
+            if (s) return s;
+        }
     }
     cudaSetDevice(g->ctx->device);
     for (Ref *r : g->inputs) {
@@ -556,6 +615,8 @@ vx_status graph_wait(Graph *g)
         return VX_FAILURE;
     }
     g->state = VX_GRAPH_STATE_COMPLETED;
+    // vxRegisterAutoAging: age after every completed execution
+    for (Delay *d : g->auto_age) delay_age(d);
     return VX_SUCCESS;
 }
 

@@ -144,6 +144,16 @@ struct Distribution : Ref {
     ~Distribution() override;
 };
 
+// vxCreateDelay: slot objects shaped like the exemplar.  vxGetReferenceFromDelay(-k) is the
+// slot object k; ageing rotates the data storage among the slot objects (AGO's agoAgeDelay
+// likewise moves buffers among the delay's children), so references handed out stay valid
+// and graphs re-plan for the new device pointers.
+struct Delay : Ref {
+    vx_enum item_type = VX_TYPE_INVALID;
+    std::vector<Ref *> slots;
+};
+vx_status delay_age(Delay *d);
+
 struct Lut : Ref {
     vx_enum data_type = VX_TYPE_UINT8;  // UINT8 (count <= 256) or INT16 (count <= 65536)
     vx_size count = 0;
@@ -180,6 +190,12 @@ struct Node : Ref {
     int32_t iparam[2] = {0, 0};       // Canny: gradient_size / norm; Harris: gradient/block size
     vx_enum eparam = 0;               // interpolation / channel / policy / termination
     bool removed = false;
+    // Device state that outlives a plan, as AGO's node scratch (localDataPtr) outlives
+    // executions: LK's Scharr row buffer and level-0 derivative carry.  Zeroed once.
+    void *state[2] = {nullptr, nullptr};
+    size_t state_bytes[2] = {0, 0};
+    void *node_state(int slot, size_t bytes);
+    ~Node() override;
 };
 
 // Low-level AGO kernels (names follow ago/ago_kernels.h) the OpenVX nodes lower to.
@@ -241,6 +257,20 @@ struct Step {
     std::vector<Part> parts;                    // optional split of `launch`, in launch order
 };
 
+// A verified plan and its captured CUDA graph, kept while another plan runs: ageing a delay
+// alternates the graph between a few storage layouts, each with its own plan.
+struct PlanState {
+    std::vector<Step> steps;
+    std::vector<void *> dev_scratch;
+    cudaGraph_t cgraph = nullptr;
+    cudaGraphExec_t cexec = nullptr;
+    std::vector<Ref *> inputs, outputs;
+    std::vector<Image *> streamed_in, streamed_out;
+    std::vector<Array *> staged_in, staged_out;
+    std::string plan_text;
+    uint64_t use = 0;                            // last use, for eviction
+};
+
 struct Graph : Ref {
     std::vector<Node *> nodes;
     std::vector<LNode> lnodes;
@@ -273,6 +303,9 @@ struct Graph : Ref {
     // expiry or capacity overflow; checked after every launch.
     uint32_t *status_host = nullptr, *status_dev = nullptr;
     std::string plan_text;                       // human-readable plan (for tests / debugging)
+    std::vector<Delay *> auto_age;               // delays aged after every execution (vxRegisterAutoAging)
+    std::map<uint64_t, PlanState> plan_cache;    // other plans by parameter signature
+    uint64_t plan_uses = 0;
     std::recursive_mutex lock;
     ~Graph() override;
 };

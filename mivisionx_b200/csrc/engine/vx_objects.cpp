@@ -364,8 +364,11 @@ vx_status scalar_sync_to_host(Scalar *s)
     return VX_SUCCESS;
 }
 
+void graph_plan_cache_clear(Graph *g);
+
 Graph::~Graph()
 {
+    graph_plan_cache_clear(this);
     if (cexec) cudaGraphExecDestroy(cexec);
     if (cgraph) cudaGraphDestroy(cgraph);
     if (ev0) cudaEventDestroy(ev0);
@@ -930,6 +933,24 @@ vx_status vxCopyThresholdRange(vx_threshold thresh, vx_pixel_value_t *lower_valu
     return VX_SUCCESS;
 }
 
+// ---------------------------------------------------------------- node state
+void *Node::node_state(int slot, size_t bytes)
+{
+    if (state[slot] && state_bytes[slot] == bytes) return state[slot];
+    if (state[slot]) cudaFree(state[slot]);
+    state[slot] = nullptr;
+    state_bytes[slot] = 0;
+    if (cudaMalloc(&state[slot], bytes) != cudaSuccess) return nullptr;
+    cudaMemset(state[slot], 0, bytes);
+    state_bytes[slot] = bytes;
+    return state[slot];
+}
+
+Node::~Node()
+{
+    for (void *p : state) if (p) cudaFree(p);
+}
+
 // ---------------------------------------------------------------- distributions
 // vx_api.cpp vxCreateDistribution ("distribution:<bins>,<offset>,<range>", ago_util.cpp:1459)
 Distribution::~Distribution() { if (dev) cudaFree(dev); }
@@ -1412,6 +1433,160 @@ vx_status vxQueryRemap(vx_remap table, vx_enum attribute, void *ptr, vx_size siz
     case VX_REMAP_DESTINATION_HEIGHT: *(vx_uint32 *)ptr = r->dst_height; return VX_SUCCESS;
     default: return VX_ERROR_NOT_SUPPORTED;
     }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- delays
+// vx_api.cpp vxCreateDelay / vxAgeDelay (ago_interface.cpp agoAgeDelay)
+namespace agovx {
+
+static void swap_image_storage(Image *a, Image *b)
+{
+    std::swap(a->planes, b->planes);
+    std::swap(a->host_valid, b->host_valid);
+    std::swap(a->dev_valid, b->dev_valid);
+    std::swap(a->valid, b->valid);
+    for (Image *img : {a, b})
+        for (size_t c = 0; c < img->children.size(); c++) {
+            img->children[c]->planes[0] = img->planes[c];
+            img->children[c]->planes[0].dev_owned = img->children[c]->planes[0].host_owned = false;
+            img->children[c]->dev_valid = img->dev_valid;
+            img->children[c]->host_valid = img->host_valid;
+        }
+}
+
+static void swap_storage(Ref *a, Ref *b)
+{
+    switch (a->type) {
+    case VX_TYPE_IMAGE: swap_image_storage(IMG(a), IMG(b)); break;
+    case VX_TYPE_PYRAMID: {
+        Pyramid *x = static_cast<Pyramid *>(a), *y = static_cast<Pyramid *>(b);
+        for (size_t l = 0; l < x->level.size(); l++) swap_image_storage(x->level[l], y->level[l]);
+        break;
+    }
+    case VX_TYPE_ARRAY: {
+        Array *x = static_cast<Array *>(a), *y = static_cast<Array *>(b);
+        std::swap(x->dev, y->dev);
+        std::swap(x->dev_count, y->dev_count);
+        std::swap(x->host, y->host);
+        std::swap(x->num_items, y->num_items);
+        std::swap(x->host_valid, y->host_valid);
+        std::swap(x->dev_valid, y->dev_valid);
+        std::swap(x->host_mapped, y->host_mapped);
+        break;
+    }
+    case VX_TYPE_SCALAR: {
+        Scalar *x = static_cast<Scalar *>(a), *y = static_cast<Scalar *>(b);
+        std::swap(x->v, y->v);
+        std::swap(x->dev, y->dev);
+        std::swap(x->dev_newer, y->dev_newer);
+        x->version++; y->version++;
+        break;
+    }
+    default: break;
+    }
+}
+
+vx_status delay_age(Delay *d)
+{
+    // the data at index 0 moves to -1, ..., and the oldest slot's storage becomes index 0
+    for (size_t k = d->slots.size() - 1; k > 0; k--) swap_storage(d->slots[k], d->slots[k - 1]);
+    return VX_SUCCESS;
+}
+
+}  // namespace agovx
+
+extern "C" {
+
+vx_delay vxCreateDelay(vx_context context, vx_reference exemplar, vx_size num_slots)
+{
+    if (!is_valid(context, VX_TYPE_CONTEXT) || !is_ref(exemplar) || num_slots < 1) return nullptr;
+    Context *c = as<Context>(context);
+    Ref *ex = as<Ref>(exemplar);
+    Delay *d = new Delay();
+    d->type = VX_TYPE_DELAY;
+    d->item_type = ex->type;
+    for (vx_size k = 0; k < num_slots; k++) {
+        Ref *r = nullptr;
+        switch (ex->type) {
+        case VX_TYPE_IMAGE: {
+            Image *e = IMG(ex);
+            if (!e->width || !e->height || e->format == VX_DF_IMAGE_VIRT) break;
+            r = make_image(c, nullptr, e->width, e->height, e->format, false);
+            break;
+        }
+        case VX_TYPE_PYRAMID: {
+            Pyramid *e = static_cast<Pyramid *>(ex);
+            r = make_pyramid(c, nullptr, e->levels, e->scale, e->width, e->height, e->format, false);
+            break;
+        }
+        case VX_TYPE_ARRAY: {
+            Array *e = static_cast<Array *>(ex);
+            if (e->item_type == VX_TYPE_INVALID) break;
+            Array *a = make_array(c, nullptr, e->item_type, e->capacity, false);
+            a->host.assign(a->capacity * a->item_size, 0);
+            r = a;
+            break;
+        }
+        case VX_TYPE_SCALAR: {
+            Scalar *e = static_cast<Scalar *>(ex);
+            r = make_scalar(c, nullptr, e->data_type, e->v.raw);
+            break;
+        }
+        default: break;
+        }
+        if (!r) { for (Ref *s : d->slots) release_ref(s); delete d; return nullptr; }
+        r->ext_count = 0;
+        r->int_count = 1;          // held by the delay
+        d->slots.push_back(r);
+    }
+    add_ref(c, d);
+    return (vx_delay)d;
+}
+
+vx_status vxReleaseDelay(vx_delay *delay)
+{
+    if (!delay || !is_valid(*delay, VX_TYPE_DELAY)) return VX_ERROR_INVALID_REFERENCE;
+    vx_status s = release_ref(as<Ref>(*delay));
+    if (!s) *delay = nullptr;
+    return s;
+}
+
+vx_status vxQueryDelay(vx_delay delay, vx_enum attribute, void *ptr, vx_size size)
+{
+    CHECK_REF(delay, VX_TYPE_DELAY);
+    Delay *d = as<Delay>(delay);
+    if (!ptr) return VX_ERROR_INVALID_PARAMETERS;
+    switch (attribute) {
+    case VX_DELAY_TYPE: if (size != sizeof(vx_enum)) return VX_ERROR_INVALID_PARAMETERS; *(vx_enum *)ptr = d->item_type; return VX_SUCCESS;
+    case VX_DELAY_SLOTS: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = d->slots.size(); return VX_SUCCESS;
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_reference vxGetReferenceFromDelay(vx_delay delay, vx_int32 index)
+{
+    if (!is_valid(delay, VX_TYPE_DELAY)) return nullptr;
+    Delay *d = as<Delay>(delay);
+    if (index > 0 || -index >= (vx_int32)d->slots.size()) return nullptr;
+    return (vx_reference)d->slots[-index];
+}
+
+vx_status vxAgeDelay(vx_delay delay)
+{
+    CHECK_REF(delay, VX_TYPE_DELAY);
+    return delay_age(as<Delay>(delay));
+}
+
+vx_status vxRegisterAutoAging(vx_graph graph, vx_delay delay)
+{
+    CHECK_REF(graph, VX_TYPE_GRAPH);
+    CHECK_REF(delay, VX_TYPE_DELAY);
+    Graph *g = as<Graph>(graph);
+    if (std::find(g->auto_age.begin(), g->auto_age.end(), as<Delay>(delay)) == g->auto_age.end())
+        g->auto_age.push_back(as<Delay>(delay));
+    return VX_SUCCESS;
 }
 
 }  // extern "C"

@@ -178,6 +178,8 @@ _SIGS = {
     "vxTableLookupNode": (vp, [vp, vp, vp, vp]), "vxIntegralImageNode": (vp, [vp, vp, vp]),
     "vxCreateDistribution": (vp, [vp, sz, i32, u32]), "vxCopyDistribution": (i32, [vp, vp, i32, i32]),
     "vxHistogramNode": (vp, [vp, vp, vp]),
+    "vxCreateDelay": (vp, [vp, vp, sz]), "vxGetReferenceFromDelay": (vp, [vp, i32]), "vxAgeDelay": (i32, [vp]),
+    "vxRegisterAutoAging": (i32, [vp, vp]), "vxQueryDelay": (i32, [vp, i32, vp, sz]),
 }
 
 _PIX = {VX_DF_IMAGE_U8: (np.uint8, 1), VX_DF_IMAGE_U16: (np.uint16, 1), VX_DF_IMAGE_S16: (np.int16, 1),
