@@ -223,6 +223,16 @@ typedef struct {
     vx_uint32 device_info, group, reserved;
 } AgoTargetAffinityInfo;
 
+/* VX_GRAPH_ATTRIBUTE_AMD_IMPORT_FROM_TEXT argument (vx_ext_amd.h AgoGraphImportInfo) */
+typedef struct {
+    vx_char *text;
+    vx_uint32 num_ref;
+    vx_reference *ref;
+    vx_int32 dumpToConsole;
+    void (*data_registry_callback_f)(void *obj, vx_reference ref, const char *name, const char *app_params);
+    void *data_registry_callback_obj;
+} AgoGraphImportInfo;
+
 /* kernels (vx_kernels.h) */
 #define VX__K(n) (VX_KERNEL_BASE(VX_ID_KHRONOS, 0) + (n))
 enum vx_kernel_e {

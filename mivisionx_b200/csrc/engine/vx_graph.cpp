@@ -628,6 +628,22 @@ vx_status graph_wait(Graph *g)
 template <class T> static T *as(void *h) { return static_cast<T *>(static_cast<Ref *>(h)); }
 #define CHECK_REF(h, T) if (!is_valid(h, T)) return VX_ERROR_INVALID_REFERENCE
 
+namespace agovx {
+Node *graph_add_node(Graph *g, vx_enum kernel, const std::vector<Ref *> &params)
+{
+    Node *n = new Node();
+    n->type = VX_TYPE_NODE;
+    n->scope = g;
+    n->kernel = kernel;
+    n->params = params;
+    for (Ref *r : n->params) retain_internal(r);
+    add_ref(g->ctx, n);
+    g->nodes.push_back(n);
+    graph_invalidate(g);
+    return n;
+}
+}  // namespace agovx
+
 extern "C" {
 
 vx_graph vxCreateGraph(vx_context context)
@@ -719,6 +735,13 @@ vx_status vxSetGraphAttribute(vx_graph graph, vx_enum attribute, const void *ptr
         if (size != sizeof(AgoTargetAffinityInfo)) return VX_ERROR_INVALID_PARAMETERS;
         g->affinity = ((const AgoTargetAffinityInfo *)ptr)->device_type;
         return VX_SUCCESS;   // every node runs on the GPU target; CPU affinity is accepted and ignored
+    case VX_GRAPH_ATTRIBUTE_AMD_IMPORT_FROM_TEXT: {     // vx_api.cpp:3183
+        if (size != sizeof(AgoGraphImportInfo) || !ptr) return VX_ERROR_INVALID_PARAMETERS;
+        std::lock_guard<std::recursive_mutex> lk(g->lock);
+        vx_status s = graph_import_text(g, (const AgoGraphImportInfo *)ptr);
+        graph_invalidate(g);
+        return s ? VX_FAILURE : VX_SUCCESS;
+    }
     default: return VX_ERROR_NOT_SUPPORTED;
     }
 }
@@ -818,6 +841,7 @@ static vx_node make_node(vx_graph graph, vx_enum kernel, std::initializer_list<R
     graph_invalidate(g);
     return (vx_node)n;
 }
+
 
 static Ref *scalar_of(vx_graph graph, vx_enum type, const void *v)
 {

@@ -153,6 +153,8 @@ struct Delay : Ref {
     std::vector<Ref *> slots;
 };
 vx_status delay_age(Delay *d);
+struct Graph;
+vx_status graph_import_text(Graph *g, const AgoGraphImportInfo *info);
 
 struct Lut : Ref {
     vx_enum data_type = VX_TYPE_UINT8;  // UINT8 (count <= 256) or INT16 (count <= 65536)

@@ -86,6 +86,7 @@ VX_THRESHOLD_THRESHOLD_UPPER = _attr_base(0, 0x80A) + 3
 VX_GRAPH_ATTRIBUTE_AMD_AFFINITY = _attr_base(VX_ID_AMD, VX_TYPE_GRAPH) + 0x01
 VX_GRAPH_ATTRIBUTE_AMD_EXPORT_TO_TEXT = _attr_base(VX_ID_AMD, VX_TYPE_GRAPH) + 0x03
 VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS = _attr_base(VX_ID_AMD, VX_TYPE_GRAPH) + 0x04
+VX_GRAPH_ATTRIBUTE_AMD_IMPORT_FROM_TEXT = _attr_base(VX_ID_AMD, VX_TYPE_GRAPH) + 0x02
 VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_LAST = _attr_base(VX_ID_AMD, VX_TYPE_GRAPH) + 0x05
 AGO_TARGET_AFFINITY_CPU, AGO_TARGET_AFFINITY_GPU = 0x10, 0x20
 
@@ -125,6 +126,15 @@ class vx_border_t(C.Structure):
 
 class vx_perf_t(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("tmp", "beg", "end", "sum", "avg", "min", "num", "max")]
+
+
+GDF_CALLBACK = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_char_p, C.c_char_p)
+
+
+class AgoGraphImportInfo(C.Structure):
+    _fields_ = [("text", C.c_char_p), ("num_ref", C.c_uint32), ("ref", C.POINTER(C.c_void_p)),
+                ("dumpToConsole", C.c_int32), ("data_registry_callback_f", GDF_CALLBACK),
+                ("data_registry_callback_obj", C.c_void_p)]
 
 
 class AgoTargetAffinityInfo(C.Structure):
@@ -272,6 +282,26 @@ class OpenVX:
     def set_graph_affinity(self, graph, device_type):
         a = AgoTargetAffinityInfo(device_type, 0, 0, 0)
         return self.vxSetGraphAttribute(graph, VX_GRAPH_ATTRIBUTE_AMD_AFFINITY, C.byref(a), C.sizeof(a))
+
+    def import_gdf(self, graph, text: str, on_data=None, refs=()):
+        """Read a text graph description into `graph` (VX_GRAPH_ATTRIBUTE_AMD_IMPORT_FROM_TEXT).
+        Returns (status, {name: (reference, params)}) for the data that carry `:<params>` (the
+        data registry callback of the reference's importer); `on_data(ref, name, params)` runs
+        inside that callback, while the text is read (where runvx applies INIT requests);
+        `refs` are the references `$1`, `$2`, ... of the text."""
+        found = {}
+
+        def cb(obj, ref, name, params):
+            found[name.decode()] = (ref, params.decode())
+            if on_data is not None:
+                on_data(ref, name.decode(), params.decode())
+
+        fn = GDF_CALLBACK(cb)
+        arr = (C.c_void_p * max(1, len(refs)))(*refs)
+        info = AgoGraphImportInfo(text.encode(), len(refs), C.cast(arr, C.POINTER(C.c_void_p)) if refs else None, 0, fn,
+                                  None)
+        st = self.vxSetGraphAttribute(graph, VX_GRAPH_ATTRIBUTE_AMD_IMPORT_FROM_TEXT, C.byref(info), C.sizeof(info))
+        return st, found
 
     def plan(self, graph):
         """The verified execution plan of a graph on this target: [(step name, kernels per run)]."""
