@@ -100,6 +100,25 @@ int agocuda_CannySobel_U16_U8_3x3_L1NORM(void *stream, uint32_t dstWidth, uint32
                                          uint16_t *pDst, uint32_t dstStride,
                                          const uint8_t *pSrc, uint32_t srcStride);
 
+/* Packed Canny gradients of the other window sizes and norms, same layout; rows [R, H-R)
+ * written (R = 1, 2, 3), the rest 0.  Each column follows the reference's own formula for
+ * it (SIMD body for x < W - W % 16 - 1, scalar code after), including the body's reads of
+ * its zeroed row scratch past the aligned width and the 7x7 body's quarter-scale sums.
+ * Replace HipExec_CannySobel_U16_U8_{3x3_L2,5x5_L1,5x5_L2,7x7_L1,7x7_L2}NORM
+ * (hipvx/hip_host_decls.h:828-851); HafCpu_CannySobel_U16_U8_3x3_L2NORM
+ * (ago_haf_cpu_canny.cpp:646), _5x5_L1NORM (:145), _5x5_L2NORM (:756), _7x7_L1NORM (:272),
+ * _7x7_L2NORM (:893). */
+int agocuda_CannySobel_U16_U8_3x3_L2NORM(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint16_t *pDst,
+                                         uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_CannySobel_U16_U8_5x5_L1NORM(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint16_t *pDst,
+                                         uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_CannySobel_U16_U8_5x5_L2NORM(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint16_t *pDst,
+                                         uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_CannySobel_U16_U8_7x7_L1NORM(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint16_t *pDst,
+                                         uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+int agocuda_CannySobel_U16_U8_7x7_L2NORM(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint16_t *pDst,
+                                         uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride);
+
 /* Non-maximum suppression + double threshold (255 / 127 / 0) on [1,W-1)x[1,H-1); strong
  * pixels are appended to pStack as (y << 16 | x) (the layout of ago_coord2d_ushort_t), in no
  * particular order, *pStackCount set to their number.  Replaces

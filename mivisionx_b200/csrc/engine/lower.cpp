@@ -41,6 +41,8 @@ static const char *kLKNames[] = {
     "ChannelExtract_U8_U32_Pos3", "ChannelCombine_U16_U8U8", "ChannelCombine_U24_U8U8U8_RGB",
     "ChannelCombine_U32_U8U8U8_UYVY", "ChannelCombine_U32_U8U8U8_YUYV", "ChannelCombine_U32_U8U8U8U8_RGBX",
     "Lut_U8_U8", "Lut_S16_S16", "IntegralImage_U32_U8", "Histogram_DATA_U8",
+    "CannySobel_U16_U8_5x5_L1NORM", "CannySobel_U16_U8_5x5_L2NORM", "CannySobel_U16_U8_7x7_L1NORM",
+    "CannySobel_U16_U8_7x7_L2NORM", "CannySuppThreshold_U8XY_U16_7x7",
 };
 static_assert(sizeof(kLKNames) / sizeof(kLKNames[0]) == (size_t)LK::COUNT, "kernel name table");
 
@@ -146,8 +148,12 @@ vx_status validate_node(Graph *g, Node *n)
     case VX_KERNEL_CANNY_EDGE_DETECTOR: {
         if (!fmt_is(p[0], VX_DF_IMAGE_U8) || !is_valid(p[1], VX_TYPE_THRESHOLD)) return VX_ERROR_INVALID_PARAMETERS;
         if (static_cast<Threshold *>(p[1])->thresh_type != VX_THRESHOLD_TYPE_RANGE) return VX_ERROR_INVALID_TYPE;
-        if (sc_i32(p[2]) != 3) return VX_ERROR_NOT_SUPPORTED;   // gradient sizes 5/7 are outside this target
-        if (sc_enum(p[3]) != VX_NORM_L1) return sc_enum(p[3]) == VX_NORM_L2 ? VX_ERROR_NOT_SUPPORTED : VX_ERROR_INVALID_VALUE;
+        const int gs = sc_i32(p[2]);
+        if (gs != 3 && gs != 5 && gs != 7) return VX_ERROR_INVALID_VALUE;
+        if (sc_enum(p[3]) != VX_NORM_L1 && sc_enum(p[3]) != VX_NORM_L2) return VX_ERROR_INVALID_VALUE;
+        // the 3x3 L2 / 5x5 / 7x7 gradient kernels exist (agocuda_CannySobel_*) but graphs
+        // using them are not enabled yet: a later context release aborted after them
+        if (gs != 3 || sc_enum(p[3]) != VX_NORM_L1) return VX_ERROR_NOT_SUPPORTED;
         return set_meta(img(4), img(0)->width, img(0)->height, VX_DF_IMAGE_U8);
     }
     case VX_KERNEL_HARRIS_CORNERS: {
@@ -367,8 +373,14 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
         Array *stack = virt_array(g, kItemCoord2dU16, (vx_size)i0->width * i0->height);
         stack->item_size = 4;
         Image *sob = virt_image(g, i0->width, i0->height, VX_DF_IMAGE_U16);
-        add(sc_enum(p[3]) == VX_NORM_L1 ? LK::CANNY_SOBEL_U16_U8_3x3_L1NORM : LK::CANNY_SOBEL_U16_U8_3x3_L2NORM, {sob, p[0]});
-        add(LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3, {p[4], stack, sob, p[1], p[2]});
+        const int gs = sc_i32(p[2]);
+        const bool l1 = sc_enum(p[3]) == VX_NORM_L1;
+        const LK sobel = gs == 3 ? (l1 ? LK::CANNY_SOBEL_U16_U8_3x3_L1NORM : LK::CANNY_SOBEL_U16_U8_3x3_L2NORM)
+                       : gs == 5 ? (l1 ? LK::CANNY_SOBEL_U16_U8_5x5_L1NORM : LK::CANNY_SOBEL_U16_U8_5x5_L2NORM)
+                                 : (l1 ? LK::CANNY_SOBEL_U16_U8_7x7_L1NORM : LK::CANNY_SOBEL_U16_U8_7x7_L2NORM);
+        add(sobel, {sob, p[0]});
+        // 7x7 gradients use the suppression variant that quarters the thresholds (:1690)
+        add(gs == 7 ? LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7 : LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3, {p[4], stack, sob, p[1], p[2]});
         add(LK::CANNY_EDGE_TRACE_U8_U8XY, {p[4], stack});
         return VX_SUCCESS;
     }
@@ -508,12 +520,17 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
 // ------------------------------------------------------------------------------------
 // data usage bookkeeping
 // ------------------------------------------------------------------------------------
+static bool is_canny_supp(LK k)
+{
+    return k == LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3 || k == LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7;
+}
+
 static int num_outputs(LK k)
 {
     switch (k) {
     case LK::SOBEL_S16S16_U8_3x3_GXY: case LK::COLOR_CONVERT_NV12_RGB: return 2;
     case LK::COLOR_CONVERT_IYUV_RGB: return 3;
-    case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: return 2;
+    case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7: return 2;
     case LK::HARRIS_MERGE_SORT_AND_PICK_XY_XYS: return 2;
     default: return 1;
     }
@@ -658,7 +675,7 @@ static vx_status sort_lnodes(Graph *g)
         for (int k = 0; k < num_outputs(live[i].k); k++) {
             Ref *o = live[i].p[k];
             if (!o) continue;
-            if (writer.count(o) && live[i].k != LK::CANNY_EDGE_TRACE_U8_U8XY && live[writer[o]].k != LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3)
+            if (writer.count(o) && live[i].k != LK::CANNY_EDGE_TRACE_U8_U8XY && !is_canny_supp(live[writer[o]].k))
                 return VX_ERROR_MULTIPLE_WRITERS;
             // edge trace updates the image written by suppression: it runs after it
             if (!writer.count(o) || live[i].k == LK::CANNY_EDGE_TRACE_U8_U8XY) writer[o] = (int)i;
@@ -682,7 +699,7 @@ static vx_status sort_lnodes(Graph *g)
         }
         if (live[i].k == LK::CANNY_EDGE_TRACE_U8_U8XY) {
             for (size_t j = 0; j < n; j++)
-                if (live[j].k == LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3 && live[j].p[0] == live[i].p[0]) {
+                if (is_canny_supp(live[j].k) && live[j].p[0] == live[i].p[0]) {
                     int l = lev(j, depth + 1);
                     if (l < 0) return -2;
                     lv = std::max(lv, l + 1);
@@ -760,7 +777,11 @@ vx_status propagate_valid_rects(Graph *g)
         case LK::SOBEL_S16S16_U8_3x3_GXY:
             // ago_kernel_api.cpp:16154 clamps with the input's size
             shrink_from(I(0), I(2), 1); shrink_from(I(1), I(2), 1); break;
-        case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: shrink_from(I(0), I(2), 1); break;
+        case LK::CANNY_SOBEL_U16_U8_5x5_L1NORM: case LK::CANNY_SOBEL_U16_U8_5x5_L2NORM:   // :17701
+            shrink_from(I(0), I(1), 2); break;
+        case LK::CANNY_SOBEL_U16_U8_7x7_L1NORM: case LK::CANNY_SOBEL_U16_U8_7x7_L2NORM:
+            shrink_from(I(0), I(1), 3); break;
+        case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7: shrink_from(I(0), I(2), 1); break;
         case LK::MAGNITUDE_S16_S16S16: {
             Image *o = I(0), *a = I(1), *b = I(2);
             o->valid = vx_rectangle_t{std::max(a->valid.start_x, b->valid.start_x), std::max(a->valid.start_y, b->valid.start_y),

@@ -423,12 +423,27 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         st.launch = [=](cudaStream_t q) { return agocuda_CannySobel_U16_U8_3x3_L1NORM(S(q), w, h, d, ds, s, ss); };
         return VX_SUCCESS;
     }
-    case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: {
+#define CANNY_SOBEL(K, FN)                                                                                      \
+    case LK::K: {                                                                                               \
+        uint16_t *d = (uint16_t *)dptr(p[0]); const uint8_t *s = dptr(p[1]);                                   \
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);                             \
+        st.launch = [=](cudaStream_t q) { return FN(S(q), w, h, d, ds, s, ss); };                              \
+        return VX_SUCCESS;                                                                                      \
+    }
+    CANNY_SOBEL(CANNY_SOBEL_U16_U8_3x3_L2NORM, agocuda_CannySobel_U16_U8_3x3_L2NORM)
+    CANNY_SOBEL(CANNY_SOBEL_U16_U8_5x5_L1NORM, agocuda_CannySobel_U16_U8_5x5_L1NORM)
+    CANNY_SOBEL(CANNY_SOBEL_U16_U8_5x5_L2NORM, agocuda_CannySobel_U16_U8_5x5_L2NORM)
+    CANNY_SOBEL(CANNY_SOBEL_U16_U8_7x7_L1NORM, agocuda_CannySobel_U16_U8_7x7_L1NORM)
+    CANNY_SOBEL(CANNY_SOBEL_U16_U8_7x7_L2NORM, agocuda_CannySobel_U16_U8_7x7_L2NORM)
+#undef CANNY_SOBEL
+    case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7: {
         uint8_t *d = dptr(p[0]); Array *stk = static_cast<Array *>(p[1]); const uint16_t *s = (const uint16_t *)dptr(p[2]);
         Threshold *t = static_cast<Threshold *>(p[3]);
         uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[2]);
-        // threshold_lower/upper .U1 passed as vx_uint16 (ago_kernel_api.cpp:17967)
-        uint16_t lo = (uint16_t)t->lower.U32, hi = (uint16_t)t->upper.U32;
+        // threshold_lower/upper .U1 passed as vx_uint16 (ago_kernel_api.cpp:17967); the 7x7
+        // variant divides both by 4 first (ago_kernel_api.cpp:18035)
+        const int32_t q4 = ln.k == LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7 ? 4 : 1;
+        uint16_t lo = (uint16_t)((int32_t)t->lower.U32 / q4), hi = (uint16_t)((int32_t)t->upper.U32 / q4);
         uint32_t *stack = (uint32_t *)stk->dev, *cnt = stk->dev_count; uint32_t cap = (uint32_t)stk->capacity;
         st.launch = [=](cudaStream_t q) {
             return agocuda_CannySuppThreshold_U8XY_U16_3x3(S(q), w, h, d, ds, s, ss, stack, cnt, cap, lo, hi);

@@ -229,6 +229,8 @@ enum class LK : int {
     CHANNEL_EXTRACT_U8_U32_POS3, CHANNEL_COMBINE_U16_U8U8, CHANNEL_COMBINE_U24_U8U8U8_RGB,
     CHANNEL_COMBINE_U32_U8U8U8_UYVY, CHANNEL_COMBINE_U32_U8U8U8_YUYV, CHANNEL_COMBINE_U32_U8U8U8U8_RGBX,
     LUT_U8_U8, LUT_S16_S16, INTEGRAL_IMAGE_U32_U8, HISTOGRAM_DATA_U8,
+    CANNY_SOBEL_U16_U8_5x5_L1NORM, CANNY_SOBEL_U16_U8_5x5_L2NORM, CANNY_SOBEL_U16_U8_7x7_L1NORM,
+    CANNY_SOBEL_U16_U8_7x7_L2NORM, CANNY_SUPP_THRESHOLD_U8XY_U16_7x7,
     COUNT
 };
 const char *lk_name(LK k);

@@ -857,13 +857,12 @@ vx_status vxReleaseThreshold(vx_threshold *thresh)
     return s;
 }
 
-static void set_pixel_int(vx_pixel_value_t &v, int32_t x, vx_enum dt)
+// The reference keeps the whole 32-bit value whatever the data type (vx_api.cpp:6328 copies
+// the pixel union); kernels read the view they need (U8 = low byte, Canny the 32-bit one).
+static void set_pixel_int(vx_pixel_value_t &v, int32_t x, vx_enum)
 {
     memset(&v, 0, sizeof(v));
-    if (dt == VX_TYPE_INT16) v.S16 = (vx_int16)x;
-    else if (dt == VX_TYPE_UINT16) v.U16 = (vx_uint16)x;
-    else if (dt == VX_TYPE_UINT8) v.U8 = (vx_uint8)x;
-    else v.S32 = x;
+    v.S32 = x;
 }
 
 static int32_t get_pixel_int(const vx_pixel_value_t &v, vx_enum dt)

@@ -116,6 +116,138 @@ __global__ void k_canny_sobel(int W, int H, uint16_t *dst, int dstStride, const 
     d[x] = canny_grad(P, simd_x0, r1m);
 }
 
+// ---------------------------------------------------------------------------------
+// Canny gradients with 3x3 L2, 5x5 and 7x7 windows (HafCpu_CannySobel_U16_U8_5x5_L1NORM
+// ago_haf_cpu_canny.cpp:145, _7x7_L1NORM :272, _3x3_L2NORM :646, _5x5_L2NORM :756,
+// _7x7_L2NORM :893).  The reference splits each row into SIMD columns [0, A - 1),
+// A = W - W % 16, computed from per-row vertical sums r0 / r1 held in zeroed node scratch
+// (r0 at +16 bytes, r1 right after, ALIGN16(W) entries each), and scalar columns from A - 1
+// on; the two formulas differ per variant (16-bit squares for 3x3 L2, a quarter-scale
+// saturating body for 7x7, Gy signs, a sign slip in the 5x5 L2 scalar top row), and the
+// SIMD part reads r0 / r1 up to R columns outside [0, A).  Each thread evaluates the
+// formula of its column, with those scratch reads resolved to the values they find there.
+// ---------------------------------------------------------------------------------
+template <int G> struct CannyWin;
+template <> struct CannyWin<3> { __device__ static int v(int k) { return k == 0 ? 2 : 1; }
+                                 __device__ static int d(int k) { return k; } };
+template <> struct CannyWin<5> { __device__ static int v(int k) { const int a = k < 0 ? -k : k; return a == 0 ? 6 : (a == 1 ? 4 : 1); }
+                                 __device__ static int d(int k) { return k == 0 ? 0 : (k < 0 ? -1 : 1) * ((k < 0 ? -k : k) == 1 ? 2 : 1); } };
+template <> struct CannyWin<7> { __device__ static int v(int k) { const int a = k < 0 ? -k : k; return a == 0 ? 20 : (a == 1 ? 15 : (a == 2 ? 6 : 1)); }
+                                 __device__ static int d(int k) { const int a = k < 0 ? -k : k; const int m = a == 0 ? 0 : (a == 1 ? 5 : (a == 2 ? 4 : 1)); return k < 0 ? -m : m; } };
+
+__device__ __forceinline__ int16_t cw16(int v) { return (int16_t)v; }
+__device__ __forceinline__ int16_t cs16(int v) { return (int16_t)max(-32768, min(32767, v)); }
+__device__ __forceinline__ int16_t cabs16(int16_t v) { return (int16_t)(v < 0 ? -(int)v : (int)v); }
+
+// a source pixel as a read at flat offset (y * L + x) of an AGO-laid-out U8 buffer (row
+// pitch L = ALIGN16(W), zero padding) finds it; 0 outside the buffer
+__device__ __forceinline__ int ago_flat_px(const uint8_t *src, int stride, int W, int H, int L, int x, int y)
+{
+    const long f = (long)y * L + x;
+    if (f < 0 || f >= (long)H * L) return 0;
+    const int yy = (int)(f / L), xx = (int)(f - (long)yy * L);
+    return xx < W ? src[(size_t)yy * stride + xx] : 0;
+}
+
+template <int G>
+struct CannyRowSums {
+    const uint8_t *s; int stride, y, A, L;
+    __device__ int vsum(int c, bool diff) const {
+        int a = 0;
+#pragma unroll
+        for (int k = -G / 2; k <= G / 2; k++)
+            a += (diff ? CannyWin<G>::d(k) : CannyWin<G>::v(k)) * s[(size_t)(y + k) * stride + c];
+        a = cw16(a);
+        return G == 7 ? (a >> 2) : a;
+    }
+    __device__ int r1(int c) const {
+        if (c < 0) { c += L; return c < A ? vsum(c, false) : 0; }   // r1[-k] is r0[L - k]
+        return c < A ? vsum(c, true) : 0;                            // unwritten or past r1: zero scratch
+    }
+    __device__ int r0(int c) const {
+        if (c < 0) return 0;                                         // the 16 zero bytes before r0
+        if (c < A) return vsum(c, false);
+        if (c < L) return 0;
+        return r1(c - L);                                            // r0[L + k] is r1[k]
+    }
+};
+
+__device__ __forceinline__ uint16_t canny_l2_pack(int16_t gx, int16_t gy, bool body3)
+{
+    float f;
+    if (body3)
+        f = __fadd_rn((float)(uint16_t)(gx * gx), (float)(uint16_t)(gy * gy));
+    else
+        f = __int2float_rn((int32_t)((uint32_t)(gx * gx) + (uint32_t)(gy * gy)));
+    int m = __float2int_rn(__fsqrt_rn(f));
+    m = max(0, min(65535, m));
+    return (uint16_t)((uint16_t)(m << 2) | canny_dir(gx, gy));
+}
+
+template <int G, bool L2>
+__global__ void k_canny_sobel_nxn(int W, int H, uint16_t *dst, int dstStride, const uint8_t *src, int srcStride)
+{
+    constexpr int R = G / 2;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    uint16_t *d = (uint16_t *)((uint8_t *)dst + (size_t)y * dstStride);
+    if (y < R || y >= H - R) { d[x] = 0; return; }
+    const int L = (W + 15) & ~15, A = W - (W & 15);
+    if (x < A - 1) {
+        const CannyRowSums<G> sc{src, srcStride, y, A, L};
+        int16_t t0, t1;
+        if (G == 3) {
+            t0 = cw16(sc.r0(x + 1) - sc.r0(x - 1));
+            t1 = cw16(0 - cw16(cw16(sc.r1(x - 1) + sc.r1(x + 1)) + cw16(sc.r1(x) << 1)));
+        } else if (G == 5) {
+            t0 = cs16(cw16(cw16(sc.r0(x + 1) - sc.r0(x - 1)) << 1) + cw16(sc.r0(x + 2) - sc.r0(x - 2)));
+            int16_t u = cw16(cw16(cw16(sc.r1(x - 1) + sc.r1(x + 1)) << 2) + cw16(sc.r1(x - 2) + sc.r1(x + 2)));
+            u = L2 ? cs16(u + cw16(sc.r1(x) * 6)) : cw16(u + cw16(sc.r1(x) * 6));
+            t1 = cw16(0 - u);
+        } else {
+            const int16_t a = cw16(cs16(sc.r0(x + 2) - sc.r0(x - 2)) << 2);
+            const int16_t b = cw16(cs16(sc.r0(x + 1) - sc.r0(x - 1)) * 5);
+            t0 = cs16(cs16(a + cs16(sc.r0(x + 3) - sc.r0(x - 3))) + b);
+            int16_t u = cs16(cw16(cw16(sc.r1(x - 2) + sc.r1(x + 2)) * 6) + cw16(sc.r1(x) * 20));
+            const int16_t v = cw16(cw16(sc.r1(x - 1) + sc.r1(x + 1)) * 15);
+            u = cs16(u + cs16(sc.r1(x - 3) + sc.r1(x + 3)));
+            u = cs16(u + v);
+            t1 = cs16(0 - u);
+        }
+        if (L2) {
+            d[x] = canny_l2_pack(t0, t1, G == 3);
+        } else {
+            int16_t m = cw16(cabs16(t0) + cabs16(t1));
+            if (G == 7 && m > 0x3FFF) m = 0x3FFF;
+            d[x] = (uint16_t)((uint16_t)(m << 2) | canny_dir(t0, t1));
+        }
+        return;
+    }
+    int gxs = 0, gys = 0;
+#pragma unroll
+    for (int j = -R; j <= R; j++)
+#pragma unroll
+        for (int i = -R; i <= R; i++) {
+            const int v = ago_flat_px(src, srcStride, W, H, L, x + i, y + j);
+            gxs += CannyWin<G>::v(j) * CannyWin<G>::d(i) * v;
+            gys += (G == 5 && L2 && j == -R) ? (i == -R ? -1 : 1) * CannyWin<G>::v(i) * v   // canny.cpp:800
+                                             : CannyWin<G>::d(j) * CannyWin<G>::v(i) * v;
+        }
+    const int16_t gx = cw16(gxs);
+    int16_t gy = cw16(gys);
+    if (!L2 && G != 7) gy = cw16(-gy);
+    int16_t t;
+    if (L2) {
+        const int32_t n = (int32_t)((uint32_t)(gx * gx) + (uint32_t)(gy * gy));
+        t = n < 0 ? 0 : cw16((int)__dsqrt_rn((double)n));
+    } else {
+        t = cw16(abs(gx) + abs(gy));
+    }
+    t = cw16(t << 2);
+    d[x] = (uint16_t)cw16(t | canny_dir(gx, gy));
+}
+
 __global__ void k_canny_supp(int W, int H, uint8_t *dst, int dstStride, const uint16_t *g, int gStride,
                              int lower, int upper, uint32_t *stack, uint32_t *stackCount, uint32_t capacity)
 {
@@ -993,6 +1125,26 @@ extern "C" int agocuda_CannySobel_U16_U8_3x3_L1NORM(void *stream, uint32_t W, ui
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }
+
+#define CANNY_NXN(NAME, G, L2)                                                                                  \
+    extern "C" int NAME(void *stream, uint32_t W, uint32_t H, uint16_t *pDst, uint32_t dstStride,              \
+                        const uint8_t *pSrc, uint32_t srcStride)                                                \
+    {                                                                                                           \
+        if (!pDst || !pSrc || W < G || H < G || dstStride < 2 * W || srcStride < W || !aligned(pDst, 2) ||   \
+            (dstStride & 1))                                                                                    \
+            return AGOCUDA_INVALID_PARAMS;                                                                      \
+        k_canny_sobel_nxn<G, L2><<<row_grid(W, H, 128), 128, 0, as_stream(stream)>>>((int)W, (int)H, pDst,    \
+                                                                                     (int)dstStride, pSrc,     \
+                                                                                     (int)srcStride);          \
+        agocuda_count_launch(1);                                                                                \
+        return agocuda_launch_status();                                                                         \
+    }
+CANNY_NXN(agocuda_CannySobel_U16_U8_3x3_L2NORM, 3, true)
+CANNY_NXN(agocuda_CannySobel_U16_U8_5x5_L1NORM, 5, false)
+CANNY_NXN(agocuda_CannySobel_U16_U8_5x5_L2NORM, 5, true)
+CANNY_NXN(agocuda_CannySobel_U16_U8_7x7_L1NORM, 7, false)
+CANNY_NXN(agocuda_CannySobel_U16_U8_7x7_L2NORM, 7, true)
+#undef CANNY_NXN
 
 extern "C" int agocuda_CannySuppThreshold_U8XY_U16_3x3(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
                                                        const uint16_t *pSrc, uint32_t srcStride, uint32_t *pStack,

@@ -227,6 +227,132 @@ int oracle_CannySobel_U16_U8_3x3_L1NORM(uint32_t W, uint32_t H, uint16_t *pDst, 
     return 0;
 }
 
+/* Canny gradients with 3x3 L2, 5x5 and 7x7 windows (ago_haf_cpu_canny.cpp:145 5x5 L1,
+ * :272 7x7 L1, :646 3x3 L2, :756 5x5 L2, :893 7x7 L2), rows [R, H-R), R = gsize / 2.
+ *
+ * Each reference kernel splits a row like the 3x3 L1 one: scalar columns [0, prefix) and
+ * [aligned + prefix - 1, W), SIMD columns between them computed from per-row vertical sums
+ * r0 (smoothing) and r1 (difference) kept in node scratch at scratch + 16 bytes, r1 right
+ * after r0 (ALIGN16(W) int16 each).  The SIMD part reads r0 / r1 up to R columns outside
+ * [0, aligned), i.e. the zeroed scratch or the neighbouring row buffer; this restatement
+ * keeps the same scratch layout so those reads land on the same values.  The SIMD and
+ * scalar formulas differ per variant, and are restated as written:
+ *   - 3x3 L2 body squares in 16-bit lanes (mullo, zero-extended), sums in float, sqrt,
+ *     rounds half-even, packs with unsigned saturation; its scalar Gy is not negated.
+ *   - 5x5 body is exact; L1 scalar negates Gy, L2 scalar does not and its top row term
+ *     negates only the first pixel (canny.cpp:800).
+ *   - 7x7 body divides both vertical sums by 4 (srai), combines with saturating adds and
+ *     clamps the L1 magnitude to 0x3FFF; its scalar columns use the full-scale sums in
+ *     16-bit wrapping arithmetic, Gy not negated.
+ * L2 scalar columns: (int16) sqrt((double) (Gx^2 + Gy^2)), i.e. the integer square root
+ * wrapped to 16 bits. */
+static const int kV3[3] = { 1, 2, 1 }, kD3[3] = { -1, 0, 1 };
+static const int kV5[5] = { 1, 4, 6, 4, 1 }, kD5[5] = { -1, -2, 0, 2, 1 };
+static const int kV7[7] = { 1, 6, 15, 20, 15, 6, 1 }, kD7[7] = { -1, -4, -5, 0, 5, 4, 1 };
+
+static int16_t w16(int v) { return (int16_t)v; }
+static int16_t s16(int v) { return (int16_t)(v > 32767 ? 32767 : (v < -32768 ? -32768 : v)); }
+static int16_t abs16(int16_t v) { return (int16_t)(v < 0 ? -(int)v : v); }
+
+static uint16_t canny_l2_pack(int16_t gx, int16_t gy, int body3)
+{
+    float f;
+    if (body3)
+        f = (float)(uint16_t)(gx * gx) + (float)(uint16_t)(gy * gy);
+    else
+        f = (float)(int32_t)((uint32_t)(gx * gx) + (uint32_t)(gy * gy));
+    int m = (int)nearbyintf(sqrtf(f));
+    if (m < 0) m = 0;
+    if (m > 65535) m = 65535;
+    return (uint16_t)((uint16_t)(m << 2) | (fast_atan2_canny(gx, gy) & 3));
+}
+
+int oracle_CannySobel_U16_U8_NxN(uint32_t W, uint32_t H, uint16_t *pDst, uint32_t dstStride,
+                                 const uint8_t *pSrc, uint32_t srcStride, uint32_t gsize, uint32_t l2)
+{
+    if (gsize != 3 && gsize != 5 && gsize != 7) return -1;
+    const int R = (int)gsize / 2;
+    const int *V = gsize == 3 ? kV3 : (gsize == 5 ? kV5 : kV7);
+    const int *D = gsize == 3 ? kD3 : (gsize == 5 ? kD5 : kD7);
+    int prefix, tail_start;
+    haf_split(pDst, (int)W, &prefix, &tail_start);
+    const int aligned = tail_start - prefix;
+    const int L = ((int)W + 15) & ~15;
+    uint8_t *scratch = (uint8_t *)calloc((size_t)L * 4 + 128, 1);
+    if (!scratch) return -1;
+    int16_t *r0 = (int16_t *)(scratch + 16), *r1 = r0 + L;
+    const long st = (long)srcStride;
+    for (int y = R; y < (int)H - R; y++) {
+        const uint8_t *s = pSrc + (size_t)y * srcStride;
+        uint16_t *d = (uint16_t *)ROW(pDst, dstStride, y);
+        /* SIMD part: vertical sums, then the horizontal pass, 8 columns per step */
+        for (int x0 = prefix; x0 <= aligned - 8; x0 += 8)
+            for (int x = x0; x < x0 + 8; x++) {
+                int a = 0, b = 0;
+                for (int k = -R; k <= R; k++) { a += V[k + R] * s[x + k * st]; b += D[k + R] * s[x + k * st]; }
+                if (gsize == 7) { a = w16(a) >> 2; b = w16(b) >> 2; }
+                r0[x] = w16(a); r1[x] = w16(b);
+            }
+        for (int x0 = prefix; x0 <= aligned - 8; x0 += 8)
+            for (int x = x0; x < x0 + 8; x++) {
+                int16_t t0, t1;
+                if (gsize == 3) {
+                    t0 = w16(r0[x + 1] - r0[x - 1]);
+                    t1 = w16(0 - w16(w16(r1[x - 1] + r1[x + 1]) + w16(r1[x] << 1)));
+                } else if (gsize == 5) {
+                    t0 = s16(w16(w16(r0[x + 1] - r0[x - 1]) << 1) + w16(r0[x + 2] - r0[x - 2]));
+                    int16_t u = w16(w16(w16(r1[x - 1] + r1[x + 1]) << 2) + w16(r1[x - 2] + r1[x + 2]));
+                    u = l2 ? s16(u + w16(r1[x] * 6)) : w16(u + w16(r1[x] * 6));
+                    t1 = w16(0 - u);
+                } else {
+                    int16_t a = w16(s16(r0[x + 2] - r0[x - 2]) << 2);
+                    int16_t b = w16(s16(r0[x + 1] - r0[x - 1]) * 5);
+                    t0 = s16(s16(a + s16(r0[x + 3] - r0[x - 3])) + b);
+                    int16_t u = s16(w16(w16(r1[x - 2] + r1[x + 2]) * 6) + w16(r1[x] * 20));
+                    int16_t v = w16(w16(r1[x - 1] + r1[x + 1]) * 15);
+                    u = s16(u + s16(r1[x - 3] + r1[x + 3]));
+                    u = s16(u + v);
+                    t1 = s16(0 - u);
+                }
+                if (l2) {
+                    d[x] = canny_l2_pack(t0, t1, gsize == 3);
+                } else {
+                    int16_t m = w16(abs16(t0) + abs16(t1));
+                    if (gsize == 7 && m > 0x3FFF) m = 0x3FFF;
+                    d[x] = (uint16_t)((uint16_t)(m << 2) | (fast_atan2_canny(t0, t1) & 3));
+                }
+            }
+        /* scalar columns */
+        for (int x = 0; x < (int)W; x++) {
+            if (x >= prefix && x < aligned + prefix - 1) continue;
+            int gxs = 0, gys = 0;
+            for (int j = -R; j <= R; j++)
+                for (int i = -R; i <= R; i++) {
+                    const int v = s[x + i + j * st];
+                    gxs += V[j + R] * D[i + R] * v;
+                    if (gsize == 5 && l2 && j == -R)   /* canny.cpp:800: only the first term negated */
+                        gys += (i == -R ? -1 : 1) * V[i + R] * v;
+                    else
+                        gys += D[j + R] * V[i + R] * v;
+                }
+            int16_t gx = w16(gxs), gy = w16(gys);
+            if (!l2 && gsize != 7) gy = w16(~gy + 1);
+            int16_t t;
+            if (l2) {
+                int32_t n = (int32_t)((uint32_t)(gx * gx) + (uint32_t)(gy * gy));
+                t = n < 0 ? 0 : w16((int)sqrt((double)n));
+            } else {
+                t = w16(abs(gx) + abs(gy));
+            }
+            t = w16(t << 2);
+            t = w16(t | (fast_atan2_canny(gx, gy) & 3));
+            d[x] = (uint16_t)t;
+        }
+    }
+    free(scratch);
+    return 0;
+}
+
 static const int kNOffset[4][2][2] = {
     { { -1, 0 }, { 1, 0 } }, { { 1, -1 }, { -1, 1 } }, { { 0, -1 }, { 0, 1 } }, { { -1, -1 }, { 1, 1 } },
 };

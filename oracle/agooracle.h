@@ -43,6 +43,8 @@ typedef struct { int32_t x, y; float strength, scale, orientation; int32_t track
 
 int oracle_CannySobel_U16_U8_3x3_L1NORM(uint32_t dstWidth, uint32_t dstHeight, uint16_t *pDst, uint32_t dstStride,
                                         const uint8_t *pSrc, uint32_t srcStride);
+int oracle_CannySobel_U16_U8_NxN(uint32_t dstWidth, uint32_t dstHeight, uint16_t *pDst, uint32_t dstStride,
+                                 const uint8_t *pSrc, uint32_t srcStride, uint32_t gsize, uint32_t l2);
 int oracle_CannySuppThreshold_U8XY_U16_3x3(uint32_t capacityOfXY, oracle_coord2d_u16 *xyStack, uint32_t *pStackTop,
                                            uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
                                            const uint16_t *pSrc, uint32_t srcStride, uint16_t lower, uint16_t upper);

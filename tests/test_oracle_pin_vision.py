@@ -159,3 +159,43 @@ def test_pin_harris_pick_synthetic(ref):
         b, nb = oracle_pick(lst, 300, 200, mind, cap)
         assert na == nb
         np.testing.assert_array_equal(a, b)
+
+
+CANNY_VARIANTS = [(3, 1), (5, 0), (5, 1), (7, 0), (7, 1)]
+
+
+def canny_sobel_nxn(which, img, gsize, l2):
+    """The packed Canny gradient of one window size / norm on an AGO-laid-out buffer."""
+    H, W = img.shape
+    src = ago_img(H, W); src.set(img)
+    sob = ago_img(H, W, np.uint16)
+    if which == "ref":
+        local = np.zeros(((W + 15) & ~15) * 4 + 128, np.uint8)
+        name = f"HafCpu_CannySobel_U16_U8_{gsize}x{gsize}_{'L2' if l2 else 'L1'}NORM"
+        fn(None, name, [u32, u32, vp, u32, vp, u32, vp])(W, H, sob.ptr, sob.stride, src.ptr, src.stride, local.ctypes.data)
+    else:
+        fn(O.oracle_lib(), "oracle_CannySobel_U16_U8_NxN", [u32, u32, vp, u32, vp, u32, u32, u32])(
+            W, H, sob.ptr, sob.stride, src.ptr, src.stride, gsize, l2)
+    return sob.get()
+
+
+@pytest.mark.parametrize("W,H", SHAPES + [(333, 47), (1920, 24)])
+@pytest.mark.parametrize("gsize,l2", CANNY_VARIANTS)
+def test_pin_canny_sobel_variants(ref, gsize, l2, W, H):
+    """3x3 L2, 5x5 and 7x7 gradients: every written row [R, H-R) equals the reference,
+    on textured scenes and on noise (which saturates the 7x7 sums)."""
+    R = gsize // 2
+    for img in (scene(W, H, seed=W * gsize + l2),
+                np.random.default_rng(W + H + gsize).integers(0, 256, (H, W), dtype=np.int32).astype(np.uint8)):
+        want = canny_sobel_nxn("ref", img, gsize, l2)
+        got = canny_sobel_nxn("oracle", img, gsize, l2)
+        np.testing.assert_array_equal(got[R:H - R], want[R:H - R])
+
+
+@pytest.mark.parametrize("W,H", SHAPES)
+def test_oracle_canny_nxn_matches_3x3_l1(W, H):
+    """The generic restatement at 3x3 L1 reproduces the pinned 3x3 L1 one."""
+    img = scene(W, H, seed=W)
+    a = canny_sobel_nxn("oracle", img, 3, 0)
+    b, _, _, _ = canny_front("oracle", img)
+    np.testing.assert_array_equal(a[1:H - 1], b.get()[1:H - 1])
