@@ -131,10 +131,16 @@ int agocuda_CannySuppThreshold_U8XY_U16_3x3(void *stream, uint32_t dstWidth, uin
                                             uint16_t hystLower, uint16_t hystUpper);
 
 /* Hysteresis in place: pixels 8-connected through non-zero pixels to a strong one become
- * 255, all others 0 (the whole image is written).  Needs `scratch` device memory of
- * agocuda_CannyEdgeTrace_scratch_size(W, H) bytes, 256-byte aligned; *pStatus gets bit 0 set
- * if a union-find walk exceeded its bound.  The reference runs this on the CPU only
- * (ago_kernel_list.cpp:486); HafCpu_CannyEdgeTrace_U8_U8XY (ago_haf_cpu_canny.cpp:598). */
+ * 255, all others 0 (the whole image is written).  The stack is expected to hold every
+ * strong pixel, as the suppression above leaves it.  An entry on a pixel that is not in the
+ * edge map (zero, or on the image border) seeds the components of its 8 neighbours, as the
+ * reference's trace grows from each entry through its neighbours; an entry outside the
+ * image is ignored and sets AGOCUDA_TRACE_STATUS_BAD_ENTRY in *pStatus.  Needs `scratch`
+ * device memory of agocuda_CannyEdgeTrace_scratch_size(W, H) bytes, 256-byte aligned;
+ * *pStatus gets bit 0 set if a union-find walk exceeded its bound.  The reference runs this
+ * on the CPU only (ago_kernel_list.cpp:486); HafCpu_CannyEdgeTrace_U8_U8XY
+ * (ago_haf_cpu_canny.cpp:598). */
+#define AGOCUDA_TRACE_STATUS_BAD_ENTRY 8u  /* an edge-trace stack entry lay outside the image */
 size_t agocuda_CannyEdgeTrace_scratch_size(uint32_t width, uint32_t height);
 int agocuda_CannyEdgeTrace_U8_U8XY(void *stream, uint32_t width, uint32_t height, uint8_t *pImg, uint32_t stride,
                                    const uint32_t *pStack, const uint32_t *pStackCount, uint32_t stackCapacity,
@@ -148,7 +154,9 @@ int agocuda_CannyEdgeTrace_U8_U8XY(void *stream, uint32_t width, uint32_t height
  * which every GPU that loads the library holds until the process exits.  Images are limited
  * to agocuda_CannyEdgeTrace_noalloc_max_pixels() = 2,097,152 pixels (W*H); larger ones return
  * -15 without launching anything.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) and should be made before any stream capture.  All calls on
+ * address (cudaGetSymbolAddress) and should be made before any stream capture; the lookup
+ * is repeated when the calling thread's current context on that device changes (after
+ * cudaDeviceReset, for instance), so that call, too, belongs outside a capture.  All calls on
  * a device share that one array: the labels are rewritten and the bitmap is cleared on every
  * call, but calls whose executions overlap on the GPU (other streams, or host threads
  * without ordering) race on it.  No counterpart in the reference (its edge trace runs on the
@@ -180,13 +188,21 @@ int agocuda_NonMaxSupp_XY_ANY_3x3(void *stream, uint32_t width, uint32_t height,
 
 /* Sort candidates (descending as int64) and keep those farther than minDistance from kept
  * ones on the reference's grid; writes vx_keypoint_t records in sorted order, *pCornerCount =
- * min(kept, capacity), *pNumCorners = kept.  At most 8192 candidates (else *pStatus |= 2 and
- * nothing is written).  The reference runs this on the CPU only (ago_kernel_list.cpp:483);
- * HafCpu_HarrisMergeSortAndPick_XY_XYS (ago_haf_cpu_harris.cpp:923). */
+ * min(kept, capacity), *pNumCorners = kept.  Up to 8192 candidates are picked by one CTA in
+ * shared memory; larger lists (the reference's holds up to W*H) by one cluster of 8 CTAs in
+ * `scratch`, which must then hold agocuda_HarrisMergeSortAndPick_scratch_size(W, H,
+ * listCapacity, minDistance) bytes, 256-byte aligned.  With scratch NULL a list above 8192
+ * sets *pStatus |= 2 and nothing is written.  A candidate outside the WxH grid is dropped
+ * and sets AGOCUDA_PICK_STATUS_BAD_ENTRY.  The reference runs this on the CPU only
+ * (ago_kernel_list.cpp:483); HafCpu_HarrisMergeSortAndPick_XY_XYS (ago_haf_cpu_harris.cpp:923). */
+#define AGOCUDA_PICK_STATUS_BAD_ENTRY 32u  /* a corner candidate lay outside the image */
+size_t agocuda_HarrisMergeSortAndPick_scratch_size(uint32_t width, uint32_t height, uint32_t listCapacity,
+                                                  float minDistance);
 int agocuda_HarrisMergeSortAndPick_XY_XYS(void *stream, uint32_t width, uint32_t height, const uint64_t *pList,
                                           const uint32_t *pListCount, uint32_t listCapacity, float minDistance,
                                           void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
-                                          uint32_t *pNumCorners, uint32_t *pStatus);
+                                          uint32_t *pNumCorners, void *scratch, size_t scratchBytes,
+                                          uint32_t *pStatus);
 
 /* ------------------------------------------------------------------------------------ */
 /* Colour conversion, scaling, warps (reference: hipvx/hip_host_decls.h color/geometric)  */
@@ -311,8 +327,10 @@ int agocuda_fused_ColorScale_RGB(void *stream, uint32_t width, uint32_t height, 
 
 /* vxHarrisCornersNode (gradient 3, block 3) as one front-end kernel (Sobel products,
  * window sums, score and non-maximum suppression from one read of the image) plus the
- * corner pick.  Scratch: agocuda_fused_HarrisCorners_scratch_size(W, H) bytes. */
-size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t width, uint32_t height);
+ * corner pick.  The candidate list holds ceil(W/2)*ceil(H/2) entries, the most the
+ * suppression can emit, so no image overflows it.  Scratch:
+ * agocuda_fused_HarrisCorners_scratch_size(W, H, minDistance) bytes. */
+size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t width, uint32_t height, float minDistance);
 int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t width, uint32_t height, const uint8_t *pSrc, uint32_t srcStride,
                                     float sensitivity, float strengthThreshold, float normFactor, float minDistance,
                                     void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,

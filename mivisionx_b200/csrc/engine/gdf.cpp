@@ -321,8 +321,7 @@ struct Importer {
                     vx_enum e;
                     if (!enum_by_name(arg.substr(1), e)) return fail(VX_ERROR_INVALID_VALUE, "unknown enum name");
                     Scalar *s = make_scalar(c, g, VX_TYPE_ENUM, &e);
-                    s->ext_count = 0;
-                    g->owned_virtual.push_back(s);
+                    s->ext_count = 0;             // held by the node it is passed to
                     params.push_back(s);
                     continue;
                 }

@@ -151,9 +151,6 @@ vx_status validate_node(Graph *g, Node *n)
         const int gs = sc_i32(p[2]);
         if (gs != 3 && gs != 5 && gs != 7) return VX_ERROR_INVALID_VALUE;
         if (sc_enum(p[3]) != VX_NORM_L1 && sc_enum(p[3]) != VX_NORM_L2) return VX_ERROR_INVALID_VALUE;
-        // the 3x3 L2 / 5x5 / 7x7 gradient kernels exist (agocuda_CannySobel_*) but graphs
-        // using them are not enabled yet: a later context release aborted after them
-        if (gs != 3 || sc_enum(p[3]) != VX_NORM_L1) return VX_ERROR_NOT_SUPPORTED;
         return set_meta(img(4), img(0)->width, img(0)->height, VX_DF_IMAGE_U8);
     }
     case VX_KERNEL_HARRIS_CORNERS: {
@@ -284,7 +281,7 @@ static Scalar *virt_scalar(Graph *g, vx_enum type, uint64_t value)
     Scalar *s = make_scalar(g->ctx, g, type, &value);
     s->is_virtual = true;
     s->ext_count = 0;
-    g->owned_virtual.push_back(s);
+    graph_own(g, s);
     return s;
 }
 
@@ -292,7 +289,7 @@ static Image *virt_image(Graph *g, uint32_t w, uint32_t h, vx_df_image f)
 {
     Image *img = make_image(g->ctx, g, w, h, f, true);
     img->ext_count = 0;
-    g->owned_virtual.push_back(img);
+    graph_own(g, img);
     return img;
 }
 
@@ -300,7 +297,7 @@ static Array *virt_array(Graph *g, vx_enum item, vx_size cap)
 {
     Array *a = make_array(g->ctx, g, item, cap, true);
     a->ext_count = 0;
-    g->owned_virtual.push_back(a);
+    graph_own(g, a);
     return a;
 }
 
@@ -721,6 +718,7 @@ vx_status lower_graph(Graph *g)
 {
     g->lnodes.clear();
     g->replaced.clear();
+    graph_release_owned(g);       // the previous lowering's virtual data (no plan names it any more)
     for (Node *n : g->nodes) {
         if (n->removed) continue;
         vx_status s = validate_node(g, n);

@@ -496,8 +496,12 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         void *out = corners->dev; uint32_t ocap = (uint32_t)corners->capacity; uint32_t *oc = corners->dev_count;
         uint32_t *nc = num ? num->dev : nullptr;
         uint32_t *status = g->status_dev;
+        const size_t sb = agocuda_HarrisMergeSortAndPick_scratch_size(w, h, lcap, mind);
+        void *scr = scratch(g, sb);
+        if (!scr) return VX_ERROR_NO_MEMORY;
+        st.num_kernels = 2;
         st.launch = [=](cudaStream_t q) {
-            return agocuda_HarrisMergeSortAndPick_XY_XYS(S(q), w, h, l, lc, lcap, mind, out, ocap, oc, nc, status);
+            return agocuda_HarrisMergeSortAndPick_XY_XYS(S(q), w, h, l, lc, lcap, mind, out, ocap, oc, nc, scr, sb, status);
         };
         return VX_SUCCESS;
     }
@@ -898,14 +902,14 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
                 if (num && scalar_alloc_device(num)) return VX_ERROR_NO_MEMORY;
                 void *out = corners->dev; const uint32_t ocap = (uint32_t)corners->capacity; uint32_t *oc = corners->dev_count;
                 uint32_t *nc = num ? num->dev : nullptr;
-                const size_t sb = agocuda_fused_HarrisCorners_scratch_size(w, h);
+                const size_t sb = agocuda_fused_HarrisCorners_scratch_size(w, h, mind);
                 void *scr = scratch(g, sb);
                 if (!scr) return VX_ERROR_NO_MEMORY;
                 fns.push_back([=](cudaStream_t q) {
                     return agocuda_fused_HarrisCorners_3x3(S(q), w, h, src, ss, k, tc, norm, mind, out, ocap, oc, nc, scr, sb, status);
                 });
                 st.parts.push_back(Part{fns.back(), c.nodes});
-                st.num_kernels += 2;
+                st.num_kernels += 3;
             }
         }
         st.launch = [fns](cudaStream_t q) {

@@ -661,9 +661,10 @@ vx_status vxReleaseGraph(vx_graph *graph)
     if (!graph || !is_valid(*graph, VX_TYPE_GRAPH)) return VX_ERROR_INVALID_REFERENCE;
     Graph *g = as<Graph>(*graph);
     if (g->scheduled) graph_wait(g);
+    *graph = nullptr;
     g->ext_count = 0;
     g->released = true;
-    *graph = nullptr;
+    if (g->int_count == 0) destroy_ref(g);   // its nodes, plans and lowered data go with it
     return VX_SUCCESS;
 }
 

@@ -74,6 +74,7 @@ struct Image : Ref {
     vx_pixel_value_t uniform_value{};
     vx_enum import_type = VX_MEMORY_TYPE_NONE;  // HOST / HIP(device) for images from handle
     Image *parent = nullptr;          // pyramid/channel parent (shares memory)
+    Image *view_of = nullptr;         // image this ROI / channel view holds an internal reference on
     std::vector<Image *> children;    // planes of multi-plane images as U8 images (AGO children)
     std::map<vx_map_id, MapInfo> maps;
     vx_map_id next_map = 1;
@@ -323,6 +324,7 @@ struct Context : Ref {
     vx_border_t immediate_border{VX_BORDER_UNDEFINED, {}};
     uint32_t affinity = AGO_TARGET_AFFINITY_GPU;
     std::vector<Kernel *> kernels;
+    bool tearing_down = false;        // vxReleaseContext deletes every object itself
 };
 
 // Optimizer flag bits of VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS (ago/ago_internal.h:123-129),
@@ -336,6 +338,9 @@ constexpr uint32_t kOptSerial = 0x00040000;         // capture on one stream (no
 void add_ref(Context *ctx, Ref *r);
 void retain_internal(Ref *r);
 void release_internal(Ref *r);
+void destroy_ref(Ref *r);
+void graph_own(Graph *g, Ref *r);             // the graph's lowering holds r until re-lowered or released
+void graph_release_owned(Graph *g);
 vx_status image_alloc_device(Image *img);
 vx_status image_sync_to_device(Image *img, cudaStream_t s);
 vx_status image_sync_to_host(Image *img);

@@ -84,8 +84,93 @@ void add_ref(Context *ctx, Ref *r)
     if (ctx) ctx->refs.push_back(r);
 }
 
+// Lifetime: an object dies when its last application reference and its last internal one
+// (a node parameter, a multi-plane parent, a pyramid, a delay, a graph's lowering) are both
+// gone, and its host and device storage go with it -- agoReleaseData (ago/ago_util.cpp:2771)
+// frees AGO's objects the same way.
 void retain_internal(Ref *r) { if (r) r->int_count++; }
-void release_internal(Ref *r) { if (r && r->int_count > 0) r->int_count--; }
+
+void release_internal(Ref *r)
+{
+    if (!r || r->int_count <= 0) return;
+    if (--r->int_count == 0 && r->ext_count == 0) destroy_ref(r);
+}
+
+void graph_own(Graph *g, Ref *r)
+{
+    retain_internal(r);
+    g->owned_virtual.push_back(r);
+}
+
+void graph_release_owned(Graph *g)
+{
+    std::vector<Ref *> owned;
+    owned.swap(g->owned_virtual);
+    for (Ref *r : owned) release_internal(r);
+}
+
+static void graph_destroy_contents(Graph *g)
+{
+    if (g->scheduled) graph_wait(g);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    graph_invalidate(g);
+    g->lnodes.clear();
+    g->replaced.clear();
+    // nodes belong to their graph: they go with it even if the application kept a handle
+    std::vector<Node *> nodes;
+    nodes.swap(g->nodes);
+    for (Node *n : nodes) destroy_ref(n);
+    graph_release_owned(g);
+    std::vector<Delay *> aged;
+    aged.swap(g->auto_age);
+    for (Delay *d : aged) release_internal(d);
+    // virtual data the application still holds outlives its graph's scope
+    for (Ref *r : g->ctx->refs) if (r->scope == g) r->scope = nullptr;
+}
+
+void destroy_ref(Ref *r)
+{
+    if (!is_ref(r) || r->type == VX_TYPE_CONTEXT) return;
+    Context *c = r->ctx;
+    if (c && c->tearing_down) return;
+    r->magic = 0;
+    if (c) {
+        auto it = std::find(c->refs.begin(), c->refs.end(), r);
+        if (it != c->refs.end()) c->refs.erase(it);
+    }
+    switch (r->type) {
+    case VX_TYPE_GRAPH: graph_destroy_contents(static_cast<Graph *>(r)); break;
+    case VX_TYPE_NODE: {
+        std::vector<Ref *> params;
+        params.swap(static_cast<Node *>(r)->params);
+        for (Ref *p : params) release_internal(p);
+        break;
+    }
+    case VX_TYPE_IMAGE: {
+        Image *img = static_cast<Image *>(r);
+        // plane images share the parent's storage: they cannot outlive it
+        std::vector<Image *> children;
+        children.swap(img->children);
+        for (Image *ch : children) { ch->parent = nullptr; ch->ext_count = ch->int_count = 0; destroy_ref(ch); }
+        if (img->view_of) release_internal(img->view_of);
+        break;
+    }
+    case VX_TYPE_PYRAMID: {
+        std::vector<Image *> levels;
+        levels.swap(static_cast<Pyramid *>(r)->level);
+        for (Image *lv : levels) release_internal(lv);
+        break;
+    }
+    case VX_TYPE_DELAY: {
+        std::vector<Ref *> slots;
+        slots.swap(static_cast<Delay *>(r)->slots);
+        for (Ref *sl : slots) release_internal(sl);
+        break;
+    }
+    default: break;
+    }
+    delete r;
+}
 
 // ---------------------------------------------------------------- images
 Image::~Image()
@@ -410,10 +495,13 @@ vx_status vxReleaseContext(vx_context *context)
     if (!context || !is_valid(*context, VX_TYPE_CONTEXT)) return VX_ERROR_INVALID_REFERENCE;
     Context *c = as<Context>(*context);
     cudaDeviceSynchronize();
-    // graphs first: they hold device work and internal references
-    for (Ref *r : c->refs) if (r->type == VX_TYPE_GRAPH) { delete r; r->magic = 0; }
-    for (Ref *r : c->refs) if (r->magic == kMagic && r->type != VX_TYPE_GRAPH) delete r;
+    c->tearing_down = true;
+    std::vector<Ref *> graphs, others;
+    for (Ref *r : c->refs) (r->type == VX_TYPE_GRAPH ? graphs : others).push_back(r);
     c->refs.clear();
+    // graphs first: their plans and captured CUDA graphs name the other objects' storage
+    for (Ref *r : graphs) { r->magic = 0; delete r; }
+    for (Ref *r : others) { r->magic = 0; delete r; }
     c->magic = 0;
     delete c;
     *context = nullptr;
@@ -505,7 +593,10 @@ static vx_status release_ref(Ref *r)
 {
     if (!is_ref(r) || r->ext_count <= 0) return VX_ERROR_INVALID_REFERENCE;
     r->ext_count--;
-    if (r->ext_count == 0) r->released = true;   // storage is reclaimed with the context
+    if (r->ext_count == 0) {
+        r->released = true;
+        if (r->int_count == 0) destroy_ref(r);
+    }
     return VX_SUCCESS;
 }
 
@@ -582,6 +673,15 @@ vx_image vxCreateUniformImage(vx_context context, vx_uint32 width, vx_uint32 hei
     return (vx_image)img;
 }
 
+// Device memory imported from the application must have the layout of the engine's own
+// planes: the kernels read and write rows with word and 16-byte vector accesses (and
+// cp.async copies), which need aligned rows; a misaligned plane is refused here instead of
+// faulting on the GPU.
+static bool device_layout_ok(const void *p, uint32_t stride)
+{
+    return ((uintptr_t)p % 256) == 0 && (stride % 64) == 0;
+}
+
 vx_image vxCreateImageFromHandle(vx_context context, vx_df_image color, const vx_imagepatch_addressing_t addrs[],
                                  void *const ptrs[], vx_enum memory_type)
 {
@@ -591,11 +691,15 @@ vx_image vxCreateImageFromHandle(vx_context context, vx_df_image color, const vx
     uint32_t w = addrs[0].dim_x, h = addrs[0].dim_y;
     int np = format_planes(color, w, h, tmp);
     if (!np) return nullptr;
+    for (int i = 0; i < np; i++) {
+        if ((uint32_t)addrs[i].stride_x != tmp[i].bpp || !ptrs[i]) return nullptr;   // packed pixels only
+        if ((uint64_t)addrs[i].stride_y < (uint64_t)tmp[i].width * tmp[i].bpp) return nullptr;
+        if (memory_type == VX_MEMORY_TYPE_HIP && !device_layout_ok(ptrs[i], (uint32_t)addrs[i].stride_y)) return nullptr;
+    }
     Image *img = make_image(as<Context>(context), nullptr, w, h, color, false);
     img->import_type = memory_type;
     for (int i = 0; i < np; i++) {
         Plane &p = img->planes[i];
-        if ((uint32_t)addrs[i].stride_x != p.bpp) return nullptr;   // packed pixels only
         if (memory_type == VX_MEMORY_TYPE_HOST) {
             p.host = (uint8_t *)ptrs[i]; p.host_stride = (uint32_t)addrs[i].stride_y; p.host_owned = false;
         } else {
@@ -612,6 +716,9 @@ vx_status vxSwapImageHandle(vx_image image, void *const new_ptrs[], void *prev_p
     CHECK_REF(image, VX_TYPE_IMAGE);
     Image *img = as<Image>(image);
     if (img->import_type == VX_MEMORY_TYPE_NONE || (int)num_planes != img->num_planes) return VX_ERROR_INVALID_PARAMETERS;
+    if (new_ptrs && img->import_type == VX_MEMORY_TYPE_HIP)
+        for (int i = 0; i < img->num_planes; i++)
+            if (new_ptrs[i] && !device_layout_ok(new_ptrs[i], img->planes[i].dev_stride)) return VX_ERROR_INVALID_PARAMETERS;
     for (int i = 0; i < img->num_planes; i++) {
         uint8_t *&slot = img->import_type == VX_MEMORY_TYPE_HOST ? img->planes[i].host : img->planes[i].dev;
         if (prev_ptrs) prev_ptrs[i] = slot;
@@ -1583,8 +1690,10 @@ vx_status vxRegisterAutoAging(vx_graph graph, vx_delay delay)
     CHECK_REF(graph, VX_TYPE_GRAPH);
     CHECK_REF(delay, VX_TYPE_DELAY);
     Graph *g = as<Graph>(graph);
-    if (std::find(g->auto_age.begin(), g->auto_age.end(), as<Delay>(delay)) == g->auto_age.end())
+    if (std::find(g->auto_age.begin(), g->auto_age.end(), as<Delay>(delay)) == g->auto_age.end()) {
         g->auto_age.push_back(as<Delay>(delay));
+        retain_internal(as<Delay>(delay));
+    }
     return VX_SUCCESS;
 }
 

@@ -8,6 +8,9 @@
 // through non-maximum suppression and hysteresis, so `ago_px` reproduces them.
 #include "agocuda_internal.cuh"
 
+#include <cooperative_groups.h>
+#include <cuda.h>
+
 #include <mutex>
 
 uint64_t agocuda_count_launch(unsigned n);
@@ -329,15 +332,34 @@ __global__ void k_hyst_union(int W, int H, int *L, uint32_t *err)
     if (x + 1 < W && __ldcg(L + p - W + 1) >= 0) uf_union(L, p, p - W + 1, err);
 }
 
-__global__ void k_hyst_mark(int W, const int *L, const uint32_t *strong, const uint32_t *strongCount, uint32_t capacity,
-                            uint32_t *rootBits)
+// Seeds from the stack.  An entry on an edge-map pixel marks its component.  An entry on a
+// pixel outside the map (zero, or on the image border, where labels are -1) marks the
+// components of its 8 neighbours instead: the reference's trace grows from every stack entry
+// through its neighbours whatever the entry's own value (ago_haf_cpu_canny.cpp:611-625).
+// Entries outside the image are skipped and flagged (AGOCUDA_TRACE_STATUS_BAD_ENTRY).
+__global__ void k_hyst_mark(int W, int H, const int *L, const uint32_t *strong, const uint32_t *strongCount,
+                            uint32_t capacity, uint32_t *rootBits, uint32_t *err)
 {
     const uint32_t n = min(*strongCount, capacity);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t xy = strong[i];
-        const int p = (int)(xy >> 16) * W + (int)(xy & 0xffff);
-        const int r = uf_find(L, p);
-        atomicOr(rootBits + (r >> 5), 1u << (r & 31));
+        const int x = (int)(xy & 0xffff), y = (int)(xy >> 16);
+        if (x >= W || y >= H) { atomicOr(err, AGOCUDA_TRACE_STATUS_BAD_ENTRY); continue; }
+        const int p = y * W + x;
+        if (L[p] >= 0) {
+            const int r = uf_find(L, p);
+            atomicOr(rootBits + (r >> 5), 1u << (r & 31));
+            continue;
+        }
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                const int x1 = x + dx, y1 = y + dy;
+                if ((dx | dy) == 0 || x1 < 0 || x1 >= W || y1 < 0 || y1 >= H) continue;
+                const int q = y1 * W + x1;
+                if (L[q] < 0) continue;
+                const int r = uf_find(L, q);
+                atomicOr(rootBits + (r >> 5), 1u << (r & 31));
+            }
     }
 }
 
@@ -983,14 +1005,16 @@ __device__ __forceinline__ uint32_t hcell(int cx, int cy) { return ((uint32_t)cx
 __global__ void __launch_bounds__(1024)
 k_harris_pick(const uint64_t *list, const uint32_t *listCount, uint32_t listCapacity, float minDistance,
               int cell, int gridW, int gridH, vx_keypoint_like *out, uint32_t outCapacity, uint32_t *outCount,
-              uint32_t *numCorners, uint32_t *status)
+              uint32_t *numCorners, uint32_t *status, bool clusterPath)
 {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     PickSmem &S = *reinterpret_cast<PickSmem *>(smem_raw);
     const int tid = threadIdx.x, nt = blockDim.x;
     const int n = (int)min(*listCount, listCapacity);
-    if (n > kPickMax) {   // more candidates than this kernel holds: report, emit nothing
-        if (tid == 0) { atomicOr(status, 2u); *outCount = 0; if (numCorners) *numCorners = 0; }
+    if (n > kPickMax) {
+        // more candidates than this kernel holds: the cluster kernel after it takes them, or,
+        // without its scratch, report and emit nothing
+        if (!clusterPath && tid == 0) { atomicOr(status, 2u); *outCount = 0; if (numCorners) *numCorners = 0; }
         return;
     }
     int np2 = 1;
@@ -1107,6 +1131,219 @@ k_harris_pick(const uint64_t *list, const uint32_t *listCount, uint32_t listCapa
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Dense candidate sets (more than kPickMax; the reference's list holds up to W*H entries,
+// ago_drama_divide.cpp:1726): the same greedy pick by one cluster of kPCtas CTAs over
+// global scratch.  The hardware schedules a cluster's CTAs together, so cluster barriers
+// (no software spin) separate the phases:
+//   1. LSD radix sort, 8 passes of 8 bits, of the keys mapped so that ascending unsigned
+//      order is the reference's descending int64 order; each pass is stable (per-CTA digit
+//      counts in global memory, per-tile warp ranks from __match_any_sync);
+//   2. a dense cell grid (head per cell, next per candidate);
+//   3. the rounds of decisions of the shared-memory kernel over the whole cluster, until no
+//      candidate is undecided (each round decides at least the highest-priority undecided
+//      candidate, so at most n rounds);
+//   4. compaction of the kept candidates in sorted order.
+// ---------------------------------------------------------------------------------
+constexpr int kPCtas = 8, kPThreads = 512, kPWarps = kPThreads / 32;
+constexpr uint64_t kSignBit = 0x8000000000000000ull;
+
+struct PickScratch { uint64_t *a, *b; uint32_t *hist; int *head, *next; uint8_t *state; uint32_t *flags; };
+
+static size_t pick_align(size_t v) { return (v + 255) & ~(size_t)255; }
+
+static size_t pick_scratch_layout(uint32_t W, uint32_t H, uint32_t listCapacity, float minDistance, void *base,
+                                  PickScratch *ps, int *cellOut, int *gwOut, int *ghOut)
+{
+    int cell = 1, gw = 1, gh = 1;
+    if (minDistance > 2.0f) {   // grid geometry of ago_kernel_api.cpp:20806-20809
+        cell = (int)floor((double)minDistance / 1.41421356237309504880);
+        gw = (int)((W + cell - 1) / cell);
+        gh = (int)((H + cell - 1) / cell);
+    }
+    if (cellOut) { *cellOut = cell; *gwOut = gw; *ghOut = gh; }
+    const size_t n = listCapacity;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += pick_align(bytes); return o; };
+    const size_t oa = take(n * 8), ob = take(n * 8), oh = take(kPCtas * 256 * 4), ohead = take((size_t)gw * gh * 4),
+                 onext = take(n * 4), ost = take(n), ofl = take(64);
+    if (ps && base) {
+        uint8_t *b = (uint8_t *)base;
+        ps->a = (uint64_t *)(b + oa); ps->b = (uint64_t *)(b + ob); ps->hist = (uint32_t *)(b + oh);
+        ps->head = (int *)(b + ohead); ps->next = (int *)(b + onext); ps->state = b + ost; ps->flags = (uint32_t *)(b + ofl);
+    }
+    return off;
+}
+
+__device__ __forceinline__ uint64_t pick_unmap(uint64_t t) { return ~t ^ kSignBit; }
+
+__global__ void __cluster_dims__(kPCtas, 1, 1) __launch_bounds__(kPThreads)
+k_harris_pick_cluster(const uint64_t *list, const uint32_t *listCount, uint32_t listCapacity, float minDistance,
+                      int cell, int gridW, int gridH, vx_keypoint_like *out, uint32_t outCapacity, uint32_t *outCount,
+                      uint32_t *numCorners, uint32_t *status, PickScratch P)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int n = (int)min(*listCount, listCapacity);
+    if (n <= kPickMax) return;                       // the shared-memory kernel took this list
+    const int rank = (int)cluster.block_rank(), tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int gtid = rank * kPThreads + tid, gstride = kPCtas * kPThreads;
+    const int per = (n + kPCtas - 1) / kPCtas;
+    const int c0 = min(rank * per, n), c1 = min(c0 + per, n);   // this CTA's contiguous chunk
+    __shared__ uint32_t hist[256], base[256];
+    __shared__ uint16_t wc[kPWarps][256];
+    __shared__ int kept;
+
+    // ---- 1. radix sort (the 8th pass leaves the keys in P.a)
+    for (int i = c0 + tid; i < c1; i += kPThreads) P.a[i] = ~(list[i] ^ kSignBit);
+    uint64_t *src = P.a, *dst = P.b;
+    for (int pass = 0; pass < 8; pass++) {
+        const int shift = pass * 8;
+        if (tid < 256) hist[tid] = 0;
+        __syncthreads();
+        for (int i = c0 + tid; i < c1; i += kPThreads) atomicAdd(&hist[(src[i] >> shift) & 255], 1u);
+        __syncthreads();
+        if (tid < 256) P.hist[rank * 256 + tid] = hist[tid];
+        __threadfence();
+        cluster.sync();
+        if (tid < 256) {   // digit d of this CTA starts after every smaller digit and after d in lower ranks
+            uint32_t tot = 0, lower = 0;
+            for (int c = 0; c < kPCtas; c++) {
+                const uint32_t v = __ldcg(&P.hist[c * 256 + tid]);
+                tot += v;
+                if (c < rank) lower += v;
+            }
+            hist[tid] = tot;
+            base[tid] = lower;
+        }
+        __syncthreads();
+        if (tid == 0) { uint32_t run = 0; for (int d = 0; d < 256; d++) { const uint32_t t = hist[d]; hist[d] = run; run += t; } }
+        __syncthreads();
+        if (tid < 256) base[tid] += hist[tid];
+        __syncthreads();
+        for (int t0 = c0; t0 < c1; t0 += kPThreads) {   // stable scatter, one tile of kPThreads keys at a time
+            const int i = t0 + tid;
+            const bool valid = i < c1;
+            const uint64_t key = valid ? src[i] : 0;
+            const int d = valid ? (int)((key >> shift) & 255) : 256;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const int r = __popc(peers & ((1u << lane) - 1));
+            for (int k = tid; k < kPWarps * 256; k += kPThreads) (&wc[0][0])[k] = 0;
+            __syncthreads();
+            if (valid && r == 0) wc[w][d] = (uint16_t)__popc(peers);
+            __syncthreads();
+            if (tid < 256) {
+                uint32_t run = 0;
+                for (int q = 0; q < kPWarps; q++) { const uint32_t c = wc[q][tid]; wc[q][tid] = (uint16_t)run; run += c; }
+                hist[tid] = run;
+            }
+            __syncthreads();
+            if (valid) dst[base[d] + wc[w][d] + r] = key;
+            __syncthreads();
+            if (tid < 256) base[tid] += hist[tid];
+            __syncthreads();
+        }
+        __threadfence();
+        cluster.sync();
+        uint64_t *t = src; src = dst; dst = t;
+    }
+    const uint64_t *key = src;
+
+    // ---- 2./3. grid and rounds of decisions
+    const bool useGrid = minDistance > 2.0f;
+    if (useGrid) {
+        for (int c = gtid; c < gridW * gridH; c += gstride) P.head[c] = -1;
+        for (int i = gtid; i < n; i += gstride) P.state[i] = 0;
+        if (gtid < 3) P.flags[gtid] = 0;
+        __threadfence();
+        cluster.sync();
+        for (int i = gtid; i < n; i += gstride) {
+            const uint64_t k = pick_unmap(key[i]);
+            const int x = kx(k), y = ky(k);
+            const int cx = x / cell, cy = y / cell;
+            if (x < 0 || y < 0 || cx >= gridW || cy >= gridH) {   // outside the image the grid covers
+                P.state[i] = 2;
+                atomicOr(status, AGOCUDA_PICK_STATUS_BAD_ENTRY);
+                continue;
+            }
+            P.next[i] = atomicExch(&P.head[cy * gridW + cx], i);
+        }
+        __threadfence();
+        cluster.sync();
+        const int md2 = (int)ceilf(__fmul_rn(minDistance, minDistance));
+        for (int round = 0; round <= n; round++) {
+            if (gtid == 0) P.flags[(round + 1) % 3] = 0;
+            bool undecided = false;
+            for (int i = gtid; i < n; i += gstride) {
+                if (__ldcg(&P.state[i])) continue;
+                const uint64_t k = pick_unmap(key[i]);
+                const int x = kx(k), y = ky(k), cx = x / cell, cy = y / cell;
+                bool blocked = false, waiting = false;
+                for (int yy = max(cy - 2, 0); yy <= min(cy + 2, gridH - 1) && !blocked; yy++)
+                    for (int xx = max(cx - 2, 0); xx <= min(cx + 2, gridW - 1) && !blocked; xx++)
+                        for (int j = __ldcg(&P.head[yy * gridW + xx]); j >= 0; j = __ldcg(&P.next[j])) {
+                            if (j >= i) continue;   // only higher-priority candidates matter
+                            const uint64_t kj = pick_unmap(key[j]);
+                            const int dx = kx(kj) - x, dy = ky(kj) - y;
+                            if (!((xx == cx && yy == cy) || (dx * dx + dy * dy < md2))) continue;
+                            const uint8_t sj = __ldcg(&P.state[j]);
+                            if (sj == 1) { blocked = true; break; }
+                            if (sj == 0) waiting = true;
+                        }
+                if (blocked) __stcg(&P.state[i], (uint8_t)2);
+                else if (!waiting) __stcg(&P.state[i], (uint8_t)1);
+                else undecided = true;
+            }
+            if (__syncthreads_or(undecided) && tid == 0) atomicOr(&P.flags[round % 3], 1u);
+            __threadfence();
+            cluster.sync();
+            if (__ldcg(&P.flags[round % 3]) == 0) break;   // the same value for every thread of the cluster
+        }
+    } else {
+        for (int i = gtid; i < n; i += gstride) P.state[i] = 1;
+        __threadfence();
+        cluster.sync();
+    }
+
+    // ---- 4. kept candidates in sorted order: per-CTA counts, then tile scans of the chunk
+    int mine = 0;
+    for (int t0 = c0; t0 < c1; t0 += kPThreads) {
+        const int i = t0 + tid;
+        mine += __syncthreads_count(i < c1 && __ldcg(&P.state[i]) == 1);
+    }
+    if (tid == 0) P.hist[rank] = (uint32_t)mine;
+    __threadfence();
+    cluster.sync();
+    if (tid == 0) {
+        int before = 0, total = 0;
+        for (int c = 0; c < kPCtas; c++) { const int v = (int)__ldcg(&P.hist[c]); total += v; if (c < rank) before += v; }
+        kept = before;
+        if (rank == 0) { *outCount = min((uint32_t)total, outCapacity); if (numCorners) *numCorners = (uint32_t)total; }
+    }
+    __syncthreads();
+    __shared__ int warpSums[kPWarps];
+    for (int t0 = c0; t0 < c1; t0 += kPThreads) {
+        const int i = t0 + tid;
+        const int f = (i < c1 && __ldcg(&P.state[i]) == 1) ? 1 : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) warpSums[w] = __popc(m);
+        __syncthreads();
+        int off = 0;
+        for (int q = 0; q < w; q++) off += warpSums[q];
+        const int pos = kept + off + __popc(m & ((1u << lane) - 1));
+        if (f && pos < (int)outCapacity) {
+            const uint64_t kk = pick_unmap(key[i]);
+            vx_keypoint_like kp;
+            kp.x = kx(kk); kp.y = ky(kk); kp.strength = ks(kk);
+            kp.scale = 0.f; kp.orientation = 0.f; kp.tracking_status = 1; kp.error = 0.f;
+            out[pos] = kp;
+        }
+        __syncthreads();
+        if (tid == 0) { int t = 0; for (int q = 0; q < kPWarps; q++) t += warpSums[q]; kept += t; }
+        __syncthreads();
+    }
+}
+
 bool aligned(const void *p, unsigned a) { return ((uintptr_t)p & (a - 1)) == 0; }
 
 }  // namespace
@@ -1173,7 +1410,7 @@ static int hysteresis_tail(cudaStream_t s, int W, int H, uint8_t *out, int outSt
     const size_t n = (size_t)W * H;
     cudaMemsetAsync(bits, 0, ((n + 31) / 32) * sizeof(uint32_t), s);
     k_hyst_union<<<row_grid(W, H, 256), 256, 0, s>>>(W, H, L, err);
-    k_hyst_mark<<<1184, 256, 0, s>>>(W, L, strong, strongCount, capacity, bits);
+    k_hyst_mark<<<1184, 256, 0, s>>>(W, H, L, strong, strongCount, capacity, bits, err);
     k_hyst_output<<<row_grid(W, H, 256), 256, 0, s>>>(W, H, out, outStride, L, bits);
     agocuda_count_launch(3);
     return agocuda_launch_status();
@@ -1206,8 +1443,28 @@ constexpr size_t kNoAllocLabelBytes = kNoAllocMaxPixels * sizeof(int);   // 8 Mi
 constexpr size_t kNoAllocBitBytes = kNoAllocMaxPixels / 8;               // 256 KiB
 static __device__ __align__(256) uint8_t g_noalloc_trace_scratch[kNoAllocLabelBytes + kNoAllocBitBytes];
 
+// The array's device address, per device, together with the context it was looked up in:
+// after cudaDeviceReset the device gets a new primary context and the module may load at
+// another address, so a changed context means a fresh lookup.
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_ptr[256];
+static CUcontext g_noalloc_ctx[256];
+
+// cuCtxGetCurrent through the runtime's entry-point query: the library does not link the
+// driver library itself, so it still loads on a host without a GPU driver.
+static CUresult current_context(CUcontext *ctx)
+{
+    using Fn = CUresult (*)(CUcontext *);
+    static Fn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (Fn) nullptr;
+        return (Fn)p;
+    }();
+    return fn ? fn(ctx) : CUDA_ERROR_NOT_FOUND;
+}
 
 extern "C" int agocuda_CannyEdgeTrace_U8_U8XY_noalloc(void *stream, uint32_t W, uint32_t H, uint8_t *pImg, uint32_t stride,
                                                       const uint32_t *pStack, const uint32_t *pStackCount,
@@ -1223,11 +1480,14 @@ extern "C" int agocuda_CannyEdgeTrace_U8_U8XY_noalloc(void *stream, uint32_t W, 
     void *base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
+        CUcontext cur = nullptr;
+        if (!g_noalloc_ptr[dev] || current_context(&cur) != CUDA_SUCCESS || cur != g_noalloc_ctx[dev]) {
             void *p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_trace_scratch);
+            e = cudaGetSymbolAddress(&p, g_noalloc_trace_scratch);   // makes the primary context current
             if (e != cudaSuccess || !p) return e != cudaSuccess ? (int)e : AGOCUDA_INVALID_PARAMS;
+            if (current_context(&cur) != CUDA_SUCCESS) return AGOCUDA_INVALID_PARAMS;
             g_noalloc_ptr[dev] = p;
+            g_noalloc_ctx[dev] = cur;
         }
         base = g_noalloc_ptr[dev];
     }
@@ -1329,20 +1589,25 @@ extern "C" int agocuda_NonMaxSupp_XY_ANY_3x3(void *stream, uint32_t W, uint32_t 
     return agocuda_launch_status();
 }
 
+extern "C" size_t agocuda_HarrisMergeSortAndPick_scratch_size(uint32_t W, uint32_t H, uint32_t listCapacity,
+                                                              float minDistance)
+{
+    return pick_scratch_layout(W, H, listCapacity, minDistance, nullptr, nullptr, nullptr, nullptr, nullptr);
+}
+
 extern "C" int agocuda_HarrisMergeSortAndPick_XY_XYS(void *stream, uint32_t W, uint32_t H, const uint64_t *pList,
                                                      const uint32_t *pListCount, uint32_t listCapacity, float minDistance,
                                                      void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
-                                                     uint32_t *pNumCorners, uint32_t *pStatus)
+                                                     uint32_t *pNumCorners, void *scratch, size_t scratchBytes,
+                                                     uint32_t *pStatus)
 {
     if (!pList || !pListCount || !pCorners || !pCornerCount || !pStatus || !W || !H || !(minDistance > 0.0f))
         return AGOCUDA_INVALID_PARAMS;
-    // grid geometry of ago_kernel_api.cpp:20806-20809
     int cell = 1, gw = 1, gh = 1;
-    if (minDistance > 2.0f) {
-        cell = (int)floor((double)minDistance / 1.41421356237309504880);
-        gw = (int)((W + cell - 1) / cell);
-        gh = (int)((H + cell - 1) / cell);
-    }
+    PickScratch ps{};
+    const size_t need = pick_scratch_layout(W, H, listCapacity, minDistance, scratch, &ps, &cell, &gw, &gh);
+    const bool cluster = scratch != nullptr && listCapacity > (uint32_t)kPickMax;
+    if (cluster && (scratchBytes < need || !aligned(scratch, 256))) return AGOCUDA_INVALID_PARAMS;
     static bool attr = false;
     const int smem = (int)sizeof(PickSmem);
     if (!attr) {
@@ -1350,24 +1615,38 @@ extern "C" int agocuda_HarrisMergeSortAndPick_XY_XYS(void *stream, uint32_t W, u
             return agocuda_launch_status();
         attr = true;
     }
-    k_harris_pick<<<1, 1024, smem, as_stream(stream)>>>(pList, pListCount, listCapacity, minDistance, cell, gw, gh,
-                                                        (vx_keypoint_like *)pCorners, cornerCapacity, pCornerCount,
-                                                        pNumCorners, pStatus);
+    cudaStream_t s = as_stream(stream);
+    k_harris_pick<<<1, 1024, smem, s>>>(pList, pListCount, listCapacity, minDistance, cell, gw, gh,
+                                        (vx_keypoint_like *)pCorners, cornerCapacity, pCornerCount, pNumCorners, pStatus,
+                                        cluster);
     agocuda_count_launch(1);
+    if (cluster) {
+        k_harris_pick_cluster<<<kPCtas, kPThreads, 0, s>>>(pList, pListCount, listCapacity, minDistance, cell, gw, gh,
+                                                           (vx_keypoint_like *)pCorners, cornerCapacity, pCornerCount,
+                                                           pNumCorners, pStatus, ps);
+        agocuda_count_launch(1);
+    }
     return agocuda_launch_status();
 }
+
+// Candidate list capacity of the fused Harris: the suppression keeps no two 8-adjacent
+// pixels (>= towards the left and upper row, > towards the right and lower row), so at most
+// one pixel of every 2x2 block survives.
+static uint32_t harris_list_capacity(uint32_t W, uint32_t H) { return ((W + 1) / 2) * ((H + 1) / 2); }
 
 extern "C" int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t W, uint32_t H, const uint8_t *pSrc, uint32_t srcStride,
                                                float sensitivity, float strengthThreshold, float normFactor, float minDistance,
                                                void *pCorners, uint32_t cornerCapacity, uint32_t *pCornerCount,
                                                uint32_t *pNumCorners, void *scratch, size_t scratchBytes, uint32_t *pStatus)
 {
-    const uint32_t cap = kPickMax * 4;   // candidate list capacity (the pick reports overflow)
+    const uint32_t cap = harris_list_capacity(W, H);
+    const size_t listBytes = pick_align((size_t)cap * 8);
     if (!pSrc || !pCorners || !pCornerCount || !scratch || !pStatus || W < 3 || H < 3 || srcStride < W ||
-        scratchBytes < 256 + (size_t)cap * 8 || !aligned(scratch, 256))
+        scratchBytes < agocuda_fused_HarrisCorners_scratch_size(W, H, minDistance) || !aligned(scratch, 256))
         return AGOCUDA_INVALID_PARAMS;
     uint32_t *cnt = (uint32_t *)scratch;
     uint64_t *list = (uint64_t *)((uint8_t *)scratch + 256);
+    void *pickScratch = (uint8_t *)scratch + 256 + listBytes;
     cudaStream_t s = as_stream(stream);
     cudaMemsetAsync(cnt, 0, 4, s);
     const int strips = (int)div_up(W, kHCols);
@@ -1377,7 +1656,12 @@ extern "C" int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t W, uint32_
     int rc = agocuda_launch_status();
     if (rc) return rc;
     return agocuda_HarrisMergeSortAndPick_XY_XYS(stream, W, H, list, cnt, cap, minDistance, pCorners, cornerCapacity,
-                                                 pCornerCount, pNumCorners, pStatus);
+                                                 pCornerCount, pNumCorners, pickScratch,
+                                                 agocuda_HarrisMergeSortAndPick_scratch_size(W, H, cap, minDistance), pStatus);
 }
 
-extern "C" size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t, uint32_t) { return 256 + (size_t)kPickMax * 4 * 8; }
+extern "C" size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t W, uint32_t H, float minDistance)
+{
+    const uint32_t cap = harris_list_capacity(W, H);
+    return 256 + pick_align((size_t)cap * 8) + agocuda_HarrisMergeSortAndPick_scratch_size(W, H, cap, minDistance);
+}

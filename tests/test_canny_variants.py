@@ -8,8 +8,8 @@ restatement (oracle_CannySobel_U16_U8_NxN, pinned to the reference HAF kernels i
 test_oracle_pin_vision.py) followed by the pinned suppression and trace.
 
 CPU: the reference library's node equals the oracle chain inside the valid rectangle.
-GPU: the gradient kernels equal the oracle plane.  The engine refuses these graphs at
-verification for now (test_engine_rejects_variants_for_now)."""
+GPU: the gradient kernels equal the oracle plane, and the engine's graphs equal the oracle
+chain."""
 import ctypes as C
 
 import numpy as np
@@ -138,15 +138,43 @@ def test_engine_gradient_kernels(cuda, agocuda, gs, norm, W, H):
 
 
 @pytest.mark.gpu
-def test_engine_rejects_variants_for_now(cuda):
-    """Graphs with these gradients are refused at verification (kernels only, so far)."""
+@pytest.mark.parametrize("W,H", [(100, 60), (333, 97), (644, 360), (3840, 2160)])
+@pytest.mark.parametrize("gs,norm", VARIANTS)
+def test_engine_canny_variants(cuda, gs, norm, W, H):
+    """The engine's graph (gradient, suppression -- quartered thresholds for 7x7 -- and the
+    device hysteresis) equals the oracle chain inside the reference's valid rectangle."""
+    _check(V.OpenVX(), gs, norm, W, H)
+
+
+@pytest.mark.gpu
+def test_engine_canny_variants_share_a_context(cuda):
+    """All variants as graphs of one context, run twice, released one by one and then with
+    the context: every graph's teardown leaves the others and the context intact."""
     api = V.OpenVX()
+    W, H = 333, 97
     ctx = api.obj(api.vxCreateContext(), "context")
     try:
-        src = api.obj(api.vxCreateImage(ctx, 64, 48, V.VX_DF_IMAGE_U8), "image")
-        dst = api.obj(api.vxCreateImage(ctx, 64, 48, V.VX_DF_IMAGE_U8), "image")
-        g = api.obj(api.vxCreateGraph(ctx), "graph")
-        api.obj(api.vxCannyEdgeDetectorNode(g, src, api.threshold_range(ctx, 600, 1200), 5, V.VX_NORM_L1, dst), "canny")
-        assert api.vxVerifyGraph(g) == V.VX_ERROR_NOT_SUPPORTED
+        img = _scene(W, H, seed=5)
+        src = api.obj(api.vxCreateImage(ctx, W, H, V.VX_DF_IMAGE_U8), "image")
+        api.write_plane(src, img)
+        graphs = []
+        for gs, norm in VARIANTS:
+            dst = api.obj(api.vxCreateImage(ctx, W, H, V.VX_DF_IMAGE_U8), "image")
+            g = api.obj(api.vxCreateGraph(ctx), "graph")
+            lo, hi = THRESH[gs]
+            n = V.VX_NORM_L1 if norm == "L1" else V.VX_NORM_L2
+            api.obj(api.vxCannyEdgeDetectorNode(g, src, api.threshold_range(ctx, lo, hi), gs, n, dst), "canny")
+            api.ok(api.vxVerifyGraph(g), "verify")
+            graphs.append((g, dst, gs, norm, lo, hi))
+        for _ in range(2):
+            for g, dst, gs, norm, lo, hi in graphs:
+                api.ok(api.vxProcessGraph(g), "process")
+                b = gs // 2 + 1
+                want = oracle_canny(img, gs, norm == "L2", lo, hi)
+                np.testing.assert_array_equal(api.read_plane(dst)[b:H - b, b:W - b], want[b:H - b, b:W - b])
+        for g, *_ in graphs[::2]:
+            api.ok(api.vxReleaseGraph(C.byref(C.c_void_p(g))), "release graph")
+        for g, dst, gs, norm, lo, hi in graphs[1::2]:
+            api.ok(api.vxProcessGraph(g), "process after other graphs were released")
     finally:
-        api.vxReleaseContext(C.byref(C.c_void_p(ctx)))
+        assert api.vxReleaseContext(C.byref(C.c_void_p(ctx))) == 0

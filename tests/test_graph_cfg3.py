@@ -43,6 +43,20 @@ def test_reference_graph_matches_oracle(W, H):
     _check(got, OC.color_scale_warp(rgb, g.matrices[0]), W, reference_run=True)
 
 
+def test_reference_graph_matches_oracle_full_size():
+    """A 3840x2160 configuration-3 frame: the reference library equals the oracle."""
+    lib = O.ref_lib()
+    if lib is None:
+        pytest.skip("reference library not built")
+    api = V.OpenVX(lib)
+    ctx = api.obj(api.vxCreateContext(), "context")
+    rgb = WL.cfg3_frame(seed=5, width=3840, height=2160)
+    g = WL.Cfg3Graph(api, ctx, [(3840, 2160)])
+    g.run([rgb])
+    got, = g.results()
+    _check(got, OC.color_scale_warp(rgb, g.matrices[0]), 3840, reference_run=True)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("flags", [None, V.OPT_NO_FUSION])
 def test_engine_cfg3(cuda, flags):

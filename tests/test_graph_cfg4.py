@@ -85,6 +85,28 @@ def test_reference_graph_matches_oracle(virtual):
     run_and_compare(api, ctx, [(320, 240), (160, 120), (256, 200)], 400, levels=4, virtual=virtual)
 
 
+def test_reference_graph_matches_oracle_full_size():
+    """Configuration-4 pairs at 1920x1080 and 3840x2160, 5 levels, 2000 points, two
+    executions: the reference library equals the oracle keypoint for keypoint."""
+    lib = O.ref_lib()
+    if lib is None:
+        pytest.skip("reference library not built")
+    api = V.OpenVX(lib)
+    ctx = api.obj(api.vxCreateContext(), "context")
+    run_and_compare(api, ctx, [(1920, 1080), (3840, 2160)], 2000, executions=2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flags", [None, V.OPT_NO_FUSION])
+def test_engine_cfg4_full_size(cuda, flags):
+    """The engine at the configuration's full frame sizes, 2000 points per pair, three
+    executions: every keypoint record equals the oracle's (positions exactly, which is
+    inside the 0.01 px bound)."""
+    api = V.OpenVX()
+    ctx = api.obj(api.vxCreateContext(), "context")
+    run_and_compare(api, ctx, [(1920, 1080), (3840, 2160), (1280, 720), (640, 480)], 2000, flags=flags)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("flags", [None, V.OPT_NO_FUSION, V.OPT_NO_GRAPH_CAPTURE])
 def test_engine_cfg4(cuda, flags):

@@ -27,17 +27,37 @@ def lib():
         "agocuda_HarrisSobel_HG3_U8_3x3": [vp, u32, u32, vp, u32, vp, u32],
         "agocuda_HarrisScore_HVC_HG3_3x3": [vp, u32, u32, vp, u32, vp, u32, f32, f32, f32],
         "agocuda_NonMaxSupp_XY_ANY_3x3": [vp, u32, u32, vp, u32, vp, vp, u32],
-        "agocuda_HarrisMergeSortAndPick_XY_XYS": [vp, u32, u32, vp, vp, u32, f32, vp, u32, vp, vp, vp],
+        "agocuda_HarrisMergeSortAndPick_XY_XYS": [vp, u32, u32, vp, vp, u32, f32, vp, u32, vp, vp, vp, sz, vp],
         "agocuda_fused_HarrisCorners_3x3": [vp, u32, u32, vp, u32, f32, f32, f32, f32, vp, u32, vp, vp, vp, sz, vp],
     }
     for n, a in sigs.items():
         getattr(L, n).argtypes = a
         getattr(L, n).restype = C.c_int
-    for n in ("agocuda_CannyEdgeTrace_scratch_size", "agocuda_fused_CannyEdgeDetector_scratch_size",
-              "agocuda_fused_HarrisCorners_scratch_size"):
+    for n in ("agocuda_CannyEdgeTrace_scratch_size", "agocuda_fused_CannyEdgeDetector_scratch_size"):
         getattr(L, n).argtypes = [u32, u32]
         getattr(L, n).restype = C.c_size_t
+    L.agocuda_fused_HarrisCorners_scratch_size.argtypes = [u32, u32, f32]
+    L.agocuda_fused_HarrisCorners_scratch_size.restype = C.c_size_t
+    L.agocuda_HarrisMergeSortAndPick_scratch_size.argtypes = [u32, u32, u32, f32]
+    L.agocuda_HarrisMergeSortAndPick_scratch_size.restype = C.c_size_t
     return L
+
+
+def _pick(lib, W, H, lst, cnt, list_cap, mind, cap, scratch=True):
+    """agocuda_HarrisMergeSortAndPick_XY_XYS -> (corners, corner count, num corners, status)."""
+    import torch
+    D = _dev()
+    corners, ccount, ncorn, status = _buf(28 * cap), _buf(4), _buf(4), _buf(4)
+    sb = lib.agocuda_HarrisMergeSortAndPick_scratch_size(W, H, list_cap, mind) if scratch else 0
+    scr = _buf(sb) if scratch else None
+    base = scr.data_ptr() + (-scr.data_ptr() % 256) if scratch else None
+    assert lib.agocuda_HarrisMergeSortAndPick_XY_XYS(D.stream_ptr(), W, H, lst.data_ptr(), cnt.data_ptr(), list_cap, mind,
+                                                     corners.data_ptr(), cap, ccount.data_ptr(), ncorn.data_ptr(),
+                                                     base, sb, status.data_ptr()) == 0
+    torch.cuda.synchronize()
+    nk = int(ccount[:4].view(torch.int32).item())
+    return (corners[:28 * nk].cpu().numpy().view(OC.KP), nk, int(ncorn[:4].view(torch.int32).item()),
+            int(status[:4].view(torch.int32).item()))
 
 
 def _dev():
@@ -123,16 +143,11 @@ def test_harris_kernels(lib, cuda, W, H):
     np.testing.assert_array_equal(key(got), key(ref_list))
     for mind, cap in ((5.0, 32768), (5.0, 7), (1.5, 32768)):
         ref_c, ref_n = OC.harris_pick(ref_list, W, H, mind, cap)
-        corners, ccount, ncorn, status = _buf(28 * cap), _buf(4), _buf(4), _buf(4)
-        assert lib.agocuda_HarrisMergeSortAndPick_XY_XYS(D.stream_ptr(), W, H, lst.data_ptr(), cnt.data_ptr(), W * H, mind,
-                                                         corners.data_ptr(), cap, ccount.data_ptr(), ncorn.data_ptr(),
-                                                         status.data_ptr()) == 0
-        torch.cuda.synchronize()
-        assert int(status[0].item()) == 0
-        nk = int(ccount[:4].view(torch.int32).item())
-        assert int(ncorn[:4].view(torch.int32).item()) == ref_n
+        got_c, nk, got_n, status = _pick(lib, W, H, lst, cnt, W * H, mind, cap)
+        assert status == 0
+        assert got_n == ref_n
         assert nk == min(ref_n, cap)
-        np.testing.assert_array_equal(corners[:28 * nk].cpu().numpy().view(OC.KP), ref_c)
+        np.testing.assert_array_equal(got_c, ref_c)
 
 
 @pytest.mark.parametrize("W,H", [(200, 120), (1920, 1080), (3840, 2160)])
@@ -142,7 +157,7 @@ def test_fused_harris(lib, cuda, W, H):
     img = _img(W, H, 9 * W + H)
     ref_c, ref_n = OC.harris(img, capacity=32768)
     src = D.DevImg(H, W).upload(img)
-    sb = lib.agocuda_fused_HarrisCorners_scratch_size(W, H)
+    sb = lib.agocuda_fused_HarrisCorners_scratch_size(W, H, 5.0)
     scr, corners, ccount, ncorn, status = _buf(sb), _buf(28 * 32768), _buf(4), _buf(4), _buf(4)
     base = scr.data_ptr() + (-scr.data_ptr() % 256)
     for _ in range(2):
@@ -154,3 +169,96 @@ def test_fused_harris(lib, cuda, W, H):
         nk = int(ccount[:4].view(torch.int32).item())
         assert int(ncorn[:4].view(torch.int32).item()) == ref_n
         np.testing.assert_array_equal(corners[:28 * nk].cpu().numpy().view(OC.KP), ref_c)
+
+
+def test_edge_trace_seeds_off_the_map(lib, cuda):
+    """Stack entries the suppression never emits: a border pixel and a zero interior pixel
+    seed the weak components around them (the reference's trace grows from every entry
+    through its 8 neighbours), an entry outside the image is ignored and flagged."""
+    import torch
+    D = _dev()
+    W, H = 200, 120
+    img = _img(W, H, 4242)
+    _, supp, strong, ref_edges = OC.canny_parts(img)
+    supp = supp.copy()
+    yb = H // 2
+    supp[yb - 1:yb + 2, 0] = 0
+    supp[yb, 1:4] = 127                       # a weak run touching column 1, seeded from (0, yb)
+    weak_only = (supp == 127) & (ref_edges == 0)
+    weak_only[:, :6] = False
+    zero_seed = None
+    for y, x in zip(*np.nonzero(weak_only[2:H - 2, 2:W - 2])):
+        y, x = y + 2, x + 2
+        for dy, dx in ((-1, 0), (1, 0), (0, -1), (0, 1)):
+            if supp[y + dy, x + dx] == 0:
+                zero_seed = (x + dx, y + dy)
+                break
+        if zero_seed:
+            break
+    assert zero_seed is not None
+    seeds = np.array([(yb << 16) | 0, (zero_seed[1] << 16) | zero_seed[0]], np.uint32)
+    stack_in = np.concatenate([strong.astype(np.uint32), seeds])
+    # oracle: the same map and stack through the restated reference trace
+    o = OC.ago_img(H, W); o.set(supp)
+    ost = np.zeros(W * H, np.uint32); ost[:len(stack_in)] = stack_in
+    OC.fn("CannyEdgeTrace_U8_U8XY")(W, H, o.ptr, o.stride, W * H, ost.ctypes.data, len(stack_in))
+    expected = o.get()
+    assert (expected != ref_edges).any(), "the extra seeds must change the result"
+    # device: the same stack plus one entry outside the image
+    dev_stack = np.concatenate([stack_in, np.array([(5 << 16) | (W + 3)], np.uint32)])
+    out = D.DevImg(H, W).upload(supp)
+    st = torch.from_numpy(dev_stack.view(np.int32).copy()).cuda()
+    cnt = torch.tensor([len(dev_stack)], dtype=torch.int32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    sb = lib.agocuda_CannyEdgeTrace_scratch_size(W, H)
+    scr = _buf(sb)
+    base = scr.data_ptr() + (-scr.data_ptr() % 256)
+    assert lib.agocuda_CannyEdgeTrace_U8_U8XY(D.stream_ptr(), W, H, out.ptr, out.stride, st.data_ptr(), cnt.data_ptr(),
+                                              len(dev_stack), base, sb, status.data_ptr()) == 0
+    got = out.download()
+    np.testing.assert_array_equal(got[1:H - 1, 1:W - 1], expected[1:H - 1, 1:W - 1])
+    assert int(status.item()) == 8            # AGOCUDA_TRACE_STATUS_BAD_ENTRY
+
+
+@pytest.mark.parametrize("W,H,mind", [(3840, 2160, 5.0), (1920, 1080, 5.0), (640, 480, 10.0), (1920, 1080, 1.5)])
+def test_harris_dense_candidates(lib, cuda, W, H, mind):
+    """Pure noise: hundreds of thousands of candidates, far above the shared-memory pick's
+    8192, so the cluster pick runs; the corner list equals the oracle's in content and order,
+    per node and fused.  Without scratch the per-node pick reports the overflow instead."""
+    import torch
+    D = _dev()
+    img = np.random.default_rng(W + H).integers(0, 256, (H, W), dtype=np.int32).astype(np.uint8)
+    ref_c, ref_n = OC.harris(img, capacity=1 << 22, min_distance=mind)
+    _, _, ref_list = OC.harris_parts(img)
+    assert len(ref_list) > 8192
+    src = D.DevImg(H, W).upload(img)
+    hg3, hvc = D.DevImg(H, W, np.float32, channels=3), D.DevImg(H, W, np.float32)
+    assert lib.agocuda_HarrisSobel_HG3_U8_3x3(D.stream_ptr(), W, H, hg3.ptr, hg3.stride, src.ptr, src.stride) == 0
+    assert lib.agocuda_HarrisScore_HVC_HG3_3x3(D.stream_ptr(), W, H, hvc.ptr, hvc.stride, hg3.ptr, hg3.stride,
+                                               0.04, 1e-3, OC.harris_norm(3)) == 0
+    lst, cnt = _buf(8 * W * H), _buf(4)
+    assert lib.agocuda_NonMaxSupp_XY_ANY_3x3(D.stream_ptr(), W, H, hvc.ptr, hvc.stride, lst.data_ptr(), cnt.data_ptr(), W * H) == 0
+    cap = 1 << 22
+    for _ in range(2):   # twice: the scratch left by the first run must not matter
+        got_c, nk, got_n, status = _pick(lib, W, H, lst, cnt, W * H, mind, cap)
+        assert status == 0
+        assert got_n == ref_n and nk == min(ref_n, cap)
+        np.testing.assert_array_equal(got_c, ref_c)
+    small = 1000   # fewer slots than corners: the first ones in order, the full count
+    got_c, nk, got_n, _ = _pick(lib, W, H, lst, cnt, W * H, mind, small)
+    assert got_n == ref_n and nk == small
+    np.testing.assert_array_equal(got_c, ref_c[:small])
+    _, nk, _, status = _pick(lib, W, H, lst, cnt, W * H, mind, cap, scratch=False)
+    assert status == 2 and nk == 0
+    # fused front end + pick
+    sb = lib.agocuda_fused_HarrisCorners_scratch_size(W, H, mind)
+    scr, corners, ccount, ncorn, st = _buf(sb), _buf(28 * cap), _buf(4), _buf(4), _buf(4)
+    base = scr.data_ptr() + (-scr.data_ptr() % 256)
+    assert lib.agocuda_fused_HarrisCorners_3x3(D.stream_ptr(), W, H, src.ptr, src.stride, 0.04, 1e-3, OC.harris_norm(3),
+                                               mind, corners.data_ptr(), cap, ccount.data_ptr(), ncorn.data_ptr(),
+                                               base, sb, st.data_ptr()) == 0
+    torch.cuda.synchronize()
+    assert int(st[:4].view(torch.int32).item()) == 0
+    nk = int(ccount[:4].view(torch.int32).item())
+    assert int(ncorn[:4].view(torch.int32).item()) == ref_n
+    np.testing.assert_array_equal(corners[:28 * nk].cpu().numpy().view(OC.KP), ref_c)

@@ -1,7 +1,7 @@
 """The allocation-free hysteresis (agocuda_CannyEdgeTrace_U8_U8XY_noalloc) must produce
-exactly what the regular entry point produces with caller-allocated scratch, on two calls in
-a row (its fixed scratch array is shared by every call and keeps the previous contents), and
-must refuse images above its size limit without launching.
+exactly what the regular entry point produces with caller-allocated scratch, on calls in a
+row of different sizes and content (its fixed scratch array is shared by every call and keeps
+the previous call's contents), and must refuse images above its size limit without launching.
 
 This file is collected last on purpose so a stop-at-first-failure run has already run every
 other test; it also passes on its own in a fresh process."""
@@ -61,15 +61,11 @@ def _copy(img_dev):
     return d
 
 
-@pytest.mark.parametrize("W,H", [(1920, 1080), (640, 480)])
-def test_noalloc_edge_trace_matches_allocating_entry_point(lib, W, H):
+def _allocating_trace(lib, supp, stack, cnt, W, H):
+    """The regular entry point, scratch allocated by the caller: the expected result."""
     import torch
 
     from devbuf import stream_ptr
-    img = WL.cfg2_scene(seed=W + 3 * H, width=W, height=H, rects=min(200, W * H // 3000))
-    supp, stack, cnt = _suppressed_map(lib, img)
-
-    # regular entry point: scratch allocated by the caller
     ref = _copy(supp)
     sb = lib.agocuda_CannyEdgeTrace_scratch_size(W, H)
     scratch = torch.zeros(sb + 256, dtype=torch.uint8, device="cuda")
@@ -77,16 +73,27 @@ def test_noalloc_edge_trace_matches_allocating_entry_point(lib, W, H):
     status = torch.zeros(4, dtype=torch.int32, device="cuda")
     assert lib.agocuda_CannyEdgeTrace_U8_U8XY(stream_ptr(), W, H, ref.ptr, ref.stride, stack.data_ptr(), cnt.data_ptr(),
                                               W * H, base, sb, status.data_ptr()) == 0
-    expected = ref.download()
     assert int(status[0].item()) == 0
+    return ref.download()
 
-    # allocation-free entry point, twice in a row on fresh copies of the same input
-    for call in range(2):
+
+def test_noalloc_edge_trace_matches_allocating_entry_point(lib):
+    """Calls in a row with different sizes and content: a large image fills most of the
+    shared array, the smaller one after it must not see any of those labels or root bits,
+    and the third call repeats the first on the array the second left behind."""
+    import torch
+
+    from devbuf import stream_ptr
+    calls = [(1920, 1080, 11), (640, 480, 29), (1920, 1080, 11)]
+    for i, (W, H, seed) in enumerate(calls):
+        img = WL.cfg2_scene(seed=seed, width=W, height=H, rects=min(200, W * H // 3000))
+        supp, stack, cnt = _suppressed_map(lib, img)
+        expected = _allocating_trace(lib, supp, stack, cnt, W, H)
         got = _copy(supp)
         st = torch.zeros(4, dtype=torch.int32, device="cuda")
         assert lib.agocuda_CannyEdgeTrace_U8_U8XY_noalloc(stream_ptr(), W, H, got.ptr, got.stride, stack.data_ptr(),
                                                           cnt.data_ptr(), W * H, st.data_ptr()) == 0
-        np.testing.assert_array_equal(got.download(), expected, err_msg=f"call {call}")
+        np.testing.assert_array_equal(got.download(), expected, err_msg=f"call {i} ({W}x{H})")
         assert int(st[0].item()) == 0
 
 
