@@ -109,7 +109,8 @@ enum vx_enum_e {
 #define VX__E(id, n) (VX_ENUM_BASE(VX_ID_KHRONOS, id) + (n))
 #define VX__A(obj, n) (VX_ATTRIBUTE_BASE(VX_ID_KHRONOS, obj) + (n))
 
-enum { VX_INPUT = VX__E(VX_ENUM_DIRECTION, 0), VX_OUTPUT = VX__E(VX_ENUM_DIRECTION, 1) };
+enum { VX_INPUT = VX__E(VX_ENUM_DIRECTION, 0), VX_OUTPUT = VX__E(VX_ENUM_DIRECTION, 1),
+       VX_BIDIRECTIONAL = VX__E(VX_ENUM_DIRECTION, 2) };
 enum { VX_ACTION_CONTINUE = VX__E(VX_ENUM_ACTION, 0), VX_ACTION_ABANDON = VX__E(VX_ENUM_ACTION, 1) };
 enum { VX_DIRECTIVE_DISABLE_LOGGING = VX__E(VX_ENUM_DIRECTIVE, 0), VX_DIRECTIVE_ENABLE_LOGGING = VX__E(VX_ENUM_DIRECTIVE, 1),
        VX_DIRECTIVE_DISABLE_PERFORMANCE = VX__E(VX_ENUM_DIRECTIVE, 2), VX_DIRECTIVE_ENABLE_PERFORMANCE = VX__E(VX_ENUM_DIRECTIVE, 3) };
@@ -248,6 +249,10 @@ enum vx_kernel_e {
     VX_KERNEL_WARP_AFFINE = VX__K(0x23), VX_KERNEL_WARP_PERSPECTIVE = VX__K(0x24),
     VX_KERNEL_HARRIS_CORNERS = VX__K(0x25), VX_KERNEL_OPTICAL_FLOW_PYR_LK = VX__K(0x27),
     VX_KERNEL_REMAP = VX__K(0x28), VX_KERNEL_HALFSCALE_GAUSSIAN = VX__K(0x29),
+    VX_KERNEL_EQUALIZE_HISTOGRAM = VX__K(0xA), VX_KERNEL_MEAN_STDDEV = VX__K(0xC), VX_KERNEL_CUSTOM_CONVOLUTION = VX__K(0x14),
+    VX_KERNEL_ACCUMULATE = VX__K(0x16), VX_KERNEL_ACCUMULATE_WEIGHTED = VX__K(0x17), VX_KERNEL_ACCUMULATE_SQUARE = VX__K(0x18),
+    VX_KERNEL_MINMAXLOC = VX__K(0x19), VX_KERNEL_MULTIPLY = VX__K(0x20), VX_KERNEL_FAST_CORNERS = VX__K(0x26),
+    VX_KERNEL_WEIGHTED_AVERAGE = VX__K(0x40),
 };
 
 /* structures */
@@ -391,6 +396,85 @@ vx_status vxSetRemapPoint(vx_remap table, vx_uint32 dst_x, vx_uint32 dst_y, vx_f
 vx_status vxCopyRemapPatch(vx_remap remap, const vx_rectangle_t *rect, vx_size user_stride_y, void *user_ptr,
                            vx_enum user_coordinate_type, vx_enum usage, vx_enum user_mem_type);
 vx_status vxQueryRemap(vx_remap table, vx_enum attribute, void *ptr, vx_size size);
+
+/* ---------------- kernels, generic nodes, parameters (vx_api.h group_kernel / group_parameter) ---------------- */
+#define VX_MAX_KERNEL_NAME (256)
+enum { VX_KERNEL_PARAMETERS = VX__A(VX_TYPE_KERNEL, 0), VX_KERNEL_NAME = VX__A(VX_TYPE_KERNEL, 1),
+       VX_KERNEL_ENUM = VX__A(VX_TYPE_KERNEL, 2), VX_KERNEL_LOCAL_DATA_SIZE = VX__A(VX_TYPE_KERNEL, 3) };
+enum { VX_PARAMETER_INDEX = VX__A(VX_TYPE_PARAMETER, 0), VX_PARAMETER_DIRECTION = VX__A(VX_TYPE_PARAMETER, 1),
+       VX_PARAMETER_TYPE = VX__A(VX_TYPE_PARAMETER, 2), VX_PARAMETER_STATE = VX__A(VX_TYPE_PARAMETER, 3),
+       VX_PARAMETER_REF = VX__A(VX_TYPE_PARAMETER, 4) };
+vx_kernel vxGetKernelByName(vx_context context, const vx_char *name);
+vx_kernel vxGetKernelByEnum(vx_context context, vx_enum kernel);
+vx_status vxQueryKernel(vx_kernel kernel, vx_enum attribute, void *ptr, vx_size size);
+vx_status vxReleaseKernel(vx_kernel *kernel);
+vx_status vxLoadKernels(vx_context context, const vx_char *module);
+vx_node vxCreateGenericNode(vx_graph graph, vx_kernel kernel);
+vx_status vxSetParameterByIndex(vx_node node, vx_uint32 index, vx_reference value);
+vx_parameter vxGetParameterByIndex(vx_node node, vx_uint32 index);
+vx_parameter vxGetKernelParameterByIndex(vx_kernel kernel, vx_uint32 index);
+vx_status vxSetParameterByReference(vx_parameter parameter, vx_reference value);
+vx_status vxQueryParameter(vx_parameter parameter, vx_enum attribute, void *ptr, vx_size size);
+vx_status vxReleaseParameter(vx_parameter *param);
+
+/* ---------------- image views, convolutions, legacy access (vx_api.h, vx_compatibility.h, vx_ext_amd.h) ---------------- */
+enum { VX_CONVOLUTION_ROWS = VX__A(VX_TYPE_CONVOLUTION, 0), VX_CONVOLUTION_COLUMNS = VX__A(VX_TYPE_CONVOLUTION, 1),
+       VX_CONVOLUTION_SCALE = VX__A(VX_TYPE_CONVOLUTION, 2), VX_CONVOLUTION_SIZE = VX__A(VX_TYPE_CONVOLUTION, 3) };
+typedef struct {
+    vx_size components;
+    vx_size planes;
+    vx_size pixelSizeInBitsNum;
+    vx_enum colorSpace;
+    vx_enum channelRange;
+    vx_size pixelSizeInBitsDenom;
+} AgoImageFormatDescription;
+typedef struct _vx_tensor_t *vx_tensor;
+vx_image vxCreateImageFromROI(vx_image img, const vx_rectangle_t *rect);
+vx_image vxCreateImageFromChannel(vx_image img, vx_enum channel);
+vx_status vxSetImageAttribute(vx_image image, vx_enum attribute, const void *ptr, vx_size size);
+void *vxFormatImagePatchAddress2d(void *ptr, vx_uint32 x, vx_uint32 y, const vx_imagepatch_addressing_t *addr);
+vx_status vxGetContextImageFormatDescription(vx_context context, vx_df_image format, AgoImageFormatDescription *desc);
+vx_status vxAccessImagePatch(vx_image image, const vx_rectangle_t *rect, vx_uint32 plane_index,
+                             vx_imagepatch_addressing_t *addr, void **ptr, vx_enum usage);
+vx_status vxCommitImagePatch(vx_image image, const vx_rectangle_t *rect, vx_uint32 plane_index,
+                             const vx_imagepatch_addressing_t *addr, const void *ptr);
+vx_status vxAccessArrayRange(vx_array arr, vx_size start, vx_size end, vx_size *stride, void **ptr, vx_enum usage);
+vx_status vxCommitArrayRange(vx_array arr, vx_size start, vx_size end, const void *ptr);
+vx_status vxAccessDistribution(vx_distribution distribution, void **ptr, vx_enum usage);
+vx_status vxCommitDistribution(vx_distribution distribution, const void *ptr);
+vx_status vxAccessLUT(vx_lut lut, void **ptr, vx_enum usage);
+vx_status vxCommitLUT(vx_lut lut, const void *ptr);
+vx_status vxReadMatrix(vx_matrix mat, void *array);
+vx_status vxWriteMatrix(vx_matrix mat, const void *array);
+vx_status vxReadScalarValue(vx_scalar ref, void *ptr);
+vx_status vxWriteScalarValue(vx_scalar ref, const void *ptr);
+vx_status vxGetRemapPoint(vx_remap table, vx_uint32 dst_x, vx_uint32 dst_y, vx_float32 *src_x, vx_float32 *src_y);
+vx_status vxGetReferenceName(vx_reference ref, vx_char name[], vx_size size);
+vx_enum vxRegisterUserStruct(vx_context context, vx_size size);
+vx_convolution vxCreateConvolution(vx_context context, vx_size columns, vx_size rows);
+vx_status vxReleaseConvolution(vx_convolution *conv);
+vx_status vxQueryConvolution(vx_convolution conv, vx_enum attribute, void *ptr, vx_size size);
+vx_status vxSetConvolutionAttribute(vx_convolution conv, vx_enum attribute, const void *ptr, vx_size size);
+vx_status vxCopyConvolutionCoefficients(vx_convolution conv, void *user_ptr, vx_enum usage, vx_enum user_mem_type);
+vx_status vxReadConvolutionCoefficients(vx_convolution conv, vx_int16 *array);
+vx_status vxWriteConvolutionCoefficients(vx_convolution conv, const vx_int16 *array);
+/* Tensors are outside this target's vision path: creation returns NULL, the other calls
+ * VX_ERROR_NOT_SUPPORTED (the symbols exist so that applications such as runvx link). */
+vx_tensor vxCreateTensor(vx_context context, vx_size number_of_dims, const vx_size *dims, vx_enum data_type,
+                         vx_int8 fixed_point_position);
+vx_tensor vxCreateVirtualTensor(vx_graph graph, vx_size number_of_dims, const vx_size *dims, vx_enum data_type,
+                                vx_int8 fixed_point_position);
+vx_tensor vxCreateTensorFromView(vx_tensor tensor, vx_size number_of_dims, const vx_size *view_start, const vx_size *view_end);
+vx_tensor vxCreateTensorFromHandle(vx_context context, vx_size number_of_dims, const vx_size *dims, vx_enum data_type,
+                                   vx_int8 fixed_point_position, const vx_size *stride, void *ptr, vx_enum memory_type);
+vx_status vxQueryTensor(vx_tensor tensor, vx_enum attribute, void *ptr, vx_size size);
+vx_status vxReleaseTensor(vx_tensor *tensor);
+vx_status vxSwapTensorHandle(vx_tensor tensor, void *new_ptr, void **prev_ptr);
+vx_status vxCopyTensorPatch(vx_tensor tensor, vx_size number_of_dims, const vx_size *view_start, const vx_size *view_end,
+                            const vx_size *user_stride, void *user_ptr, vx_enum usage, vx_enum user_memory_type);
+vx_status vxMapTensorPatch(vx_tensor tensor, vx_size number_of_dims, const vx_size *view_start, const vx_size *view_end,
+                           vx_map_id *map_id, vx_size *stride, void **ptr, vx_enum usage, vx_enum mem_type);
+vx_status vxUnmapTensorPatch(vx_tensor tensor, const vx_map_id map_id);
 
 /* ---------------- node factories (vx_nodes.h) ---------------- */
 vx_node vxColorConvertNode(vx_graph graph, vx_image input, vx_image output);

@@ -83,9 +83,19 @@ static int channel_index(vx_enum ch)
 
 static bool fmt_is(Ref *r, vx_df_image f) { return r && r->type == VX_TYPE_IMAGE && IMG(r)->format == f && IMG(r)->num_planes; }
 
+vx_status check_node_params(Node *n);   // vx_kernels.cpp: required parameters present, types as declared
+
 vx_status validate_node(Graph *g, Node *n)
 {
     (void)g;
+    if (vx_status s = check_node_params(n)) return s;
+    for (Ref *r : n->params)
+        if (r && r->type == VX_TYPE_IMAGE && IMG(r)->roi_view) {
+            // the kernels address whole aligned rows of their planes; a window into another
+            // image's rows is for the application's copies and maps, not for graph nodes
+            log_error(n, VX_ERROR_NOT_SUPPORTED, "ERROR: vxVerifyGraph: ROI views (vxCreateImageFromROI) cannot be node parameters on this target\n");
+            return VX_ERROR_NOT_SUPPORTED;
+        }
     auto &p = n->params;
     auto img = [&](int i) { return i < (int)p.size() && p[i] && p[i]->type == VX_TYPE_IMAGE ? IMG(p[i]) : nullptr; };
     switch (n->kernel) {

@@ -75,6 +75,9 @@ struct Image : Ref {
     vx_enum import_type = VX_MEMORY_TYPE_NONE;  // HOST / HIP(device) for images from handle
     Image *parent = nullptr;          // pyramid/channel parent (shares memory)
     Image *view_of = nullptr;         // image this ROI / channel view holds an internal reference on
+    std::vector<Image *> views;       // ROI views of this image (vxCreateImageFromROI): share its storage
+    uint32_t view_x = 0, view_y = 0;  // a ROI view's offset in its parent's plane 0, in pixels
+    bool roi_view = false;
     std::vector<Image *> children;    // planes of multi-plane images as U8 images (AGO children)
     std::map<vx_map_id, MapInfo> maps;
     vx_map_id next_map = 1;
@@ -180,6 +183,14 @@ struct Kernel : Ref {
     vx_enum id = 0;
     std::string kname;
     int num_params = 0;
+    const char *sig = "";             // parameter directions and types (vx_kernels.cpp)
+};
+
+struct Convolution : Ref {
+    vx_size columns = 0, rows = 0;
+    vx_uint32 scale = 1;
+    std::vector<vx_int16> coeffs;     // rows x columns, row-major as the application writes them
+    uint64_t version = 0;
 };
 
 struct Node : Ref {
@@ -317,6 +328,7 @@ struct Graph : Ref {
 
 struct Context : Ref {
     int device = 0;
+    std::vector<vx_size> user_structs;   // vxRegisterUserStruct sizes, by enum - VX_TYPE_USER_STRUCT_START
     std::vector<Ref *> refs;          // every object created in this context
     vx_log_callback_f log_cb = nullptr;
     bool log_reentrant = false;
@@ -342,6 +354,7 @@ void destroy_ref(Ref *r);
 void graph_own(Graph *g, Ref *r);             // the graph's lowering holds r until re-lowered or released
 void graph_release_owned(Graph *g);
 vx_status image_alloc_device(Image *img);
+void image_refresh_views(Image *root);
 vx_status image_sync_to_device(Image *img, cudaStream_t s);
 vx_status image_sync_to_host(Image *img);
 vx_status array_alloc_device(Array *a);

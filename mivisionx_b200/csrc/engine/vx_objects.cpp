@@ -152,7 +152,11 @@ void destroy_ref(Ref *r)
         std::vector<Image *> children;
         children.swap(img->children);
         for (Image *ch : children) { ch->parent = nullptr; ch->ext_count = ch->int_count = 0; destroy_ref(ch); }
-        if (img->view_of) release_internal(img->view_of);
+        if (img->roi_view && img->parent) {
+            auto &v = img->parent->views;
+            v.erase(std::remove(v.begin(), v.end(), img), v.end());
+        }
+        if (img->view_of) { Image *p = img->view_of; img->view_of = nullptr; release_internal(p); }
         break;
     }
     case VX_TYPE_PYRAMID: {
@@ -222,6 +226,29 @@ Image *make_image(Context *ctx, Graph *scope, uint32_t w, uint32_t h, vx_df_imag
     return img;
 }
 
+// Plane images (AGO children) alias the parent's planes; ROI views alias a window of plane 0.
+// Called whenever the parent's storage moves (allocation, host mirror, handle swap, ageing).
+void image_refresh_views(Image *root)
+{
+    for (size_t c = 0; c < root->children.size(); c++) {
+        Plane &cp = root->children[c]->planes[0];
+        const Plane &p = root->planes[c];
+        cp.dev = p.dev; cp.dev_stride = p.dev_stride;
+        cp.host = p.host; cp.host_stride = p.host_stride;
+        cp.dev_owned = cp.host_owned = false;
+    }
+    const Plane &p = root->planes[0];
+    for (Image *v : root->views) {
+        Plane &vp = v->planes[0];
+        const size_t off_dev = (size_t)v->view_y * p.dev_stride + (size_t)v->view_x * p.bpp;
+        const size_t off_host = (size_t)v->view_y * p.host_stride + (size_t)v->view_x * p.bpp;
+        vp.bpp = p.bpp;
+        vp.dev = p.dev ? p.dev + off_dev : nullptr; vp.dev_stride = p.dev_stride;
+        vp.host = p.host ? p.host + off_host : nullptr; vp.host_stride = p.host_stride;
+        vp.dev_owned = vp.host_owned = false;
+    }
+}
+
 // every CUDA call is made on the context's device (VX_CONTEXT_ATTRIBUTE_AMD_HIP_DEVICE)
 static void use_device(Ref *r)
 {
@@ -247,11 +274,7 @@ vx_status image_alloc_device(Image *img)
         p.dev_owned = true;
         if (!p.host_stride) p.host_stride = p.dev_stride;
     }
-    // children (planes of multi-plane images) alias the parent's planes
-    for (size_t c = 0; c < img->children.size(); c++) {
-        Plane &cp = img->children[c]->planes[0];
-        cp.dev = img->planes[c].dev; cp.dev_stride = img->planes[c].dev_stride;
-    }
+    image_refresh_views(img);
     if (img->uniform || (!img->dev_valid && !img->host_valid)) {
         // uniform images and fresh images: materialise on the host and upload
         if (img->uniform) {
@@ -289,10 +312,7 @@ static vx_status ensure_host(Image *img)
         p.host = (uint8_t *)h;
         p.host_owned = true;
     }
-    for (size_t c = 0; c < root->children.size(); c++) {
-        Plane &cp = root->children[c]->planes[0];
-        cp.host = root->planes[c].host; cp.host_stride = root->planes[c].host_stride;
-    }
+    image_refresh_views(root);
     return VX_SUCCESS;
 }
 
@@ -365,6 +385,9 @@ Array *make_array(Context *ctx, Graph *scope, vx_enum item_type, vx_size capacit
     a->is_virtual = virt;
     a->item_type = item_type;
     a->item_size = type_size(item_type);
+    // user structs (vxRegisterUserStruct): enums from 0x100 in registration order
+    if (!a->item_size && ctx && item_type >= 0x100 && (size_t)(item_type - 0x100) < ctx->user_structs.size())
+        a->item_size = ctx->user_structs[(size_t)(item_type - 0x100)];
     a->capacity = capacity;
     add_ref(ctx, a);
     return a;
@@ -595,7 +618,15 @@ static vx_status release_ref(Ref *r)
     r->ext_count--;
     if (r->ext_count == 0) {
         r->released = true;
+        // a plane handed out by vxCreateImageFromChannel stays with its parent but stops
+        // holding it; the parent may then go, and takes its planes with it
+        Image *hold = nullptr;
+        if (r->type == VX_TYPE_IMAGE && !static_cast<Image *>(r)->roi_view) {
+            hold = static_cast<Image *>(r)->view_of;
+            static_cast<Image *>(r)->view_of = nullptr;
+        }
         if (r->int_count == 0) destroy_ref(r);
+        if (hold) release_internal(hold);
     }
     return VX_SUCCESS;
 }
@@ -724,6 +755,7 @@ vx_status vxSwapImageHandle(vx_image image, void *const new_ptrs[], void *prev_p
         if (prev_ptrs) prev_ptrs[i] = slot;
         if (new_ptrs) slot = (uint8_t *)new_ptrs[i];
     }
+    image_refresh_views(img);
     if (img->import_type == VX_MEMORY_TYPE_HOST) { img->host_valid = new_ptrs != nullptr; img->dev_valid = false; }
     else img->dev_valid = new_ptrs != nullptr;
     // pointers are baked into captured launches: graphs using this image re-capture
@@ -1297,8 +1329,9 @@ vx_status vxCopyMatrix(vx_matrix matrix, void *user_ptr, vx_enum usage, vx_enum 
 // ---------------------------------------------------------------- arrays
 vx_array vxCreateArray(vx_context context, vx_enum item_type, vx_size capacity)
 {
-    if (!is_valid(context, VX_TYPE_CONTEXT) || !type_size(item_type) || !capacity) return nullptr;
+    if (!is_valid(context, VX_TYPE_CONTEXT) || !capacity) return nullptr;
     Array *a = make_array(as<Context>(context), nullptr, item_type, capacity, false);
+    if (!a->item_size) { destroy_ref(a); return nullptr; }
     a->host.assign(a->capacity * a->item_size, 0);
     return (vx_array)a;
 }
@@ -1553,13 +1586,10 @@ static void swap_image_storage(Image *a, Image *b)
     std::swap(a->host_valid, b->host_valid);
     std::swap(a->dev_valid, b->dev_valid);
     std::swap(a->valid, b->valid);
-    for (Image *img : {a, b})
-        for (size_t c = 0; c < img->children.size(); c++) {
-            img->children[c]->planes[0] = img->planes[c];
-            img->children[c]->planes[0].dev_owned = img->children[c]->planes[0].host_owned = false;
-            img->children[c]->dev_valid = img->dev_valid;
-            img->children[c]->host_valid = img->host_valid;
-        }
+    for (Image *img : {a, b}) {
+        image_refresh_views(img);
+        for (Image *c : img->children) { c->dev_valid = img->dev_valid; c->host_valid = img->host_valid; }
+    }
 }
 
 static void swap_storage(Ref *a, Ref *b)

@@ -22,6 +22,8 @@ REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(REF_DIR, "libagooracle.so")
 REF_SO = os.path.join(REF_DIR, "libopenvx_ref.so")
 REF_SYMS = os.path.join(REF_DIR, "ref_symbols.txt")
+RUNVX_REF = os.path.join(REF_DIR, "runvx_ref")      # reference runvx on the reference library
+RUNVX_B200 = os.path.join(REF_DIR, "runvx_b200")    # the same runvx on this project's libopenvx.so
 REFERENCE_TREE = "/root/reference/amd_openvx/openvx"
 
 _oracle = None
@@ -35,7 +37,7 @@ def build(with_reference: bool | None = None) -> None:
     if with_reference is None:
         with_reference = os.path.isdir(REFERENCE_TREE)
     if with_reference:
-        targets.append("ref")
+        targets += ["ref", "runvx"]
     subprocess.run(["make", "-s", "-C", HERE, f"-j{min(16, os.cpu_count() or 4)}"] + targets, check=True)
 
 
