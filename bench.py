@@ -393,6 +393,84 @@ def run_reference_arm(a, wl_name):
 
 
 # ------------------------------------------------------------------------------------------
+def device_value(api, wl, B, plain, steps, warmup, ws, rank, local):
+    """Device-resident Mpixels/s of `B` frames of workload `wl` in one graph (fused+batched,
+    or the plain one-launch-per-node form), in a context of its own that is released after:
+    returns (Mpixels/s over all ranks, ms per step, algorithmic bytes per step, kernels per
+    step)."""
+    import torch
+
+    from mivisionx_b200 import vx as V
+    ctx = api.obj(api.vxCreateContext(), "context")
+    api.set_device(ctx, local)
+    try:
+        frames = wl.make_frames(frame_seed(rank), B)
+        g = wl.build(api, ctx, B, flags=V.OPT_NO_FUSION if plain else None)
+        g.run(frames)
+        alg = wl.alg_bytes(g, B)
+        kernels = sum(k for _, k in api.plan(g.graph))
+        for _ in range(warmup):
+            g.run()
+        torch.cuda.synchronize()
+        _barrier(ws)
+        ms = []
+        for _ in range(steps):
+            g.run()
+            ms.append(api.gpu_ms_last(g.graph))
+        torch.cuda.synchronize()
+        _barrier(ws)
+        ms_step = _max_over_ranks(sum(ms), ws) / steps
+        px = sum(int(f.shape[0] * f.shape[1]) for f in frames)
+        return px * ws / (ms_step / 1e3) / 1e6, ms_step, alg, kernels
+    finally:
+        api.vxReleaseContext(C.byref(C.c_void_p(ctx)))
+
+
+# Configurations of the metric besides the headline one, reported in `per_graph` of the
+# default line: each at its own batch, fused and plain, with the roofline fraction and a
+# short one-core sample of the reference CPU library.
+PER_GRAPH = ["gauss_sobel_mag_depth_thresh_1080p", "color_geometry_4k", "pyramid_lk_uneven_x64", "motion_mask_4k"]
+
+
+def per_graph_lines(a, api, ws, rank, local):
+    peak, peak_kind = _peaks()
+    out = {}
+    steps, warmup = max(3, min(a.steps, 10)), 3
+    for name in PER_GRAPH:
+        wl = WORKLOADS[name]
+        v, ms, alg, kernels = device_value(api, wl, wl.frames, False, steps, warmup, ws, rank, local)
+        vp, msp, _, kp = device_value(api, wl, wl.frames, True, steps, warmup, ws, rank, local)
+        achieved = alg / (ms / 1e3) / 1e9
+        entry = {"value": round(v, 1), "unit": "Mpixels/s", "ms_per_step": round(ms, 4), "frames_per_step_per_gpu": wl.frames,
+                 "kernels_per_step": kernels, "plain": {"value": round(vp, 1), "ms_per_step": round(msp, 4),
+                                                        "kernels_per_step": kp, "fused_over_plain": round(v / vp, 2)},
+                 "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                              "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "alg_bytes_per_step": alg},
+                 "cpu_baseline": None, "graph": wl.desc}
+        if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+            r = reference_cpu(name, 1, a.per_graph_cpu_seconds)
+            if r is not None:
+                entry["cpu_baseline"] = {"value": round(r[0], 2), "unit": "Mpixels/s", "cores": 1, "kind": "reference",
+                                         "sample": f"{r[2]} runs of the one-unit graph through the reference AGO CPU "
+                                                   f"library ({r[1]:.1f} s, 1 core)"}
+        out[name] = entry
+    # configuration 5: the differentiable F32 warp (no OpenVX graph; no plain form)
+    v, ms, launches = diffwarp_value(32, steps, warmup, ws)
+    achieved = 12.0 * 32 * 1024 * 1024 / (ms / 1e3) / 1e9
+    entry = {"value": round(v, 1), "unit": "Mpixels/s", "ms_per_step": round(ms, 4), "frames_per_step_per_gpu": 32,
+             "kernels_per_step": launches / steps, "plain": None,
+             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind},
+             "cpu_baseline": None, "graph": DIFFWARP_DESC}
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cv, dt, n = _diffwarp_cpu(a.per_graph_cpu_seconds)
+        entry["cpu_baseline"] = {"value": round(cv, 2), "unit": "Mpixels/s", "cores": 1, "kind": "port",
+                                 "sample": f"{n} x warp + loss + adjoint of one 1024x1024 image in FP64 numpy "
+                                           f"({dt:.1f} s, 1 core); the reference has no F32 warp"}
+    out[DIFFWARP] = entry
+    return out
+
+
 def run_ours(a, wl_name):
     import numpy as np
     import torch
@@ -527,6 +605,14 @@ def run_ours(a, wl_name):
     e2e = px_step * ws / (e2e_ms / 1e3) / 1e6
     e2e_copy = px_step * ws / (e2e_copy_ms / 1e3) / 1e6
 
+    # the same workload in the plain one-launch-per-node form (the metric's "batched vs plain")
+    plain = None
+    if not a.plain:
+        vp, msp, _, kp = device_value(api, wl, B, True, a.steps, a.warmup, ws, rank, local)
+        plain = {"value": round(vp, 1), "unit": "Mpixels/s", "ms_per_step": round(msp, 4), "kernels_per_step": kp,
+                 "fused_over_plain": round(value / vp, 2)}
+    per_graph = per_graph_lines(a, api, ws, rank, local) if a.per_graph else None
+
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (ms_step / 1e3) / 1e9
     traffic, traffic_note = None, None
@@ -565,6 +651,8 @@ def run_ours(a, wl_name):
             "gpu_launches": kernels_per_step * a.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "plain": plain,
+            "per_graph": per_graph,
         }))
     if ws > 1:
         import torch.distributed as dist
@@ -607,6 +695,36 @@ def _diffwarp_cpu(seconds, size=1024):
         n += 1
     dt = time.perf_counter() - t0
     return n * size * size / dt / 1e6, dt, n
+
+
+def diffwarp_value(N, steps, warmup, ws, S=1024):
+    """Device time of the fused warp + L2 + adjoint step on N images: (Mpixels/s over all
+    ranks, ms per step, launches in the timed steps)."""
+    import torch
+
+    from mivisionx_b200 import diffwarp, native
+    imgs, gt, init = _diffwarp_inputs(N, S)
+    d_img = torch.from_numpy(imgs).cuda()
+    d_gt, d_th = torch.from_numpy(gt).cuda(), torch.from_numpy(init).cuda()
+    d_tgt = diffwarp.warp_affine(d_img, d_gt)
+    gsrc = torch.zeros_like(d_img)
+    acc = torch.zeros((N, 7), dtype=torch.float64, device="cuda")
+    lib = native.agocuda()
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        diffwarp.warp_affine_l2_step(d_img, d_th, d_tgt, gsrc=gsrc, acc=acc)
+    torch.cuda.synchronize()
+    _barrier(ws)
+    n0 = lib.agocuda_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        diffwarp.warp_affine_l2_step(d_img, d_th, d_tgt, gsrc=gsrc, acc=acc)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.agocuda_launch_count() - n0
+    ms = _max_over_ranks(e0.elapsed_time(e1) / steps, ws)
+    return N * S * S * ws / (ms / 1e3) / 1e6, ms, launches
 
 
 def run_diffwarp(a):
@@ -732,6 +850,23 @@ def run_diffwarp_reference(a):
     return 0
 
 
+def spawn_ranks(n, argv):
+    """`--gpus N` without torchrun: start N local ranks of this script, one per GPU, with the
+    torchrun environment (127.0.0.1 rendezvous); rank 0 prints the line.  Returns the worst
+    exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + list(argv), env=env))
+    rcs = [p.wait() for p in procs]
+    return max(rcs, key=abs)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -744,7 +879,14 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true",
                     help="run the one-launch-per-node plan (the unfused, unbatched comparison form)")
+    ap.add_argument("--no-per-graph", dest="per_graph", action="store_false",
+                    help="leave out the other configurations (per_graph) of the default line")
+    ap.add_argument("--per-graph-cpu-seconds", type=float, default=3.0)
     a = ap.parse_args(argv)
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(a.gpus, argv if argv is not None else sys.argv[1:])
+    if a.workload != DEFAULT_WORKLOAD or a.plain:
+        a.per_graph = False
     if a.workload == DIFFWARP:
         if a.impl == "ours":
             a.warmup = max(a.warmup, 3)

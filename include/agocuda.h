@@ -362,6 +362,26 @@ int agocuda_WarpAffine_F32_L2_step_batch(void *stream, int n, int width, int hei
                                          long long tBatch, int tStride, int srcWidth, int srcHeight, const float *pSrc,
                                          long long srcBatch, int srcStride, const float *theta, float border,
                                          float *pGradSrc, double *pGradThetaLoss);
+/* WarpPerspective F32 bilinear with a constant border, the perspective counterpart of the
+ * three entry points above: theta holds 9 floats per image, the ago_perspective_matrix_t
+ * m[3][3] of the reference's U8 WarpPerspective in storage order (m00 m01 m02 / m10 m11 m12 /
+ * m20 m21 m22; ago_haf_cpu_geometric.cpp:1594-1602):  z = m02*x + m12*y + m22,
+ * xs = (m00*x + m10*y + m20) / z,  ys = (m01*x + m11*y + m21) / z; z == 0 samples the border.
+ * The adjoint adds 9 theta gradients (double) per image; the L2 step adds 9 gradients and then
+ * the loss (10 doubles per image).  No counterpart in the reference (its warps are U8 only). */
+int agocuda_WarpPerspective_F32_Bilinear_Constant_batch(void *stream, int n, int width, int height, float *pDst,
+                                                        long long dstBatch, int dstStride, int srcWidth, int srcHeight,
+                                                        const float *pSrc, long long srcBatch, int srcStride,
+                                                        const float *theta, float border);
+int agocuda_WarpPerspective_F32_Bilinear_Constant_adjoint_batch(void *stream, int n, int width, int height,
+                                                                const float *pGradOut, long long goBatch, int goStride,
+                                                                int srcWidth, int srcHeight, const float *pSrc,
+                                                                long long srcBatch, int srcStride, const float *theta,
+                                                                float border, float *pGradSrc, double *pGradTheta);
+int agocuda_WarpPerspective_F32_L2_step_batch(void *stream, int n, int width, int height, const float *pTarget,
+                                              long long tBatch, int tStride, int srcWidth, int srcHeight, const float *pSrc,
+                                              long long srcBatch, int srcStride, const float *theta, float border,
+                                              float *pGradSrc, double *pGradThetaLoss);
 int agocuda_Remap_F32_Bilinear_Constant_batch(void *stream, int n, int width, int height, float *pDst, long long dstBatch,
                                               int dstStride, int srcWidth, int srcHeight, const float *pSrc,
                                               long long srcBatch, int srcStride, const float *pField, long long fieldBatch,

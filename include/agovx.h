@@ -209,7 +209,8 @@ enum { VX_GRAPH_ATTRIBUTE_AMD_AFFINITY = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GR
        VX_GRAPH_ATTRIBUTE_AMD_EXPORT_TO_TEXT = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GRAPH) + 0x03,
        VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GRAPH) + 0x04,
        VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_LAST = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GRAPH) + 0x05,
-       VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_AVG = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GRAPH) + 0x06 };
+       VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_AVG = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GRAPH) + 0x06,
+       VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_PROFILE = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GRAPH) + 0x07 };
 enum { VX_NODE_ATTRIBUTE_AMD_AFFINITY = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_NODE) + 0x01,
        VX_NODE_ATTRIBUTE_AMD_HIP_STREAM = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_NODE) + 0x03 };
 enum { VX_IMAGE_ATTRIBUTE_AMD_HIP_BUFFER = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_IMAGE) + 0x06 };
@@ -396,6 +397,14 @@ vx_status vxSetRemapPoint(vx_remap table, vx_uint32 dst_x, vx_uint32 dst_y, vx_f
 vx_status vxCopyRemapPatch(vx_remap remap, const vx_rectangle_t *rect, vx_size user_stride_y, void *user_ptr,
                            vx_enum user_coordinate_type, vx_enum usage, vx_enum user_mem_type);
 vx_status vxQueryRemap(vx_remap table, vx_enum attribute, void *ptr, vx_size size);
+
+/* Graph time as VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_{LAST,AVG} report it, in ns (vx_ext_amd.h) */
+typedef struct {
+    vx_uint64 kernel_enqueue;
+    vx_uint64 kernel_wait;
+    vx_uint64 buffer_read;
+    vx_uint64 buffer_write;
+} AgoGraphPerfInternalInfo;
 
 /* ---------------- kernels, generic nodes, parameters (vx_api.h group_kernel / group_parameter) ---------------- */
 #define VX_MAX_KERNEL_NAME (256)

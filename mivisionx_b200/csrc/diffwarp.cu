@@ -1,11 +1,15 @@
-// diffwarp.cu -- differentiable F32 warps on sm_100a: bilinear WarpAffine and Remap with a
-// constant border, their adjoints, and a fused "warp + L2 loss + adjoint" step.
+// diffwarp.cu -- differentiable F32 warps on sm_100a: bilinear WarpAffine, WarpPerspective
+// and Remap with a constant border, their adjoints, and fused "warp + L2 loss + adjoint"
+// steps.
 //
 // The reference has no F32 warp (its warps validate U8 only, ago_kernel_api.cpp:19255); the
-// coordinate convention is that of its U8 WarpAffine (ago_haf_cpu_geometric.cpp:679-684,
-// ago_affine_matrix_t m[3][2]):  xs = m00*x + m10*y + m20,  ys = m01*x + m11*y + m21, theta
-// holding (m00, m01, m10, m11, m20, m21).  Bilinear interpolation from floor(xs), floor(ys);
-// each of the four taps outside the source reads the border value.
+// coordinate conventions are those of its U8 warps.  WarpAffine (ago_haf_cpu_geometric.cpp:
+// 679-684, ago_affine_matrix_t m[3][2]):  xs = m00*x + m10*y + m20,  ys = m01*x + m11*y + m21,
+// theta holding (m00, m01, m10, m11, m20, m21).  WarpPerspective (ago_haf_cpu_geometric.cpp:
+// 1594-1602, ago_perspective_matrix_t m[3][3]):  z = m02*x + m12*y + m22,
+// xs = (m00*x + m10*y + m20) / z,  ys = (m01*x + m11*y + m21) / z, theta holding the nine
+// entries in storage order; z == 0 samples the border.  Bilinear interpolation from
+// floor(xs), floor(ys); each of the four taps outside the source reads the border value.
 //
 // Adjoint: d/dsrc scatters gout times the tap weights (red.global.add on the source
 // gradient); d/dtheta sums gout * (dout/dxs * dxs/dtheta + dout/dys * dys/dtheta) with
@@ -35,6 +39,7 @@ __device__ __forceinline__ Taps taps(const float *src, int stride, int W, int H,
     const bool far = !(fx0 > -2.0 && fx0 < (double)W + 1.0 && fy0 > -2.0 && fy0 < (double)H + 1.0);
     t.x0 = far ? -2 : (int)fx0;
     t.y0 = far ? -2 : (int)fy0;
+    if (far) { t.fx = 0.f; t.fy = 0.f; }     // NaN / infinite positions: the border, exactly
     const int x1 = t.x0 + 1, y1 = t.y0 + 1;
     const bool cx0 = t.x0 >= 0 && t.x0 < W, cx1 = x1 >= 0 && x1 < W, cy0 = t.y0 >= 0 && t.y0 < H, cy1 = y1 >= 0 && y1 < H;
     t.k00 = cx0 && cy0; t.k01 = cx1 && cy0; t.k10 = cx0 && cy1; t.k11 = cx1 && cy1;
@@ -94,18 +99,29 @@ enum Mode { kForward = 0, kAdjoint = 1, kFusedL2 = 2 };
 
 // One thread per output pixel of image blockIdx.z.  Modes: forward (out), adjoint (gout ->
 // gsrc, gtheta), fused L2 step (target -> gsrc, gtheta and loss with gout = 2 (out - target)).
-template <int MODE>
+// NT = 6: affine; NT = 9: perspective.  Per image the adjoint adds NT theta gradients, the
+// fused step NT gradients and then the loss.
+template <int MODE, int NT>
 __global__ void __launch_bounds__(256)
-k_warp_affine_f32(int W, int H, Img32 src, Img32 out, Img32 aux, const float *theta, float border, Img32 gsrc,
-                  double *gtheta)
+k_warp_f32(int W, int H, Img32 src, Img32 out, Img32 aux, const float *theta, float border, Img32 gsrc, double *gtheta)
 {
     const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5), n = blockIdx.z;
-    const float *th = theta + 6 * n;
-    float acc[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float *th = theta + NT * n;
+    float acc[NT + 1];
+#pragma unroll
+    for (int k = 0; k <= NT; k++) acc[k] = 0.f;
     if (x < W && y < H) {
         const float fx = (float)x, fy = (float)y;
-        const double xs = (double)th[0] * x + (double)th[2] * y + (double)th[4];
-        const double ys = (double)th[1] * x + (double)th[3] * y + (double)th[5];
+        double xs, ys, iz = 1.0;
+        if (NT == 6) {
+            xs = (double)th[0] * x + (double)th[2] * y + (double)th[4];
+            ys = (double)th[1] * x + (double)th[3] * y + (double)th[5];
+        } else {
+            const double z = (double)th[2] * x + (double)th[5] * y + (double)th[8];
+            iz = z != 0.0 ? 1.0 / z : 0.0;
+            xs = z != 0.0 ? ((double)th[0] * x + (double)th[3] * y + (double)th[6]) * iz : __longlong_as_double(0x7ff8000000000000ll);
+            ys = z != 0.0 ? ((double)th[1] * x + (double)th[4] * y + (double)th[7]) * iz : xs;
+        }
         const Taps t = taps(src.p + src.batch * n, src.stride, src.W, src.H, xs, ys, border);
         if (MODE == kForward) {
             out.p[out.batch * n + (size_t)y * out.stride + x] = interp(t);
@@ -115,19 +131,29 @@ k_warp_affine_f32(int W, int H, Img32 src, Img32 out, Img32 aux, const float *th
                 g = aux.p[aux.batch * n + (size_t)y * aux.stride + x];
             } else {
                 const float r = interp(t) - aux.p[aux.batch * n + (size_t)y * aux.stride + x];
-                acc[6] = r * r;
+                acc[NT] = r * r;
                 g = 2.f * r;
             }
             scatter(gsrc.p + gsrc.batch * n, gsrc.stride, t, g);
             const float gx = g * dout_dxs(t), gy = g * dout_dys(t);
-            acc[0] = gx * fx; acc[1] = gy * fx; acc[2] = gx * fy; acc[3] = gy * fy; acc[4] = gx; acc[5] = gy;
+            if (NT == 6) {
+                acc[0] = gx * fx; acc[1] = gy * fx; acc[2] = gx * fy; acc[3] = gy * fy; acc[4] = gx; acc[5] = gy;
+            } else if (iz != 0.0 && (gx != 0.f || gy != 0.f)) {   // a sample on the border has no theta term
+                // d(xs)/d(m00, m10, m20) = (x, y, 1) / z; d(xs)/d(m02, m12, m22) = -xs (x, y, 1) / z; same for ys
+                const double gxz = gx * iz, gyz = gy * iz, q = -((double)gx * xs + (double)gy * ys) * iz;
+                acc[0] = (float)(gxz * x); acc[1] = (float)(gyz * x); acc[2] = (float)(q * x);
+                acc[3] = (float)(gxz * y); acc[4] = (float)(gyz * y); acc[5] = (float)(q * y);
+                acc[6] = (float)gxz; acc[7] = (float)gyz; acc[8] = (float)q;
+            }
         }
     }
     if (MODE == kAdjoint) {
-        const float v[6] = {acc[0], acc[1], acc[2], acc[3], acc[4], acc[5]};
-        block_add<6>(v, gtheta + 6 * n);
+        float v[NT];
+#pragma unroll
+        for (int k = 0; k < NT; k++) v[k] = acc[k];
+        block_add<NT>(v, gtheta + NT * n);
     } else if (MODE == kFusedL2) {
-        block_add<7>(acc, gtheta + 7 * n);         // six gradients, then the loss, per image
+        block_add<NT + 1>(acc, gtheta + (NT + 1) * n);
     }
 }
 
@@ -169,7 +195,7 @@ extern "C" int agocuda_WarpAffine_F32_Bilinear_Constant_batch(void *stream, int 
     if (!pDst || !pSrc || !theta || !batch_ok(n, W, H, srcW, srcH) || dstStride < W || srcStride < srcW)
         return AGOCUDA_INVALID_PARAMS;
     const dim3 grd(div_up(W, 32), div_up(H, 8), n);
-    k_warp_affine_f32<kForward><<<grd, 256, 0, as_stream(stream)>>>(
+    k_warp_f32<kForward, 6><<<grd, 256, 0, as_stream(stream)>>>(
         W, H, img32(pSrc, srcBatch, srcStride, srcW, srcH), img32(pDst, dstBatch, dstStride, W, H), Img32{}, theta, border,
         Img32{}, nullptr);
     agocuda_count_launch(1);
@@ -186,7 +212,7 @@ extern "C" int agocuda_WarpAffine_F32_Bilinear_Constant_adjoint_batch(void *stre
         srcStride < srcW)
         return AGOCUDA_INVALID_PARAMS;
     const dim3 grd(div_up(W, 32), div_up(H, 8), n);
-    k_warp_affine_f32<kAdjoint><<<grd, 256, 0, as_stream(stream)>>>(
+    k_warp_f32<kAdjoint, 6><<<grd, 256, 0, as_stream(stream)>>>(
         W, H, img32(pSrc, srcBatch, srcStride, srcW, srcH), Img32{}, img32(pGradOut, goBatch, goStride, W, H), theta, border,
         img32(pGradSrc, srcBatch, srcStride, srcW, srcH), pGradTheta);
     agocuda_count_launch(1);
@@ -202,7 +228,7 @@ extern "C" int agocuda_WarpAffine_F32_L2_step_batch(void *stream, int n, int W, 
         srcStride < srcW)
         return AGOCUDA_INVALID_PARAMS;
     const dim3 grd(div_up(W, 32), div_up(H, 8), n);
-    k_warp_affine_f32<kFusedL2><<<grd, 256, 0, as_stream(stream)>>>(
+    k_warp_f32<kFusedL2, 6><<<grd, 256, 0, as_stream(stream)>>>(
         W, H, img32(pSrc, srcBatch, srcStride, srcW, srcH), Img32{}, img32(pTarget, tBatch, tStride, W, H), theta, border,
         img32(pGradSrc, srcBatch, srcStride, srcW, srcH), pGradThetaLoss);
     agocuda_count_launch(1);
@@ -239,6 +265,55 @@ extern "C" int agocuda_Remap_F32_Bilinear_Constant_adjoint_batch(void *stream, i
         W, H, img32(pSrc, srcBatch, srcStride, srcW, srcH), Img32{}, img32(pGradOut, goBatch, goStride, W, H),
         (const float2 *)pField, fieldBatch, fieldStride, border, img32(pGradSrc, srcBatch, srcStride, srcW, srcH),
         (float2 *)pGradField);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_WarpPerspective_F32_Bilinear_Constant_batch(void *stream, int n, int W, int H, float *pDst,
+                                                                   long long dstBatch, int dstStride, int srcW, int srcH,
+                                                                   const float *pSrc, long long srcBatch, int srcStride,
+                                                                   const float *theta, float border)
+{
+    if (!pDst || !pSrc || !theta || !batch_ok(n, W, H, srcW, srcH) || dstStride < W || srcStride < srcW)
+        return AGOCUDA_INVALID_PARAMS;
+    const dim3 grd(div_up(W, 32), div_up(H, 8), n);
+    k_warp_f32<kForward, 9><<<grd, 256, 0, as_stream(stream)>>>(
+        W, H, img32(pSrc, srcBatch, srcStride, srcW, srcH), img32(pDst, dstBatch, dstStride, W, H), Img32{}, theta, border,
+        Img32{}, nullptr);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_WarpPerspective_F32_Bilinear_Constant_adjoint_batch(void *stream, int n, int W, int H,
+                                                                           const float *pGradOut, long long goBatch,
+                                                                           int goStride, int srcW, int srcH,
+                                                                           const float *pSrc, long long srcBatch,
+                                                                           int srcStride, const float *theta, float border,
+                                                                           float *pGradSrc, double *pGradTheta)
+{
+    if (!pGradOut || !pSrc || !theta || !pGradSrc || !pGradTheta || !batch_ok(n, W, H, srcW, srcH) || goStride < W ||
+        srcStride < srcW)
+        return AGOCUDA_INVALID_PARAMS;
+    const dim3 grd(div_up(W, 32), div_up(H, 8), n);
+    k_warp_f32<kAdjoint, 9><<<grd, 256, 0, as_stream(stream)>>>(
+        W, H, img32(pSrc, srcBatch, srcStride, srcW, srcH), Img32{}, img32(pGradOut, goBatch, goStride, W, H), theta, border,
+        img32(pGradSrc, srcBatch, srcStride, srcW, srcH), pGradTheta);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_WarpPerspective_F32_L2_step_batch(void *stream, int n, int W, int H, const float *pTarget,
+                                                         long long tBatch, int tStride, int srcW, int srcH, const float *pSrc,
+                                                         long long srcBatch, int srcStride, const float *theta, float border,
+                                                         float *pGradSrc, double *pGradThetaLoss)
+{
+    if (!pTarget || !pSrc || !theta || !pGradSrc || !pGradThetaLoss || !batch_ok(n, W, H, srcW, srcH) || tStride < W ||
+        srcStride < srcW)
+        return AGOCUDA_INVALID_PARAMS;
+    const dim3 grd(div_up(W, 32), div_up(H, 8), n);
+    k_warp_f32<kFusedL2, 9><<<grd, 256, 0, as_stream(stream)>>>(
+        W, H, img32(pSrc, srcBatch, srcStride, srcW, srcH), Img32{}, img32(pTarget, tBatch, tStride, W, H), theta, border,
+        img32(pGradSrc, srcBatch, srcStride, srcW, srcH), pGradThetaLoss);
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }

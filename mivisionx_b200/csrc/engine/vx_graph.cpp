@@ -589,6 +589,8 @@ vx_status graph_wait(Graph *g)
         return VX_FAILURE;
     }
     cudaEventElapsedTime(&g->gpu_ms_last, g->ev0, g->ev1);
+    g->gpu_ns_total += (double)g->gpu_ms_last * 1e6;
+    g->gpu_runs++;
     // host-imported output images the CUDA graph did not download (pageable buffers, the
     // serial or uncaptured forms): copy them back, so the application's buffers are current
     for (Ref *r : g->outputs) {
@@ -708,11 +710,32 @@ vx_status vxQueryGraph(vx_graph graph, vx_enum attribute, void *ptr, vx_size siz
         if (size != sizeof(AgoTargetAffinityInfo)) return VX_ERROR_INVALID_PARAMETERS;
         memset(ptr, 0, size); ((AgoTargetAffinityInfo *)ptr)->device_type = AGO_TARGET_AFFINITY_GPU; return VX_SUCCESS;
     case VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_LAST: case VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_AVG: {
-        // device time of the last launch (CUDA events), reported in vx_perf_t nanoseconds
-        if (size != sizeof(vx_perf_t)) return VX_ERROR_INVALID_PARAMETERS;
-        vx_perf_t p = g->perf;
-        p.tmp = (vx_uint64)(g->gpu_ms_last * 1e6);
-        *(vx_perf_t *)ptr = p; return VX_SUCCESS;
+        // vx_api.cpp:3106: AgoGraphPerfInternalInfo in nanoseconds; kernel_wait is the device
+        // time of the launch (CUDA events around the captured graph), last or averaged; the
+        // host<->device copies happen inside that launch, so the buffer times stay 0
+        if (size != sizeof(AgoGraphPerfInternalInfo) || !ptr) return VX_ERROR_INVALID_PARAMETERS;
+        AgoGraphPerfInternalInfo p{};
+        if (attribute == VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_LAST) p.kernel_wait = (vx_uint64)(g->gpu_ms_last * 1e6);
+        else if (g->gpu_runs) p.kernel_wait = (vx_uint64)(g->gpu_ns_total / (double)g->gpu_runs);
+        *(AgoGraphPerfInternalInfo *)ptr = p; return VX_SUCCESS;
+    }
+    case VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_PROFILE: {
+        // ago_interface.cpp:2740 layout: a header and one line per timed object; the nodes of
+        // this target run inside one captured CUDA graph, so the lines are the graph's host
+        // time (vxProcessGraph) and its device time (CUDA events around the launch)
+        const char *file = (const char *)ptr;
+        FILE *fp = (!file || !strcmp(file, "stdout")) ? stdout : fopen(file, "w");
+        if (!fp) return VX_FAILURE;
+        fprintf(fp, " COUNT,tmp(ms),avg(ms),min(ms),max(ms),DEV,KERNEL\n");
+        if (g->perf.num > 0)
+            fprintf(fp, "%6d,%7.3f,%7.3f,%7.3f,%7.3f,GPU,GRAPH\n", (int)g->perf.num, g->perf.tmp * 1e-6, g->perf.avg * 1e-6,
+                    g->perf.min * 1e-6, g->perf.max * 1e-6);
+        if (g->gpu_runs > 0)
+            fprintf(fp, "%6d,%7.3f,%7.3f,      -,      -,GPU,GRAPH(device)\n", (int)g->gpu_runs, (double)g->gpu_ms_last,
+                    g->gpu_ns_total * 1e-6 / (double)g->gpu_runs);
+        fflush(fp);
+        if (fp != stdout) fclose(fp);
+        return VX_SUCCESS;
     }
     case VX_GRAPH_ATTRIBUTE_AMD_EXPORT_TO_TEXT: {
         // the verified plan as text: one line per step ("kernel nodes...")

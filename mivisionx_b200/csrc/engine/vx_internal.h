@@ -314,6 +314,8 @@ struct Graph : Ref {
     vx_status last_status = VX_SUCCESS;
     vx_perf_t perf{};
     float gpu_ms_last = 0.f;
+    double gpu_ns_total = 0.0;                   // device time of all launches (the AVG attribute)
+    uint64_t gpu_runs = 0;
     uint64_t param_signature = 0;                // hash of by-value kernel parameters at capture
     // Device-side status word (mapped pinned memory): kernels set bits on bounded-wait
     // expiry or capacity overflow; checked after every launch.

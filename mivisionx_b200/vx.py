@@ -96,6 +96,11 @@ OPT_NO_GRAPH_CAPTURE = 0x00020000  # launch the steps directly instead of one CU
 
 
 # ---------------------------------------------------------------- structures
+class AgoGraphPerfInternalInfo(C.Structure):
+    _fields_ = [("kernel_enqueue", C.c_uint64), ("kernel_wait", C.c_uint64), ("buffer_read", C.c_uint64),
+                ("buffer_write", C.c_uint64)]
+
+
 class vx_imagepatch_addressing_t(C.Structure):
     _fields_ = [("dim_x", C.c_uint32), ("dim_y", C.c_uint32), ("stride_x", C.c_int32), ("stride_y", C.c_int32),
                 ("scale_x", C.c_uint32), ("scale_y", C.c_uint32), ("step_x", C.c_uint32), ("step_y", C.c_uint16),
@@ -326,9 +331,9 @@ class OpenVX:
 
     def gpu_ms_last(self, graph) -> float:
         """Device time of the graph's last launch (CUDA events on its stream), in ms."""
-        p = vx_perf_t()
+        p = AgoGraphPerfInternalInfo()
         self.ok(self.vxQueryGraph(graph, VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_LAST, C.byref(p), C.sizeof(p)), "perf")
-        return p.tmp / 1e6
+        return p.kernel_wait / 1e6
 
     # ---- images
     def query_image(self, img):

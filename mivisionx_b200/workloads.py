@@ -564,6 +564,31 @@ def cfg5_params(n: int = 32, seed: int = 5, size: int = 1024):
     return np.array(gt), np.array(init)
 
 
+def perspective_theta(affine: np.ndarray, px: float, py: float, size: int) -> np.ndarray:
+    """The nine entries (m00, m01, m02, m10, m11, m12, m20, m21, m22) of a perspective map
+    output -> source: the affine map `affine` (affine_theta order) with a projective row that
+    tilts the plane by px, py (z = 1 + (px (x - c) + py (y - c)) / size about the centre c), so
+    z stays near 1 over the image."""
+    a, d, b, e, c0, f0 = (float(v) for v in affine)
+    c = (size - 1) / 2.0
+    g, h = px / size, py / size
+    i = 1.0 - g * c - h * c
+    # xs = (a x + b y + c0) / z keeps the affine map at the centre, where z = 1
+    return np.array([a, d, g, b, e, h, c0, f0, i], np.float64)
+
+
+def cfg5_perspective_params(n: int = 32, seed: int = 6, size: int = 1024):
+    """(ground truth, initial estimate) perspective theta per image: the affine draws of
+    cfg5_params plus a tilt U(+-0.05) in each direction; the estimate perturbs the tilt by
+    U(+-0.01)."""
+    gt_a, init_a = cfg5_params(n, seed, size)
+    u = uniform01(seed, 4 * n, stream=45).reshape(n, 4) * 2.0 - 1.0
+    gt = [perspective_theta(gt_a[i], 0.05 * u[i, 0], 0.05 * u[i, 1], size) for i in range(n)]
+    init = [perspective_theta(init_a[i], 0.05 * u[i, 0] + 0.01 * u[i, 2], 0.05 * u[i, 1] + 0.01 * u[i, 3], size)
+            for i in range(n)]
+    return np.array(gt), np.array(init)
+
+
 def cfg5_field(seed: int = 5, size: int = 1024, amplitude: float = 4.0) -> np.ndarray:
     """(size, size, 2) float32 displacement field, smooth, within +-amplitude px."""
     yy, xx = np.meshgrid(np.arange(size, dtype=np.float64), np.arange(size, dtype=np.float64), indexing="ij")

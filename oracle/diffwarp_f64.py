@@ -9,7 +9,9 @@ these follow the coordinate convention of its U8 WarpAffine (ago_haf_cpu_geometr
 
 with bilinear interpolation and a constant border: each of the four taps outside the source
 reads the border value.  theta is the 6 matrix entries in storage order
-(m00, m01, m10, m11, m20, m21).  The remap variant samples at (x + dx[y, x], y + dy[y, x]).
+(m00, m01, m10, m11, m20, m21).  The perspective variant follows the reference's U8
+WarpPerspective (ago_haf_cpu_geometric.cpp:1594-1602) with its 9 entries in storage order.
+The remap variant samples at (x + dx[y, x], y + dy[y, x]).
 Loss: sum over pixels of (out - target)^2.
 
 `*_frozen` evaluate the same interpolation with every pixel's integer cell fixed to the cell
@@ -70,6 +72,41 @@ def warp_affine(src, theta, border=0.0, cells=None):
 def affine_cells(theta, H, W):
     xs, ys, _, _ = affine_coords(theta, H, W)
     return _cells(xs, ys)
+
+
+def perspective_coords(theta, H, W):
+    """Source positions of the perspective warp (ago_haf_cpu_geometric.cpp:1594-1602,
+    ago_perspective_matrix_t m[3][3] in storage order): z = m02 x + m12 y + m22,
+    xs = (m00 x + m10 y + m20) / z, ys = (m01 x + m11 y + m21) / z."""
+    yy, xx = np.meshgrid(np.arange(H, dtype=np.float64), np.arange(W, dtype=np.float64), indexing="ij")
+    a, d, g, b, e, h, c, f, i = (float(t) for t in theta)
+    z = g * xx + h * yy + i
+    return (a * xx + b * yy + c) / z, (d * xx + e * yy + f) / z, z, xx, yy
+
+
+def warp_perspective(src, theta, border=0.0, cells=None):
+    H, W = src.shape
+    xs, ys, _, _, _ = perspective_coords(theta, H, W)
+    return sample(src, xs, ys, border, cells)
+
+
+def perspective_cells(theta, H, W):
+    xs, ys, _, _, _ = perspective_coords(theta, H, W)
+    return _cells(xs, ys)
+
+
+def warp_perspective_adjoint(src, theta, gout, border=0.0):
+    """(dL/dsrc, dL/dtheta) for L = sum(gout * warp_perspective(src, theta)); theta order as
+    perspective_coords: d xs / d(m00, m10, m20) = (x, y, 1) / z, d xs / d(m02, m12, m22) =
+    -xs (x, y, 1) / z, and the same for ys with (m01, m11, m21)."""
+    H, W = src.shape
+    xs, ys, z, xx, yy = perspective_coords(theta, H, W)
+    gsrc, gxs, gys = _sample_adjoint(src, xs, ys, gout, border)
+    q = -(gxs * xs + gys * ys) / z
+    gx, gy = gxs / z, gys / z
+    gtheta = np.array([(gx * xx).sum(), (gy * xx).sum(), (q * xx).sum(), (gx * yy).sum(), (gy * yy).sum(),
+                       (q * yy).sum(), gx.sum(), gy.sum(), q.sum()])
+    return gsrc, gtheta
 
 
 def remap(src, field, border=0.0, cells=None):

@@ -15,7 +15,8 @@ AGOCUDA_H = os.path.join(ROOT, "include", "agocuda.h")
 REF_INC = "/root/reference/amd_openvx/openvx/include"
 
 STRUCTS = ["vx_imagepatch_addressing_t", "vx_perf_t", "vx_keypoint_t", "vx_rectangle_t", "vx_coordinates2df_t",
-           "vx_pixel_value_t", "vx_border_t", "AgoTargetAffinityInfo"]
+           "vx_pixel_value_t", "vx_border_t", "AgoTargetAffinityInfo", "AgoGraphPerfInternalInfo",
+           "AgoImageFormatDescription"]
 
 
 def _enum_names():

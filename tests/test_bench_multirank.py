@@ -59,3 +59,21 @@ def test_reference_arm_runs_on_rank0_only(monkeypatch):
     monkeypatch.setattr(bench, "reference_cpu", lambda *a, **k: called.append(a))
     assert bench.run_reference_arm(None, bench.DEFAULT_WORKLOAD) == 0   # returns before reading its arguments
     assert not called
+
+
+def test_gpus_flag_spawns_ranks():
+    """`bench.py --gpus 2` outside torchrun starts two local ranks itself (torchrun's
+    environment, 127.0.0.1 rendezvous); with the reference arm rank 0 alone prints its line
+    and both exit 0."""
+    import json
+    import subprocess
+    import oracle
+    if oracle.ref_lib() is None:
+        pytest.skip("reference library not built")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--impl", "reference",
+                        "--steps", "1", "--warmup", "0", "--workload", "gauss_sobel_mag_depth_thresh_1080p"],
+                       capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    assert lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2 and lines[0]["value"] > 0
