@@ -306,6 +306,23 @@ int agocuda_fused_GaussSobelMagDepthThresh(void *stream, const agocuda_frame *fr
                                            uint32_t maxWidth, uint32_t maxHeight,
                                            int32_t shift, int32_t threshold);
 
+/* The same chain as a persistent kernel: blocksPerSM x (number of SMs) resident blocks of
+ * warpsPerBlock warps take tiles -- 256 columns x warpsPerBlock * rowsPerThread rows of one
+ * frame -- from one queue over every frame of the batch, whatever their sizes, so uneven
+ * batches leave no idle tail per frame.  tilePrefix (device) holds numFrames + 1 entries:
+ * frame i's tiles are [tilePrefix[i], tilePrefix[i+1]), each frame's count given by
+ * agocuda_fused_GaussSobelMagDepthThresh_tiles.  queue (device, 8-byte aligned) is two zeroed
+ * words owned by the launch site; the launch leaves them zero again.  rowsPerThread in
+ * {6, 12, 18, 24}, warpsPerBlock in {2, 4, 8} (tiles returns 0 for other shapes); the
+ * autotuner (mivisionx_b200/autotune.py) picks them per frame size.  No counterpart in the
+ * reference (its HIP target launches one kernel per node and image). */
+uint32_t agocuda_fused_GaussSobelMagDepthThresh_tiles(uint32_t width, uint32_t height, uint32_t rowsPerThread,
+                                                     uint32_t warpsPerBlock);
+int agocuda_fused_GaussSobelMagDepthThresh_persistent(void *stream, const agocuda_frame *frames, uint32_t numFrames,
+                                                      const uint32_t *tilePrefix, uint32_t *queue, uint32_t rowsPerThread,
+                                                      uint32_t warpsPerBlock, uint32_t blocksPerSM, int32_t shift,
+                                                      int32_t threshold);
+
 /* vxCannyEdgeDetectorNode (gradient 3, L1 norm) as one front-end kernel (gradient,
  * suppression, thresholds and label initialisation from one read of the image) plus the
  * union-find hysteresis; the 0/255 edge map is bit-identical to the unfused graph inside
@@ -415,6 +432,15 @@ typedef struct agocuda_half_job {
 uint32_t agocuda_ScaleGaussianHalf_tiles(uint32_t dstWidth, uint32_t dstHeight);
 int agocuda_fused_ScaleGaussianHalf_batch(void *stream, const agocuda_half_job *jobs, uint32_t numJobs,
                                           uint32_t totalTiles);
+/* Persistent form of the batch: blocksPerSM x (number of SMs) resident blocks of `threads`
+ * threads take tiles (8 * threads columns x rows rows of one level) from one queue over the
+ * jobs; job j's tileBegin counts tiles of this shape (agocuda_ScaleGaussianHalf_tiles_shape).
+ * threads in {32, 64, 128}, rows in {2, 4, 8}.  queue: two zeroed device words (8-byte
+ * aligned) owned by the launch site, left zero again.  No counterpart in the reference. */
+uint32_t agocuda_ScaleGaussianHalf_tiles_shape(uint32_t dstWidth, uint32_t dstHeight, uint32_t threads, uint32_t rows);
+int agocuda_fused_ScaleGaussianHalf_persistent(void *stream, const agocuda_half_job *jobs, uint32_t numJobs,
+                                               uint32_t totalTiles, uint32_t *queue, uint32_t threads, uint32_t rows,
+                                               uint32_t blocksPerSM);
 
 /* ---------------------------------------------------------------- pyramidal LK */
 #define AGOCUDA_LK_MAX_LEVELS 12

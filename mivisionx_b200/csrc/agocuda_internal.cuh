@@ -20,6 +20,15 @@ static inline cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
 
 static inline unsigned div_up(unsigned a, unsigned b) { return (a + b - 1) / b; }
 
+// Multiprocessors of the current device (persistent kernels size their grid by it).
+static inline int agocuda_sm_count()
+{
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 148;
+    return n > 0 ? n : 148;
+}
+
 // The reference HAF kernels split each row into a scalar prefix (bytes up to the next
 // 16-byte boundary of the destination row pointer, used as a pixel count), a 16-wide SIMD
 // body and a scalar tail of (width - prefix) & 15 pixels, and some of them round

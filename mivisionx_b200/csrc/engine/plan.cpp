@@ -24,6 +24,8 @@ bool lnode_is_output(const LNode &ln, size_t i);
 
 static cudaStream_t S(cudaStream_t s) { return s; }
 
+std::vector<uint32_t> tune_lookup(const char *kernel, uint32_t w, uint32_t h, const std::vector<uint32_t> &dflt);
+
 static uint8_t *dptr(Ref *r) { return IMG(r)->planes[0].dev; }
 static uint32_t dstride(Ref *r) { return IMG(r)->planes[0].dev_stride; }
 static uint32_t W(Ref *r) { return IMG(r)->width; }
@@ -181,8 +183,26 @@ static vx_status lk_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step
 // ScaleGaussianHalf levels of many images in one launch (one job per lowered node)
 static vx_status half_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step &st)
 {
-    // launches over groups of images (tile numbering restarts in every group)
-    const size_t kGroupJobs = 2 * kGroupFrames;
+    // launch shape from the autotuner's table (largest output of the batch): threads per
+    // block, rows per thread, resident blocks per SM, persistent queue or one block per tile
+    uint32_t bw = 0, bh = 0;
+    bool streamed = false;
+    for (LNode *n : nodes) {
+        const Image *d = IMG(n->p[0]), *s0 = IMG(n->p[1]);
+        if ((uint64_t)d->width * d->height > (uint64_t)bw * bh) { bw = d->width; bh = d->height; }
+        const Image *root = s0->parent ? s0->parent : s0;
+        if (root->import_type == VX_MEMORY_TYPE_HOST) streamed = true;
+    }
+    std::vector<uint32_t> cfg = tune_lookup("ScaleGaussianHalf_U8_U8_5x5", bw, bh, {32, 8, 1, 0});
+    if (cfg[3] && !agocuda_ScaleGaussianHalf_tiles_shape(bw, bh, cfg[0], cfg[1])) cfg = {32, 8, 1, 0};
+    const bool persistent = cfg[3] != 0;
+    auto tiles_of = [&](const Image *d) {
+        return persistent ? agocuda_ScaleGaussianHalf_tiles_shape(d->width, d->height, cfg[0], cfg[1])
+                          : agocuda_ScaleGaussianHalf_tiles(d->width, d->height);
+    };
+    // launches over groups of images (tile numbering restarts in every group); images uploaded
+    // from application buffers go in groups so the first ones compute while the rest arrive
+    const size_t kGroupJobs = (streamed || !persistent) ? 2 * kGroupFrames : nodes.size();
     std::vector<agocuda_half_job> jobs;
     std::vector<uint32_t> group_tiles;
     uint32_t tiles = 0;
@@ -191,7 +211,7 @@ static vx_status half_batch_step(Graph *g, const std::vector<LNode *> &nodes, St
         const Image *d = IMG(nodes[i]->p[0]), *s = IMG(nodes[i]->p[1]);
         agocuda_half_job j{s->planes[0].dev, d->planes[0].dev, s->width, s->height, s->planes[0].dev_stride,
                            d->width, d->height, d->planes[0].dev_stride, tiles, 0};
-        tiles += agocuda_ScaleGaussianHalf_tiles(d->width, d->height);
+        tiles += tiles_of(d);
         jobs.push_back(j);
     }
     group_tiles.push_back(tiles);
@@ -200,11 +220,24 @@ static vx_status half_batch_step(Graph *g, const std::vector<LNode *> &nodes, St
     if (cudaMemcpy(dev, jobs.data(), jobs.size() * sizeof(agocuda_half_job), cudaMemcpyHostToDevice) != cudaSuccess)
         return VX_FAILURE;
     std::vector<std::function<int(cudaStream_t)>> fns;
+    uint32_t *queues = nullptr;
+    if (persistent) {
+        queues = (uint32_t *)scratch(g, 2 * sizeof(uint32_t) * group_tiles.size());
+        if (!queues) return VX_ERROR_NO_MEMORY;
+    }
+    const uint32_t threads = cfg[0], rows = cfg[1], bps = cfg[2];
     for (size_t k0 = 0, gi = 0; k0 < jobs.size(); k0 += kGroupJobs, gi++) {
         const size_t k1 = std::min(jobs.size(), k0 + kGroupJobs);
         const agocuda_half_job *d0 = dev + k0;
         const uint32_t n = (uint32_t)(k1 - k0), t = group_tiles[gi];
-        fns.push_back([=](cudaStream_t q) { return agocuda_fused_ScaleGaussianHalf_batch(S(q), d0, n, t); });
+        if (persistent) {
+            uint32_t *queue = queues + 2 * gi;
+            fns.push_back([=](cudaStream_t q) {
+                return agocuda_fused_ScaleGaussianHalf_persistent(S(q), d0, n, t, queue, threads, rows, bps);
+            });
+        } else {
+            fns.push_back([=](cudaStream_t q) { return agocuda_fused_ScaleGaussianHalf_batch(S(q), d0, n, t); });
+        }
         st.parts.push_back(Part{fns.back(), std::vector<LNode *>(nodes.begin() + k0, nodes.begin() + k1)});
     }
     st.num_kernels = (int)fns.size();
@@ -976,16 +1009,49 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
         if (!dev) return VX_ERROR_NO_MEMORY;
         cudaMemcpy(dev, fr.data(), fr.size() * sizeof(agocuda_frame), cudaMemcpyHostToDevice);
         const int32_t shift = (int32_t)c0.key[0], thr = (int32_t)c0.key[1];
+        // launch shape from the autotuner's table (largest frame of the batch): rows per
+        // thread, warps per block, resident blocks per SM, persistent tile queue or grid
+        uint32_t bw = 0, bh = 0;
+        for (const agocuda_frame &f : fr)
+            if ((uint64_t)f.width * f.height > (uint64_t)bw * bh) { bw = f.width; bh = f.height; }
+        std::vector<uint32_t> cfg = tune_lookup("fused_GaussSobelMagDepthThresh", bw, bh, {18, 4, 6, 1});
+        if (!agocuda_fused_GaussSobelMagDepthThresh_tiles(bw, bh, cfg[0], cfg[1])) cfg = {18, 4, 6, 1};
+        // frames uploaded from application buffers inside the CUDA graph go in groups, so the
+        // first group computes while later frames are on the bus; resident frames share one queue
+        bool streamed = false;
+        for (Chain &c : chains) {
+            Image *s0 = IMG(c.src), *root = s0->parent ? s0->parent : s0;
+            if (root->import_type == VX_MEMORY_TYPE_HOST) streamed = true;
+        }
+        const size_t group = streamed ? kGroupFrames : fr.size();
         std::vector<std::function<int(cudaStream_t)>> fns;
-        for (size_t k0 = 0; k0 < fr.size(); k0 += kGroupFrames) {
-            const size_t k1 = std::min(fr.size(), k0 + kGroupFrames);
+        for (size_t k0 = 0; k0 < fr.size(); k0 += group) {
+            const size_t k1 = std::min(fr.size(), k0 + group);
             uint32_t gw = 0, gh = 0;
             for (size_t k = k0; k < k1; k++) { gw = std::max(gw, fr[k].width); gh = std::max(gh, fr[k].height); }
             const agocuda_frame *d0 = dev + k0;
             const uint32_t n = (uint32_t)(k1 - k0);
-            fns.push_back([=](cudaStream_t q) {
-                return agocuda_fused_GaussSobelMagDepthThresh(S(q), d0, n, gw, gh, shift, thr);
-            });
+            if (cfg[3]) {
+                // tile prefix of the group's frames, then the queue words
+                std::vector<uint32_t> pre(n + 1 + 2, 0);
+                for (uint32_t k = 0; k < n; k++)
+                    pre[k + 1] = pre[k] + agocuda_fused_GaussSobelMagDepthThresh_tiles(fr[k0 + k].width, fr[k0 + k].height,
+                                                                                       cfg[0], cfg[1]);
+                if (pre.size() % 2) pre.push_back(0);
+                uint32_t *dpre = (uint32_t *)scratch(g, pre.size() * sizeof(uint32_t));
+                if (!dpre) return VX_ERROR_NO_MEMORY;
+                cudaMemcpy(dpre, pre.data(), pre.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+                uint32_t *queue = dpre + ((n + 1 + 1) & ~1u);        // 8-byte aligned, zero
+                const uint32_t rows = cfg[0], warps = cfg[1], bps = cfg[2];
+                fns.push_back([=](cudaStream_t q) {
+                    return agocuda_fused_GaussSobelMagDepthThresh_persistent(S(q), d0, n, dpre, queue, rows, warps, bps,
+                                                                             shift, thr);
+                });
+            } else {
+                fns.push_back([=](cudaStream_t q) {
+                    return agocuda_fused_GaussSobelMagDepthThresh(S(q), d0, n, gw, gh, shift, thr);
+                });
+            }
             Part pt{fns.back(), {}};
             for (size_t k = k0; k < k1; k++) for (LNode *nd : chains[k].nodes) pt.nodes.push_back(nd);
             st.parts.push_back(std::move(pt));

@@ -180,10 +180,10 @@ vx_status vxAccessImagePatch(vx_image image, const vx_rectangle_t *rect, vx_uint
         if (!addr->stride_x) {        // the caller's buffer in the image's own packing
             const Plane &p = img->planes[plane_index];
             const uint32_t sx = img->width / p.width, sy = img->height / p.height;
-            addr->dim_x = (rect->end_x - rect->start_x + sx - 1) / sx;
-            addr->dim_y = (rect->end_y - rect->start_y + sy - 1) / sy;
+            addr->dim_x = rect->end_x - rect->start_x;     // image pixels; the plane holds dim / scale
+            addr->dim_y = rect->end_y - rect->start_y;
             addr->stride_x = (vx_int32)p.bpp;
-            addr->stride_y = (vx_int32)(addr->dim_x * p.bpp);
+            addr->stride_y = (vx_int32)(((addr->dim_x + sx - 1) / sx) * p.bpp);
             addr->scale_x = VX_SCALE_UNITY / sx; addr->scale_y = VX_SCALE_UNITY / sy;
             addr->step_x = addr->step_y = 1;
         }

@@ -878,7 +878,9 @@ vx_status vxMapImagePatch(vx_image image, const vx_rectangle_t *rect, vx_uint32 
     Plane &p = img->planes[plane_index];
     uint8_t *base = p.host + (size_t)y0 * p.host_stride + (size_t)x0 * p.bpp;
     memset(addr, 0, sizeof(*addr));
-    addr->dim_x = x1 - x0; addr->dim_y = y1 - y0;
+    // dim_x / dim_y count the patch in image (plane 0) pixels; scale_x / scale_y shrink them to
+    // the plane's elements, as vx_api.cpp:2159-2161 reports a subsampled plane
+    addr->dim_x = rect->end_x - rect->start_x; addr->dim_y = rect->end_y - rect->start_y;
     addr->stride_x = (vx_int32)p.bpp; addr->stride_y = (vx_int32)p.host_stride;
     addr->scale_x = VX_SCALE_UNITY * p.width / img->width; addr->scale_y = VX_SCALE_UNITY * p.height / img->height;
     addr->step_x = 1; addr->step_y = 1;

@@ -242,15 +242,13 @@ __device__ __forceinline__ uint32_t nonneg_bytes(float a, float b, float c, floa
 __device__ __forceinline__ float c1_lo(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8404992.0f; }
 __device__ __forceinline__ float c1_hi(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8404992.0f; }
 
-__global__ void __launch_bounds__(kC1BX * kC1BY)
-k_fused_gauss_sobelmag_thresh(const agocuda_frame *frames, float tRound, float tTrunc)
+// The rows [y0, y0 + ROWS) of one thread's 8 columns at x (clipped to [2, H-2)).
+template <int ROWS>
+__device__ __forceinline__ void c1_rows(const agocuda_frame &f, int x, int y0, float tRound, float tTrunc)
 {
-    const agocuda_frame f = frames[blockIdx.z];
     const int W = (int)f.width, H = (int)f.height;
-    const int x = (blockIdx.x * kC1BX + threadIdx.x) * 8;
-    const int y0 = 2 + (blockIdx.y * kC1BY + threadIdx.y) * kC1Rows;
     if (x >= W || y0 >= H - 2) return;
-    const int y1 = min(y0 + kC1Rows, H - 2);
+    const int y1 = min(y0 + ROWS, H - 2);
     const int ss = (int)f.srcStride;
     const uint8_t *src = f.src;
     float T[8];                                    // -256 T per column (trunc / round span)
@@ -320,6 +318,70 @@ k_fused_gauss_sobelmag_thresh(const agocuda_frame *frames, float tRound, float t
         if (y + 2 >= y1) break;
         step(y + 2, h[2], h[0], h[1], g[2], g[0], g[1], hp[2], hp[0], hp[1]);
     }
+}
+
+__global__ void __launch_bounds__(kC1BX * kC1BY)
+k_fused_gauss_sobelmag_thresh(const agocuda_frame *frames, float tRound, float tTrunc)
+{
+    const agocuda_frame f = frames[blockIdx.z];
+    const int x = (blockIdx.x * kC1BX + threadIdx.x) * 8;
+    const int y0 = 2 + (blockIdx.y * kC1BY + threadIdx.y) * kC1Rows;
+    c1_rows<kC1Rows>(f, x, y0, tRound, tTrunc);
+}
+
+// Persistent form: gridDim.x resident blocks take tiles (256 columns x BY * ROWS rows of one
+// frame) from one queue spanning every frame of the batch, whatever their sizes.  tilePrefix
+// holds each frame's first tile (numFrames + 1 entries).  queue[0] is the next tile,
+// queue[1] counts finished blocks; the last block to finish puts both back to 0, so the
+// launch leaves the queue ready for the next one (a launch site owns its queue words).
+__device__ __forceinline__ uint32_t frame_of_tile(const uint32_t *prefix, uint32_t n, uint32_t t)
+{
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t queue_next(uint32_t *queue)
+{
+    __shared__ uint32_t next;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) next = atomicAdd(queue, 1u);
+    __syncthreads();
+    return next;
+}
+
+__device__ __forceinline__ void queue_done(uint32_t *queue)
+{
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 1, 1u) == gridDim.x - 1) {   // every block has taken its last tile
+            atomicExch(queue, 0u);
+            atomicExch(queue + 1, 0u);
+        }
+    }
+}
+
+template <int ROWS, int BY>
+__global__ void __launch_bounds__(kC1BX * BY)
+k_fused_c1_persistent(const agocuda_frame *frames, const uint32_t *tilePrefix, uint32_t numFrames, uint32_t *queue,
+                      float tRound, float tTrunc)
+{
+    const uint32_t total = __ldg(tilePrefix + numFrames);
+    for (;;) {
+        const uint32_t t = queue_next(queue);
+        if (t >= total) break;
+        const uint32_t fi = frame_of_tile(tilePrefix, numFrames, t);
+        const agocuda_frame f = frames[fi];
+        const uint32_t local = t - __ldg(tilePrefix + fi);
+        const uint32_t tilesX = (f.width + kC1BX * 8 - 1) / (kC1BX * 8);
+        const int x = (int)((local % tilesX) * kC1BX + threadIdx.x) * 8;
+        const int y0 = 2 + (int)((local / tilesX) * BY + threadIdx.y) * ROWS;
+        c1_rows<ROWS>(f, x, y0, tRound, tTrunc);
+    }
+    queue_done(queue);
 }
 
 unsigned long long g_launches = 0;
@@ -419,4 +481,57 @@ extern "C" int agocuda_fused_GaussSobelMagDepthThresh(void *stream, const agocud
     k_fused_gauss_sobelmag_thresh<<<grd, dim3(kC1BX, kC1BY), 0, as_stream(stream)>>>(frames, (float)tRound, (float)tTrunc);
     agocuda_count_launch(1);
     return agocuda_launch_status();
+}
+
+// ---- persistent form and its tuning space
+static bool c1_shape_ok(uint32_t rows, uint32_t warps)
+{
+    return (rows == 6 || rows == 12 || rows == 18 || rows == 24) && (warps == 2 || warps == 4 || warps == 8);
+}
+
+extern "C" uint32_t agocuda_fused_GaussSobelMagDepthThresh_tiles(uint32_t W, uint32_t H, uint32_t rowsPerThread,
+                                                                uint32_t warpsPerBlock)
+{
+    if (!c1_shape_ok(rowsPerThread, warpsPerBlock) || W < 5 || H < 5) return 0;
+    return div_up(W, kC1BX * 8) * div_up(H - 4, warpsPerBlock * rowsPerThread);
+}
+
+template <int ROWS, int BY>
+static cudaError_t c1_launch(cudaStream_t s, unsigned blocks, const agocuda_frame *frames, const uint32_t *prefix,
+                             uint32_t n, uint32_t *queue, float tR, float tT)
+{
+    k_fused_c1_persistent<ROWS, BY><<<blocks, dim3(kC1BX, BY), 0, s>>>(frames, prefix, n, queue, tR, tT);
+    return cudaPeekAtLastError();
+}
+
+extern "C" int agocuda_fused_GaussSobelMagDepthThresh_persistent(void *stream, const agocuda_frame *frames,
+                                                                 uint32_t numFrames, const uint32_t *tilePrefix,
+                                                                 uint32_t *queue, uint32_t rowsPerThread,
+                                                                 uint32_t warpsPerBlock, uint32_t blocksPerSM,
+                                                                 int32_t shift, int32_t threshold)
+{
+    if (!frames || !tilePrefix || !queue || !numFrames || !c1_shape_ok(rowsPerThread, warpsPerBlock) || !blocksPerSM ||
+        blocksPerSM > 32 || shift < 0 || shift > 15 || ((uintptr_t)queue & 7))
+        return AGOCUDA_INVALID_PARAMS;
+    const int t = (int)(uint8_t)threshold;
+    const double kNever = -256.0 * 4194304.0;
+    double tRound = kNever, tTrunc = kNever;
+    if (t < 255) {
+        long long M = (long long)(t + 1) << shift;
+        if (M <= 2048) {
+            tRound = -256.0 * (double)(M * M - M + 1);
+            tTrunc = -256.0 * (double)(M * M);
+        }
+    }
+    const unsigned blocks = (unsigned)agocuda_sm_count() * blocksPerSM;
+    cudaStream_t s = as_stream(stream);
+    const float tR = (float)tRound, tT = (float)tTrunc;
+    cudaError_t e = cudaErrorInvalidValue;
+#define C1_CASE(R, B) \
+    if (rowsPerThread == R && warpsPerBlock == B) e = c1_launch<R, B>(s, blocks, frames, tilePrefix, numFrames, queue, tR, tT);
+    C1_CASE(6, 2) C1_CASE(6, 4) C1_CASE(6, 8) C1_CASE(12, 2) C1_CASE(12, 4) C1_CASE(12, 8)
+    C1_CASE(18, 2) C1_CASE(18, 4) C1_CASE(18, 8) C1_CASE(24, 2) C1_CASE(24, 4) C1_CASE(24, 8)
+#undef C1_CASE
+    agocuda_count_launch(1);
+    return e == cudaSuccess ? agocuda_launch_status() : (int)e;
 }

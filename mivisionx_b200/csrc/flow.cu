@@ -119,14 +119,14 @@ __device__ __forceinline__ void half_hsum(const uint32_t w[6], uint32_t h[4])
     }
 }
 
-template <int CO>
+template <int CO, int ROWS = kHalfRows>
 __device__ __forceinline__ void half_tile(const agocuda_half_job &J, int ox, int oy0)
 {
     const int oW = (int)J.dstW, oH = (int)J.dstH;
     const int ro = (J.srcH & 1) ? 0 : 1;              // centre row parity (sampleFirstRow = H odd)
     const int x0 = 2 * ox - 4;
     const bool edge = (ox == 0) || (x0 + 24 > (int)J.srcW);
-    const int yEnd = min(oy0 + kHalfRows, oH);
+    const int yEnd = min(oy0 + ROWS, oH);
     uint32_t h[5][4];
     int have = 0;                                    // rows of h[] valid for the current output row
     for (int oy = oy0; oy < yEnd; oy++) {
@@ -188,6 +188,44 @@ __global__ void __launch_bounds__(kHalfThreads) k_gauss_half(const agocuda_half_
     if (ox >= (int)J.dstW) return;
     if (J.srcW & 1) half_tile<0>(J, ox, oy0);
     else half_tile<1>(J, ox, oy0);
+}
+
+// Persistent form with a tunable tile: THREADS threads x 8 columns wide, ROWS rows high.
+// Blocks take tiles from one queue over the jobs' tiles (job j's tiles start at
+// jobs[j].tileBegin for this tile shape); queue words as in the config-1 chain.
+template <int THREADS, int ROWS>
+__global__ void __launch_bounds__(THREADS) k_gauss_half_persistent(const agocuda_half_job *jobs, uint32_t numJobs,
+                                                                    uint32_t totalTiles, uint32_t *queue)
+{
+    __shared__ uint32_t next;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) next = atomicAdd(queue, 1u);
+        __syncthreads();
+        const uint32_t t = next;
+        if (t >= totalTiles) break;
+        uint32_t lo = 0, hi = numJobs - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].tileBegin <= t) lo = mid; else hi = mid - 1;
+        }
+        const agocuda_half_job J = jobs[lo];
+        const uint32_t local = t - J.tileBegin;
+        const uint32_t tilesX = (J.dstW + 8 * THREADS - 1) / (8 * THREADS);
+        const int ox = (int)(local % tilesX) * 8 * THREADS + 8 * (int)threadIdx.x;
+        const int oy0 = (int)(local / tilesX) * ROWS;
+        if (ox < (int)J.dstW) {
+            if (J.srcW & 1) half_tile<0, ROWS>(J, ox, oy0);
+            else half_tile<1, ROWS>(J, ox, oy0);
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 1, 1u) == gridDim.x - 1) {
+            atomicExch(queue, 0u);
+            atomicExch(queue + 1, 0u);
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kHalfThreads) k_gauss_half_one(const agocuda_half_job J)
@@ -656,6 +694,42 @@ extern "C" int agocuda_fused_ScaleGaussianHalf_batch(void *stream, const agocuda
 extern "C" uint32_t agocuda_ScaleGaussianHalf_tiles(uint32_t dstWidth, uint32_t dstHeight)
 {
     return ((dstWidth + kHalfCols - 1) / kHalfCols) * ((dstHeight + kHalfRows - 1) / kHalfRows);
+}
+
+static bool half_shape_ok(uint32_t threads, uint32_t rows)
+{
+    return (threads == 32 || threads == 64 || threads == 128) && (rows == 2 || rows == 4 || rows == 8);
+}
+
+extern "C" uint32_t agocuda_ScaleGaussianHalf_tiles_shape(uint32_t dstWidth, uint32_t dstHeight, uint32_t threads,
+                                                         uint32_t rows)
+{
+    if (!half_shape_ok(threads, rows)) return 0;
+    return ((dstWidth + 8 * threads - 1) / (8 * threads)) * ((dstHeight + rows - 1) / rows);
+}
+
+template <int T, int R>
+static void half_persistent_launch(cudaStream_t s, unsigned blocks, const agocuda_half_job *jobs, uint32_t n,
+                                   uint32_t total, uint32_t *queue)
+{
+    k_gauss_half_persistent<T, R><<<blocks, T, 0, s>>>(jobs, n, total, queue);
+}
+
+extern "C" int agocuda_fused_ScaleGaussianHalf_persistent(void *stream, const agocuda_half_job *jobs, uint32_t numJobs,
+                                                          uint32_t totalTiles, uint32_t *queue, uint32_t threads,
+                                                          uint32_t rows, uint32_t blocksPerSM)
+{
+    if (!jobs || !numJobs || !totalTiles || !queue || ((uintptr_t)queue & 7) || !half_shape_ok(threads, rows) ||
+        !blocksPerSM || blocksPerSM > 32)
+        return AGOCUDA_INVALID_PARAMS;
+    const unsigned blocks = (unsigned)agocuda_sm_count() * blocksPerSM;
+    cudaStream_t s = as_stream(stream);
+#define HALF_CASE(T, R) if (threads == T && rows == R) half_persistent_launch<T, R>(s, blocks, jobs, numJobs, totalTiles, queue);
+    HALF_CASE(32, 2) HALF_CASE(32, 4) HALF_CASE(32, 8) HALF_CASE(64, 2) HALF_CASE(64, 4) HALF_CASE(64, 8)
+    HALF_CASE(128, 2) HALF_CASE(128, 4) HALF_CASE(128, 8)
+#undef HALF_CASE
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
 }
 
 extern "C" size_t agocuda_OpticalFlowPyrLK_scharr_rows_size(uint32_t width0)
