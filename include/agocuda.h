@@ -166,6 +166,38 @@ int agocuda_CannyEdgeTrace_U8_U8XY_noalloc(void *stream, uint32_t width, uint32_
                                            const uint32_t *pStack, const uint32_t *pStackCount, uint32_t stackCapacity,
                                            uint32_t *pStatus);
 
+/* Convolve (vxConvolveNode): U8 source, U8 or S16 destination, cols in {3, 5, 7, 9}, rows
+ * odd in [3, 9]; `conv` is a HOST pointer to the rows x cols coefficients in vx_convolution
+ * order (applied flipped, as OpenVX defines convolution), `shift` = log2 of the scale.
+ * Columns [simdBegin, simdEnd) take the reference SIMD body's arithmetic (sum shifted right
+ * logically, then saturated), the others its scalar loops' (the unshifted sum saturated);
+ * rows [rows/2, H - rows/2) are written.  HafCpu_Convolve_{U8,S16}_U8_{3,5,7,9}xN
+ * (ago_haf_cpu_filter.cpp:2676-3830); replaces HipExec_Convolve_{U8,S16}_U8
+ * (hipvx/hip_host_decls.h:653/658), which takes device float coefficients instead. */
+int agocuda_Convolve_U8_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                           const uint8_t *pSrc, uint32_t srcStride, const int16_t *conv, uint32_t cols, uint32_t rows,
+                           int32_t shift, int32_t simdBegin, int32_t simdEnd);
+int agocuda_Convolve_S16_U8(void *stream, uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                            const uint8_t *pSrc, uint32_t srcStride, const int16_t *conv, uint32_t cols, uint32_t rows,
+                            int32_t shift, int32_t simdBegin, int32_t simdEnd);
+
+/* Harris gradient products with 5x5 or 7x7 Sobel taps (gradientSize 5 or 7), every column,
+ * rows [gs/2, H - gs/2) (the others written 0); the taps leaving the row read the neighbouring
+ * rows' bytes as AGO lays an image out (row pitch ALIGN16(W), zero padding).  Replaces
+ * HipExec_HarrisSobel_HG3_U8_{5x5,7x7} (hipvx/hip_host_decls.h:872); HafCpu_HarrisSobel_HG3_U8_5x5 /
+ * _7x7 (ago_haf_cpu_harris.cpp:333 / :455). */
+int agocuda_HarrisSobel_HG3_U8_NxN(void *stream, uint32_t width, uint32_t height, float *pDst, uint32_t dstStride,
+                                   const uint8_t *pSrc, uint32_t srcStride, uint32_t gradientSize);
+/* Harris score over a 5x5 or 7x7 block (blockSize 5 or 7) of gradient products, in the
+ * reference's summation order, 0 within blockSize/2 of a border; with blockSize 7 the score of
+ * column x is stored at x - 1, as the reference stores it.  normFactor: (255 * 2^(gs-1) *
+ * blockSize)^4 (ago_kernel_api.cpp:17012, :17083).  Replaces HipExec_HarrisScore_HVC_HG3_{5x5,7x7}
+ * (hipvx/hip_host_decls.h:886);
+ * HafCpu_HarrisScore_HVC_HG3_5x5 / _7x7 (ago_haf_cpu_harris.cpp:661 / :731). */
+int agocuda_HarrisScore_HVC_HG3_NxN(void *stream, uint32_t width, uint32_t height, float *pDst, uint32_t dstStride,
+                                    const float *pSrc, uint32_t srcStride, float sensitivity, float strengthThreshold,
+                                    float normFactor, uint32_t blockSize);
+
 /* Harris gradient products {gx*gx, gx*gy, gy*gy} (float x3 per pixel) of rows [1, H-1);
  * rows 0 and H-1 are written 0.  Replaces HipExec_HarrisSobel_HG3_U8_3x3
  * (hipvx/hip_host_decls.h:868); HafCpu_HarrisSobel_HG3_U8_3x3 (ago_haf_cpu_harris.cpp:85). */

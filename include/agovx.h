@@ -523,6 +523,7 @@ vx_node vxIntegralImageNode(vx_graph graph, vx_image input, vx_image output);
 vx_node vxHistogramNode(vx_graph graph, vx_image input, vx_distribution distribution);
 vx_node vxChannelCombineNode(vx_graph graph, vx_image plane0, vx_image plane1, vx_image plane2, vx_image plane3,
                              vx_image output);
+vx_node vxConvolveNode(vx_graph graph, vx_image input, vx_convolution conv, vx_image output);
 
 #ifdef __cplusplus
 }

@@ -64,3 +64,18 @@ struct vx_keypoint_like {
 };
 
 __device__ __forceinline__ int byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xff; }
+
+// Byte (r, c) of a U8 image stored as AGO stores it: row pitch ALIGN16(W), rows contiguous,
+// zeros before the first and after the last row and between W and the pitch.  Reading
+// column -1 therefore gives the previous row's padding (0) or, when W % 16 == 0, its last
+// pixel; column W gives padding or the next row's first pixel.  The reference's stencils
+// make such reads at the image edges.
+__device__ __forceinline__ uint32_t ago_byte(const uint8_t *img, size_t stride, int W, int H, int r, int c)
+{
+    if (c >= 0 && c < W && r >= 0 && r < H) return img[(size_t)r * stride + c];
+    const long long S = (W + 15) & ~15;
+    const long long f = (long long)r * S + c;
+    if (f < 0 || f >= (long long)H * S) return 0;
+    const int rr = (int)(f / S), cc = (int)(f - rr * S);
+    return cc < W ? img[(size_t)rr * stride + cc] : 0;
+}

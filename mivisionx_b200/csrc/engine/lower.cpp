@@ -43,6 +43,8 @@ static const char *kLKNames[] = {
     "Lut_U8_U8", "Lut_S16_S16", "IntegralImage_U32_U8", "Histogram_DATA_U8",
     "CannySobel_U16_U8_5x5_L1NORM", "CannySobel_U16_U8_5x5_L2NORM", "CannySobel_U16_U8_7x7_L1NORM",
     "CannySobel_U16_U8_7x7_L2NORM", "CannySuppThreshold_U8XY_U16_7x7",
+    "Convolve_U8_U8", "Convolve_S16_U8",
+    "HarrisSobel_HG3_U8_5x5", "HarrisSobel_HG3_U8_7x7", "HarrisScore_HVC_HG3_5x5", "HarrisScore_HVC_HG3_7x7",
 };
 static_assert(sizeof(kLKNames) / sizeof(kLKNames[0]) == (size_t)LK::COUNT, "kernel name table");
 
@@ -165,7 +167,10 @@ vx_status validate_node(Graph *g, Node *n)
     }
     case VX_KERNEL_HARRIS_CORNERS: {
         if (!fmt_is(p[0], VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
-        if (sc_i32(p[4]) != 3 || sc_i32(p[5]) != 3) return VX_ERROR_NOT_SUPPORTED;   // 3x3 gradient + block only
+        for (int i : {4, 5}) {                             // gradient and block sizes (ago_drama_divide.cpp:1748, :1764)
+            const int32_t v = sc_i32(p[i]);
+            if (v != 3 && v != 5 && v != 7) return VX_ERROR_INVALID_VALUE;
+        }
         if (!is_valid(p[6], VX_TYPE_ARRAY)) return VX_ERROR_INVALID_PARAMETERS;
         Array *a = static_cast<Array *>(p[6]);
         if (a->item_type == VX_TYPE_INVALID && a->is_virtual) { a->item_type = VX_TYPE_KEYPOINT; a->item_size = sizeof(vx_keypoint_t); }
@@ -201,6 +206,16 @@ vx_status validate_node(Graph *g, Node *n)
     case VX_KERNEL_INTEGRAL_IMAGE:                      // ValidateArguments_Img_1OUT_1IN(U32, U8)
         if (!fmt_is(p[0], VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
         return set_meta(img(1), img(0)->width, img(0)->height, VX_DF_IMAGE_U32);
+    case VX_KERNEL_CUSTOM_CONVOLUTION: {                // agoKernel_Convolve_{U8,S16}_U8 validate (:15615)
+        if (!fmt_is(p[0], VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
+        const Convolution *cv = static_cast<Convolution *>(p[1]);
+        if (!(cv->rows & 1) || !(cv->columns & 1)) return VX_ERROR_INVALID_DIMENSION;
+        Image *o = img(2);
+        // the divide picks the U8 kernel for a U8 output and the S16 one otherwise
+        // (ago_drama_divide.cpp:892), whose meta sets S16
+        const vx_df_image f = o && o->format == VX_DF_IMAGE_U8 ? VX_DF_IMAGE_U8 : VX_DF_IMAGE_S16;
+        return set_meta(o, img(0)->width, img(0)->height, f);
+    }
     case VX_KERNEL_TABLE_LOOKUP: {                      // ovxKernel_TableLookup (ago_kernel_api.cpp)
         Image *i0 = img(0);
         if (!is_valid(p[1], VX_TYPE_LUT) || !i0 || !i0->num_planes) return VX_ERROR_INVALID_PARAMETERS;
@@ -398,8 +413,11 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
         Array *xys = virt_array(g, kItemKeypointXYS, (vx_size)i0->width * i0->height);
         xys->item_size = 8;
         Scalar *sw = virt_scalar(g, VX_TYPE_UINT32, i0->width), *sh = virt_scalar(g, VX_TYPE_UINT32, i0->height);
-        add(LK::HARRIS_SOBEL_HG3_U8_3x3, {hg3, p[0]});
-        add(LK::HARRIS_SCORE_HVC_HG3_3x3, {hvc, hg3, p[3], p[1], p[4]});
+        const int32_t gs = sc_i32(p[4]), bs = sc_i32(p[5]);
+        add(gs == 3 ? LK::HARRIS_SOBEL_HG3_U8_3x3 : gs == 5 ? LK::HARRIS_SOBEL_HG3_U8_5x5 : LK::HARRIS_SOBEL_HG3_U8_7x7,
+            {hg3, p[0]});
+        add(bs == 3 ? LK::HARRIS_SCORE_HVC_HG3_3x3 : bs == 5 ? LK::HARRIS_SCORE_HVC_HG3_5x5 : LK::HARRIS_SCORE_HVC_HG3_7x7,
+            {hvc, hg3, p[3], p[1], p[4]});
         add(LK::NON_MAX_SUPP_XY_ANY_3x3, {xys, hvc});
         add(LK::HARRIS_MERGE_SORT_AND_PICK_XY_XYS, {p[6], p.size() > 7 ? p[7] : nullptr, xys, p[2], sw, sh});
         return VX_SUCCESS;
@@ -442,6 +460,9 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
     }
     case VX_KERNEL_INTEGRAL_IMAGE: add(LK::INTEGRAL_IMAGE_U32_U8, {p[1], p[0]}); return VX_SUCCESS;     // :772
     case VX_KERNEL_HISTOGRAM: add(LK::HISTOGRAM_DATA_U8, {p[1], p[0]}); return VX_SUCCESS;             // :639
+    case VX_KERNEL_CUSTOM_CONVOLUTION:                                                                 // :877
+        add(IMG(p[2])->format == VX_DF_IMAGE_U8 ? LK::CONVOLVE_U8_U8 : LK::CONVOLVE_S16_U8, {p[2], p[0], p[1]});
+        return VX_SUCCESS;
     case VX_KERNEL_TABLE_LOOKUP:                                                                       // :618
         add(IMG(p[0])->format == VX_DF_IMAGE_U8 ? LK::LUT_U8_U8 : LK::LUT_S16_S16, {p[2], p[0], p[1]});
         return VX_SUCCESS;
@@ -786,7 +807,10 @@ vx_status propagate_valid_rects(Graph *g)
             // ago_kernel_api.cpp:16154 clamps with the input's size
             shrink_from(I(0), I(2), 1); shrink_from(I(1), I(2), 1); break;
         case LK::CANNY_SOBEL_U16_U8_5x5_L1NORM: case LK::CANNY_SOBEL_U16_U8_5x5_L2NORM:   // :17701
+        case LK::HARRIS_SOBEL_HG3_U8_5x5: case LK::HARRIS_SCORE_HVC_HG3_5x5:            // :16850, :17046
             shrink_from(I(0), I(1), 2); break;
+        case LK::HARRIS_SOBEL_HG3_U8_7x7: case LK::HARRIS_SCORE_HVC_HG3_7x7:
+            shrink_from(I(0), I(1), 3); break;
         case LK::CANNY_SOBEL_U16_U8_7x7_L1NORM: case LK::CANNY_SOBEL_U16_U8_7x7_L2NORM:
             shrink_from(I(0), I(1), 3); break;
         case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7: shrink_from(I(0), I(2), 1); break;
@@ -817,6 +841,17 @@ vx_status propagate_valid_rects(Graph *g)
         }
         case LK::BOX_U8_U8_3x3: case LK::DILATE_U8_U8_3x3: case LK::ERODE_U8_U8_3x3: case LK::MEDIAN_U8_U8_3x3:
             shrink_from(I(0), I(1), 1); break;                  // e.g. :15033 (Box)
+        case LK::CONVOLVE_U8_U8: case LK::CONVOLVE_S16_U8: {   // :15654: columns / 2 and rows / 2
+            Image *o = I(0);
+            const Image *in = I(1);
+            const Convolution *cv = static_cast<const Convolution *>(ln.p[2]);
+            const uint32_t M = (uint32_t)cv->columns >> 1, N = (uint32_t)cv->rows >> 1;
+            o->valid.start_x = std::min(in->valid.start_x + M, o->width);
+            o->valid.start_y = std::min(in->valid.start_y + N, o->height);
+            o->valid.end_x = (uint32_t)std::max((int)in->valid.end_x - (int)M, 0);
+            o->valid.end_y = (uint32_t)std::max((int)in->valid.end_y - (int)N, 0);
+            break;
+        }
         case LK::ABS_DIFF_U8_U8U8: case LK::ABS_DIFF_S16_S16S16_SAT:
         case LK::ADD_U8_U8U8_WRAP: case LK::ADD_U8_U8U8_SAT: case LK::ADD_S16_U8U8: case LK::ADD_S16_S16U8_WRAP:
         case LK::ADD_S16_S16U8_SAT: case LK::ADD_S16_S16S16_WRAP: case LK::ADD_S16_S16S16_SAT:

@@ -60,13 +60,15 @@ static const LNode *reader_of(Graph *g, Ref *d)
     return nullptr;
 }
 
-// Harris score normalisation of the AGO wrapper (ago_kernel_api.cpp:16941-16942), in float.
-static float harris_norm(int32_t gs)
+// Harris score normalisation of the AGO wrappers (ago_kernel_api.cpp:16941-16942 for 3x3
+// blocks, :17012-17013 for 5x5, :17083-17084 for 7x7), in float: ((f*f)*f)*f with
+// f = 255 * 2^(gradient_size-1) * block_size.
+static float harris_norm(int32_t gs, int32_t bs = 3)
 {
-    volatile float f = 255.0f * (float)(1 << (gs - 1)) * 3;
-    f = f * f;
-    f = f * (255.0f * (float)(1 << (gs - 1)) * 3);
-    f = f * (255.0f * (float)(1 << (gs - 1)) * 3);
+    const float f0 = 255.0f * (float)(1 << (gs - 1)) * (float)bs;
+    volatile float f = f0 * f0;
+    f = f * f0;
+    f = f * f0;
     return f;
 }
 
@@ -381,6 +383,26 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         st.launch = [=](cudaStream_t q) { return agocuda_IntegralImage_U32_U8(S(q), w, h, d, ds, s, ss, scr, sb); };
         return VX_SUCCESS;
     }
+    case LK::CONVOLVE_U8_U8: case LK::CONVOLVE_S16_U8: {
+        // coefficients and shift by value: a change re-plans (the convolution's version is
+        // part of the graph's parameter hash)
+        const Convolution *cv = static_cast<Convolution *>(p[2]);
+        const uint32_t cols = (uint32_t)cv->columns, rows = (uint32_t)cv->rows;
+        std::vector<int16_t> k = cv->coeffs;
+        int32_t shift = 0;
+        while (shift < 31 && (1u << shift) < cv->scale) shift++;
+        uint8_t *d = dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        // AGO rows are 16-byte aligned: SIMD body [0, W - W % 16), scalar tail after it
+        const int32_t sb = 0, se = (int32_t)(w - (w & 15));
+        if (ln.k == LK::CONVOLVE_U8_U8)
+            st.launch = [=](cudaStream_t q) { return agocuda_Convolve_U8_U8(S(q), w, h, d, ds, s, ss, k.data(), cols, rows, shift, sb, se); };
+        else
+            st.launch = [=](cudaStream_t q) {
+                return agocuda_Convolve_S16_U8(S(q), w, h, (int16_t *)d, ds, s, ss, k.data(), cols, rows, shift, sb, se);
+            };
+        return VX_SUCCESS;
+    }
     case LK::LUT_U8_U8: case LK::LUT_S16_S16: {
         // the table's current contents go to device memory with the plan; a changed table
         // changes the graph's parameter hash and re-plans
@@ -509,6 +531,22 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         float k = sc_f32(p[2]), tc = sc_f32(p[3]);
         float norm = harris_norm(sc_i32(p[4]));
         st.launch = [=](cudaStream_t q) { return agocuda_HarrisScore_HVC_HG3_3x3(S(q), w, h, d, ds, s, ss, k, tc, norm); };
+        return VX_SUCCESS;
+    }
+    case LK::HARRIS_SOBEL_HG3_U8_5x5: case LK::HARRIS_SOBEL_HG3_U8_7x7: {
+        float *d = (float *)dptr(p[0]); const uint8_t *s = dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        const uint32_t gs = ln.k == LK::HARRIS_SOBEL_HG3_U8_5x5 ? 5 : 7;
+        st.launch = [=](cudaStream_t q) { return agocuda_HarrisSobel_HG3_U8_NxN(S(q), w, h, d, ds, s, ss, gs); };
+        return VX_SUCCESS;
+    }
+    case LK::HARRIS_SCORE_HVC_HG3_5x5: case LK::HARRIS_SCORE_HVC_HG3_7x7: {
+        float *d = (float *)dptr(p[0]); const float *s = (const float *)dptr(p[1]);
+        uint32_t w = W(p[0]), h = H(p[0]), ds = dstride(p[0]), ss = dstride(p[1]);
+        float k = sc_f32(p[2]), tc = sc_f32(p[3]);
+        const uint32_t bs = ln.k == LK::HARRIS_SCORE_HVC_HG3_5x5 ? 5 : 7;
+        float norm = harris_norm(sc_i32(p[4]), (int32_t)bs);
+        st.launch = [=](cudaStream_t q) { return agocuda_HarrisScore_HVC_HG3_NxN(S(q), w, h, d, ds, s, ss, k, tc, norm, bs); };
         return VX_SUCCESS;
     }
     case LK::NON_MAX_SUPP_XY_ANY_3x3: {

@@ -138,11 +138,13 @@ vx_status vxSetImageAttribute(vx_image image, vx_enum attribute, const void *ptr
     }
 }
 
+// x and y count image (plane 0) pixels; a plane subsampled by 2 has scale VX_SCALE_UNITY / 2,
+// so (scale * x) / VX_SCALE_UNITY is its element (vx_api.cpp:27-36, vxComputePatchOffset).
 void *vxFormatImagePatchAddress2d(void *ptr, vx_uint32 x, vx_uint32 y, const vx_imagepatch_addressing_t *addr)
 {
-    if (!ptr || !addr || x >= addr->dim_x || y >= addr->dim_y || !addr->scale_x || !addr->scale_y) return nullptr;
-    const vx_size ox = (vx_size)x * VX_SCALE_UNITY / addr->scale_x, oy = (vx_size)y * VX_SCALE_UNITY / addr->scale_y;
-    return (uint8_t *)ptr + oy * (vx_size)(vx_int64)addr->stride_y + ox * (vx_size)(vx_int64)addr->stride_x;
+    if (!ptr || !addr || x >= addr->dim_x || y >= addr->dim_y) return nullptr;
+    const vx_size ox = (vx_size)addr->scale_x * x / VX_SCALE_UNITY, oy = (vx_size)addr->scale_y * y / VX_SCALE_UNITY;
+    return (uint8_t *)ptr + (vx_int64)oy * addr->stride_y + (vx_int64)ox * addr->stride_x;
 }
 
 vx_status vxGetContextImageFormatDescription(vx_context context, vx_df_image format, AgoImageFormatDescription *desc)
@@ -185,7 +187,7 @@ vx_status vxAccessImagePatch(vx_image image, const vx_rectangle_t *rect, vx_uint
             addr->stride_x = (vx_int32)p.bpp;
             addr->stride_y = (vx_int32)(((addr->dim_x + sx - 1) / sx) * p.bpp);
             addr->scale_x = VX_SCALE_UNITY / sx; addr->scale_y = VX_SCALE_UNITY / sy;
-            addr->step_x = addr->step_y = 1;
+            addr->step_x = sx; addr->step_y = sy;
         }
         if (reads(usage)) {
             vx_status s = vxCopyImagePatch(image, rect, plane_index, addr, *ptr, VX_READ_ONLY, VX_MEMORY_TYPE_HOST);

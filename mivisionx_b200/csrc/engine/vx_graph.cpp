@@ -80,6 +80,7 @@ static uint64_t param_signature(Graph *g)
             case VX_TYPE_THRESHOLD: h = fnv(h, &static_cast<Threshold *>(r)->version, 8); break;
             case VX_TYPE_MATRIX: h = fnv(h, &static_cast<Matrix *>(r)->version, 8); break;
             case VX_TYPE_LUT: h = fnv(h, &static_cast<Lut *>(r)->version, 8); break;
+            case VX_TYPE_CONVOLUTION: h = fnv(h, &static_cast<Convolution *>(r)->version, 8); break;
             case VX_TYPE_REMAP: h = fnv(h, &static_cast<Remap *>(r)->version, 8); break;
             case VX_TYPE_IMAGE: {
                 Image *img = IMG(r);
@@ -988,5 +989,8 @@ vx_node vxHistogramNode(vx_graph graph, vx_image input, vx_distribution distribu
 vx_node vxChannelCombineNode(vx_graph graph, vx_image plane0, vx_image plane1, vx_image plane2, vx_image plane3,
                              vx_image output)
 { return make_node(graph, VX_KERNEL_CHANNEL_COMBINE, {R(plane0), R(plane1), R(plane2), R(plane3), R(output)}); }
+
+vx_node vxConvolveNode(vx_graph graph, vx_image input, vx_convolution conv, vx_image output)
+{ return make_node(graph, VX_KERNEL_CUSTOM_CONVOLUTION, {R(input), R(conv), R(output)}); }
 
 }  // extern "C"

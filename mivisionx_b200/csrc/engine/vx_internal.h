@@ -243,6 +243,8 @@ enum class LK : int {
     LUT_U8_U8, LUT_S16_S16, INTEGRAL_IMAGE_U32_U8, HISTOGRAM_DATA_U8,
     CANNY_SOBEL_U16_U8_5x5_L1NORM, CANNY_SOBEL_U16_U8_5x5_L2NORM, CANNY_SOBEL_U16_U8_7x7_L1NORM,
     CANNY_SOBEL_U16_U8_7x7_L2NORM, CANNY_SUPP_THRESHOLD_U8XY_U16_7x7,
+    CONVOLVE_U8_U8, CONVOLVE_S16_U8,
+    HARRIS_SOBEL_HG3_U8_5x5, HARRIS_SOBEL_HG3_U8_7x7, HARRIS_SCORE_HVC_HG3_5x5, HARRIS_SCORE_HVC_HG3_7x7,
     COUNT
 };
 const char *lk_name(LK k);

@@ -879,11 +879,13 @@ vx_status vxMapImagePatch(vx_image image, const vx_rectangle_t *rect, vx_uint32 
     uint8_t *base = p.host + (size_t)y0 * p.host_stride + (size_t)x0 * p.bpp;
     memset(addr, 0, sizeof(*addr));
     // dim_x / dim_y count the patch in image (plane 0) pixels; scale_x / scale_y shrink them to
-    // the plane's elements, as vx_api.cpp:2159-2161 reports a subsampled plane
+    // the plane's elements and step_x / step_y are the image pixels per element, as
+    // vx_api.cpp:2159-2164 reports a subsampled plane
     addr->dim_x = rect->end_x - rect->start_x; addr->dim_y = rect->end_y - rect->start_y;
     addr->stride_x = (vx_int32)p.bpp; addr->stride_y = (vx_int32)p.host_stride;
-    addr->scale_x = VX_SCALE_UNITY * p.width / img->width; addr->scale_y = VX_SCALE_UNITY * p.height / img->height;
-    addr->step_x = 1; addr->step_y = 1;
+    const uint32_t sx = p.width < img->width ? 2 : 1, sy = p.height < img->height ? 2 : 1;
+    addr->scale_x = VX_SCALE_UNITY / sx; addr->scale_y = VX_SCALE_UNITY / sy;
+    addr->step_x = sx; addr->step_y = sy;
     *ptr = base;
     vx_map_id id = img->next_map++;
     img->maps[id] = MapInfo{plane_index, *rect, usage, base};

@@ -22,20 +22,6 @@ uint64_t agocuda_count_launch(unsigned n);
 
 namespace {
 
-// Byte (r, c) of a U8 image stored as AGO stores it: row pitch ALIGN16(W), rows contiguous,
-// zeros before the first and after the last row and between W and the pitch.  Reading
-// column -1 therefore gives the previous row's padding (0) or, when W % 16 == 0, its last
-// pixel; column W gives padding or the next row's first pixel.
-__device__ __forceinline__ uint32_t ago_byte(const uint8_t *img, size_t stride, int W, int H, int r, int c)
-{
-    if (c >= 0 && c < W && r >= 0 && r < H) return img[(size_t)r * stride + c];
-    const long long S = (W + 15) & ~15;
-    const long long f = (long long)r * S + c;
-    if (f < 0 || f >= (long long)H * S) return 0;
-    const int rr = (int)(f / S), cc = (int)(f - rr * S);
-    return cc < W ? img[(size_t)rr * stride + cc] : 0;
-}
-
 // ---------------------------------------------------------------------------------
 // ScaleGaussianHalf 5x5.  A thread produces 8 output pixels x 8 output rows.  Pixel
 // pairs live in the two 16-bit halves of a 32-bit register (horizontal sums <= 4080,

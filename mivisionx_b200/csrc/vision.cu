@@ -1344,6 +1344,79 @@ k_harris_pick_cluster(const uint64_t *list, const uint32_t *listCount, uint32_t 
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Harris with 5x5 / 7x7 gradients (HafCpu_HarrisSobel_HG3_U8_{5x5,7x7}, ago_haf_cpu_harris.cpp:
+// 333, :455) and 5x5 / 7x7 blocks (HafCpu_HarrisScore_HVC_HG3_{5x5,7x7}, :661, :731), one
+// thread per pixel.  Gradients: separable integer taps over every column (the taps leaving
+// the row read the neighbouring rows' bytes as AGO lays them out), products rounded to
+// float; rows within gs/2 of the top and bottom written 0 (never written by the reference,
+// zero in its buffers).  Scores: window sums in the reference's (row, column) order, no
+// fused multiply-adds; the 7x7 kernel stores column x's score at x - 1 as the reference does
+// (it writes its third border zero without advancing its output pointer).
+// ---------------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(256) k_harris_sobel_nxn(int W, int H, float *dst, int dstStride, const uint8_t *src,
+                                                         int srcStride)
+{
+    const int x = blockIdx.x * 64 + (threadIdx.x & 63), y = blockIdx.y * 4 + (threadIdx.x >> 6);
+    if (x >= W || y >= H) return;
+    constexpr int R = G / 2;
+    float *o = (float *)((uint8_t *)dst + (size_t)y * dstStride) + 3 * x;
+    if (y < R || y >= H - R) { o[0] = 0.f; o[1] = 0.f; o[2] = 0.f; return; }
+    const int d5[5] = {-1, -2, 0, 2, 1}, s5[5] = {1, 4, 6, 4, 1};
+    const int d7[7] = {-1, -4, -5, 0, 5, 4, 1}, s7[7] = {1, 6, 15, 20, 15, 6, 1};
+    const bool inside = x >= R && x < W - R;
+    int gx = 0, gy = 0;
+#pragma unroll
+    for (int v = -R; v <= R; v++) {
+        int hd = 0, hs = 0;
+        const uint8_t *row = src + (size_t)(y + v) * srcStride;
+#pragma unroll
+        for (int u = -R; u <= R; u++) {
+            const int p = inside ? (int)row[x + u] : (int)ago_byte(src, (size_t)srcStride, W, H, y + v, x + u);
+            hd += (G == 5 ? d5[u + R] : d7[u + R]) * p;
+            hs += (G == 5 ? s5[u + R] : s7[u + R]) * p;
+        }
+        gx += (G == 5 ? s5[v + R] : s7[v + R]) * hd;
+        gy += (G == 5 ? d5[v + R] : d7[v + R]) * hs;
+    }
+    const float fx = (float)gx, fy = (float)gy;
+    o[0] = __fmul_rn(fx, fx);
+    o[1] = __fmul_rn(fx, fy);
+    o[2] = __fmul_rn(fy, fy);
+}
+
+template <int B>
+__global__ void __launch_bounds__(256) k_harris_score_nxn(int W, int H, float *dst, int dstStride, const float *src,
+                                                         int srcStride, float k, float Tc, float norm)
+{
+    const int x = blockIdx.x * 64 + (threadIdx.x & 63), y = blockIdx.y * 4 + (threadIdx.x >> 6);
+    if (x >= W || y >= H) return;
+    constexpr int R = B / 2, SHIFT = B == 7 ? 1 : 0;
+    // output column x holds the score of column x + SHIFT
+    const int c = x + SHIFT;
+    float v = 0.f;
+    if (y >= R && y < H - R && c >= R && c < W - R) {
+        float gx2 = 0.f, gy2 = 0.f, gxy2 = 0.f;
+#pragma unroll
+        for (int j = -R; j <= R; j++) {
+            const float *t = (const float *)((const uint8_t *)src + (size_t)(y + j) * srcStride);
+#pragma unroll
+            for (int i = -R; i <= R; i++) {
+                gx2 = __fadd_rn(gx2, t[3 * (c + i) + 0]);
+                gxy2 = __fadd_rn(gxy2, t[3 * (c + i) + 1]);
+                gy2 = __fadd_rn(gy2, t[3 * (c + i) + 2]);
+            }
+        }
+        const float traceA = __fadd_rn(gx2, gy2);
+        const float detA = __fsub_rn(__fmul_rn(gx2, gy2), __fmul_rn(gxy2, gxy2));
+        float Mc = __fsub_rn(detA, __fmul_rn(__fmul_rn(k, traceA), traceA));
+        Mc = __fdiv_rn(Mc, norm);
+        v = Mc > Tc ? Mc : 0.f;
+    }
+    *(float *)((uint8_t *)dst + (size_t)y * dstStride + 4 * (size_t)x) = v;
+}
+
 bool aligned(const void *p, unsigned a) { return ((uintptr_t)p & (a - 1)) == 0; }
 
 }  // namespace
@@ -1664,4 +1737,37 @@ extern "C" size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t W, uint32_t 
 {
     const uint32_t cap = harris_list_capacity(W, H);
     return 256 + pick_align((size_t)cap * 8) + agocuda_HarrisMergeSortAndPick_scratch_size(W, H, cap, minDistance);
+}
+
+extern "C" int agocuda_HarrisSobel_HG3_U8_NxN(void *stream, uint32_t W, uint32_t H, float *pDst, uint32_t dstStride,
+                                              const uint8_t *pSrc, uint32_t srcStride, uint32_t gradientSize)
+{
+    if (!pDst || !pSrc || (gradientSize != 5 && gradientSize != 7) || W < gradientSize || H < gradientSize ||
+        dstStride < 12 * W || srcStride < W || !aligned(pDst, 4) || (dstStride & 3))
+        return AGOCUDA_INVALID_PARAMS;
+    const dim3 grd(div_up(W, 64), div_up(H, 4));
+    if (gradientSize == 5)
+        k_harris_sobel_nxn<5><<<grd, 256, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride);
+    else
+        k_harris_sobel_nxn<7><<<grd, 256, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" int agocuda_HarrisScore_HVC_HG3_NxN(void *stream, uint32_t W, uint32_t H, float *pDst, uint32_t dstStride,
+                                               const float *pSrc, uint32_t srcStride, float sensitivity,
+                                               float strengthThreshold, float normFactor, uint32_t blockSize)
+{
+    if (!pDst || !pSrc || (blockSize != 5 && blockSize != 7) || W < blockSize || H < blockSize || dstStride < 4 * W ||
+        srcStride < 12 * W || !aligned(pDst, 4) || !aligned(pSrc, 4) || (dstStride & 3) || (srcStride & 3))
+        return AGOCUDA_INVALID_PARAMS;
+    const dim3 grd(div_up(W, 64), div_up(H, 4));
+    if (blockSize == 5)
+        k_harris_score_nxn<5><<<grd, 256, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride,
+                                                                  sensitivity, strengthThreshold, normFactor);
+    else
+        k_harris_score_nxn<7><<<grd, 256, 0, as_stream(stream)>>>((int)W, (int)H, pDst, (int)dstStride, pSrc, (int)srcStride,
+                                                                  sensitivity, strengthThreshold, normFactor);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
 }

@@ -189,6 +189,9 @@ _SIGS = {
     "vxXorNode": (vp, [vp, vp, vp, vp]), "vxNotNode": (vp, [vp, vp, vp]),
     "vxAddNode": (vp, [vp, vp, vp, i32, vp]), "vxSubtractNode": (vp, [vp, vp, vp, i32, vp]),
     "vxChannelCombineNode": (vp, [vp, vp, vp, vp, vp, vp]),
+    "vxConvolveNode": (vp, [vp, vp, vp, vp]),
+    "vxCreateConvolution": (vp, [vp, sz, sz]), "vxCopyConvolutionCoefficients": (i32, [vp, vp, i32, i32]),
+    "vxSetConvolutionAttribute": (i32, [vp, i32, vp, sz]), "vxReleaseConvolution": (i32, [C.POINTER(vp)]),
     "vxCreateLUT": (vp, [vp, i32, sz]), "vxCopyLUT": (i32, [vp, vp, i32, i32]), "vxQueryLUT": (i32, [vp, i32, vp, sz]),
     "vxTableLookupNode": (vp, [vp, vp, vp, vp]), "vxIntegralImageNode": (vp, [vp, vp, vp]),
     "vxCreateDistribution": (vp, [vp, sz, i32, u32]), "vxCopyDistribution": (i32, [vp, vp, i32, i32]),
@@ -273,6 +276,16 @@ class OpenVX:
         h = self.obj(self.vxCreateMatrix(ctx, VX_TYPE_FLOAT32, cols, rows), "matrix")
         self.ok(self.vxCopyMatrix(h, m.ctypes.data, VX_WRITE_ONLY, VX_MEMORY_TYPE_HOST), "vxCopyMatrix")
         return h
+
+    def convolution(self, ctx, coeffs: np.ndarray, scale: int = 1):
+        """vx_convolution of `coeffs` (rows x columns int16) with `scale` (a power of two)."""
+        k = np.ascontiguousarray(coeffs, dtype=np.int16)
+        rows, cols = k.shape
+        c = self.obj(self.vxCreateConvolution(ctx, cols, rows), "convolution")
+        self.ok(self.vxCopyConvolutionCoefficients(c, k.ctypes.data, VX_WRITE_ONLY, VX_MEMORY_TYPE_HOST), "coefficients")
+        v = C.c_uint32(scale)
+        self.ok(self.vxSetConvolutionAttribute(c, _attr_base(0, 0x80C) + 2, C.byref(v), 4), "scale")
+        return c
 
     def set_border(self, node, mode, value=0):
         b = vx_border_t()

@@ -44,6 +44,58 @@ int oracle_Gaussian_U8_U8_3x3(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t ds
     return 0;
 }
 
+/* ago_haf_cpu_filter.cpp:2676 (S16 3xN), :2858 (U8 3xN), :3037/:3170 (5xN), :3301/:3434 (7xN),
+ * :3565/:3698 (9xN).  Rows: dstHeight rows from pDst/pSrc (the wrapper starts them rows/2
+ * rows into the image, ago_kernel_api.cpp:15590).  Columns [0, W): prefix = bytes to the
+ * next 16-byte boundary of the destination row, body, postfix = (W - prefix) & 15. */
+static int conv_sum(const uint8_t *s, int st, int x, const int16_t *conv, int cols, int rows)
+{
+    int idx = cols * rows - 1, sum = 0;
+    for (int i = -(rows >> 1); i <= (rows >> 1); i++)
+        for (int j = -(cols >> 1); j <= (cols >> 1); j++) sum += (int)s[i * st + x + j] * (int)conv[idx--];
+    return sum;
+}
+
+static int conv_clamp(int v, int lo, int hi) { return v < lo ? lo : v > hi ? hi : v; }
+
+static int conv_rows(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, int bpp, const uint8_t *pSrc,
+                     uint32_t srcStride, const int16_t *conv, uint32_t cols, uint32_t rows, int32_t shift)
+{
+    const int lo = bpp == 1 ? 0 : -32768, hi = bpp == 1 ? 255 : 32767;
+    for (uint32_t y = 0; y < H; y++) {
+        const uint8_t *s = (const uint8_t *)ROW(pSrc, srcStride, y);
+        uint8_t *d = (uint8_t *)ROW(pDst, dstStride, y);
+        int prefix = (int)((uintptr_t)d & 15);
+        prefix = prefix ? 16 - prefix : 0;
+        const int postfix = ((int)W - prefix) & 15;
+        for (int x = 0; x < (int)W; x++) {
+            const int sum = conv_sum(s, (int)srcStride, x, conv, (int)cols, (int)rows);
+            int v;
+            if (x < prefix || x >= (int)W - postfix) {
+                v = conv_clamp(sum, lo, hi);                       /* scalar loops: no shift */
+            } else {
+                const int sh = (int)(int32_t)((uint32_t)sum >> shift);   /* _mm_srli_epi32 */
+                v = conv_clamp(conv_clamp(sh, -32768, 32767), lo, hi);  /* packs_epi32 (+ packus_epi16) */
+            }
+            if (bpp == 1) d[x] = (uint8_t)v;
+            else ((int16_t *)d)[x] = (int16_t)v;
+        }
+    }
+    return 0;
+}
+
+int oracle_Convolve_U8_U8(uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride, const uint8_t *pSrc,
+                          uint32_t srcStride, const int16_t *conv, uint32_t cols, uint32_t rows, int32_t shift)
+{
+    return conv_rows(W, H, pDst, dstStride, 1, pSrc, srcStride, conv, cols, rows, shift);
+}
+
+int oracle_Convolve_S16_U8(uint32_t W, uint32_t H, int16_t *pDst, uint32_t dstStride, const uint8_t *pSrc,
+                           uint32_t srcStride, const int16_t *conv, uint32_t cols, uint32_t rows, int32_t shift)
+{
+    return conv_rows(W, H, (uint8_t *)pDst, dstStride, 2, pSrc, srcStride, conv, cols, rows, shift);
+}
+
 static inline void sobel3(const uint8_t *s, int st, int x, int *gx, int *gy)
 {
     *gx = (s[x + 1 - st] - s[x - 1 - st]) + 2 * (s[x + 1] - s[x - 1]) + (s[x + 1 + st] - s[x - 1 + st]);
@@ -476,6 +528,77 @@ int oracle_HarrisScore_HVC_HG3_3x3(uint32_t W, uint32_t H, float *pDstVc, uint32
     }
     memset(ROW(pDstVc, dstStride, H - 1), 0, dstStride);
     return 0;
+}
+
+/* Separable 5x5 / 7x7 Sobel of HafCpu_HarrisSobel_HG3_U8_{5x5,7x7}: derivative taps d and
+ * smoothing taps s; gx = smoothing down the rows of the rows' horizontal derivatives, gy =
+ * derivative down the rows of the rows' horizontal smoothing (exact integers). */
+static const int kHarrisD5[5] = {-1, -2, 0, 2, 1}, kHarrisS5[5] = {1, 4, 6, 4, 1};
+static const int kHarrisD7[7] = {-1, -4, -5, 0, 5, 4, 1}, kHarrisS7[7] = {1, 6, 15, 20, 15, 6, 1};
+
+int oracle_HarrisSobel_HG3_U8_NxN(uint32_t W, uint32_t H, float *pDst, uint32_t dstStride, const uint8_t *pSrc,
+                                  uint32_t srcStride, uint32_t gs)
+{
+    const int r = (int)gs / 2;
+    const int *d = gs == 5 ? kHarrisD5 : kHarrisD7, *sm = gs == 5 ? kHarrisS5 : kHarrisS7;
+    for (int y = r; y < (int)H - r; y++) {
+        float *o = (float *)ROW(pDst, dstStride, y);
+        for (int x = 0; x < (int)W; x++) {
+            int gx = 0, gy = 0;
+            for (int v = -r; v <= r; v++) {
+                const uint8_t *row = (const uint8_t *)ROW(pSrc, srcStride, y + v);
+                int hd = 0, hs = 0;
+                for (int u = -r; u <= r; u++) {
+                    hd += d[u + r] * (int)row[x + u];
+                    hs += sm[u + r] * (int)row[x + u];
+                }
+                gx += sm[v + r] * hd;
+                gy += d[v + r] * hs;
+            }
+            o[3 * x + 0] = (float)gx * (float)gx;
+            o[3 * x + 1] = (float)gx * (float)gy;
+            o[3 * x + 2] = (float)gy * (float)gy;
+        }
+    }
+    return 0;
+}
+
+int oracle_HarrisScore_HVC_HG3_NxN(uint32_t W, uint32_t H, float *pDstVc, uint32_t dstStride, const float *pSrcGxy,
+                                   uint32_t srcStride, float k, float Tc, float norm, uint32_t bs)
+{
+    const int r = (int)bs / 2;
+    /* the 7x7 kernel writes its third left-border zero without advancing the output pointer
+     * (ago_haf_cpu_harris.cpp:758-763): column x's score lands at x - 1, and the last column
+     * of the rows it processes is never written (0 here, as in AGO's zeroed buffers) */
+    const int shift = bs == 7 ? 1 : 0;
+    for (int y = 0; y < (int)H; y++) {
+        float *d = (float *)ROW(pDstVc, dstStride, y);
+        for (int x = 0; x < (int)W; x++) d[x] = 0;
+        if (y < r || y >= (int)H - r) continue;
+        for (int x = r; x < (int)W - r; x++) {
+            float gx2 = 0, gy2 = 0, gxy2 = 0;
+            for (int j = -r; j <= r; j++) {
+                const float *t = (const float *)ROW(pSrcGxy, srcStride, y + j);
+                for (int i = -r; i <= r; i++) {
+                    gx2 += t[3 * (x + i) + 0];
+                    gxy2 += t[3 * (x + i) + 1];
+                    gy2 += t[3 * (x + i) + 2];
+                }
+            }
+            float traceA = gx2 + gy2;
+            float detA = (gx2 * gy2) - (gxy2 * gxy2);
+            float Mc = detA - (k * traceA * traceA);
+            Mc /= norm;
+            d[x - shift] = (Mc > Tc) ? Mc : 0;
+        }
+    }
+    return 0;
+}
+
+float oracle_harris_norm_factor_block(int32_t gs, int32_t bs)
+{
+    float f = 255.0f * (float)(1 << (gs - 1)) * (float)bs;
+    return f * f * f * f;
 }
 
 /* ago_haf_cpu_harris.cpp:882 HafCpu_NonMaxSupp_XY_ANY_3x3: keep v if >= the three pixels

@@ -27,6 +27,16 @@ int oracle_SobelMagnitude_S16_U8_3x3(uint32_t dstWidth, uint32_t dstHeight, int1
                                      const uint8_t *pSrc, uint32_t srcStride);
 int oracle_Sobel_S16S16_U8_3x3_GXY(uint32_t dstWidth, uint32_t dstHeight, int16_t *pGx, uint32_t gxStride,
                                    int16_t *pGy, uint32_t gyStride, const uint8_t *pSrc, uint32_t srcStride);
+/* ago_haf_cpu_filter.cpp:2676-3830 HafCpu_Convolve_{S16,U8}_U8_{3,5,7,9}xN, one function for
+ * every width (cols = 3, 5, 7, 9; rows odd): the kernel applied flipped, sums in int32; SIMD
+ * body columns shift logically by `shift` then saturate (to int16, then to u8), the scalar
+ * prefix and postfix columns saturate the sum without shifting. */
+int oracle_Convolve_U8_U8(uint32_t dstWidth, uint32_t dstHeight, uint8_t *pDst, uint32_t dstStride,
+                          const uint8_t *pSrc, uint32_t srcStride, const int16_t *conv, uint32_t cols, uint32_t rows,
+                          int32_t shift);
+int oracle_Convolve_S16_U8(uint32_t dstWidth, uint32_t dstHeight, int16_t *pDst, uint32_t dstStride,
+                           const uint8_t *pSrc, uint32_t srcStride, const int16_t *conv, uint32_t cols, uint32_t rows,
+                           int32_t shift);
 /* ---- arithmetic (ago_haf_cpu_arithmetic.cpp) ---- */
 int oracle_Magnitude_S16_S16S16(uint32_t dstWidth, uint32_t dstHeight, int16_t *pMag, uint32_t magStride,
                                 const int16_t *pGx, uint32_t gxStride, const int16_t *pGy, uint32_t gyStride);
@@ -56,6 +66,19 @@ int oracle_HarrisSobel_HG3_U8_3x3(uint32_t dstWidth, uint32_t dstHeight, float *
 int oracle_HarrisScore_HVC_HG3_3x3(uint32_t dstWidth, uint32_t dstHeight, float *pDstVc, uint32_t dstStride,
                                    const float *pSrcGxy, uint32_t srcStride, float sensitivity, float threshold,
                                    float normFactor);
+/* ago_haf_cpu_harris.cpp:333 / :455 HafCpu_HarrisSobel_HG3_U8_{5x5,7x7} (gs = 5 or 7): pDst and
+ * pSrc at row 0; rows [gs/2, H - gs/2) written, all columns (reading outside the row at the
+ * edges). */
+int oracle_HarrisSobel_HG3_U8_NxN(uint32_t dstWidth, uint32_t dstHeight, float *pDstGxy, uint32_t dstStride,
+                                  const uint8_t *pSrc, uint32_t srcStride, uint32_t gs);
+/* ago_haf_cpu_harris.cpp:596 / :661 / :731 HafCpu_HarrisScore_HVC_HG3_{3x3,5x5,7x7} (bs = 3, 5, 7):
+ * window sums in the reference's (j, i) order, rows and columns within bs/2 of a border 0; the
+ * 7x7 kernel stores column x's score at x - 1 (an output pointer it does not advance). */
+int oracle_HarrisScore_HVC_HG3_NxN(uint32_t dstWidth, uint32_t dstHeight, float *pDstVc, uint32_t dstStride,
+                                   const float *pSrcGxy, uint32_t srcStride, float sensitivity, float threshold,
+                                   float normFactor, uint32_t bs);
+/* the score normalisation of the AGO wrappers (ago_kernel_api.cpp:16941, :17012, :17083) */
+float oracle_harris_norm_factor_block(int32_t gs, int32_t bs);
 int oracle_NonMaxSupp_XY_ANY_3x3(uint32_t capacity, oracle_xys *list, uint32_t *pCount, uint32_t srcWidth,
                                  uint32_t srcHeight, const float *pSrc, uint32_t srcStride);
 int oracle_HarrisMergeSortAndPick_XY_XYS(uint32_t capacity, oracle_keypoint *corners, uint32_t *pCount,

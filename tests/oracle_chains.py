@@ -44,6 +44,8 @@ _SIGS.update({
     "CannyEdgeTrace_U8_U8XY": [u32, u32, vp, u32, u32, vp, u32],
     "HarrisSobel_HG3_U8_3x3": [u32, u32, vp, u32, vp, u32],
     "HarrisScore_HVC_HG3_3x3": [u32, u32, vp, u32, vp, u32, C.c_float, C.c_float, C.c_float],
+    "HarrisSobel_HG3_U8_NxN": [u32, u32, vp, u32, vp, u32, u32],
+    "HarrisScore_HVC_HG3_NxN": [u32, u32, vp, u32, vp, u32, C.c_float, C.c_float, C.c_float, u32],
     "NonMaxSupp_XY_ANY_3x3": [u32, vp, C.POINTER(C.c_uint32), u32, u32, vp, u32],
     "HarrisMergeSortAndPick_XY_XYS": [u32, vp, C.POINTER(C.c_uint32), vp, u32, C.c_float, u32, u32],
 })
@@ -84,15 +86,29 @@ def canny(img: np.ndarray, lower=80, upper=100):
     return canny_parts(img, lower, upper)[3], (2, 2, w - 2, h - 2)
 
 
-def harris_parts(img: np.ndarray, k=0.04, tc=1e-3):
+def harris_norm_block(gs, bs):
+    f = O.oracle_lib().oracle_harris_norm_factor_block
+    f.argtypes, f.restype = [i32, i32], C.c_float
+    return f(gs, bs)
+
+
+def harris_parts(img: np.ndarray, k=0.04, tc=1e-3, gs=3, bs=3):
+    """HarrisSobel_HG3_U8_{gs}x{gs}, HarrisScore_HVC_HG3_{bs}x{bs} (normalised by
+    (255 * 2^(gs-1) * bs)^4) and NonMaxSupp_XY_ANY_3x3 on AGO-laid-out zeroed buffers."""
     h, w = img.shape
     src = ago_img(h, w); src.set(img)
     hg3 = ago_img(h, w, np.float32, 3)
     hvc = ago_img(h, w, np.float32)
     lst = np.zeros(w * h, XYS)
     cnt = C.c_uint32(0)
-    fn("HarrisSobel_HG3_U8_3x3")(w, h, hg3.ptr, hg3.stride, src.ptr, src.stride)
-    fn("HarrisScore_HVC_HG3_3x3")(w, h, hvc.ptr, hvc.stride, hg3.ptr, hg3.stride, k, tc, harris_norm(3))
+    if gs == 3:
+        fn("HarrisSobel_HG3_U8_3x3")(w, h, hg3.ptr, hg3.stride, src.ptr, src.stride)
+    else:
+        fn("HarrisSobel_HG3_U8_NxN")(w, h, hg3.ptr, hg3.stride, src.ptr, src.stride, gs)
+    if bs == 3:
+        fn("HarrisScore_HVC_HG3_3x3")(w, h, hvc.ptr, hvc.stride, hg3.ptr, hg3.stride, k, tc, harris_norm_block(gs, 3))
+    else:
+        fn("HarrisScore_HVC_HG3_NxN")(w, h, hvc.ptr, hvc.stride, hg3.ptr, hg3.stride, k, tc, harris_norm_block(gs, bs), bs)
     fn("NonMaxSupp_XY_ANY_3x3")(w * h, lst.ctypes.data, C.byref(cnt), w, h, hvc.ptr, hvc.stride)
     return hg3.get(), hvc.get(), lst[:cnt.value].copy()
 
@@ -164,10 +180,10 @@ def color_scale_warp(rgb: np.ndarray, matrix: np.ndarray):
     return out
 
 
-def harris(img: np.ndarray, k=0.04, tc=1e-3, min_distance=5.0, capacity=1 << 20):
-    """vxHarrisCornersNode (gradient 3, block 3): (corners, num_corners)."""
+def harris(img: np.ndarray, k=0.04, tc=1e-3, min_distance=5.0, capacity=1 << 20, gs=3, bs=3):
+    """vxHarrisCornersNode (gradient gs, block bs): (corners, num_corners)."""
     h, w = img.shape
-    return harris_pick(harris_parts(img, k, tc)[2], w, h, min_distance, capacity)
+    return harris_pick(harris_parts(img, k, tc, gs, bs)[2], w, h, min_distance, capacity)
 
 
 def shrink(rect, n):

@@ -62,6 +62,18 @@ CASES = [
     _unary("filter/Sobel_S16_U8_3x3_GX", "sobel_3x3", "U008", "S016", 1, " null"),
     Case("filter/Sobel_S16_U8_3x3_GY", [("input_1", 1920, 1080, "U008")], [("output_1", 1920, 1080, "S016", 1)], [],
          "node org.khronos.openvx.sobel_3x3 input_1 null output_1"),
+    Case("filter/Convolve_U8_U8_3x3", [("input_1", 1920, 1080, "U008")], [("output_1", 1920, 1080, "U008", 1)],
+         ["data input_matrix = convolution:3,3:INIT,{-1;-1;-1;-1;16;-1;-1;-1;-1}"],
+         "node org.khronos.openvx.custom_convolution input_1 input_matrix output_1"),
+    Case("filter/Convolve_S16_U8_3x3", [("input_1", 1920, 1080, "U008")], [("output_1", 1920, 1080, "S016", 1)],
+         ["data input_matrix = convolution:3,3:INIT,{1;2;1;0;0;0;-1;-2;-1}"],
+         "node org.khronos.openvx.custom_convolution input_1 input_matrix output_1"),
+    Case("filter/Convolve_U8_U8_9x3", [("input_1", 1920, 1080, "U008")], [("output_1", 1920, 1080, "U008", 4)],
+         ["data input_matrix = convolution:9,3:INIT,{" + ";".join(str((7 * i) % 11 - 5) for i in range(27)) + "}"],
+         "node org.khronos.openvx.custom_convolution input_1 input_matrix output_1"),
+    Case("filter/Convolve_S16_U8_9x3", [("input_1", 1920, 1080, "U008")], [("output_1", 1920, 1080, "S016", 4)],
+         ["data input_matrix = convolution:9,3:INIT,{" + ";".join(str((13 * i) % 17 - 8) for i in range(27)) + "}"],
+         "node org.khronos.openvx.custom_convolution input_1 input_matrix output_1"),
     # color/
     Case("color/ChannelCombine_U16_U8U8", [("input_1", 960, 540, "U008"), ("input_2", 960, 540, "U008")],
          [("output_1", 1920, 1080, "NV12", 0)], ["data luma = image:1920,1080,U008"],

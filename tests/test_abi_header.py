@@ -84,3 +84,31 @@ def test_ctypes_mirrors_match_agocuda_structs():
         assert int(got[n]) == ctypes.sizeof(cls), n
     for f in ("count", "scharrWords", "windowDimension", "newCapacity"):
         assert int(got["lk." + f]) == getattr(native.LkFrame, f).offset, f
+
+
+def test_patch_address_matches_reference():
+    """vxFormatImagePatchAddress2d on addressing structures as vxMapImagePatch reports a full
+    plane and a plane subsampled by 2 (scale VX_SCALE_UNITY / 2, step 2; vx_api.cpp:27-36,
+    :2159-2164): the same byte offset as the reference library's, for every (x, y) probed,
+    and NULL outside the patch."""
+    import ctypes as C
+    import oracle as O
+    from mivisionx_b200 import native
+    from mivisionx_b200 import vx as V
+    ref = O.ref_lib()
+    if ref is None or not os.path.exists(native.OPENVX_SO):
+        pytest.skip("libraries not built")
+    fns = []
+    for lib in (native.openvx(), ref):
+        f = lib.vxFormatImagePatchAddress2d
+        f.argtypes, f.restype = [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(V.vx_imagepatch_addressing_t)], C.c_void_p
+        fns.append(f)
+    base = 1 << 20
+    for scale, step, bpp in ((1024, 1, 1), (1024, 1, 2), (512, 2, 1), (512, 2, 2)):
+        a = V.vx_imagepatch_addressing_t()
+        a.dim_x, a.dim_y, a.stride_x, a.stride_y = 1280, 720, bpp, 1344
+        a.scale_x = a.scale_y = scale
+        a.step_x = a.step_y = step
+        for x, y in ((0, 0), (1, 0), (2, 0), (3, 5), (1279, 719), (640, 2), (1280, 0), (0, 720)):
+            got, want = fns[0](base, x, y, C.byref(a)), fns[1](base, x, y, C.byref(a))
+            assert got == want, (scale, bpp, x, y, got, want)
