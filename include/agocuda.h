@@ -166,6 +166,22 @@ int agocuda_CannyEdgeTrace_U8_U8XY_noalloc(void *stream, uint32_t width, uint32_
                                            const uint32_t *pStack, const uint32_t *pStackCount, uint32_t stackCapacity,
                                            uint32_t *pStatus);
 
+/* FAST-9 corners (vxFastCornersNode): rows 3 .. H-4 of a U8 image; without suppression every
+ * column (the circle of the three outer columns reads across the row ends as AGO's layout
+ * holds the image: pitch ALIGN16(W), zero padding) with strength = strengthThreshold; with
+ * suppression columns 3 .. W-4, strength = the reference's binary-searched corner strength,
+ * kept when >= the upper and left neighbours and > the right and lower ones.  Writes
+ * vx_keypoint_t records in raster order, *pCornerCount = min(found, capacity), *pNumCorners =
+ * found (either may be NULL).  `scratch` (256-byte aligned) holds
+ * agocuda_FastCorners_scratch_size(W, H) bytes.  Four kernels.  HafCpu_FastCorners_XY_U8_
+ * {NoSupression,Supression} (ago_haf_cpu_fast_corners.cpp:414, :599); replaces
+ * HipExec_FastCorners_XY_U8_{NoSupression,Supression} (hipvx/hip_host_decls.h:858/863), which
+ * append in arbitrary order. */
+size_t agocuda_FastCorners_scratch_size(uint32_t width, uint32_t height);
+int agocuda_FastCorners_XY_U8(void *stream, uint32_t width, uint32_t height, const uint8_t *pSrc, uint32_t srcStride,
+                              float strengthThreshold, int32_t nonmaxSuppression, void *pCorners, uint32_t cornerCapacity,
+                              uint32_t *pCornerCount, uint32_t *pNumCorners, void *scratch, size_t scratchBytes);
+
 /* Convolve (vxConvolveNode): U8 source, U8 or S16 destination, cols in {3, 5, 7, 9}, rows
  * odd in [3, 9]; `conv` is a HOST pointer to the rows x cols coefficients in vx_convolution
  * order (applied flipped, as OpenVX defines convolution), `shift` = log2 of the scale.

@@ -502,6 +502,8 @@ vx_node vxWarpPerspectiveNode(vx_graph graph, vx_image input, vx_matrix matrix, 
 vx_node vxHarrisCornersNode(vx_graph graph, vx_image input, vx_scalar strength_thresh, vx_scalar min_distance,
                             vx_scalar sensitivity, vx_int32 gradient_size, vx_int32 block_size, vx_array corners,
                             vx_scalar num_corners);
+vx_node vxFastCornersNode(vx_graph graph, vx_image input, vx_scalar strength_thresh, vx_bool nonmax_suppression,
+                          vx_array corners, vx_scalar num_corners);
 vx_node vxOpticalFlowPyrLKNode(vx_graph graph, vx_pyramid old_images, vx_pyramid new_images, vx_array old_points,
                                vx_array new_points_estimates, vx_array new_points, vx_enum termination, vx_scalar epsilon,
                                vx_scalar num_iterations, vx_scalar use_initial_estimate, vx_size window_dimension);

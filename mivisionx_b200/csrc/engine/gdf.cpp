@@ -86,6 +86,7 @@ const NamedEnum kKernels[] = {
     {"xor", VX_KERNEL_XOR}, {"not", VX_KERNEL_NOT}, {"add", VX_KERNEL_ADD}, {"subtract", VX_KERNEL_SUBTRACT},
     {"warp_affine", VX_KERNEL_WARP_AFFINE}, {"warp_perspective", VX_KERNEL_WARP_PERSPECTIVE},
     {"harris_corners", VX_KERNEL_HARRIS_CORNERS}, {"optical_flow_pyr_lk", VX_KERNEL_OPTICAL_FLOW_PYR_LK},
+    {"fast_corners", VX_KERNEL_FAST_CORNERS},
     {"remap", VX_KERNEL_REMAP}, {"halfscale_gaussian", VX_KERNEL_HALFSCALE_GAUSSIAN},
 };
 

@@ -45,6 +45,7 @@ static const char *kLKNames[] = {
     "CannySobel_U16_U8_7x7_L2NORM", "CannySuppThreshold_U8XY_U16_7x7",
     "Convolve_U8_U8", "Convolve_S16_U8",
     "HarrisSobel_HG3_U8_5x5", "HarrisSobel_HG3_U8_7x7", "HarrisScore_HVC_HG3_5x5", "HarrisScore_HVC_HG3_7x7",
+    "FastCorners_XY_U8_Supression", "FastCorners_XY_U8_NoSupression",
 };
 static_assert(sizeof(kLKNames) / sizeof(kLKNames[0]) == (size_t)LK::COUNT, "kernel name table");
 
@@ -173,6 +174,18 @@ vx_status validate_node(Graph *g, Node *n)
         }
         if (!is_valid(p[6], VX_TYPE_ARRAY)) return VX_ERROR_INVALID_PARAMETERS;
         Array *a = static_cast<Array *>(p[6]);
+        if (a->item_type == VX_TYPE_INVALID && a->is_virtual) { a->item_type = VX_TYPE_KEYPOINT; a->item_size = sizeof(vx_keypoint_t); }
+        if (a->item_type != VX_TYPE_KEYPOINT) return VX_ERROR_INVALID_TYPE;
+        if (!a->capacity) return VX_ERROR_INVALID_DIMENSION;
+        return VX_SUCCESS;
+    }
+    case VX_KERNEL_FAST_CORNERS: {                     // agoKernel_FastCorners_XY_U8_* validate (ago_kernel_api.cpp:16606)
+        if (!fmt_is(p[0], VX_DF_IMAGE_U8)) return VX_ERROR_INVALID_FORMAT;
+        if (img(0)->width < 7 || img(0)->height < 7) return VX_ERROR_INVALID_DIMENSION;
+        if (!is_valid(p[1], VX_TYPE_SCALAR) || static_cast<Scalar *>(p[1])->data_type != VX_TYPE_FLOAT32) return VX_ERROR_INVALID_TYPE;
+        if (!is_valid(p[2], VX_TYPE_SCALAR)) return VX_ERROR_INVALID_PARAMETERS;
+        if (!is_valid(p[3], VX_TYPE_ARRAY)) return VX_ERROR_INVALID_PARAMETERS;
+        Array *a = static_cast<Array *>(p[3]);
         if (a->item_type == VX_TYPE_INVALID && a->is_virtual) { a->item_type = VX_TYPE_KEYPOINT; a->item_size = sizeof(vx_keypoint_t); }
         if (a->item_type != VX_TYPE_KEYPOINT) return VX_ERROR_INVALID_TYPE;
         if (!a->capacity) return VX_ERROR_INVALID_DIMENSION;
@@ -422,6 +435,13 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
         add(LK::HARRIS_MERGE_SORT_AND_PICK_XY_XYS, {p[6], p.size() > 7 ? p[7] : nullptr, xys, p[2], sw, sh});
         return VX_SUCCESS;
     }
+    case VX_KERNEL_FAST_CORNERS: {                                                                     // :1789
+        // {corners, num_corners, input, strength}; the suppression flag picks the kernel
+        const bool sup = static_cast<Scalar *>(p[2])->v.i32 != 0;
+        add(sup ? LK::FAST_CORNERS_XY_U8_SUPRESSION : LK::FAST_CORNERS_XY_U8_NOSUPRESSION,
+            {p[3], p.size() > 4 ? p[4] : nullptr, p[0], p[1]});
+        return VX_SUCCESS;
+    }
     case VX_KERNEL_COLOR_CONVERT: {                                                                    // :200-256
         Image *o = IMG(p[1]);
         if (o->format == VX_DF_IMAGE_NV12) {
@@ -560,6 +580,7 @@ static int num_outputs(LK k)
     case LK::COLOR_CONVERT_IYUV_RGB: return 3;
     case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3: case LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7: return 2;
     case LK::HARRIS_MERGE_SORT_AND_PICK_XY_XYS: return 2;
+    case LK::FAST_CORNERS_XY_U8_SUPRESSION: case LK::FAST_CORNERS_XY_U8_NOSUPRESSION: return 2;
     default: return 1;
     }
 }

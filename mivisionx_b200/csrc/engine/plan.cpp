@@ -576,6 +576,25 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         };
         return VX_SUCCESS;
     }
+    case LK::FAST_CORNERS_XY_U8_SUPRESSION: case LK::FAST_CORNERS_XY_U8_NOSUPRESSION: {
+        Array *corners = static_cast<Array *>(p[0]);
+        Scalar *num = p[1] ? static_cast<Scalar *>(p[1]) : nullptr;
+        if (num && scalar_alloc_device(num)) return VX_ERROR_NO_MEMORY;
+        const uint8_t *s = dptr(p[2]);
+        uint32_t w = W(p[2]), h = H(p[2]), ss = dstride(p[2]);
+        const float thr = sc_f32(p[3]);
+        const int32_t sup = ln.k == LK::FAST_CORNERS_XY_U8_SUPRESSION;
+        void *out = corners->dev; uint32_t ocap = (uint32_t)corners->capacity; uint32_t *oc = corners->dev_count;
+        uint32_t *nc = num ? num->dev : nullptr;
+        const size_t sb = agocuda_FastCorners_scratch_size(w, h);
+        void *scr = scratch(g, sb);
+        if (!scr) return VX_ERROR_NO_MEMORY;
+        st.num_kernels = 4;
+        st.launch = [=](cudaStream_t q) {
+            return agocuda_FastCorners_XY_U8(S(q), w, h, s, ss, thr, sup, out, ocap, oc, nc, scr, sb);
+        };
+        return VX_SUCCESS;
+    }
     case LK::COLOR_CONVERT_NV12_RGB: {
         uint8_t *y = dptr(p[0]), *uv = dptr(p[1]); const uint8_t *s = dptr(p[2]);
         uint32_t w = W(p[2]), h = H(p[2]), ys = dstride(p[0]), uvs = dstride(p[1]), ss = dstride(p[2]);

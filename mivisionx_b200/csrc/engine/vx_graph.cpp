@@ -928,6 +928,13 @@ vx_node vxHarrisCornersNode(vx_graph graph, vx_image input, vx_scalar strength_t
                       scalar_of(graph, VX_TYPE_INT32, &block_size), R(corners), R(num_corners)});
 }
 
+vx_node vxFastCornersNode(vx_graph graph, vx_image input, vx_scalar strength_thresh, vx_bool nonmax_suppression,
+                          vx_array corners, vx_scalar num_corners)
+{
+    return make_node(graph, VX_KERNEL_FAST_CORNERS,
+                     {R(input), R(strength_thresh), scalar_of(graph, VX_TYPE_BOOL, &nonmax_suppression), R(corners), R(num_corners)});
+}
+
 vx_node vxOpticalFlowPyrLKNode(vx_graph graph, vx_pyramid old_images, vx_pyramid new_images, vx_array old_points,
                                vx_array new_points_estimates, vx_array new_points, vx_enum termination, vx_scalar epsilon,
                                vx_scalar num_iterations, vx_scalar use_initial_estimate, vx_size window_dimension)

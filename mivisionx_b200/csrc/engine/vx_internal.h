@@ -245,6 +245,7 @@ enum class LK : int {
     CANNY_SOBEL_U16_U8_7x7_L2NORM, CANNY_SUPP_THRESHOLD_U8XY_U16_7x7,
     CONVOLVE_U8_U8, CONVOLVE_S16_U8,
     HARRIS_SOBEL_HG3_U8_5x5, HARRIS_SOBEL_HG3_U8_7x7, HARRIS_SCORE_HVC_HG3_5x5, HARRIS_SCORE_HVC_HG3_7x7,
+    FAST_CORNERS_XY_U8_SUPRESSION, FAST_CORNERS_XY_U8_NOSUPRESSION,
     COUNT
 };
 const char *lk_name(LK k);

@@ -178,6 +178,7 @@ _SIGS = {
     "vxThresholdNode": (vp, [vp, vp, vp, vp]),
     "vxCannyEdgeDetectorNode": (vp, [vp, vp, vp, i32, i32, vp]),
     "vxHarrisCornersNode": (vp, [vp, vp, vp, vp, vp, i32, i32, vp, vp]),
+    "vxFastCornersNode": (vp, [vp, vp, vp, i32, vp, vp]),
     "vxColorConvertNode": (vp, [vp, vp, vp]), "vxChannelExtractNode": (vp, [vp, vp, i32, vp]),
     "vxScaleImageNode": (vp, [vp, vp, vp, i32]), "vxWarpAffineNode": (vp, [vp, vp, vp, i32, vp]),
     "vxWarpPerspectiveNode": (vp, [vp, vp, vp, i32, vp]), "vxRemapNode": (vp, [vp, vp, vp, i32, vp]),

@@ -601,6 +601,134 @@ float oracle_harris_norm_factor_block(int32_t gs, int32_t bs)
     return f * f * f * f;
 }
 
+/* ============================== FAST corners ============================== */
+
+/* The 16 pixels of the radius-3 Bresenham circle, clockwise from the pixel three rows above
+ * (ago_haf_cpu_fast_corners.cpp:36 generateOffset), as (dx, dy). */
+static const int kFastDx[16] = {0, 1, 2, 3, 3, 3, 2, 1, 0, -1, -2, -3, -3, -3, -2, -1};
+static const int kFastDy[16] = {-3, -3, -2, -1, 0, 1, 2, 3, 3, 3, 2, 1, 0, -1, -2, -3};
+
+/* bit i of the result: circle pixels i .. i+8 (mod 16) all set in the 16-bit mask m */
+static int fast_arc9(uint32_t m)
+{
+    uint32_t r = m | (m << 16);
+    uint32_t a = r & (r >> 1);
+    a &= a >> 2;
+    a &= a >> 4;
+    a &= r >> 8;
+    return (a & 0xFFFFu) != 0;
+}
+
+/* circle pixel i of candidate p, read by raw offset as the reference does (p[offset]) */
+static void fast_circle(const uint8_t *p, int stride, int b[16])
+{
+    for (int i = 0; i < 16; i++) b[i] = p[kFastDy[i] * stride + kFastDx[i]];
+}
+
+/* masks of the circle pixels brighter than c + t / darker than c - t in 16-bit arithmetic
+ * (:58 generateMasks_C, :297 isCorner_SSE) */
+static void fast_masks(int c, const int b[16], int t, uint32_t *plus, uint32_t *minus)
+{
+    const int16_t hi = (int16_t)(c + t), lo = (int16_t)(c - t);
+    *plus = *minus = 0;
+    for (int i = 0; i < 16; i++) {
+        if ((int16_t)b[i] > hi) *plus |= 1u << i;
+        if ((int16_t)b[i] < lo) *minus |= 1u << i;
+    }
+}
+
+/* the strength search of :216 checkForCornerAndGetStrength: a binary search between t (a
+ * corner) and 255 (never one) for the largest threshold that still makes a corner */
+static int fast_search(int c, const int b[16], int t, int sign)
+{
+    int lower = t, upper = 255;
+    while (upper - lower > 1) {
+        const int mid = (upper + lower) >> 1;
+        uint32_t plus, minus;
+        fast_masks(c, b, mid, &plus, &minus);
+        if (fast_arc9(sign > 0 ? plus : minus)) lower = mid;
+        else upper = mid;
+    }
+    return lower;
+}
+
+static int fast_strength(const uint8_t *p, int stride, int t)
+{
+    int b[16];
+    fast_circle(p, stride, b);
+    const int c = p[0];
+    uint32_t plus, minus;
+    fast_masks(c, b, t, &plus, &minus);
+    const int sp = fast_arc9(plus) ? fast_search(c, b, t, 1) : 0;
+    const int sn = fast_arc9(minus) ? fast_search(c, b, t, -1) : 0;
+    return sp > sn ? sp : sn;
+}
+
+static void fast_emit(oracle_keypoint *corners, uint32_t capacity, uint32_t *n, int x, int y, float strength)
+{
+    if (*n < capacity) {
+        oracle_keypoint *k = &corners[*n];
+        k->x = x; k->y = y; k->strength = strength;
+        k->scale = 0; k->orientation = 0; k->tracking_status = 1; k->error = 0;
+    }
+    (*n)++;
+}
+
+/* :414 HafCpu_FastCorners_XY_U8_NoSupression: rows 3 .. H-4, every column (the circle of the
+ * three outer columns on each side reads across the row's end, into the neighbouring row or
+ * the row padding); strength = strength_threshold. */
+int oracle_FastCorners_XY_U8_NoSupression(uint32_t capacity, oracle_keypoint *corners, uint32_t *pCount, uint32_t W,
+                                          uint32_t H, const uint8_t *pSrc, uint32_t srcStride, float strengthThreshold)
+{
+    const int t = (int16_t)floorf(strengthThreshold);
+    uint32_t n = 0;
+    for (int y = 3; y < (int)H - 3; y++)
+        for (int x = 0; x < (int)W; x++) {
+            const uint8_t *p = pSrc + (size_t)y * srcStride + x;
+            int b[16];
+            fast_circle(p, (int)srcStride, b);
+            uint32_t plus, minus;
+            fast_masks(p[0], b, t, &plus, &minus);
+            if (fast_arc9(plus) || fast_arc9(minus)) fast_emit(corners, capacity, &n, x, y, strengthThreshold);
+        }
+    *pCount = n;
+    return 0;
+}
+
+int oracle_FastCorners_strength(uint8_t *pDst, uint32_t W, uint32_t H, const uint8_t *pSrc, uint32_t srcStride,
+                                float strengthThreshold)
+{
+    const int t = (int16_t)floorf(strengthThreshold);
+    memset(pDst, 0, (size_t)W * H);
+    for (int y = 3; y < (int)H - 3; y++)
+        for (int x = 3; x < (int)W - 3; x++)
+            pDst[(size_t)y * W + x] = (uint8_t)fast_strength(pSrc + (size_t)y * srcStride + x, (int)srcStride, t);
+    return 0;
+}
+
+/* :599 HafCpu_FastCorners_XY_U8_Supression: strengths of rows 3 .. H-4 and columns 3 .. W-4
+ * into a zeroed W x H map, then keep v != 0 when v >= the three neighbours above and the left
+ * one, and v > the right one and the three below; strength = v. */
+int oracle_FastCorners_XY_U8_Supression(uint32_t capacity, oracle_keypoint *corners, uint32_t *pCount, uint32_t W,
+                                        uint32_t H, const uint8_t *pSrc, uint32_t srcStride, float strengthThreshold)
+{
+    uint8_t *s = (uint8_t *)malloc((size_t)W * H);
+    if (!s) return -1;
+    oracle_FastCorners_strength(s, W, H, pSrc, srcStride, strengthThreshold);
+    uint32_t n = 0;
+    for (int y = 3; y < (int)H - 3; y++)
+        for (int x = 3; x < (int)W - 3; x++) {
+            const uint8_t *q = s + (size_t)y * W + x;
+            const uint8_t v = q[0];
+            const uint8_t *u = q - W, *d = q + W;
+            if (v && v >= u[-1] && v >= u[0] && v >= u[1] && v >= q[-1] && v > q[1] && v > d[-1] && v > d[0] && v > d[1])
+                fast_emit(corners, capacity, &n, x, y, (float)v);
+        }
+    free(s);
+    *pCount = n;
+    return 0;
+}
+
 /* ago_haf_cpu_harris.cpp:882 HafCpu_NonMaxSupp_XY_ANY_3x3: keep v if >= the three pixels
  * above and the left one, > the right one and the three below; raster-order list. */
 int oracle_NonMaxSupp_XY_ANY_3x3(uint32_t capacity, oracle_xys *list, uint32_t *pCount, uint32_t W, uint32_t H,

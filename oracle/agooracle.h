@@ -79,6 +79,16 @@ int oracle_HarrisScore_HVC_HG3_NxN(uint32_t dstWidth, uint32_t dstHeight, float 
                                    float normFactor, uint32_t bs);
 /* the score normalisation of the AGO wrappers (ago_kernel_api.cpp:16941, :17012, :17083) */
 float oracle_harris_norm_factor_block(int32_t gs, int32_t bs);
+
+/* FAST-9 corners (ago_haf_cpu_fast_corners.cpp:414, :599) on an AGO-laid-out U8 buffer:
+ * raster-ordered keypoints, *pCount = all corners found (items beyond capacity dropped). */
+int oracle_FastCorners_XY_U8_NoSupression(uint32_t capacity, oracle_keypoint *corners, uint32_t *pCount, uint32_t W,
+                                          uint32_t H, const uint8_t *pSrc, uint32_t srcStride, float strengthThreshold);
+int oracle_FastCorners_XY_U8_Supression(uint32_t capacity, oracle_keypoint *corners, uint32_t *pCount, uint32_t W,
+                                        uint32_t H, const uint8_t *pSrc, uint32_t srcStride, float strengthThreshold);
+/* per-pixel FAST strength of the suppression variant (0 where no corner), W x H bytes */
+int oracle_FastCorners_strength(uint8_t *pDst, uint32_t W, uint32_t H, const uint8_t *pSrc, uint32_t srcStride,
+                                float strengthThreshold);
 int oracle_NonMaxSupp_XY_ANY_3x3(uint32_t capacity, oracle_xys *list, uint32_t *pCount, uint32_t srcWidth,
                                  uint32_t srcHeight, const float *pSrc, uint32_t srcStride);
 int oracle_HarrisMergeSortAndPick_XY_XYS(uint32_t capacity, oracle_keypoint *corners, uint32_t *pCount,
