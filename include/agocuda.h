@@ -371,10 +371,13 @@ int agocuda_fused_GaussSobelMagDepthThresh_persistent(void *stream, const agocud
                                                       uint32_t warpsPerBlock, uint32_t blocksPerSM, int32_t shift,
                                                       int32_t threshold);
 
-/* vxCannyEdgeDetectorNode (gradient 3, L1 norm) as one front-end kernel (gradient,
- * suppression, thresholds and label initialisation from one read of the image) plus the
- * union-find hysteresis; the 0/255 edge map is bit-identical to the unfused graph inside
- * its valid region.  Scratch: agocuda_fused_CannyEdgeDetector_scratch_size(W, H) bytes. */
+/* vxCannyEdgeDetectorNode (gradient 3, L1 norm) in four kernels: a front end per 64x32 tile
+ * (gradient, suppression, thresholds and connected components of the edge candidates in
+ * shared memory, from one read of the image) that writes the final bytes of every component
+ * it sees whole or holding a strong pixel, then unions of the components that cross tile
+ * borders, their strong bits, and a pass that sets the remaining runs of strong components;
+ * the 0/255 edge map is bit-identical to the unfused graph inside its valid region.
+ * Scratch: agocuda_fused_CannyEdgeDetector_scratch_size(W, H) bytes. */
 size_t agocuda_fused_CannyEdgeDetector_scratch_size(uint32_t width, uint32_t height);
 int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t width, uint32_t height,
                                            uint8_t *pDst, uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride,

@@ -982,7 +982,7 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
                     return agocuda_fused_CannyEdgeDetector_3x3_L1(S(q), w, h, dst, ds, src, ss, lo, hi, scr, sb, status);
                 });
                 st.parts.push_back(Part{fns.back(), c.nodes});
-                st.num_kernels += 5;
+                st.num_kernels += 4;
             } else {
                 LNode *sc = c.nodes[1], *pk = c.nodes[3];
                 const float k = sc_f32(sc->p[2]), tc = sc_f32(sc->p[3]), norm = harris_norm(sc_i32(sc->p[4]));

@@ -380,16 +380,48 @@ __global__ void k_hyst_output(int W, int H, uint8_t *out, int outStride, const i
 // Fused Canny: gradient, suppression and double threshold for a 64x32 tile from one read
 // of the image, then hysteresis as block-based connected components.  The tile's
 // non-zero pixels are labelled in shared memory (lock-free union-find over the W, NW, N
-// and NE neighbours, i.e. 8-connectivity), so only pixels on tile borders reach the global
-// union-find.  Global node ("slot") of a tile pixel: tile * kTS + local index; a
-// component's final root is its smallest local-root slot.  The result is the same set of
-// 255 pixels as the per-pixel union-find above: 8-connected components of the interior
-// non-zero pixels that hold a strong (255) pixel.
+// and NE neighbours, i.e. 8-connectivity).  A component with no pixel on the tile's border
+// ring is final in the tile, and so is one holding a strong pixel: the front writes their
+// bytes.  The other components ("open": at most 94 per tile) get a slot and a node of a
+// compact global union-find (tile * kOpenMax + slot); the ring pixels' slots go to global
+// memory for the unions across tile borders, and the runs of open components without a
+// strong pixel go to a per-tile list that the last pass sets to 255 where the merged
+// component turned out strong.  The result is the same set of 255 pixels as the per-pixel
+// union-find above: 8-connected components of the interior non-zero pixels that hold a
+// strong (255) pixel.
 // ---------------------------------------------------------------------------------
 constexpr int kTW = 64, kTH = 32, kTS = kTW * kTH;   // tile and its slot count
 constexpr int kIH = kTH + 4;                         // input tile rows (halo 2)
 constexpr int kGH = kTH + 2;                         // gradient tile rows (halo 1)
-constexpr uint16_t kNoLabel = 0xFFFF;
+// open components per tile (those touching its 188-pixel border ring: at most 94), runs per
+// tile (at most 32 per 64-pixel row), ring pixels per tile
+constexpr int kOpenMax = 128, kRunMax = kTS / 2, kBorder = 2 * kTW + 2 * kTH;
+
+// per-tile hysteresis state in global memory: ring labels (open slot or -1; top row, bottom
+// row, left column, right column), the union-find over open slots (node = tile * kOpenMax +
+// slot), strong bits per node, open-slot counts, and the runs left for the patch pass
+struct CannyTiles {
+    int16_t *blab;
+    int *uf;
+    uint32_t *sbits, *nOpen, *runCount, *runs;
+    int tilesX, tilesY;
+};
+
+// global node of the open component at pixel (x, y), which lies on its tile's border ring;
+// -1 where that pixel is not an edge candidate
+__device__ __forceinline__ int ring_node(const CannyTiles &T, int x, int y)
+{
+    const int tx = x / kTW, ty = y / kTH, lx = x - tx * kTW, ly = y - ty * kTH;
+    const int tile = ty * T.tilesX + tx;
+    int idx;
+    if (ly == 0) idx = lx;
+    else if (ly == kTH - 1) idx = kTW + lx;
+    else if (lx == 0) idx = 2 * kTW + ly;
+    else if (lx == kTW - 1) idx = 2 * kTW + kTH + ly;
+    else return -1;
+    const int s = __ldg(T.blab + (size_t)tile * kBorder + idx);
+    return s < 0 ? -1 : tile * kOpenMax + s;
+}
 
 __device__ __forceinline__ int sfind(const int *lab, int x)
 {
@@ -440,17 +472,17 @@ __device__ __forceinline__ uint32_t canny_pack_biased(uint32_t bx, uint32_t by)
 
 __device__ __forceinline__ int sG_mag3(uint32_t g) { return (int)(g | 3u); }   // (mag << 2) | 3: compares as mag
 
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 5)
 k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, int lower, int upper,
-                  uint16_t *__restrict__ lab16, int labPitch, int *__restrict__ uf, uint32_t *__restrict__ bits,
-                  uint32_t *__restrict__ roots)
+                  uint8_t *__restrict__ dst, int dstStride, CannyTiles T, uint32_t *__restrict__ err)
 {
     __shared__ __align__(16) uint32_t sIn[kIH][kInWords];
     __shared__ __align__(16) uint16_t sG[kGH][kGC];
     __shared__ __align__(16) int sLab[kTS];
     __shared__ unsigned long long sNZ[kTH], sST[kTH];   // per tile row: non-zero / strong pixels
     __shared__ int16_t sV[kIH];                          // per gradient row: vertical sum of column W-1
-    __shared__ uint32_t sStrongRoot[kTS / 32], sRoot[kTS / 32];
+    __shared__ uint32_t sStrongRoot[kTS / 32], sOpen[kTS / 32], sOpenPre[kTS / 32], sOpenStrong[kOpenMax / 32];
+    __shared__ int sRunN;
     const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH, tid = threadIdx.x;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x;
 
@@ -473,7 +505,9 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
         }
         sIn[r][q] = w;
     }
-    if (tid < kTS / 32) { sStrongRoot[tid] = 0; sRoot[tid] = 0; }
+    if (tid < kTS / 32) { sStrongRoot[tid] = 0; sOpen[tid] = 0; }
+    if (tid < kOpenMax / 32) sOpenStrong[tid] = 0;
+    if (tid == 0) sRunN = 0;
     const bool needV = x0 == 0 && (W & 15) == 0 && W >= 16;
     if (needV && tid < kGH) {
         const int y = y0 - 1 + tid;
@@ -623,122 +657,189 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
             }
         }
     }
-    if (y < H && x0 + c0 < W) {
-        uint32_t w[4];
+    // components with a pixel on the tile's border ring are open: they may continue in a
+    // neighbouring tile, so they go to the global union-find; the others are final here
+    if (r == 0 || r == kTH - 1) {
+        int last = -1;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const uint32_t lo = root[2 * j] >= 0 ? (uint32_t)root[2 * j] : kNoLabel;
-            const uint32_t hi = root[2 * j + 1] >= 0 ? (uint32_t)root[2 * j + 1] : kNoLabel;
-            w[j] = lo | (hi << 16);
-        }
-        *(uint4 *)&lab16[(size_t)y * labPitch + x0 + c0] = make_uint4(w[0], w[1], w[2], w[3]);
+        for (int j = 0; j < 8; j++)
+            if (root[j] >= 0 && root[j] != last) {
+                last = root[j];
+                atomicOr(&sOpen[last >> 5], 1u << (last & 31));
+            }
+    } else {
+        if (sgm == 0 && root[0] >= 0) atomicOr(&sOpen[root[0] >> 5], 1u << (root[0] & 31));
+        if (sgm == 7 && root[7] >= 0) atomicOr(&sOpen[root[7] >> 5], 1u << (root[7] & 31));
     }
-    uint32_t own = 0;                      // local roots among this thread's 8 pixels
-#pragma unroll
-    for (int j = 0; j < 8; j++)
-        if (root[j] == i0 + j) { uf[(size_t)tile * kTS + i0 + j] = tile * kTS + i0 + j; own |= 1u << j; }
-    if (own) atomicOr(&sRoot[i0 >> 5], own << (i0 & 31));
     __syncthreads();
-    if (tid < kTS / 32) {
-        bits[(size_t)tile * (kTS / 32) + tid] = sStrongRoot[tid];
-        roots[(size_t)tile * (kTS / 32) + tid] = sRoot[tid];
+    if (tid < 32) {                       // open slots: exclusive prefix of the 64 words' counts
+        const uint32_t n0 = __popc(sOpen[2 * tid]), n1 = __popc(sOpen[2 * tid + 1]);
+        uint32_t inc = n0 + n1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (tid >= o) inc += v;
+        }
+        sOpenPre[2 * tid] = inc - n0 - n1;
+        sOpenPre[2 * tid + 1] = inc - n1;
+        if (tid == 31) {
+            T.nOpen[tile] = min(inc, (uint32_t)kOpenMax);
+            if (inc > (uint32_t)kOpenMax) atomicOr(err, 1u);   // not reachable: a ring holds <= 94 components
+        }
     }
-}
+    __syncthreads();
+    auto oslot = [&](int rt) {
+        const int w = rt >> 5;
+        return (int)(sOpenPre[w] + __popc(sOpen[w] & ((1u << (rt & 31)) - 1u)));
+    };
+    auto ring_label = [&](int rt) -> int16_t {
+        if (rt < 0) return -1;
+        const int o = oslot(rt);
+        return o < kOpenMax ? (int16_t)o : (int16_t)-1;
+    };
+    auto is_strong = [&](int rt) { return (sStrongRoot[rt >> 5] >> (rt & 31)) & 1; };
 
-__device__ __forceinline__ int slot_of(const uint16_t *lab16, int labPitch, int tilesX, int x, int y)
-{
-    const uint16_t l = lab16[(size_t)y * labPitch + x];
-    if (l == kNoLabel) return -1;
-    return ((y / kTH) * tilesX + x / kTW) * kTS + l;
+    // edge bytes: 255 for the pixels of components holding a strong pixel of this tile (such a
+    // component is strong whatever it joins), else 0; open components without one are
+    // patched after the global resolve
+    if (y < H && x0 + c0 < W) {
+        uint32_t lo = 0, hi = 0;
+        int last = -1;
+        uint32_t lastV = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (root[j] < 0) continue;
+            if (root[j] != last) { last = root[j]; lastV = is_strong(last) ? 0xFFu : 0u; }
+            if (j < 4) lo |= lastV << (8 * j);
+            else hi |= lastV << (8 * (j - 4));
+        }
+        uint8_t *o = dst + (size_t)y * dstStride + x0 + c0;
+        const int n = min(8, W - (x0 + c0));
+        if (n == 8 && ((uintptr_t)o & 7) == 0) {
+            *(uint2 *)o = make_uint2(lo, hi);
+        } else {
+            for (int j = 0; j < n; j++) o[j] = (uint8_t)((j < 4 ? lo >> (8 * j) : hi >> (8 * (j - 4))) & 0xFF);
+        }
+    }
+    // labels of the ring pixels (open slot or -1): top row, bottom row, left column, right column
+    {
+        int16_t *bl = T.blab + (size_t)tile * kBorder;
+        if (r == 0 || r == kTH - 1) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) bl[(r == 0 ? 0 : kTW) + c0 + j] = ring_label(root[j]);
+        }
+        if (sgm == 0) bl[2 * kTW + r] = ring_label(root[0]);
+        if (sgm == 7) bl[2 * kTW + kTH + r] = ring_label(root[7]);
+    }
+    // runs of open components that hold no strong pixel here: (row, column, length, slot),
+    // appended with one shared-memory atomic per warp
+    {
+        uint32_t pend = 0;
+        uint32_t sb = (uint32_t)((m & ~(m << 1)) >> c0) & 0xff;
+        while (sb) {
+            const int j = __ffs(sb) - 1;
+            sb &= sb - 1;
+            const int rt = sLab[i0 + j];          // a run start holds its root
+            if (((sOpen[rt >> 5] >> (rt & 31)) & 1) && !is_strong(rt) && oslot(rt) < kOpenMax) pend |= 1u << j;
+        }
+        const int lane = tid & 31, cnt = __popc(pend);
+        int inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        int base = 0;
+        if (lane == 31 && inc) base = atomicAdd(&sRunN, inc);
+        base = __shfl_sync(0xffffffffu, base, 31) + inc - cnt;
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const int rt = sLab[i0 + j], c = c0 + j;
+            const unsigned long long rest = ~(m >> c);
+            const int len = rest ? __ffsll((long long)rest) - 1 : kTW - c;
+            const uint32_t e = (uint32_t)r | ((uint32_t)c << 5) | ((uint32_t)(len - 1) << 11) | ((uint32_t)oslot(rt) << 17);
+            if (base < kRunMax) T.runs[(size_t)tile * kRunMax + base] = e;
+            base++;
+        }
+    }
+    // union-find nodes of the open slots, and which of them hold a strong pixel
+    if (tid < kTS / 32) {
+        uint32_t ow = sOpen[tid];
+        const uint32_t sw = sStrongRoot[tid];
+        int o = (int)sOpenPre[tid];
+        while (ow) {
+            const int b = __ffs(ow) - 1;
+            ow &= ow - 1;
+            if (o < kOpenMax) {
+                T.uf[(size_t)tile * kOpenMax + o] = tile * kOpenMax + o;
+                if ((sw >> b) & 1) atomicOr(&sOpenStrong[o >> 5], 1u << (o & 31));
+            }
+            o++;
+        }
+    }
+    __syncthreads();
+    if (tid < kOpenMax / 32) T.sbits[(size_t)tile * (kOpenMax / 32) + tid] = sOpenStrong[tid];
+    if (tid == 0) T.runCount[tile] = (uint32_t)min(sRunN, kRunMax);
 }
 
 // unions across tile borders: the W / NW / N / NE neighbours of a tile's left column, top
-// row and right column that lie in another tile
-__global__ void k_canny_ccl_border(int W, int H, const uint16_t *__restrict__ lab16, int labPitch, int tilesX,
-                                   int *uf, uint32_t *err)
+// row and right column that lie in another tile (both ends are ring pixels of their tiles)
+__global__ void k_canny_ccl_border(int W, int H, CannyTiles T, uint32_t *err)
 {
     constexpr int kPer = kTH + kTW + kTH;
     const int tile = blockIdx.y, b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= kPer) return;
-    const int x0 = (tile % tilesX) * kTW, y0 = (tile / tilesX) * kTH;
+    const int x0 = (tile % T.tilesX) * kTW, y0 = (tile / T.tilesX) * kTH;
     int x, y;
     if (b < kTH) { x = x0; y = y0 + b; }
     else if (b < kTH + kTW) { x = x0 + b - kTH; y = y0; }
     else { x = x0 + kTW - 1; y = y0 + b - kTH - kTW; }
     if (x >= W || y >= H) return;
-    const int sp = slot_of(lab16, labPitch, tilesX, x, y);
+    const int sp = ring_node(T, x, y);
     if (sp < 0) return;
     const int dx[4] = {-1, -1, 0, 1}, dy[4] = {0, -1, -1, -1};
     for (int k = 0; k < 4; k++) {
         const int nx = x + dx[k], ny = y + dy[k];
         if (nx < 0 || ny < 0 || nx >= W) continue;
         if (nx >= x0 && nx < x0 + kTW && ny >= y0) continue;     // same tile: done locally
-        const int sq = slot_of(lab16, labPitch, tilesX, nx, ny);
-        if (sq >= 0) uf_union(uf, sp, sq, err);
+        const int sq = ring_node(T, nx, ny);
+        if (sq >= 0) uf_union(T.uf, sp, sq, err);
     }
 }
 
-// strong bits from local roots to the roots of their merged components
-__global__ void k_canny_ccl_mark(const int *uf, uint32_t *bits, uint32_t words)
+// after the unions: every open node points straight at its component's root (path
+// compression; concurrent readers see the old parent or the root, both lead to the root),
+// and a node holding a strong pixel sets its root's strong bit.  One thread per node.
+__global__ void k_canny_ccl_flatten(CannyTiles T, int nodes)
 {
-    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
-        uint32_t m = bits[w];
-        while (m) {
-            const int s = (int)(w * 32 + __ffs(m) - 1);
-            m &= m - 1;
-            const int r = uf_find_ro(uf, s);
-            if (r != s) atomicOr(bits + (r >> 5), 1u << (r & 31));
-        }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    const int tile = i / kOpenMax, o = i - tile * kOpenMax;
+    if (o >= (int)__ldg(T.nOpen + tile)) return;
+    const int rt = uf_find(T.uf, i);
+    if (rt != i) {
+        T.uf[i] = rt;
+        if ((__ldcg(T.sbits + (i >> 5)) >> (i & 31)) & 1) atomicOr(T.sbits + (rt >> 5), 1u << (rt & 31));
     }
 }
 
-// every local root: the strong bit of its component's final root, kept in the root bitmap
-// (each word is rewritten by the one thread that reads it)
-__global__ void k_canny_ccl_resolve(const int *uf, const uint32_t *bits, uint32_t *roots, uint32_t words)
+// the runs of open components without a strong pixel in their tile: 255 where the merged
+// component is strong (the front wrote 0); a warp per tile
+__global__ void __launch_bounds__(256) k_canny_ccl_patch(int tiles, CannyTiles T, uint8_t *__restrict__ dst, int dstStride)
 {
-    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
-        uint32_t m = roots[w], strong = 0;
-        while (m) {
-            const int b = __ffs(m) - 1;
-            m &= m - 1;
-            const int r = uf_find_ro(uf, (int)(w * 32 + b));
-            if ((__ldg(bits + (r >> 5)) >> (r & 31)) & 1) strong |= 1u << b;
+    const int tile = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (tile >= tiles) return;
+    const int n = (int)T.runCount[tile];
+    const int x0 = (tile % T.tilesX) * kTW, y0 = (tile / T.tilesX) * kTH;
+    for (int k = lane; k < n; k += 32) {
+        const uint32_t e = T.runs[(size_t)tile * kRunMax + k];
+        const int r = (int)(e & 31), c = (int)((e >> 5) & 63), len = (int)((e >> 11) & 63) + 1, s = (int)(e >> 17);
+        const int g = __ldg(T.uf + tile * kOpenMax + s);          // flattened: the component's root
+        if ((__ldg(T.sbits + (g >> 5)) >> (g & 31)) & 1) {
+            uint8_t *o = dst + (size_t)(y0 + r) * dstStride + x0 + c;
+            for (int q = 0; q < len; q++) o[q] = 255;
         }
-        roots[w] = strong;
-    }
-}
-
-// 8 pixels per thread: local label -> its local root's resolved strong bit -> 0/255
-__global__ void k_canny_ccl_output(int W, int H, const uint16_t *__restrict__ lab16, int labPitch, int tilesX,
-                                   const uint32_t *__restrict__ strongRoots, uint8_t *__restrict__ out, int outStride)
-{
-    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * 8, y = blockIdx.y;
-    if (x >= W) return;
-    const uint16_t *lr = lab16 + (size_t)y * labPitch;
-    uint8_t v[8];
-    const int tileBase = ((y / kTH) * tilesX + x / kTW) * kTS;   // 8 pixels never straddle a tile (kTW % 8 == 0)
-    int lastSlot = -1, lastVal = 0;                               // neighbours usually share a component
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        v[k] = 0;
-        if (x + k >= W) continue;
-        const uint16_t l = lr[x + k];
-        if (l == kNoLabel) continue;
-        const int slot = tileBase + l;
-        if (slot != lastSlot) {
-            lastSlot = slot;
-            lastVal = (__ldg(strongRoots + (slot >> 5)) >> (slot & 31)) & 1 ? 255 : 0;
-        }
-        v[k] = (uint8_t)lastVal;
-    }
-    uint8_t *o = out + (size_t)y * outStride + x;
-    if (x + 8 <= W && ((uintptr_t)o & 7) == 0) {
-        uint2 w;
-        w.x = v[0] | (v[1] << 8) | (v[2] << 16) | ((uint32_t)v[3] << 24);
-        w.y = v[4] | (v[5] << 8) | (v[6] << 16) | ((uint32_t)v[7] << 24);
-        *(uint2 *)o = w;
-    } else {
-        for (int k = 0; k < 8 && x + k < W; k++) o[k] = v[k];
     }
 }
 
@@ -1575,29 +1676,29 @@ extern "C" int agocuda_CannyEdgeTrace_U8_U8XY_noalloc(void *stream, uint32_t W, 
 
 extern "C" size_t agocuda_CannyEdgeTrace_noalloc_max_pixels(void) { return kNoAllocMaxPixels; }
 
-// scratch of the fused Canny: tile-local labels (u16, pitched), the global union-find over
-// tile slots (int per slot) and the strong-root bitmap (one bit per slot)
-struct CannyScratch { uint16_t *lab; int labPitch; int *uf; uint32_t *bits, *roots; size_t bytes; int tilesX, tilesY; };
-
-static CannyScratch canny_scratch_layout(uint32_t W, uint32_t H, void *base)
+// scratch of the fused Canny: the per-tile state of CannyTiles, each array 256-byte aligned
+static size_t canny_tiles_layout(uint32_t W, uint32_t H, void *base, CannyTiles *T)
 {
-    CannyScratch c{};
+    CannyTiles c{};
     c.tilesX = (int)div_up(W, kTW);
     c.tilesY = (int)div_up(H, kTH);
-    const size_t slots = (size_t)c.tilesX * c.tilesY * kTS;
-    c.labPitch = (int)((W + 7) & ~7u);                       // elements (16-byte rows)
-    const size_t labBytes = ((size_t)c.labPitch * H * 2 + 255) & ~(size_t)255;
-    const size_t ufBytes = (slots * 4 + 255) & ~(size_t)255;
-    const size_t bitBytes = ((slots / 8) + 255) & ~(size_t)255;
-    c.bytes = labBytes + ufBytes + 2 * bitBytes;
-    if (base) {
+    const size_t tiles = (size_t)c.tilesX * c.tilesY;
+    auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t sizes[6] = {al(tiles * kBorder * 2), al(tiles * kOpenMax * 4), al(tiles * (kOpenMax / 8)),
+                             al(tiles * 4), al(tiles * 4), al(tiles * kRunMax * 4)};
+    size_t off[6], o = 0;
+    for (int i = 0; i < 6; i++) { off[i] = o; o += sizes[i]; }
+    if (base && T) {
         uint8_t *p = (uint8_t *)base;
-        c.lab = (uint16_t *)p;
-        c.uf = (int *)(p + labBytes);
-        c.bits = (uint32_t *)(p + labBytes + ufBytes);
-        c.roots = (uint32_t *)(p + labBytes + ufBytes + bitBytes);
+        c.blab = (int16_t *)(p + off[0]);
+        c.uf = (int *)(p + off[1]);
+        c.sbits = (uint32_t *)(p + off[2]);
+        c.nOpen = (uint32_t *)(p + off[3]);
+        c.runCount = (uint32_t *)(p + off[4]);
+        c.runs = (uint32_t *)(p + off[5]);
+        *T = c;
     }
-    return c;
+    return o;
 }
 
 extern "C" int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t W, uint32_t H, uint8_t *pDst, uint32_t dstStride,
@@ -1607,26 +1708,23 @@ extern "C" int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t W, 
     if (!pDst || !pSrc || !scratch || !pStatus || W < 3 || H < 3 || dstStride < W || srcStride < W || W > 65535 ||
         H > 65535 || !aligned(scratch, 256))
         return AGOCUDA_INVALID_PARAMS;
-    const CannyScratch c = canny_scratch_layout(W, H, scratch);
-    if (scratchBytes < c.bytes || (size_t)c.tilesX * c.tilesY * kTS >= (1ull << 31)) return AGOCUDA_INVALID_PARAMS;
+    CannyTiles T{};
+    if (scratchBytes < canny_tiles_layout(W, H, scratch, &T)) return AGOCUDA_INVALID_PARAMS;
     cudaStream_t s = as_stream(stream);
-    const int tiles = c.tilesX * c.tilesY;
-    k_canny_ccl_front<<<dim3(c.tilesX, c.tilesY), 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper,
-                                                               c.lab, c.labPitch, c.uf, c.bits, c.roots);
+    const int tiles = T.tilesX * T.tilesY, nodes = tiles * kOpenMax;
+    k_canny_ccl_front<<<dim3(T.tilesX, T.tilesY), 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper,
+                                                               pDst, (int)dstStride, T, pStatus);
     constexpr int kPer = kTH + kTW + kTH;
-    k_canny_ccl_border<<<dim3(div_up(kPer, 128), tiles), 128, 0, s>>>((int)W, (int)H, c.lab, c.labPitch, c.tilesX, c.uf, pStatus);
-    const uint32_t words = (uint32_t)tiles * (kTS / 32);
-    k_canny_ccl_mark<<<div_up(words, 256), 256, 0, s>>>(c.uf, c.bits, words);
-    k_canny_ccl_resolve<<<div_up(words, 256), 256, 0, s>>>(c.uf, c.bits, c.roots, words);
-    k_canny_ccl_output<<<dim3(div_up(div_up(W, 8), 128), H), 128, 0, s>>>((int)W, (int)H, c.lab, c.labPitch, c.tilesX,
-                                                                          c.roots, pDst, (int)dstStride);
-    agocuda_count_launch(5);
+    k_canny_ccl_border<<<dim3(div_up(kPer, 128), tiles), 128, 0, s>>>((int)W, (int)H, T, pStatus);
+    k_canny_ccl_flatten<<<div_up(nodes, 256), 256, 0, s>>>(T, nodes);
+    k_canny_ccl_patch<<<div_up(tiles, 8), 256, 0, s>>>(tiles, T, pDst, (int)dstStride);
+    agocuda_count_launch(4);
     return agocuda_launch_status();
 }
 
 extern "C" size_t agocuda_fused_CannyEdgeDetector_scratch_size(uint32_t W, uint32_t H)
 {
-    return canny_scratch_layout(W, H, nullptr).bytes + 256;   // + room to align an arbitrary base to 256
+    return canny_tiles_layout(W, H, nullptr, nullptr) + 256;   // + room to align an arbitrary base to 256
 }
 
 extern "C" int agocuda_HarrisSobel_HG3_U8_3x3(void *stream, uint32_t W, uint32_t H, float *pDst, uint32_t dstStride,

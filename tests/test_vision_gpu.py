@@ -120,6 +120,32 @@ def test_fused_canny(lib, cuda, W, H):
     assert int(status[0].item()) == 0
 
 
+@pytest.mark.parametrize("W,H,lo,hi", [(3, 3, 20, 40), (65, 33, 20, 40), (130, 70, 40, 200), (333, 97, 10, 30),
+                                       (1023, 517, 60, 120), (3840, 2160, 30, 90)])
+@pytest.mark.parametrize("dst_off", [0, 1])
+def test_fused_canny_dense(lib, cuda, W, H, lo, hi, dst_off):
+    """Noise with low thresholds: components of every shape cross tile borders, open runs
+    without strong pixels wait for the patch pass, tiles hang over the right and bottom
+    image edges; an output plane starting off an 8-byte boundary takes the byte stores."""
+    D = _dev()
+    img = np.random.default_rng(W * H + lo).integers(0, 256, (H, W), dtype=np.int32).astype(np.uint8)
+    ref_edges = OC.canny_parts(img, lo, hi)[3]
+    src = D.DevImg(H, W).upload(img)
+    out = D.DevImg(H, W, align_off=dst_off)
+    sb = lib.agocuda_fused_CannyEdgeDetector_scratch_size(W, H)
+    scr, status = _buf(sb), _buf(4)
+    base = scr.data_ptr() + (-scr.data_ptr() % 256)
+    for _ in range(2):
+        assert lib.agocuda_fused_CannyEdgeDetector_3x3_L1(D.stream_ptr(), W, H, out.ptr, out.stride, src.ptr, src.stride,
+                                                          lo, hi, base, sb - 256, status.data_ptr()) == 0
+        edges = out.download()
+        np.testing.assert_array_equal(edges[1:H - 1, 1:W - 1], ref_edges[1:H - 1, 1:W - 1])
+        assert not edges[0].any() and not edges[H - 1].any() and not edges[:, 0].any() and not edges[:, W - 1].any()
+    assert int(status[0].item()) == 0
+    if W > 100:
+        assert (ref_edges == 255).mean() > 0.01
+
+
 @pytest.mark.parametrize("W,H", [(64, 48), (36, 19), (200, 120), (1920, 1080)])
 def test_harris_kernels(lib, cuda, W, H):
     import torch
