@@ -213,7 +213,9 @@ enum { VX_GRAPH_ATTRIBUTE_AMD_AFFINITY = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GR
        VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_PROFILE = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_GRAPH) + 0x07 };
 enum { VX_NODE_ATTRIBUTE_AMD_AFFINITY = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_NODE) + 0x01,
        VX_NODE_ATTRIBUTE_AMD_HIP_STREAM = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_NODE) + 0x03 };
-enum { VX_IMAGE_ATTRIBUTE_AMD_HIP_BUFFER = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_IMAGE) + 0x06 };
+enum { VX_IMAGE_ATTRIBUTE_AMD_GPU_BUFFER_OFFSET = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_IMAGE) + 0x02,
+       VX_IMAGE_ATTRIBUTE_AMD_GPU_BUFFER_STRIDE = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_IMAGE) + 0x04,
+       VX_IMAGE_ATTRIBUTE_AMD_HIP_BUFFER = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_IMAGE) + 0x06 };
 enum { VX_DIRECTIVE_AMD_READ_ONLY = VX_ENUM_BASE(VX_ID_AMD, VX_ENUM_DIRECTIVE) + 0x01,
        VX_DIRECTIVE_AMD_COPY_TO_HIPMEM = VX_ENUM_BASE(VX_ID_AMD, VX_ENUM_DIRECTIVE) + 0x02,
        VX_DIRECTIVE_AMD_ENABLE_PROFILE_CAPTURE = VX_ENUM_BASE(VX_ID_AMD, VX_ENUM_DIRECTIVE) + 0x03,
@@ -425,6 +427,28 @@ vx_parameter vxGetKernelParameterByIndex(vx_kernel kernel, vx_uint32 index);
 vx_status vxSetParameterByReference(vx_parameter parameter, vx_reference value);
 vx_status vxQueryParameter(vx_parameter parameter, vx_enum attribute, void *ptr, vx_size size);
 vx_status vxReleaseParameter(vx_parameter *param);
+
+/* ---------------- user kernels (vx_api.h group_user_kernels; vx_ext_amd.h) ---------------- */
+typedef struct _vx_meta_format *vx_meta_format;
+typedef vx_status (*vx_kernel_f)(vx_node node, const vx_reference *parameters, vx_uint32 num);
+typedef vx_status (*vx_kernel_initialize_f)(vx_node node, const vx_reference *parameters, vx_uint32 num);
+typedef vx_status (*vx_kernel_deinitialize_f)(vx_node node, const vx_reference *parameters, vx_uint32 num);
+typedef vx_status (*vx_kernel_validate_f)(vx_node node, const vx_reference parameters[], vx_uint32 num, vx_meta_format metas[]);
+typedef vx_status (*vx_kernel_image_valid_rectangle_f)(vx_node node, vx_uint32 index, const vx_rectangle_t *const input_valid[],
+                                                       vx_rectangle_t *const output_valid[]);
+typedef vx_status (*vx_publish_kernels_f)(vx_context context);
+enum { VX_VALID_RECT_CALLBACK = VX__A(VX_TYPE_META_FORMAT, 1) };
+enum { VX_KERNEL_ATTRIBUTE_AMD_GPU_BUFFER_ACCESS_ENABLE = VX_ATTRIBUTE_BASE(VX_ID_AMD, VX_TYPE_KERNEL) + 0x05 };
+vx_kernel vxAddUserKernel(vx_context context, const vx_char name[VX_MAX_KERNEL_NAME], vx_enum enumeration,
+                          vx_kernel_f func_ptr, vx_uint32 numParams, vx_kernel_validate_f validate,
+                          vx_kernel_initialize_f init, vx_kernel_deinitialize_f deinit);
+vx_status vxAddParameterToKernel(vx_kernel kernel, vx_uint32 index, vx_enum dir, vx_enum data_type, vx_enum state);
+vx_status vxFinalizeKernel(vx_kernel kernel);
+vx_status vxRemoveKernel(vx_kernel kernel);
+vx_status vxSetKernelAttribute(vx_kernel kernel, vx_enum attribute, const void *ptr, vx_size size);
+vx_status vxSetMetaFormatAttribute(vx_meta_format meta, vx_enum attribute, const void *ptr, vx_size size);
+vx_status vxQueryMetaFormatAttribute(vx_meta_format meta, vx_enum attribute, void *ptr, vx_size size);
+vx_status vxSetMetaFormatFromReference(vx_meta_format meta, vx_reference exemplar);
 
 /* ---------------- image views, convolutions, legacy access (vx_api.h, vx_compatibility.h, vx_ext_amd.h) ---------------- */
 enum { VX_CONVOLUTION_ROWS = VX__A(VX_TYPE_CONVOLUTION, 0), VX_CONVOLUTION_COLUMNS = VX__A(VX_TYPE_CONVOLUTION, 1),

@@ -46,6 +46,7 @@ static const char *kLKNames[] = {
     "Convolve_U8_U8", "Convolve_S16_U8",
     "HarrisSobel_HG3_U8_5x5", "HarrisSobel_HG3_U8_7x7", "HarrisScore_HVC_HG3_5x5", "HarrisScore_HVC_HG3_7x7",
     "FastCorners_XY_U8_Supression", "FastCorners_XY_U8_NoSupression",
+    "UserKernel",
 };
 static_assert(sizeof(kLKNames) / sizeof(kLKNames[0]) == (size_t)LK::COUNT, "kernel name table");
 
@@ -88,10 +89,62 @@ static bool fmt_is(Ref *r, vx_df_image f) { return r && r->type == VX_TYPE_IMAGE
 
 vx_status check_node_params(Node *n);   // vx_kernels.cpp: required parameters present, types as declared
 
+// A user kernel's node: its validator describes each output in a vx_meta_format (types as
+// declared by default); virtual outputs take the described format and size, others must match
+// (ago_interface.cpp:1275-1380).
+static vx_status validate_user_node(Node *n)
+{
+    Kernel *k = n->ukernel;
+    const size_t np = n->params.size();
+    std::vector<MetaFormat> metas(np);
+    std::vector<vx_meta_format> mp(np);
+    for (size_t i = 0; i < np; i++) {
+        if (k->uparams[i].dir == VX_OUTPUT && k->uparams[i].type != VX_TYPE_REFERENCE) metas[i].type = k->uparams[i].type;
+        mp[i] = reinterpret_cast<vx_meta_format>(&metas[i]);
+    }
+    const vx_status s = k->validate((vx_node)n, (const vx_reference *)n->params.data(), (vx_uint32)np, mp.data());
+    if (s) {
+        log_error(n, s, "ERROR: vxVerifyGraph: kernel %s: kernel_validate failed (%d)\n", k->kname.c_str(), s);
+        return s;
+    }
+    for (size_t i = 0; i < np; i++) {
+        Ref *r = n->params[i];
+        if (!r || k->uparams[i].dir != VX_OUTPUT) continue;
+        const MetaFormat &m = metas[i];
+        if (m.type && m.type != r->type) return VX_ERROR_INVALID_TYPE;
+        if (r->type == VX_TYPE_IMAGE) {
+            Image *o = IMG(r);
+            if (o->num_planes == 0) {
+                if (!o->is_virtual) return VX_ERROR_INVALID_PARAMETERS;
+                if (!o->width) o->width = m.width;
+                if (!o->height) o->height = m.height;
+                if (o->format == VX_DF_IMAGE_VIRT) o->format = m.format;
+                image_init_planes(o);
+                if (!o->num_planes) return VX_ERROR_INVALID_FORMAT;
+            }
+            if (m.format && o->format != m.format) return VX_ERROR_INVALID_FORMAT;
+            if ((m.width && o->width != m.width) || (m.height && o->height != m.height)) return VX_ERROR_INVALID_DIMENSION;
+        } else if (r->type == VX_TYPE_ARRAY) {
+            Array *a = static_cast<Array *>(r);
+            if (a->item_type == VX_TYPE_INVALID && a->is_virtual && m.item_type) {
+                a->item_type = m.item_type;
+                a->item_size = type_size(m.item_type);
+            }
+            if (m.item_type && a->item_type != m.item_type) return VX_ERROR_INVALID_TYPE;
+            if (a->is_virtual && !a->capacity) a->capacity = m.capacity;
+            if (m.capacity && a->capacity < m.capacity) return VX_ERROR_INVALID_DIMENSION;
+        } else if (r->type == VX_TYPE_SCALAR) {
+            if (m.scalar_type && static_cast<Scalar *>(r)->data_type != m.scalar_type) return VX_ERROR_INVALID_TYPE;
+        }
+    }
+    return VX_SUCCESS;
+}
+
 vx_status validate_node(Graph *g, Node *n)
 {
     (void)g;
     if (vx_status s = check_node_params(n)) return s;
+    if (n->ukernel) return validate_user_node(n);
     for (Ref *r : n->params)
         if (r && r->type == VX_TYPE_IMAGE && IMG(r)->roi_view) {
             // the kernels address whole aligned rows of their planes; a window into another
@@ -351,6 +404,19 @@ static vx_status divide_node(Graph *g, Node *n, std::vector<LNode> &out)
         LNode ln; ln.k = k; ln.p = std::move(args); ln.origin = n; ln.border = n->border;
         out.push_back(std::move(ln));
     };
+    if (n->ukernel) {
+        // one host step; outputs first (the lowered-node convention), the callback gets the
+        // node's own parameter order.  Bidirectional parameters count as inputs here.
+        LNode ln;
+        ln.k = LK::USER_KERNEL;
+        ln.origin = n;
+        ln.border = n->border;
+        for (size_t i = 0; i < p.size(); i++) if (n->ukernel->uparams[i].dir == VX_OUTPUT) ln.p.push_back(p[i]);
+        ln.nout = (int)ln.p.size();
+        for (size_t i = 0; i < p.size(); i++) if (n->ukernel->uparams[i].dir != VX_OUTPUT) ln.p.push_back(p[i]);
+        out.push_back(std::move(ln));
+        return VX_SUCCESS;
+    }
     switch (n->kernel) {
     case VX_KERNEL_GAUSSIAN_3x3: add(LK::GAUSSIAN_U8_U8_3x3, {p[1], p[0]}); return VX_SUCCESS;   // :863
     case VX_KERNEL_SOBEL_3x3:                                                                      // :509
@@ -573,7 +639,7 @@ static bool is_canny_supp(LK k)
     return k == LK::CANNY_SUPP_THRESHOLD_U8XY_U16_3x3 || k == LK::CANNY_SUPP_THRESHOLD_U8XY_U16_7x7;
 }
 
-static int num_outputs(LK k)
+static int num_outputs_k(LK k)
 {
     switch (k) {
     case LK::SOBEL_S16S16_U8_3x3_GXY: case LK::COLOR_CONVERT_NV12_RGB: return 2;
@@ -585,7 +651,9 @@ static int num_outputs(LK k)
     }
 }
 
-bool lnode_is_output(const LNode &ln, size_t i) { return (int)i < num_outputs(ln.k); }
+static int num_outputs(const LNode &ln) { return ln.nout >= 0 ? ln.nout : num_outputs_k(ln.k); }
+
+bool lnode_is_output(const LNode &ln, size_t i) { return (int)i < num_outputs(ln); }
 
 // the root data object a reference aliases (planes alias their image, levels their pyramid)
 static Ref *root_of(Ref *r)
@@ -599,7 +667,7 @@ static int input_uses(Graph *g, Ref *d, const LNode *except_a = nullptr, const L
     int n = 0;
     for (const LNode &ln : g->lnodes) {
         if (ln.removed || &ln == except_a || &ln == except_b) continue;
-        for (size_t i = num_outputs(ln.k); i < ln.p.size(); i++) if (ln.p[i] == d) n++;
+        for (size_t i = num_outputs(ln); i < ln.p.size(); i++) if (ln.p[i] == d) n++;
         // Canny edge trace reads-modifies-writes its image; the stack is its input
         if (ln.k == LK::CANNY_EDGE_TRACE_U8_U8XY && ln.p[0] == d) n++;
     }
@@ -692,7 +760,7 @@ static bool remove_unused_pass(Graph *g)
     for (LNode &ln : g->lnodes) {
         if (ln.removed) continue;
         bool all_unused = true;
-        for (int i = 0; i < num_outputs(ln.k); i++) {
+        for (int i = 0; i < num_outputs(ln); i++) {
             Ref *o = ln.p[i];
             if (!o) continue;
             Ref *root = root_of(o);
@@ -721,7 +789,7 @@ static vx_status sort_lnodes(Graph *g)
     // writer of each data object
     std::map<Ref *, int> writer;
     for (size_t i = 0; i < n; i++)
-        for (int k = 0; k < num_outputs(live[i].k); k++) {
+        for (int k = 0; k < num_outputs(live[i]); k++) {
             Ref *o = live[i].p[k];
             if (!o) continue;
             if (writer.count(o) && live[i].k != LK::CANNY_EDGE_TRACE_U8_U8XY && !is_canny_supp(live[writer[o]].k))
@@ -733,7 +801,7 @@ static vx_status sort_lnodes(Graph *g)
         if (depth > (int)n + 1) return -2;
         if (level[i] >= 0) return level[i];
         int lv = 0;
-        for (size_t k = num_outputs(live[i].k); k < live[i].p.size(); k++) {
+        for (size_t k = num_outputs(live[i]); k < live[i].p.size(); k++) {
             Ref *d = live[i].p[k];
             if (!d) continue;
             std::vector<Ref *> deps{d};
@@ -908,12 +976,16 @@ vx_status propagate_valid_rects(Graph *g)
                                       (in->valid.end_x + 1) >> 1, (in->valid.end_y + 1) >> 1};
             break;
         }
+        case LK::USER_KERNEL:                                  // AGO_KERNEL_FLAG_VALID_RECT_RESET (vx_api.cpp:2601)
+            for (int i = 0; i < ln.nout; i++)
+                if (ln.p[i] && ln.p[i]->type == VX_TYPE_IMAGE) I(i)->valid = vx_rectangle_t{0, 0, I(i)->width, I(i)->height};
+            break;
         default: break;   // no callback in the reference: the output keeps its rectangle
         }
     }
     // multi-plane images report the rectangle of plane 0
     for (LNode &ln : g->lnodes)
-        for (int i = 0; i < num_outputs(ln.k); i++)
+        for (int i = 0; i < num_outputs(ln); i++)
             if (ln.p[i] && ln.p[i]->type == VX_TYPE_IMAGE && IMG(ln.p[i])->parent && IMG(ln.p[i])->parent->children[0] == ln.p[i])
                 IMG(ln.p[i])->parent->valid = IMG(ln.p[i])->valid;
     return VX_SUCCESS;

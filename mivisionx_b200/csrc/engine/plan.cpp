@@ -576,6 +576,15 @@ static vx_status plain_step(Graph *g, LNode &ln, Step &st)
         };
         return VX_SUCCESS;
     }
+    case LK::USER_KERNEL: {
+        // the node's kernel_f on the host, between the device steps (launches are not captured)
+        Node *n = ln.origin;
+        g->host_steps = true;
+        st.num_kernels = 0;
+        st.name = "user:" + n->ukernel->kname;
+        st.launch = [g, n](cudaStream_t q) { return run_user_node(g, n, q); };
+        return VX_SUCCESS;
+    }
     case LK::FAST_CORNERS_XY_U8_SUPRESSION: case LK::FAST_CORNERS_XY_U8_NOSUPRESSION: {
         Array *corners = static_cast<Array *>(p[0]);
         Scalar *num = p[1] ? static_cast<Scalar *>(p[1]) : nullptr;
@@ -1129,6 +1138,7 @@ vx_status plan_graph(Graph *g)
     for (void *p : g->dev_scratch) cudaFree(p);
     g->dev_scratch.clear();
     g->steps.clear();
+    g->host_steps = false;
     g->inputs.clear();
     g->outputs.clear();
 

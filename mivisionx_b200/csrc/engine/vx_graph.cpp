@@ -229,7 +229,8 @@ static cudaEvent_t cap_event(Graph *g)
 static vx_status capture(Graph *g)
 {
     release_capture(g);
-    if (g->optimizer_flags & kOptNoGraphCapture) return VX_SUCCESS;
+    // user kernels run on the host between launches: such plans launch step by step
+    if ((g->optimizer_flags & kOptNoGraphCapture) || g->host_steps) return VX_SUCCESS;
     const bool serial = (g->optimizer_flags & (kOptSerial | kOptNoFusion)) != 0;
 
     // ---- parts, in plan order, with the data they touch
@@ -439,9 +440,107 @@ static vx_status capture(Graph *g)
     return VX_SUCCESS;
 }
 
+// User-kernel nodes: deinitialize (agoShutdownNode) before a re-verification and at
+// teardown, initialize (agoInitializeNode) after a verification, allocating
+// VX_KERNEL_LOCAL_DATA_SIZE bytes of node local data first.
+void user_nodes_deinit(Graph *g)
+{
+    for (Node *n : g->nodes) {
+        if (!n->ukernel || !n->initialized) continue;
+        if (n->ukernel->deinit)
+            n->ukernel->deinit((vx_node)n, (const vx_reference *)n->params.data(), (vx_uint32)n->params.size());
+        if (n->local_owned) { free(n->local_ptr); n->local_ptr = nullptr; n->local_size = 0; n->local_owned = false; }
+        n->initialized = false;
+    }
+}
+
+static vx_status user_nodes_init(Graph *g)
+{
+    for (Node *n : g->nodes) {
+        if (!n->ukernel || n->removed || n->initialized) continue;
+        Kernel *k = n->ukernel;
+        if (k->local_size) {
+            n->local_ptr = calloc(1, k->local_size);
+            if (!n->local_ptr) return VX_ERROR_NO_MEMORY;
+            n->local_size = k->local_size;
+            n->local_owned = true;
+        }
+        n->initialized = true;
+        if (k->init) {
+            const vx_status s = k->init((vx_node)n, (const vx_reference *)n->params.data(), (vx_uint32)n->params.size());
+            if (s) {
+                log_error(n, s, "ERROR: vxVerifyGraph: kernel %s: initialize failed (%d)\n", k->kname.c_str(), s);
+                return s;
+            }
+        }
+    }
+    return VX_SUCCESS;
+}
+
+// The data a user kernel's node reads are current on the device (every earlier step ran
+// there, and host-written outputs of earlier user nodes were uploaded): host copies refresh on
+// access.
+static void mark_device_current(Ref *r)
+{
+    if (r->type == VX_TYPE_IMAGE) {
+        Image *root = IMG(r)->parent ? IMG(r)->parent : IMG(r);
+        if (root->num_planes && root->planes[0].dev) { root->dev_valid = true; root->host_valid = false; }
+    } else if (r->type == VX_TYPE_ARRAY) {
+        Array *a = static_cast<Array *>(r);
+        if (a->dev) { a->dev_valid = true; a->host_valid = false; }
+    } else if (r->type == VX_TYPE_PYRAMID) {
+        for (Image *lv : static_cast<Pyramid *>(r)->level) mark_device_current(lv);
+    } else if (r->type == VX_TYPE_SCALAR) {
+        Scalar *sc = static_cast<Scalar *>(r);
+        if (sc->dev) sc->dev_newer = true;
+    }
+}
+
+// host-written outputs of a user node go to the device before the next step reads them
+static vx_status upload_written(Ref *r, cudaStream_t q)
+{
+    if (r->type == VX_TYPE_IMAGE) return image_sync_to_device(IMG(r)->parent ? IMG(r)->parent : IMG(r), q);
+    if (r->type == VX_TYPE_ARRAY) return array_sync_to_device(static_cast<Array *>(r), q);
+    if (r->type == VX_TYPE_PYRAMID) {
+        for (Image *lv : static_cast<Pyramid *>(r)->level)
+            if (vx_status s = image_sync_to_device(lv, q)) return s;
+    }
+    return VX_SUCCESS;
+}
+
+// A user kernel's node at execution time (ago_interface.cpp:2432, ago_util_hip.cpp:708).
+// Host kernels: the stream drains, the kernel reads through the host access calls and its
+// outputs are uploaded afterwards.  Device-buffer kernels: the kernel enqueues its own work
+// on the graph's stream (VX_NODE_ATTRIBUTE_AMD_HIP_STREAM) and the stream keeps the order.
+int run_user_node(Graph *g, Node *n, cudaStream_t q)
+{
+    Kernel *k = n->ukernel;
+    const size_t np = n->params.size();
+    auto dir = [&](size_t i) { return i < k->uparams.size() ? k->uparams[i].dir : (vx_enum)VX_INPUT; };
+    if (!k->gpu_access && cudaStreamSynchronize(q) != cudaSuccess) return -1;
+    for (size_t i = 0; i < np; i++)
+        if (n->params[i] && dir(i) != VX_OUTPUT) mark_device_current(n->params[i]);
+    g->ctx->in_user_kernel++;
+    const vx_status s = k->func((vx_node)n, (const vx_reference *)n->params.data(), (vx_uint32)np);
+    g->ctx->in_user_kernel--;
+    n->status = s;
+    if (s != VX_SUCCESS) {
+        log_error(n, s, "ERROR: kernel %s exec failed (%d)\n", k->kname.c_str(), s);
+        return -2;
+    }
+    for (size_t i = 0; i < np; i++) {
+        Ref *r = n->params[i];
+        if (!r || dir(i) == VX_INPUT) continue;
+        if (k->gpu_access) mark_device_current(r);
+        else if (upload_written(r, q)) return -3;
+    }
+    return 0;
+}
+
 vx_status graph_verify(Graph *g)
 {
     std::lock_guard<std::recursive_mutex> lk(g->lock);
+    user_nodes_deinit(g);
     graph_invalidate(g);
     cudaSetDevice(g->ctx->device);
     if (!g->stream && cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) return VX_ERROR_NO_RESOURCES;
@@ -459,6 +558,8 @@ vx_status graph_verify(Graph *g)
     if (s) return s;
     g->param_signature = param_signature(g);
     s = capture(g);
+    if (s) return s;
+    s = user_nodes_init(g);
     if (s) return s;
     g->verified = true;
     g->state = VX_GRAPH_STATE_VERIFIED;
@@ -785,7 +886,8 @@ vx_status vxQueryNode(vx_node node, vx_enum attribute, void *ptr, vx_size size)
     case VX_NODE_PERFORMANCE: if (size != sizeof(vx_perf_t)) return VX_ERROR_INVALID_PARAMETERS; *(vx_perf_t *)ptr = n->perf; return VX_SUCCESS;
     case VX_NODE_BORDER: if (size != sizeof(vx_border_t)) return VX_ERROR_INVALID_PARAMETERS; *(vx_border_t *)ptr = n->border; return VX_SUCCESS;
     case VX_NODE_PARAMETERS: if (size != 4) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = (vx_uint32)n->params.size(); return VX_SUCCESS;
-    case VX_NODE_LOCAL_DATA_SIZE: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = 0; return VX_SUCCESS;
+    case VX_NODE_LOCAL_DATA_SIZE: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = n->local_size; return VX_SUCCESS;
+    case VX_NODE_LOCAL_DATA_PTR: if (size != sizeof(void *)) return VX_ERROR_INVALID_PARAMETERS; *(void **)ptr = n->local_ptr; return VX_SUCCESS;
     case VX_NODE_ATTRIBUTE_AMD_AFFINITY:
         if (size != sizeof(AgoTargetAffinityInfo)) return VX_ERROR_INVALID_PARAMETERS;
         memset(ptr, 0, size); ((AgoTargetAffinityInfo *)ptr)->device_type = AGO_TARGET_AFFINITY_GPU; return VX_SUCCESS;
@@ -812,6 +914,17 @@ vx_status vxSetNodeAttribute(vx_node node, vx_enum attribute, const void *ptr, v
     case VX_NODE_ATTRIBUTE_AMD_AFFINITY:
         if (size != sizeof(AgoTargetAffinityInfo)) return VX_ERROR_INVALID_PARAMETERS;
         n->affinity = ((const AgoTargetAffinityInfo *)ptr)->device_type;
+        return VX_SUCCESS;
+    // user-kernel node local data, settable when the kernel declares no local data size
+    // (vx_types.h VX_NODE_LOCAL_DATA_SIZE / _PTR)
+    case VX_NODE_LOCAL_DATA_SIZE:
+        if (size != sizeof(vx_size) || !n->ukernel || n->ukernel->local_size) return VX_ERROR_NOT_SUPPORTED;
+        n->local_size = *(const vx_size *)ptr;
+        return VX_SUCCESS;
+    case VX_NODE_LOCAL_DATA_PTR:
+        if (size != sizeof(void *) || !n->ukernel || n->ukernel->local_size) return VX_ERROR_NOT_SUPPORTED;
+        if (n->local_owned) { free(n->local_ptr); n->local_owned = false; }
+        n->local_ptr = *(void *const *)ptr;
         return VX_SUCCESS;
     default: return VX_ERROR_NOT_SUPPORTED;
     }

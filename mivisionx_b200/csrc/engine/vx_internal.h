@@ -179,11 +179,40 @@ struct Remap : Ref {
 // ------------------------------------------------------------------------------------
 // Kernels, nodes and graphs
 // ------------------------------------------------------------------------------------
+// A parameter a user kernel declares (vxAddParameterToKernel).
+struct UserParam {
+    vx_enum dir = 0, type = 0, state = 0;
+    bool set = false;
+};
+
 struct Kernel : Ref {
     vx_enum id = 0;
     std::string kname;
     int num_params = 0;
     const char *sig = "";             // parameter directions and types (vx_kernels.cpp)
+    // user kernels (vxAddUserKernel, vx_api.cpp:2584): host callbacks and declared parameters
+    bool user = false, finalized = false;
+    bool gpu_access = false;          // VX_KERNEL_ATTRIBUTE_AMD_GPU_BUFFER_ACCESS_ENABLE: works on device buffers
+    vx_kernel_f func = nullptr;
+    vx_kernel_validate_f validate = nullptr;
+    vx_kernel_initialize_f init = nullptr;
+    vx_kernel_deinitialize_f deinit = nullptr;
+    std::vector<UserParam> uparams;
+    vx_size local_size = 0;           // VX_KERNEL_LOCAL_DATA_SIZE
+};
+
+// vx_meta_format: what a user kernel's validator says about one output parameter.
+struct MetaFormat {
+    uint32_t magic = 0x4d455441u;
+    vx_enum type = 0;                 // VX_TYPE_IMAGE / ARRAY / SCALAR / PYRAMID (0: not set)
+    vx_df_image format = 0;
+    vx_uint32 width = 0, height = 0;
+    vx_enum item_type = 0;
+    vx_size capacity = 0;
+    vx_enum scalar_type = 0;
+    vx_size levels = 0;
+    vx_float32 scale = 0.f;
+    vx_kernel_image_valid_rectangle_f valid_rect = nullptr;
 };
 
 struct Convolution : Ref {
@@ -209,6 +238,12 @@ struct Node : Ref {
     void *state[2] = {nullptr, nullptr};
     size_t state_bytes[2] = {0, 0};
     void *node_state(int slot, size_t bytes);
+    // user-kernel nodes: the kernel object, VX_NODE_LOCAL_DATA_SIZE / _PTR and whether the
+    // kernel's initialize callback has run for the current verification
+    Kernel *ukernel = nullptr;
+    vx_size local_size = 0;
+    void *local_ptr = nullptr;
+    bool local_owned = false, initialized = false;
     ~Node() override;
 };
 
@@ -246,6 +281,7 @@ enum class LK : int {
     CONVOLVE_U8_U8, CONVOLVE_S16_U8,
     HARRIS_SOBEL_HG3_U8_5x5, HARRIS_SOBEL_HG3_U8_7x7, HARRIS_SCORE_HVC_HG3_5x5, HARRIS_SCORE_HVC_HG3_7x7,
     FAST_CORNERS_XY_U8_SUPRESSION, FAST_CORNERS_XY_U8_NOSUPRESSION,
+    USER_KERNEL,                      // a vxAddUserKernel node, run on the host
     COUNT
 };
 const char *lk_name(LK k);
@@ -258,6 +294,7 @@ struct LNode {
     vx_border_t border{VX_BORDER_UNDEFINED, {}};
     bool removed = false;
     int level = 0;                    // hierarchical level (longest path from graph inputs)
+    int nout = -1;                    // outputs first; -1: the count the kernel kind implies
 };
 
 // One unit of device work in the execution plan: recorded into the CUDA graph.
@@ -299,6 +336,7 @@ struct Graph : Ref {
     std::vector<Ref *> owned_virtual;            // virtual data created for lowering
     std::vector<void *> dev_scratch;             // device allocations owned by the plan
     bool verified = false;
+    bool host_steps = false;          // the plan calls user kernels on the host: launches are not captured
     vx_enum state = VX_GRAPH_STATE_UNVERIFIED;
     uint32_t optimizer_flags = 0;
     uint32_t affinity = 0;
@@ -342,6 +380,7 @@ struct Context : Ref {
     uint32_t affinity = AGO_TARGET_AFFINITY_GPU;
     std::vector<Kernel *> kernels;
     bool tearing_down = false;        // vxReleaseContext deletes every object itself
+    int in_user_kernel = 0;           // > 0 while a user kernel's callback runs: virtual data may be accessed
 };
 
 // Optimizer flag bits of VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS (ago/ago_internal.h:123-129),
@@ -362,6 +401,8 @@ vx_status image_alloc_device(Image *img);
 void image_refresh_views(Image *root);
 vx_status image_sync_to_device(Image *img, cudaStream_t s);
 vx_status image_sync_to_host(Image *img);
+void user_nodes_deinit(Graph *g);                 // vx_graph.cpp
+int run_user_node(Graph *g, Node *n, cudaStream_t q);
 vx_status array_alloc_device(Array *a);
 vx_status array_sync_to_device(Array *a, cudaStream_t s);
 vx_status array_sync_to_host(Array *a);

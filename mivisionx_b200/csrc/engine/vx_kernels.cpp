@@ -139,11 +139,49 @@ Kernel *context_kernel(Context *c, const KernelSpec *s)
 
 template <class T> T *as(void *h) { return static_cast<T *>(static_cast<Ref *>(h)); }
 
+constexpr vx_uint32 kMaxUserParams = 32;   // AGO_MAX_PARAMS
+
+// a user kernel of the context by name (exact) or by enumeration
+Kernel *user_kernel(Context *c, const char *name, vx_enum id, bool byName)
+{
+    for (Kernel *k : c->kernels)
+        if (k->user && (byName ? (name && k->kname == name) : k->id == id)) return k;
+    return nullptr;
+}
+
 }  // namespace
+
+// Parameters a node of a user kernel must have: every required one set, types as declared
+// (VX_TYPE_REFERENCE accepts any object).
+static vx_status check_user_params(Node *n)
+{
+    Kernel *k = n->ukernel;
+    if (n->params.size() != k->uparams.size()) return VX_ERROR_INVALID_PARAMETERS;
+    for (size_t i = 0; i < n->params.size(); i++) {
+        const UserParam &up = k->uparams[i];
+        Ref *r = n->params[i];
+        if (!r) {
+            if (up.state == VX_PARAMETER_STATE_REQUIRED) {
+                log_error(n, VX_ERROR_NOT_SUFFICIENT, "ERROR: vxVerifyGraph: %s: required parameter %zu is not set\n",
+                          k->kname.c_str(), i);
+                return VX_ERROR_NOT_SUFFICIENT;
+            }
+            continue;
+        }
+        if (!is_ref(r)) return VX_ERROR_INVALID_REFERENCE;
+        if (up.type != VX_TYPE_REFERENCE && r->type != up.type) {
+            log_error(n, VX_ERROR_INVALID_TYPE, "ERROR: vxVerifyGraph: %s: parameter %zu has type 0x%x, expected 0x%x\n",
+                      k->kname.c_str(), i, r->type, up.type);
+            return VX_ERROR_INVALID_TYPE;
+        }
+    }
+    return VX_SUCCESS;
+}
 
 // Every required parameter of the node is set and every parameter has its declared type.
 vx_status check_node_params(Node *n)
 {
+    if (n->ukernel) return check_user_params(n);
     const KernelSpec *s = spec_by_enum(n->kernel);
     if (!s) return VX_SUCCESS;       // not in the table: the kernel's own validation decides
     const size_t np = strlen(s->sig) / 2;
@@ -186,6 +224,11 @@ extern "C" {
 vx_kernel vxGetKernelByName(vx_context context, const vx_char *name)
 {
     if (!is_valid(context, VX_TYPE_CONTEXT)) return nullptr;
+    if (Kernel *u = user_kernel(as<Context>(context), name, 0, true)) {
+        u->ext_count++;
+        u->released = false;
+        return (vx_kernel)u;
+    }
     const KernelSpec *s = spec_by_name(name);
     if (!s) {
         log_error(as<Ref>(context), VX_ERROR_INVALID_PARAMETERS, "ERROR: vxGetKernelByName: kernel %s is not known\n",
@@ -201,6 +244,11 @@ vx_kernel vxGetKernelByName(vx_context context, const vx_char *name)
 vx_kernel vxGetKernelByEnum(vx_context context, vx_enum kernel)
 {
     if (!is_valid(context, VX_TYPE_CONTEXT)) return nullptr;
+    if (Kernel *u = user_kernel(as<Context>(context), nullptr, kernel, false)) {
+        u->ext_count++;
+        u->released = false;
+        return (vx_kernel)u;
+    }
     const KernelSpec *s = spec_by_enum(kernel);
     if (!s) return nullptr;
     Kernel *k = context_kernel(as<Context>(context), s);
@@ -231,7 +279,7 @@ vx_status vxQueryKernel(vx_kernel kernel, vx_enum attribute, void *ptr, vx_size 
         snprintf((char *)ptr, size, "%s", k->kname.c_str());
         return VX_SUCCESS;
     case VX_KERNEL_ENUM: if (size != sizeof(vx_enum)) return VX_ERROR_INVALID_PARAMETERS; *(vx_enum *)ptr = k->id; return VX_SUCCESS;
-    case VX_KERNEL_LOCAL_DATA_SIZE: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = 0; return VX_SUCCESS;
+    case VX_KERNEL_LOCAL_DATA_SIZE: if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS; *(vx_size *)ptr = k->local_size; return VX_SUCCESS;
     default: return VX_ERROR_NOT_SUPPORTED;
     }
 }
@@ -240,8 +288,11 @@ vx_node vxCreateGenericNode(vx_graph graph, vx_kernel kernel)
 {
     if (!is_valid(graph, VX_TYPE_GRAPH) || !is_valid(kernel, VX_TYPE_KERNEL)) return nullptr;
     Kernel *k = as<Kernel>(kernel);
+    if (k->user && !k->finalized) return nullptr;
     std::vector<Ref *> params((size_t)k->num_params, nullptr);
-    return (vx_node)graph_add_node(as<Graph>(graph), k->id, params);
+    Node *n = graph_add_node(as<Graph>(graph), k->id, params);
+    if (n && k->user) n->ukernel = k;
+    return (vx_node)n;
 }
 
 vx_status vxSetParameterByIndex(vx_node node, vx_uint32 index, vx_reference value)
@@ -250,7 +301,11 @@ vx_status vxSetParameterByIndex(vx_node node, vx_uint32 index, vx_reference valu
     Node *n = as<Node>(node);
     if (index >= n->params.size()) return VX_ERROR_INVALID_PARAMETERS;
     if (value && !is_ref(value)) return VX_ERROR_INVALID_REFERENCE;
-    const KernelSpec *s = spec_by_enum(n->kernel);
+    const KernelSpec *s = n->ukernel ? nullptr : spec_by_enum(n->kernel);
+    if (value && n->ukernel) {
+        const vx_enum want = n->ukernel->uparams[index].type, got = as<Ref>(value)->type;
+        if (want != VX_TYPE_REFERENCE && got != want) return VX_ERROR_INVALID_TYPE;
+    }
     if (value && s) {
         const vx_enum want = type_of(s->sig[2 * index + 1]);
         const vx_enum got = as<Ref>(value)->type;
@@ -307,8 +362,18 @@ vx_status vxQueryParameter(vx_parameter parameter, vx_enum attribute, void *ptr,
     CHECK_REF(parameter, VX_TYPE_PARAMETER);
     Parameter *p = as<Parameter>(parameter);
     if (!ptr) return VX_ERROR_INVALID_PARAMETERS;
-    const KernelSpec *s = spec_by_enum(p->node ? p->node->kernel : p->kernel->id);
+    Kernel *uk = p->node ? p->node->ukernel : (p->kernel->user ? p->kernel : nullptr);
+    const KernelSpec *s = uk ? nullptr : spec_by_enum(p->node ? p->node->kernel : p->kernel->id);
     const char *sig = s ? s->sig + 2 * p->index : "i*";
+    if (uk) {
+        const UserParam &up = uk->uparams[p->index];
+        switch (attribute) {
+        case VX_PARAMETER_DIRECTION: if (size != sizeof(vx_enum)) return VX_ERROR_INVALID_PARAMETERS; *(vx_enum *)ptr = up.dir; return VX_SUCCESS;
+        case VX_PARAMETER_TYPE: if (size != sizeof(vx_enum)) return VX_ERROR_INVALID_PARAMETERS; *(vx_enum *)ptr = up.type; return VX_SUCCESS;
+        case VX_PARAMETER_STATE: if (size != sizeof(vx_enum)) return VX_ERROR_INVALID_PARAMETERS; *(vx_enum *)ptr = up.state; return VX_SUCCESS;
+        default: break;
+        }
+    }
     switch (attribute) {
     case VX_PARAMETER_INDEX: if (size != sizeof(vx_uint32)) return VX_ERROR_INVALID_PARAMETERS; *(vx_uint32 *)ptr = p->index; return VX_SUCCESS;
     case VX_PARAMETER_DIRECTION: if (size != sizeof(vx_enum)) return VX_ERROR_INVALID_PARAMETERS; *(vx_enum *)ptr = direction_of(sig[0]); return VX_SUCCESS;
@@ -334,8 +399,7 @@ vx_status vxReleaseParameter(vx_parameter *param)
 }
 
 // vxLoadKernels (vx_api.cpp:2325 -> agoLoadModule, ago_interface.cpp:1128): open the module
-// library and call its vxPublishKernels.  User kernels (vxAddUserKernel) are not part of
-// this target, so a module that publishes any fails to load.
+// library and call its vxPublishKernels, which adds its kernels with vxAddUserKernel.
 vx_status vxLoadKernels(vx_context context, const vx_char *module)
 {
     CHECK_REF(context, VX_TYPE_CONTEXT);
@@ -355,6 +419,190 @@ vx_status vxLoadKernels(vx_context context, const vx_char *module)
         return VX_ERROR_INVALID_MODULE;
     }
     return pub(context);
+}
+
+// ---------------------------------------------------------------- user kernels
+// vxAddUserKernel / vxAddParameterToKernel / vxFinalizeKernel / vxRemoveKernel /
+// vxSetKernelAttribute (vx_api.cpp:2584-2800).  A user kernel's node runs its kernel_f on the
+// host when the graph executes; with VX_KERNEL_ATTRIBUTE_AMD_GPU_BUFFER_ACCESS_ENABLE it gets
+// device buffers (VX_IMAGE_ATTRIBUTE_AMD_HIP_BUFFER) and the graph's CUDA stream
+// (VX_NODE_ATTRIBUTE_AMD_HIP_STREAM) instead of host access.
+vx_kernel vxAddUserKernel(vx_context context, const vx_char name[VX_MAX_KERNEL_NAME], vx_enum enumeration,
+                          vx_kernel_f func_ptr, vx_uint32 numParams, vx_kernel_validate_f validate,
+                          vx_kernel_initialize_f init, vx_kernel_deinitialize_f deinit)
+{
+    if (!is_valid(context, VX_TYPE_CONTEXT) || !name || !func_ptr || !validate || numParams == 0 ||
+        numParams > kMaxUserParams)
+        return nullptr;
+    Context *c = as<Context>(context);
+    if (user_kernel(c, name, 0, true) || user_kernel(c, nullptr, enumeration, false) || spec_by_enum(enumeration) ||
+        spec_by_name(name)) {
+        log_error(as<Ref>(context), VX_ERROR_INVALID_PARAMETERS, "ERROR: vxAddUserKernel: %s / 0x%x is already a kernel\n",
+                  name, enumeration);
+        return nullptr;
+    }
+    Kernel *k = new Kernel();
+    k->type = VX_TYPE_KERNEL;
+    k->id = enumeration;
+    k->kname = name;
+    k->user = true;
+    k->func = func_ptr;
+    k->validate = validate;
+    k->init = init;
+    k->deinit = deinit;
+    k->num_params = (int)numParams;
+    k->uparams.resize(numParams);
+    k->ext_count = 1;
+    k->int_count = 1;                // the context's kernel list
+    add_ref(c, k);
+    c->kernels.push_back(k);
+    return (vx_kernel)k;
+}
+
+vx_status vxAddParameterToKernel(vx_kernel kernel, vx_uint32 index, vx_enum dir, vx_enum data_type, vx_enum state)
+{
+    CHECK_REF(kernel, VX_TYPE_KERNEL);
+    Kernel *k = as<Kernel>(kernel);
+    if (!k->user || k->finalized || index >= kMaxUserParams) return VX_ERROR_INVALID_PARAMETERS;
+    if (dir != VX_INPUT && dir != VX_OUTPUT && dir != VX_BIDIRECTIONAL) return VX_ERROR_INVALID_PARAMETERS;
+    if (state != VX_PARAMETER_STATE_REQUIRED && state != VX_PARAMETER_STATE_OPTIONAL) return VX_ERROR_INVALID_PARAMETERS;
+    if (data_type == VX_TYPE_DELAY && dir != VX_INPUT) return VX_ERROR_INVALID_PARAMETERS;
+    if (index >= k->uparams.size()) k->uparams.resize(index + 1);
+    k->uparams[index] = UserParam{dir, data_type, state, true};
+    k->num_params = (int)k->uparams.size();
+    return VX_SUCCESS;
+}
+
+vx_status vxFinalizeKernel(vx_kernel kernel)
+{
+    CHECK_REF(kernel, VX_TYPE_KERNEL);
+    Kernel *k = as<Kernel>(kernel);
+    if (!k->user || k->finalized || k->uparams.empty()) return VX_ERROR_INVALID_REFERENCE;
+    for (const UserParam &up : k->uparams)
+        if (!up.set) return VX_ERROR_INVALID_REFERENCE;
+    k->finalized = true;
+    return VX_SUCCESS;
+}
+
+vx_status vxRemoveKernel(vx_kernel kernel)
+{
+    CHECK_REF(kernel, VX_TYPE_KERNEL);
+    Kernel *k = as<Kernel>(kernel);
+    if (!k->user) return VX_ERROR_INVALID_PARAMETERS;      // built-in kernels stay
+    Context *c = k->ctx;
+    for (size_t i = 0; i < c->kernels.size(); i++)
+        if (c->kernels[i] == k) { c->kernels.erase(c->kernels.begin() + (long)i); break; }
+    k->finalized = false;            // no new nodes; existing nodes keep their callbacks
+    k->ext_count = 0;
+    return VX_SUCCESS;
+}
+
+vx_status vxSetKernelAttribute(vx_kernel kernel, vx_enum attribute, const void *ptr, vx_size size)
+{
+    CHECK_REF(kernel, VX_TYPE_KERNEL);
+    Kernel *k = as<Kernel>(kernel);
+    if (!ptr) return VX_ERROR_INVALID_PARAMETERS;
+    switch (attribute) {
+    case VX_KERNEL_LOCAL_DATA_SIZE:
+        if (size != sizeof(vx_size)) return VX_ERROR_INVALID_PARAMETERS;
+        k->local_size = *(const vx_size *)ptr;
+        return VX_SUCCESS;
+    case VX_KERNEL_ATTRIBUTE_AMD_GPU_BUFFER_ACCESS_ENABLE:
+        if (size != sizeof(vx_bool)) return VX_ERROR_INVALID_PARAMETERS;
+        if (!k->user || k->finalized) return VX_ERROR_NOT_SUPPORTED;
+        k->gpu_access = *(const vx_bool *)ptr == vx_true_e;
+        return VX_SUCCESS;
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+// ---------------------------------------------------------------- meta formats
+static MetaFormat *meta_of(vx_meta_format m)
+{
+    MetaFormat *f = reinterpret_cast<MetaFormat *>(m);
+    return f && f->magic == MetaFormat{}.magic ? f : nullptr;
+}
+
+vx_status vxSetMetaFormatAttribute(vx_meta_format meta, vx_enum attribute, const void *ptr, vx_size size)
+{
+    MetaFormat *m = meta_of(meta);
+    if (!m) return VX_ERROR_INVALID_REFERENCE;
+    if (!ptr) return VX_ERROR_INVALID_PARAMETERS;
+    auto take = [&](auto &dst, vx_enum type) {
+        if (size != sizeof(dst)) return VX_ERROR_INVALID_PARAMETERS;
+        memcpy(&dst, ptr, sizeof(dst));
+        if (type) m->type = type;
+        return VX_SUCCESS;
+    };
+    switch (attribute) {
+    case VX_IMAGE_FORMAT: return take(m->format, VX_TYPE_IMAGE);
+    case VX_IMAGE_WIDTH: return take(m->width, VX_TYPE_IMAGE);
+    case VX_IMAGE_HEIGHT: return take(m->height, VX_TYPE_IMAGE);
+    case VX_ARRAY_ITEMTYPE: return take(m->item_type, VX_TYPE_ARRAY);
+    case VX_ARRAY_CAPACITY: return take(m->capacity, VX_TYPE_ARRAY);
+    case VX_SCALAR_TYPE: return take(m->scalar_type, VX_TYPE_SCALAR);
+    case VX_PYRAMID_LEVELS: return take(m->levels, VX_TYPE_PYRAMID);
+    case VX_PYRAMID_SCALE: return take(m->scale, VX_TYPE_PYRAMID);
+    case VX_PYRAMID_FORMAT: return take(m->format, VX_TYPE_PYRAMID);
+    case VX_PYRAMID_WIDTH: return take(m->width, VX_TYPE_PYRAMID);
+    case VX_PYRAMID_HEIGHT: return take(m->height, VX_TYPE_PYRAMID);
+    case VX_VALID_RECT_CALLBACK: return take(m->valid_rect, 0);
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_status vxQueryMetaFormatAttribute(vx_meta_format meta, vx_enum attribute, void *ptr, vx_size size)
+{
+    MetaFormat *m = meta_of(meta);
+    if (!m) return VX_ERROR_INVALID_REFERENCE;
+    if (!ptr) return VX_ERROR_INVALID_PARAMETERS;
+    auto give = [&](const auto &src) {
+        if (size != sizeof(src)) return VX_ERROR_INVALID_PARAMETERS;
+        memcpy(ptr, &src, sizeof(src));
+        return VX_SUCCESS;
+    };
+    switch (attribute) {
+    case VX_IMAGE_FORMAT: case VX_PYRAMID_FORMAT: return give(m->format);
+    case VX_IMAGE_WIDTH: case VX_PYRAMID_WIDTH: return give(m->width);
+    case VX_IMAGE_HEIGHT: case VX_PYRAMID_HEIGHT: return give(m->height);
+    case VX_ARRAY_ITEMTYPE: return give(m->item_type);
+    case VX_ARRAY_CAPACITY: return give(m->capacity);
+    case VX_SCALAR_TYPE: return give(m->scalar_type);
+    case VX_PYRAMID_LEVELS: return give(m->levels);
+    case VX_PYRAMID_SCALE: return give(m->scale);
+    case VX_VALID_RECT_CALLBACK: return give(m->valid_rect);
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
+}
+
+vx_status vxSetMetaFormatFromReference(vx_meta_format meta, vx_reference exemplar)
+{
+    MetaFormat *m = meta_of(meta);
+    if (!m) return VX_ERROR_INVALID_REFERENCE;
+    if (!is_ref(exemplar)) return VX_ERROR_INVALID_REFERENCE;
+    Ref *r = as<Ref>(exemplar);
+    switch (r->type) {
+    case VX_TYPE_IMAGE: {
+        Image *img = static_cast<Image *>(r);
+        m->type = VX_TYPE_IMAGE; m->format = img->format; m->width = img->width; m->height = img->height;
+        return VX_SUCCESS;
+    }
+    case VX_TYPE_ARRAY: {
+        Array *a = static_cast<Array *>(r);
+        m->type = VX_TYPE_ARRAY; m->item_type = a->item_type; m->capacity = a->capacity;
+        return VX_SUCCESS;
+    }
+    case VX_TYPE_SCALAR:
+        m->type = VX_TYPE_SCALAR; m->scalar_type = static_cast<Scalar *>(r)->data_type;
+        return VX_SUCCESS;
+    case VX_TYPE_PYRAMID: {
+        Pyramid *py = static_cast<Pyramid *>(r);
+        m->type = VX_TYPE_PYRAMID; m->levels = py->levels; m->scale = py->scale; m->format = py->format;
+        m->width = py->width; m->height = py->height;
+        return VX_SUCCESS;
+    }
+    default: return VX_ERROR_NOT_SUPPORTED;
+    }
 }
 
 }  // extern "C"

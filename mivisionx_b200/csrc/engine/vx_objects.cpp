@@ -113,6 +113,7 @@ static void graph_destroy_contents(Graph *g)
 {
     if (g->scheduled) graph_wait(g);
     if (g->stream) cudaStreamSynchronize(g->stream);
+    user_nodes_deinit(g);
     graph_invalidate(g);
     g->lnodes.clear();
     g->replaced.clear();
@@ -522,6 +523,8 @@ vx_status vxReleaseContext(vx_context *context)
     std::vector<Ref *> graphs, others;
     for (Ref *r : c->refs) (r->type == VX_TYPE_GRAPH ? graphs : others).push_back(r);
     c->refs.clear();
+    // user kernels' deinitialize callbacks run while every object still exists
+    for (Ref *r : graphs) user_nodes_deinit(static_cast<Graph *>(r));
     // graphs first: their plans and captured CUDA graphs name the other objects' storage
     for (Ref *r : graphs) { r->magic = 0; delete r; }
     for (Ref *r : others) { r->magic = 0; delete r; }
@@ -785,9 +788,20 @@ vx_status vxQueryImage(vx_image image, vx_enum attribute, void *ptr, vx_size siz
     case VX_IMAGE_UNIFORM_VALUE: if (size != sizeof(vx_pixel_value_t)) return VX_ERROR_INVALID_PARAMETERS; *(vx_pixel_value_t *)ptr = img->uniform_value; return VX_SUCCESS;
     case VX_IMAGE_ATTRIBUTE_AMD_HIP_BUFFER:
         if (size != sizeof(void *)) return VX_ERROR_INVALID_PARAMETERS;
-        if (image_sync_to_device(img, 0)) return VX_FAILURE;
-        cudaDeviceSynchronize();
+        if (!img->ctx->in_user_kernel) {           // inside a user kernel the stream orders the data
+            if (image_sync_to_device(img, 0)) return VX_FAILURE;
+            cudaDeviceSynchronize();
+        } else if (image_alloc_device(img->parent ? img->parent : img)) {
+            return VX_ERROR_NO_MEMORY;
+        }
         *(void **)ptr = img->planes[0].dev; return VX_SUCCESS;
+    case VX_IMAGE_ATTRIBUTE_AMD_GPU_BUFFER_OFFSET:     // plane 0 starts at the buffer
+        if (size != sizeof(vx_uint32)) return VX_ERROR_INVALID_PARAMETERS;
+        *(vx_uint32 *)ptr = 0; return VX_SUCCESS;
+    case VX_IMAGE_ATTRIBUTE_AMD_GPU_BUFFER_STRIDE:     // device row pitch of plane 0, bytes
+        if (size != sizeof(vx_uint32)) return VX_ERROR_INVALID_PARAMETERS;
+        if (image_alloc_device(img->parent ? img->parent : img)) return VX_ERROR_NO_MEMORY;
+        *(vx_uint32 *)ptr = img->planes[0].dev_stride; return VX_SUCCESS;
     default: return VX_ERROR_NOT_SUPPORTED;
     }
 }
@@ -816,7 +830,7 @@ vx_status vxCopyImagePatch(vx_image image, const vx_rectangle_t *image_rect, vx_
 {
     CHECK_REF(image, VX_TYPE_IMAGE);
     Image *img = as<Image>(image);
-    if (img->is_virtual || !user_addr || !user_ptr) return VX_ERROR_INVALID_PARAMETERS;
+    if ((img->is_virtual && !img->ctx->in_user_kernel) || !user_addr || !user_ptr) return VX_ERROR_INVALID_PARAMETERS;
     use_device(img);
     if (usage != VX_READ_ONLY && usage != VX_WRITE_ONLY) return VX_ERROR_INVALID_PARAMETERS;
     uint32_t x0, y0, x1, y1;
@@ -867,7 +881,7 @@ vx_status vxMapImagePatch(vx_image image, const vx_rectangle_t *rect, vx_uint32 
     (void)flags;
     CHECK_REF(image, VX_TYPE_IMAGE);
     Image *img = as<Image>(image);
-    if (img->is_virtual || !map_id || !addr || !ptr) return VX_ERROR_INVALID_PARAMETERS;
+    if ((img->is_virtual && !img->ctx->in_user_kernel) || !map_id || !addr || !ptr) return VX_ERROR_INVALID_PARAMETERS;
     if (mem_type != VX_MEMORY_TYPE_HOST) return VX_ERROR_NOT_SUPPORTED;
     vx_rectangle_t full{0, 0, img->width, img->height};
     if (!rect) rect = &full;
@@ -1091,6 +1105,7 @@ void *Node::node_state(int slot, size_t bytes)
 Node::~Node()
 {
     for (void *p : state) if (p) cudaFree(p);
+    if (local_owned) free(local_ptr);
 }
 
 // ---------------------------------------------------------------- distributions

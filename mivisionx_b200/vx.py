@@ -90,6 +90,19 @@ VX_GRAPH_ATTRIBUTE_AMD_IMPORT_FROM_TEXT = _attr_base(VX_ID_AMD, VX_TYPE_GRAPH) +
 VX_GRAPH_ATTRIBUTE_AMD_PERFORMANCE_INTERNAL_LAST = _attr_base(VX_ID_AMD, VX_TYPE_GRAPH) + 0x05
 AGO_TARGET_AFFINITY_CPU, AGO_TARGET_AFFINITY_GPU = 0x10, 0x20
 
+VX_INPUT, VX_OUTPUT, VX_BIDIRECTIONAL = _enum_base(0, 0x00) + 0, _enum_base(0, 0x00) + 1, _enum_base(0, 0x00) + 2
+VX_PARAMETER_STATE_REQUIRED, VX_PARAMETER_STATE_OPTIONAL = _enum_base(0, 0x08) + 0, _enum_base(0, 0x08) + 1
+VX_KERNEL_LOCAL_DATA_SIZE = _attr_base(0, 0x804) + 3
+VX_NODE_STATUS = _attr_base(0, 0x803) + 0
+VX_NODE_LOCAL_DATA_SIZE = _attr_base(0, 0x803) + 3
+VX_NODE_LOCAL_DATA_PTR = _attr_base(0, 0x803) + 4
+VX_NODE_ATTRIBUTE_AMD_HIP_STREAM = _attr_base(VX_ID_AMD, 0x803) + 0x03
+VX_KERNEL_ATTRIBUTE_AMD_GPU_BUFFER_ACCESS_ENABLE = _attr_base(VX_ID_AMD, 0x804) + 0x05
+VX_IMAGE_ATTRIBUTE_AMD_GPU_BUFFER_STRIDE = _attr_base(VX_ID_AMD, VX_TYPE_IMAGE) + 0x04
+VX_IMAGE_ATTRIBUTE_AMD_HIP_BUFFER = _attr_base(VX_ID_AMD, VX_TYPE_IMAGE) + 0x06
+VX_ID_USER = 0xFFE
+VX_KERNEL_BASE_USER = _enum_base(VX_ID_USER, 0)   # VX_KERNEL_BASE(VX_ID_USER, 0): enumerations for user kernels
+
 # optimizer flag bits this target adds to VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS
 OPT_NO_FUSION = 0x00010000        # one launch per lowered node ("plain" form)
 OPT_NO_GRAPH_CAPTURE = 0x00020000  # launch the steps directly instead of one CUDA graph
@@ -199,7 +212,21 @@ _SIGS = {
     "vxHistogramNode": (vp, [vp, vp, vp]),
     "vxCreateDelay": (vp, [vp, vp, sz]), "vxGetReferenceFromDelay": (vp, [vp, i32]), "vxAgeDelay": (i32, [vp]),
     "vxRegisterAutoAging": (i32, [vp, vp]), "vxQueryDelay": (i32, [vp, i32, vp, sz]),
+    # kernels, generic nodes and user kernels
+    "vxGetKernelByName": (vp, [vp, C.c_char_p]), "vxGetKernelByEnum": (vp, [vp, i32]),
+    "vxReleaseKernel": (i32, [C.POINTER(vp)]), "vxQueryKernel": (i32, [vp, i32, vp, sz]),
+    "vxCreateGenericNode": (vp, [vp, vp]), "vxSetParameterByIndex": (i32, [vp, u32, vp]),
+    "vxQueryNode": (i32, [vp, i32, vp, sz]),
+    "vxAddUserKernel": (vp, [vp, C.c_char_p, i32, vp, u32, vp, vp, vp]),
+    "vxAddParameterToKernel": (i32, [vp, u32, i32, i32, i32]), "vxFinalizeKernel": (i32, [vp]),
+    "vxRemoveKernel": (i32, [vp]), "vxSetKernelAttribute": (i32, [vp, i32, vp, sz]),
+    "vxSetMetaFormatAttribute": (i32, [vp, i32, vp, sz]), "vxSetMetaFormatFromReference": (i32, [vp, vp]),
+    "vxQueryMetaFormatAttribute": (i32, [vp, i32, vp, sz]),
 }
+
+# user-kernel callbacks (vx_types.h vx_kernel_f / vx_kernel_validate_f / vx_kernel_initialize_f)
+KernelF = C.CFUNCTYPE(i32, vp, C.POINTER(vp), u32)
+KernelValidateF = C.CFUNCTYPE(i32, vp, C.POINTER(vp), u32, C.POINTER(vp))
 
 _PIX = {VX_DF_IMAGE_U8: (np.uint8, 1), VX_DF_IMAGE_U16: (np.uint16, 1), VX_DF_IMAGE_S16: (np.int16, 1),
         VX_DF_IMAGE_RGB: (np.uint8, 3), VX_DF_IMAGE_RGBX: (np.uint8, 4), VX_DF_IMAGE_F32_AMD: (np.float32, 1),

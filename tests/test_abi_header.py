@@ -51,7 +51,9 @@ def test_enums_and_structs_match_reference():
 
 
 def _declared(path, prefix):
+    """Functions the header declares (typedefs of function pointers are not symbols)."""
     src = re.sub(r"/\*.*?\*/", "", open(path).read(), flags=re.S)
+    src = re.sub(r"typedef[^;]*;", "", src)
     return sorted(set(re.findall(r"\b(" + prefix + r"\w+)\s*\(", src)))
 
 
