@@ -492,7 +492,7 @@ def run_ours(a, wl_name):
     ctx = api.obj(api.vxCreateContext(), "context")
     api.set_device(ctx, local)
     frames = wl.make_frames(frame_seed(rank), B)
-    g = wl.build(api, ctx, B, flags=V.OPT_NO_FUSION if a.plain else None)
+    g = wl.build(api, ctx, B, flags=((V.OPT_NO_FUSION if a.plain else 0) | a.opt_flags) or None)
     plan = api.plan(g.graph)
     kernels_per_step = sum(k for _, k in plan)
     # page-locked host buffers, one per image plane: (rows, row bytes)
@@ -558,7 +558,7 @@ def run_ours(a, wl_name):
 
     # (a) images created from the application's page-locked buffers: vxProcessGraph uploads
     # the inputs and downloads the outputs inside its CUDA graph, overlapped with the kernels
-    gh = wl.build(api, ctx, B, flags=V.OPT_NO_FUSION if a.plain else None,
+    gh = wl.build(api, ctx, B, flags=((V.OPT_NO_FUSION if a.plain else 0) | a.opt_flags) or None,
                   host_io=wl.host_io([[p.numpy() for p in ps] for ps in pin_in],
                                      [[p.numpy() for p in ps] for ps in pin_out]))
     in_arrays_h = [(arr, buf, isz, n) for (arr, kp), (_, buf, isz, n) in
@@ -877,6 +877,9 @@ def main(argv=None):
     ap.add_argument("--frames", type=int, default=0, help="frames per step per GPU (default: the workload's)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--opt-flags", type=lambda v: int(v, 0), default=0,
+                    help="extra VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS bits for the timed graph (e.g. 0x80000: "
+                         "pixel chains stage tiles with cp.async instead of TMA)")
     ap.add_argument("--plain", action="store_true",
                     help="run the one-launch-per-node plan (the unfused, unbatched comparison form)")
     ap.add_argument("--no-per-graph", dest="per_graph", action="store_false",

@@ -814,6 +814,24 @@ int agocuda_fused_PixelChain_U8(void *stream, const agocuda_pixel_program *progr
                                 const agocuda_pixel_frame *frames, uint32_t numFrames, uint32_t maxWidth,
                                 uint32_t maxHeight);
 
+/* The same chain with each block's input tiles staged by TMA: one 2D tensor copy per plane
+ * (box 160 x (64 + 2 x stencils) bytes) completing on a shared-memory mbarrier, instead of
+ * ~700 16-byte cp.async copies per plane.  `maps` is a DEVICE array of
+ * agocuda_PixelChain_tensor_maps_size(numFrames) bytes (64-byte aligned) filled on the host
+ * by agocuda_PixelChain_tensor_maps for the same program and frames (source and side planes
+ * need 16-byte aligned bases and strides).  Results are identical to
+ * agocuda_fused_PixelChain_U8 inside the chain's valid rectangle.  A block whose copies do not
+ * complete within a bounded wait sets AGOCUDA_PX_STATUS_TMA_TIMEOUT in *pStatus.  No
+ * counterpart in the reference (its OpenCL supernodes, ago_drama_alloc.cpp:484, load per
+ * work-item). */
+#define AGOCUDA_PX_STATUS_TMA_TIMEOUT 128u
+size_t agocuda_PixelChain_tensor_maps_size(uint32_t numFrames);
+int agocuda_PixelChain_tensor_maps(const agocuda_pixel_program *program, const agocuda_pixel_frame *framesHost,
+                                   uint32_t numFrames, void *mapsHost, size_t mapsBytes);
+int agocuda_fused_PixelChain_U8_tma(void *stream, const agocuda_pixel_program *program,
+                                    const agocuda_pixel_frame *frames, const void *maps, uint32_t numFrames,
+                                    uint32_t maxWidth, uint32_t maxHeight, uint32_t *pStatus);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1039,6 +1039,20 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
         if (!dev) return VX_ERROR_NO_MEMORY;
         cudaMemcpy(dev, fr.data(), fr.size() * sizeof(agocuda_pixel_frame), cudaMemcpyHostToDevice);
         const agocuda_pixel_program prog = c0.prog;
+        // TMA staging: one tensor map per plane of every frame, encoded now, kept on the device
+        uint8_t *maps = nullptr;
+        const size_t mapsPerFrame = agocuda_PixelChain_tensor_maps_size(1);
+        if (!(g->optimizer_flags & kOptNoTma)) {
+            const size_t mb = agocuda_PixelChain_tensor_maps_size((uint32_t)fr.size());
+            std::vector<uint64_t> host((mb + 7) / 8 + 8);
+            void *h = (void *)(((uintptr_t)host.data() + 63) & ~(uintptr_t)63);
+            if (agocuda_PixelChain_tensor_maps(&prog, fr.data(), (uint32_t)fr.size(), h, mb) == 0) {
+                maps = (uint8_t *)scratch(g, mb);
+                if (!maps) return VX_ERROR_NO_MEMORY;
+                cudaMemcpy(maps, h, mb, cudaMemcpyHostToDevice);
+            }
+        }
+        uint32_t *status = g->status_dev;
         std::vector<std::function<int(cudaStream_t)>> fns;
         for (size_t k0 = 0; k0 < fr.size(); k0 += kGroupFrames) {
             const size_t k1 = std::min(fr.size(), k0 + kGroupFrames);
@@ -1046,7 +1060,14 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
             for (size_t k = k0; k < k1; k++) { gw = std::max(gw, fr[k].width); gh = std::max(gh, fr[k].height); }
             const agocuda_pixel_frame *d0 = dev + k0;
             const uint32_t n = (uint32_t)(k1 - k0);
-            fns.push_back([=](cudaStream_t q) { return agocuda_fused_PixelChain_U8(S(q), &prog, d0, n, gw, gh); });
+            if (maps) {
+                const uint8_t *m0 = maps + k0 * mapsPerFrame;
+                fns.push_back([=](cudaStream_t q) {
+                    return agocuda_fused_PixelChain_U8_tma(S(q), &prog, d0, m0, n, gw, gh, status);
+                });
+            } else {
+                fns.push_back([=](cudaStream_t q) { return agocuda_fused_PixelChain_U8(S(q), &prog, d0, n, gw, gh); });
+            }
             Part pt{fns.back(), {}};
             for (size_t k = k0; k < k1; k++) for (LNode *nd : chains[k].nodes) pt.nodes.push_back(nd);
             st.parts.push_back(std::move(pt));

@@ -10,6 +10,7 @@
 // f16x2 min / max order exactly like the bytes.
 #include "agocuda_internal.cuh"
 
+#include <cuda.h>          // CUtensorMap and its enums (the encoder comes through the runtime)
 #include <mutex>
 
 uint64_t agocuda_count_launch(unsigned n);
@@ -218,7 +219,9 @@ extern "C" int agocuda_Threshold_U8_U8_Range(void *stream, uint32_t dstWidth, ui
 //
 // A block owns a 128x64 output tile.  It copies the input (and each side input of a binary
 // op) over the tile plus 16 columns and K rows on every side, K = number of 3x3 stages, into
-// shared memory with 16-byte cp.async copies, all in flight at once; each 3x3 stage shrinks
+// shared memory: with one TMA tensor copy per plane (cp.async.bulk.tensor.2d, box 160 x
+// (64 + 2K) bytes, completion counted on an mbarrier; rows and columns outside the image come
+// back as zeros), or in the other form with 16-byte cp.async copies; each 3x3 stage shrinks
 // the rows it produces by one on each side (the columns keep a margin of at least 4, enough
 // for K <= 4) and runs on 16-bit lanes of 8 pixels per thread; element-wise stages update in
 // place.  Pixels inside the chain's valid rectangle read only image pixels, so they equal
@@ -420,38 +423,91 @@ __device__ __forceinline__ uint32_t ew_word(int code, int sideFirst, int p0, int
     return v;
 }
 
-// dynamic shared memory: two buffers of BH x 40 words, then one per side input
-__global__ void __launch_bounds__(kPxThreads)
-k_pixel_chain(const agocuda_pixel_program prog, const agocuda_pixel_frame *__restrict__ frames, int K, int nSides)
+constexpr int kPxMapsPerFrame = 1 + AGOCUDA_PX_MAX_SIDES;   // tensor maps: source, then the side planes
+constexpr int kTmaWaitLimit = 1 << 20;                       // bounded mbarrier waits
+
+// words of one shared-memory plane; TMA destinations start on 128-byte boundaries
+__host__ __device__ constexpr int px_plane_words(int BH, bool tma)
 {
-    extern __shared__ uint32_t smem[];
+    return tma ? ((BH * kPxWords + 31) & ~31) : BH * kPxWords;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// dynamic shared memory: two buffers of BH x 40 words, then one per side input
+template <bool TMA>
+__global__ void __launch_bounds__(kPxThreads)
+k_pixel_chain(const agocuda_pixel_program prog, const agocuda_pixel_frame *__restrict__ frames,
+              const CUtensorMap *__restrict__ maps, int K, int nSides, uint32_t *status)
+{
+    extern __shared__ __align__(128) uint32_t smem[];
     __shared__ int4 sop[AGOCUDA_PX_MAX_OPS];            // code, side, sideFirst, p0 | p1 << 16
+    __shared__ __align__(8) uint64_t bar;
     const agocuda_pixel_frame f = frames[blockIdx.z];
     const int W = (int)f.width, H = (int)f.height;
     const int x0 = blockIdx.x * kPxTW, y0 = blockIdx.y * kPxTH, tid = threadIdx.x;
     if (x0 >= W || y0 >= H) return;
-    const int BH = kPxTH + 2 * K, plane = BH * kPxWords;
+    const int BH = kPxTH + 2 * K, plane = px_plane_words(BH, TMA);
     uint32_t *const buf0 = smem, *const buf1 = smem + plane;
     uint32_t *const side = smem + 2 * plane;
     if (tid < prog.numOps) {
         const agocuda_pixel_op &o = prog.ops[tid];
         sop[tid] = make_int4(o.code, o.side, o.sideFirst, (o.p0 & 0xffff) | (o.p1 << 16));
     }
-    // every 16-byte chunk of every plane in flight at once (cp.async, global -> shared); a
-    // chunk outside the row is read from inside it instead (its columns are outside the image)
-    for (int s = -1; s < nSides; s++) {
-        const agocuda_pixel_frame *fp = frames + blockIdx.z;   // side[s]: indexed in global memory
-        const uint8_t *base = s < 0 ? f.src : fp->side[s];
-        const int stride = (int)(s < 0 ? f.srcStride : fp->sideStride[s]);
-        uint32_t *dst = s < 0 ? buf0 : side + s * plane;
-        for (int i = tid; i < BH * kPxChunks; i += kPxThreads) {
-            const int r = i / kPxChunks, c = i - r * kPxChunks;
-            const int y = clampi(y0 - K + r, 0, H - 1), x = clampi(x0 - 16 + 16 * c, 0, stride - 16);
-            const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + r * kPxWords + 4 * c);
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(base + (size_t)y * stride + x) : "memory");
+    if constexpr (TMA) {
+        // one thread arms the barrier with the bytes of every plane and issues one tensor copy
+        // per plane, its box at columns x0-16 .. x0+143 and rows y0-K .. y0+63+K of this
+        // frame's plane (each plane has its own map); the block waits on the barrier
+        const uint32_t b = smem_u32(&bar);
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t bytes = (uint32_t)((1 + nSides) * BH * kPxWords * 4);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+            const CUtensorMap *m = maps + (size_t)blockIdx.z * kPxMapsPerFrame;
+            for (int s = -1; s < nSides; s++) {
+                const uint32_t d = smem_u32(s < 0 ? buf0 : side + s * plane);
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                    ::"r"(d), "l"((uint64_t)(m + 1 + s)), "r"(x0 - 16), "r"(y0 - K), "r"(b) : "memory");
+            }
+        }
+        bool done = false;
+        for (int i = 0; i < kTmaWaitLimit && !done; i++) done = mbar_try_wait(b, 0);
+        if (!done) {
+            // the copies did not complete: report it, give them one more bounded wait, leave
+            if (tid == 0) atomicOr(status, AGOCUDA_PX_STATUS_TMA_TIMEOUT);
+            for (int i = 0; i < kTmaWaitLimit && !done; i++) done = mbar_try_wait(b, 0);
+            return;
+        }
+    } else {
+        // every 16-byte chunk of every plane in flight at once (cp.async, global -> shared); a
+        // chunk outside the row is read from inside it instead (its columns are outside the image)
+        for (int s = -1; s < nSides; s++) {
+            const agocuda_pixel_frame *fp = frames + blockIdx.z;   // side[s]: indexed in global memory
+            const uint8_t *base = s < 0 ? f.src : fp->side[s];
+            const int stride = (int)(s < 0 ? f.srcStride : fp->sideStride[s]);
+            uint32_t *dst = s < 0 ? buf0 : side + s * plane;
+            for (int i = tid; i < BH * kPxChunks; i += kPxThreads) {
+                const int r = i / kPxChunks, c = i - r * kPxChunks;
+                const int y = clampi(y0 - K + r, 0, H - 1), x = clampi(x0 - 16 + 16 * c, 0, stride - 16);
+                const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + r * kPxWords + 4 * c);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(base + (size_t)y * stride + x) : "memory");
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     int cur = 0, st = 0;
     const int pp = 1 + tid % kPxPairs, grp = tid / kPxPairs;
@@ -501,45 +557,119 @@ k_pixel_chain(const agocuda_pixel_program prog, const agocuda_pixel_frame *__res
     }
 }
 
-}  // namespace
-
-extern "C" int agocuda_fused_PixelChain_U8(void *stream, const agocuda_pixel_program *program,
-                                           const agocuda_pixel_frame *frames, uint32_t numFrames, uint32_t maxWidth,
-                                           uint32_t maxHeight)
+// stencil count and side-plane count of a program; false when it is not a valid chain
+static bool chain_shape(const agocuda_pixel_program *program, int &K, int &nSides)
 {
-    if (!program || !frames || !numFrames || numFrames > 65535 || !maxWidth || !maxHeight || program->numOps < 1 ||
-        program->numOps > AGOCUDA_PX_MAX_OPS)
-        return AGOCUDA_INVALID_PARAMS;
-    int K = 0, nSides = 0;
+    K = 0;
+    nSides = 0;
+    if (!program || program->numOps < 1 || program->numOps > AGOCUDA_PX_MAX_OPS) return false;
     for (int k = 0; k < program->numOps; k++) {
         const agocuda_pixel_op &op = program->ops[k];
-        if (op.code < AGOCUDA_PX_NOT || op.code > AGOCUDA_PX_GAUSSIAN3x3) return AGOCUDA_INVALID_PARAMS;
+        if (op.code < AGOCUDA_PX_NOT || op.code > AGOCUDA_PX_GAUSSIAN3x3) return false;
         const bool stencil = op.code >= AGOCUDA_PX_BOX3x3;
         const bool binary = op.code >= AGOCUDA_PX_AND && op.code <= AGOCUDA_PX_SUB_SAT;
         if (stencil) K++;
         if (binary) {
-            if (op.side < 0 || op.side >= AGOCUDA_PX_MAX_SIDES) return AGOCUDA_INVALID_PARAMS;
+            if (op.side < 0 || op.side >= AGOCUDA_PX_MAX_SIDES) return false;
             nSides = op.side + 1 > nSides ? op.side + 1 : nSides;
         } else if (op.side >= AGOCUDA_PX_MAX_SIDES) {
-            return AGOCUDA_INVALID_PARAMS;
+            return false;
         }
     }
-    if (K > AGOCUDA_PX_MAX_STENCILS) return AGOCUDA_INVALID_PARAMS;
+    return K <= AGOCUDA_PX_MAX_STENCILS;
+}
+
+template <bool TMA>
+static int launch_chain(void *stream, const agocuda_pixel_program *program, const agocuda_pixel_frame *frames,
+                        const CUtensorMap *maps, uint32_t numFrames, uint32_t maxWidth, uint32_t maxHeight,
+                        uint32_t *pStatus)
+{
+    int K, nSides;
+    if (!chain_shape(program, K, nSides) || !frames || !numFrames || numFrames > 65535 || !maxWidth || !maxHeight)
+        return AGOCUDA_INVALID_PARAMS;
     agocuda_pixel_program p = *program;
     for (int k = 0; k < p.numOps; k++) {   // unary ops read no side operand
         const int c = p.ops[k].code;
         if (!(c >= AGOCUDA_PX_AND && c <= AGOCUDA_PX_SUB_SAT)) p.ops[k].side = -1;
     }
     dim3 grd(div_up(maxWidth, kPxTW), div_up(maxHeight, kPxTH), numFrames);
-    const size_t smem = (size_t)(2 + nSides) * (kPxTH + 2 * K) * kPxWords * sizeof(uint32_t);
+    const size_t smem = (size_t)(2 + nSides) * px_plane_words(kPxTH + 2 * K, TMA) * sizeof(uint32_t);
     static std::once_flag once;
     std::call_once(once, [] {   // up to 5 planes of 72 x 40 words: above the 48 KB default
-        cudaFuncSetAttribute(k_pixel_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (2 + AGOCUDA_PX_MAX_SIDES) * (kPxTH + 2 * AGOCUDA_PX_MAX_STENCILS) * kPxWords * 4);
+        cudaFuncSetAttribute(k_pixel_chain<TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (2 + AGOCUDA_PX_MAX_SIDES) * px_plane_words(kPxTH + 2 * AGOCUDA_PX_MAX_STENCILS, TMA) * 4);
     });
-    k_pixel_chain<<<grd, kPxThreads, smem, as_stream(stream)>>>(p, frames, K, nSides);
+    k_pixel_chain<TMA><<<grd, kPxThreads, smem, as_stream(stream)>>>(p, frames, maps, K, nSides, pStatus);
     agocuda_count_launch(1);
     return agocuda_launch_status();
+}
+
+}  // namespace
+
+extern "C" int agocuda_fused_PixelChain_U8(void *stream, const agocuda_pixel_program *program,
+                                           const agocuda_pixel_frame *frames, uint32_t numFrames, uint32_t maxWidth,
+                                           uint32_t maxHeight)
+{
+    return launch_chain<false>(stream, program, frames, nullptr, numFrames, maxWidth, maxHeight, nullptr);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiled encode_tiled()
+{
+    static EncodeTiled fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiled) nullptr;
+        return (EncodeTiled)p;
+    }();
+    return fn;
+}
+
+extern "C" size_t agocuda_PixelChain_tensor_maps_size(uint32_t numFrames)
+{
+    return (size_t)numFrames * kPxMapsPerFrame * sizeof(CUtensorMap);
+}
+
+extern "C" int agocuda_PixelChain_tensor_maps(const agocuda_pixel_program *program, const agocuda_pixel_frame *framesHost,
+                                              uint32_t numFrames, void *mapsHost, size_t mapsBytes)
+{
+    int K, nSides;
+    if (!chain_shape(program, K, nSides) || !framesHost || !numFrames || !mapsHost ||
+        ((uintptr_t)mapsHost & 63) || mapsBytes < agocuda_PixelChain_tensor_maps_size(numFrames))
+        return AGOCUDA_INVALID_PARAMS;
+    EncodeTiled enc = encode_tiled();
+    if (!enc) return AGOCUDA_INVALID_PARAMS;
+    CUtensorMap *maps = (CUtensorMap *)mapsHost;
+    memset(maps, 0, agocuda_PixelChain_tensor_maps_size(numFrames));
+    for (uint32_t i = 0; i < numFrames; i++) {
+        const agocuda_pixel_frame &f = framesHost[i];
+        for (int s = -1; s < nSides; s++) {
+            const uint8_t *base = s < 0 ? f.src : f.side[s];
+            const uint32_t stride = s < 0 ? f.srcStride : f.sideStride[s];
+            if (!base || ((uintptr_t)base & 15) || (stride & 15) || stride < f.width || !f.width || !f.height)
+                return AGOCUDA_INVALID_PARAMS;
+            const cuuint64_t dims[2] = {f.width, f.height}, strides[1] = {stride};
+            const cuuint32_t box[2] = {(cuuint32_t)(kPxWords * 4), (cuuint32_t)(kPxTH + 2 * K)}, estr[2] = {1, 1};
+            if (enc(&maps[i * kPxMapsPerFrame + 1 + s], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)base, dims, strides, box,
+                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return AGOCUDA_INVALID_PARAMS;
+        }
+    }
+    return 0;
+}
+
+extern "C" int agocuda_fused_PixelChain_U8_tma(void *stream, const agocuda_pixel_program *program,
+                                               const agocuda_pixel_frame *frames, const void *maps, uint32_t numFrames,
+                                               uint32_t maxWidth, uint32_t maxHeight, uint32_t *pStatus)
+{
+    if (!maps || ((uintptr_t)maps & 63) || !pStatus) return AGOCUDA_INVALID_PARAMS;
+    return launch_chain<true>(stream, program, frames, (const CUtensorMap *)maps, numFrames, maxWidth, maxHeight, pStatus);
 }
 
 // ---------------------------------------------------------------------------------

@@ -183,14 +183,20 @@ EXPECTED_PLAN = {
 }
 
 
+FORMS = {"tma": None, "cp_async": V.OPT_NO_TMA, "plain": V.OPT_NO_FUSION}
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("fuse", [True, False])
+@pytest.mark.parametrize("form", sorted(FORMS))
 @pytest.mark.parametrize("name", sorted(CHAINS))
-def test_engine_chain(cuda, name, fuse):
+def test_engine_chain(cuda, name, form):
+    """Fused chains with tiles staged by TMA tensor copies (the default) or by cp.async, and
+    the one-launch-per-node form, all equal the oracle on the valid rectangle."""
     api = V.OpenVX()
     sizes = [(1920, 1080), (37, 21), (640, 360), (129, 67), (8, 3)]
     frames = _frames(sizes, seed=7 * len(name))
-    res, plan = run_chains(api, CHAINS[name], frames, flags=None if fuse else V.OPT_NO_FUSION)
+    fuse = form != "plain"
+    res, plan = run_chains(api, CHAINS[name], frames, flags=FORMS[form])
     _check(res, CHAINS[name], frames)
     names = [s for s, _ in plan]
     if not fuse:
@@ -211,7 +217,7 @@ def test_engine_self_operand_splits_chain(cuda):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("flags", [None, V.OPT_NO_FUSION])
+@pytest.mark.parametrize("flags", [None, V.OPT_NO_TMA, V.OPT_NO_FUSION])
 def test_engine_motion_graph(cuda, flags):
     api = V.OpenVX()
     ctx = api.obj(api.vxCreateContext(), "context")
@@ -220,7 +226,7 @@ def test_engine_motion_graph(cuda, flags):
         pairs = [WL.motion_pair(seed=i + 1, width=w, height=h, rects=max(2, w * h // 20000)) for i, (w, h) in enumerate(sizes)]
         g = WL.MotionGraph(api, ctx, sizes, flags=flags)
         plan = api.plan(g.graph)
-        if flags is None:
+        if flags != V.OPT_NO_FUSION:
             assert plan == [("fused_PixelChain x11", 2)], plan
         for rep in range(2):
             g.run([f for p in pairs for f in p])
