@@ -492,6 +492,20 @@ uint32_t agocuda_ScaleGaussianHalf_tiles_shape(uint32_t dstWidth, uint32_t dstHe
 int agocuda_fused_ScaleGaussianHalf_persistent(void *stream, const agocuda_half_job *jobs, uint32_t numJobs,
                                                uint32_t totalTiles, uint32_t *queue, uint32_t threads, uint32_t rows,
                                                uint32_t blocksPerSM);
+/* TMA-staged form of the batch: a block of 112 threads makes 112 x 32 outputs of one level
+ * from one 256 x 68-byte source box copied by TMA onto an mbarrier (the box columns outside
+ * the row then take the bytes of AGO's buffer layout), so results equal the other forms bit
+ * for bit.  job j's tileBegin counts tiles of this shape (agocuda_ScaleGaussianHalf_tiles_tma);
+ * `maps` is a DEVICE array of numJobs 128-byte tensor maps (64-byte aligned) filled on the
+ * host by agocuda_ScaleGaussianHalf_tensor_maps from the same jobs.  A block whose copy does
+ * not complete within a bounded wait sets AGOCUDA_HALF_STATUS_TMA_TIMEOUT in *pStatus.  No
+ * counterpart in the reference. */
+#define AGOCUDA_HALF_STATUS_TMA_TIMEOUT 256u
+uint32_t agocuda_ScaleGaussianHalf_tiles_tma(uint32_t dstWidth, uint32_t dstHeight);
+int agocuda_ScaleGaussianHalf_tensor_maps(const agocuda_half_job *jobsHost, uint32_t numJobs, void *mapsHost,
+                                          size_t mapsBytes);
+int agocuda_fused_ScaleGaussianHalf_tma(void *stream, const agocuda_half_job *jobs, const void *maps, uint32_t numJobs,
+                                        uint32_t totalTiles, uint32_t *pStatus);
 
 /* ---------------------------------------------------------------- pyramidal LK */
 #define AGOCUDA_LK_MAX_LEVELS 12

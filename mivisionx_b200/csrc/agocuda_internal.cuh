@@ -1,5 +1,6 @@
 // agocuda_internal.cuh -- helpers shared by the sm_100a kernels behind include/agocuda.h.
 #pragma once
+#include <cuda.h>          // CUtensorMap and its enums (the encoder comes through the runtime)
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "agocuda.h"
@@ -19,6 +20,47 @@ static inline int agocuda_launch_status()
 static inline cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
 
 static inline unsigned div_up(unsigned a, unsigned b) { return (a + b - 1) / b; }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link); null
+// when the driver does not provide it.
+using agocuda_encode_tiled_fn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                             const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                             CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                             CUtensorMapFloatOOBfill);
+static inline agocuda_encode_tiled_fn agocuda_encode_tiled()
+{
+    static agocuda_encode_tiled_fn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (agocuda_encode_tiled_fn) nullptr;
+        return (agocuda_encode_tiled_fn)p;
+    }();
+    return fn;
+}
+
+// A 2D U8 tensor map of a pitched plane with a boxW x boxH box; zero fill outside the plane.
+static inline bool agocuda_u8_tensor_map(CUtensorMap *m, const void *base, uint32_t width, uint32_t height,
+                                         uint32_t stride, uint32_t boxW, uint32_t boxH)
+{
+    agocuda_encode_tiled_fn enc = agocuda_encode_tiled();
+    if (!enc || !base || ((uintptr_t)base & 15) || (stride & 15) || stride < width || !width || !height) return false;
+    const cuuint64_t dims[2] = {width, height}, strides[1] = {stride};
+    const cuuint32_t box[2] = {boxW, boxH}, estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+__device__ __forceinline__ uint32_t smem_addr_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbarrier_try_wait_parity(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
 
 // Multiprocessors of the current device (persistent kernels size their grid by it).
 static inline int agocuda_sm_count()

@@ -183,6 +183,55 @@ static vx_status lk_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step
 }
 
 // ScaleGaussianHalf levels of many images in one launch (one job per lowered node)
+// The TMA-staged batch: one launch per group of levels, source boxes copied by TMA through a
+// tensor map per level encoded here.  False when a level's planes cannot be mapped.
+static bool half_batch_tma(Graph *g, const std::vector<LNode *> &nodes, Step &st, vx_status &err)
+{
+    // groups of 16 levels: the groups are separate branches of the captured graph, and with
+    // frames from application buffers the first groups start while later frames upload
+    const size_t kGroupJobs = 2 * kGroupFrames;
+    std::vector<agocuda_half_job> jobs;
+    std::vector<uint32_t> group_tiles;
+    uint32_t tiles = 0;
+    for (size_t i = 0; i < nodes.size(); i++) {
+        if (i % kGroupJobs == 0 && i) { group_tiles.push_back(tiles); tiles = 0; }
+        const Image *d = IMG(nodes[i]->p[0]), *s = IMG(nodes[i]->p[1]);
+        jobs.push_back(agocuda_half_job{s->planes[0].dev, d->planes[0].dev, s->width, s->height, s->planes[0].dev_stride,
+                                        d->width, d->height, d->planes[0].dev_stride, tiles, 0});
+        tiles += agocuda_ScaleGaussianHalf_tiles_tma(d->width, d->height);
+    }
+    group_tiles.push_back(tiles);
+    const size_t mb = jobs.size() * 128;
+    std::vector<uint64_t> host(mb / 8 + 8);
+    void *h = (void *)(((uintptr_t)host.data() + 63) & ~(uintptr_t)63);
+    if (agocuda_ScaleGaussianHalf_tensor_maps(jobs.data(), (uint32_t)jobs.size(), h, mb) != 0) return false;
+    agocuda_half_job *dev = (agocuda_half_job *)scratch(g, jobs.size() * sizeof(agocuda_half_job));
+    uint8_t *maps = (uint8_t *)scratch(g, mb);
+    if (!dev || !maps) { err = VX_ERROR_NO_MEMORY; return true; }
+    if (cudaMemcpy(dev, jobs.data(), jobs.size() * sizeof(agocuda_half_job), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(maps, h, mb, cudaMemcpyHostToDevice) != cudaSuccess) {
+        err = VX_FAILURE;
+        return true;
+    }
+    uint32_t *status = g->status_dev;
+    std::vector<std::function<int(cudaStream_t)>> fns;
+    for (size_t k0 = 0, gi = 0; k0 < jobs.size(); k0 += kGroupJobs, gi++) {
+        const size_t k1 = std::min(jobs.size(), k0 + kGroupJobs);
+        const agocuda_half_job *d0 = dev + k0;
+        const uint8_t *m0 = maps + k0 * 128;
+        const uint32_t n = (uint32_t)(k1 - k0), t = group_tiles[gi];
+        fns.push_back([=](cudaStream_t q) { return agocuda_fused_ScaleGaussianHalf_tma(S(q), d0, m0, n, t, status); });
+        st.parts.push_back(Part{fns.back(), std::vector<LNode *>(nodes.begin() + k0, nodes.begin() + k1)});
+    }
+    st.num_kernels = (int)fns.size();
+    st.launch = [fns](cudaStream_t q) {
+        for (auto &f : fns) { int rc = f(q); if (rc) return rc; }
+        return 0;
+    };
+    err = VX_SUCCESS;
+    return true;
+}
+
 static vx_status half_batch_step(Graph *g, const std::vector<LNode *> &nodes, Step &st)
 {
     // launch shape from the autotuner's table (largest output of the batch): threads per
@@ -194,6 +243,10 @@ static vx_status half_batch_step(Graph *g, const std::vector<LNode *> &nodes, St
         if ((uint64_t)d->width * d->height > (uint64_t)bw * bh) { bw = d->width; bh = d->height; }
         const Image *root = s0->parent ? s0->parent : s0;
         if (root->import_type == VX_MEMORY_TYPE_HOST) streamed = true;
+    }
+    if (!(g->optimizer_flags & kOptNoTma)) {
+        vx_status err = VX_SUCCESS;
+        if (half_batch_tma(g, nodes, st, err)) return err;
     }
     std::vector<uint32_t> cfg = tune_lookup("ScaleGaussianHalf_U8_U8_5x5", bw, bh, {32, 8, 1, 0});
     if (cfg[3] && !agocuda_ScaleGaussianHalf_tiles_shape(bw, bh, cfg[0], cfg[1])) cfg = {32, 8, 1, 0};

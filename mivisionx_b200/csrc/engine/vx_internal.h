@@ -389,7 +389,7 @@ constexpr uint32_t kOptNoDivide = 0x1, kOptNoRemoveCopy = 0x2, kOptNoRemoveUnuse
 constexpr uint32_t kOptNoFusion = 0x00010000;       // one launch per lowered node ("plain" form)
 constexpr uint32_t kOptNoGraphCapture = 0x00020000; // launch steps directly instead of a CUDA graph
 constexpr uint32_t kOptSerial = 0x00040000;         // capture on one stream (no concurrent branches)
-constexpr uint32_t kOptNoTma = 0x00080000;          // fused pixel chains stage tiles with cp.async, not TMA
+constexpr uint32_t kOptNoTma = 0x00080000;          // pixel chains and pyramid levels load tiles without TMA
 
 // helpers implemented in vx_objects.cpp
 void add_ref(Context *ctx, Ref *r);

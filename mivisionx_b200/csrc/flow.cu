@@ -225,6 +225,129 @@ __global__ void __launch_bounds__(kHalfThreads) k_gauss_half_one(const agocuda_h
 }
 
 // ---------------------------------------------------------------------------------
+// TMA-staged form: a block of 112 threads produces 112 output columns x 32 output rows of one
+// level.  One tensor copy brings the source box -- columns 2*ox0-16 .. 2*ox0+239, rows
+// 2*oy0+ro-2 .. +67 -- into shared memory (completion on an mbarrier, bounded wait; the box
+// start column is a multiple of 16 bytes); box columns outside the row are then rewritten with
+// the bytes AGO's buffer layout holds there (ago_byte), so every output equals the register
+// form's.  A thread computes 8 output columns x 4 output rows from shared-memory words.
+// ---------------------------------------------------------------------------------
+constexpr int kHtCols = 112, kHtRows = 32, kHtThreads = 112;
+constexpr int kHtGroups = kHtCols / 8;                  // 14 column groups of 8 outputs
+constexpr int kHtRowsPerThread = kHtRows / (kHtThreads / kHtGroups);   // 4
+constexpr int kHtBoxW = 256, kHtBoxH = 2 * kHtRows + 4;
+constexpr int kHtWaitLimit = 1 << 20;
+
+template <int CO>
+__device__ __forceinline__ void half_rows_smem(const agocuda_half_job &J, const uint8_t (*tile)[kHtBoxW], int sx0,
+                                               int sy0, int ox, int oyA, int oyB)
+{
+    const int oW = (int)J.dstW, oH = (int)J.dstH;
+    const int ro = (J.srcH & 1) ? 0 : 1;
+    const int c0 = 2 * ox - 4 - sx0;                    // tile column of the thread's first word
+    uint32_t h[5][4];
+    int have = 0;
+    auto row_sum = [&](int r, uint32_t hq[4]) {
+        const uint32_t *p = (const uint32_t *)&tile[r][c0];
+        uint32_t w[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) w[k] = p[k];
+        half_hsum<CO>(w, hq);
+    };
+    for (int oy = oyA; oy < oyB; oy++) {
+        uint8_t *d = J.dst + (size_t)oy * J.dstStride + ox;
+        uint32_t out0 = 0, out1 = 0;
+        if (oy >= 1 && oy <= oH - 2) {
+            const int rc = 2 * oy + ro - sy0;           // centre source row, in the tile
+            if (have == 0) {
+#pragma unroll
+                for (int i = 0; i < 5; i++) row_sum(rc - 2 + i, h[i]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; q++) { h[0][q] = h[2][q]; h[1][q] = h[3][q]; h[2][q] = h[4][q]; }
+                row_sum(rc + 1, h[3]);
+                row_sum(rc + 2, h[4]);
+            }
+            have = 1;
+            uint32_t b[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t v = h[0][q] + h[4][q] + 6u * h[2][q] + 4u * (h[1][q] + h[3][q]);
+                b[q] = (v >> 8) & 0x00FF00FFu;
+            }
+            out0 = __byte_perm(b[0], b[1], 0x6420);
+            out1 = __byte_perm(b[2], b[3], 0x6420);
+        } else {
+            have = 0;
+        }
+        if (ox + 8 <= oW) {
+            *(uint2 *)d = make_uint2(out0, out1);
+        } else {
+            for (int i = 0; ox + i < oW; i++) d[i] = (uint8_t)((i < 4 ? out0 >> (8 * i) : out1 >> (8 * (i - 4))) & 0xFF);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kHtThreads) k_gauss_half_tma(const agocuda_half_job *jobs, const CUtensorMap *maps,
+                                                               uint32_t numJobs, uint32_t *status)
+{
+    __shared__ __align__(128) uint8_t tile[kHtBoxH][kHtBoxW];
+    __shared__ __align__(8) uint64_t bar;
+    uint32_t lo = 0, hi = numJobs - 1;
+    const uint32_t t = blockIdx.x;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].tileBegin <= t) lo = mid; else hi = mid - 1;
+    }
+    const agocuda_half_job J = jobs[lo];
+    const uint32_t local = t - J.tileBegin;
+    const uint32_t tilesX = (J.dstW + kHtCols - 1) / kHtCols;
+    const int ox0 = (int)(local % tilesX) * kHtCols, oy0 = (int)(local / tilesX) * kHtRows;
+    const int ro = (J.srcH & 1) ? 0 : 1;
+    const int sx0 = 2 * ox0 - 16, sy0 = 2 * oy0 + ro - 2;
+    const int tid = threadIdx.x;
+    const uint32_t b = smem_addr_u32(&bar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kHtBoxW * kHtBoxH) : "memory");
+        asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                     ::"r"(smem_addr_u32(&tile[0][0])), "l"((uint64_t)(maps + lo)), "r"(sx0), "r"(sy0), "r"(b) : "memory");
+    }
+    bool done = false;
+    for (int i = 0; i < kHtWaitLimit && !done; i++) done = mbarrier_try_wait_parity(b, 0);
+    if (!done) {
+        if (tid == 0) atomicOr(status, AGOCUDA_HALF_STATUS_TMA_TIMEOUT);
+        for (int i = 0; i < kHtWaitLimit && !done; i++) done = mbarrier_try_wait_parity(b, 0);
+        return;
+    }
+    // box columns the tile reads that lie outside the row take AGO's bytes: 16 on the left at
+    // most, on the right from the row end to the last column read
+    const int W = (int)J.srcW, H = (int)J.srcH;
+    const int cEnd = min(kHtBoxW, 2 * (min(ox0 + kHtCols, (int)J.dstW) - ox0) + 36);
+    const int lEnd = max(0, min(-sx0, cEnd)), rBeg = max(W - sx0, 0);
+    const int nL = lEnd, nR = max(0, cEnd - rBeg), per = nL + nR;
+    if (per > 0) {
+        const int rows = min(kHtBoxH, 2 * (min(oy0 + kHtRows, (int)J.dstH) - oy0) + 4);
+        for (int i = tid; i < rows * per; i += kHtThreads) {
+            const int r = i / per, k = i - r * per;
+            const int c = k < nL ? k : rBeg + (k - nL);
+            tile[r][c] = (uint8_t)ago_byte(J.src, (size_t)J.srcStride, W, H, sy0 + r, sx0 + c);
+        }
+        __syncthreads();
+    }
+    const int ox = ox0 + 8 * (tid % kHtGroups);
+    const int oyA = oy0 + kHtRowsPerThread * (tid / kHtGroups);
+    const int oyB = min(oyA + kHtRowsPerThread, (int)J.dstH);
+    if (ox >= (int)J.dstW || oyA >= oyB) return;
+    if (J.srcW & 1) half_rows_smem<0>(J, tile, sx0, sy0, ox, oyA, oyB);
+    else half_rows_smem<1>(J, tile, sx0, sy0, ox, oyA, oyB);
+}
+
+// ---------------------------------------------------------------------------------
 // Pyramidal LK
 // ---------------------------------------------------------------------------------
 constexpr int kLkWarps = 8;
@@ -673,6 +796,35 @@ extern "C" int agocuda_fused_ScaleGaussianHalf_batch(void *stream, const agocuda
 {
     if (!jobs || !numJobs || !totalTiles) return AGOCUDA_INVALID_PARAMS;
     k_gauss_half<<<totalTiles, kHalfThreads, 0, as_stream(stream)>>>(jobs, numJobs);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+extern "C" uint32_t agocuda_ScaleGaussianHalf_tiles_tma(uint32_t dstWidth, uint32_t dstHeight)
+{
+    return ((dstWidth + kHtCols - 1) / kHtCols) * ((dstHeight + kHtRows - 1) / kHtRows);
+}
+
+extern "C" int agocuda_ScaleGaussianHalf_tensor_maps(const agocuda_half_job *jobsHost, uint32_t numJobs, void *mapsHost,
+                                                     size_t mapsBytes)
+{
+    if (!jobsHost || !numJobs || !mapsHost || ((uintptr_t)mapsHost & 63) || mapsBytes < numJobs * sizeof(CUtensorMap))
+        return AGOCUDA_INVALID_PARAMS;
+    CUtensorMap *maps = (CUtensorMap *)mapsHost;
+    for (uint32_t i = 0; i < numJobs; i++) {
+        const agocuda_half_job &j = jobsHost[i];
+        if (!half_job_ok(j.dstW, j.dstH, j.dst, j.dstStride, j.srcW, j.srcH, j.src, j.srcStride) ||
+            !agocuda_u8_tensor_map(&maps[i], j.src, j.srcW, j.srcH, j.srcStride, kHtBoxW, kHtBoxH))
+            return AGOCUDA_INVALID_PARAMS;
+    }
+    return 0;
+}
+
+extern "C" int agocuda_fused_ScaleGaussianHalf_tma(void *stream, const agocuda_half_job *jobs, const void *maps,
+                                                   uint32_t numJobs, uint32_t totalTiles, uint32_t *pStatus)
+{
+    if (!jobs || !maps || ((uintptr_t)maps & 63) || !numJobs || !totalTiles || !pStatus) return AGOCUDA_INVALID_PARAMS;
+    k_gauss_half_tma<<<totalTiles, kHtThreads, 0, as_stream(stream)>>>(jobs, (const CUtensorMap *)maps, numJobs, pStatus);
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }

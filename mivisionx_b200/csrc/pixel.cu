@@ -10,7 +10,6 @@
 // f16x2 min / max order exactly like the bytes.
 #include "agocuda_internal.cuh"
 
-#include <cuda.h>          // CUtensorMap and its enums (the encoder comes through the runtime)
 #include <mutex>
 
 uint64_t agocuda_count_launch(unsigned n);
@@ -432,15 +431,8 @@ __host__ __device__ constexpr int px_plane_words(int BH, bool tma)
     return tma ? ((BH * kPxWords + 31) & ~31) : BH * kPxWords;
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
-    return ok != 0;
-}
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return smem_addr_u32(p); }
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) { return mbarrier_try_wait_parity(bar, parity); }
 
 // dynamic shared memory: two buffers of BH x 40 words, then one per side input
 template <bool TMA>
@@ -613,23 +605,6 @@ extern "C" int agocuda_fused_PixelChain_U8(void *stream, const agocuda_pixel_pro
     return launch_chain<false>(stream, program, frames, nullptr, numFrames, maxWidth, maxHeight, nullptr);
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
-using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-static EncodeTiled encode_tiled()
-{
-    static EncodeTiled fn = [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            return (EncodeTiled) nullptr;
-        return (EncodeTiled)p;
-    }();
-    return fn;
-}
-
 extern "C" size_t agocuda_PixelChain_tensor_maps_size(uint32_t numFrames)
 {
     return (size_t)numFrames * kPxMapsPerFrame * sizeof(CUtensorMap);
@@ -642,8 +617,6 @@ extern "C" int agocuda_PixelChain_tensor_maps(const agocuda_pixel_program *progr
     if (!chain_shape(program, K, nSides) || !framesHost || !numFrames || !mapsHost ||
         ((uintptr_t)mapsHost & 63) || mapsBytes < agocuda_PixelChain_tensor_maps_size(numFrames))
         return AGOCUDA_INVALID_PARAMS;
-    EncodeTiled enc = encode_tiled();
-    if (!enc) return AGOCUDA_INVALID_PARAMS;
     CUtensorMap *maps = (CUtensorMap *)mapsHost;
     memset(maps, 0, agocuda_PixelChain_tensor_maps_size(numFrames));
     for (uint32_t i = 0; i < numFrames; i++) {
@@ -651,13 +624,8 @@ extern "C" int agocuda_PixelChain_tensor_maps(const agocuda_pixel_program *progr
         for (int s = -1; s < nSides; s++) {
             const uint8_t *base = s < 0 ? f.src : f.side[s];
             const uint32_t stride = s < 0 ? f.srcStride : f.sideStride[s];
-            if (!base || ((uintptr_t)base & 15) || (stride & 15) || stride < f.width || !f.width || !f.height)
-                return AGOCUDA_INVALID_PARAMS;
-            const cuuint64_t dims[2] = {f.width, f.height}, strides[1] = {stride};
-            const cuuint32_t box[2] = {(cuuint32_t)(kPxWords * 4), (cuuint32_t)(kPxTH + 2 * K)}, estr[2] = {1, 1};
-            if (enc(&maps[i * kPxMapsPerFrame + 1 + s], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)base, dims, strides, box,
-                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            if (!agocuda_u8_tensor_map(&maps[i * kPxMapsPerFrame + 1 + s], base, f.width, f.height, stride, kPxWords * 4,
+                                       kPxTH + 2 * K))
                 return AGOCUDA_INVALID_PARAMS;
         }
     }

@@ -106,7 +106,7 @@ VX_KERNEL_BASE_USER = _enum_base(VX_ID_USER, 0)   # VX_KERNEL_BASE(VX_ID_USER, 0
 # optimizer flag bits this target adds to VX_GRAPH_ATTRIBUTE_AMD_OPTIMIZER_FLAGS
 OPT_NO_FUSION = 0x00010000        # one launch per lowered node ("plain" form)
 OPT_NO_GRAPH_CAPTURE = 0x00020000  # launch the steps directly instead of one CUDA graph
-OPT_NO_TMA = 0x00080000            # fused pixel chains stage tiles with cp.async instead of TMA
+OPT_NO_TMA = 0x00080000            # pixel chains and pyramid levels load their tiles without TMA
 
 
 # ---------------------------------------------------------------- structures
