@@ -4,10 +4,11 @@ with seeded random input frames instead of the reference's uniform images, so th
 output pixel depends on the input.
 
 Each case gives the data and node statements of its graph; `gdf(case, tmp, mode)` writes the
-text for one runvx run: mode "write" saves every output image (the reference run), mode
-"compare" checks every output image against those files with runvx's own compare facility
-(utilities/runvx/vxImage.cpp:599), inside the rectangle the reference defines (a stencil's
-border is undefined in OpenVX with border mode UNDEFINED)."""
+text for one runvx run: mode "write" saves every output image and keypoint array (the
+reference run), mode "compare" checks every output against those files with runvx's own
+compare facilities (utilities/runvx/vxImage.cpp:599 inside the rectangle the reference
+defines -- a stencil's border is undefined in OpenVX with border mode UNDEFINED --, and
+utilities/runvx/vxArray.cpp:462 for keypoints: coordinates exact, strengths within 1e-10)."""
 from __future__ import annotations
 
 import os
@@ -35,6 +36,7 @@ class Case:
     outputs: list                  # (data name, W, H, format, margin)
     lines: list = field(default_factory=list)    # other data statements
     node: str = ""
+    arrays: list = field(default_factory=list)   # keypoint array outputs: (data name, capacity)
 
 
 def _unary(name, kernel, fmt_in, fmt_out, margin=0, extra="", w=1920, h=1080, ow=None, oh=None, lines=()):
@@ -163,6 +165,25 @@ for gs in (3, 5, 7):
             f"node org.khronos.openvx.canny_edge_detector inter_luma input_hyst input_gradient_size !NORM_{norm} output_1"))
 
 
+# vision/: Harris at each gradient / block size and FAST with and without suppression, on a
+# seeded random 1280x720 frame (W % 16 == 0: the gradient and circle reads across row ends
+# reach the neighbouring rows); every corner of the list is compared
+for gs, tc in ((3, 1e-4), (5, 1e-3), (7, 1e-3)):
+    CASES.append(Case(
+        f"vision/Harris_{gs}x{gs}", [("input_1", 1280, 720, "U008")], [],
+        [f"data strength = scalar:FLOAT32,{tc}", "data min_distance = scalar:FLOAT32,6.0",
+         "data sensitivity = scalar:FLOAT32,0.05", f"data grad_size = scalar:INT32,{gs}",
+         f"data block_size = scalar:INT32,{gs}", "data num_corners = scalar:SIZE,0"],
+        "node org.khronos.openvx.harris_corners input_1 strength min_distance sensitivity grad_size block_size "
+        "output_1 num_corners", arrays=[("output_1", 60000)]))
+for sup in (0, 1):
+    CASES.append(Case(
+        f"vision/FastCorners_XY_U8_{'Supression' if sup else 'NoSupression'}", [("input_1", 1280, 720, "U008")], [],
+        ["data strength = scalar:FLOAT32,45.0", f"data nonmax = scalar:BOOL,{sup}", "data num_corners = scalar:SIZE,0"],
+        "node org.khronos.openvx.fast_corners input_1 strength nonmax output_1 num_corners",
+        arrays=[("output_1", 400000)]))
+
+
 def case_ids():
     return [c.name.split("/")[1] for c in CASES]
 
@@ -191,5 +212,8 @@ def gdf(case: Case, tmp: str, mode: str) -> str:
         else:
             io = f"COMPARE,{ref},rect{{{margin};{margin};{w - margin};{h - margin}}}"
         lines.append(f"data {name} = image:{w},{h},{fmt}:{io}")
+    for name, cap in case.arrays:
+        ref = os.path.join(tmp, f"ref_{name}.bin")
+        lines.append(f"data {name} = array:KEYPOINT,{cap}:{'WRITE' if mode == 'write' else 'COMPARE'},{ref}")
     lines.append(case.node)
     return "\n".join(lines) + "\n"

@@ -49,6 +49,9 @@ def test_reference_runvx_runs_case(tmp_path, case):
     for name, w, h, fmt, _ in case.outputs:
         p = os.path.join(tmp, f"ref_{name}.raw")
         assert os.path.getsize(p) == RC.frame_bytes(w, h, fmt), (name, out)
+    for name, cap in case.arrays:                  # vx_keypoint_t records, 28 bytes each
+        n = os.path.getsize(os.path.join(tmp, f"ref_{name}.bin"))
+        assert n % 28 == 0 and 0 < n // 28 <= cap, (name, n, out)
 
 
 @pytest.mark.gpu
@@ -63,4 +66,4 @@ def test_runvx_on_this_library_matches_reference(cuda, tmp_path, case):
     rc, out = _run(O.RUNVX_B200, RC.gdf(case, tmp, "compare"), tmp, "b200")
     assert rc == 0, out
     assert "MISMATCHED" not in out, out
-    assert out.count("COMPARE MATCHED") == len(case.outputs), out
+    assert out.count("COMPARE MATCHED") == len(case.outputs) + len(case.arrays), out
