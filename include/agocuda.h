@@ -354,6 +354,23 @@ int agocuda_fused_GaussSobelMagDepthThresh(void *stream, const agocuda_frame *fr
                                            uint32_t maxWidth, uint32_t maxHeight,
                                            int32_t shift, int32_t threshold);
 
+/* The same chain with each block's source tile copied into shared memory by one TMA tensor
+ * copy (cp.async.bulk.tensor.2d on an mbarrier) and the Sobel / threshold stage in exact
+ * fp32; output identical to agocuda_fused_GaussSobelMagDepthThresh.  `maps` is a DEVICE array
+ * of numFrames 128-byte tensor maps (64-byte aligned) that
+ * agocuda_fused_GaussSobelMagDepthThresh_tensor_maps encodes on the host from the same frame
+ * descriptors (each source row pointer 16-byte aligned, pitch a multiple of 16 bytes, the
+ * SobelMagnitude SIMD span's bounds multiples of 8; AGOCUDA_INVALID_PARAMS otherwise).  A
+ * block whose copy does not complete within a bounded wait sets
+ * AGOCUDA_C1_STATUS_TMA_TIMEOUT in *pStatus (device memory).  No counterpart in the reference. */
+#define AGOCUDA_C1_STATUS_TMA_TIMEOUT 512u
+size_t agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(uint32_t numFrames);
+int agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(const agocuda_frame *framesHost, uint32_t numFrames,
+                                                      void *mapsHost, size_t mapsBytes);
+int agocuda_fused_GaussSobelMagDepthThresh_tma(void *stream, const agocuda_frame *frames, const void *maps,
+                                               uint32_t numFrames, uint32_t maxWidth, uint32_t maxHeight,
+                                               int32_t shift, int32_t threshold, uint32_t *pStatus);
+
 /* The same chain as a persistent kernel: blocksPerSM x (number of SMs) resident blocks of
  * warpsPerBlock warps take tiles -- 256 columns x warpsPerBlock * rowsPerThread rows of one
  * frame -- from one queue over every frame of the batch, whatever their sizes, so uneven

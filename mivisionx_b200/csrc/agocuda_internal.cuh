@@ -52,6 +52,22 @@ static inline bool agocuda_u8_tensor_map(CUtensorMap *m, const void *base, uint3
                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// A 2D tensor map of a pitched U8 plane seen as rows of 32-bit elements (widthBytes rounded
+// up to whole elements, which must lie inside the row pitch), so that one box can span up to
+// 1024 bytes of a row; zero fill outside the plane.
+static inline bool agocuda_u8_as_u32_tensor_map(CUtensorMap *m, const void *base, uint32_t widthBytes, uint32_t height,
+                                                uint32_t stride, uint32_t boxWords, uint32_t boxH)
+{
+    agocuda_encode_tiled_fn enc = agocuda_encode_tiled();
+    const uint32_t words = (widthBytes + 3) / 4;
+    if (!enc || !base || ((uintptr_t)base & 15) || (stride & 15) || stride < 4 * words || !widthBytes || !height)
+        return false;
+    const cuuint64_t dims[2] = {words, height}, strides[1] = {stride};
+    const cuuint32_t box[2] = {boxWords, boxH}, estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, (void *)base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 __device__ __forceinline__ uint32_t smem_addr_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ bool mbarrier_try_wait_parity(uint32_t bar, uint32_t parity)

@@ -1164,6 +1164,20 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
             if (root->import_type == VX_MEMORY_TYPE_HOST) streamed = true;
         }
         const size_t group = streamed ? kGroupFrames : fr.size();
+        // TMA staging (the default): one tensor map per frame, encoded now, kept on the device
+        uint8_t *maps = nullptr;
+        const size_t mapBytes = agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(1);
+        if (!(g->optimizer_flags & kOptNoTma)) {
+            const size_t mb = agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size((uint32_t)fr.size());
+            std::vector<uint64_t> host((mb + 7) / 8 + 8);
+            void *h = (void *)(((uintptr_t)host.data() + 63) & ~(uintptr_t)63);
+            if (agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(fr.data(), (uint32_t)fr.size(), h, mb) == 0) {
+                maps = (uint8_t *)scratch(g, mb);
+                if (!maps) return VX_ERROR_NO_MEMORY;
+                cudaMemcpy(maps, h, mb, cudaMemcpyHostToDevice);
+            }
+        }
+        uint32_t *status = g->status_dev;
         std::vector<std::function<int(cudaStream_t)>> fns;
         for (size_t k0 = 0; k0 < fr.size(); k0 += group) {
             const size_t k1 = std::min(fr.size(), k0 + group);
@@ -1171,7 +1185,12 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
             for (size_t k = k0; k < k1; k++) { gw = std::max(gw, fr[k].width); gh = std::max(gh, fr[k].height); }
             const agocuda_frame *d0 = dev + k0;
             const uint32_t n = (uint32_t)(k1 - k0);
-            if (cfg[3]) {
+            if (maps) {
+                const uint8_t *m0 = maps + k0 * mapBytes;
+                fns.push_back([=](cudaStream_t q) {
+                    return agocuda_fused_GaussSobelMagDepthThresh_tma(S(q), d0, m0, n, gw, gh, shift, thr, status);
+                });
+            } else if (cfg[3]) {
                 // tile prefix of the group's frames, then the queue words
                 std::vector<uint32_t> pre(n + 1 + 2, 0);
                 for (uint32_t k = 0; k < n; k++)

@@ -8,6 +8,7 @@
 // contiguous bytes per row, so every global access is a full coalesced line.
 #include "agocuda_internal.cuh"
 #include <math.h>
+#include <string.h>
 
 namespace {
 
@@ -384,6 +385,153 @@ k_fused_c1_persistent(const agocuda_frame *frames, const uint32_t *tilePrefix, u
     queue_done(queue);
 }
 
+// ---------------------------------------------------------------------------------
+// TMA-staged form of the chain.  A block of 32 x kC1tBY threads owns 256 columns x
+// kC1tBY * kC1tRows output rows of one frame.  One thread copies the block's source box --
+// columns x0-16 .. x0+271, rows y0-2 .. y0 + kC1tBY * kC1tRows + 1 -- into shared memory with
+// one 2D tensor copy on an mbarrier: the plane is described to TMA as rows of 32-bit
+// elements, so a single 72-element box spans the 264 columns the tile reads (a box
+// dimension holds at most 256 elements); TMA writes zeros outside the plane.
+//
+// Each thread owns 8 columns and walks down kC1tRows rows.  The Gaussian stays in 16-bit
+// lanes as in the register form; the Sobel and the threshold test run in exact fp32 on the
+// FMA pipe instead of in lanes:
+//   t  = 6144 + G * 2^-7       the masked 16G lane dropped into the mantissa of 6144 (one permute)
+//   gx = [1 2 1]^T (t[c+1] - t[c-1]),  gy = [1 2 1] (t[r+1] - t[r-1])   = k * 2^-7, |k| <= 1020
+//   r  = T - gx^2 - gy^2,  T = (n_min - 1/2) * 2^-14                   multiples of 2^-15, |r| < 2^8
+// Every value is exact (t in [4096, 8192) has ulp 2^-11), so r < 0 <=> gx^2 + gy^2 >= n_min
+// in integers, r is never 0, and the sign byte of r replicated by one permute is the
+// output byte (255 where the chain's threshold passes).
+// ---------------------------------------------------------------------------------
+constexpr int kC1tRows = 36, kC1tBY = 2;
+constexpr int kC1tBoxW = 72;                            // 32-bit elements: 288 bytes per row
+constexpr int kC1tBoxH = kC1tBY * kC1tRows + 4;
+constexpr int kC1tWaitLimit = 1 << 20;                  // bounded mbarrier waits
+
+// t of the lo / hi 16-bit lane of a masked Gaussian word
+__device__ __forceinline__ float c1_tlo(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x45C00000u, 0x7610)); }
+__device__ __forceinline__ float c1_thi(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x45C00000u, 0x7632)); }
+
+// t at columns x-1 .. x+8 from the lane words (x, x+2), (x+1, x+3), (x+4, x+6), (x+5, x+7), (x-1, x+8)
+__device__ __forceinline__ void c1_tcols(const C1Row &g, float *t)
+{
+    t[0] = c1_tlo(g.b);  t[1] = c1_tlo(g.e1); t[2] = c1_tlo(g.o1); t[3] = c1_thi(g.e1); t[4] = c1_thi(g.o1);
+    t[5] = c1_tlo(g.e2); t[6] = c1_tlo(g.o2); t[7] = c1_thi(g.e2); t[8] = c1_thi(g.o2); t[9] = c1_thi(g.b);
+}
+
+// bytes 0 and 1: 0xFF where a (resp. b) is negative, else 0 (prmt sign-replicate selectors)
+__device__ __forceinline__ uint32_t c1_sign_pair(float a, float b)
+{
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, 0xFFFB;" : "=r"(r) : "r"(__float_as_uint(a)), "r"(__float_as_uint(b)));
+    return r;
+}
+
+// Output rows [ys, ye) of a thread's 8 columns at x (columns from W on are not stored), from
+// hrow(y): the lane sums of source row y (rows ys-2 .. ye+1 are asked for once each, in order).
+template <class HROW>
+__device__ __forceinline__ void c1t_rows(HROW &hrow, int ys, int ye, int x, int W, uint8_t *dst, uint32_t dstStride,
+                                         float T)
+{
+    // rolling rows of output row y: h of input rows y, y+1; t of rows y-1, y; d = t[c+1] - t[c-1]
+    // of row y; D = d(y-1) + d(y); all rotated by the 6-way unrolled loop
+    C1Row h0, h1, h2;
+    float t0[10], t1[10], t2[10], d0[8], d1[8], D0[8], D1[8];
+    {
+        const C1Row a = hrow(ys - 2), c = hrow(ys - 1);
+        h0 = hrow(ys);
+        h1 = hrow(ys + 1);
+        c1_tcols(c1_gauss(a, c, h0), t0);
+        c1_tcols(c1_gauss(c, h0, h1), t1);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            d0[j] = t1[j + 2] - t1[j];
+            D0[j] = (t0[j + 2] - t0[j]) + d0[j];
+        }
+    }
+    auto step = [&](int y, const C1Row &hA, const C1Row &hB, C1Row &hC, const float *tA, float *tC, const float *dB,
+                    float *dC, const float *DA, float *DB) {
+        hC = hrow(y + 2);
+        c1_tcols(c1_gauss(hA, hB, hC), tC);               // t of row y+1
+        float r[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            dC[j] = tC[j + 2] - tC[j];
+            DB[j] = dB[j] + dC[j];
+            const float gx = DA[j] + DB[j];
+            const float e0 = tC[j] - tA[j], e1 = tC[j + 1] - tA[j + 1], e2 = tC[j + 2] - tA[j + 2];
+            const float gy = __fmaf_rn(e1, 2.0f, e0) + e2;
+            r[j] = __fmaf_rn(-gx, gx, __fmaf_rn(-gy, gy, T));
+        }
+        const uint32_t lo = __byte_perm(c1_sign_pair(r[0], r[1]), c1_sign_pair(r[2], r[3]), 0x5410);
+        const uint32_t hi = __byte_perm(c1_sign_pair(r[4], r[5]), c1_sign_pair(r[6], r[7]), 0x5410);
+        uint8_t *o = dst + (size_t)y * dstStride + x;
+        if (x < W) *(uint32_t *)o = lo;
+        if (x + 4 < W) *(uint32_t *)(o + 4) = hi;
+    };
+    for (int y = ys; y < ye; y += 6) {                    // y is uniform across the thread's loop
+        step(y, h0, h1, h2, t0, t2, d0, d1, D0, D1);
+        if (y + 1 >= ye) break;
+        step(y + 1, h1, h2, h0, t1, t0, d1, d0, D1, D0);
+        if (y + 2 >= ye) break;
+        step(y + 2, h2, h0, h1, t2, t1, d0, d1, D0, D1);
+        if (y + 3 >= ye) break;
+        step(y + 3, h0, h1, h2, t0, t2, d1, d0, D1, D0);
+        if (y + 4 >= ye) break;
+        step(y + 4, h1, h2, h0, t1, t0, d0, d1, D0, D1);
+        if (y + 5 >= ye) break;
+        step(y + 5, h2, h0, h1, t2, t1, d1, d0, D1, D0);
+    }
+}
+
+__global__ void __launch_bounds__(32 * kC1tBY, 12)      // 80 registers: 12 blocks' worth per SM
+k_fused_c1_tma(const agocuda_frame *__restrict__ frames, const CUtensorMap *__restrict__ maps, float tRound,
+               float tTrunc, uint32_t *status)
+{
+    __shared__ __align__(128) uint32_t sm[kC1tBoxH * kC1tBoxW];
+    __shared__ __align__(8) uint64_t bar;
+    const int x0 = blockIdx.x * 256, y0 = 2 + blockIdx.y * (kC1tBY * kC1tRows);
+    const int lane = threadIdx.x, tid = threadIdx.x + 32 * threadIdx.y;
+    const uint32_t b = smem_addr_u32(&bar);
+    // the copy is issued before the frame descriptor arrives (the box depends on the block
+    // index only; a box outside a smaller frame of the batch reads zeros)
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kC1tBoxH * kC1tBoxW * 4)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+            ::"r"(smem_addr_u32(sm)), "l"((uint64_t)(maps + blockIdx.z)), "r"((x0 - 16) / 4), "r"(y0 - 2), "r"(b)
+            : "memory");
+    }
+    const agocuda_frame f = frames[blockIdx.z];
+    const int W = (int)f.width, H = (int)f.height;
+    __syncthreads();                                      // the barrier is initialised
+    bool done = false;
+    for (int i = 0; i < kC1tWaitLimit && !done; i++) done = mbarrier_try_wait_parity(b, 0);
+    if (!done) {
+        // the copy did not complete: report it, give it one more bounded wait, leave
+        if (tid == 0) atomicOr(status, AGOCUDA_C1_STATUS_TMA_TIMEOUT);
+        for (int i = 0; i < kC1tWaitLimit && !done; i++) done = mbarrier_try_wait_parity(b, 0);
+        return;
+    }
+    if (x0 >= W || y0 >= H - 2) return;                   // uniform over the block
+    const int x = x0 + 8 * lane, ys = y0 + (int)threadIdx.y * kC1tRows, ye = min(ys + kC1tRows, H - 2);
+    if (x >= W || ys >= ye) return;
+    // T of the thread's 8 columns: all in the SIMD body or all in a scalar part (the span's
+    // bounds are multiples of 8, checked when the tensor maps are made)
+    const float T = (x < f.simdBegin || x >= f.simdEnd) ? tTrunc : tRound;
+    // words of columns x-4 .. x+11 of source row yy: shared byte offset 12 + 8 lane in its box row
+    const uint32_t *col = sm + 3 + 2 * lane - (y0 - 2) * kC1tBoxW;
+    auto hrow = [&](int yy) {
+        const uint32_t *p = col + yy * kC1tBoxW;
+        const uint2 m = *(const uint2 *)(p + 1);
+        return c1_hsum(p[0], m.x, m.y, p[3]);
+    };
+    c1t_rows(hrow, ys, ye, x, W, f.dst, f.dstStride, T);
+}
+
 unsigned long long g_launches = 0;
 
 bool aligned(const void *p, unsigned a) { return ((uintptr_t)p & (a - 1)) == 0; }
@@ -479,6 +627,60 @@ extern "C" int agocuda_fused_GaussSobelMagDepthThresh(void *stream, const agocud
     }
     dim3 grd(div_up(maxWidth, kC1BX * 8), div_up(maxHeight - 4, kC1BY * kC1Rows), numFrames);
     k_fused_gauss_sobelmag_thresh<<<grd, dim3(kC1BX, kC1BY), 0, as_stream(stream)>>>(frames, (float)tRound, (float)tTrunc);
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
+}
+
+// ---- TMA-staged form
+static void c1_thresholds(int32_t shift, int32_t threshold, float &tRound, float &tTrunc)
+{
+    // T = (n_min - 1/2) * 2^-14 (exact: n_min <= 2^22); never-passing thresholds get a T
+    // above the largest gx^2 + gy^2 (2 * 1020^2 * 2^-14 < 128)
+    const int t = (int)(uint8_t)threshold;
+    tRound = tTrunc = 1024.0f;
+    if (t < 255) {
+        const long long M = (long long)(t + 1) << shift;
+        if (M <= 2048) {
+            tRound = (float)(((double)(M * M - M + 1) - 0.5) / 16384.0);
+            tTrunc = (float)(((double)(M * M) - 0.5) / 16384.0);
+        }
+    }
+}
+
+extern "C" size_t agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(uint32_t numFrames)
+{
+    return (size_t)numFrames * sizeof(CUtensorMap);
+}
+
+extern "C" int agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(const agocuda_frame *framesHost, uint32_t numFrames,
+                                                                 void *mapsHost, size_t mapsBytes)
+{
+    if (!framesHost || !numFrames || !mapsHost || ((uintptr_t)mapsHost & 63) ||
+        mapsBytes < agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(numFrames))
+        return AGOCUDA_INVALID_PARAMS;
+    CUtensorMap *maps = (CUtensorMap *)mapsHost;
+    memset(maps, 0, agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(numFrames));
+    for (uint32_t i = 0; i < numFrames; i++) {
+        const agocuda_frame &f = framesHost[i];
+        if (f.width < 5 || f.height < 5 || (f.simdBegin & 7) || (f.simdEnd & 7) ||
+            !agocuda_u8_as_u32_tensor_map(&maps[i], f.src, f.width, f.height, f.srcStride, kC1tBoxW, kC1tBoxH))
+            return AGOCUDA_INVALID_PARAMS;
+    }
+    return 0;
+}
+
+extern "C" int agocuda_fused_GaussSobelMagDepthThresh_tma(void *stream, const agocuda_frame *frames, const void *maps,
+                                                         uint32_t numFrames, uint32_t maxWidth, uint32_t maxHeight,
+                                                         int32_t shift, int32_t threshold, uint32_t *pStatus)
+{
+    if (!frames || !maps || ((uintptr_t)maps & 63) || !pStatus || !numFrames || numFrames > 65535 || maxWidth < 5 ||
+        maxHeight < 5 || shift < 0 || shift > 15)
+        return AGOCUDA_INVALID_PARAMS;
+    float tRound, tTrunc;
+    c1_thresholds(shift, threshold, tRound, tTrunc);
+    dim3 grd(div_up(maxWidth, 256), div_up(maxHeight - 4, kC1tBY * kC1tRows), numFrames);
+    k_fused_c1_tma<<<grd, dim3(32, kC1tBY), 0, as_stream(stream)>>>(frames, (const CUtensorMap *)maps, tRound, tTrunc,
+                                                                     pStatus);
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }

@@ -25,8 +25,11 @@ AGOCUDA_SIGNATURES = {
     "agocuda_ColorDepth_U8_S16_Sat": [vp, u32, u32, vp, u32, vp, u32, i32],
     "agocuda_Threshold_U8_U8_Binary": [vp, u32, u32, vp, u32, vp, u32, i32],
     "agocuda_fused_GaussSobelMagDepthThresh": [vp, vp, u32, u32, u32, i32, i32],
+    "agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size": [u32],
+    "agocuda_fused_GaussSobelMagDepthThresh_tensor_maps": [vp, u32, vp, C.c_size_t],
+    "agocuda_fused_GaussSobelMagDepthThresh_tma": [vp, vp, vp, u32, u32, u32, i32, i32, vp],
 }
-_RESTYPES = {"agocuda_launch_count": u64}
+_RESTYPES = {"agocuda_launch_count": u64, "agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size": C.c_size_t}
 
 
 class AgoFrame(C.Structure):

@@ -135,6 +135,50 @@ def test_fused_cfg1_batched_uneven(lib, cuda, rng, shift, thr):
         np.testing.assert_array_equal(got[sy:ey, sx:ex], ref[sy:ey, sx:ex], err_msg=f"{W}x{H}")
 
 
+@pytest.mark.parametrize("shift,thr", [(0, 128), (1, 40), (0, 0), (0, 255), (2, 10), (4, 127)])
+def test_fused_cfg1_tma_batched_uneven(lib, cuda, rng, shift, thr):
+    """The TMA-staged chain (tensor maps encoded on the host, fp32 Sobel stage): the same
+    uneven batch bit-exact in [2, W-2) x [2, H-2), including high-contrast frames whose
+    gradients reach the largest magnitudes, and no timeout status."""
+    import ctypes as C
+    import torch
+    from mivisionx_b200.native import AgoFrame
+    D = _dev()
+    sizes = [(1920, 1080), (37, 11), (640, 480), (20, 9), (130, 66), (300, 257)]
+    imgs, srcs, dsts, frames = [], [], [], []
+    for i, (W, H) in enumerate(sizes):
+        img = rng.integers(0, 256, (H, W), dtype=np.uint8) if i % 2 == 0 else \
+            (rng.integers(0, 2, (H, W)) * 255).astype(np.uint8)
+        s, d = D.DevImg(H, W).upload(img), D.DevImg(H, W)
+        imgs.append(img); srcs.append(s); dsts.append(d)
+        frames.append(AgoFrame(s.ptr, d.ptr, W, H, s.stride, d.stride, 0, W - (W % 16)))
+    n = len(frames)
+    mb = lib.agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(n)
+    assert mb == 128 * n
+    host = np.zeros(mb + 64, np.uint8)
+    off = (-host.ctypes.data) % 64
+    arr = (AgoFrame * n)(*frames)
+    assert lib.agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(arr, n, host.ctypes.data + off, mb) == 0
+    dmaps = torch.from_numpy(host[off:off + mb].copy()).cuda()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    fd = _frames_dev(frames)
+    mw, mh = max(w for w, _ in sizes), max(h for _, h in sizes)
+    assert lib.agocuda_fused_GaussSobelMagDepthThresh_tma(D.stream_ptr(), fd.data_ptr(), dmaps.data_ptr(), n, mw, mh,
+                                                          shift, thr, status.data_ptr()) == 0
+    for img, d, (W, H) in zip(imgs, dsts, sizes):
+        ref, (sx, sy, ex, ey) = OC.cfg1_chain(img, shift, thr)
+        got = d.download()
+        np.testing.assert_array_equal(got[sy:ey, sx:ex], ref[sy:ey, sx:ex], err_msg=f"{W}x{H}")
+    assert int(status.item()) == 0
+    # misaligned maps buffer and unaligned source pitch are refused
+    assert lib.agocuda_fused_GaussSobelMagDepthThresh_tma(D.stream_ptr(), fd.data_ptr(), dmaps.data_ptr() + 8, n, mw,
+                                                          mh, shift, thr, status.data_ptr()) == -10
+    bad = (AgoFrame * 1)(AgoFrame(srcs[0].ptr, dsts[0].ptr, 1920, 1080, 1928, dsts[0].stride, 0, 1920))
+    assert lib.agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(bad, 1, host.ctypes.data + off, mb) == -10
+    odd = (AgoFrame * 1)(AgoFrame(srcs[0].ptr, dsts[0].ptr, 1920, 1080, srcs[0].stride, dsts[0].stride, 4, 1920))
+    assert lib.agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(odd, 1, host.ctypes.data + off, mb) == -10
+
+
 def test_invalid_params(lib, cuda):
     D = _dev()
     assert lib.agocuda_Gaussian_U8_U8_3x3(D.stream_ptr(), 2, 2, 0, 16, 0, 16) == -10

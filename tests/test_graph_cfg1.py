@@ -47,7 +47,7 @@ def test_pcg32_known_answer():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("flags", [None, V.OPT_NO_FUSION, V.OPT_NO_GRAPH_CAPTURE])
+@pytest.mark.parametrize("flags", [None, V.OPT_NO_FUSION, V.OPT_NO_GRAPH_CAPTURE, V.OPT_NO_TMA])
 def test_engine_cfg1_uneven_batch(cuda, flags):
     api = V.OpenVX()
     ctx = api.obj(api.vxCreateContext(), "context")
@@ -55,7 +55,7 @@ def test_engine_cfg1_uneven_batch(cuda, flags):
     frames = [WL.cfg1_image(seed=i + 3, width=w, height=h) for i, (w, h) in enumerate(sizes)]
     g = WL.Cfg1Graph(api, ctx, sizes, 0, 128, flags=flags)
     plan = api.plan_text(g.graph)
-    if flags is None or flags == V.OPT_NO_GRAPH_CAPTURE:
+    if flags in (None, V.OPT_NO_GRAPH_CAPTURE, V.OPT_NO_TMA):
         assert plan.strip() == "fused_GaussSobelMagDepthThresh x4", plan
     else:
         assert "SobelMagnitude_S16_U8_3x3" in plan and "fused" not in plan, plan
