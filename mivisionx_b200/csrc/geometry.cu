@@ -328,6 +328,163 @@ __global__ void k_fused_rgb_yuv_scale(int W, int H, const uint8_t *src, int ss, 
     }
 }
 
+// The same outputs with one thread per 8 columns (four 2x2 blocks) walking down kCsRows block
+// rows: 64-bit loads of the 24 RGB bytes of each row and 64/32-bit stores of the planes where
+// the group lies in the SIMD body (x + 8 <= W & ~3, buffers aligned), and the Y of the row
+// above a block -- the area scaler's first row -- carried from the previous block row instead
+// of recomputed.  The arithmetic of each block is rgb_block's, so outputs are identical.
+//
+// In the SIMD body Y, U and V lie in [0, 256) (the weights of Y are positive and sum to 1; U
+// and V are at least 0.5), so trunc_sat16 and sat8 reduce to truncation, done as one
+// round-toward-zero add of 2^23 on the FMA pipe instead of a conversion on the XU pipe: the
+// word is 0x4B000000 + value.  The integer averages then run on those biased words (every
+// bias term divides by the shift that follows, modulo 2^32) and the low bytes are packed.
+constexpr int kCsRows = 8;
+constexpr uint32_t kBias23 = 0x4B000000u;
+
+__device__ __forceinline__ uint32_t trunc_b(float f) { return __float_as_uint(__fadd_rz(f, 8388608.0f)); }
+
+// Y of one pixel as rgb_block computes it, as a biased word (low byte = Y)
+__device__ __forceinline__ uint32_t rgb_y_b(int R, int G, int B, bool simd)
+{
+    if (simd) {
+        float fy, fu, fv;
+        rgb_yuv(R, G, B, fy, fu, fv);
+        return trunc_b(fy);
+    }
+    const float rg = __fadd_rn(__fmul_rn((float)R, 0.2126f), __fmul_rn((float)G, 0.7152f));
+    return kBias23 + (uint32_t)(uint8_t)__double2int_rz(__dadd_rn((double)rg, __dmul_rn((double)B, 0.0722)));
+}
+
+// rgb_block's SIMD body on biased words
+__device__ __forceinline__ void rgb_block_b(const int (&px)[4][3], uint32_t (&y)[4], uint32_t &U, uint32_t &V)
+{
+    uint32_t uu[4], vv[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        float fy, fu, fv;
+        rgb_yuv(px[i][0], px[i][1], px[i][2], fy, fu, fv);
+        y[i] = trunc_b(fy);
+        uu[i] = trunc_b(fu);
+        vv[i] = trunc_b(fv);
+    }
+    const uint32_t ua = (uu[0] + uu[2] + 1) >> 1, ub = (uu[1] + uu[3] + 1) >> 1;
+    const uint32_t va = (vv[0] + vv[2] + 1) >> 1, vb = (vv[1] + vv[3] + 1) >> 1;
+    U = (ua + ub + 1) >> 1;
+    V = (va + vb + 1) >> 1;
+}
+
+// the low bytes of four words
+__device__ __forceinline__ uint32_t pack_lo4(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+    return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
+}
+
+__global__ void __launch_bounds__(128)
+k_fused_rgb_yuv_scale8(int W, int H, const uint8_t *src, int ss, uint8_t *y1, int y1s, uint8_t *uv, int uvs,
+                       uint8_t *y2, int y2s, uint8_t *pu, int us, uint8_t *pv, int vs, uint8_t *outB, int obs,
+                       uint8_t *outA, int oas)
+{
+    const int g = blockIdx.x * 32 + threadIdx.x, x = 8 * g, bx0 = 4 * g;
+    const int by0 = (blockIdx.y * 4 + threadIdx.y) * kCsRows, nby = H / 2;
+    if (x >= W || by0 >= nby) return;
+    const int by1 = min(by0 + kCsRows, nby), simdEnd = W & ~3, scaleEnd = (W / 2) & ~7;
+    const bool full = x + 8 <= simdEnd;         // four blocks, SIMD-body arithmetic, vector access
+    const bool scaled = bx0 < scaleEnd;         // then all four blocks are below the bound (multiples of 4 / 8)
+    const int nb = min(4, (W - x) / 2);         // blocks of the group inside the image (W even)
+    uint32_t above[8];                          // Y of row 2 by - 1 (the area scaler's first row), biased
+    if (scaled && by0 > 0) {
+        const uint8_t *sp = src + (size_t)(2 * by0 - 1) * ss + 3 * x;
+#pragma unroll
+        for (int j = 0; j < 8; j++) above[j] = rgb_y_b(sp[3 * j], sp[3 * j + 1], sp[3 * j + 2], x + (j & ~1) < simdEnd);
+    }
+    // the 48 RGB bytes of a block row (full groups), loaded one block row ahead
+    uint32_t na[6], nb6[6];
+    auto load_rows = [&](int by) {
+        const uint8_t *s0 = src + (size_t)(2 * by) * ss + 3 * x, *s1 = s0 + ss;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const uint2 va = *(const uint2 *)(s0 + 8 * k), vb = *(const uint2 *)(s1 + 8 * k);
+            na[2 * k] = va.x; na[2 * k + 1] = va.y; nb6[2 * k] = vb.x; nb6[2 * k + 1] = vb.y;
+        }
+    };
+    if (full) load_rows(by0);
+    for (int by = by0; by < by1; by++) {
+        const int yr = 2 * by;
+        const uint8_t *s0 = src + (size_t)yr * ss + 3 * x, *s1 = s0 + ss;
+        uint32_t yy[4][4], U[4], V[4];          // biased words
+        if (full) {
+            uint32_t a[6], b[6];
+#pragma unroll
+            for (int k = 0; k < 6; k++) { a[k] = na[k]; b[k] = nb6[k]; }
+            if (by + 1 < by1) load_rows(by + 1);
+            auto byteA = [&](int k) { return (int)((a[k >> 2] >> (8 * (k & 3))) & 0xff); };
+            auto byteB = [&](int k) { return (int)((b[k >> 2] >> (8 * (k & 3))) & 0xff); };
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                int px[4][3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    px[0][c] = byteA(6 * i + c); px[1][c] = byteA(6 * i + 3 + c);
+                    px[2][c] = byteB(6 * i + c); px[3][c] = byteB(6 * i + 3 + c);
+                }
+                rgb_block_b(px, yy[i], U[i], V[i]);
+            }
+            const uint2 r0 = make_uint2(pack_lo4(yy[0][0], yy[0][1], yy[1][0], yy[1][1]),
+                                        pack_lo4(yy[2][0], yy[2][1], yy[3][0], yy[3][1]));
+            const uint2 r1 = make_uint2(pack_lo4(yy[0][2], yy[0][3], yy[1][2], yy[1][3]),
+                                        pack_lo4(yy[2][2], yy[2][3], yy[3][2], yy[3][3]));
+            *(uint2 *)(y1 + (size_t)yr * y1s + x) = r0;
+            *(uint2 *)(y1 + (size_t)(yr + 1) * y1s + x) = r1;
+            *(uint2 *)(y2 + (size_t)yr * y2s + x) = r0;
+            *(uint2 *)(y2 + (size_t)(yr + 1) * y2s + x) = r1;
+            *(uint2 *)(uv + (size_t)by * uvs + x) = make_uint2(pack_lo4(U[0], V[0], U[1], V[1]), pack_lo4(U[2], V[2], U[3], V[3]));
+            *(uint32_t *)(pu + (size_t)by * us + bx0) = pack_lo4(U[0], U[1], U[2], U[3]);
+            *(uint32_t *)(pv + (size_t)by * vs + bx0) = pack_lo4(V[0], V[1], V[2], V[3]);
+        } else {
+            for (int i = 0; i < nb; i++) {
+                const int xb = x + 2 * i;
+                int px[4][3], y4[4], u1, v1;
+                const uint8_t *p0 = s0 + 6 * i, *p1 = s1 + 6 * i;
+                for (int c = 0; c < 3; c++) { px[0][c] = p0[c]; px[1][c] = p0[3 + c]; px[2][c] = p1[c]; px[3][c] = p1[3 + c]; }
+                rgb_block(px, xb < simdEnd, y4, u1, v1);
+                for (int k = 0; k < 4; k++) yy[i][k] = kBias23 + (uint32_t)y4[k];
+                U[i] = kBias23 + (uint32_t)u1;
+                V[i] = kBias23 + (uint32_t)v1;
+                uint8_t *ya = y1 + (size_t)yr * y1s + xb, *yb = y2 + (size_t)yr * y2s + xb;
+                ya[0] = yb[0] = (uint8_t)y4[0]; ya[1] = yb[1] = (uint8_t)y4[1];
+                ya[y1s] = (uint8_t)y4[2]; ya[y1s + 1] = (uint8_t)y4[3];
+                yb[y2s] = (uint8_t)y4[2]; yb[y2s + 1] = (uint8_t)y4[3];
+                uint8_t *c = uv + (size_t)by * uvs + xb;
+                c[0] = (uint8_t)u1; c[1] = (uint8_t)v1;
+                pu[(size_t)by * us + bx0 + i] = (uint8_t)u1;
+                pv[(size_t)by * vs + bx0 + i] = (uint8_t)v1;
+            }
+        }
+        // half-size bilinear: two rounded stages below the bound, one stage beyond it; area:
+        // rows 2 by - 1 (0 for by = 0) and 2 by, below the bound only (biased words: the bias
+        // of a sum of two, 150 * 2^24, divides by 2; of four, 300 * 2^24 = 44 * 2^24 modulo 2^32, by 4)
+        if (scaled) {
+            uint32_t ob[4], oa[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t t1 = (yy[i][0] + yy[i][1] + 1) >> 1, t2 = (yy[i][2] + yy[i][3] + 1) >> 1;
+                ob[i] = (t1 + t2 + 1) >> 1;
+                const uint32_t ya = by == 0 ? yy[i][0] + yy[i][1] : above[2 * i] + above[2 * i + 1];
+                const uint32_t yb = by == 0 ? yy[i][2] + yy[i][3] : yy[i][0] + yy[i][1];
+                oa[i] = (ya + yb + 2) >> 2;
+                above[2 * i] = yy[i][2];
+                above[2 * i + 1] = yy[i][3];
+            }
+            *(uint32_t *)(outB + (size_t)by * obs + bx0) = pack_lo4(ob[0], ob[1], ob[2], ob[3]);
+            *(uint32_t *)(outA + (size_t)by * oas + bx0) = pack_lo4(oa[0], oa[1], oa[2], oa[3]);
+        } else {
+            for (int i = 0; i < nb; i++)
+                outB[(size_t)by * obs + bx0 + i] = (uint8_t)((yy[i][0] + yy[i][1] + yy[i][2] + yy[i][3] + 2) >> 2);
+        }
+    }
+}
+
 bool aligned(const void *p, unsigned a) { return ((uintptr_t)p & (a - 1)) == 0; }
 
 ScaleParams scale_params(int kind, uint32_t sW, uint32_t sH, uint32_t dW, uint32_t dH)
@@ -466,11 +623,23 @@ extern "C" int agocuda_fused_ColorScale_RGB(void *stream, uint32_t W, uint32_t H
     if (!pSrc || !pNV12Y || !pNV12UV || !pIYUVY || !pU || !pV || !pHalfBilinear || !pHalfArea || W < 16 || H < 4 ||
         (W & 1) || (H & 1) || srcStride < 3 * W)
         return AGOCUDA_INVALID_PARAMS;
-    dim3 blk(64, 4), grd(div_up(W / 2, 64), div_up(H / 2, 4));
-    k_fused_rgb_yuv_scale<<<grd, blk, 0, as_stream(stream)>>>((int)W, (int)H, pSrc, (int)srcStride, pNV12Y, (int)nv12YStride,
-                                                               pNV12UV, (int)nv12UVStride, pIYUVY, (int)iyuvYStride, pU,
-                                                               (int)uStride, pV, (int)vStride, pHalfBilinear, (int)hbStride,
-                                                               pHalfArea, (int)haStride);
+    // vector form: 8-byte aligned source, Y and UV rows, 4-byte aligned U, V and scaled rows
+    const bool vec = aligned(pSrc, 8) && srcStride % 8 == 0 && aligned(pNV12Y, 8) && nv12YStride % 8 == 0 &&
+                     aligned(pNV12UV, 8) && nv12UVStride % 8 == 0 && aligned(pIYUVY, 8) && iyuvYStride % 8 == 0 &&
+                     aligned(pU, 4) && uStride % 4 == 0 && aligned(pV, 4) && vStride % 4 == 0 &&
+                     aligned(pHalfBilinear, 4) && hbStride % 4 == 0 && aligned(pHalfArea, 4) && haStride % 4 == 0;
+    if (vec) {
+        dim3 blk(32, 4), grd(div_up(W / 8 + 1, 32), div_up(H / 2, 4 * kCsRows));
+        k_fused_rgb_yuv_scale8<<<grd, blk, 0, as_stream(stream)>>>(
+            (int)W, (int)H, pSrc, (int)srcStride, pNV12Y, (int)nv12YStride, pNV12UV, (int)nv12UVStride, pIYUVY,
+            (int)iyuvYStride, pU, (int)uStride, pV, (int)vStride, pHalfBilinear, (int)hbStride, pHalfArea, (int)haStride);
+    } else {
+        dim3 blk(64, 4), grd(div_up(W / 2, 64), div_up(H / 2, 4));
+        k_fused_rgb_yuv_scale<<<grd, blk, 0, as_stream(stream)>>>((int)W, (int)H, pSrc, (int)srcStride, pNV12Y,
+                                                                   (int)nv12YStride, pNV12UV, (int)nv12UVStride, pIYUVY,
+                                                                   (int)iyuvYStride, pU, (int)uStride, pV, (int)vStride,
+                                                                   pHalfBilinear, (int)hbStride, pHalfArea, (int)haStride);
+    }
     agocuda_count_launch(1);
     return agocuda_launch_status();
 }
