@@ -472,7 +472,7 @@ __device__ __forceinline__ uint32_t canny_pack_biased(uint32_t bx, uint32_t by)
 
 __device__ __forceinline__ int sG_mag3(uint32_t g) { return (int)(g | 3u); }   // (mag << 2) | 3: compares as mag
 
-__global__ void __launch_bounds__(256, 5)
+__global__ void __launch_bounds__(256, 6)
 k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, int lower, int upper,
                   uint8_t *__restrict__ dst, int dstStride, CannyTiles T, uint32_t *__restrict__ err)
 {
