@@ -394,7 +394,11 @@ int agocuda_fused_GaussSobelMagDepthThresh_persistent(void *stream, const agocud
  * it sees whole or holding a strong pixel, then unions of the components that cross tile
  * borders, their strong bits, and a pass that sets the remaining runs of strong components;
  * the 0/255 edge map is bit-identical to the unfused graph inside its valid region.
- * Scratch: agocuda_fused_CannyEdgeDetector_scratch_size(W, H) bytes. */
+ * Scratch: agocuda_fused_CannyEdgeDetector_scratch_size(W, H) bytes.  Where pSrc is 16-byte
+ * aligned and srcStride a multiple of 16 the front's input tiles are copied by TMA (a tensor
+ * map made by the call); a copy that does not complete within a bounded wait sets
+ * AGOCUDA_CANNY_STATUS_TMA_TIMEOUT in *pStatus. */
+#define AGOCUDA_CANNY_STATUS_TMA_TIMEOUT 1024u
 size_t agocuda_fused_CannyEdgeDetector_scratch_size(uint32_t width, uint32_t height);
 int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t width, uint32_t height,
                                            uint8_t *pDst, uint32_t dstStride, const uint8_t *pSrc, uint32_t srcStride,

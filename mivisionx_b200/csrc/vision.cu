@@ -7,6 +7,7 @@
 // first pixel of the next row when W % 16 == 0, else 0.  The values enter the interior
 // through non-maximum suppression and hysteresis, so `ago_px` reproduces them.
 #include "agocuda_internal.cuh"
+#include <string.h>
 
 #include <cooperative_groups.h>
 #include <cuda.h>
@@ -472,11 +473,19 @@ __device__ __forceinline__ uint32_t canny_pack_biased(uint32_t bx, uint32_t by)
 
 __device__ __forceinline__ int sG_mag3(uint32_t g) { return (int)(g | 3u); }   // (mag << 2) | 3: compares as mag
 
+// TMA form of the input tile: one box of 96 x 36 bytes, columns x0-16 .. x0+79 (a TMA box
+// starts on a 16-byte column), copied onto an mbarrier; word kInOffTma of a row is column x0-4
+constexpr int kInPitchTma = 24, kInOffTma = 3;
+constexpr int kCannyWaitLimit = 1 << 20;                 // bounded mbarrier waits
+
+template <bool TMA>
 __global__ void __launch_bounds__(256, 6)
 k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, int lower, int upper,
-                  uint8_t *__restrict__ dst, int dstStride, CannyTiles T, uint32_t *__restrict__ err)
+                  uint8_t *__restrict__ dst, int dstStride, CannyTiles T, uint32_t *__restrict__ err,
+                  const __grid_constant__ CUtensorMap map)
 {
-    __shared__ __align__(16) uint32_t sIn[kIH][kInWords];
+    constexpr int kPitch = TMA ? kInPitchTma : kInWords, kOff = TMA ? kInOffTma : 0;
+    __shared__ __align__(128) uint32_t sIn[kIH][kPitch];
     __shared__ __align__(16) uint16_t sG[kGH][kGC];
     __shared__ __align__(16) int sLab[kTS];
     __shared__ unsigned long long sNZ[kTH], sST[kTH];   // per tile row: non-zero / strong pixels
@@ -488,22 +497,35 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
 
     // ---- input words; words reaching outside the image follow the reference's reads
     // outside rows (ago_px), byte by byte
-    const bool al = (((uintptr_t)src | (uintptr_t)srcStride) & 3) == 0;
-    static_assert(kIH * kInWords <= 3 * 256, "three words per thread");
-#pragma unroll
-    for (int it = 0; it < 3; it++) {
-        const int i = tid + it * 256;
-        if (i >= kIH * kInWords) break;
-        const int r = i / kInWords, q = i - r * kInWords;
-        const int y = y0 - 2 + r, x = x0 - 4 + 4 * q;
-        uint32_t w;
-        if (al && (unsigned)y < (unsigned)H && x >= 0 && x + 4 <= W) {
-            w = __ldg((const uint32_t *)(src + (size_t)y * srcStride + x));
-        } else {
-            w = 0;
-            for (int k = 0; k < 4; k++) w |= (uint32_t)ago_px(src, srcStride, W, H, x + k, y) << (8 * k);
+    __shared__ __align__(8) uint64_t bar;
+    if constexpr (TMA) {
+        if (tid == 0) {
+            const uint32_t b = smem_addr_u32(&bar);
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kIH * kPitch * 4) : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                ::"r"(smem_addr_u32(&sIn[0][0])), "l"((uint64_t)&map), "r"(x0 - 16), "r"(y0 - 2), "r"(b) : "memory");
         }
-        sIn[r][q] = w;
+    } else {
+        const bool al = (((uintptr_t)src | (uintptr_t)srcStride) & 3) == 0;
+        static_assert(kIH * kInWords <= 3 * 256, "three words per thread");
+#pragma unroll
+        for (int it = 0; it < 3; it++) {
+            const int i = tid + it * 256;
+            if (i >= kIH * kInWords) break;
+            const int r = i / kInWords, q = i - r * kInWords;
+            const int y = y0 - 2 + r, x = x0 - 4 + 4 * q;
+            uint32_t w;
+            if (al && (unsigned)y < (unsigned)H && x >= 0 && x + 4 <= W) {
+                w = __ldg((const uint32_t *)(src + (size_t)y * srcStride + x));
+            } else {
+                w = 0;
+                for (int k = 0; k < 4; k++) w |= (uint32_t)ago_px(src, srcStride, W, H, x + k, y) << (8 * k);
+            }
+            sIn[r][q] = w;
+        }
     }
     if (tid < kTS / 32) { sStrongRoot[tid] = 0; sOpen[tid] = 0; }
     if (tid < kOpenMax / 32) sOpenStrong[tid] = 0;
@@ -517,6 +539,33 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
             : 0;
     }
     __syncthreads();
+    if constexpr (TMA) {
+        const uint32_t b = smem_addr_u32(&bar);
+        bool done = false;
+        for (int i = 0; i < kCannyWaitLimit && !done; i++) done = mbarrier_try_wait_parity(b, 0);
+        if (!__syncthreads_and(done)) {
+            // the copy did not complete: report it, give it one more bounded wait, leave
+            if (tid == 0) atomicOr(err, AGOCUDA_CANNY_STATUS_TMA_TIMEOUT);
+            for (int i = 0; i < kCannyWaitLimit && !done; i++) done = mbarrier_try_wait_parity(b, 0);
+            return;
+        }
+        // TMA writes zeros outside the plane, as ago_px reads except where the row pitch is W
+        // (W % 16 == 0): there column -1 is the previous row's last pixel and column W the next
+        // row's first
+        if ((W & 15) == 0) {
+            uint8_t *b8 = (uint8_t *)&sIn[0][0];
+            if (x0 == 0 && tid < kIH) {
+                const int y = y0 - 2 + tid;
+                b8[tid * kPitch * 4 + 15] = (y >= 1 && y < H) ? src[(size_t)(y - 1) * srcStride + W - 1] : 0;
+            }
+            const int cw = W - (x0 - 16);
+            if (cw < kPitch * 4 && tid >= 64 && tid < 64 + kIH) {
+                const int r = tid - 64, y = y0 - 2 + r;
+                b8[r * kPitch * 4 + cw] = (y >= 0 && y + 1 < H) ? src[(size_t)(y + 1) * srcStride] : 0;
+            }
+        }
+        __syncthreads();
+    }
 
     // ---- packed gradient, 4 columns per item, in 16-bit lanes
     for (int i = tid; i < kGH * kInWords; i += blockDim.x) {
@@ -526,7 +575,7 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
         if (y >= 1 && y < H - 1) {
             Lanes4 t, m, b;
             {
-                const uint32_t *r0 = sIn[gr], *r1 = sIn[gr + 1], *r2 = sIn[gr + 2];
+                const uint32_t *r0 = sIn[gr] + kOff, *r1 = sIn[gr + 1] + kOff, *r2 = sIn[gr + 2] + kOff;
                 const int ql = q > 0 ? q - 1 : q, qr = q + 1 < kInWords ? q + 1 : q;   // edge items: unused columns
                 t = lanes4(r0[ql], r0[q], r0[qr]);
                 m = lanes4(r1[ql], r1[q], r1[qr]);
@@ -551,7 +600,7 @@ k_canny_ccl_front(int W, int H, const uint8_t *__restrict__ src, int srcStride, 
             }
             if (xq == 0 && W >= 16) {      // the reference's SIMD-body formula at x = 0
                 const uint8_t *b8 = (const uint8_t *)sIn;
-                auto P = [&](int dx, int dy) { return (int)b8[(gr + 1 + dy) * (kInWords * 4) + 4 + dx]; };
+                auto P = [&](int dx, int dy) { return (int)b8[(gr + 1 + dy) * (kPitch * 4) + 4 * kOff + 4 + dx]; };
                 g0 = canny_grad(P, true, (W & 15) == 0 ? (int)sV[gr] : 0);
             }
             out0 = g0 | (g1 << 16);
@@ -1712,8 +1761,16 @@ extern "C" int agocuda_fused_CannyEdgeDetector_3x3_L1(void *stream, uint32_t W, 
     if (scratchBytes < canny_tiles_layout(W, H, scratch, &T)) return AGOCUDA_INVALID_PARAMS;
     cudaStream_t s = as_stream(stream);
     const int tiles = T.tilesX * T.tilesY, nodes = tiles * kOpenMax;
-    k_canny_ccl_front<<<dim3(T.tilesX, T.tilesY), 256, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper,
-                                                               pDst, (int)dstStride, T, pStatus);
+    // the input tiles come by TMA where the plane allows a tensor map (16-byte aligned rows);
+    // the map is a kernel parameter, so a captured launch keeps it
+    CUtensorMap map;
+    memset(&map, 0, sizeof(map));
+    if (agocuda_u8_tensor_map(&map, pSrc, W, H, srcStride, kInPitchTma * 4, kIH))
+        k_canny_ccl_front<true><<<dim3(T.tilesX, T.tilesY), 256, 0, s>>>(
+            (int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper, pDst, (int)dstStride, T, pStatus, map);
+    else
+        k_canny_ccl_front<false><<<dim3(T.tilesX, T.tilesY), 256, 0, s>>>(
+            (int)W, (int)H, pSrc, (int)srcStride, hystLower, hystUpper, pDst, (int)dstStride, T, pStatus, map);
     constexpr int kPer = kTH + kTW + kTH;
     k_canny_ccl_border<<<dim3(div_up(kPer, 128), tiles), 128, 0, s>>>((int)W, (int)H, T, pStatus);
     k_canny_ccl_flatten<<<div_up(nodes, 256), 256, 0, s>>>(T, nodes);

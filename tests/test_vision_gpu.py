@@ -121,16 +121,20 @@ def test_fused_canny(lib, cuda, W, H):
 
 
 @pytest.mark.parametrize("W,H,lo,hi", [(3, 3, 20, 40), (65, 33, 20, 40), (130, 70, 40, 200), (333, 97, 10, 30),
-                                       (1023, 517, 60, 120), (3840, 2160, 30, 90)])
-@pytest.mark.parametrize("dst_off", [0, 1])
-def test_fused_canny_dense(lib, cuda, W, H, lo, hi, dst_off):
+                                       (1023, 517, 60, 120), (3840, 2160, 30, 90), (64, 40, 20, 40),
+                                       (1024, 80, 10, 30)])
+@pytest.mark.parametrize("dst_off,src_off", [(0, 0), (1, 0), (0, 4)])
+def test_fused_canny_dense(lib, cuda, W, H, lo, hi, dst_off, src_off):
     """Noise with low thresholds: components of every shape cross tile borders, open runs
     without strong pixels wait for the patch pass, tiles hang over the right and bottom
-    image edges; an output plane starting off an 8-byte boundary takes the byte stores."""
+    image edges; an output plane starting off an 8-byte boundary takes the byte stores.  A
+    16-byte aligned source is staged by TMA (with W % 16 == 0 the bytes the reference reads
+    left of column 0 and at column W come from the neighbouring rows), a source 4 bytes off
+    by word loads."""
     D = _dev()
     img = np.random.default_rng(W * H + lo).integers(0, 256, (H, W), dtype=np.int32).astype(np.uint8)
     ref_edges = OC.canny_parts(img, lo, hi)[3]
-    src = D.DevImg(H, W).upload(img)
+    src = D.DevImg(H, W, align_off=src_off).upload(img)
     out = D.DevImg(H, W, align_off=dst_off)
     sb = lib.agocuda_fused_CannyEdgeDetector_scratch_size(W, H)
     scr, status = _buf(sb), _buf(4)
