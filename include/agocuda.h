@@ -418,7 +418,11 @@ int agocuda_fused_ColorScale_RGB(void *stream, uint32_t width, uint32_t height, 
  * window sums, score and non-maximum suppression from one read of the image) plus the
  * corner pick.  The candidate list holds ceil(W/2)*ceil(H/2) entries, the most the
  * suppression can emit, so no image overflows it.  Scratch:
- * agocuda_fused_HarrisCorners_scratch_size(W, H, minDistance) bytes. */
+ * agocuda_fused_HarrisCorners_scratch_size(W, H, minDistance) bytes.  Where pSrc is 16-byte
+ * aligned and srcStride a multiple of 16 the front end's source rows are copied by TMA (a
+ * tensor map made by the call); a copy that does not complete within a bounded wait sets
+ * AGOCUDA_HARRIS_STATUS_TMA_TIMEOUT in *pStatus. */
+#define AGOCUDA_HARRIS_STATUS_TMA_TIMEOUT 2048u
 size_t agocuda_fused_HarrisCorners_scratch_size(uint32_t width, uint32_t height, float minDistance);
 int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t width, uint32_t height, const uint8_t *pSrc, uint32_t srcStride,
                                     float sensitivity, float strengthThreshold, float normFactor, float minDistance,

@@ -1011,16 +1011,63 @@ __device__ __forceinline__ uint32_t harris_word(const uint8_t *src, int stride, 
 __device__ __forceinline__ float lane_lo(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8389632.0f; }
 __device__ __forceinline__ float lane_hi(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8389632.0f; }
 
+// TMA form: each warp copies its source rows ys-3 .. ys+kHRows+2, columns from (xs-4) rounded
+// down to 16 bytes, 144 bytes wide, into shared memory with one tensor copy on its own
+// mbarrier (the warps of a block are independent)
+constexpr int kHBoxW = 144, kHBoxH = kHRows + 6;
+constexpr int kHBoxSlot = (kHBoxH * kHBoxW + 127) & ~127;   // a TMA destination starts on 128 bytes
+
+template <bool TMA>
 __global__ void __launch_bounds__(128)
 k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, float k, float Tc, float norm,
-              uint64_t *list, uint32_t *count, uint32_t capacity)
+              uint64_t *list, uint32_t *count, uint32_t capacity, uint32_t *pStatus, const __grid_constant__ CUtensorMap map)
 {
-    const int lane = threadIdx.x & 31;
-    const int xs = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kHCols;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int xs = (blockIdx.x * (blockDim.x >> 5) + wib) * kHCols;
     if (xs >= W) return;                                   // warp-uniform
     const int xl = xs - 4 + 4 * lane;                      // this lane's columns xl .. xl+3
     const int ys = blockIdx.y * kHRows, yEnd = min(ys + kHRows, H);
     const bool fast = ((((uintptr_t)src | (uintptr_t)srcStride) & 3) == 0) && xl >= 0 && xl + 4 <= W;
+    __shared__ __align__(128) uint8_t sBox[TMA ? 4 : 1][TMA ? kHBoxSlot : 16];
+    static_assert(kHBoxSlot % 128 == 0, "each warp's box starts on a 128-byte boundary");
+    __shared__ __align__(8) uint64_t sBar[4];
+    const int bx = (xs - 4) & ~15;                         // box start column
+    if constexpr (TMA) {
+        const uint32_t b = smem_addr_u32(&sBar[wib]);
+        if (lane == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kHBoxH * kHBoxW) : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                ::"r"(smem_addr_u32(sBox[wib])), "l"((uint64_t)&map), "r"(bx), "r"(ys - 3), "r"(b) : "memory");
+        }
+        __syncwarp();
+        bool done = false;
+        for (int i = 0; i < kCannyWaitLimit && !done; i++) done = mbarrier_try_wait_parity(b, 0);
+        if (!__all_sync(0xffffffffu, done)) {
+            // the copy did not complete: report it, give it one more bounded wait, leave
+            if (lane == 0) atomicOr(pStatus, AGOCUDA_HARRIS_STATUS_TMA_TIMEOUT);
+            for (int i = 0; i < kCannyWaitLimit && !done; i++) done = mbarrier_try_wait_parity(b, 0);
+            return;
+        }
+        // TMA writes zeros outside the plane, as ago_px reads except where the row pitch is W
+        // (W % 16 == 0): column -1 is the previous row's last pixel, column W the next row's first
+        if ((W & 15) == 0) {
+            uint8_t *row = sBox[wib];
+            for (int i = lane; i < kHBoxH; i += 32) {
+                const int y = ys - 3 + i;
+                if (bx < 0) row[i * kHBoxW - 1 - bx] = (y >= 1 && y < H) ? src[(size_t)(y - 1) * srcStride + W - 1] : 0;
+                if (W - bx < kHBoxW) row[i * kHBoxW + W - bx] = (y >= 0 && y + 1 < H) ? src[(size_t)(y + 1) * srcStride] : 0;
+            }
+        }
+        __syncwarp();
+    }
+    // source word of this lane at row y
+    auto word = [&](int y) -> uint32_t {
+        if constexpr (TMA) return *(const uint32_t *)(sBox[wib] + (y - (ys - 3)) * kHBoxW + (xl - bx));
+        else return harris_word(src, srcStride, W, H, xl, y, fast);
+    };
     const bool outLane = lane >= 1 && lane <= 30;
     bool gradCol[4], scoreCol[4];
 #pragma unroll
@@ -1037,7 +1084,7 @@ k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, floa
     Lanes4 X[3] = {};
     float P[3][3][4] = {};
     float S[3][6] = {};
-    uint32_t next = harris_word(src, srcStride, W, H, xl, ys - 3, fast);
+    uint32_t next = word(ys - 3);
     const int rLast = yEnd + 2;
 
     // one input row r: t, m = rows r-2, r-1 (b receives row r); v0, v1 = products at
@@ -1047,7 +1094,7 @@ k_harris_rows(int W, int H, const uint8_t *__restrict__ src, int srcStride, floa
                     const float (&v1)[3][4], float (&p)[3][4], const float (&sA)[6], const float (&sB)[6],
                     float (&sc)[6]) {
         const uint32_t cur = next;
-        if (r + 1 <= rLast) next = harris_word(src, srcStride, W, H, xl, r + 1, fast);
+        if (r + 1 <= rLast) next = word(r + 1);
         b = lanes4(__shfl_up_sync(0xffffffffu, cur, 1), cur, __shfl_down_sync(0xffffffffu, cur, 1));
         // gradient at g = r - 1 (HafCpu_HarrisSobel_HG3_U8_3x3, harris.cpp:85)
         const int g = r - 1;
@@ -1878,8 +1925,17 @@ extern "C" int agocuda_fused_HarrisCorners_3x3(void *stream, uint32_t W, uint32_
     cudaStream_t s = as_stream(stream);
     cudaMemsetAsync(cnt, 0, 4, s);
     const int strips = (int)div_up(W, kHCols);
-    k_harris_rows<<<dim3(div_up(strips, 4), div_up(H, kHRows)), 128, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, sensitivity,
-                                                                             strengthThreshold, normFactor, list, cnt, cap);
+    // the source rows come by TMA where the plane allows a tensor map (16-byte aligned rows);
+    // the map is a kernel parameter, so a captured launch keeps it
+    CUtensorMap map;
+    memset(&map, 0, sizeof(map));
+    const dim3 grd(div_up(strips, 4), div_up(H, kHRows));
+    if (agocuda_u8_tensor_map(&map, pSrc, W, H, srcStride, kHBoxW, kHBoxH))
+        k_harris_rows<true><<<grd, 128, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, sensitivity, strengthThreshold,
+                                                normFactor, list, cnt, cap, pStatus, map);
+    else
+        k_harris_rows<false><<<grd, 128, 0, s>>>((int)W, (int)H, pSrc, (int)srcStride, sensitivity, strengthThreshold,
+                                                 normFactor, list, cnt, cap, pStatus, map);
     agocuda_count_launch(1);
     int rc = agocuda_launch_status();
     if (rc) return rc;

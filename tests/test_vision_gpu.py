@@ -180,13 +180,17 @@ def test_harris_kernels(lib, cuda, W, H):
         np.testing.assert_array_equal(got_c, ref_c)
 
 
-@pytest.mark.parametrize("W,H", [(200, 120), (1920, 1080), (3840, 2160)])
-def test_fused_harris(lib, cuda, W, H):
+@pytest.mark.parametrize("W,H,src_off", [(200, 120, 0), (1920, 1080, 0), (3840, 2160, 0), (64, 40, 0), (250, 70, 0),
+                                         (1920, 1080, 4), (250, 70, 1)])
+def test_fused_harris(lib, cuda, W, H, src_off):
+    """A 16-byte aligned source is staged by TMA (with W % 16 == 0 the bytes the reference
+    reads left of column 0 and at column W come from the neighbouring rows), a source 4 bytes
+    off by word loads, one 1 byte off byte by byte."""
     import torch
     D = _dev()
     img = _img(W, H, 9 * W + H)
     ref_c, ref_n = OC.harris(img, capacity=32768)
-    src = D.DevImg(H, W).upload(img)
+    src = D.DevImg(H, W, align_off=src_off).upload(img)
     sb = lib.agocuda_fused_HarrisCorners_scratch_size(W, H, 5.0)
     scr, corners, ccount, ncorn, status = _buf(sb), _buf(28 * 32768), _buf(4), _buf(4), _buf(4)
     base = scr.data_ptr() + (-scr.data_ptr() % 256)
