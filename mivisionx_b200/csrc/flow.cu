@@ -681,9 +681,11 @@ __device__ void lk_track_point(const agocuda_lk_frame &F, uint32_t pt, LkWarpSme
     (void)pStatus;
 }
 
-// 4 resident blocks (64 registers): the tracking loop is latency-bound, more warps beat the
-// few register spills this costs
-__global__ void __launch_bounds__(kLkWarps * 32, 4) k_lk_track(agocuda_lk_frame *frames, uint32_t *pStatus)
+// 8 resident blocks (64 warps per SM, 32 registers): the tracking loop is latency-bound (its
+// sums keep the reference's addition order, so each is one dependent chain), and more warps
+// beat the register spills this costs (measured: 2.79 ms per pyramid + LK step at 4 blocks,
+// 2.61 at 6, 2.55 at 8)
+__global__ void __launch_bounds__(kLkWarps * 32, 8) k_lk_track(agocuda_lk_frame *frames, uint32_t *pStatus)
 {
     __shared__ LkWarpSmem smem[kLkWarps];
     const agocuda_lk_frame &F = frames[blockIdx.y];
