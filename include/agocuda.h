@@ -370,6 +370,18 @@ int agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(const agocuda_frame *fram
 int agocuda_fused_GaussSobelMagDepthThresh_tma(void *stream, const agocuda_frame *frames, const void *maps,
                                                uint32_t numFrames, uint32_t maxWidth, uint32_t maxHeight,
                                                int32_t shift, int32_t threshold, uint32_t *pStatus);
+/* The same with the tile shape chosen: warpsPerBlock warps of rowsPerWarp output rows each
+ * (256 columns); rowsPerWarp in {18, 24, 36, 48}, warpsPerBlock in {1, 2, 4} but not 48 x 4
+ * (AGOCUDA_INVALID_PARAMS otherwise).  The maps must come from the _shape encoder with the
+ * same shape (a map's box height is the shape's).  The plain functions above use 36 x 2;
+ * the autotuner (mivisionx_b200/autotune.py) picks a shape per frame size. */
+int agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_shape(const agocuda_frame *framesHost, uint32_t numFrames,
+                                                            uint32_t rowsPerWarp, uint32_t warpsPerBlock,
+                                                            void *mapsHost, size_t mapsBytes);
+int agocuda_fused_GaussSobelMagDepthThresh_tma_shape(void *stream, const agocuda_frame *frames, const void *maps,
+                                                     uint32_t numFrames, uint32_t maxWidth, uint32_t maxHeight,
+                                                     int32_t shift, int32_t threshold, uint32_t rowsPerWarp,
+                                                     uint32_t warpsPerBlock, uint32_t *pStatus);
 
 /* The same chain as a persistent kernel: blocksPerSM x (number of SMs) resident blocks of
  * warpsPerBlock warps take tiles -- 256 columns x warpsPerBlock * rowsPerThread rows of one

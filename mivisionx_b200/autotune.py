@@ -10,8 +10,11 @@ warm-up launches, the median of 7), and keeps the fastest.  Every candidate's ou
 byte-identical to the default form's output on the same batch, or the candidate is dropped.
 
 Kernels and their parameters (the `params` of a table entry):
-* fused_GaussSobelMagDepthThresh (the configuration-1 chain): [rows per thread, warps per
-  block, resident blocks per SM, persistent]; persistent = 0 is the one-block-per-tile grid.
+* fused_GaussSobelMagDepthThresh_tma (the configuration-1 chain, TMA-staged: the default
+  form): [rows per warp, warps per block].
+* fused_GaussSobelMagDepthThresh (the configuration-1 chain, register form, used with the
+  no-TMA optimizer flag): [rows per thread, warps per block, resident blocks per SM,
+  persistent]; persistent = 0 is the one-block-per-tile grid.
 * ScaleGaussianHalf_U8_U8_5x5 (a Gaussian pyramid level): [threads per block, rows per
   thread, resident blocks per SM, persistent].
 """
@@ -44,6 +47,9 @@ def _lib():
         "agocuda_ScaleGaussianHalf_tiles": (u32, [u32, u32]),
         "agocuda_ScaleGaussianHalf_tiles_shape": (u32, [u32, u32, u32, u32]),
         "agocuda_fused_ScaleGaussianHalf_persistent": (C.c_int, [vp, vp, u32, u32, vp, u32, u32, u32]),
+        "agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size": (C.c_size_t, [u32]),
+        "agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_shape": (C.c_int, [vp, u32, u32, u32, vp, C.c_size_t]),
+        "agocuda_fused_GaussSobelMagDepthThresh_tma_shape": (C.c_int, [vp, vp, vp, u32, u32, u32, i32, i32, u32, u32, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -118,6 +124,49 @@ def tune_chain(L, W, H, quick=False):
     return results, n
 
 
+TMA_CHAIN_SHAPES = [(36, 2), (18, 1), (24, 1), (36, 1), (48, 1), (18, 2), (24, 2), (48, 2), (18, 4), (24, 4), (36, 4)]
+
+
+def tune_chain_tma(L, W, H, quick=False):
+    """The TMA-staged chain: every tile shape against the register grid form's output."""
+    import torch
+
+    from . import native
+    n = max(2, int(2 * L2_BYTES // (2 * W * H)) + 1)
+    stride = (W + 255) // 256 * 256
+    src = torch.randint(0, 256, (n, H, stride), dtype=torch.uint8, device="cuda")
+    dst = torch.zeros((n, H, stride), dtype=torch.uint8, device="cuda")
+    frames = (native.AgoFrame * n)()
+    for i in range(n):
+        frames[i] = native.AgoFrame(src[i].data_ptr(), dst[i].data_ptr(), W, H, stride, stride, 0, W - W % 16)
+    dframes = torch.frombuffer(bytearray(bytes(frames)), dtype=torch.uint8).cuda()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    _check(L.agocuda_fused_GaussSobelMagDepthThresh(sp, dframes.data_ptr(), n, W, H, 0, 128), "chain")
+    torch.cuda.synchronize()
+    want = dst.clone()
+    mb = L.agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(n)
+    results = []
+    for rows, warps in (TMA_CHAIN_SHAPES[:4] if quick else TMA_CHAIN_SHAPES):
+        host = np.zeros(mb + 64, np.uint8)
+        off = (-host.ctypes.data) % 64
+        _check(L.agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_shape(frames, n, rows, warps, host.ctypes.data + off, mb),
+               "tensor maps")
+        dmaps = torch.from_numpy(host[off:off + mb].copy()).cuda()
+
+        def run(rows=rows, warps=warps, dmaps=dmaps):
+            _check(L.agocuda_fused_GaussSobelMagDepthThresh_tma_shape(sp, dframes.data_ptr(), dmaps.data_ptr(), n, W, H, 0,
+                                                                      128, rows, warps, status.data_ptr()), "tma")
+        dst.zero_()
+        run()
+        torch.cuda.synchronize()
+        if not torch.equal(dst[:, 2:H - 2, 2:W - 2], want[:, 2:H - 2, 2:W - 2]) or int(status.item()):
+            continue
+        results.append(([rows, warps], _time(run, stream)))
+    return results, n
+
+
 # ------------------------------------------------------------------ pyramid level
 def tune_half(L, W, H, quick=False):
     """W x H: the source image of the level (the output is ceil(W/2) x ceil(H/2))."""
@@ -170,24 +219,34 @@ CHAIN_SHAPES = [(640, 480), (1280, 720), (1920, 1080), (3840, 2160)]
 HALF_SHAPES = [(3840, 2160), (1920, 1080), (1280, 720), (960, 540), (640, 480), (480, 270), (320, 240), (240, 135)]
 
 
-def run(out=DEFAULT_OUT, quick=False, log=print):
+def run(out=DEFAULT_OUT, quick=False, log=print, only=None):
+    """Tune every kernel (or only the named ones, keeping the other entries of the table at
+    `out`) and write the table."""
     import torch
     L = _lib()
     entries = []
-    for kernel, shapes, fn, px_of in (("fused_GaussSobelMagDepthThresh", CHAIN_SHAPES, tune_chain, lambda w, h: w * h),
+    if only and os.path.exists(out):
+        entries = [e for e in json.load(open(out))["entries"] if e["kernel"] not in only]
+    for kernel, shapes, fn, px_of in (("fused_GaussSobelMagDepthThresh_tma", CHAIN_SHAPES, tune_chain_tma, lambda w, h: w * h),
+                                      ("fused_GaussSobelMagDepthThresh", CHAIN_SHAPES, tune_chain, lambda w, h: w * h),
                                       ("ScaleGaussianHalf_U8_U8_5x5", HALF_SHAPES, tune_half,
                                        lambda w, h: ((w + 1) // 2) * ((h + 1) // 2))):
+        if only and kernel not in only:
+            continue
         for (W, H) in shapes:
             res, n = fn(L, W, H, quick)
+            default_us = res[0][1]                            # the first candidate is the default shape
             res.sort(key=lambda r: r[1])
             best, us = res[0]
-            grid_us = next(t for p, t in res if p[3] == 0)
+            grid_us = next((t for p, t in res if len(p) == 4 and p[3] == 0), default_us)
             key_w, key_h = (W, H) if kernel.startswith("fused") else ((W + 1) // 2, (H + 1) // 2)
             entries.append({"kernel": kernel, "width": key_w, "height": key_h, "params": best,
                             "us_per_launch": round(us, 2), "frames": n,
                             "gpx_per_s": round(px_of(W, H) * n / us / 1e3, 1),
-                            "grid_us_per_launch": round(grid_us, 2), "candidates": len(res)})
-            log(f"{kernel} {key_w}x{key_h}: {best} {us:.1f} us (grid form {grid_us:.1f} us, {len(res)} candidates)")
+                            "default_us_per_launch": round(default_us, 2), "candidates": len(res)})
+            if len(best) == 4:
+                entries[-1]["grid_us_per_launch"] = round(grid_us, 2)
+            log(f"{kernel} {key_w}x{key_h}: {best} {us:.1f} us (default {default_us:.1f} us, {len(res)} candidates)")
     table = {"device": torch.cuda.get_device_name(0), "sm_count": torch.cuda.get_device_properties(0).multi_processor_count,
              "generated_by": "python -m mivisionx_b200.autotune", "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
              "entries": entries}
@@ -201,8 +260,9 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.environ.get("AGO_B200_TUNE_FILE") or DEFAULT_OUT)
     ap.add_argument("--quick", action="store_true", help="a smaller search (for tests)")
+    ap.add_argument("--only", action="append", help="tune this kernel only (repeatable); the table's other entries stay")
     a = ap.parse_args(argv)
-    run(a.out, a.quick)
+    run(a.out, a.quick, only=a.only)
 
 
 if __name__ == "__main__":

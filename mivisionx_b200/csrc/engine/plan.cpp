@@ -1167,11 +1167,19 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
         // TMA staging (the default): one tensor map per frame, encoded now, kept on the device
         uint8_t *maps = nullptr;
         const size_t mapBytes = agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(1);
+        // its tile shape from the autotuner's table (rows per warp, warps per block)
+        std::vector<uint32_t> tshape = tune_lookup("fused_GaussSobelMagDepthThresh_tma", bw, bh, {36, 2});
         if (!(g->optimizer_flags & kOptNoTma)) {
             const size_t mb = agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size((uint32_t)fr.size());
             std::vector<uint64_t> host((mb + 7) / 8 + 8);
             void *h = (void *)(((uintptr_t)host.data() + 63) & ~(uintptr_t)63);
-            if (agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(fr.data(), (uint32_t)fr.size(), h, mb) == 0) {
+            int rc = agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_shape(fr.data(), (uint32_t)fr.size(), tshape[0],
+                                                                              tshape[1], h, mb);
+            if (rc != 0 && (tshape[0] != 36 || tshape[1] != 2)) {   // a shape this library does not build
+                tshape = {36, 2};
+                rc = agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_shape(fr.data(), (uint32_t)fr.size(), 36, 2, h, mb);
+            }
+            if (rc == 0) {
                 maps = (uint8_t *)scratch(g, mb);
                 if (!maps) return VX_ERROR_NO_MEMORY;
                 cudaMemcpy(maps, h, mb, cudaMemcpyHostToDevice);
@@ -1187,8 +1195,10 @@ static vx_status build_fused_batch(Graph *g, std::vector<Chain> &chains, Step &s
             const uint32_t n = (uint32_t)(k1 - k0);
             if (maps) {
                 const uint8_t *m0 = maps + k0 * mapBytes;
+                const uint32_t tr = tshape[0], tw = tshape[1];
                 fns.push_back([=](cudaStream_t q) {
-                    return agocuda_fused_GaussSobelMagDepthThresh_tma(S(q), d0, m0, n, gw, gh, shift, thr, status);
+                    return agocuda_fused_GaussSobelMagDepthThresh_tma_shape(S(q), d0, m0, n, gw, gh, shift, thr, tr, tw,
+                                                                           status);
                 });
             } else if (cfg[3]) {
                 // tile prefix of the group's frames, then the queue words

@@ -403,9 +403,11 @@ k_fused_c1_persistent(const agocuda_frame *frames, const uint32_t *tilePrefix, u
 // in integers, r is never 0, and the sign byte of r replicated by one permute is the
 // output byte (255 where the chain's threshold passes).
 // ---------------------------------------------------------------------------------
-constexpr int kC1tRows = 36, kC1tBY = 2;
+constexpr int kC1tRows = 36, kC1tBY = 2;              // default shape (rows per warp, warps per block)
 constexpr int kC1tBoxW = 72;                            // 32-bit elements: 288 bytes per row
-constexpr int kC1tBoxH = kC1tBY * kC1tRows + 4;
+__host__ __device__ constexpr int c1t_box_h(int rows, int by) { return by * rows + 4; }
+// resident blocks at 80 registers a thread (the launch bound of each shape)
+__host__ __device__ constexpr int c1t_min_blocks(int by) { return 65536 / (32 * by * 80); }
 constexpr int kC1tWaitLimit = 1 << 20;                  // bounded mbarrier waits
 
 // t of the lo / hi 16-bit lane of a masked Gaussian word
@@ -484,10 +486,12 @@ __device__ __forceinline__ void c1t_rows(HROW &hrow, int ys, int ye, int x, int 
     }
 }
 
-__global__ void __launch_bounds__(32 * kC1tBY, 12)      // 80 registers: 12 blocks' worth per SM
+template <int ROWS, int BY>
+__global__ void __launch_bounds__(32 * BY, c1t_min_blocks(BY))
 k_fused_c1_tma(const agocuda_frame *__restrict__ frames, const CUtensorMap *__restrict__ maps, float tRound,
                float tTrunc, uint32_t *status)
 {
+    constexpr int kC1tBoxH = c1t_box_h(ROWS, BY), kC1tRows = ROWS, kC1tBY = BY;
     __shared__ __align__(128) uint32_t sm[kC1tBoxH * kC1tBoxW];
     __shared__ __align__(8) uint64_t bar;
     const int x0 = blockIdx.x * 256, y0 = 2 + blockIdx.y * (kC1tBY * kC1tRows);
@@ -652,37 +656,74 @@ extern "C" size_t agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(uint32
     return (size_t)numFrames * sizeof(CUtensorMap);
 }
 
-extern "C" int agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(const agocuda_frame *framesHost, uint32_t numFrames,
-                                                                 void *mapsHost, size_t mapsBytes)
+// tile shapes of the TMA form (rows per warp, warps per block): the autotuner's space; a
+// shape's box (BY * ROWS + 4 rows of 288 bytes) stays within 48 KB of static shared memory
+#define C1T_SHAPES(X) X(18, 1) X(24, 1) X(36, 1) X(48, 1) X(18, 2) X(24, 2) X(36, 2) X(48, 2) X(18, 4) X(24, 4) X(36, 4)
+
+static bool c1t_shape_ok(uint32_t rows, uint32_t warps)
 {
-    if (!framesHost || !numFrames || !mapsHost || ((uintptr_t)mapsHost & 63) ||
+#define C1T_OK(R, B) if (rows == R && warps == B) return true;
+    C1T_SHAPES(C1T_OK)
+#undef C1T_OK
+    return false;
+}
+
+extern "C" int agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_shape(const agocuda_frame *framesHost,
+                                                                       uint32_t numFrames, uint32_t rowsPerWarp,
+                                                                       uint32_t warpsPerBlock, void *mapsHost,
+                                                                       size_t mapsBytes)
+{
+    if (!framesHost || !numFrames || !mapsHost || ((uintptr_t)mapsHost & 63) || !c1t_shape_ok(rowsPerWarp, warpsPerBlock) ||
         mapsBytes < agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(numFrames))
         return AGOCUDA_INVALID_PARAMS;
+    const uint32_t boxH = (uint32_t)c1t_box_h((int)rowsPerWarp, (int)warpsPerBlock);
     CUtensorMap *maps = (CUtensorMap *)mapsHost;
     memset(maps, 0, agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_size(numFrames));
     for (uint32_t i = 0; i < numFrames; i++) {
         const agocuda_frame &f = framesHost[i];
         if (f.width < 5 || f.height < 5 || (f.simdBegin & 7) || (f.simdEnd & 7) ||
-            !agocuda_u8_as_u32_tensor_map(&maps[i], f.src, f.width, f.height, f.srcStride, kC1tBoxW, kC1tBoxH))
+            !agocuda_u8_as_u32_tensor_map(&maps[i], f.src, f.width, f.height, f.srcStride, kC1tBoxW, boxH))
             return AGOCUDA_INVALID_PARAMS;
     }
     return 0;
+}
+
+extern "C" int agocuda_fused_GaussSobelMagDepthThresh_tensor_maps(const agocuda_frame *framesHost, uint32_t numFrames,
+                                                                 void *mapsHost, size_t mapsBytes)
+{
+    return agocuda_fused_GaussSobelMagDepthThresh_tensor_maps_shape(framesHost, numFrames, kC1tRows, kC1tBY, mapsHost,
+                                                                    mapsBytes);
+}
+
+extern "C" int agocuda_fused_GaussSobelMagDepthThresh_tma_shape(void *stream, const agocuda_frame *frames,
+                                                               const void *maps, uint32_t numFrames, uint32_t maxWidth,
+                                                               uint32_t maxHeight, int32_t shift, int32_t threshold,
+                                                               uint32_t rowsPerWarp, uint32_t warpsPerBlock,
+                                                               uint32_t *pStatus)
+{
+    if (!frames || !maps || ((uintptr_t)maps & 63) || !pStatus || !numFrames || numFrames > 65535 || maxWidth < 5 ||
+        maxHeight < 5 || shift < 0 || shift > 15 || !c1t_shape_ok(rowsPerWarp, warpsPerBlock))
+        return AGOCUDA_INVALID_PARAMS;
+    float tRound, tTrunc;
+    c1_thresholds(shift, threshold, tRound, tTrunc);
+    cudaStream_t s = as_stream(stream);
+    const CUtensorMap *m = (const CUtensorMap *)maps;
+#define C1T_LAUNCH(R, B)                                                                                           \
+    if (rowsPerWarp == R && warpsPerBlock == B)                                                                    \
+        k_fused_c1_tma<R, B><<<dim3(div_up(maxWidth, 256), div_up(maxHeight - 4, B * R), numFrames), dim3(32, B), 0, s>>>( \
+            frames, m, tRound, tTrunc, pStatus);
+    C1T_SHAPES(C1T_LAUNCH)
+#undef C1T_LAUNCH
+    agocuda_count_launch(1);
+    return agocuda_launch_status();
 }
 
 extern "C" int agocuda_fused_GaussSobelMagDepthThresh_tma(void *stream, const agocuda_frame *frames, const void *maps,
                                                          uint32_t numFrames, uint32_t maxWidth, uint32_t maxHeight,
                                                          int32_t shift, int32_t threshold, uint32_t *pStatus)
 {
-    if (!frames || !maps || ((uintptr_t)maps & 63) || !pStatus || !numFrames || numFrames > 65535 || maxWidth < 5 ||
-        maxHeight < 5 || shift < 0 || shift > 15)
-        return AGOCUDA_INVALID_PARAMS;
-    float tRound, tTrunc;
-    c1_thresholds(shift, threshold, tRound, tTrunc);
-    dim3 grd(div_up(maxWidth, 256), div_up(maxHeight - 4, kC1tBY * kC1tRows), numFrames);
-    k_fused_c1_tma<<<grd, dim3(32, kC1tBY), 0, as_stream(stream)>>>(frames, (const CUtensorMap *)maps, tRound, tTrunc,
-                                                                     pStatus);
-    agocuda_count_launch(1);
-    return agocuda_launch_status();
+    return agocuda_fused_GaussSobelMagDepthThresh_tma_shape(stream, frames, maps, numFrames, maxWidth, maxHeight, shift,
+                                                           threshold, kC1tRows, kC1tBY, pStatus);
 }
 
 // ---- persistent form and its tuning space

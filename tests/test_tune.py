@@ -62,18 +62,47 @@ def test_committed_table_is_well_formed():
         pytest.skip("no committed table")
     t = json.load(open(path))
     kernels = {e["kernel"] for e in t["entries"]}
-    assert {"fused_GaussSobelMagDepthThresh", "ScaleGaussianHalf_U8_U8_5x5"} <= kernels
+    assert {"fused_GaussSobelMagDepthThresh_tma", "fused_GaussSobelMagDepthThresh", "ScaleGaussianHalf_U8_U8_5x5"} <= kernels
     for e in t["entries"]:
-        assert len(e["params"]) == 4 and e["width"] > 0 and e["height"] > 0
+        n = 2 if e["kernel"].endswith("_tma") else 4
+        assert len(e["params"]) == n and e["width"] > 0 and e["height"] > 0
+        if e["kernel"].endswith("_tma"):
+            rows, warps = e["params"]
+            assert rows in (18, 24, 36, 48) and warps in (1, 2, 4) and (rows, warps) != (48, 4)
 
 
 CHAIN_SHAPES = [[18, 4, 6, 0], [6, 2, 1, 1], [12, 8, 3, 1], [24, 4, 2, 1], [18, 2, 12, 1]]
 HALF_SHAPES = [[32, 8, 1, 0], [32, 2, 16, 1], [64, 4, 4, 1], [128, 8, 1, 1], [128, 2, 4, 1]]
 
 
+TMA_CHAIN_SHAPES = [[36, 2], [18, 1], [24, 1], [36, 1], [48, 1], [18, 2], [24, 2], [48, 2], [18, 4], [24, 4], [36, 4]]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("params", TMA_CHAIN_SHAPES)
+def test_tma_chain_shapes_match_oracle(cuda, table, params):
+    """Every tile shape of the TMA-staged chain, taken from the table by the engine."""
+    import oracle_chains as OC
+    table([{"kernel": "fused_GaussSobelMagDepthThresh_tma", "width": 1920, "height": 1080, "params": params}])
+    api = V.OpenVX()
+    ctx = api.obj(api.vxCreateContext(), "context")
+    try:
+        sizes = [(1920, 1080), (640, 480), (333, 97), (1920, 1080), (64, 48), (3840, 2160)]
+        frames = [WL.cfg1_image(seed=50 + i, width=w, height=h) for i, (w, h) in enumerate(sizes)]
+        g = WL.Cfg1Graph(api, ctx, sizes)
+        for _ in range(2):
+            g.run(frames)
+            for out, img in zip(g.results(), frames):
+                ref, (sx, sy, ex, ey) = OC.cfg1_chain(img, 0, 128)
+                np.testing.assert_array_equal(out[0][sy:ey, sx:ex], ref[sy:ey, sx:ex])
+    finally:
+        api.vxReleaseContext(C.byref(C.c_void_p(ctx)))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("params", CHAIN_SHAPES)
 def test_chain_shapes_match_oracle(cuda, table, params):
+    """The register form's shapes (the no-TMA optimizer flag selects that form)."""
     import oracle_chains as OC
     table([{"kernel": "fused_GaussSobelMagDepthThresh", "width": 1920, "height": 1080, "params": params}])
     api = V.OpenVX()
@@ -81,7 +110,7 @@ def test_chain_shapes_match_oracle(cuda, table, params):
     try:
         sizes = [(1920, 1080), (640, 480), (333, 97), (1920, 1080), (64, 48)]
         frames = [WL.cfg1_image(seed=30 + i, width=w, height=h) for i, (w, h) in enumerate(sizes)]
-        g = WL.Cfg1Graph(api, ctx, sizes)
+        g = WL.Cfg1Graph(api, ctx, sizes, flags=V.OPT_NO_TMA)
         for _ in range(2):      # the queue words must be back to zero for the second launch
             g.run(frames)
             for out, img in zip(g.results(), frames):
