@@ -231,7 +231,9 @@ __global__ void k_warp_affine_bilinear(int W4, int H, uint8_t *dst, int ds, int 
         fy[k] = __fsub_rn(ys, (float)yi);
         ok[k] = !a.checkBorder || (xs >= 0.f && xs < (float)sW && ys >= 0.f && ys < (float)sH);
         int py, pxx;
-        if (yi >= 0 && yi < sH && xi >= 0 && xi < ss) {          // flat index inside, no wrap
+        if (!ok[k]) {                                          // outside the source: the border value, no reads
+            py = 0; pxx = 0;
+        } else if (yi >= 0 && yi < sH && xi >= 0 && xi < ss) { // flat index inside, no wrap
             py = yi; pxx = xi;
         } else {                                               // the reference clamps the flat index
             long long idx = (long long)yi * ss + xi;
@@ -245,7 +247,9 @@ __global__ void k_warp_affine_bilinear(int W4, int H, uint8_t *dst, int ds, int 
     int q[4][4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        if (t[k].direct) {
+        if (!ok[k]) {
+            q[k][0] = q[k][1] = q[k][2] = q[k][3] = 0;
+        } else if (t[k].direct) {
             q[k][0] = t[k].p[0]; q[k][1] = t[k].p[1]; q[k][2] = t[k].p[ss]; q[k][3] = t[k].p[ss + 1];
         } else {   // the reference reads 4 bytes at the (clamped) index and at index + stride
             q[k][0] = ago_px8(src, ss, sW, sH, t[k].px, t[k].py);
