@@ -997,7 +997,7 @@ __global__ void k_harris_nms(int W, int H, const float *sc, int scStride, uint64
 // below 2^24, i.e. exactly the float sums the reference forms in any order.  The score
 // keeps the reference's float operation order, and its division is skipped only where the
 // result cannot exceed the threshold.
-constexpr int kHRows = 32, kHCols = 120;
+constexpr int kHRows = 64, kHCols = 120;
 
 __device__ __forceinline__ uint32_t harris_word(const uint8_t *src, int stride, int W, int H, int x, int y, bool fast)
 {
